@@ -1,0 +1,211 @@
+"""azimuth_b200: B200-native render path for azimuth scenes.
+
+Python access to the C-ABI of ``libazimuth_b200.so`` (include/azimuth_gpu.h,
+include/azimuth_scenes.h).  The render work runs only in the native library's
+CUDA kernels; if the library or a GPU is missing, calls raise.
+
+Typical use::
+
+    from azimuth_b200 import generate_scene, GpuScene
+    sc = generate_scene(0, seed=0, width=256, height=256, spp=16)
+    with GpuScene(sc) as g:
+        film = g.render(sc)              # numpy (H, W, 4): rgb sum, weight sum
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _native
+from ._native import GenParams, GeneratedScene, RenderOpts, RenderStats, Scissor, Vec2u, Ray3, lib
+
+SCENE_CORNELL = 0
+SCENE_DENSE_MESH = 1
+SCENE_MOTION_ENV = 2
+SCENE_INTERIOR = 3
+SCENE_FEATURES = 100
+SCENE_ENV_SPHERES = 101
+
+FILTER_BOX = 0
+FILTER_GAUSSIAN = 1
+
+FLAG_COUNT_TRAVERSAL = 1
+FLAG_NO_GRAPH = 2
+
+STATUS = {0: "AZ_OK", 1: "AZ_ERR_INVALID_ARGUMENT", 2: "AZ_ERR_INVALID_SCENE", 3: "AZ_ERR_OUT_OF_MEMORY",
+          4: "AZ_ERR_CUDA", 5: "AZ_ERR_TIMEOUT", 6: "AZ_ERR_UNSUPPORTED", 7: "AZ_ERR_NO_DEVICE"}
+
+
+class AzError(RuntimeError):
+    def __init__(self, code, what):
+        msg = lib().az_gpu_last_error().decode(errors="replace") if hasattr(lib(), "az_gpu_last_error") else ""
+        super().__init__("%s failed: %s (%s)" % (what, STATUS.get(code, code), msg))
+        self.code = code
+
+
+def _check(code, what):
+    if code != 0:
+        raise AzError(code, what)
+
+
+class Scene:
+    """A generated azimuth scene (azimuth structs owned by the native library)."""
+
+    def __init__(self, scene_id, seed=0, width=0, height=0, spp=0, max_depth=0, detail=0, filter=-1,
+                 importance_sampling=-1, env_width=0, env_height=0):
+        self._g = GeneratedScene()
+        p = GenParams(width, height, spp, max_depth, detail, filter, importance_sampling, env_width, env_height)
+        rc = lib().az_scene_generate(int(scene_id), int(seed), C.byref(p), C.byref(self._g))
+        if rc != 0:
+            raise RuntimeError("az_scene_generate(%d) failed with %d" % (scene_id, rc))
+        self.scene_id = scene_id
+        self.seed = seed
+
+    @property
+    def scene_ptr(self):
+        return self._g.scene
+
+    @property
+    def camera_ptr(self):
+        return self._g.camera
+
+    @property
+    def epsilons_ptr(self):
+        return self._g.epsilons
+
+    @property
+    def filter_type(self):
+        return self._g.filter_type
+
+    @property
+    def perlin_gradients(self):
+        return self._g.perlin_gradients
+
+    @property
+    def triangle_count(self):
+        return self._g.triangle_count
+
+    @property
+    def sphere_count(self):
+        return self._g.sphere_count
+
+    def resolution(self):
+        # az_camera.Resolution at byte offset 340 (include/az_abi.h)
+        buf = (C.c_uint32 * 2).from_address(self._g.camera + 340)
+        return int(buf[0]), int(buf[1])
+
+    def sample_count(self):
+        return int(C.c_uint32.from_address(self._g.camera + 384).value)
+
+    def max_depth(self):
+        return int(C.c_uint32.from_address(self._g.scene + 2720).value)
+
+    def close(self):
+        if self._g.owner:
+            lib().az_scene_release(C.byref(self._g))
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def generate_scene(scene_id, seed=0, **kw):
+    return Scene(scene_id, seed, **kw)
+
+
+def full_scissor(scene):
+    w, h = scene.resolution()
+    return Scissor(Vec2u(w, h), Vec2u(0, 0))
+
+
+def make_opts(scene=None, seed=0, stream=None, device=0, flags=0, chunk_samples=0, block_size=0):
+    o = RenderOpts()
+    o.seed = seed
+    o.perlin_gradients = scene.perlin_gradients if scene is not None else None
+    o.stream = stream
+    o.device = device
+    o.flags = flags
+    o.chunk_samples = chunk_samples
+    o.block_size = block_size
+    return o
+
+
+def produce_image(scene, pixels=None, scissor=None, filter_type=None, backface_culling=0, seed=0, device=0):
+    """az_gpu_produce_image on a host film (numpy float32 (H, W, 4)); returns the film."""
+    w, h = scene.resolution()
+    if pixels is None:
+        pixels = np.zeros((h, w, 4), np.float32)
+    assert pixels.dtype == np.float32 and pixels.shape == (h, w, 4) and pixels.flags.c_contiguous
+    sc = scissor or full_scissor(scene)
+    ft = scene.filter_type if filter_type is None else filter_type
+    o = make_opts(scene, seed=seed, device=device)
+    _check(lib().az_gpu_produce_image(pixels.ctypes.data, scene.scene_ptr, scene.camera_ptr, scene.epsilons_ptr,
+                                      sc, ft, backface_culling, C.byref(o)), "az_gpu_produce_image")
+    return pixels
+
+
+class GpuScene:
+    """A device-resident scene (az_gpu_scene_create / az_gpu_scene_destroy)."""
+
+    def __init__(self, scene, device=0):
+        self.scene = scene
+        self.device = device
+        self._h = C.c_void_p()
+        o = make_opts(scene, device=device)
+        _check(lib().az_gpu_scene_create(scene.scene_ptr, C.byref(o), C.byref(self._h)), "az_gpu_scene_create")
+
+    def render_device(self, film_ptr, camera_ptr=None, scissor=None, filter_type=None, seed=0, stream=None,
+                      stats=False, flags=0, chunk_samples=0):
+        """az_gpu_render into a DEVICE film pointer; returns az_render_stats as a dict if stats."""
+        sc = scissor or full_scissor(self.scene)
+        ft = self.scene.filter_type if filter_type is None else filter_type
+        o = make_opts(self.scene, seed=seed, stream=stream, device=self.device, flags=flags,
+                      chunk_samples=chunk_samples)
+        st = RenderStats() if stats else None
+        _check(lib().az_gpu_render(self._h, film_ptr, camera_ptr or self.scene.camera_ptr, self.scene.epsilons_ptr,
+                                   sc, ft, 0, C.byref(o), C.byref(st) if st is not None else None),
+               "az_gpu_render")
+        if st is None:
+            return None
+        return {"samples": st.samples, "extend_rays": st.extend_rays, "shadow_rays": st.shadow_rays,
+                "chunks": st.chunks, "retries": st.retries, "kernel_launches": st.kernel_launches,
+                "gpu_ms": st.gpu_ms,
+                "node_visits": st.reserved[0] | (st.reserved[1] << 32),
+                "prim_visits": st.reserved[2] | (st.reserved[3] << 32)}
+
+    def closest_hit(self, rays, cull=0, eps=0.0):
+        """rays: numpy (N, 7) float32 [origin, direction, T]; returns (hit, uid, face, t)."""
+        rays = np.ascontiguousarray(rays, np.float32)
+        n = rays.shape[0]
+        hit = np.zeros(n, np.uint32)
+        uid = np.zeros(n, np.uint32)
+        face = np.zeros(n, np.uint32)
+        t = np.zeros(n, np.float32)
+        o = make_opts(self.scene, device=self.device)
+        _check(lib().az_gpu_closest_hit(self._h, rays.ctypes.data, n, cull, eps, hit.ctypes.data, uid.ctypes.data,
+                                        face.ctypes.data, t.ctypes.data, C.byref(o)), "az_gpu_closest_hit")
+        return hit, uid, face, t
+
+    def close(self):
+        if self._h:
+            lib().az_gpu_scene_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def device_info(device=0):
+    buf = C.create_string_buffer(256)
+    rc = lib().az_gpu_device_info(device, buf, 256)
+    return buf.value.decode() if rc == 0 else None

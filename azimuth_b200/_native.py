@@ -1,0 +1,99 @@
+"""ctypes view of the C-ABI in include/azimuth_gpu.h and include/azimuth_scenes.h.
+
+The library is ``azimuth_b200/libazimuth_b200.so`` (built in-tree by
+``azimuth_b200/build.py``).  Loading fails loudly when it is missing: there is
+no Python or CPU fallback for the render path.
+"""
+import ctypes as C
+import os
+
+_LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libazimuth_b200.so")
+_lib = None
+
+
+class Vec2u(C.Structure):
+    _fields_ = [("x", C.c_uint32), ("y", C.c_uint32)]
+
+
+class Vec3(C.Structure):
+    _fields_ = [("x", C.c_float), ("y", C.c_float), ("z", C.c_float)]
+
+
+class Scissor(C.Structure):
+    """az_scissor: {Max, Min}, rows/cols in [Min, Max) (src/azimuth_main.cpp:35-38)."""
+    _fields_ = [("Max", Vec2u), ("Min", Vec2u)]
+
+
+class Ray3(C.Structure):
+    _fields_ = [("Origin", Vec3), ("Direction", Vec3), ("T", C.c_float)]
+
+
+class GenParams(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("spp", C.c_uint32),
+                ("max_depth", C.c_uint32), ("detail", C.c_uint32), ("filter", C.c_int32),
+                ("importance_sampling", C.c_int32), ("env_width", C.c_uint32),
+                ("env_height", C.c_uint32)]
+
+
+class GeneratedScene(C.Structure):
+    _fields_ = [("scene", C.c_void_p), ("camera", C.c_void_p), ("epsilons", C.c_void_p),
+                ("filter_type", C.c_int32), ("backface_culling", C.c_uint32),
+                ("perlin_gradients", C.c_void_p), ("triangle_count", C.c_uint64),
+                ("sphere_count", C.c_uint64), ("owner", C.c_void_p)]
+
+
+class RenderOpts(C.Structure):
+    _fields_ = [("seed", C.c_uint64), ("perlin_gradients", C.c_void_p), ("stream", C.c_void_p),
+                ("device", C.c_int32), ("flags", C.c_uint32), ("chunk_samples", C.c_uint32),
+                ("bvh_width", C.c_uint32), ("block_size", C.c_uint32),
+                ("reserved", C.c_uint32 * 5)]
+
+
+class RenderStats(C.Structure):
+    _fields_ = [("samples", C.c_uint64), ("extend_rays", C.c_uint64), ("shadow_rays", C.c_uint64),
+                ("chunks", C.c_uint32), ("retries", C.c_uint32), ("kernel_launches", C.c_uint64),
+                ("gpu_ms", C.c_float), ("extend_ms", C.c_float), ("reserved", C.c_uint32 * 6)]
+
+
+def lib():
+    """Load (once) and return the native library; raises if it was not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            raise RuntimeError("azimuth_b200 native library missing: %s (run python -m azimuth_b200.build)"
+                               % _LIB_PATH)
+        _lib = C.CDLL(_LIB_PATH)
+        _declare(_lib)
+    return _lib
+
+
+def library_path():
+    return _LIB_PATH
+
+
+def _declare(L):
+    vp, u32, i32, u64 = C.c_void_p, C.c_uint32, C.c_int32, C.c_uint64
+    L.az_scene_generate.argtypes = [i32, u64, C.POINTER(GenParams), C.POINTER(GeneratedScene)]
+    L.az_scene_generate.restype = i32
+    L.az_scene_release.argtypes = [C.POINTER(GeneratedScene)]
+    L.az_scene_release.restype = None
+    if hasattr(L, "az_gpu_produce_image"):
+        L.az_gpu_last_error.argtypes = []
+        L.az_gpu_last_error.restype = C.c_char_p
+        L.az_gpu_produce_image.argtypes = [vp, vp, vp, vp, Scissor, i32, u32, C.POINTER(RenderOpts)]
+        L.az_gpu_produce_image.restype = i32
+        L.az_gpu_scene_create.argtypes = [vp, C.POINTER(RenderOpts), C.POINTER(vp)]
+        L.az_gpu_scene_create.restype = i32
+        L.az_gpu_scene_destroy.argtypes = [vp]
+        L.az_gpu_scene_destroy.restype = None
+        L.az_gpu_render.argtypes = [vp, vp, vp, vp, Scissor, i32, u32, C.POINTER(RenderOpts),
+                                    C.POINTER(RenderStats)]
+        L.az_gpu_render.restype = i32
+        L.az_gpu_closest_hit.argtypes = [vp, vp, u32, i32, C.c_float, vp, vp, vp, vp, vp]
+        L.az_gpu_closest_hit.restype = i32
+        L.az_gpu_device_info.argtypes = [i32, vp, u32]
+        L.az_gpu_device_info.restype = i32
+        L.az_rng_u01.argtypes = [u64, u32, u32, u32, u32, u32]
+        L.az_rng_u01.restype = C.c_float
+        L.az_rng_philox4x32_10.argtypes = [vp, u32, u32, vp]
+        L.az_rng_philox4x32_10.restype = None

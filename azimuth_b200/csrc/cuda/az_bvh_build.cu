@@ -1,0 +1,252 @@
+// GPU LBVH construction (Karras, "Maximizing Parallelism in the Construction
+// of BVHs, Octrees, and k-d Trees", HPG 2012): 30-bit Morton codes of the box
+// centroids with the primitive index as tie-break, a radix sort, one thread
+// per internal node to find its range and split, and a bottom-up pass that
+// fills each node with the (slightly enlarged) boxes of both children.
+#include <cub/cub.cuh>
+
+#include <cfloat>
+
+#include "az_internal.h"
+
+namespace az {
+namespace {
+
+__device__ __forceinline__ uint32_t expand_bits(uint32_t v) {
+    v = (v * 0x00010001u) & 0xFF0000FFu;
+    v = (v * 0x00000101u) & 0x0F00F00Fu;
+    v = (v * 0x00000011u) & 0xC30C30C3u;
+    v = (v * 0x00000005u) & 0x49249249u;
+    return v;
+}
+
+__global__ void k_bounds_reduce(const float4 *lo, const float4 *hi, uint32_t n, float *out6) {
+    // centroid bounds: one block, strided
+    __shared__ float s[6][256];
+    float mn[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, mx[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+        float4 a = lo[i], b = hi[i];
+        float c[3] = {0.5f * (a.x + b.x), 0.5f * (a.y + b.y), 0.5f * (a.z + b.z)};
+        for (int k = 0; k < 3; k++) {
+            mn[k] = fminf(mn[k], c[k]);
+            mx[k] = fmaxf(mx[k], c[k]);
+        }
+    }
+    for (int k = 0; k < 3; k++) {
+        s[k][threadIdx.x] = mn[k];
+        s[3 + k][threadIdx.x] = mx[k];
+    }
+    __syncthreads();
+    for (uint32_t st = blockDim.x / 2; st > 0; st >>= 1) {
+        if (threadIdx.x < st)
+            for (int k = 0; k < 3; k++) {
+                s[k][threadIdx.x] = fminf(s[k][threadIdx.x], s[k][threadIdx.x + st]);
+                s[3 + k][threadIdx.x] = fmaxf(s[3 + k][threadIdx.x], s[3 + k][threadIdx.x + st]);
+            }
+        __syncthreads();
+    }
+    if (threadIdx.x < 6) out6[threadIdx.x] = s[threadIdx.x][0];
+}
+
+__global__ void k_morton(const float4 *lo, const float4 *hi, uint32_t n, const float *bounds6,
+                         unsigned long long *keys) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 a = lo[i], b = hi[i];
+    float c[3] = {0.5f * (a.x + b.x), 0.5f * (a.y + b.y), 0.5f * (a.z + b.z)};
+    uint32_t q[3];
+    for (int k = 0; k < 3; k++) {
+        float ext = bounds6[3 + k] - bounds6[k];
+        float u = ext > 0.0f ? (c[k] - bounds6[k]) / ext : 0.5f;
+        u = fminf(fmaxf(u, 0.0f), 1.0f);
+        q[k] = min((uint32_t)(u * 1024.0f), 1023u);
+    }
+    uint32_t m = (expand_bits(q[0]) << 2) | (expand_bits(q[1]) << 1) | expand_bits(q[2]);
+    keys[i] = ((unsigned long long)m << 32) | i;
+}
+
+__device__ __forceinline__ int delta(const unsigned long long *k, int n, int i, int j) {
+    if (j < 0 || j >= n) return -1;
+    return __clzll(k[i] ^ k[j]);
+}
+
+// One thread per internal node i in [0, n-2]: children (internal index or
+// leaf flagged with bit 31) and parents.
+__global__ void k_karras(const unsigned long long *k, int n, uint32_t *left, uint32_t *right, int *parent_int,
+                         int *parent_leaf) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    int d = (delta(k, n, i, i + 1) - delta(k, n, i, i - 1)) > 0 ? 1 : -1;
+    int dmin = delta(k, n, i, i - d);
+    int lmax = 2;
+    while (delta(k, n, i, i + lmax * d) > dmin) lmax <<= 1;
+    int l = 0;
+    for (int t = lmax >> 1; t >= 1; t >>= 1)
+        if (delta(k, n, i, i + (l + t) * d) > dmin) l += t;
+    int j = i + l * d;
+    int dnode = delta(k, n, i, j);
+    int s = 0;
+    int t = l;
+    do {
+        t = (t + 1) >> 1;
+        if (delta(k, n, i, i + (s + t) * d) > dnode) s += t;
+    } while (t > 1);
+    int gamma = i + s * d + min(d, 0);
+    int lo = min(i, j), hi = max(i, j);
+    uint32_t lc, rc;
+    if (lo == gamma) {
+        lc = 0x80000000u | (uint32_t)gamma;
+        parent_leaf[gamma] = i;
+    } else {
+        lc = (uint32_t)gamma;
+        parent_int[gamma] = i;
+    }
+    if (hi == gamma + 1) {
+        rc = 0x80000000u | (uint32_t)(gamma + 1);
+        parent_leaf[gamma + 1] = i;
+    } else {
+        rc = (uint32_t)(gamma + 1);
+        parent_int[gamma + 1] = i;
+    }
+    left[i] = lc;
+    right[i] = rc;
+}
+
+__device__ __forceinline__ void pad_box(float4 &lo, float4 &hi) {
+    // enlarge by 2^-19 of the largest magnitude so that rounding in the slab
+    // test never rejects a primitive lying on a face of its box
+    float m = fmaxf(fmaxf(fmaxf(fabsf(lo.x), fabsf(lo.y)), fmaxf(fabsf(lo.z), fabsf(hi.x))),
+                    fmaxf(fabsf(hi.y), fabsf(hi.z)));
+    float p = m * 1.9073486328125e-06f + 1e-30f;
+    lo.x -= p; lo.y -= p; lo.z -= p;
+    hi.x += p; hi.y += p; hi.z += p;
+}
+
+// Bottom-up: one thread per leaf walks to the root; the second child to
+// arrive at a node writes it.
+__global__ void k_fill(const unsigned long long *keys, const float4 *plo, const float4 *phi, int n,
+                       const uint32_t *left, const uint32_t *right, const int *parent_int, const int *parent_leaf,
+                       float4 *ilo, float4 *ihi, unsigned int *visits, azd::BVHNode *nodes, uint32_t node_base,
+                       uint32_t leaf_base) {
+    int leaf = blockIdx.x * blockDim.x + threadIdx.x;
+    if (leaf >= n) return;
+    int node = parent_leaf[leaf];
+    while (node >= 0) {
+        __threadfence();
+        if (atomicAdd(&visits[node], 1u) == 0) return;  // first arrival: the sibling finishes the node
+        __threadfence();
+        uint32_t c[2] = {left[node], right[node]};
+        float4 blo[2], bhi[2];
+        uint32_t ref[2], cnt[2];
+        for (int s = 0; s < 2; s++) {
+            if (c[s] & 0x80000000u) {
+                uint32_t li = c[s] & 0x7FFFFFFFu;
+                uint32_t prim = (uint32_t)(keys[li] & 0xFFFFFFFFull);
+                blo[s] = plo[prim];
+                bhi[s] = phi[prim];
+                ref[s] = leaf_base + li;
+                cnt[s] = 1;
+            } else {
+                blo[s] = __ldcg(ilo + c[s]);
+                bhi[s] = __ldcg(ihi + c[s]);
+                ref[s] = node_base + c[s];
+                cnt[s] = 0;
+            }
+        }
+        float4 ulo = make_float4(fminf(blo[0].x, blo[1].x), fminf(blo[0].y, blo[1].y), fminf(blo[0].z, blo[1].z), 0);
+        float4 uhi = make_float4(fmaxf(bhi[0].x, bhi[1].x), fmaxf(bhi[0].y, bhi[1].y), fmaxf(bhi[0].z, bhi[1].z), 0);
+        __stcg(ilo + node, ulo);
+        __stcg(ihi + node, uhi);
+        pad_box(blo[0], bhi[0]);
+        pad_box(blo[1], bhi[1]);
+        azd::BVHNode out;
+        out.bx = make_float4(blo[0].x, bhi[0].x, blo[1].x, bhi[1].x);
+        out.by = make_float4(blo[0].y, bhi[0].y, blo[1].y, bhi[1].y);
+        out.bz = make_float4(blo[0].z, bhi[0].z, blo[1].z, bhi[1].z);
+        out.ch = make_uint4(ref[0], ref[1], cnt[0], cnt[1]);
+        nodes[node_base + node] = out;
+        node = parent_int[node];
+    }
+}
+
+__global__ void k_extract_perm(const unsigned long long *keys, uint32_t n, uint32_t *perm) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) perm[i] = (uint32_t)(keys[i] & 0xFFFFFFFFull);
+}
+
+__global__ void k_single(const float4 *lo, const float4 *hi, azd::BVHNode *nodes, uint32_t node_base,
+                         uint32_t leaf_base, uint32_t *perm) {
+    float4 a = lo[0], b = hi[0];
+    pad_box(a, b);
+    azd::BVHNode out;
+    // child 1 is an empty box (lo > hi) that no ray enters
+    out.bx = make_float4(a.x, b.x, FLT_MAX, -FLT_MAX);
+    out.by = make_float4(a.y, b.y, FLT_MAX, -FLT_MAX);
+    out.bz = make_float4(a.z, b.z, FLT_MAX, -FLT_MAX);
+    out.ch = make_uint4(leaf_base, leaf_base, 1u, 1u);
+    nodes[node_base] = out;
+    perm[0] = 0;
+}
+
+template <typename T>
+struct Scratch {
+    T *p = nullptr;
+    ~Scratch() {
+        if (p) cudaFree(p);
+    }
+    cudaError_t alloc(size_t n) { return cudaMalloc((void **)&p, n * sizeof(T) + 16); }
+};
+
+}  // namespace
+
+int BuildLBVH(const float4 *d_lo, const float4 *d_hi, uint32_t n, azd::BVHNode *d_nodes, uint32_t node_base,
+              uint32_t leaf_base, uint32_t *d_perm, cudaStream_t stream, uint32_t *root_out) {
+    if (n == 0) {
+        *root_out = 0xFFFFFFFFu;
+        return AZ_OK;
+    }
+    *root_out = node_base;
+    if (n == 1) {
+        k_single<<<1, 1, 0, stream>>>(d_lo, d_hi, d_nodes, node_base, leaf_base, d_perm);
+        AZ_CUDA_TRY(cudaGetLastError());
+        return AZ_OK;
+    }
+    Scratch<float> bounds;
+    Scratch<unsigned long long> keys, keys_sorted;
+    Scratch<uint32_t> left, right;
+    Scratch<int> parent_int, parent_leaf;
+    Scratch<float4> ilo, ihi;
+    Scratch<unsigned int> visits;
+    Scratch<unsigned char> temp;
+    AZ_CUDA_TRY(bounds.alloc(6));
+    AZ_CUDA_TRY(keys.alloc(n));
+    AZ_CUDA_TRY(keys_sorted.alloc(n));
+    AZ_CUDA_TRY(left.alloc(n));
+    AZ_CUDA_TRY(right.alloc(n));
+    AZ_CUDA_TRY(parent_int.alloc(n));
+    AZ_CUDA_TRY(parent_leaf.alloc(n));
+    AZ_CUDA_TRY(ilo.alloc(n));
+    AZ_CUDA_TRY(ihi.alloc(n));
+    AZ_CUDA_TRY(visits.alloc(n));
+    size_t temp_bytes = 0;
+    AZ_CUDA_TRY(cub::DeviceRadixSort::SortKeys(nullptr, temp_bytes, keys.p, keys_sorted.p, (int)n, 0, 62, stream));
+    AZ_CUDA_TRY(temp.alloc(temp_bytes));
+    const int B = 256;
+    uint32_t grid = (n + B - 1) / B;
+    k_bounds_reduce<<<1, 256, 0, stream>>>(d_lo, d_hi, n, bounds.p);
+    k_morton<<<grid, B, 0, stream>>>(d_lo, d_hi, n, bounds.p, keys.p);
+    AZ_CUDA_TRY(cudaGetLastError());
+    AZ_CUDA_TRY(cub::DeviceRadixSort::SortKeys(temp.p, temp_bytes, keys.p, keys_sorted.p, (int)n, 0, 62, stream));
+    AZ_CUDA_TRY(cudaMemsetAsync(parent_int.p, 0xFF, n * sizeof(int), stream));   // root's parent = -1
+    AZ_CUDA_TRY(cudaMemsetAsync(visits.p, 0, n * sizeof(unsigned int), stream));
+    k_karras<<<grid, B, 0, stream>>>(keys_sorted.p, (int)n, left.p, right.p, parent_int.p, parent_leaf.p);
+    k_fill<<<grid, B, 0, stream>>>(keys_sorted.p, d_lo, d_hi, (int)n, left.p, right.p, parent_int.p, parent_leaf.p,
+                                   ilo.p, ihi.p, visits.p, d_nodes, node_base, leaf_base);
+    k_extract_perm<<<grid, B, 0, stream>>>(keys_sorted.p, n, d_perm);
+    AZ_CUDA_TRY(cudaGetLastError());
+    // scratch is freed when this returns: finish the work that uses it
+    AZ_CUDA_TRY(cudaStreamSynchronize(stream));
+    return AZ_OK;
+}
+
+}  // namespace az

@@ -1,0 +1,177 @@
+// extern "C" entry points of include/azimuth_gpu.h.
+//
+// Each call selects opts->device, runs on opts->stream (or a private stream),
+// catches every CUDA error into an AZ_* status and never throws across the ABI.
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <string>
+
+#include "az_internal.h"
+
+namespace az {
+
+namespace {
+thread_local std::string t_last_error;
+}
+
+int SetError(int code, const std::string &msg) {
+    t_last_error = msg;
+    return code;
+}
+
+int CudaError(cudaError_t e, const char *what) {
+    int code = e == cudaErrorMemoryAllocation ? AZ_ERR_OUT_OF_MEMORY
+               : (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) ? AZ_ERR_NO_DEVICE
+                                                                             : AZ_ERR_CUDA;
+    cudaGetLastError();  // clear a sticky non-fatal error state
+    return SetError(code, std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
+}
+
+// Picks the device and the stream for one call; owns a private stream when
+// the caller passed none.
+struct CallContext {
+    cudaStream_t stream = nullptr;
+    bool own = false;
+    int begin(const az_render_opts *opts) {
+        int dev = opts ? opts->device : 0;
+        int n = 0;
+        cudaError_t e = cudaGetDeviceCount(&n);
+        if (e != cudaSuccess || n == 0) return SetError(AZ_ERR_NO_DEVICE, "no CUDA device available");
+        if (dev < 0 || dev >= n) return SetError(AZ_ERR_INVALID_ARGUMENT, "device ordinal out of range");
+        AZ_CUDA_TRY(cudaSetDevice(dev));
+        if (opts && opts->stream) {
+            stream = (cudaStream_t)opts->stream;
+        } else {
+            AZ_CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+            own = true;
+        }
+        return AZ_OK;
+    }
+    ~CallContext() {
+        if (own && stream) {
+            cudaStreamSynchronize(stream);
+            cudaStreamDestroy(stream);
+        }
+    }
+};
+
+}  // namespace az
+
+struct az_gpu_scene {
+    az::GpuScene *impl;
+};
+
+using namespace az;
+
+extern "C" const char *az_gpu_last_error(void) { return t_last_error.c_str(); }
+
+extern "C" int az_gpu_device_info(int32_t device, char *name, uint32_t name_len) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return SetError(AZ_ERR_NO_DEVICE, "no CUDA device available");
+    }
+    if (device < 0 || device >= n) return SetError(AZ_ERR_INVALID_ARGUMENT, "device ordinal out of range");
+    cudaDeviceProp p;
+    AZ_CUDA_TRY(cudaGetDeviceProperties(&p, device));
+    if (name && name_len) {
+        snprintf(name, name_len, "%s|sm_%d%d|%d SMs|%zu MiB", p.name, p.major, p.minor, p.multiProcessorCount,
+                 (size_t)(p.totalGlobalMem >> 20));
+    }
+    return AZ_OK;
+}
+
+extern "C" int az_gpu_scene_create(const az_scene *scene, const az_render_opts *opts, az_gpu_scene **out) {
+    if (!scene || !out) return SetError(AZ_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    CallContext ctx;
+    int rc = ctx.begin(opts);
+    if (rc != AZ_OK) return rc;
+    GpuScene *g = nullptr;
+    rc = BuildGpuScene(scene, opts, ctx.stream, &g);
+    if (rc != AZ_OK) return rc;
+    az_gpu_scene *h = new (std::nothrow) az_gpu_scene{g};
+    if (!h) {
+        delete g;
+        return SetError(AZ_ERR_OUT_OF_MEMORY, "host allocation failed");
+    }
+    *out = h;
+    return AZ_OK;
+}
+
+extern "C" void az_gpu_scene_destroy(az_gpu_scene *s) {
+    if (!s) return;
+    if (s->impl) {
+        cudaSetDevice(s->impl->device);
+        cudaDeviceSynchronize();
+        delete s->impl;
+    }
+    delete s;
+}
+
+extern "C" int az_gpu_render(az_gpu_scene *scene, az_pixel *film, const az_camera *camera,
+                             const az_epsilon_values *epsilons, az_scissor scissor, int32_t filter_type,
+                             uint32_t backface_culling, const az_render_opts *opts, az_render_stats *stats) {
+    if (!scene || !scene->impl || !film || !camera) return SetError(AZ_ERR_INVALID_ARGUMENT, "null argument");
+    CallContext ctx;
+    int rc = ctx.begin(opts);
+    if (rc != AZ_OK) return rc;
+    return Render(*scene->impl, film, camera, epsilons, scissor, filter_type, backface_culling, opts, ctx.stream,
+                  stats);
+}
+
+extern "C" int az_gpu_produce_image(az_pixel *pixels, const az_scene *scene, const az_camera *camera,
+                                    const az_epsilon_values *epsilons, az_scissor scissor, int32_t filter_type,
+                                    uint32_t backface_culling, const az_render_opts *opts) {
+    if (!pixels || !scene || !camera) return SetError(AZ_ERR_INVALID_ARGUMENT, "null argument");
+    CallContext ctx;
+    int rc = ctx.begin(opts);
+    if (rc != AZ_OK) return rc;
+    GpuScene *g = nullptr;
+    rc = BuildGpuScene(scene, opts, ctx.stream, &g);
+    if (rc != AZ_OK) return rc;
+    std::unique_ptr<GpuScene> hold(g);
+    size_t bytes = (size_t)camera->Resolution.x * camera->Resolution.y * sizeof(az_pixel);
+    az_pixel *d_film = nullptr;
+    AZ_CUDA_TRY(cudaMallocAsync((void **)&d_film, bytes, ctx.stream));
+    // the film accumulates: start from the caller's sums
+    cudaError_t e = cudaMemcpyAsync(d_film, pixels, bytes, cudaMemcpyHostToDevice, ctx.stream);
+    if (e != cudaSuccess) {
+        cudaFreeAsync(d_film, ctx.stream);
+        return CudaError(e, "film upload");
+    }
+    rc = Render(*g, d_film, camera, epsilons, scissor, filter_type, backface_culling, opts, ctx.stream, nullptr);
+    if (rc == AZ_OK) {
+        e = cudaMemcpyAsync(pixels, d_film, bytes, cudaMemcpyDeviceToHost, ctx.stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx.stream);
+        if (e != cudaSuccess) rc = CudaError(e, "film download");
+    }
+    cudaFreeAsync(d_film, ctx.stream);
+    cudaStreamSynchronize(ctx.stream);
+    return rc;
+}
+
+extern "C" int az_gpu_closest_hit(az_gpu_scene *scene, const az_ray3 *rays, uint32_t count, int32_t cull,
+                                  float hit_epsilon, uint32_t *out_hit, uint32_t *out_uid, uint32_t *out_face,
+                                  float *out_t, const az_render_opts *opts) {
+    if (!scene || !scene->impl || (count && (!rays || !out_hit || !out_uid || !out_face || !out_t)))
+        return SetError(AZ_ERR_INVALID_ARGUMENT, "null argument");
+    CallContext ctx;
+    int rc = ctx.begin(opts);
+    if (rc != AZ_OK) return rc;
+    return ClosestHit(*scene->impl, rays, count, cull, hit_epsilon, out_hit, out_uid, out_face, out_t, ctx.stream);
+}
+
+extern "C" float az_rng_u01(uint64_t seed, uint32_t pixel, uint32_t sample, uint32_t digits, uint32_t level,
+                            uint32_t dim) {
+    azd::NodeRng r;
+    r.init(seed, pixel, sample, digits, level);
+    r.skip(dim);
+    return r.next();
+}
+
+extern "C" void az_rng_philox4x32_10(const uint32_t counter[4], uint32_t key0, uint32_t key1, uint32_t out[4]) {
+    azd::philox4x32_10(counter[0], counter[1], counter[2], counter[3], key0, key1, out);
+}

@@ -1,0 +1,62 @@
+// Internal host-side declarations shared by the CUDA translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "az_render.h"
+#include "az_scene_dev.cuh"
+#include "azimuth_gpu.h"
+
+namespace az {
+
+// Status plus message; stored per thread for az_gpu_last_error().
+int SetError(int code, const std::string &msg);
+int CudaError(cudaError_t e, const char *what);
+
+#define AZ_CUDA_TRY(expr)                                       \
+    do {                                                        \
+        cudaError_t az_e_ = (expr);                             \
+        if (az_e_ != cudaSuccess) return ::az::CudaError(az_e_, #expr); \
+    } while (0)
+
+// A device allocation owned by a GpuScene.
+struct DevBuf {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+};
+
+struct GpuScene {
+    int device = 0;
+    azd::DevScene dev{};
+    std::vector<DevBuf> bufs;
+    uint64_t triangle_count = 0;
+    uint64_t sphere_count = 0;
+    uint64_t node_count = 0;
+    uint32_t max_bvh_depth = 0;
+    size_t device_bytes = 0;
+    WaveBuffers waves;           // reused across render calls on this scene
+    ~GpuScene();
+    void *Alloc(size_t bytes);   // nullptr on failure
+};
+
+// Builds the device scene from azimuth's structs (az_scene_upload.cu).
+int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_t stream, GpuScene **out);
+
+// LBVH over `n` boxes (device arrays lo/hi of float4).  Writes nodes into
+// `nodes` starting at `node_base` (n-1 nodes, or 1 for n == 1) and the sorted
+// primitive order into `perm`.  Leaf child references are `leaf_base + sorted
+// position`.  Returns the root node index.
+int BuildLBVH(const float4 *d_lo, const float4 *d_hi, uint32_t n, azd::BVHNode *d_nodes, uint32_t node_base,
+              uint32_t leaf_base, uint32_t *d_perm, cudaStream_t stream, uint32_t *root_out);
+
+int SetupCamera(const az_camera *c, az_scissor sc, int32_t filter, uint32_t cull, const az_epsilon_values *eps,
+                uint64_t seed, CameraParams &cam);
+int Render(GpuScene &G, az_pixel *film, const az_camera *camera, const az_epsilon_values *eps, az_scissor sc,
+           int32_t filter, uint32_t cull, const az_render_opts *opts, cudaStream_t st, az_render_stats *stats);
+int ClosestHit(GpuScene &G, const az_ray3 *rays, uint32_t n, int32_t cull, float eps, uint32_t *out_hit,
+               uint32_t *out_uid, uint32_t *out_face, float *out_t, cudaStream_t st);
+
+}  // namespace az

@@ -1,0 +1,691 @@
+// Wavefront path tracer reproducing azimuth's estimator (TraceRay,
+// src/azimuth_main.cpp:966-1133) on the GPU.
+//
+// A camera sample in azimuth is a recursive tree: every non-emitting hit adds
+// its direct light and ambient term and recurses into a diffuse scatter ray,
+// a mirror ray and the dielectric refraction and reflection rays.  Here every
+// tree node is one queue entry carrying the product of the weights above it
+// ("throughput"); levels are processed breadth-first over a wave of samples:
+//
+//   camera  -> queue[1]                    (GetSampleCoord + GetRayForPixel)
+//   per level L = 1 .. MaxRecursionDepth+1:
+//     extend  queue[L]  -> hits            (RayEntityIntersection)
+//     shade   hits      -> queue[L+1], shadow queue, per-sample sums
+//     shadow  shadow queue -> per-sample sums (the visibility tests of CalculateLighting)
+//   splat   per-sample sums -> film        (ComputeSampleWeight, box or Gaussian)
+//
+// The counter RNG is keyed by the tree node, so the order in which the GPU
+// visits nodes does not change any random number: the result equals azimuth's
+// own tree up to float summation order.  Child nodes whose weight is exactly
+// zero (e.g. the scatter ray of a pure mirror) are not traced; azimuth traces
+// them and multiplies their radiance by zero.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "az_internal.h"
+#include "az_render.h"
+#include "az_shade.cuh"
+
+namespace az {
+namespace {
+
+using namespace azd;
+
+// Shadow-query kinds (CalculateLighting occlusion rules, src/azimuth_main.cpp:685-712)
+enum : uint32_t {
+    SHADOW_TMAX = 0,     // point/area/spot: occluded by a hit with t < 1 - ShadowRay epsilon
+    SHADOW_ANY = 1,      // directional light and environment ray: occluded by any hit
+    SHADOW_ENTITY = 2    // entity light: occluded unless the nearest hit is the light's entity
+};
+
+// flags packed into d.w of a path entry
+enum : uint32_t { PF_INSIDE = 1u, PF_ATTEN = 2u };
+
+__host__ __device__ __forceinline__ void sample_of(const CameraParams &cam, uint64_t s, uint32_t &row,
+                                                   uint32_t &col, uint32_t &sx, uint32_t &sy) {
+    uint64_t pix = s % cam.npix, k = s / cam.npix;
+    row = cam.r0 + (uint32_t)(pix / cam.wsc);
+    col = cam.c0 + (uint32_t)(pix % cam.wsc);
+    sx = (uint32_t)(k % cam.sqrt_spp);
+    sy = (uint32_t)(k / cam.sqrt_spp);
+}
+
+__device__ __forceinline__ uint32_t push_slot(uint32_t *counter) {
+    // warp-aggregated atomic increment
+    uint32_t mask = __activemask();
+    int lane = threadIdx.x & 31;
+    int leader = __ffs(mask) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(mask));
+    base = __shfl_sync(mask, base, leader);
+    return base + (uint32_t)__popc(mask & ((1u << lane) - 1u));
+}
+
+__device__ __forceinline__ void add_accum(float4 *accum, uint32_t slot, f3 v) {
+    if (is_zero(v)) return;
+    atomicAdd(&accum[slot].x, v.x);
+    atomicAdd(&accum[slot].y, v.y);
+    atomicAdd(&accum[slot].z, v.z);
+}
+
+__device__ __forceinline__ void push_path(const WaveQueues &Q, int buf, uint32_t level, f3 o, float time, f3 d,
+                                          uint32_t flags, f3 tp, uint32_t slot, f3 att, uint32_t digits) {
+    uint32_t i = push_slot(&Q.counts[level]);
+    if (i >= Q.cap_q) {
+        Q.counts[AZ_COUNT_OVERFLOW] = 1;   // this wave is re-run with fewer samples
+        return;
+    }
+    Q.o[buf][i] = make_float4(o.x, o.y, o.z, time);
+    Q.d[buf][i] = make_float4(d.x, d.y, d.z, __uint_as_float(flags));
+    Q.tp[buf][i] = make_float4(tp.x, tp.y, tp.z, __uint_as_float(slot));
+    Q.att[buf][i] = make_float4(att.x, att.y, att.z, 0.0f);
+    Q.digits[buf][i] = digits;
+}
+
+__device__ __forceinline__ void push_shadow(const WaveQueues &Q, uint32_t level, f3 o, float time, f3 d,
+                                            float tmax, f3 c, uint32_t slot, uint32_t kind, uint32_t uid) {
+    uint32_t i = push_slot(&Q.counts[AZ_COUNT_SHADOW + level]);
+    if (i >= Q.cap_s) {
+        Q.counts[AZ_COUNT_OVERFLOW] = 1;
+        return;
+    }
+    Q.so[i] = make_float4(o.x, o.y, o.z, time);
+    Q.sd[i] = make_float4(d.x, d.y, d.z, tmax);
+    Q.sc[i] = make_float4(c.x, c.y, c.z, __uint_as_float(slot));
+    Q.smeta[i] = (kind << 30) | (uid & 0x3FFFFFFFu);
+}
+
+// GetSampleCoord + GetRayForPixel (src/azimuth_main.cpp:1135-1178).
+__global__ void k_camera(CameraParams cam, WaveQueues Q, uint64_t wave_start, uint32_t n) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t row, col, sx, sy;
+    sample_of(cam, wave_start + i, row, col, sx, sy);
+    NodeRng rng;
+    rng.init(cam.seed, (row << 16) | col, (sy << 16) | sx, 0u, 0u);
+    float cx = (float)col + (0.5f * cam.inv_sqrt + (float)sx * cam.inv_sqrt);
+    float cy = (float)row + (0.5f * cam.inv_sqrt + (float)sy * cam.inv_sqrt);
+    // the lens pair is drawn y first: GCC evaluates the two Random01()
+    // arguments of Vec2(...) right to left in the oracle build
+    float ly = rng.next() - 0.5f;
+    float lx = rng.next() - 0.5f;
+    lx *= cam.aperture;
+    ly *= cam.aperture;
+    f3 offx = cam.axx * lx, offy = cam.axy * ly;
+    f3 dir = normalize(cam.base + cx * cam.stepx - cy * cam.stepy - offx - offy);
+    f3 o = cam.pos + offx + offy;
+    float time = rng.next();
+    Q.o[1][i] = make_float4(o.x, o.y, o.z, time);
+    Q.d[1][i] = make_float4(dir.x, dir.y, dir.z, __uint_as_float(0u));
+    Q.tp[1][i] = make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(i));
+    Q.att[1][i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    Q.digits[1][i] = 0u;
+    Q.accum[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+}
+
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_extend(DevScene S, CameraParams cam, WaveQueues Q, uint32_t level) {
+    const int buf = level & 1;
+    const uint32_t n = min(Q.counts[level], Q.cap_q);
+    uint32_t *cnt = cam.count_traversal ? Q.counts + AZ_COUNT_NODES : nullptr;
+    for (uint32_t i = blockIdx.x * BLOCK + threadIdx.x; i < n; i += gridDim.x * BLOCK) {
+        float4 o = Q.o[buf][i], d = Q.d[buf][i];
+        Ray r;
+        r.o = mk(o.x, o.y, o.z);
+        r.d = mk(d.x, d.y, d.z);
+        r.time = o.w;
+        Hit h;
+        trace<Q_CLOSEST>(S, r, cam.cull != 0, cam.eps_isect, FLT_MAX, h, cnt);
+        Q.hit[i] = make_uint4(__float_as_uint(h.t), __float_as_uint(h.tl), h.prim, h.ent);
+    }
+}
+
+__device__ __forceinline__ f3 ld3(const float *p) { return mk(p[0], p[1], p[2]); }
+
+// One tree node: direct light, ambient and children (TraceRay body,
+// src/azimuth_main.cpp:974-1130).
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_shade(DevScene S, CameraParams cam, WaveQueues Q, uint64_t wave_start,
+                                                 uint32_t level) {
+    const int buf = level & 1, nbuf = buf ^ 1;
+    const uint32_t n = min(Q.counts[level], Q.cap_q);
+    const bool can_spawn = level + 1 <= S.max_depth + 1;   // child's RecursionDepth <= MaxRecursionDepth
+    const float seps = cam.eps_shadow;
+    for (uint32_t i = blockIdx.x * BLOCK + threadIdx.x; i < n; i += gridDim.x * BLOCK) {
+        const float4 o4 = Q.o[buf][i], d4 = Q.d[buf][i], tp4 = Q.tp[buf][i];
+        const uint4 hh = Q.hit[i];
+        const uint32_t flags = __float_as_uint(d4.w);
+        const uint32_t slot = __float_as_uint(tp4.w);
+        f3 tp = mk(tp4.x, tp4.y, tp4.z);
+        Ray r;
+        r.o = mk(o4.x, o4.y, o4.z);
+        r.d = mk(d4.x, d4.y, d4.z);
+        r.time = o4.w;
+        Hit h;
+        h.t = __uint_as_float(hh.x);
+        h.tl = __uint_as_float(hh.y);
+        h.prim = hh.z;
+        h.ent = hh.w;
+        uint32_t row, col, sx, sy;
+        sample_of(cam, wave_start + slot, row, col, sx, sy);
+        if (h.ent == 0xFFFFFFFFu) {
+            // a miss returns 0, except for the primary ray, whose sample then takes
+            // the background (RayTravelDistance == 0, src/azimuth_main.cpp:1374-1384)
+            if (level == 1)
+                add_accum(Q.accum, slot, background(S, r.d, (int32_t)cam.width - 1, (int32_t)cam.height - 1, row, col));
+            continue;
+        }
+        const bool inside = (flags & PF_INSIDE) != 0;
+        if (flags & PF_ATTEN) {
+            // Beer attenuation of a refracted or internally reflected subtree by
+            // the distance to its first hit (src/azimuth_main.cpp:921-935, :955-962)
+            float4 a = Q.att[buf][i];
+            tp = had(tp, mk(expf(a.x * h.t), expf(a.y * h.t), expf(a.z * h.t)));
+        }
+        const DevEntity &e = S.ents[h.ent];
+        if (e.is_emitter) {
+            add_accum(Q.accum, slot, had(tp, ld3(e.radiance)));   // :984-985
+            continue;
+        }
+        NodeRng rng;
+        const uint32_t digits = Q.digits[buf][i];
+        rng.init(cam.seed, (row << 16) | col, (sy << 16) | sx, digits, level);
+        const Surface s = surface_at(S, r, h);
+        const DevMaterial &m = S.materials[e.material];
+        f3 dcol = ld3(m.diffuse), scol = ld3(m.specular);
+        f3 local = mk(0.0f, 0.0f, 0.0f);   // this node's own radiance (before `tp`)
+        bool ignore_ambient = false;
+        if (e.texture_index) {
+            const DevTexture &tex = S.textures[e.texture_index - 1];
+            f3 ts = sample_texture(S, tex, s.p, s.u, s.v);
+            if (tex.blend == 0) {           // ReplaceAll: DiffuseContribution starts at (1,1,1)
+                dcol = ts;
+                local = dcol;
+                ignore_ambient = true;
+            } else if (tex.blend == 1) {    // ReplaceDiffuse
+                dcol = ts;
+            } else {                        // BlendDiffuse
+                dcol = dcol + ts;
+                dcol = dcol * 0.5f;
+            }
+        }
+        // CalculateLighting (:605-779): one sample and one visibility test per light
+        for (uint32_t li = 0; li < S.light_count; li++) {
+            const DevLight &L = S.lights[li];
+            f3 ldir = mk(0.0f, 0.0f, 0.0f), I = ld3(L.intensity);
+            uint32_t kind = SHADOW_TMAX;
+            float falloff = 1.0f, ldist = 1.0f, invpdf = 1.0f;
+            if (L.type == LIGHT_POINT) {
+                ldir = ld3(L.position) - s.p;
+                ldist = length(ldir);
+            } else if (L.type == LIGHT_AREA) {
+                // GCC evaluates the second Random01() of this sum first
+                float u1 = rng.next();
+                float u0 = rng.next();
+                f3 lp = ld3(L.position) + ld3(L.edge0) * u0 + ld3(L.edge1) * u1;
+                falloff = dot(normalize(lp - s.p), ld3(L.normal));
+                if (falloff < 0.0f) falloff *= -1.0f;
+                ldir = lp - s.p;
+                ldist = length(ldir);
+            } else if (L.type == LIGHT_DIRECTIONAL) {
+                ldir = normalize(-ld3(L.position));
+                kind = SHADOW_ANY;
+            } else if (L.type == LIGHT_SPOT) {
+                ldir = ld3(L.position) - s.p;
+                ldist = length(ldir);
+                float ct = dot(normalize(-ldir), normalize(ld3(L.spot_dir)));
+                if (ct < L.cos_half_coverage) {
+                    falloff = 0.0f;
+                } else if (ct > L.cos_half_falloff) {
+                    falloff = 1.0f;
+                } else {
+                    falloff = (ct - L.cos_half_coverage) / (L.cos_half_falloff - L.cos_half_coverage);
+                    falloff = powf(falloff, 4.0f);
+                    if (falloff < 0.0f) falloff = 0.0f;
+                    else if (falloff > 1.0f) falloff = 1.0f;
+                }
+            } else {
+                sample_entity_light(S, L, s.p, rng, ldir, invpdf);
+                I = ld3(L.intensity);
+                kind = SHADOW_ENTITY;
+            }
+            if (ldist == 0.0f) ldist = 0.001f;
+            if (inside) continue;   // no direct light inside a dielectric (:714)
+            f3 dc, sc;
+            if (!light_contribution(dc, sc, m, I, ldir, r.d, s.n, ldist, falloff, invpdf)) continue;
+            f3 c = had(tp, had(dcol, dc) + had(scol, sc));
+            if (is_zero(c)) continue;
+            push_shadow(Q, level, s.p + (ldir * seps), r.time, ldir, 1.0f - seps, c, slot, kind, L.uid);
+        }
+        if (S.use_env_map) {
+            // cosine-sampled environment ray (:724-778); not gated by InsideDielectric
+            float phi = 2.0f * AZD_PI_F32 * rng.next();
+            float cp = cosf(phi), sp = sinf(phi);
+            float theta = asinf(sqrtf(rng.next()));
+            float ct = cosf(theta), st = sinf(theta);
+            f3 U, V;
+            onb(s.n, U, V);
+            f3 Ld = normalize(U * st * cp + V * st * sp + s.n * ct);
+            float u = (-atan2f(Ld.z, Ld.x) + AZD_PI_F32) / (2.0f * AZD_PI_F32), v = acosf(Ld.y) / AZD_PI_F32;
+            f3 I = sample_texture(S, S.textures[S.env_texture], mk(u, v, 1.0f), u, v);
+            float ca = dot(Ld, s.n);
+            if (ca == 0.0f) ca = 0.000001f;
+            f3 dc, sc;
+            if (light_contribution(dc, sc, m, I, Ld, r.d, s.n, 1.0f, 1.0f, AZD_PI_F32 / ca)) {
+                f3 c = had(tp, had(dcol, dc) + had(scol, sc));
+                if (!is_zero(c)) push_shadow(Q, level, s.p + (Ld * seps), r.time, Ld, FLT_MAX, c, slot, SHADOW_ANY, 0u);
+            }
+        }
+        uint32_t next_child = 0;
+        if (S.path_trace) {
+            // diffuse scatter ray (:1029-1083): child 0
+            float theta = S.importance_sampling ? asinf(sqrtf(rng.next())) : acosf(rng.next());
+            float ct = cosf(theta), st = sinf(theta);
+            float phi = 2.0f * AZD_PI_F32 * rng.next();
+            float cp = cosf(phi), sp = sinf(phi);
+            f3 U, V;
+            onb(s.n, U, V);
+            f3 Sd = normalize(U * st * cp + V * st * sp + s.n * ct);
+            float invpdf;
+            if (S.importance_sampling) {
+                float cs = dot(Sd, s.n);
+                if (cs == 0.0f) cs = 0.000001f;
+                invpdf = AZD_PI_F32 / cs;
+            } else {
+                invpdf = AZD_PI_F32 * 2.0f;
+            }
+            f3 dc, sc;
+            if (can_spawn && light_contribution(dc, sc, m, mk(1.0f, 1.0f, 1.0f), Sd, r.d, s.n, 1.0f, 1.0f, invpdf)) {
+                f3 ctp = had(tp, had(dcol, dc) + had(scol, sc));
+                if (!is_zero(ctp))
+                    push_path(Q, nbuf, level + 1, s.p + (Sd * seps), r.time, Sd, flags & PF_INSIDE, ctp, slot,
+                              mk(0.0f, 0.0f, 0.0f), child_digits(digits, level, 0));
+            }
+            next_child = 1;
+        }
+        // ReplaceAll's (1,1,1) start value and the ambient term (:1000-1020, :1086-1099)
+        f3 own = local;
+        if ((!inside || !m.transparent) && !ignore_ambient) own = own + had(ld3(m.ambient), ld3(S.ambient));
+        add_accum(Q.accum, slot, had(tp, own));
+        if (m.is_mirror) {
+            // CalculateMirrorContribution (:781-854)
+            f3 rd = reflect(-r.d, s.n);
+            if (m.glossiness != 0.0f) {
+                f3 rp = mk(fabsf(rd.x), fabsf(rd.y), fabsf(rd.z));
+                if (rp.x < rp.y) {
+                    if (rp.x < rp.z) { rp = rd; rp.x = rp.x < 0.0f ? -1.0f : 1.0f; }
+                    else { rp = rd; rp.z = rp.z < 0.0f ? -1.0f : 1.0f; }
+                } else {
+                    if (rp.y < rp.z) { rp = rd; rp.y = rp.y < 0.0f ? -1.0f : 1.0f; }
+                    else { rp = rd; rp.z = rp.z < 0.0f ? -1.0f : 1.0f; }
+                }
+                rp = normalize(rp);
+                f3 uu = cross(rp, rd), vv = cross(uu, rd);
+                // GCC evaluates the second Random01() of this sum first
+                float b = rng.next();
+                float a = rng.next();
+                rd = rd + (2.0f * m.glossiness) * (uu * (a - 0.5f) + vv * (b - 0.5f));
+                rd = normalize(rd);
+            }
+            f3 ctp = had(tp, ld3(m.mirror));
+            if (can_spawn && !is_zero(ctp))
+                push_path(Q, nbuf, level + 1, s.p + (rd * 0.000825f), r.time, rd, flags & PF_INSIDE, ctp, slot,
+                          mk(0.0f, 0.0f, 0.0f), child_digits(digits, level, next_child));
+            next_child++;
+        }
+        if (m.transparent) {
+            // CalculateTransparencyContribution (:856-964)
+            f3 T = ld3(m.transparency);
+            float to = m.refraction_index, from = 1.0f;
+            if (inside) {
+                from = m.refraction_index;
+                to = 1.0f;
+            }
+            f3 N = s.n;
+            float ct = -dot(r.d, N);
+            if (ct < 0.0f) {
+                N = -s.n;
+                ct = -dot(r.d, N);
+            }
+            float ratio = from / to;
+            float delta = 1.0f - (ratio * ratio) * (1.0f - ct * ct);
+            float refl;
+            f3 att = mk(T.x - 1.0f, T.y - 1.0f, T.z - 1.0f);
+            if (delta <= 0.0f) {
+                refl = 1.0f;
+            } else {
+                float cphi = sqrtf(delta);
+                float cair = inside ? cphi : ct;
+                float icair = 1.0f - cair;
+                float q = (from - to) / (from + to);
+                float r0 = q * q;
+                refl = r0 + (1.0f - r0) * powf(icair, 5.0f);
+                f3 td = (r.d + N * ct) * ratio - N * cphi;
+                td = normalize(td);
+                f3 ctp = tp * (1.0f - refl);
+                if (can_spawn && !is_zero(ctp))
+                    push_path(Q, nbuf, level + 1, s.p + (td * 0.0001f), r.time, td,
+                              (inside ? 0u : PF_INSIDE) | (inside ? 0u : PF_ATTEN), ctp, slot, att,
+                              child_digits(digits, level, next_child));
+                next_child++;
+            }
+            f3 rd = reflect(-r.d, N);
+            f3 ctp = tp * refl;
+            if (can_spawn && !is_zero(ctp))
+                push_path(Q, nbuf, level + 1, s.p + (rd * 0.0001f), r.time, rd,
+                          (inside ? PF_INSIDE : 0u) | (inside ? PF_ATTEN : 0u), ctp, slot, att,
+                          child_digits(digits, level, next_child));
+        }
+    }
+}
+
+// Visibility of the queued light samples; unoccluded ones are added to their sample.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_shadow(DevScene S, CameraParams cam, WaveQueues Q, uint32_t level) {
+    const uint32_t n = min(Q.counts[AZ_COUNT_SHADOW + level], Q.cap_s);
+    uint32_t *cnt = cam.count_traversal ? Q.counts + AZ_COUNT_NODES : nullptr;
+    for (uint32_t i = blockIdx.x * BLOCK + threadIdx.x; i < n; i += gridDim.x * BLOCK) {
+        float4 o = Q.so[i], d = Q.sd[i], c = Q.sc[i];
+        uint32_t meta = Q.smeta[i];
+        uint32_t kind = meta >> 30, uid = meta & 0x3FFFFFFFu;
+        Ray r;
+        r.o = mk(o.x, o.y, o.z);
+        r.d = mk(d.x, d.y, d.z);
+        r.time = o.w;
+        Hit h;
+        bool visible;
+        if (kind == SHADOW_ENTITY) {
+            bool any = trace<Q_CLOSEST>(S, r, false, 0.0f, FLT_MAX, h, cnt);
+            visible = !any || (S.ents[h.ent].uid & 0x3FFFFFFFu) == uid;
+        } else {
+            visible = !trace<Q_ANY>(S, r, false, 0.0f, kind == SHADOW_ANY ? FLT_MAX : d.w, h, cnt);
+        }
+        if (visible) add_accum(Q.accum, __float_as_uint(c.w), mk(c.x, c.y, c.z));
+    }
+}
+
+// ComputeSampleWeight (src/azimuth_main.cpp:1209-1254) for every sample of the wave.
+__global__ void k_splat(CameraParams cam, WaveQueues Q, uint64_t wave_start, uint32_t n, az_pixel *film) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (Q.counts[AZ_COUNT_OVERFLOW]) return;   // the wave is re-run
+    uint32_t row, col, sx, sy;
+    sample_of(cam, wave_start + i, row, col, sx, sy);
+    float4 a = Q.accum[i];
+    float4 *f = reinterpret_cast<float4 *>(film);
+    if (cam.filter == AZ_Filter_Box) {
+        atomicAdd(&f[(size_t)row * cam.width + col], make_float4(a.x, a.y, a.z, 1.0f));
+        return;
+    }
+    float cx = (float)col + (0.5f * cam.inv_sqrt + (float)sx * cam.inv_sqrt);
+    float cy = (float)row + (0.5f * cam.inv_sqrt + (float)sy * cam.inv_sqrt);
+    int32_t w1 = (int32_t)cam.width - 1, h1 = (int32_t)cam.height - 1;
+    int32_t x0 = max((int32_t)col - cam.gk, 0), x1 = min((int32_t)col + cam.gk, w1);
+    int32_t y0 = max((int32_t)row - cam.gk, 0), y1 = min((int32_t)row + cam.gk, h1);
+    for (int32_t gy = y0; gy <= y1; gy++)
+        for (int32_t gx = x0; gx <= x1; gx++) {
+            float dx = cx - ((float)gx + 0.5f), dy = cy - ((float)gy + 0.5f);
+            float d2 = dx * dx + dy * dy;
+            float g = cam.g_norm * expf(cam.g_neg * d2);
+            atomicAdd(&f[(size_t)gy * cam.width + gx], make_float4(a.x * g, a.y * g, a.z * g, g));
+        }
+}
+
+constexpr int kBlock = 128;
+
+}  // namespace
+
+// Camera basis and pixel steps of ProduceImageInLinearSpace
+// (src/azimuth_main.cpp:1265-1347), evaluated on the host in float.
+int SetupCamera(const az_camera *c, az_scissor sc, int32_t filter, uint32_t cull, const az_epsilon_values *eps,
+                uint64_t seed, CameraParams &cam) {
+    using azd::f3;
+    auto v = [](const az_vec3 &a) { return azd::mk(a.x, a.y, a.z); };
+    if (c->Resolution.x == 0 || c->Resolution.y == 0 || c->Resolution.x > 65535 || c->Resolution.y > 65535)
+        return SetError(AZ_ERR_INVALID_ARGUMENT, "camera resolution must be 1..65535 per axis");
+    f3 gaze = v(c->Gaze);
+    if (c->GazeIsPoint) gaze = v(c->Gaze) - v(c->Position);
+    f3 gn = azd::normalize(gaze);
+    f3 az = -gn, ax, ay;
+    if (c->IsLeftHanded) {
+        ax = azd::normalize(azd::cross(azd::normalize(v(c->Up)), gn));
+        ay = azd::cross(ax, az);
+    } else {
+        ax = azd::normalize(azd::cross(gn, azd::normalize(v(c->Up))));
+        ay = azd::cross(az, ax);
+    }
+    float fdn = 1.0f;
+    if (c->FocusDistance != 0.0f) fdn = c->FocusDistance / c->NearDistance;
+    memset(&cam, 0, sizeof(cam));
+    cam.width = c->Resolution.x;
+    cam.height = c->Resolution.y;
+    az_vec4 np = c->NearPlane;   // r, l, b, t
+    if (c->Type == AZ_Camera_Simple) {
+        float hh = c->NearDistance * tanf((c->FovY / 2.0f / 180.0f) * (float)3.14159265359);
+        float ar = (float)cam.width / (float)cam.height;
+        float wh = ar * hh;
+        np.w = +hh;
+        np.z = -hh;
+        np.x = +wh;
+        np.y = -wh;
+    }
+    float psx = (np.x - np.y) / (float)cam.width, psy = (np.w - np.z) / (float)cam.height;
+    cam.stepx = ax * psx * fdn;
+    cam.stepy = ay * psy * fdn;
+    f3 tl = v(c->Position) + c->NearDistance * gn + np.y * ax + np.w * ay;
+    cam.base = (tl - v(c->Position)) * fdn;
+    cam.pos = v(c->Position);
+    cam.axx = ax;
+    cam.axy = ay;
+    cam.aperture = c->ApertureSize;
+    cam.sqrt_spp = (uint32_t)sqrtf((float)c->SampleCount);
+    cam.inv_sqrt = 1.0f / cam.sqrt_spp;
+    float gr = 1.5f, sigma = gr / 3.0f, two = 2.0f * (sigma * sigma);
+    cam.g_neg = -1.0f / two;
+    cam.g_norm = 1.0f / (two * (float)3.14159265359);
+    cam.gk = (int32_t)ceilf(gr - 0.5f);
+    uint32_t r1 = std::min(sc.Max.y, cam.height), c1 = std::min(sc.Max.x, cam.width);
+    cam.r0 = sc.Min.y;
+    cam.c0 = sc.Min.x;
+    cam.hsc = r1 > cam.r0 ? r1 - cam.r0 : 0;
+    cam.wsc = c1 > cam.c0 ? c1 - cam.c0 : 0;
+    cam.npix = (uint64_t)cam.hsc * cam.wsc;
+    if (filter != AZ_Filter_Box && filter != AZ_Filter_Gaussian) return SetError(AZ_ERR_INVALID_ARGUMENT, "unknown filter");
+    cam.filter = filter;
+    cam.seed = seed;
+    cam.eps_isect = eps ? eps->Intersection : 0.0f;
+    cam.eps_shadow = eps ? eps->ShadowRay : 0.000275f;
+    cam.cull = cull;
+    return AZ_OK;
+}
+
+WaveBuffers::~WaveBuffers() {
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+}
+
+int WaveBuffers::Ensure(uint32_t chunk, uint32_t cap_q, uint32_t cap_s) {
+    if (chunk <= this->chunk && cap_q <= q.cap_q && cap_s <= q.cap_s && !ptrs.empty()) return AZ_OK;
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    ptrs.clear();
+    memset(&q, 0, sizeof(q));
+    auto alloc = [&](size_t bytes) -> void * {
+        void *p = nullptr;
+        if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+        ptrs.push_back(p);
+        return p;
+    };
+    for (int b = 0; b < 2; b++) {
+        q.o[b] = (float4 *)alloc((size_t)cap_q * sizeof(float4));
+        q.d[b] = (float4 *)alloc((size_t)cap_q * sizeof(float4));
+        q.tp[b] = (float4 *)alloc((size_t)cap_q * sizeof(float4));
+        q.att[b] = (float4 *)alloc((size_t)cap_q * sizeof(float4));
+        q.digits[b] = (uint32_t *)alloc((size_t)cap_q * sizeof(uint32_t));
+        if (!q.o[b] || !q.d[b] || !q.tp[b] || !q.att[b] || !q.digits[b]) return SetError(AZ_ERR_OUT_OF_MEMORY, "wave queues");
+    }
+    q.hit = (uint4 *)alloc((size_t)cap_q * sizeof(uint4));
+    q.so = (float4 *)alloc((size_t)cap_s * sizeof(float4));
+    q.sd = (float4 *)alloc((size_t)cap_s * sizeof(float4));
+    q.sc = (float4 *)alloc((size_t)cap_s * sizeof(float4));
+    q.smeta = (uint32_t *)alloc((size_t)cap_s * sizeof(uint32_t));
+    q.accum = (float4 *)alloc((size_t)chunk * sizeof(float4));
+    q.counts = (uint32_t *)alloc(AZ_COUNT_TOTAL * sizeof(uint32_t));
+    if (!q.hit || !q.so || !q.sd || !q.sc || !q.smeta || !q.accum || !q.counts)
+        return SetError(AZ_ERR_OUT_OF_MEMORY, "wave queues");
+    q.cap_q = cap_q;
+    q.cap_s = cap_s;
+    this->chunk = chunk;
+    return AZ_OK;
+}
+
+// Renders samples [start, start+n) of the scissor into `film`; returns the
+// per-wave counters (path and shadow queue sizes per level, overflow flag).
+static int RenderWave(const GpuScene &G, const CameraParams &cam, WaveBuffers &W, uint64_t start, uint32_t n,
+                      az_pixel *film, cudaStream_t st, int sms, RenderCounters &rc) {
+    WaveQueues Q = W.q;
+    AZ_CUDA_TRY(cudaMemsetAsync(Q.counts, 0, AZ_COUNT_TOTAL * sizeof(uint32_t), st));
+    uint32_t first = n;
+    AZ_CUDA_TRY(cudaMemcpyAsync(Q.counts + 1, &first, sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    k_camera<<<(n + 255) / 256, 256, 0, st>>>(cam, Q, start, n);
+    rc.launches++;
+    const uint32_t levels = std::min<uint32_t>(G.dev.max_depth + 1, AZ_MAX_LEVELS - 2);
+    const int grid = sms * 16;
+    for (uint32_t L = 1; L <= levels; L++) {
+        k_extend<kBlock><<<grid, kBlock, 0, st>>>(G.dev, cam, Q, L);
+        k_shade<kBlock><<<grid, kBlock, 0, st>>>(G.dev, cam, Q, start, L);
+        k_shadow<kBlock><<<grid, kBlock, 0, st>>>(G.dev, cam, Q, L);
+        rc.launches += 3;
+    }
+    k_splat<<<(n + 255) / 256, 256, 0, st>>>(cam, Q, start, n, film);
+    rc.launches++;
+    AZ_CUDA_TRY(cudaGetLastError());
+    return AZ_OK;
+}
+
+int Render(GpuScene &G, az_pixel *film, const az_camera *camera, const az_epsilon_values *eps, az_scissor sc,
+           int32_t filter, uint32_t cull, const az_render_opts *opts, cudaStream_t st, az_render_stats *stats) {
+    CameraParams cam;
+    int rc = SetupCamera(camera, sc, filter, cull, eps, opts ? opts->seed : 0, cam);
+    if (rc != AZ_OK) return rc;
+    cam.count_traversal = opts && (opts->flags & AZ_FLAG_COUNT_TRAVERSAL) ? 1u : 0u;
+    if (G.dev.max_depth + 1 > AZ_MAX_LEVELS - 2) return SetError(AZ_ERR_UNSUPPORTED, "MaxRecursionDepth above 60");
+    uint64_t total = cam.npix * (uint64_t)cam.sqrt_spp * cam.sqrt_spp;
+    if (stats) memset(stats, 0, sizeof(*stats));
+    if (total == 0) return AZ_OK;
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, G.device);
+    uint32_t chunk = opts && opts->chunk_samples ? opts->chunk_samples : (1u << 22);
+    chunk = (uint32_t)std::min<uint64_t>(chunk, total);
+    uint32_t per_node_shadow = G.dev.light_count + (G.dev.use_env_map ? 1u : 0u);
+    WaveBuffers &W = G.waves;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (stats) {
+        AZ_CUDA_TRY(cudaEventCreate(&e0));
+        AZ_CUDA_TRY(cudaEventCreate(&e1));
+        AZ_CUDA_TRY(cudaEventRecord(e0, st));
+    }
+    RenderCounters counters{};
+    std::vector<uint32_t> host_counts(AZ_COUNT_TOTAL);
+    uint64_t pos = 0;
+    while (pos < total) {
+        uint32_t n = (uint32_t)std::min<uint64_t>(chunk, total - pos);
+        uint32_t cap_q = std::max<uint32_t>(n + n / 2, 1024);
+        uint32_t cap_s = std::max<uint32_t>((uint32_t)std::min<uint64_t>((uint64_t)cap_q * std::max(per_node_shadow, 1u),
+                                                                         (uint64_t)n * 4), 1024);
+        rc = W.Ensure(n, cap_q, cap_s);
+        if (rc != AZ_OK) return rc;
+        rc = RenderWave(G, cam, W, pos, n, film, st, sms, counters);
+        if (rc != AZ_OK) return rc;
+        AZ_CUDA_TRY(cudaMemcpyAsync(host_counts.data(), W.q.counts, AZ_COUNT_TOTAL * sizeof(uint32_t),
+                                    cudaMemcpyDeviceToHost, st));
+        AZ_CUDA_TRY(cudaStreamSynchronize(st));
+        if (host_counts[AZ_COUNT_OVERFLOW]) {
+            // a queue overflowed: this wave wrote nothing; retry it with half the samples
+            if (n <= 1024) return SetError(AZ_ERR_OUT_OF_MEMORY, "wave queue overflow with 1024 samples");
+            chunk = std::max<uint32_t>(n / 2, 1024);
+            counters.retries++;
+            continue;
+        }
+        for (uint32_t L = 1; L < AZ_MAX_LEVELS; L++) {
+            counters.extend += host_counts[L];
+            counters.shadow += host_counts[AZ_COUNT_SHADOW + L];
+        }
+        counters.nodes += host_counts[AZ_COUNT_NODES];
+        counters.prims += host_counts[AZ_COUNT_NODES + 1];
+        counters.chunks++;
+        pos += n;
+    }
+    if (stats) {
+        AZ_CUDA_TRY(cudaEventRecord(e1, st));
+        AZ_CUDA_TRY(cudaEventSynchronize(e1));
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        stats->samples = total;
+        stats->extend_rays = counters.extend;
+        stats->shadow_rays = counters.shadow;
+        stats->chunks = counters.chunks;
+        stats->retries = counters.retries;
+        stats->kernel_launches = counters.launches;
+        stats->gpu_ms = ms;
+        stats->reserved[0] = (uint32_t)counters.nodes;
+        stats->reserved[1] = (uint32_t)(counters.nodes >> 32);
+        stats->reserved[2] = (uint32_t)counters.prims;
+        stats->reserved[3] = (uint32_t)(counters.prims >> 32);
+    }
+    return AZ_OK;
+}
+
+// ---- closest-hit queries for the parity tests ----
+namespace {
+__global__ void k_closest(DevScene S, const az_ray3 *rays, uint32_t n, uint32_t cull, float eps, uint32_t *hit,
+                          uint32_t *uid, uint32_t *face, float *t) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    az_ray3 rr = rays[i];
+    Ray r;
+    r.o = mk(rr.Origin.x, rr.Origin.y, rr.Origin.z);
+    r.d = mk(rr.Direction.x, rr.Direction.y, rr.Direction.z);
+    r.time = rr.T;
+    Hit h;
+    bool ok = trace<Q_CLOSEST>(S, r, cull != 0, eps, FLT_MAX, h);
+    hit[i] = ok ? 1u : 0u;
+    uid[i] = ok ? S.ents[h.ent].uid : 0xFFFFFFFFu;
+    face[i] = ok && h.prim != 0xFFFFFFFFu ? S.tri_attr[h.prim].face_id : 0xFFFFFFFFu;
+    t[i] = ok ? h.t : 0.0f;
+}
+}  // namespace
+
+int ClosestHit(GpuScene &G, const az_ray3 *rays, uint32_t n, int32_t cull, float eps, uint32_t *out_hit,
+               uint32_t *out_uid, uint32_t *out_face, float *out_t, cudaStream_t st) {
+    if (n == 0) return AZ_OK;
+    void *buf = nullptr;
+    size_t bytes = (size_t)n * (sizeof(az_ray3) + 3 * sizeof(uint32_t) + sizeof(float)) + 64;
+    AZ_CUDA_TRY(cudaMalloc(&buf, bytes));
+    char *p = (char *)buf;
+    az_ray3 *d_rays = (az_ray3 *)p;
+    p += ((size_t)n * sizeof(az_ray3) + 15) & ~(size_t)15;
+    uint32_t *d_hit = (uint32_t *)p;
+    uint32_t *d_uid = d_hit + n;
+    uint32_t *d_face = d_uid + n;
+    float *d_t = (float *)(d_face + n);
+    int rc = AZ_OK;
+    cudaError_t e = cudaMemcpyAsync(d_rays, rays, (size_t)n * sizeof(az_ray3), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        k_closest<<<(n + 127) / 128, 128, 0, st>>>(G.dev, d_rays, n, (uint32_t)cull, eps, d_hit, d_uid, d_face, d_t);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out_hit, d_hit, n * 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out_uid, d_uid, n * 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out_face, d_face, n * 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out_t, d_t, n * 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) rc = CudaError(e, "closest-hit query");
+    cudaFree(buf);
+    return rc;
+}
+
+}  // namespace az

@@ -1,0 +1,61 @@
+// Wavefront render state shared between the render driver and the C-ABI.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "az_device_math.cuh"
+
+namespace az {
+
+constexpr uint32_t AZ_MAX_LEVELS = 64;                   // tree levels kept in the counters
+constexpr uint32_t AZ_COUNT_SHADOW = AZ_MAX_LEVELS;      // shadow-queue sizes per level
+constexpr uint32_t AZ_COUNT_OVERFLOW = 2 * AZ_MAX_LEVELS;
+constexpr uint32_t AZ_COUNT_NODES = 2 * AZ_MAX_LEVELS + 2;  // node visits, primitive visits
+constexpr uint32_t AZ_COUNT_TOTAL = 2 * AZ_MAX_LEVELS + 8;
+
+// Camera and film parameters of one render call (ProduceImageInLinearSpace's
+// locals, src/azimuth_main.cpp:1265-1347).
+struct CameraParams {
+    azd::f3 base, pos, axx, axy, stepx, stepy;
+    float aperture, inv_sqrt;
+    uint32_t sqrt_spp, width, height;
+    uint32_t r0, c0, wsc, hsc;     // scissor origin and size
+    uint64_t npix;
+    int32_t filter;
+    float g_norm, g_neg;
+    int32_t gk;
+    uint64_t seed;
+    float eps_isect, eps_shadow;
+    uint32_t cull;
+    uint32_t count_traversal;
+};
+
+// Device queues of one wave of camera samples (structure of arrays).
+struct WaveQueues {
+    float4 *o[2], *d[2], *tp[2], *att[2];   // path nodes, ping-pong by level parity
+    uint32_t *digits[2];
+    uint4 *hit;
+    uint32_t cap_q;
+    float4 *so, *sd, *sc;                   // shadow queue
+    uint32_t *smeta;
+    uint32_t cap_s;
+    float4 *accum;                          // per-sample radiance sums
+    uint32_t *counts;                       // see AZ_COUNT_*
+};
+
+struct WaveBuffers {
+    WaveQueues q{};
+    uint32_t chunk = 0;
+    std::vector<void *> ptrs;
+    ~WaveBuffers();
+    int Ensure(uint32_t chunk, uint32_t cap_q, uint32_t cap_s);
+};
+
+struct RenderCounters {
+    uint64_t extend = 0, shadow = 0, nodes = 0, prims = 0, launches = 0;
+    uint32_t chunks = 0, retries = 0;
+};
+
+}  // namespace az

@@ -1,0 +1,612 @@
+// Flattening azimuth's scene pointer graph into the device layout of
+// az_scene_dev.cuh, upload, and BVH construction.
+//
+// The entity tree under scene.BVHRoot (src/azimuth_bvh.cpp) is only walked to
+// find its leaves; the device BVHs are rebuilt on the GPU.  Mesh instances
+// (src/azimuth_main.cpp:244-281) whose transformation, inverse and motion are
+// bitwise identical are merged into one bottom-level BVH: every per-instance
+// quantity azimuth computes (local ray, world t) is then the same for all of
+// them, so only the choice between exactly tied hits can differ.
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+
+#include "az_internal.h"
+
+namespace az {
+
+GpuScene::~GpuScene() {
+    for (auto &b : bufs)
+        if (b.ptr) cudaFree(b.ptr);
+}
+
+void *GpuScene::Alloc(size_t bytes) {
+    void *p = nullptr;
+    if (bytes == 0) bytes = 16;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+    bufs.push_back(DevBuf{p, bytes});
+    device_bytes += bytes;
+    return p;
+}
+
+namespace {
+
+using azd::f3;
+using azd::m34;
+using azd::mk;
+
+m34 ToM34(const az_mat4 &m) {
+    m34 r;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 4; j++) r.e[4 * i + j] = m.E[i][j];
+    return r;
+}
+
+bool IsIdentity(const m34 &m) {
+    static const float id[12] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0};
+    return memcmp(m.e, id, sizeof(id)) == 0;
+}
+
+struct Box {
+    float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX};
+    float hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    void grow(float x, float y, float z) {
+        lo[0] = fminf(lo[0], x); lo[1] = fminf(lo[1], y); lo[2] = fminf(lo[2], z);
+        hi[0] = fmaxf(hi[0], x); hi[1] = fmaxf(hi[1], y); hi[2] = fmaxf(hi[2], z);
+    }
+    void grow(const Box &b) {
+        grow(b.lo[0], b.lo[1], b.lo[2]);
+        grow(b.hi[0], b.hi[1], b.hi[2]);
+    }
+    bool valid() const { return lo[0] <= hi[0] && lo[1] <= hi[1] && lo[2] <= hi[2]; }
+};
+
+// World box of a local box under an affine transform and linear motion over
+// the shutter [0,1] (the bound azimuth's importer uses, src/azimuth_xml.cpp:3791-3875).
+Box XformBox(const Box &b, const m34 &m, const float motion[3]) {
+    Box r;
+    for (int c = 0; c < 8; c++) {
+        f3 p = mk(c & 1 ? b.hi[0] : b.lo[0], c & 2 ? b.hi[1] : b.lo[1], c & 4 ? b.hi[2] : b.lo[2]);
+        // evaluate in double and round outward so the box stays conservative
+        double x = (double)m.e[0] * p.x + (double)m.e[1] * p.y + (double)m.e[2] * p.z + m.e[3];
+        double y = (double)m.e[4] * p.x + (double)m.e[5] * p.y + (double)m.e[6] * p.z + m.e[7];
+        double z = (double)m.e[8] * p.x + (double)m.e[9] * p.y + (double)m.e[10] * p.z + m.e[11];
+        r.grow(nextafterf((float)x, -FLT_MAX), nextafterf((float)y, -FLT_MAX), nextafterf((float)z, -FLT_MAX));
+        r.grow(nextafterf((float)x, FLT_MAX), nextafterf((float)y, FLT_MAX), nextafterf((float)z, FLT_MAX));
+    }
+    if (motion[0] != 0.0f || motion[1] != 0.0f || motion[2] != 0.0f) {
+        Box m2 = r;
+        for (int k = 0; k < 3; k++) {
+            m2.lo[k] += motion[k];
+            m2.hi[k] += motion[k];
+        }
+        r.grow(m2);
+    }
+    return r;
+}
+
+struct GroupKey {
+    unsigned char bytes[2 * sizeof(m34) + 12 + 4];
+    bool operator<(const GroupKey &o) const { return memcmp(bytes, o.bytes, sizeof(bytes)) < 0; }
+};
+
+struct HostGroup {
+    azd::DevGroup g{};
+    std::vector<azd::DevTri> tris;
+    std::vector<azd::DevTriAttr> attr;
+    Box local;
+};
+
+struct Flattener {
+    const az_scene *s;
+    std::vector<azd::DevEntity> ents;
+    std::vector<Box> ent_box;            // world boxes of sphere entities
+    std::vector<HostGroup> groups;
+    std::map<GroupKey, uint32_t> group_of;
+    int raw_group = -1;
+    std::string err;
+
+    azd::DevEntity BaseEntity(const az_entity *e) {
+        azd::DevEntity d;
+        memset(&d, 0, sizeof(d));
+        d.inv = ToM34(e->InvTransformationMatrix);
+        d.xf = ToM34(e->TransformationMatrix);
+        d.motion[0] = e->MotionVector.x; d.motion[1] = e->MotionVector.y; d.motion[2] = e->MotionVector.z;
+        d.radiance[0] = e->Radiance.x; d.radiance[1] = e->Radiance.y; d.radiance[2] = e->Radiance.z;
+        d.is_emitter = e->IsEmitter ? 1u : 0u;
+        d.texture_index = e->TextureIndex;
+        d.material = e->MaterialIndex;
+        d.uid = e->UniqueEntityID;
+        return d;
+    }
+
+    bool AddTriangle(HostGroup &g, const az_entity *t, uint32_t ent) {
+        azd::DevTri tr;
+        const az_vec3 &p0 = t->P0, &p1 = t->P1, &p2 = t->P2;
+        // E1 = P0-P1 and E2 = P0-P2 in float: the A..H of src/azimuth_main.cpp:158-168
+        tr.a = make_float4(p0.x, p0.y, p0.z, p0.x - p1.x);
+        tr.b = make_float4(p0.y - p1.y, p0.z - p1.z, p0.x - p2.x, p0.y - p2.y);
+        tr.c = make_float4(p0.z - p2.z, t->FaceNormal.x, t->FaceNormal.y, t->FaceNormal.z);
+        g.tris.push_back(tr);
+        azd::DevTriAttr a;
+        memset(&a, 0, sizeof(a));
+        a.n0[0] = t->N0.x; a.n0[1] = t->N0.y; a.n0[2] = t->N0.z;
+        a.n1[0] = t->N1.x; a.n1[1] = t->N1.y; a.n1[2] = t->N1.z;
+        a.n2[0] = t->N2.x; a.n2[1] = t->N2.y; a.n2[2] = t->N2.z;
+        a.uv0[0] = t->UV0.x; a.uv0[1] = t->UV0.y;
+        a.uv1[0] = t->UV1.x; a.uv1[1] = t->UV1.y;
+        a.uv2[0] = t->UV2.x; a.uv2[1] = t->UV2.y;
+        a.shading_mode = t->ShadingMode;
+        a.texture_index = t->TextureIndex;
+        a.face_id = t->ID;
+        a.entity = ent;
+        g.attr.push_back(a);
+        g.local.grow(p0.x, p0.y, p0.z);
+        g.local.grow(p1.x, p1.y, p1.z);
+        g.local.grow(p2.x, p2.y, p2.z);
+        return true;
+    }
+
+    // Depth-first walk of an entity tree to its leaves.
+    template <typename F>
+    bool Walk(const az_entity *root, F &&leaf, const char *what) {
+        if (!root) {
+            err = std::string("null entity in ") + what;
+            return false;
+        }
+        std::vector<const az_entity *> st{root};
+        size_t guard = 0;
+        while (!st.empty()) {
+            const az_entity *e = st.back();
+            st.pop_back();
+            if (++guard > (size_t)1 << 34) {
+                err = std::string("entity tree too large in ") + what;
+                return false;
+            }
+            if (e->Type == AZ_Entity_BVHNode) {
+                if (!e->Left || !e->Right) {
+                    err = std::string("BVH node without children in ") + what;
+                    return false;
+                }
+                st.push_back(e->Right);
+                st.push_back(e->Left);
+            } else if (!leaf(e)) {
+                return false;
+            }
+        }
+        return true;
+    }
+
+    bool Run() {
+        return Walk(s->BVHRoot, [&](const az_entity *e) -> bool {
+            uint32_t idx = (uint32_t)ents.size();
+            azd::DevEntity d = BaseEntity(e);
+            switch (e->Type) {
+                case AZ_Entity_Sphere: {
+                    d.type = azd::ENT_SPHERE;
+                    d.center[0] = e->Center.x; d.center[1] = e->Center.y; d.center[2] = e->Center.z;
+                    d.radius = e->Radius;
+                    Box local;
+                    float r = fabsf(e->Radius);
+                    local.grow(e->Center.x - r, e->Center.y - r, e->Center.z - r);
+                    local.grow(e->Center.x + r, e->Center.y + r, e->Center.z + r);
+                    ents.push_back(d);
+                    ent_box.push_back(XformBox(local, d.xf, d.motion));
+                    return true;
+                }
+                case AZ_Entity_Triangle: {
+                    // top-level triangle: tested with the world ray as is
+                    d.type = azd::ENT_TRIANGLE;
+                    if (raw_group < 0) {
+                        raw_group = (int)groups.size();
+                        groups.emplace_back();
+                        HostGroup &g = groups.back();
+                        g.g.inv = ToM34(az_mat4{{{1, 0, 0, 0}, {0, 1, 0, 0}, {0, 0, 1, 0}, {0, 0, 0, 1}}});
+                        g.g.xf = g.g.inv;
+                        g.g.raw = 1;
+                        g.g.identity = 1;
+                    }
+                    d.group = (uint32_t)raw_group;
+                    ents.push_back(d);
+                    ent_box.push_back(Box());
+                    return AddTriangle(groups[raw_group], e, idx);
+                }
+                case AZ_Entity_MeshInstance: {
+                    d.type = azd::ENT_INSTANCE;
+                    if (!e->Mesh) {
+                        err = "mesh instance without mesh";
+                        return false;
+                    }
+                    GroupKey key;
+                    memcpy(key.bytes, &d.inv, sizeof(m34));
+                    memcpy(key.bytes + sizeof(m34), &d.xf, sizeof(m34));
+                    memcpy(key.bytes + 2 * sizeof(m34), d.motion, 12);
+                    memset(key.bytes + 2 * sizeof(m34) + 12, 0, 4);
+                    auto it = group_of.find(key);
+                    uint32_t gi;
+                    if (it == group_of.end()) {
+                        gi = (uint32_t)groups.size();
+                        group_of.emplace(key, gi);
+                        groups.emplace_back();
+                        HostGroup &g = groups.back();
+                        g.g.inv = d.inv;
+                        g.g.xf = d.xf;
+                        memcpy(g.g.motion, d.motion, 12);
+                        g.g.identity = IsIdentity(d.inv) && IsIdentity(d.xf) && d.motion[0] == 0.0f &&
+                                       d.motion[1] == 0.0f && d.motion[2] == 0.0f;
+                    } else {
+                        gi = it->second;
+                    }
+                    d.group = gi;
+                    ents.push_back(d);
+                    ent_box.push_back(Box());
+                    HostGroup *gp = &groups[gi];
+                    return Walk(e->Mesh->BVH, [&](const az_entity *t) -> bool {
+                        if (t->Type != AZ_Entity_Triangle) {
+                            err = "mesh BVH leaf is not a triangle";
+                            return false;
+                        }
+                        return AddTriangle(*gp, t, idx);
+                    }, "mesh BVH");
+                }
+                default:
+                    err = "unexpected entity type";
+                    return false;
+            }
+        }, "scene BVH");
+    }
+};
+
+azd::DevTexture ToDevTexture(const az_texture &t, std::vector<unsigned char> &texels, std::vector<uint32_t> &perms,
+                             std::string &err) {
+    azd::DevTexture d;
+    memset(&d, 0, sizeof(d));
+    d.type = t.Type;
+    d.format = t.PixelFormat;
+    d.width = t.Width;
+    d.height = t.Height;
+    d.inv_width = t.InvWidth;
+    d.inv_height = t.InvHeight;
+    d.normalizer = t.Normalizer;
+    d.bump_mul = t.BumpMapMultiplier;
+    d.wrap = t.WrapMode;
+    d.filter = t.Filter;
+    d.blend = t.BlendMode;
+    d.bump = t.BumpMap;
+    if (t.Type == AZ_TextureType_PerlinNoise) {
+        d.scaling = t.ScalingFactor;
+        d.appearance = t.PerlinAppearance;
+        d.perm_offset = (uint32_t)perms.size();
+        for (int i = 0; i < AZ_PERLIN_GRADIENT_SIZE; i++) perms.push_back(t.Perm[i]);
+    } else if (t.Pixels && t.Width && t.Height) {
+        size_t bpp = t.PixelFormat == AZ_PixelFormat_RGB_F32 ? 12 : 3;
+        size_t bytes = (size_t)t.Width * t.Height * bpp;
+        size_t off = (texels.size() + 15) & ~(size_t)15;
+        texels.resize(off + bytes);
+        memcpy(texels.data() + off, t.Pixels, bytes);
+        d.texel_offset = off;
+    } else {
+        d.width = d.height = 0;  // not loaded: sampling it is an error caught at validation
+    }
+    (void)err;
+    return d;
+}
+
+template <typename T>
+T *Upload(GpuScene &G, const std::vector<T> &v, cudaStream_t st, int &rc) {
+    T *p = (T *)G.Alloc(v.size() * sizeof(T));
+    if (!p) {
+        rc = SetError(AZ_ERR_OUT_OF_MEMORY, "device allocation failed");
+        return nullptr;
+    }
+    if (!v.empty()) {
+        cudaError_t e = cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) {
+            rc = CudaError(e, "cudaMemcpyAsync(scene)");
+            return nullptr;
+        }
+    }
+    return p;
+}
+
+__global__ void k_gather_tris(const azd::DevTri *src, const azd::DevTriAttr *src_attr, const uint32_t *perm,
+                              uint32_t n, azd::DevTri *dst, azd::DevTriAttr *dst_attr) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t s = perm[i];
+    dst[i] = src[s];
+    dst_attr[i] = src_attr[s];
+}
+
+__global__ void k_gather_u32(const uint32_t *src, const uint32_t *perm, uint32_t n, uint32_t *dst) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = src[perm[i]];
+}
+
+__global__ void k_tri_boxes(const azd::DevTri *t, uint32_t n, float4 *lo, float4 *hi) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    azd::DevTri tr = t[i];
+    float p0x = tr.a.x, p0y = tr.a.y, p0z = tr.a.z;
+    // P1 = P0 - E1, P2 = P0 - E2 recomputed only for bounds: widen by one ulp
+    float p1x = p0x - tr.a.w, p1y = p0y - tr.b.x, p1z = p0z - tr.b.y;
+    float p2x = p0x - tr.b.z, p2y = p0y - tr.b.w, p2z = p0z - tr.c.x;
+    float4 l = make_float4(fminf(p0x, fminf(p1x, p2x)), fminf(p0y, fminf(p1y, p2y)), fminf(p0z, fminf(p1z, p2z)), 0);
+    float4 h = make_float4(fmaxf(p0x, fmaxf(p1x, p2x)), fmaxf(p0y, fmaxf(p1y, p2y)), fmaxf(p0z, fmaxf(p1z, p2z)), 0);
+    l.x = nextafterf(l.x, -FLT_MAX); l.y = nextafterf(l.y, -FLT_MAX); l.z = nextafterf(l.z, -FLT_MAX);
+    h.x = nextafterf(h.x, FLT_MAX); h.y = nextafterf(h.y, FLT_MAX); h.z = nextafterf(h.z, FLT_MAX);
+    lo[i] = l;
+    hi[i] = h;
+}
+
+}  // namespace
+
+int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_t st, GpuScene **out) {
+    if (!scene || !out) return SetError(AZ_ERR_INVALID_ARGUMENT, "null scene");
+    *out = nullptr;
+    std::unique_ptr<GpuScene> G(new GpuScene());
+    G->device = opts ? opts->device : 0;
+    Flattener F;
+    F.s = scene;
+    if (!scene->BVHRoot) return SetError(AZ_ERR_INVALID_SCENE, "scene has no BVHRoot");
+    if (!F.Run()) return SetError(AZ_ERR_INVALID_SCENE, F.err);
+
+    // ---- materials, textures, lights, validation ----
+    std::vector<azd::DevMaterial> mats(scene->MaterialCount);
+    for (uint32_t i = 0; i < scene->MaterialCount; i++) {
+        const az_material &m = scene->Materials[i];
+        azd::DevMaterial &d = mats[i];
+        memset(&d, 0, sizeof(d));
+        memcpy(d.ambient, &m.AmbientReflectance, 12);
+        memcpy(d.diffuse, &m.DiffuseReflectance, 12);
+        memcpy(d.specular, &m.SpecularReflectance, 12);
+        memcpy(d.mirror, &m.MirrorReflectance, 12);
+        memcpy(d.transparency, &m.Transparency, 12);
+        d.refraction_index = m.RefractionIndex;
+        d.glossiness = m.Glossiness;
+        d.exponent = m.BRDF.Exponent;
+        d.brdf_refractive_index = m.BRDF.RefractiveIndex;
+        d.brdf_type = m.BRDF.Type;
+        uint32_t tb[3], mb[3];
+        memcpy(tb, &m.Transparency, 12);
+        memcpy(mb, &m.MirrorReflectance, 12);
+        d.transparent = (tb[0] | tb[1] | tb[2]) != 0;
+        d.is_mirror = (mb[0] | mb[1] | mb[2]) != 0;
+        if (m.BRDF.Type > AZ_BRDF_TorranceSparrow) return SetError(AZ_ERR_INVALID_SCENE, "unknown BRDF type");
+    }
+    bool uses_perlin = false;
+    std::vector<unsigned char> texels;
+    std::vector<uint32_t> perms;
+    std::vector<azd::DevTexture> texs;
+    std::string err;
+    for (uint32_t i = 0; i < scene->TextureCount; i++) {
+        texs.push_back(ToDevTexture(scene->Textures[i], texels, perms, err));
+        uses_perlin |= scene->Textures[i].Type == AZ_TextureType_PerlinNoise;
+    }
+    uint32_t bg_idx = (uint32_t)texs.size();
+    texs.push_back(ToDevTexture(scene->BackgroundTexture, texels, perms, err));
+    uint32_t env_idx = (uint32_t)texs.size();
+    texs.push_back(ToDevTexture(scene->EnvironmentMap, texels, perms, err));
+    if (scene->UseBackgroundTexture) uses_perlin |= scene->BackgroundTexture.Type == AZ_TextureType_PerlinNoise;
+    if (scene->UseEnvironmentMap) uses_perlin |= scene->EnvironmentMap.Type == AZ_TextureType_PerlinNoise;
+    if (uses_perlin && (!opts || !opts->perlin_gradients))
+        return SetError(AZ_ERR_INVALID_ARGUMENT, "a Perlin texture is used but opts.perlin_gradients is NULL");
+    auto tex_ok = [&](uint32_t ti) {
+        const azd::DevTexture &t = texs[ti];
+        return t.type == AZ_TextureType_PerlinNoise || (t.width > 0 && t.height > 0);
+    };
+    for (const azd::DevEntity &e : F.ents) {
+        if (!e.is_emitter && e.material >= scene->MaterialCount)
+            return SetError(AZ_ERR_INVALID_SCENE, "entity material index out of range");
+        if (e.texture_index && (e.texture_index > scene->TextureCount || !tex_ok(e.texture_index - 1)))
+            return SetError(AZ_ERR_INVALID_SCENE, "entity texture index out of range or texture not loaded");
+    }
+    if (scene->UseEnvironmentMap && !tex_ok(env_idx))
+        return SetError(AZ_ERR_INVALID_SCENE, "environment map not loaded");
+    if (scene->UseBackgroundTexture && !scene->UseEnvironmentMap && !tex_ok(bg_idx))
+        return SetError(AZ_ERR_INVALID_SCENE, "background texture not loaded");
+
+    std::vector<azd::DevLight> lights;
+    std::vector<azd::DevLightTri> light_tris;
+    uint32_t light_draws = 0;
+    for (uint32_t i = 0; i < scene->LightCount; i++) {
+        const az_light &L = scene->Lights[i];
+        azd::DevLight d;
+        memset(&d, 0, sizeof(d));
+        d.type = L.Type;
+        memcpy(d.position, &L.Position, 12);
+        memcpy(d.intensity, &L.Intensity, 12);
+        memcpy(d.edge0, &L.EdgeVectors[0], 12);
+        memcpy(d.edge1, &L.EdgeVectors[1], 12);
+        memcpy(d.normal, &L.Normal, 12);
+        memcpy(d.spot_dir, &L.SpotDirection, 12);
+        d.cos_half_coverage = L.CosHalfCoverage;
+        d.cos_half_falloff = L.CosHalfFallOff;
+        if (L.Type == AZ_Light_Area) light_draws += 2;
+        if (L.Type == AZ_Light_Entity) {
+            const az_entity &E = L.Entity;
+            d.uid = E.UniqueEntityID;
+            memcpy(d.intensity, &E.Radiance, 12);
+            d.inv = ToM34(E.InvTransformationMatrix);
+            d.xf = ToM34(E.TransformationMatrix);
+            if (E.Type == AZ_Entity_Sphere) {
+                d.entity_type = azd::ENT_SPHERE;
+                memcpy(d.center, &E.Center, 12);
+                d.radius = E.Radius;
+                light_draws += 2;
+            } else if (E.Type == AZ_Entity_MeshInstance && E.Mesh && E.Mesh->Triangles && E.Mesh->TriangleCount) {
+                d.entity_type = azd::ENT_INSTANCE;
+                d.tri_offset = (uint32_t)light_tris.size();
+                d.tri_count = E.Mesh->TriangleCount;
+                d.total_area = E.Mesh->TotalArea;
+                for (uint32_t k = 0; k < E.Mesh->TriangleCount; k++) {
+                    const az_triangle &T = E.Mesh->Triangles[k];
+                    light_tris.push_back(azd::DevLightTri{make_float4(T.P0.x, T.P0.y, T.P0.z, T.N.x),
+                                                          make_float4(T.P1.x, T.P1.y, T.P1.z, T.N.y),
+                                                          make_float4(T.P2.x, T.P2.y, T.P2.z, T.N.z)});
+                }
+                light_draws += 3;
+            } else {
+                return SetError(AZ_ERR_INVALID_SCENE, "entity light is neither a sphere nor a mesh with triangles");
+            }
+        } else if (L.Type > AZ_Light_Entity) {
+            return SetError(AZ_ERR_INVALID_SCENE, "unknown light type");
+        }
+        lights.push_back(d);
+    }
+
+    // ---- upload primitives, build BLAS per group and the TLAS ----
+    int rc = AZ_OK;
+    uint64_t total_tris = 0;
+    for (auto &g : F.groups) total_tris += g.tris.size();
+    if (total_tris >= (1ull << 27)) return SetError(AZ_ERR_UNSUPPORTED, "more than 2^27 triangles");
+    std::vector<azd::DevTri> all_tris;
+    std::vector<azd::DevTriAttr> all_attr;
+    all_tris.reserve(total_tris);
+    all_attr.reserve(total_tris);
+    for (auto &g : F.groups) {
+        g.g.tri_begin = (uint32_t)all_tris.size();
+        all_tris.insert(all_tris.end(), g.tris.begin(), g.tris.end());
+        all_attr.insert(all_attr.end(), g.attr.begin(), g.attr.end());
+        g.g.tri_end = (uint32_t)all_tris.size();
+        std::vector<azd::DevTri>().swap(g.tris);
+        std::vector<azd::DevTriAttr>().swap(g.attr);
+    }
+    // TLAS primitives: spheres and groups
+    std::vector<uint32_t> tlas;
+    std::vector<float4> tlo, thi;
+    for (uint32_t i = 0; i < F.ents.size(); i++) {
+        if (F.ents[i].type != azd::ENT_SPHERE) continue;
+        const Box &b = F.ent_box[i];
+        tlas.push_back(i);
+        tlo.push_back(make_float4(b.lo[0], b.lo[1], b.lo[2], 0));
+        thi.push_back(make_float4(b.hi[0], b.hi[1], b.hi[2], 0));
+    }
+    for (uint32_t gi = 0; gi < F.groups.size(); gi++) {
+        HostGroup &g = F.groups[gi];
+        if (g.g.tri_end == g.g.tri_begin) continue;
+        Box wb = g.g.raw ? g.local : XformBox(g.local, g.g.xf, g.g.motion);
+        tlas.push_back(AZD_TLAS_GROUP | gi);
+        tlo.push_back(make_float4(wb.lo[0], wb.lo[1], wb.lo[2], 0));
+        thi.push_back(make_float4(wb.hi[0], wb.hi[1], wb.hi[2], 0));
+    }
+    uint32_t node_total = 0;
+    for (auto &g : F.groups) {
+        uint32_t n = g.g.tri_end - g.g.tri_begin;
+        node_total += n > 1 ? n - 1 : (n == 1 ? 1 : 0);
+    }
+    node_total += tlas.size() > 1 ? (uint32_t)tlas.size() - 1 : (uint32_t)tlas.size();
+
+    azd::DevTri *d_tris_unsorted = (azd::DevTri *)G->Alloc(all_tris.size() * sizeof(azd::DevTri));
+    azd::DevTriAttr *d_attr_unsorted = (azd::DevTriAttr *)G->Alloc(all_attr.size() * sizeof(azd::DevTriAttr));
+    azd::DevTri *d_tris = (azd::DevTri *)G->Alloc(all_tris.size() * sizeof(azd::DevTri));
+    azd::DevTriAttr *d_attr = (azd::DevTriAttr *)G->Alloc(all_attr.size() * sizeof(azd::DevTriAttr));
+    azd::BVHNode *d_nodes = (azd::BVHNode *)G->Alloc((size_t)node_total * sizeof(azd::BVHNode));
+    float4 *d_lo = (float4 *)G->Alloc((std::max(all_tris.size(), tlas.size()) + 1) * sizeof(float4));
+    float4 *d_hi = (float4 *)G->Alloc((std::max(all_tris.size(), tlas.size()) + 1) * sizeof(float4));
+    uint32_t *d_perm = (uint32_t *)G->Alloc((std::max(all_tris.size(), tlas.size()) + 1) * sizeof(uint32_t));
+    if (!d_tris_unsorted || !d_attr_unsorted || !d_tris || !d_attr || !d_nodes || !d_lo || !d_hi || !d_perm)
+        return SetError(AZ_ERR_OUT_OF_MEMORY, "device allocation failed");
+    if (!all_tris.empty()) {
+        AZ_CUDA_TRY(cudaMemcpyAsync(d_tris_unsorted, all_tris.data(), all_tris.size() * sizeof(azd::DevTri),
+                                    cudaMemcpyHostToDevice, st));
+        AZ_CUDA_TRY(cudaMemcpyAsync(d_attr_unsorted, all_attr.data(), all_attr.size() * sizeof(azd::DevTriAttr),
+                                    cudaMemcpyHostToDevice, st));
+    }
+    uint32_t node_base = 0;
+    for (auto &g : F.groups) {
+        uint32_t n = g.g.tri_end - g.g.tri_begin;
+        if (n == 0) {
+            g.g.root = 0xFFFFFFFFu;
+            continue;
+        }
+        const int B = 256;
+        k_tri_boxes<<<(n + B - 1) / B, B, 0, st>>>(d_tris_unsorted + g.g.tri_begin, n, d_lo, d_hi);
+        AZ_CUDA_TRY(cudaGetLastError());
+        uint32_t root;
+        rc = BuildLBVH(d_lo, d_hi, n, d_nodes, node_base, g.g.tri_begin, d_perm, st, &root);
+        if (rc != AZ_OK) return rc;
+        g.g.root = root;
+        node_base += n > 1 ? n - 1 : 1;
+        k_gather_tris<<<(n + B - 1) / B, B, 0, st>>>(d_tris_unsorted + g.g.tri_begin, d_attr_unsorted + g.g.tri_begin,
+                                                     d_perm, n, d_tris + g.g.tri_begin, d_attr + g.g.tri_begin);
+        AZ_CUDA_TRY(cudaGetLastError());
+    }
+    uint32_t *d_tlas = (uint32_t *)G->Alloc((tlas.size() + 1) * sizeof(uint32_t));
+    uint32_t *d_tlas_unsorted = (uint32_t *)G->Alloc((tlas.size() + 1) * sizeof(uint32_t));
+    if (!d_tlas || !d_tlas_unsorted) return SetError(AZ_ERR_OUT_OF_MEMORY, "device allocation failed");
+    uint32_t tlas_root = 0xFFFFFFFFu;
+    if (!tlas.empty()) {
+        AZ_CUDA_TRY(cudaMemcpyAsync(d_lo, tlo.data(), tlo.size() * sizeof(float4), cudaMemcpyHostToDevice, st));
+        AZ_CUDA_TRY(cudaMemcpyAsync(d_hi, thi.data(), thi.size() * sizeof(float4), cudaMemcpyHostToDevice, st));
+        AZ_CUDA_TRY(cudaMemcpyAsync(d_tlas_unsorted, tlas.data(), tlas.size() * sizeof(uint32_t),
+                                    cudaMemcpyHostToDevice, st));
+        rc = BuildLBVH(d_lo, d_hi, (uint32_t)tlas.size(), d_nodes, node_base, 0, d_perm, st, &tlas_root);
+        if (rc != AZ_OK) return rc;
+        node_base += tlas.size() > 1 ? (uint32_t)tlas.size() - 1 : 1;
+        const int B = 256;
+        k_gather_u32<<<((uint32_t)tlas.size() + B - 1) / B, B, 0, st>>>(d_tlas_unsorted, d_perm, (uint32_t)tlas.size(),
+                                                                          d_tlas);
+        AZ_CUDA_TRY(cudaGetLastError());
+    }
+
+    std::vector<azd::DevGroup> dgroups;
+    for (auto &g : F.groups) dgroups.push_back(g.g);
+    std::vector<float> grad(3 * AZ_PERLIN_GRADIENT_SIZE, 0.0f);
+    if (opts && opts->perlin_gradients) memcpy(grad.data(), opts->perlin_gradients, grad.size() * sizeof(float));
+    if (perms.empty()) perms.push_back(0);
+    if (texels.empty()) texels.resize(16);
+
+    azd::DevScene &D = G->dev;
+    D.tris = d_tris;
+    D.tri_attr = d_attr;
+    D.ents = Upload(*G, F.ents, st, rc);
+    D.groups = Upload(*G, dgroups, st, rc);
+    D.tlas_prims = d_tlas;
+    D.nodes = d_nodes;
+    D.materials = Upload(*G, mats, st, rc);
+    D.textures = Upload(*G, texs, st, rc);
+    D.lights = Upload(*G, lights, st, rc);
+    D.light_tris = Upload(*G, light_tris, st, rc);
+    D.perlin_perm = Upload(*G, perms, st, rc);
+    D.perlin_grad = Upload(*G, grad, st, rc);
+    D.texels = Upload(*G, texels, st, rc);
+    if (rc != AZ_OK) return rc;
+    D.tlas_root = tlas_root;
+    D.ent_count = (uint32_t)F.ents.size();
+    D.group_count = (uint32_t)dgroups.size();
+    D.material_count = scene->MaterialCount;
+    D.texture_count = scene->TextureCount;
+    D.light_count = (uint32_t)lights.size();
+    D.bg_texture = bg_idx;
+    D.env_texture = env_idx;
+    memcpy(D.ambient, &scene->AmbientLight, 12);
+    memcpy(D.background, &scene->BackgroundColor, 12);
+    D.use_bg_texture = scene->UseBackgroundTexture ? 1u : 0u;
+    D.use_env_map = scene->UseEnvironmentMap ? 1u : 0u;
+    D.max_depth = scene->MaxRecursionDepth;
+    D.path_trace = scene->PathTrace ? 1u : 0u;
+    D.importance_sampling = scene->ImportanceSampling ? 1u : 0u;
+    D.light_draws = light_draws;
+    AZ_CUDA_TRY(cudaStreamSynchronize(st));
+    // the unsorted copies and build scratch are no longer needed
+    for (auto &b : G->bufs) {
+        if (b.ptr == d_tris_unsorted || b.ptr == d_attr_unsorted || b.ptr == d_lo || b.ptr == d_hi ||
+            b.ptr == d_perm || b.ptr == d_tlas_unsorted) {
+            cudaFree(b.ptr);
+            G->device_bytes -= b.bytes;
+            b.ptr = nullptr;
+        }
+    }
+    G->triangle_count = total_tris;
+    G->sphere_count = tlas.size() - dgroups.size();
+    G->node_count = node_total;
+    *out = G.release();
+    return AZ_OK;
+}
+
+}  // namespace az

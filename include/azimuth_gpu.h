@@ -1,0 +1,119 @@
+/*
+ * azimuth_gpu.h -- C-ABI of the B200 render path.
+ *
+ * Drop-in for azimuth's render core: the scene, camera and epsilon structs are
+ * azimuth's own (see az_abi.h), and the film is azimuth's `pixel` buffer
+ * ({rgb sum, weight sum} per pixel, src/azimuth_main.cpp:45-48).  No function
+ * throws, traps the GPU or falls back to the CPU; every call returns an
+ * AZ_* status and az_gpu_last_error() describes the last failure of the
+ * calling thread.
+ *
+ * Randomness: azimuth's Random01 (src/azimuth_math.cpp:1-8, libc rand()) is
+ * replaced by a counter-based RNG.  Every TraceRay activation of a camera
+ * sample is a node of the sample's path tree; draw `dim` of node (level,
+ * digits) of sample (SampleX, SampleY) of pixel (Row, Col) is lane dim&3 of
+ * Philox-4x32-10 with counter {Row<<16|Col, SampleY<<16|SampleX, digits,
+ * level<<24 | dim>>2} and key `seed`, mapped to [0,1) as (x>>8)*2^-24.
+ * Level 0 is the camera (lens y, lens x, shutter time), level 1 the primary
+ * TraceRay, and child k (0..3, in azimuth's call order: scatter, mirror,
+ * refraction, reflection) of a node at level L adds k << 2*(L-1) to digits.
+ */
+#ifndef AZIMUTH_GPU_H
+#define AZIMUTH_GPU_H
+
+#include "az_abi.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    AZ_OK = 0,
+    AZ_ERR_INVALID_ARGUMENT = 1,
+    AZ_ERR_INVALID_SCENE = 2,
+    AZ_ERR_OUT_OF_MEMORY = 3,
+    AZ_ERR_CUDA = 4,
+    AZ_ERR_TIMEOUT = 5,
+    AZ_ERR_UNSUPPORTED = 6,
+    AZ_ERR_NO_DEVICE = 7
+};
+
+/* az_render_opts.flags */
+enum {
+    AZ_FLAG_NONE = 0,
+    AZ_FLAG_COUNT_TRAVERSAL = 1u << 0,  /* fill az_render_stats node/primitive visit counters */
+    AZ_FLAG_NO_GRAPH = 1u << 1          /* launch the per-bounce stages directly, not as a CUDA graph */
+};
+
+typedef struct az_render_opts {
+    uint64_t seed;                  /* counter-RNG key */
+    const float *perlin_gradients;  /* azimuth's PerlinGradient[256] (src/azimuth_texture.h:17-18),
+                                       256*3 floats; required when a Perlin texture is used */
+    void *stream;                   /* cudaStream_t to run on, or NULL for the library's own stream */
+    int32_t device;                 /* CUDA device ordinal */
+    uint32_t flags;                 /* AZ_FLAG_* */
+    uint32_t chunk_samples;         /* camera samples in flight per wave; 0 = automatic */
+    uint32_t bvh_width;             /* 0 or 2 (binary BVH) */
+    uint32_t block_size;            /* threads per block for the wavefront kernels; 0 = automatic */
+    uint32_t reserved[5];
+} az_render_opts;
+
+typedef struct az_render_stats {
+    uint64_t samples;               /* camera samples rendered */
+    uint64_t extend_rays;           /* closest-hit queries (path segments) */
+    uint64_t shadow_rays;           /* NEE visibility queries */
+    uint32_t chunks;
+    uint32_t retries;               /* waves re-run with fewer samples after a queue overflow */
+    uint64_t kernel_launches;
+    float gpu_ms;                   /* device time of the render, CUDA events on the render stream */
+    float extend_ms;                /* reserved */
+    uint32_t reserved[6];
+} az_render_stats;
+
+typedef struct az_gpu_scene az_gpu_scene;
+
+/* Flatten `scene` (walking its BVH trees to the leaves), upload it and build
+ * the device BVHs.  The host scene is only read. */
+int az_gpu_scene_create(const az_scene *scene, const az_render_opts *opts, az_gpu_scene **out);
+void az_gpu_scene_destroy(az_gpu_scene *scene);
+
+/* ProduceImageInLinearSpace (src/azimuth_main.cpp:1256-1263) on the GPU:
+ * accumulates every camera sample of the scissor rectangle into the HOST film
+ * `pixels` (W*H entries, caller-zeroed or holding earlier sums), with
+ * filter_type AZ_Filter_Box or AZ_Filter_Gaussian (src/azimuth_main.cpp:1209-1254).
+ * Builds and frees a device scene for this one call. */
+int az_gpu_produce_image(az_pixel *pixels, const az_scene *scene, const az_camera *camera,
+                         const az_epsilon_values *epsilons, az_scissor scissor, int32_t filter_type,
+                         uint32_t backface_culling, const az_render_opts *opts);
+
+/* Same render on a device scene; `film` is a DEVICE pointer to W*H az_pixel
+ * that is accumulated into.  Runs on opts->stream; returns after the work is
+ * queued unless `stats` is non-NULL (then it synchronises and fills it). */
+int az_gpu_render(az_gpu_scene *scene, az_pixel *film, const az_camera *camera,
+                  const az_epsilon_values *epsilons, az_scissor scissor, int32_t filter_type,
+                  uint32_t backface_culling, const az_render_opts *opts, az_render_stats *stats);
+
+/* Closest hit for `count` HOST rays (azimuth's RayEntityIntersection on the
+ * scene root, src/azimuth_main.cpp:53-385).  Per ray: hit flag, UniqueEntityID
+ * of the top-level entity, face id (entity.ID of the triangle hit inside a
+ * mesh instance, else 0xFFFFFFFF) and world t.  Synchronous. */
+int az_gpu_closest_hit(az_gpu_scene *scene, const az_ray3 *rays, uint32_t count, int32_t cull,
+                       float hit_epsilon, uint32_t *out_hit, uint32_t *out_uid, uint32_t *out_face,
+                       float *out_t, const az_render_opts *opts);
+
+/* Device name, SM count and memory; returns AZ_ERR_NO_DEVICE without a GPU. */
+int az_gpu_device_info(int32_t device, char *name, uint32_t name_len);
+
+/* The counter RNG on the host: draw `dim` of tree node (level, digits) of
+ * camera sample `sample` (SampleY<<16|SampleX) of pixel `pixel` (Row<<16|Col),
+ * exactly as the kernels draw it; and the raw Philox-4x32-10 block function. */
+float az_rng_u01(uint64_t seed, uint32_t pixel, uint32_t sample, uint32_t digits, uint32_t level, uint32_t dim);
+void az_rng_philox4x32_10(const uint32_t counter[4], uint32_t key0, uint32_t key1, uint32_t out[4]);
+
+/* Message of the last failed call on this thread ("" if none). */
+const char *az_gpu_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,275 @@
+/*
+ * Oracle harness around azimuth's own render code (test infrastructure only).
+ *
+ * This translation unit #includes azimuth's unity build
+ * (src/azimuth_main.cpp, patched by oracle/patch_reference.py) with
+ * -Dmain=azimuth_main, so every static routine of the reference is callable
+ * here.  It exports a small C interface used by the tests and by the CPU
+ * baseline leg of bench.py:
+ *
+ *   azref_produce_image   ProduceImageInLinearSpace (src/azimuth_main.cpp:1256)
+ *                         over N threads with RenderScene's scanline split
+ *                         (src/azimuth_main.cpp:1815-1867), any filter
+ *   azref_closest_hit     RayEntityIntersection on the scene root
+ *                         (src/azimuth_main.cpp:53-385), plus the face id of
+ *                         a mesh-instance hit (src/azimuth_main.cpp:244-281)
+ *   azref_construct_bvh*  ConstructBVH / ConstructBVHTrianglesOnly
+ *                         (src/azimuth_bvh.cpp:1-328)
+ *   azref_*perlin*, azref_sample_texture, azref_eval_brdf
+ *                         per-routine known-answer access
+ *
+ * It also defines the counter-RNG hooks that the patched Random01,
+ * GetSampleCoord and TraceRay call (see oracle/shim/az_oracle_compat.h).
+ */
+#include "azimuth_main.cpp"
+
+#include <omp.h>
+#include "az_abi.h"
+#include "az_rng_oracle.h"
+
+/* ---- the reference structs and the C mirror must share one layout ---- */
+#define AZ_SAME(T, AT, F) static_assert(offsetof(T, F) == offsetof(AT, F), #T "." #F)
+static_assert(sizeof(entity) == sizeof(az_entity), "entity");
+static_assert(sizeof(mesh) == sizeof(az_mesh), "mesh");
+static_assert(sizeof(light) == sizeof(az_light), "light");
+static_assert(sizeof(material) == sizeof(az_material), "material");
+static_assert(sizeof(texture) == sizeof(az_texture), "texture");
+static_assert(sizeof(camera) == sizeof(az_camera), "camera");
+static_assert(sizeof(scene) == sizeof(az_scene), "scene");
+static_assert(sizeof(pixel) == sizeof(az_pixel), "pixel");
+static_assert(sizeof(ray_hit) == sizeof(az_ray_hit), "ray_hit");
+AZ_SAME(entity, az_entity, Center); AZ_SAME(entity, az_entity, Radius);
+AZ_SAME(entity, az_entity, P0); AZ_SAME(entity, az_entity, N2);
+AZ_SAME(entity, az_entity, FaceNormal); AZ_SAME(entity, az_entity, UV2);
+AZ_SAME(entity, az_entity, ShadingMode); AZ_SAME(entity, az_entity, AABB);
+AZ_SAME(entity, az_entity, Mesh); AZ_SAME(entity, az_entity, BaseMeshID);
+AZ_SAME(entity, az_entity, Right); AZ_SAME(entity, az_entity, Left);
+AZ_SAME(entity, az_entity, InvTransformationMatrix);
+AZ_SAME(entity, az_entity, TransformationMatrix);
+AZ_SAME(entity, az_entity, MotionVector); AZ_SAME(entity, az_entity, Radiance);
+AZ_SAME(entity, az_entity, IsEmitter); AZ_SAME(entity, az_entity, TextureIndex);
+AZ_SAME(entity, az_entity, MaterialIndex); AZ_SAME(entity, az_entity, ID);
+AZ_SAME(entity, az_entity, UniqueEntityID); AZ_SAME(entity, az_entity, Type);
+AZ_SAME(mesh, az_mesh, BVH); AZ_SAME(mesh, az_mesh, Triangles);
+AZ_SAME(mesh, az_mesh, TotalArea); AZ_SAME(mesh, az_mesh, TriangleCount);
+AZ_SAME(mesh, az_mesh, ShadingMode);
+AZ_SAME(light, az_light, Position); AZ_SAME(light, az_light, Intensity);
+AZ_SAME(light, az_light, EdgeVectors); AZ_SAME(light, az_light, Normal);
+AZ_SAME(light, az_light, Direction); AZ_SAME(light, az_light, SpotDirection);
+AZ_SAME(light, az_light, CosHalfFallOff); AZ_SAME(light, az_light, Entity);
+AZ_SAME(light, az_light, Type);
+AZ_SAME(material, az_material, DiffuseReflectance);
+AZ_SAME(material, az_material, Transparency);
+AZ_SAME(material, az_material, Glossiness); AZ_SAME(material, az_material, ID);
+AZ_SAME(texture, az_texture, Pixels); AZ_SAME(texture, az_texture, Normalizer);
+AZ_SAME(texture, az_texture, Perm); AZ_SAME(texture, az_texture, ScalingFactor);
+AZ_SAME(texture, az_texture, PerlinAppearance);
+AZ_SAME(texture, az_texture, BumpMapMultiplier); AZ_SAME(texture, az_texture, Type);
+AZ_SAME(camera, az_camera, NearPlane); AZ_SAME(camera, az_camera, FovY);
+AZ_SAME(camera, az_camera, Position); AZ_SAME(camera, az_camera, Resolution);
+AZ_SAME(camera, az_camera, ApertureSize); AZ_SAME(camera, az_camera, SampleCount);
+AZ_SAME(camera, az_camera, Type);
+AZ_SAME(scene, az_scene, BackgroundTexture); AZ_SAME(scene, az_scene, BVHRoot);
+AZ_SAME(scene, az_scene, EnvironmentMap); AZ_SAME(scene, az_scene, MaxRecursionDepth);
+AZ_SAME(scene, az_scene, ImportanceSampling);
+
+/* ------------------------- counter-RNG hooks -------------------------- */
+namespace {
+struct NodeCtx {
+    uint32_t Level;      /* 0 = camera context, 1 = root TraceRay, ... */
+    uint32_t Digits;     /* child index (2 bits) per level >= 2         */
+    uint32_t Dim;        /* draws consumed by this node so far          */
+    uint32_t NextChild;  /* TraceRay calls made from this node so far   */
+};
+const int MaxNodeStack = 96;
+uint64_t GSeed = 0;
+uint32_t GSetupDim = 0;
+thread_local NodeCtx TStack[MaxNodeStack];
+thread_local int TTop = -1;
+thread_local uint32_t TPixel = 0, TSample = 0;
+}
+
+extern "C" float AzOracleRandom01(void) {
+    if (TTop < 0) {
+        /* outside any camera sample: the scene-setup stream (e.g. InitPerlinNoise) */
+        return az_oracle_u01(GSeed, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFu, GSetupDim++);
+    }
+    NodeCtx &C = TStack[TTop];
+    return az_oracle_u01(GSeed, TPixel, TSample, C.Digits, C.Level, C.Dim++);
+}
+
+extern "C" void AzOracleBeginSample(unsigned Row, unsigned Col, unsigned SampleX, unsigned SampleY) {
+    TPixel = (Row << 16) | Col;
+    TSample = (SampleY << 16) | SampleX;
+    TTop = 0;
+    TStack[0] = NodeCtx{0, 0, 0, 0};
+}
+
+extern "C" void AzOracleEnterNode(void) {
+    if (TTop < 0) {            /* TraceRay outside a sample: give it a context */
+        TTop = 0;
+        TStack[0] = NodeCtx{0, 0, 0, 0};
+    }
+    if (TTop + 1 >= MaxNodeStack) { abort(); }
+    NodeCtx &P = TStack[TTop];
+    uint32_t K = P.NextChild++;
+    NodeCtx C;
+    C.Level = P.Level + 1;
+    C.Digits = P.Digits;
+    if (C.Level >= 2 && C.Level - 2 < 16) { C.Digits |= (K & 3u) << (2u * (C.Level - 2u)); }
+    C.Dim = 0;
+    C.NextChild = 0;
+    TStack[++TTop] = C;
+}
+
+extern "C" void AzOracleLeaveNode(void) { --TTop; }
+
+/* ------------------------------ C interface ---------------------------- */
+extern "C" {
+
+void azref_set_seed(uint64_t Seed) { GSeed = Seed; GSetupDim = 0; }
+void azref_end_sample(void) { TTop = -1; }
+float azref_random01(void) { return AzOracleRandom01(); }
+
+/* RenderScene's thread split (src/azimuth_main.cpp:1815-1867) without the file
+ * output and with the filter as a parameter (RenderScene hard-codes Box). */
+void azref_produce_image(az_pixel *Pixels, az_scene *Scene, az_camera *Camera,
+                         az_epsilon_values *Epsilons, az_scissor Scissor,
+                         int FilterType, int BackfaceCulling, uint32_t ThreadCount) {
+    if (ThreadCount == 0) { ThreadCount = 1; }
+    uint32_t RowMin = Scissor.Min.y;
+    uint32_t RowMax = Scissor.Max.y;
+    if (RowMax > Camera->Resolution.y) { RowMax = Camera->Resolution.y; }
+    uint32_t Rows = RowMax > RowMin ? RowMax - RowMin : 0;
+    if (ThreadCount > Rows && Rows > 0) { ThreadCount = Rows; }
+
+    thread_handle *Handles = (thread_handle *)calloc(ThreadCount, sizeof(thread_handle));
+    produce_image_params *Params =
+        (produce_image_params *)calloc(ThreadCount, sizeof(produce_image_params));
+    uint32_t MinPer = Rows / ThreadCount;
+    uint32_t Residual = Rows - MinPer * ThreadCount;
+    uint32_t Consumed = RowMin;
+    for (uint32_t I = 0; I < ThreadCount; I++) {
+        uint32_t Lines = MinPer + (Residual ? 1u : 0u);
+        if (Residual) { Residual--; }
+        produce_image_params *P = Params + I;
+        P->Scissor.Max = Vec2u(Scissor.Max.x, Consumed + Lines);
+        P->Scissor.Min = Vec2u(Scissor.Min.x, Consumed);
+        P->Pixels = (pixel *)Pixels;
+        P->Scene = (scene *)Scene;
+        P->Camera = (camera *)Camera;
+        P->Epsilons = (epsilon_values *)Epsilons;
+        P->FilterType = (filter_type)FilterType;
+        P->BackfaceCulling = (b32)BackfaceCulling;
+        u32 ThreadID;
+        PlatformCreateThread(&Handles[I], ProduceImageInLinearSpaceMT, P, &ThreadID, 0);
+        Consumed += Lines;
+    }
+    PlatformWaitForThreads(ThreadCount, Handles, true, true, 0);
+    free(Handles);
+    free(Params);
+}
+
+/* Closest hit on the scene root for a batch of rays (src/azimuth_main.cpp:53-385).
+ * Outputs per ray: hit flag, UniqueEntityID of the top-level entity, face id
+ * (entity.ID of the triangle inside a mesh instance; 0xFFFFFFFF otherwise),
+ * t, and P/Normal/UV as 8 floats. */
+int azref_closest_hit(az_scene *AScene, const az_ray3 *Rays, uint32_t Count, int Cull,
+                      float HitEpsilon, uint32_t *OutHit, uint32_t *OutUid,
+                      uint32_t *OutFace, float *OutT, float *OutPNUV, int Threads) {
+    scene *Scene = (scene *)AScene;
+    if (Threads <= 0) { Threads = 1; }
+#pragma omp parallel for num_threads(Threads) schedule(dynamic, 256)
+    for (int64_t I = 0; I < (int64_t)Count; I++) {
+        ray3 Ray;
+        memcpy(&Ray, Rays + I, sizeof(ray3));
+        ray_hit Hit = {0};
+        Hit.t = f32_Max;
+        b32 Ok = RayEntityIntersection(&Hit, Ray, Scene->BVHRoot, Scene->Textures,
+                                       (b32)Cull, HitEpsilon);
+        OutHit[I] = Ok ? 1u : 0u;
+        OutUid[I] = 0xFFFFFFFFu;
+        OutFace[I] = 0xFFFFFFFFu;
+        OutT[I] = Ok ? Hit.t : 0.0f;
+        float *Pn = OutPNUV + 8 * I;
+        memset(Pn, 0, 8 * sizeof(float));
+        if (!Ok) { continue; }
+        entity *E = Hit.Entity;
+        OutUid[I] = E->UniqueEntityID;
+        if (E->Type == EntityType_Triangle) {
+            OutFace[I] = E->ID;
+        } else if (E->Type == EntityType_MeshInstance) {
+            /* the instance path of src/azimuth_main.cpp:246-255, to read the face */
+            ray3 R = Ray;
+            vec3 Motion = R.T * E->MotionVector;
+            R.Origin -= Motion;
+            ray3 LocalRay = GetLocalRay(R, E->InvTransformationMatrix);
+            ray_hit LocalHit = {0};
+            LocalHit.t = f32_Max;
+            if (RayEntityIntersection(&LocalHit, LocalRay, E->Mesh->BVH, Scene->Textures,
+                                      (b32)Cull, HitEpsilon)) {
+                OutFace[I] = LocalHit.Entity->ID;
+            }
+        }
+        Pn[0] = Hit.P.x; Pn[1] = Hit.P.y; Pn[2] = Hit.P.z;
+        Pn[3] = Hit.Normal.x; Pn[4] = Hit.Normal.y; Pn[5] = Hit.Normal.z;
+        Pn[6] = Hit.UV.u; Pn[7] = Hit.UV.v;
+    }
+    return 0;
+}
+
+int azref_construct_bvh(az_entity **Root, az_entity *Entities, uint32_t Count) {
+    return ConstructBVH((entity **)Root, (entity *)Entities, Count) ? 1 : 0;
+}
+
+int azref_construct_bvh_triangles(az_entity **Root, az_entity *Triangles, uint32_t Count) {
+    return ConstructBVHTrianglesOnly((entity **)Root, (entity *)Triangles, Count) ? 1 : 0;
+}
+
+/* InitPerlinNoise (src/azimuth_texture.h:106-132) on the setup RNG stream. */
+void azref_init_perlin(az_texture *Texture) { InitPerlinNoise((texture *)Texture); }
+
+void azref_get_perlin_gradients(float *Out768) {
+    for (int I = 0; I < PerlinGradientSize; I++) {
+        Out768[3 * I + 0] = PerlinGradient[I].x;
+        Out768[3 * I + 1] = PerlinGradient[I].y;
+        Out768[3 * I + 2] = PerlinGradient[I].z;
+    }
+}
+
+void azref_set_perlin_gradients(const float *In768) {
+    for (int I = 0; I < PerlinGradientSize; I++) {
+        PerlinGradient[I] = Vec3(In768[3 * I + 0], In768[3 * I + 1], In768[3 * I + 2]);
+    }
+    PerlinGradientFilled = true;
+}
+
+float azref_sample_perlin(az_texture *Texture, float X, float Y, float Z) {
+    return SamplePerlinNoise((texture *)Texture, Vec3(X, Y, Z));
+}
+
+void azref_sample_texture(az_texture *Texture, float X, float Y, float Z, float U, float V,
+                          float *Out3) {
+    vec3 R = SampleTexture((texture *)Texture, Vec3(X, Y, Z), Vec2(U, V));
+    Out3[0] = R.x; Out3[1] = R.y; Out3[2] = R.z;
+}
+
+/* CalculateLightContribution (src/azimuth_main.cpp:571-603) on zeroed
+ * accumulators: returns Diffuse and Specular contributions (3+3 floats). */
+void azref_light_contribution(az_brdf *Brdf, const float *Intensity3, const float *LightDir3,
+                              const float *ViewDir3, const float *Normal3, float Distance,
+                              float FallOff, float InvPdf, float *Out6) {
+    vec3 D = Vec3(0.0f, 0.0f, 0.0f), S = Vec3(0.0f, 0.0f, 0.0f);
+    CalculateLightContribution(&D, &S, (brdf *)Brdf,
+                               Vec3(Intensity3[0], Intensity3[1], Intensity3[2]),
+                               Vec3(LightDir3[0], LightDir3[1], LightDir3[2]),
+                               Vec3(ViewDir3[0], ViewDir3[1], ViewDir3[2]),
+                               Vec3(Normal3[0], Normal3[1], Normal3[2]),
+                               Distance, FallOff, InvPdf);
+    Out6[0] = D.x; Out6[1] = D.y; Out6[2] = D.z;
+    Out6[3] = S.x; Out6[4] = S.y; Out6[5] = S.z;
+}
+
+uint32_t azref_sizeof_entity(void) { return (uint32_t)sizeof(entity); }
+
+}  /* extern "C" */
