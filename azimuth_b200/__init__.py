@@ -30,6 +30,7 @@ FILTER_GAUSSIAN = 1
 
 FLAG_COUNT_TRAVERSAL = 1
 FLAG_NO_GRAPH = 2
+FLAG_TIME_STAGES = 4
 
 STATUS = {0: "AZ_OK", 1: "AZ_ERR_INVALID_ARGUMENT", 2: "AZ_ERR_INVALID_SCENE", 3: "AZ_ERR_OUT_OF_MEMORY",
           4: "AZ_ERR_CUDA", 5: "AZ_ERR_TIMEOUT", 6: "AZ_ERR_UNSUPPORTED", 7: "AZ_ERR_NO_DEVICE"}
@@ -166,13 +167,20 @@ class GpuScene:
         _check(lib().az_gpu_render(self._h, film_ptr, camera_ptr or self.scene.camera_ptr, self.scene.epsilons_ptr,
                                    sc, ft, 0, C.byref(o), C.byref(st) if st is not None else None),
                "az_gpu_render")
-        if st is None:
-            return None
-        return {"samples": st.samples, "extend_rays": st.extend_rays, "shadow_rays": st.shadow_rays,
-                "chunks": st.chunks, "retries": st.retries, "kernel_launches": st.kernel_launches,
-                "gpu_ms": st.gpu_ms,
-                "node_visits": st.reserved[0] | (st.reserved[1] << 32),
-                "prim_visits": st.reserved[2] | (st.reserved[3] << 32)}
+        return _stats(st)
+
+    def render_host(self, pixels, camera_ptr=None, scissor=None, filter_type=None, seed=0, stream=None,
+                    flags=0, chunk_samples=0):
+        """az_gpu_render_host: HOST film (numpy float32 (H, W, 4), ideally pinned) in and out."""
+        sc = scissor or full_scissor(self.scene)
+        ft = self.scene.filter_type if filter_type is None else filter_type
+        o = make_opts(self.scene, seed=seed, stream=stream, device=self.device, flags=flags,
+                      chunk_samples=chunk_samples)
+        st = RenderStats()
+        ptr = pixels.ctypes.data if hasattr(pixels, "ctypes") else pixels
+        _check(lib().az_gpu_render_host(self._h, ptr, camera_ptr or self.scene.camera_ptr, self.scene.epsilons_ptr,
+                                        sc, ft, 0, C.byref(o), C.byref(st)), "az_gpu_render_host")
+        return _stats(st)
 
     def closest_hit(self, rays, cull=0, eps=0.0):
         """rays: numpy (N, 7) float32 [origin, direction, T]; returns (hit, uid, face, t)."""
@@ -203,6 +211,15 @@ class GpuScene:
             self.close()
         except Exception:
             pass
+
+
+def _stats(st):
+    if st is None:
+        return None
+    return {"samples": st.samples, "extend_rays": st.extend_rays, "shadow_rays": st.shadow_rays,
+            "chunks": st.chunks, "retries": st.retries, "kernel_launches": st.kernel_launches,
+            "gpu_ms": st.gpu_ms, "extend_ms": st.extend_ms, "shade_ms": st.shade_ms, "shadow_ms": st.shadow_ms,
+            "node_visits": st.node_visits, "prim_visits": st.prim_visits, "extend_launches": st.extend_launches}
 
 
 def device_info(device=0):

@@ -52,7 +52,9 @@ class RenderOpts(C.Structure):
 class RenderStats(C.Structure):
     _fields_ = [("samples", C.c_uint64), ("extend_rays", C.c_uint64), ("shadow_rays", C.c_uint64),
                 ("chunks", C.c_uint32), ("retries", C.c_uint32), ("kernel_launches", C.c_uint64),
-                ("gpu_ms", C.c_float), ("extend_ms", C.c_float), ("reserved", C.c_uint32 * 6)]
+                ("gpu_ms", C.c_float), ("extend_ms", C.c_float), ("shade_ms", C.c_float),
+                ("shadow_ms", C.c_float), ("node_visits", C.c_uint64), ("prim_visits", C.c_uint64),
+                ("extend_launches", C.c_uint32), ("reserved", C.c_uint32 * 3)]
 
 
 def lib():
@@ -89,6 +91,9 @@ def _declare(L):
         L.az_gpu_render.argtypes = [vp, vp, vp, vp, Scissor, i32, u32, C.POINTER(RenderOpts),
                                     C.POINTER(RenderStats)]
         L.az_gpu_render.restype = i32
+        L.az_gpu_render_host.argtypes = [vp, vp, vp, vp, Scissor, i32, u32, C.POINTER(RenderOpts),
+                                         C.POINTER(RenderStats)]
+        L.az_gpu_render_host.restype = i32
         L.az_gpu_closest_hit.argtypes = [vp, vp, u32, i32, C.c_float, vp, vp, vp, vp, vp]
         L.az_gpu_closest_hit.restype = i32
         L.az_gpu_device_info.argtypes = [i32, vp, u32]

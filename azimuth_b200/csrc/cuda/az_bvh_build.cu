@@ -131,7 +131,7 @@ __global__ void k_fill(const unsigned long long *keys, const float4 *plo, const 
     int leaf = blockIdx.x * blockDim.x + threadIdx.x;
     if (leaf >= n) return;
     int node = parent_leaf[leaf];
-    while (node >= 0) {
+    for (int guard = 0; node >= 0 && guard < n; guard++) {
         __threadfence();
         if (atomicAdd(&visits[node], 1u) == 0) return;  // first arrival: the sibling finishes the node
         __threadfence();

@@ -122,6 +122,31 @@ extern "C" int az_gpu_render(az_gpu_scene *scene, az_pixel *film, const az_camer
                   stats);
 }
 
+extern "C" int az_gpu_render_host(az_gpu_scene *scene, az_pixel *pixels, const az_camera *camera,
+                                  const az_epsilon_values *epsilons, az_scissor scissor, int32_t filter_type,
+                                  uint32_t backface_culling, const az_render_opts *opts, az_render_stats *stats) {
+    if (!scene || !scene->impl || !pixels || !camera) return SetError(AZ_ERR_INVALID_ARGUMENT, "null argument");
+    CallContext ctx;
+    int rc = ctx.begin(opts);
+    if (rc != AZ_OK) return rc;
+    GpuScene &G = *scene->impl;
+    size_t bytes = (size_t)camera->Resolution.x * camera->Resolution.y * sizeof(az_pixel);
+    if (G.host_film_bytes < bytes) {
+        if (G.host_film_dev) cudaFree(G.host_film_dev);
+        G.host_film_dev = nullptr;
+        G.host_film_bytes = 0;
+        AZ_CUDA_TRY(cudaMalloc((void **)&G.host_film_dev, bytes));
+        G.host_film_bytes = bytes;
+    }
+    AZ_CUDA_TRY(cudaMemcpyAsync(G.host_film_dev, pixels, bytes, cudaMemcpyHostToDevice, ctx.stream));
+    rc = Render(G, G.host_film_dev, camera, epsilons, scissor, filter_type, backface_culling, opts, ctx.stream,
+                stats);
+    if (rc != AZ_OK) return rc;
+    AZ_CUDA_TRY(cudaMemcpyAsync(pixels, G.host_film_dev, bytes, cudaMemcpyDeviceToHost, ctx.stream));
+    AZ_CUDA_TRY(cudaStreamSynchronize(ctx.stream));
+    return AZ_OK;
+}
+
 extern "C" int az_gpu_produce_image(az_pixel *pixels, const az_scene *scene, const az_camera *camera,
                                     const az_epsilon_values *epsilons, az_scissor scissor, int32_t filter_type,
                                     uint32_t backface_culling, const az_render_opts *opts) {

@@ -38,6 +38,8 @@ struct GpuScene {
     uint32_t max_bvh_depth = 0;
     size_t device_bytes = 0;
     WaveBuffers waves;           // reused across render calls on this scene
+    az_pixel *host_film_dev = nullptr;   // device film of az_gpu_render_host
+    size_t host_film_bytes = 0;
     ~GpuScene();
     void *Alloc(size_t bytes);   // nullptr on failure
 };

@@ -21,6 +21,7 @@
 // them and multiplies their radiance by zero.
 #include <algorithm>
 #include <cstring>
+#include <memory>
 #include <vector>
 
 #include "az_internal.h"
@@ -136,7 +137,7 @@ __global__ void __launch_bounds__(BLOCK) k_extend(DevScene S, CameraParams cam, 
         r.d = mk(d.x, d.y, d.z);
         r.time = o.w;
         Hit h;
-        trace<Q_CLOSEST>(S, r, cam.cull != 0, cam.eps_isect, FLT_MAX, h, cnt);
+        trace<Q_CLOSEST>(S, r, cam.cull != 0, cam.eps_isect, FLT_MAX, h, cnt, Q.counts + AZ_COUNT_ERROR);
         Q.hit[i] = make_uint4(__float_as_uint(h.t), __float_as_uint(h.tl), h.prim, h.ent);
     }
 }
@@ -396,10 +397,10 @@ __global__ void __launch_bounds__(BLOCK) k_shadow(DevScene S, CameraParams cam, 
         Hit h;
         bool visible;
         if (kind == SHADOW_ENTITY) {
-            bool any = trace<Q_CLOSEST>(S, r, false, 0.0f, FLT_MAX, h, cnt);
+            bool any = trace<Q_CLOSEST>(S, r, false, 0.0f, FLT_MAX, h, cnt, Q.counts + AZ_COUNT_ERROR);
             visible = !any || (S.ents[h.ent].uid & 0x3FFFFFFFu) == uid;
         } else {
-            visible = !trace<Q_ANY>(S, r, false, 0.0f, kind == SHADOW_ANY ? FLT_MAX : d.w, h, cnt);
+            visible = !trace<Q_ANY>(S, r, false, 0.0f, kind == SHADOW_ANY ? FLT_MAX : d.w, h, cnt, Q.counts + AZ_COUNT_ERROR);
         }
         if (visible) add_accum(Q.accum, __float_as_uint(c.w), mk(c.x, c.y, c.z));
     }
@@ -540,10 +541,39 @@ int WaveBuffers::Ensure(uint32_t chunk, uint32_t cap_q, uint32_t cap_s) {
     return AZ_OK;
 }
 
+// CUDA events between the stages of every level; summed per stage.
+struct StageTimer {
+    std::vector<cudaEvent_t> ev;
+    std::vector<int> kind;   // event k ends stage kind[k]-1 when kind[k] > 0
+    float ms[3] = {0, 0, 0};
+    void Mark(cudaStream_t st, int k) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        cudaEventRecord(e, st);
+        ev.push_back(e);
+        kind.push_back(k);
+    }
+    void Collect() {   // after a stream synchronize
+        for (size_t i = 1; i < ev.size(); i++) {
+            if (kind[i] >= 1 && kind[i - 1] == kind[i] - 1) {
+                float t = 0.0f;
+                cudaEventElapsedTime(&t, ev[i - 1], ev[i]);
+                ms[kind[i] - 1] += t;
+            }
+        }
+        for (cudaEvent_t e : ev) cudaEventDestroy(e);
+        ev.clear();
+        kind.clear();
+    }
+    ~StageTimer() {
+        for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    }
+};
+
 // Renders samples [start, start+n) of the scissor into `film`; returns the
 // per-wave counters (path and shadow queue sizes per level, overflow flag).
 static int RenderWave(const GpuScene &G, const CameraParams &cam, WaveBuffers &W, uint64_t start, uint32_t n,
-                      az_pixel *film, cudaStream_t st, int sms, RenderCounters &rc) {
+                      az_pixel *film, cudaStream_t st, int sms, RenderCounters &rc, StageTimer *timer) {
     WaveQueues Q = W.q;
     AZ_CUDA_TRY(cudaMemsetAsync(Q.counts, 0, AZ_COUNT_TOTAL * sizeof(uint32_t), st));
     uint32_t first = n;
@@ -553,10 +583,15 @@ static int RenderWave(const GpuScene &G, const CameraParams &cam, WaveBuffers &W
     const uint32_t levels = std::min<uint32_t>(G.dev.max_depth + 1, AZ_MAX_LEVELS - 2);
     const int grid = sms * 16;
     for (uint32_t L = 1; L <= levels; L++) {
+        if (timer) timer->Mark(st, 0);
         k_extend<kBlock><<<grid, kBlock, 0, st>>>(G.dev, cam, Q, L);
+        if (timer) timer->Mark(st, 1);
         k_shade<kBlock><<<grid, kBlock, 0, st>>>(G.dev, cam, Q, start, L);
+        if (timer) timer->Mark(st, 2);
         k_shadow<kBlock><<<grid, kBlock, 0, st>>>(G.dev, cam, Q, L);
+        if (timer) timer->Mark(st, 3);
         rc.launches += 3;
+        rc.extend_launches++;
     }
     k_splat<<<(n + 255) / 256, 256, 0, st>>>(cam, Q, start, n, film);
     rc.launches++;
@@ -588,6 +623,8 @@ int Render(GpuScene &G, az_pixel *film, const az_camera *camera, const az_epsilo
     }
     RenderCounters counters{};
     std::vector<uint32_t> host_counts(AZ_COUNT_TOTAL);
+    std::unique_ptr<StageTimer> timer;
+    if (stats && opts && (opts->flags & AZ_FLAG_TIME_STAGES)) timer.reset(new StageTimer());
     uint64_t pos = 0;
     while (pos < total) {
         uint32_t n = (uint32_t)std::min<uint64_t>(chunk, total - pos);
@@ -596,11 +633,14 @@ int Render(GpuScene &G, az_pixel *film, const az_camera *camera, const az_epsilo
                                                                          (uint64_t)n * 4), 1024);
         rc = W.Ensure(n, cap_q, cap_s);
         if (rc != AZ_OK) return rc;
-        rc = RenderWave(G, cam, W, pos, n, film, st, sms, counters);
+        rc = RenderWave(G, cam, W, pos, n, film, st, sms, counters, timer.get());
         if (rc != AZ_OK) return rc;
         AZ_CUDA_TRY(cudaMemcpyAsync(host_counts.data(), W.q.counts, AZ_COUNT_TOTAL * sizeof(uint32_t),
                                     cudaMemcpyDeviceToHost, st));
         AZ_CUDA_TRY(cudaStreamSynchronize(st));
+        if (timer) timer->Collect();
+        if (host_counts[AZ_COUNT_ERROR])
+            return SetError(AZ_ERR_CUDA, "BVH traversal exceeded its step limit (corrupt hierarchy)");
         if (host_counts[AZ_COUNT_OVERFLOW]) {
             // a queue overflowed: this wave wrote nothing; retry it with half the samples
             if (n <= 1024) return SetError(AZ_ERR_OUT_OF_MEMORY, "wave queue overflow with 1024 samples");
@@ -631,10 +671,14 @@ int Render(GpuScene &G, az_pixel *film, const az_camera *camera, const az_epsilo
         stats->retries = counters.retries;
         stats->kernel_launches = counters.launches;
         stats->gpu_ms = ms;
-        stats->reserved[0] = (uint32_t)counters.nodes;
-        stats->reserved[1] = (uint32_t)(counters.nodes >> 32);
-        stats->reserved[2] = (uint32_t)counters.prims;
-        stats->reserved[3] = (uint32_t)(counters.prims >> 32);
+        stats->node_visits = counters.nodes;
+        stats->prim_visits = counters.prims;
+        stats->extend_launches = (uint32_t)counters.extend_launches;
+        if (timer) {
+            stats->extend_ms = timer->ms[0];
+            stats->shade_ms = timer->ms[1];
+            stats->shadow_ms = timer->ms[2];
+        }
     }
     return AZ_OK;
 }

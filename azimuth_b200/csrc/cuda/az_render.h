@@ -13,6 +13,7 @@ constexpr uint32_t AZ_MAX_LEVELS = 64;                   // tree levels kept in 
 constexpr uint32_t AZ_COUNT_SHADOW = AZ_MAX_LEVELS;      // shadow-queue sizes per level
 constexpr uint32_t AZ_COUNT_OVERFLOW = 2 * AZ_MAX_LEVELS;
 constexpr uint32_t AZ_COUNT_NODES = 2 * AZ_MAX_LEVELS + 2;  // node visits, primitive visits
+constexpr uint32_t AZ_COUNT_ERROR = 2 * AZ_MAX_LEVELS + 4;  // traversal step limit reached
 constexpr uint32_t AZ_COUNT_TOTAL = 2 * AZ_MAX_LEVELS + 8;
 
 // Camera and film parameters of one render call (ProduceImageInLinearSpace's
@@ -54,7 +55,7 @@ struct WaveBuffers {
 };
 
 struct RenderCounters {
-    uint64_t extend = 0, shadow = 0, nodes = 0, prims = 0, launches = 0;
+    uint64_t extend = 0, shadow = 0, nodes = 0, prims = 0, launches = 0, extend_launches = 0;
     uint32_t chunks = 0, retries = 0;
 };
 

@@ -22,6 +22,7 @@ namespace az {
 GpuScene::~GpuScene() {
     for (auto &b : bufs)
         if (b.ptr) cudaFree(b.ptr);
+    if (host_film_dev) cudaFree(host_film_dev);
 }
 
 void *GpuScene::Alloc(size_t bytes) {
@@ -399,6 +400,10 @@ int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_
         const azd::DevTexture &t = texs[ti];
         return t.type == AZ_TextureType_PerlinNoise || (t.width > 0 && t.height > 0);
     };
+    for (const HostGroup &g : F.groups)
+        for (const azd::DevTriAttr &a : g.attr)
+            if (a.texture_index && (a.texture_index > scene->TextureCount || !tex_ok(a.texture_index - 1)))
+                return SetError(AZ_ERR_INVALID_SCENE, "triangle texture index out of range or texture not loaded");
     for (const azd::DevEntity &e : F.ents) {
         if (!e.is_emitter && e.material >= scene->MaterialCount)
             return SetError(AZ_ERR_INVALID_SCENE, "entity material index out of range");

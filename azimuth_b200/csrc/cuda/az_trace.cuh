@@ -154,8 +154,9 @@ __device__ __forceinline__ DevTri load_tri(const DevTri *tris, uint32_t i) {
 #define AZD_ENT_EXIT 0xFFFFFFFFu
 #define AZD_STACK 64
 
+// leaf entry: flag, 3 bits of count-1 (leaves hold at most 8 primitives), 27 bits of start
 __device__ __forceinline__ uint32_t leaf_entry(uint32_t start, uint32_t count) {
-    return AZD_ENT_LEAF | ((count - 1u) << 27) | start;
+    return AZD_ENT_LEAF | (((count - 1u) & 7u) << 27) | (start & 0x07FFFFFFu);
 }
 
 enum QueryKind : uint32_t {
@@ -167,9 +168,13 @@ enum QueryKind : uint32_t {
 // (best.ent == 0xFFFFFFFF: none).  For Q_ANY returns true as soon as a
 // primitive's world t < tmax.  `counts` (optional) accumulates node and
 // primitive visits.
+// A valid BVH needs far fewer steps; the cap only guards against a corrupt
+// tree looping forever.  When hit, the query stops and sets *err.
+#define AZD_MAX_STEPS (1u << 22)
+
 template <QueryKind KIND>
 __device__ bool trace(const DevScene &S, const Ray &wr, bool cull, float eps, float tmax, Hit &best,
-                      uint32_t *counts = nullptr) {
+                      uint32_t *counts = nullptr, uint32_t *err = nullptr) {
     best.t = FLT_MAX;
     best.tl = 0.0f;
     best.prim = 0xFFFFFFFFu;
@@ -193,7 +198,12 @@ __device__ bool trace(const DevScene &S, const Ray &wr, bool cull, float eps, fl
     uint32_t nodes_visited = 0, prims_visited = 0;
 
     uint32_t cur = S.tlas_root;  // inner node index or an entry
+    uint32_t steps = 0;
     while (true) {
+        if (++steps > AZD_MAX_STEPS) {
+            if (err) atomicOr(err, 1u);
+            break;
+        }
         if (cur == AZD_ENT_EXIT) {
             // leaving a BLAS: azimuth's instance path keeps the nearest local hit
             // and recomputes its world t (src/azimuth_main.cpp:256-276)
@@ -228,7 +238,7 @@ __device__ bool trace(const DevScene &S, const Ray &wr, bool cull, float eps, fl
             in_blas = false;
             cur = 0xFFFFFFFEu;  // pop next
         } else if (cur & AZD_ENT_LEAF) {
-            uint32_t start = cur & 0x07FFFFFFu, count = ((cur >> 27) & 0xFu) + 1u;
+            uint32_t start = cur & 0x07FFFFFFu, count = ((cur >> 27) & 7u) + 1u;
             cur = 0xFFFFFFFEu;
             if (in_blas) {
                 for (uint32_t i = 0; i < count; i++) {

@@ -1,0 +1,321 @@
+"""Benchmark: Mpaths/s of azimuth's render path on B200 (dense-mesh workload).
+
+Workload (one "step" = one frame): the dense-mesh scene -- the Cornell walls and
+area light around a seeded, Perlin-displaced icosphere of 1,310,720 triangles
+whose faces are split round-robin over azimuth's seven BRDF models -- at
+1024x1024, 64 samples per pixel, MaxRecursionDepth 8, cosine importance
+sampling with area-light next-event estimation and the Gaussian film filter.
+Data are synthetic (seeded generator), the scene is built in azimuth's own
+structs.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+GPU arm: the scene is uploaded once (az_gpu_scene_create); each step renders
+the frame into a device film with az_gpu_render; K steps are timed with CUDA
+events on the render stream, between a barrier and a synchronize, max over
+ranks.  Each rank renders its own frame with its own seed (weak scaling, no
+collective on the data path).  `e2e` repeats the measurement through
+az_gpu_render_host, the host-film entry point, with the film copied in and out
+every step.
+
+Reference arm (--impl reference): azimuth's own ProduceImageInLinearSpace
+(oracle/_ref/libazref_fast.so, the -O3 -ffast-math build) on all host cores,
+each step a bounded sample of the same frame (8 rows x 32 pixels spread over
+the image, all 64 samples and full depth), rank 0 only.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "Mpaths/s on 1 B200; equal-time relMSE guided vs plain GPU vs FP64 converged"
+WORKLOAD = "dense mesh + importance sampling: 1,310,720-triangle Perlin-displaced icosphere in a Cornell box, " \
+           "7 BRDFs, 1024x1024, 64 spp, depth 8, cosine sampling + area-light NEE, Gaussian filter"
+SCENE_ARGS = dict(scene_id=1, seed=0)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--chunk", type=int, default=0, help="camera samples per wave (0 = library default)")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """Samples SM clocks and throttle reasons with nvidia-smi while running."""
+
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active," \
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown," \
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=5)
+        return self.summary()
+
+    def summary(self):
+        mhz, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                mhz.append(float(r[1]))
+                mx = float(r[2])
+                for k, name in enumerate(names):
+                    if r[5 + k].lower().startswith("active"):
+                        reasons.add(name)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(mhz)}
+
+
+def reference_sample_scissors(w, h):
+    """8 rows spread over the frame, 32 columns each at spread positions."""
+    out = []
+    for k in range(8):
+        row = (2 * k + 1) * h // 16
+        col = ((5 * k + 3) % 16) * w // 16
+        out.append((row, row + 1, col, col + 32))
+    return out
+
+
+def run_reference_sample(scene, steps, warmup, threads):
+    """azimuth's ProduceImageInLinearSpace over the bounded sample; returns paths/s and seconds."""
+    sys.path.insert(0, os.path.join(REPO, "tests"))
+    import oracle_lib as ol
+    fast = ol.have_ref(fast=True)
+    kind = "reference" if fast else "port"
+    w, h = scene.resolution()
+    spp = int(int(scene.sample_count() ** 0.5) ** 2)
+    boxes = reference_sample_scissors(w, h)
+    paths_per_step = sum((r1 - r0) * (c1 - c0) for r0, r1, c0, c1 in boxes) * spp
+
+    def one_step(seed):
+        for r0, r1, c0, c1 in boxes:
+            sc = ol.scissor_of(scene, rows=(r0, r1), cols=(c0, c1))
+            if fast:
+                ol.ref_film(scene, seed=seed, threads=threads, scissor=sc, fast=True)
+            else:
+                ol.port_film(scene, seed=seed, threads=threads, scissor=sc)
+
+    for i in range(warmup):
+        one_step(100 + i)
+    t0 = time.monotonic()
+    for i in range(steps):
+        one_step(i)
+    dt = time.monotonic() - t0
+    return paths_per_step * steps / dt, dt, paths_per_step, kind
+
+
+def reference_arm(args):
+    import azimuth_b200 as az
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    scene = az.generate_scene(SCENE_ARGS["scene_id"], seed=SCENE_ARGS["seed"])
+    pps, dt, per_step, kind = run_reference_sample(scene, args.steps, args.warmup, threads)
+    value = pps / 1e6
+    sample = "per step: 8 rows x 32 px spread over the 1024x1024 frame, 64 spp, depth 8 (%d paths)" % per_step
+    out = {"metric": METRIC, "value": value, "unit": "Mpaths/s", "impl": "reference", "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * dt / max(args.steps, 1),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "data": "synthetic (seeded generator, azimuth structs)",
+           "config": {"workload": WORKLOAD, "parallelism": "host threads (%d)" % threads, "sample": sample},
+           "cpu_baseline": {"value": value, "unit": "Mpaths/s", "cores": threads, "kind": kind, "sample": sample},
+           "e2e": {"value": value, "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return reference_arm(args)
+
+    import numpy as np
+    import torch
+    import azimuth_b200 as az
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    scene = az.generate_scene(SCENE_ARGS["scene_id"], seed=SCENE_ARGS["seed"])
+    w, h = scene.resolution()
+    spp = int(int(scene.sample_count() ** 0.5) ** 2)
+    paths_per_frame = w * h * spp
+    t0 = time.time()
+    gs = az.GpuScene(scene, device=local)
+    torch.cuda.synchronize()
+    upload_s = time.time() - t0
+
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+    film = torch.zeros((h, w, 4), device="cuda", dtype=torch.float32)
+    seed = 1000 * rank
+
+    def step(i, flags=0, stats=False):
+        return gs.render_device(film.data_ptr(), seed=seed + i, stream=sptr, flags=flags, stats=stats,
+                                chunk_samples=args.chunk)
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    launches = 0
+    extend_ms = 0.0
+    extend_launches = 0
+    seg = shadow = 0
+    for i in range(args.steps):
+        st = step(args.warmup + i, flags=az.FLAG_TIME_STAGES, stats=True)
+        launches += st["kernel_launches"]
+        extend_ms += st["extend_ms"]
+        extend_launches += st["extend_launches"]
+        seg += st["extend_rays"]
+        shadow += st["shadow_rays"]
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    ms_per_step = ms / args.steps
+    value = world * paths_per_frame * args.steps / (ms / 1000.0) / 1e6
+
+    # end to end through the host-film entry point (film in and out every step)
+    host_film = torch.zeros((h, w, 4), dtype=torch.float32).pin_memory()
+    hf = host_film.numpy()
+    gs.render_host(hf, seed=seed, stream=sptr, chunk_samples=args.chunk)   # warm the host-film path
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.monotonic()
+    e_steps = max(1, min(args.steps, 3))
+    for i in range(e_steps):
+        gs.render_host(hf, seed=seed + i, stream=sptr, chunk_samples=args.chunk)
+    e2e_s = time.monotonic() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": world * paths_per_frame * e_steps / e2e_s / 1e6, "unit": "Mpaths/s",
+           "h2d_bytes_per_step": int(w * h * 16), "d2h_bytes_per_step": int(w * h * 16),
+           "api": "az_gpu_render_host (device scene resident, host film copied in and out)"}
+
+    # roofline of the closest-hit (extend) kernel: algorithmic bytes from a
+    # counting pass over one frame (node/primitive visits), time from the timed run
+    cnt = step(0, flags=az.FLAG_COUNT_TRAVERSAL, stats=True)
+    torch.cuda.synchronize()
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    # node visits are counted in both extend and shadow queries; scale to the
+    # extend share by ray count (visits per query are similar within 2x)
+    frac_ext = cnt["extend_rays"] / max(1, cnt["extend_rays"] + cnt["shadow_rays"])
+    ext_nodes = cnt["node_visits"] * frac_ext
+    ext_prims = cnt["prim_visits"] * frac_ext
+    bytes_per_frame = cnt["extend_rays"] * (32 + 16) + ext_nodes * 64 + ext_prims * 48
+    per_launch_bytes = bytes_per_frame / max(1, cnt["extend_launches"])
+    per_launch_ms = extend_ms / max(1, extend_launches)
+    achieved = per_launch_bytes / (per_launch_ms / 1000.0) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                "traffic": None, "kernel": "k_extend (closest-hit traversal)",
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650",
+                "bytes_per_segment": bytes_per_frame / max(1, cnt["extend_rays"]),
+                "node_visits_per_segment": ext_nodes / max(1, cnt["extend_rays"]),
+                "prim_visits_per_segment": ext_prims / max(1, cnt["extend_rays"]),
+                "extend_share_of_step": extend_ms / max(ms, 1e-9)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            threads = os.cpu_count() or 1
+            pps, dt, per_step, kind = run_reference_sample(scene, 1, 0, threads)
+            cpu = {"value": pps / 1e6, "unit": "Mpaths/s", "cores": threads, "kind": kind,
+                   "sample": "8 rows x 32 px spread over the frame, 64 spp, depth 8 (%d paths), "
+                             "azimuth -O3 -ffast-math build" % per_step, "seconds": dt}
+        except Exception as ex:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": "Mpaths/s", "cores": 0, "kind": "unavailable", "sample": str(ex)}
+
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator, azimuth structs)",
+               "config": {"workload": WORKLOAD, "triangles": int(scene.triangle_count), "width": w, "height": h,
+                          "spp": spp, "max_depth": scene.max_depth(), "paths_per_step_per_gpu": paths_per_frame,
+                          "parallelism": "dp%d (one frame per GPU, own seed)" % world,
+                          "l2": "inputs larger than L2 (scene ~%.0f MB on device)" % (
+                              (scene.triangle_count * (48 + 80 + 64)) / 1e6),
+                          "scene_upload_s": upload_s},
+               "segments_per_s": world * seg / (ms / 1000.0), "rays_per_s": world * (seg + shadow) / (ms / 1000.0),
+               "gpu_launches": int(launches), "e2e": e2e, "roofline": roofline, "clocks": clk}
+        if cpu:
+            out["cpu_baseline"] = cpu
+        print(json.dumps(out), flush=True)
+    gs.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

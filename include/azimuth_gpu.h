@@ -42,7 +42,8 @@ enum {
 enum {
     AZ_FLAG_NONE = 0,
     AZ_FLAG_COUNT_TRAVERSAL = 1u << 0,  /* fill az_render_stats node/primitive visit counters */
-    AZ_FLAG_NO_GRAPH = 1u << 1          /* launch the per-bounce stages directly, not as a CUDA graph */
+    AZ_FLAG_NO_GRAPH = 1u << 1,         /* launch the per-bounce stages directly, not as a CUDA graph */
+    AZ_FLAG_TIME_STAGES = 1u << 2       /* time each stage with CUDA events (az_render_stats *_ms) */
 };
 
 typedef struct az_render_opts {
@@ -66,8 +67,13 @@ typedef struct az_render_stats {
     uint32_t retries;               /* waves re-run with fewer samples after a queue overflow */
     uint64_t kernel_launches;
     float gpu_ms;                   /* device time of the render, CUDA events on the render stream */
-    float extend_ms;                /* reserved */
-    uint32_t reserved[6];
+    float extend_ms;                /* with AZ_FLAG_TIME_STAGES: closest-hit stage */
+    float shade_ms;                 /* with AZ_FLAG_TIME_STAGES: shading stage */
+    float shadow_ms;                /* with AZ_FLAG_TIME_STAGES: visibility stage */
+    uint64_t node_visits;           /* with AZ_FLAG_COUNT_TRAVERSAL: BVH nodes visited */
+    uint64_t prim_visits;           /* with AZ_FLAG_COUNT_TRAVERSAL: primitives tested */
+    uint32_t extend_launches;       /* closest-hit stage launches */
+    uint32_t reserved[3];
 } az_render_stats;
 
 typedef struct az_gpu_scene az_gpu_scene;
@@ -92,6 +98,12 @@ int az_gpu_produce_image(az_pixel *pixels, const az_scene *scene, const az_camer
 int az_gpu_render(az_gpu_scene *scene, az_pixel *film, const az_camera *camera,
                   const az_epsilon_values *epsilons, az_scissor scissor, int32_t filter_type,
                   uint32_t backface_culling, const az_render_opts *opts, az_render_stats *stats);
+
+/* ProduceImageInLinearSpace on a device scene with a HOST film: copies
+ * `pixels` to the device, renders into it and copies it back (synchronous). */
+int az_gpu_render_host(az_gpu_scene *scene, az_pixel *pixels, const az_camera *camera,
+                       const az_epsilon_values *epsilons, az_scissor scissor, int32_t filter_type,
+                       uint32_t backface_culling, const az_render_opts *opts, az_render_stats *stats);
 
 /* Closest hit for `count` HOST rays (azimuth's RayEntityIntersection on the
  * scene root, src/azimuth_main.cpp:53-385).  Per ray: hit flag, UniqueEntityID
