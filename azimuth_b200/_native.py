@@ -94,6 +94,8 @@ def _declare(L):
         L.az_gpu_render_host.argtypes = [vp, vp, vp, vp, Scissor, i32, u32, C.POINTER(RenderOpts),
                                          C.POINTER(RenderStats)]
         L.az_gpu_render_host.restype = i32
+        L.az_gpu_render_noalloc.argtypes = [vp, vp, vp, vp, Scissor, i32, u32, C.POINTER(RenderOpts)]
+        L.az_gpu_render_noalloc.restype = i32
         L.az_gpu_closest_hit.argtypes = [vp, vp, u32, i32, C.c_float, vp, vp, vp, vp, vp]
         L.az_gpu_closest_hit.restype = i32
         L.az_gpu_device_info.argtypes = [i32, vp, u32]

@@ -59,9 +59,6 @@ struct CallContext {
 
 }  // namespace az
 
-struct az_gpu_scene {
-    az::GpuScene *impl;
-};
 
 using namespace az;
 

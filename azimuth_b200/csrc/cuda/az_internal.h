@@ -62,3 +62,8 @@ int ClosestHit(GpuScene &G, const az_ray3 *rays, uint32_t n, int32_t cull, float
                uint32_t *out_uid, uint32_t *out_face, float *out_t, cudaStream_t st);
 
 }  // namespace az
+
+// The opaque handle of include/azimuth_gpu.h.
+struct az_gpu_scene {
+    az::GpuScene *impl;
+};

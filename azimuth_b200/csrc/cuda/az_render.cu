@@ -22,6 +22,8 @@
 #include <algorithm>
 #include <cstring>
 #include <memory>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "az_internal.h"
@@ -733,3 +735,124 @@ int ClosestHit(GpuScene &G, const az_ray3 *rays, uint32_t n, int32_t cull, float
 }
 
 }  // namespace az
+
+// ---------------------------------------------------------------------------
+// az_gpu_render_noalloc: the same render with the wave queues in a fixed
+// static device array, for callers that must not allocate device memory.
+// ---------------------------------------------------------------------------
+namespace az {
+namespace {
+
+constexpr uint32_t kStaticWave = 16384;                          // camera samples per wave, maximum
+constexpr uint32_t kStaticCapQ = kStaticWave + kStaticWave / 2;  // path-queue entries per level buffer
+constexpr uint32_t kStaticCapS = 4 * kStaticCapQ;                // light-sample (shadow) entries
+constexpr size_t Align256(size_t x) { return (x + 255) & ~(size_t)255; }
+constexpr size_t kQ16 = Align256((size_t)kStaticCapQ * 16), kQ4 = Align256((size_t)kStaticCapQ * 4);
+constexpr size_t kS16 = Align256((size_t)kStaticCapS * 16), kS4 = Align256((size_t)kStaticCapS * 4);
+constexpr size_t kA16 = Align256((size_t)kStaticWave * 16), kC4 = Align256((size_t)AZ_COUNT_TOTAL * 4);
+constexpr size_t kStaticBytes = 2 * (4 * kQ16 + kQ4) + kQ16 + 3 * kS16 + kS4 + kA16 + kC4;  // 9,110,272 B
+
+// One copy per GPU that loads this library, held until the process exits.
+// Host code must not use this name as an address: it resolves the device
+// address once per device with cudaGetSymbolAddress (StaticWaveScratch).
+static __device__ __align__(256) unsigned char g_wave_scratch[kStaticBytes];
+
+std::mutex g_wave_scratch_mu;
+void *g_wave_scratch_addr[256] = {};
+
+// Device address of g_wave_scratch on the current device (set-up on first use).
+int StaticWaveScratch(int device, void **out) {
+    std::lock_guard<std::mutex> lock(g_wave_scratch_mu);
+    if (device < 0 || device >= 256) return SetError(AZ_ERR_INVALID_ARGUMENT, "device ordinal out of range");
+    if (!g_wave_scratch_addr[device]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_wave_scratch);
+        if (e != cudaSuccess) return CudaError(e, "cudaGetSymbolAddress(wave scratch)");
+        g_wave_scratch_addr[device] = p;
+    }
+    *out = g_wave_scratch_addr[device];
+    return AZ_OK;
+}
+
+WaveQueues CarveStaticQueues(unsigned char *p) {
+    WaveQueues q;
+    memset(&q, 0, sizeof(q));
+    for (int b = 0; b < 2; b++) {
+        q.o[b] = (float4 *)p; p += kQ16;
+        q.d[b] = (float4 *)p; p += kQ16;
+        q.tp[b] = (float4 *)p; p += kQ16;
+        q.att[b] = (float4 *)p; p += kQ16;
+        q.digits[b] = (uint32_t *)p; p += kQ4;
+    }
+    q.hit = (uint4 *)p; p += kQ16;
+    q.so = (float4 *)p; p += kS16;
+    q.sd = (float4 *)p; p += kS16;
+    q.sc = (float4 *)p; p += kS16;
+    q.smeta = (uint32_t *)p; p += kS4;
+    q.accum = (float4 *)p; p += kA16;
+    q.counts = (uint32_t *)p;
+    q.cap_q = kStaticCapQ;
+    q.cap_s = kStaticCapS;
+    return q;
+}
+
+}  // namespace
+}  // namespace az
+
+extern "C" int az_gpu_render_noalloc(az_gpu_scene *scene, az_pixel *film, const az_camera *camera,
+                                     const az_epsilon_values *epsilons, az_scissor scissor, int32_t filter_type,
+                                     uint32_t backface_culling, const az_render_opts *opts) {
+    using namespace az;
+    if (!scene || !scene->impl || !film || !camera) return SetError(AZ_ERR_INVALID_ARGUMENT, "null argument");
+    const GpuScene &G = *scene->impl;
+    const int device = opts ? opts->device : G.device;
+    uint32_t wave = opts && opts->chunk_samples ? opts->chunk_samples : kStaticWave;
+    if (wave > kStaticWave)
+        return SetError(AZ_ERR_INVALID_ARGUMENT,
+                        "chunk_samples " + std::to_string(wave) + " exceeds the static wave scratch of " +
+                            std::to_string(kStaticWave) + " camera samples");
+    if (G.dev.max_depth + 1 > AZ_MAX_LEVELS - 2) return SetError(AZ_ERR_UNSUPPORTED, "MaxRecursionDepth above 60");
+    AZ_CUDA_TRY(cudaSetDevice(device));
+    cudaStream_t st = opts && opts->stream ? (cudaStream_t)opts->stream : cudaStreamPerThread;
+    void *base = nullptr;
+    int rc = StaticWaveScratch(device, &base);
+    if (rc != AZ_OK) return rc;
+    CameraParams cam;
+    rc = SetupCamera(camera, scissor, filter_type, backface_culling, epsilons, opts ? opts->seed : 0, cam);
+    if (rc != AZ_OK) return rc;
+    const uint64_t total = cam.npix * (uint64_t)cam.sqrt_spp * cam.sqrt_spp;
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    const WaveQueues Q = CarveStaticQueues((unsigned char *)base);
+    const uint32_t levels = std::min<uint32_t>(G.dev.max_depth + 1, AZ_MAX_LEVELS - 2);
+    const int grid = sms * 16;
+    uint32_t host_counts[AZ_COUNT_TOTAL];
+    uint64_t pos = 0;
+    while (pos < total) {
+        const uint32_t n = (uint32_t)std::min<uint64_t>(wave, total - pos);
+        // the array keeps the previous call's contents: the counters start at
+        // zero, every other entry is written before it is read
+        AZ_CUDA_TRY(cudaMemsetAsync(Q.counts, 0, AZ_COUNT_TOTAL * sizeof(uint32_t), st));
+        AZ_CUDA_TRY(cudaMemcpyAsync(Q.counts + 1, &n, sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+        k_camera<<<(n + 255) / 256, 256, 0, st>>>(cam, Q, pos, n);
+        for (uint32_t L = 1; L <= levels; L++) {
+            k_extend<kBlock><<<grid, kBlock, 0, st>>>(G.dev, cam, Q, L);
+            k_shade<kBlock><<<grid, kBlock, 0, st>>>(G.dev, cam, Q, pos, L);
+            k_shadow<kBlock><<<grid, kBlock, 0, st>>>(G.dev, cam, Q, L);
+        }
+        k_splat<<<(n + 255) / 256, 256, 0, st>>>(cam, Q, pos, n, film);
+        AZ_CUDA_TRY(cudaGetLastError());
+        AZ_CUDA_TRY(cudaMemcpyAsync(host_counts, Q.counts, sizeof(host_counts), cudaMemcpyDeviceToHost, st));
+        AZ_CUDA_TRY(cudaStreamSynchronize(st));
+        if (host_counts[AZ_COUNT_ERROR])
+            return SetError(AZ_ERR_CUDA, "BVH traversal exceeded its step limit (corrupt hierarchy)");
+        if (host_counts[AZ_COUNT_OVERFLOW]) {
+            // the wave wrote nothing to the film; rerun it with half the samples
+            if (n <= 256) return SetError(AZ_ERR_OUT_OF_MEMORY, "static wave queues overflow with 256 samples");
+            wave = n / 2;
+            continue;
+        }
+        pos += n;
+    }
+    return AZ_OK;
+}

@@ -105,6 +105,26 @@ int az_gpu_render_host(az_gpu_scene *scene, az_pixel *pixels, const az_camera *c
                        const az_epsilon_values *epsilons, az_scissor scissor, int32_t filter_type,
                        uint32_t backface_culling, const az_render_opts *opts, az_render_stats *stats);
 
+/* Allocation-free variant of az_gpu_render; it has no counterpart in azimuth.
+ *
+ * For callers that must not allocate device memory while rendering: code
+ * running inside CUDA stream capture (where cudaMalloc is not permitted),
+ * hosts whose caching allocator owns all device memory, and real-time loops
+ * that keep a fixed memory budget.  The scene (created earlier with
+ * az_gpu_scene_create) and the DEVICE film are passed in as usual; the wave
+ * queues live in one static device array of 9,110,272 bytes (8.7 MiB) that
+ * every GPU loading this library holds until the process exits, which caps a
+ * wave at 16384 camera samples: opts->chunk_samples above 16384 is rejected
+ * with AZ_ERR_INVALID_ARGUMENT.  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress), so make that first call
+ * before any stream capture begins.  All calls share the array: calls that
+ * overlap on the GPU (other threads or streams) race and must be serialised
+ * by the caller.  Synchronous; runs on opts->stream, or on the per-thread
+ * default stream when that is NULL; never calls cudaMalloc or cudaFree. */
+int az_gpu_render_noalloc(az_gpu_scene *scene, az_pixel *film, const az_camera *camera,
+                          const az_epsilon_values *epsilons, az_scissor scissor, int32_t filter_type,
+                          uint32_t backface_culling, const az_render_opts *opts);
+
 /* Closest hit for `count` HOST rays (azimuth's RayEntityIntersection on the
  * scene root, src/azimuth_main.cpp:53-385).  Per ray: hit flag, UniqueEntityID
  * of the top-level entity, face id (entity.ID of the triangle hit inside a
