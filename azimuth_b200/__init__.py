@@ -120,8 +120,9 @@ def full_scissor(scene):
     return Scissor(Vec2u(w, h), Vec2u(0, 0))
 
 
-def make_opts(scene=None, seed=0, stream=None, device=0, flags=0, chunk_samples=0, block_size=0):
+def make_opts(scene=None, seed=0, stream=None, device=0, flags=0, chunk_samples=0, block_size=0, variant=0):
     o = RenderOpts()
+    o.variant = variant
     o.seed = seed
     o.perlin_gradients = scene.perlin_gradients if scene is not None else None
     o.stream = stream
@@ -156,13 +157,23 @@ class GpuScene:
         o = make_opts(scene, device=device)
         _check(lib().az_gpu_scene_create(scene.scene_ptr, C.byref(o), C.byref(self._h)), "az_gpu_scene_create")
 
+    def autotune(self, seed=0, stream=None):
+        """az_gpu_autotune: picks the traversal launch variant for this scene; returns (variant, ms)."""
+        o = make_opts(self.scene, seed=seed, stream=stream, device=self.device)
+        v = C.c_uint32()
+        ms = C.c_float()
+        _check(lib().az_gpu_autotune(self._h, self.scene.camera_ptr, self.scene.epsilons_ptr, full_scissor(self.scene),
+                                     self.scene.filter_type, 0, C.byref(o), C.byref(v), C.byref(ms)),
+               "az_gpu_autotune")
+        return v.value, ms.value
+
     def render_device(self, film_ptr, camera_ptr=None, scissor=None, filter_type=None, seed=0, stream=None,
-                      stats=False, flags=0, chunk_samples=0):
+                      stats=False, flags=0, chunk_samples=0, variant=0):
         """az_gpu_render into a DEVICE film pointer; returns az_render_stats as a dict if stats."""
         sc = scissor or full_scissor(self.scene)
         ft = self.scene.filter_type if filter_type is None else filter_type
         o = make_opts(self.scene, seed=seed, stream=stream, device=self.device, flags=flags,
-                      chunk_samples=chunk_samples)
+                      chunk_samples=chunk_samples, variant=variant)
         st = RenderStats() if stats else None
         _check(lib().az_gpu_render(self._h, film_ptr, camera_ptr or self.scene.camera_ptr, self.scene.epsilons_ptr,
                                    sc, ft, 0, C.byref(o), C.byref(st) if st is not None else None),

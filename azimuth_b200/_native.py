@@ -45,8 +45,8 @@ class GeneratedScene(C.Structure):
 class RenderOpts(C.Structure):
     _fields_ = [("seed", C.c_uint64), ("perlin_gradients", C.c_void_p), ("stream", C.c_void_p),
                 ("device", C.c_int32), ("flags", C.c_uint32), ("chunk_samples", C.c_uint32),
-                ("bvh_width", C.c_uint32), ("block_size", C.c_uint32),
-                ("reserved", C.c_uint32 * 5)]
+                ("bvh_width", C.c_uint32), ("block_size", C.c_uint32), ("variant", C.c_uint32),
+                ("reserved", C.c_uint32 * 4)]
 
 
 class RenderStats(C.Structure):
@@ -94,6 +94,8 @@ def _declare(L):
         L.az_gpu_render_host.argtypes = [vp, vp, vp, vp, Scissor, i32, u32, C.POINTER(RenderOpts),
                                          C.POINTER(RenderStats)]
         L.az_gpu_render_host.restype = i32
+        L.az_gpu_autotune.argtypes = [vp, vp, vp, Scissor, i32, u32, C.POINTER(RenderOpts), vp, vp]
+        L.az_gpu_autotune.restype = i32
         L.az_gpu_render_noalloc.argtypes = [vp, vp, vp, vp, Scissor, i32, u32, C.POINTER(RenderOpts)]
         L.az_gpu_render_noalloc.restype = i32
         L.az_gpu_closest_hit.argtypes = [vp, vp, u32, i32, C.c_float, vp, vp, vp, vp, vp]

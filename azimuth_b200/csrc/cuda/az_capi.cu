@@ -175,6 +175,17 @@ extern "C" int az_gpu_produce_image(az_pixel *pixels, const az_scene *scene, con
     return rc;
 }
 
+extern "C" int az_gpu_autotune(az_gpu_scene *scene, const az_camera *camera, const az_epsilon_values *epsilons,
+                               az_scissor scissor, int32_t filter_type, uint32_t backface_culling,
+                               const az_render_opts *opts, uint32_t *variant_out, float *ms_out) {
+    if (!scene || !scene->impl || !camera) return SetError(AZ_ERR_INVALID_ARGUMENT, "null argument");
+    CallContext ctx;
+    int rc = ctx.begin(opts);
+    if (rc != AZ_OK) return rc;
+    return Autotune(*scene->impl, camera, epsilons, scissor, filter_type, backface_culling, opts, ctx.stream,
+                    variant_out, ms_out);
+}
+
 extern "C" int az_gpu_closest_hit(az_gpu_scene *scene, const az_ray3 *rays, uint32_t count, int32_t cull,
                                   float hit_epsilon, uint32_t *out_hit, uint32_t *out_uid, uint32_t *out_face,
                                   float *out_t, const az_render_opts *opts) {

@@ -38,6 +38,7 @@ struct GpuScene {
     uint32_t max_bvh_depth = 0;
     size_t device_bytes = 0;
     WaveBuffers waves;           // reused across render calls on this scene
+    uint32_t variant = 2;        // traversal launch configuration (128 threads, 8 blocks/SM; az_gpu_autotune)
     az_pixel *host_film_dev = nullptr;   // device film of az_gpu_render_host
     size_t host_film_bytes = 0;
     ~GpuScene();
@@ -54,10 +55,19 @@ int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_
 int BuildLBVH(const float4 *d_lo, const float4 *d_hi, uint32_t n, azd::BVHNode *d_nodes, uint32_t node_base,
               uint32_t leaf_base, uint32_t *d_perm, cudaStream_t stream, uint32_t *root_out);
 
+// Collapse of a binary BVH (nodes `bin`, global index of bin[0] = bin_base)
+// into 8-wide nodes appended to `out`; `prim_order[j]` receives the sorted
+// primitive position of output slot prim_out_base + j.
+int CollapseToWide(const std::vector<azd::BVHNode> &bin, uint32_t bin_base, uint32_t bin_root, uint32_t max_leaf,
+                   std::vector<azd::WideNode> &out, std::vector<uint32_t> &prim_order, uint32_t prim_out_base,
+                   uint32_t *root_out, uint32_t *depth_out);
+
 int SetupCamera(const az_camera *c, az_scissor sc, int32_t filter, uint32_t cull, const az_epsilon_values *eps,
                 uint64_t seed, CameraParams &cam);
 int Render(GpuScene &G, az_pixel *film, const az_camera *camera, const az_epsilon_values *eps, az_scissor sc,
            int32_t filter, uint32_t cull, const az_render_opts *opts, cudaStream_t st, az_render_stats *stats);
+int Autotune(GpuScene &G, const az_camera *camera, const az_epsilon_values *eps, az_scissor sc, int32_t filter,
+             uint32_t cull, const az_render_opts *opts, cudaStream_t st, uint32_t *best_out, float *ms_out);
 int ClosestHit(GpuScene &G, const az_ray3 *rays, uint32_t n, int32_t cull, float eps, uint32_t *out_hit,
                uint32_t *out_uid, uint32_t *out_face, float *out_t, cudaStream_t st);
 

@@ -20,6 +20,7 @@
 // zero (e.g. the scatter ray of a pure mirror) are not traced; azimuth traces
 // them and multiplies their radiance by zero.
 #include <algorithm>
+#include <cfloat>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -127,8 +128,8 @@ __global__ void k_camera(CameraParams cam, WaveQueues Q, uint64_t wave_start, ui
     Q.accum[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 }
 
-template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_extend(DevScene S, CameraParams cam, WaveQueues Q, uint32_t level) {
+template <int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) k_extend(DevScene S, CameraParams cam, WaveQueues Q, uint32_t level) {
     const int buf = level & 1;
     const uint32_t n = min(Q.counts[level], Q.cap_q);
     uint32_t *cnt = cam.count_traversal ? Q.counts + AZ_COUNT_NODES : nullptr;
@@ -147,10 +148,14 @@ __global__ void __launch_bounds__(BLOCK) k_extend(DevScene S, CameraParams cam, 
 __device__ __forceinline__ f3 ld3(const float *p) { return mk(p[0], p[1], p[2]); }
 
 // One tree node: direct light, ambient and children (TraceRay body,
-// src/azimuth_main.cpp:974-1130).
-template <int BLOCK>
+// src/azimuth_main.cpp:974-1130).  FEAT (DevScene.features) compiles out the
+// parts a scene cannot reach: textures, environment map, mirror/dielectric
+// branches, point/area/directional/spot lights.
+template <int BLOCK, uint32_t FEAT>
 __global__ void __launch_bounds__(BLOCK) k_shade(DevScene S, CameraParams cam, WaveQueues Q, uint64_t wave_start,
                                                  uint32_t level) {
+    constexpr bool TEX = FEAT & FEAT_TEXTURES, ENV = FEAT & FEAT_ENV, SPECIAL = FEAT & FEAT_SPECIAL,
+                   LIGHTS = FEAT & FEAT_ANALYTIC_LIGHTS;
     const int buf = level & 1, nbuf = buf ^ 1;
     const uint32_t n = min(Q.counts[level], Q.cap_q);
     const bool can_spawn = level + 1 <= S.max_depth + 1;   // child's RecursionDepth <= MaxRecursionDepth
@@ -194,12 +199,12 @@ __global__ void __launch_bounds__(BLOCK) k_shade(DevScene S, CameraParams cam, W
         NodeRng rng;
         const uint32_t digits = Q.digits[buf][i];
         rng.init(cam.seed, (row << 16) | col, (sy << 16) | sx, digits, level);
-        const Surface s = surface_at(S, r, h);
+        const Surface s = surface_at<TEX>(S, r, h);
         const DevMaterial &m = S.materials[e.material];
         f3 dcol = ld3(m.diffuse), scol = ld3(m.specular);
         f3 local = mk(0.0f, 0.0f, 0.0f);   // this node's own radiance (before `tp`)
         bool ignore_ambient = false;
-        if (e.texture_index) {
+        if (TEX && e.texture_index) {
             const DevTexture &tex = S.textures[e.texture_index - 1];
             f3 ts = sample_texture(S, tex, s.p, s.u, s.v);
             if (tex.blend == 0) {           // ReplaceAll: DiffuseContribution starts at (1,1,1)
@@ -219,7 +224,11 @@ __global__ void __launch_bounds__(BLOCK) k_shade(DevScene S, CameraParams cam, W
             f3 ldir = mk(0.0f, 0.0f, 0.0f), I = ld3(L.intensity);
             uint32_t kind = SHADOW_TMAX;
             float falloff = 1.0f, ldist = 1.0f, invpdf = 1.0f;
-            if (L.type == LIGHT_POINT) {
+            if (!LIGHTS || L.type == LIGHT_ENTITY) {
+                sample_entity_light(S, L, s.p, rng, ldir, invpdf);
+                I = ld3(L.intensity);
+                kind = SHADOW_ENTITY;
+            } else if (L.type == LIGHT_POINT) {
                 ldir = ld3(L.position) - s.p;
                 ldist = length(ldir);
             } else if (L.type == LIGHT_AREA) {
@@ -248,10 +257,6 @@ __global__ void __launch_bounds__(BLOCK) k_shade(DevScene S, CameraParams cam, W
                     if (falloff < 0.0f) falloff = 0.0f;
                     else if (falloff > 1.0f) falloff = 1.0f;
                 }
-            } else {
-                sample_entity_light(S, L, s.p, rng, ldir, invpdf);
-                I = ld3(L.intensity);
-                kind = SHADOW_ENTITY;
             }
             if (ldist == 0.0f) ldist = 0.001f;
             if (inside) continue;   // no direct light inside a dielectric (:714)
@@ -259,9 +264,11 @@ __global__ void __launch_bounds__(BLOCK) k_shade(DevScene S, CameraParams cam, W
             if (!light_contribution(dc, sc, m, I, ldir, r.d, s.n, ldist, falloff, invpdf)) continue;
             f3 c = had(tp, had(dcol, dc) + had(scol, sc));
             if (is_zero(c)) continue;
-            push_shadow(Q, level, s.p + (ldir * seps), r.time, ldir, 1.0f - seps, c, slot, kind, L.uid);
+            // entity lights carry the light index (their identity test needs the light)
+            push_shadow(Q, level, s.p + (ldir * seps), r.time, ldir, 1.0f - seps, c, slot, kind,
+                        kind == SHADOW_ENTITY ? li : 0u);
         }
-        if (S.use_env_map) {
+        if (ENV && S.use_env_map) {
             // cosine-sampled environment ray (:724-778); not gated by InsideDielectric
             float phi = 2.0f * AZD_PI_F32 * rng.next();
             float cp = cosf(phi), sp = sinf(phi);
@@ -311,6 +318,7 @@ __global__ void __launch_bounds__(BLOCK) k_shade(DevScene S, CameraParams cam, W
         f3 own = local;
         if ((!inside || !m.transparent) && !ignore_ambient) own = own + had(ld3(m.ambient), ld3(S.ambient));
         add_accum(Q.accum, slot, had(tp, own));
+        if (!SPECIAL) continue;
         if (m.is_mirror) {
             // CalculateMirrorContribution (:781-854)
             f3 rd = reflect(-r.d, s.n);
@@ -384,8 +392,8 @@ __global__ void __launch_bounds__(BLOCK) k_shade(DevScene S, CameraParams cam, W
 }
 
 // Visibility of the queued light samples; unoccluded ones are added to their sample.
-template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_shadow(DevScene S, CameraParams cam, WaveQueues Q, uint32_t level) {
+template <int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) k_shadow(DevScene S, CameraParams cam, WaveQueues Q, uint32_t level) {
     const uint32_t n = min(Q.counts[AZ_COUNT_SHADOW + level], Q.cap_s);
     uint32_t *cnt = cam.count_traversal ? Q.counts + AZ_COUNT_NODES : nullptr;
     for (uint32_t i = blockIdx.x * BLOCK + threadIdx.x; i < n; i += gridDim.x * BLOCK) {
@@ -399,10 +407,21 @@ __global__ void __launch_bounds__(BLOCK) k_shadow(DevScene S, CameraParams cam, 
         Hit h;
         bool visible;
         if (kind == SHADOW_ENTITY) {
-            bool any = trace<Q_CLOSEST>(S, r, false, 0.0f, FLT_MAX, h, cnt, Q.counts + AZ_COUNT_ERROR);
-            visible = !any || (S.ents[h.ent].uid & 0x3FFFFFFFu) == uid;
+            // occluded unless the nearest hit is the light's entity: find the
+            // light's own nearest hit exactly, then look for anything else before it
+            const DevLight &L = S.lights[uid];
+            float tl;
+            int lh = light_entity_hit(S, L, r, tl);
+            if (lh < 0) {
+                bool any = trace<Q_CLOSEST>(S, r, false, 0.0f, FLT_MAX, h, cnt, Q.counts + AZ_COUNT_ERROR);
+                visible = !any || S.ents[h.ent].uid == L.uid;
+            } else {
+                visible = !trace<Q_ANY>(S, r, false, 0.0f, lh ? tl : FLT_MAX, h, cnt, Q.counts + AZ_COUNT_ERROR,
+                                        L.ent_index);
+            }
         } else {
-            visible = !trace<Q_ANY>(S, r, false, 0.0f, kind == SHADOW_ANY ? FLT_MAX : d.w, h, cnt, Q.counts + AZ_COUNT_ERROR);
+            visible = !trace<Q_ANY>(S, r, false, 0.0f, kind == SHADOW_ANY ? FLT_MAX : d.w, h, cnt,
+                                    Q.counts + AZ_COUNT_ERROR);
         }
         if (visible) add_accum(Q.accum, __float_as_uint(c.w), mk(c.x, c.y, c.z));
     }
@@ -436,6 +455,64 @@ __global__ void k_splat(CameraParams cam, WaveQueues Q, uint64_t wave_start, uin
 }
 
 constexpr int kBlock = 128;
+
+// Launch configurations of the two traversal kernels (threads per block,
+// minimum resident blocks per SM, which caps registers); chosen per scene by
+// az_gpu_autotune.
+struct Variant {
+    int block, minb;
+};
+constexpr Variant kVariants[] = {{128, 1}, {128, 6}, {128, 8}, {256, 1}, {256, 3}, {64, 1}, {64, 12}};
+constexpr uint32_t kVariantCount = sizeof(kVariants) / sizeof(kVariants[0]);
+
+template <uint32_t F>
+void LaunchShadeF(int grid, const DevScene &S, const CameraParams &cam, const WaveQueues &Q, uint64_t start,
+                  uint32_t L, cudaStream_t st) {
+    k_shade<kBlock, F><<<grid, kBlock, 0, st>>>(S, cam, Q, start, L);
+}
+
+void LaunchShade(int grid, const DevScene &S, const CameraParams &cam, const WaveQueues &Q, uint64_t start,
+                 uint32_t L, cudaStream_t st) {
+    switch (S.features & 15u) {
+        case 0: LaunchShadeF<0>(grid, S, cam, Q, start, L, st); break;
+        case 1: LaunchShadeF<1>(grid, S, cam, Q, start, L, st); break;
+        case 2: LaunchShadeF<2>(grid, S, cam, Q, start, L, st); break;
+        case 3: LaunchShadeF<3>(grid, S, cam, Q, start, L, st); break;
+        case 4: LaunchShadeF<4>(grid, S, cam, Q, start, L, st); break;
+        case 5: LaunchShadeF<5>(grid, S, cam, Q, start, L, st); break;
+        case 6: LaunchShadeF<6>(grid, S, cam, Q, start, L, st); break;
+        case 7: LaunchShadeF<7>(grid, S, cam, Q, start, L, st); break;
+        case 8: LaunchShadeF<8>(grid, S, cam, Q, start, L, st); break;
+        case 9: LaunchShadeF<9>(grid, S, cam, Q, start, L, st); break;
+        case 10: LaunchShadeF<10>(grid, S, cam, Q, start, L, st); break;
+        case 11: LaunchShadeF<11>(grid, S, cam, Q, start, L, st); break;
+        case 12: LaunchShadeF<12>(grid, S, cam, Q, start, L, st); break;
+        case 13: LaunchShadeF<13>(grid, S, cam, Q, start, L, st); break;
+        case 14: LaunchShadeF<14>(grid, S, cam, Q, start, L, st); break;
+        default: LaunchShadeF<15>(grid, S, cam, Q, start, L, st); break;
+    }
+}
+
+template <int B, int M>
+void LaunchTraversal(bool shadow, int sms, const DevScene &S, const CameraParams &cam, const WaveQueues &Q,
+                     uint32_t L, cudaStream_t st) {
+    const int grid = sms * (2048 / B);
+    if (shadow) k_shadow<B, M><<<grid, B, 0, st>>>(S, cam, Q, L);
+    else k_extend<B, M><<<grid, B, 0, st>>>(S, cam, Q, L);
+}
+
+void LaunchTraversalVariant(uint32_t v, bool shadow, int sms, const DevScene &S, const CameraParams &cam,
+                            const WaveQueues &Q, uint32_t L, cudaStream_t st) {
+    switch (v) {
+        case 1: LaunchTraversal<128, 6>(shadow, sms, S, cam, Q, L, st); break;
+        case 2: LaunchTraversal<128, 8>(shadow, sms, S, cam, Q, L, st); break;
+        case 3: LaunchTraversal<256, 1>(shadow, sms, S, cam, Q, L, st); break;
+        case 4: LaunchTraversal<256, 3>(shadow, sms, S, cam, Q, L, st); break;
+        case 5: LaunchTraversal<64, 1>(shadow, sms, S, cam, Q, L, st); break;
+        case 6: LaunchTraversal<64, 12>(shadow, sms, S, cam, Q, L, st); break;
+        default: LaunchTraversal<128, 1>(shadow, sms, S, cam, Q, L, st); break;
+    }
+}
 
 }  // namespace
 
@@ -584,13 +661,14 @@ static int RenderWave(const GpuScene &G, const CameraParams &cam, WaveBuffers &W
     rc.launches++;
     const uint32_t levels = std::min<uint32_t>(G.dev.max_depth + 1, AZ_MAX_LEVELS - 2);
     const int grid = sms * 16;
+    const uint32_t v = cam.variant;
     for (uint32_t L = 1; L <= levels; L++) {
         if (timer) timer->Mark(st, 0);
-        k_extend<kBlock><<<grid, kBlock, 0, st>>>(G.dev, cam, Q, L);
+        LaunchTraversalVariant(v, false, sms, G.dev, cam, Q, L, st);
         if (timer) timer->Mark(st, 1);
-        k_shade<kBlock><<<grid, kBlock, 0, st>>>(G.dev, cam, Q, start, L);
+        LaunchShade(grid, G.dev, cam, Q, start, L, st);
         if (timer) timer->Mark(st, 2);
-        k_shadow<kBlock><<<grid, kBlock, 0, st>>>(G.dev, cam, Q, L);
+        LaunchTraversalVariant(v, true, sms, G.dev, cam, Q, L, st);
         if (timer) timer->Mark(st, 3);
         rc.launches += 3;
         rc.extend_launches++;
@@ -607,6 +685,8 @@ int Render(GpuScene &G, az_pixel *film, const az_camera *camera, const az_epsilo
     int rc = SetupCamera(camera, sc, filter, cull, eps, opts ? opts->seed : 0, cam);
     if (rc != AZ_OK) return rc;
     cam.count_traversal = opts && (opts->flags & AZ_FLAG_COUNT_TRAVERSAL) ? 1u : 0u;
+    cam.variant = opts && opts->variant ? opts->variant - 1 : G.variant;
+    if (cam.variant >= kVariantCount) return SetError(AZ_ERR_INVALID_ARGUMENT, "unknown launch variant");
     if (G.dev.max_depth + 1 > AZ_MAX_LEVELS - 2) return SetError(AZ_ERR_UNSUPPORTED, "MaxRecursionDepth above 60");
     uint64_t total = cam.npix * (uint64_t)cam.sqrt_spp * cam.sqrt_spp;
     if (stats) memset(stats, 0, sizeof(*stats));
@@ -682,6 +762,46 @@ int Render(GpuScene &G, az_pixel *film, const az_camera *camera, const az_epsilo
             stats->shadow_ms = timer->ms[2];
         }
     }
+    return AZ_OK;
+}
+
+// Times every launch variant on a band of the frame (the middle eighth of the
+// scissor's rows, all samples) and keeps the fastest for this scene.
+int Autotune(GpuScene &G, const az_camera *camera, const az_epsilon_values *eps, az_scissor sc, int32_t filter,
+             uint32_t cull, const az_render_opts *opts, cudaStream_t st, uint32_t *best_out, float *ms_out) {
+    CameraParams cam;
+    int rc = SetupCamera(camera, sc, filter, cull, eps, opts ? opts->seed : 0, cam);
+    if (rc != AZ_OK) return rc;
+    uint32_t rows = std::max<uint32_t>(1, cam.hsc / 8);
+    az_scissor band = sc;
+    band.Min.y = cam.r0 + (cam.hsc - rows) / 2;
+    band.Max.y = band.Min.y + rows;
+    band.Min.x = cam.c0;
+    band.Max.x = cam.c0 + cam.wsc;
+    size_t bytes = (size_t)cam.width * cam.height * sizeof(az_pixel);
+    az_pixel *film = nullptr;
+    AZ_CUDA_TRY(cudaMalloc((void **)&film, bytes));
+    float best_ms = FLT_MAX;
+    uint32_t best = 0;
+    az_render_opts o;
+    if (opts) o = *opts;
+    else memset(&o, 0, sizeof(o));
+    for (uint32_t v = 0; v < kVariantCount && rc == AZ_OK; v++) {
+        o.variant = v + 1;
+        o.flags &= ~(uint32_t)AZ_FLAG_TIME_STAGES;
+        az_render_stats stats;
+        for (int rep = 0; rep < 2 && rc == AZ_OK; rep++)   // the first run warms caches and allocates queues
+            rc = Render(G, film, camera, eps, band, filter, cull, &o, st, &stats);
+        if (rc == AZ_OK && stats.gpu_ms < best_ms) {
+            best_ms = stats.gpu_ms;
+            best = v;
+        }
+    }
+    cudaFree(film);
+    if (rc != AZ_OK) return rc;
+    G.variant = best;
+    if (best_out) *best_out = best + 1;
+    if (ms_out) *ms_out = best_ms;
     return AZ_OK;
 }
 
@@ -820,6 +940,8 @@ extern "C" int az_gpu_render_noalloc(az_gpu_scene *scene, az_pixel *film, const 
     CameraParams cam;
     rc = SetupCamera(camera, scissor, filter_type, backface_culling, epsilons, opts ? opts->seed : 0, cam);
     if (rc != AZ_OK) return rc;
+    cam.variant = opts && opts->variant ? opts->variant - 1 : G.variant;
+    if (cam.variant >= kVariantCount) return SetError(AZ_ERR_INVALID_ARGUMENT, "unknown launch variant");
     const uint64_t total = cam.npix * (uint64_t)cam.sqrt_spp * cam.sqrt_spp;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -836,9 +958,9 @@ extern "C" int az_gpu_render_noalloc(az_gpu_scene *scene, az_pixel *film, const 
         AZ_CUDA_TRY(cudaMemcpyAsync(Q.counts + 1, &n, sizeof(uint32_t), cudaMemcpyHostToDevice, st));
         k_camera<<<(n + 255) / 256, 256, 0, st>>>(cam, Q, pos, n);
         for (uint32_t L = 1; L <= levels; L++) {
-            k_extend<kBlock><<<grid, kBlock, 0, st>>>(G.dev, cam, Q, L);
-            k_shade<kBlock><<<grid, kBlock, 0, st>>>(G.dev, cam, Q, pos, L);
-            k_shadow<kBlock><<<grid, kBlock, 0, st>>>(G.dev, cam, Q, L);
+            LaunchTraversalVariant(cam.variant, false, sms, G.dev, cam, Q, L, st);
+            LaunchShade(grid, G.dev, cam, Q, pos, L, st);
+            LaunchTraversalVariant(cam.variant, true, sms, G.dev, cam, Q, L, st);
         }
         k_splat<<<(n + 255) / 256, 256, 0, st>>>(cam, Q, pos, n, film);
         AZ_CUDA_TRY(cudaGetLastError());

@@ -31,6 +31,7 @@ struct CameraParams {
     float eps_isect, eps_shadow;
     uint32_t cull;
     uint32_t count_traversal;
+    uint32_t variant;              // launch configuration of the traversal kernels
 };
 
 // Device queues of one wave of camera samples (structure of arrays).

@@ -71,6 +71,24 @@ struct __align__(16) BVHNode {
     uint4 ch;    // child0, child1, count0, count1 (count 0: inner node index; else primitive range start)
 };
 
+// 8-wide compressed node (80 B = five 16-byte fetches).  Child boxes are
+// quantised to 8 bits per bound on a per-node grid: lo = p + q_lo * 2^e,
+// hi = p + q_hi * 2^e, rounded outward so the decoded boxes contain the true
+// ones.  Slot s holds the child whose centre lies on the side given by the
+// bits of s (bit a set: upper half along axis a), so visiting slots in the
+// order of (s XOR ray-octant) is near-first.
+struct __align__(16) WideNode {
+    float px, py, pz;
+    uint8_t ex, ey, ez;       // biased float exponents of the grid step per axis
+    uint8_t imask;            // bit s: slot s is an inner node
+    uint32_t child_base;      // first inner child node; inner children are consecutive in slot order
+    uint32_t prim_base;       // first primitive of the leaf children
+    uint8_t meta[8];          // inner: 0; leaf: (count << 5) | offset from prim_base; empty: 0 with imask bit clear
+    uint8_t qlo_x[8], qlo_y[8], qlo_z[8];
+    uint8_t qhi_x[8], qhi_y[8], qhi_z[8];
+};
+static_assert(sizeof(WideNode) == 80, "wide node is five 16-byte words");
+
 // Textures (src/azimuth_texture.h:52-86), compacted for the device.
 struct __align__(16) DevTexture {
     uint32_t type, format, width, height;
@@ -108,6 +126,8 @@ struct __align__(16) DevLight {
     float total_area;
     uint32_t tri_offset;      // into light_tris (mesh light's `triangle` array)
     m34 inv, xf;
+    float motion[3];          // the light entity's MotionVector
+    uint32_t ent_index;       // dense index of the light's entity in ents[], or 0xFFFFFFFF
 };
 
 struct __align__(16) DevLightTri {
@@ -116,6 +136,9 @@ struct __align__(16) DevLightTri {
     float4 p2n;  // P2.xyz, N.z
 };
 
+// DevScene.features: parts of the shading code a scene can reach.
+enum : uint32_t { FEAT_TEXTURES = 1u, FEAT_ENV = 2u, FEAT_SPECIAL = 4u, FEAT_ANALYTIC_LIGHTS = 8u };
+
 // Everything a kernel needs, passed by value.
 struct DevScene {
     const DevTri *tris;
@@ -123,7 +146,8 @@ struct DevScene {
     const DevEntity *ents;
     const DevGroup *groups;
     const uint32_t *tlas_prims;
-    const BVHNode *nodes;
+    const BVHNode *nodes;           // binary nodes (unused once wide nodes exist)
+    const WideNode *wnodes;
     const DevMaterial *materials;
     const DevTexture *textures;     // [0 .. texture_count) = scene.Textures
     const DevLight *lights;
@@ -139,6 +163,7 @@ struct DevScene {
     uint32_t use_bg_texture, use_env_map;
     uint32_t max_depth, path_trace, importance_sampling;
     uint32_t light_draws;           // RNG draws made by the light loop at every vertex
+    uint32_t features;              // FEAT_* bits
 };
 
 }  // namespace azd

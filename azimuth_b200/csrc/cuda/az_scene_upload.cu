@@ -63,7 +63,6 @@ struct Box {
         grow(b.lo[0], b.lo[1], b.lo[2]);
         grow(b.hi[0], b.hi[1], b.hi[2]);
     }
-    bool valid() const { return lo[0] <= hi[0] && lo[1] <= hi[1] && lo[2] <= hi[2]; }
 };
 
 // World box of a local box under an affine transform and linear motion over
@@ -435,6 +434,13 @@ int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_
         if (L.Type == AZ_Light_Entity) {
             const az_entity &E = L.Entity;
             d.uid = E.UniqueEntityID;
+            memcpy(d.motion, &E.MotionVector, 12);
+            d.ent_index = 0xFFFFFFFFu;
+            for (uint32_t k = 0; k < F.ents.size(); k++)
+                if (F.ents[k].uid == E.UniqueEntityID) {
+                    d.ent_index = k;
+                    break;
+                }
             memcpy(d.intensity, &E.Radiance, 12);
             d.inv = ToM34(E.InvTransformationMatrix);
             d.xf = ToM34(E.TransformationMatrix);
@@ -522,7 +528,40 @@ int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_
         AZ_CUDA_TRY(cudaMemcpyAsync(d_attr_unsorted, all_attr.data(), all_attr.size() * sizeof(azd::DevTriAttr),
                                     cudaMemcpyHostToDevice, st));
     }
+    // Per hierarchy: LBVH on the GPU, read back, collapse to 8-wide nodes on the
+    // host, then gather the primitives once into wide-leaf order.
+    std::vector<azd::WideNode> wide;
+    uint32_t wide_depth = 0;
+    auto collapse = [&](uint32_t n, uint32_t node_base, uint32_t bin_root, uint32_t prim_base, uint32_t max_leaf,
+                        std::vector<uint32_t> &comp, uint32_t *wroot) -> int {
+        uint32_t nb = n > 1 ? n - 1 : 1;
+        std::vector<azd::BVHNode> bin(nb);
+        std::vector<uint32_t> perm(n);
+        AZ_CUDA_TRY(cudaMemcpyAsync(bin.data(), d_nodes + node_base, nb * sizeof(azd::BVHNode),
+                                    cudaMemcpyDeviceToHost, st));
+        AZ_CUDA_TRY(cudaMemcpyAsync(perm.data(), d_perm, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        AZ_CUDA_TRY(cudaStreamSynchronize(st));
+        std::vector<uint32_t> order;
+        order.reserve(n);
+        uint32_t depth = 0;
+        int rc2 = CollapseToWide(bin, node_base, bin_root, max_leaf, wide, order, prim_base, wroot, &depth);
+        if (rc2 != AZ_OK) return rc2;
+        if (order.size() != n) return SetError(AZ_ERR_CUDA, "BVH collapse lost primitives");
+        wide_depth = std::max(wide_depth, depth);
+        // output slot j holds sorted position order[j], i.e. unsorted primitive perm[order[j] - prim_base]
+        comp.resize(n);
+        std::vector<uint8_t> seen(n, 0);
+        for (uint32_t j = 0; j < n; j++) {
+            uint32_t sp = order[j] - prim_base;
+            if (sp >= n || perm[sp] >= n || seen[perm[sp]])
+                return SetError(AZ_ERR_CUDA, "BVH collapse did not produce a permutation of the primitives");
+            seen[perm[sp]] = 1;
+            comp[j] = perm[sp];
+        }
+        return AZ_OK;
+    };
     uint32_t node_base = 0;
+    std::vector<uint32_t> comp;
     for (auto &g : F.groups) {
         uint32_t n = g.g.tri_end - g.g.tri_begin;
         if (n == 0) {
@@ -532,32 +571,45 @@ int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_
         const int B = 256;
         k_tri_boxes<<<(n + B - 1) / B, B, 0, st>>>(d_tris_unsorted + g.g.tri_begin, n, d_lo, d_hi);
         AZ_CUDA_TRY(cudaGetLastError());
-        uint32_t root;
+        uint32_t root, wroot;
         rc = BuildLBVH(d_lo, d_hi, n, d_nodes, node_base, g.g.tri_begin, d_perm, st, &root);
         if (rc != AZ_OK) return rc;
-        g.g.root = root;
+        rc = collapse(n, node_base, root, g.g.tri_begin, 2, comp, &wroot);
+        if (rc != AZ_OK) return rc;
+        g.g.root = wroot;
         node_base += n > 1 ? n - 1 : 1;
+        AZ_CUDA_TRY(cudaMemcpyAsync(d_perm, comp.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
         k_gather_tris<<<(n + B - 1) / B, B, 0, st>>>(d_tris_unsorted + g.g.tri_begin, d_attr_unsorted + g.g.tri_begin,
                                                      d_perm, n, d_tris + g.g.tri_begin, d_attr + g.g.tri_begin);
         AZ_CUDA_TRY(cudaGetLastError());
+        AZ_CUDA_TRY(cudaStreamSynchronize(st));
     }
     uint32_t *d_tlas = (uint32_t *)G->Alloc((tlas.size() + 1) * sizeof(uint32_t));
     uint32_t *d_tlas_unsorted = (uint32_t *)G->Alloc((tlas.size() + 1) * sizeof(uint32_t));
     if (!d_tlas || !d_tlas_unsorted) return SetError(AZ_ERR_OUT_OF_MEMORY, "device allocation failed");
     uint32_t tlas_root = 0xFFFFFFFFu;
     if (!tlas.empty()) {
+        uint32_t n = (uint32_t)tlas.size();
         AZ_CUDA_TRY(cudaMemcpyAsync(d_lo, tlo.data(), tlo.size() * sizeof(float4), cudaMemcpyHostToDevice, st));
         AZ_CUDA_TRY(cudaMemcpyAsync(d_hi, thi.data(), thi.size() * sizeof(float4), cudaMemcpyHostToDevice, st));
-        AZ_CUDA_TRY(cudaMemcpyAsync(d_tlas_unsorted, tlas.data(), tlas.size() * sizeof(uint32_t),
-                                    cudaMemcpyHostToDevice, st));
-        rc = BuildLBVH(d_lo, d_hi, (uint32_t)tlas.size(), d_nodes, node_base, 0, d_perm, st, &tlas_root);
+        AZ_CUDA_TRY(cudaMemcpyAsync(d_tlas_unsorted, tlas.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+        uint32_t root;
+        rc = BuildLBVH(d_lo, d_hi, n, d_nodes, node_base, 0, d_perm, st, &root);
         if (rc != AZ_OK) return rc;
-        node_base += tlas.size() > 1 ? (uint32_t)tlas.size() - 1 : 1;
+        // top-level leaves hold one primitive each (a group is entered from its leaf)
+        rc = collapse(n, node_base, root, 0, 1, comp, &tlas_root);
+        if (rc != AZ_OK) return rc;
+        node_base += n > 1 ? n - 1 : 1;
         const int B = 256;
-        k_gather_u32<<<((uint32_t)tlas.size() + B - 1) / B, B, 0, st>>>(d_tlas_unsorted, d_perm, (uint32_t)tlas.size(),
-                                                                          d_tlas);
+        AZ_CUDA_TRY(cudaMemcpyAsync(d_perm, comp.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+        k_gather_u32<<<(n + B - 1) / B, B, 0, st>>>(d_tlas_unsorted, d_perm, n, d_tlas);
         AZ_CUDA_TRY(cudaGetLastError());
     }
+    azd::WideNode *d_wide = (azd::WideNode *)G->Alloc((wide.size() + 1) * sizeof(azd::WideNode));
+    if (!d_wide) return SetError(AZ_ERR_OUT_OF_MEMORY, "device allocation failed");
+    if (!wide.empty())
+        AZ_CUDA_TRY(cudaMemcpyAsync(d_wide, wide.data(), wide.size() * sizeof(azd::WideNode), cudaMemcpyHostToDevice,
+                                    st));
 
     std::vector<azd::DevGroup> dgroups;
     for (auto &g : F.groups) dgroups.push_back(g.g);
@@ -572,7 +624,8 @@ int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_
     D.ents = Upload(*G, F.ents, st, rc);
     D.groups = Upload(*G, dgroups, st, rc);
     D.tlas_prims = d_tlas;
-    D.nodes = d_nodes;
+    D.nodes = nullptr;
+    D.wnodes = d_wide;
     D.materials = Upload(*G, mats, st, rc);
     D.textures = Upload(*G, texs, st, rc);
     D.lights = Upload(*G, lights, st, rc);
@@ -597,11 +650,18 @@ int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_
     D.path_trace = scene->PathTrace ? 1u : 0u;
     D.importance_sampling = scene->ImportanceSampling ? 1u : 0u;
     D.light_draws = light_draws;
+    D.features = 0;
+    if (scene->TextureCount > 0) D.features |= azd::FEAT_TEXTURES;
+    if (scene->UseEnvironmentMap) D.features |= azd::FEAT_ENV;
+    for (const azd::DevMaterial &m : mats)
+        if (m.transparent || m.is_mirror) D.features |= azd::FEAT_SPECIAL;
+    for (const azd::DevLight &l : lights)
+        if (l.type != azd::LIGHT_ENTITY) D.features |= azd::FEAT_ANALYTIC_LIGHTS;
     AZ_CUDA_TRY(cudaStreamSynchronize(st));
     // the unsorted copies and build scratch are no longer needed
     for (auto &b : G->bufs) {
         if (b.ptr == d_tris_unsorted || b.ptr == d_attr_unsorted || b.ptr == d_lo || b.ptr == d_hi ||
-            b.ptr == d_perm || b.ptr == d_tlas_unsorted) {
+            b.ptr == d_perm || b.ptr == d_tlas_unsorted || b.ptr == d_nodes) {
             cudaFree(b.ptr);
             G->device_bytes -= b.bytes;
             b.ptr = nullptr;
@@ -609,7 +669,8 @@ int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_
     }
     G->triangle_count = total_tris;
     G->sphere_count = tlas.size() - dgroups.size();
-    G->node_count = node_total;
+    G->node_count = wide.size();
+    G->max_bvh_depth = wide_depth;
     *out = G.release();
     return AZ_OK;
 }

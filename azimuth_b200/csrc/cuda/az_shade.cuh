@@ -131,6 +131,8 @@ __device__ __forceinline__ void apply_bump(const DevScene &S, const DevTexture &
 }
 
 // Recompute P, normal and UV of a hit exactly as azimuth does when it finds it.
+// TEX = false when the scene has no textures (no bump mapping to apply).
+template <bool TEX>
 __device__ Surface surface_at(const DevScene &S, const Ray &wr, const Hit &h) {
     Surface s;
     s.ent = h.ent;
@@ -151,7 +153,7 @@ __device__ Surface surface_at(const DevScene &S, const Ray &wr, const Hit &h) {
         const float two_pi = AZD_PI_F32 * 2.0f;
         s.p = wp;
         bool deferred = false;
-        if (e.texture_index) {
+        if (TEX && e.texture_index) {
             const DevTexture &tex = S.textures[e.texture_index - 1];
             s.n = hn;
             deferred = true;
@@ -202,7 +204,7 @@ __device__ Surface surface_at(const DevScene &S, const Ray &wr, const Hit &h) {
     }
     s.u = ((alpha * a.uv0[0]) + (beta * a.uv1[0])) + (gamma * a.uv2[0]);
     s.v = ((alpha * a.uv0[1]) + (beta * a.uv1[1])) + (gamma * a.uv2[1]);
-    if (a.texture_index) {
+    if (TEX && a.texture_index) {
         const DevTexture &tex = S.textures[a.texture_index - 1];
         if (tex.bump) {
             float div = ((a.uv1[0] - a.uv0[0]) * (a.uv2[1] - a.uv0[1])) - ((a.uv1[1] - a.uv0[1]) * (a.uv2[0] - a.uv0[0]));
@@ -327,6 +329,41 @@ __device__ void sample_entity_light(const DevScene &S, const DevLight &L, f3 hp,
         invpdf = (area * ca) / (l * l);
     }
     dir = vector_xf(L.xf, ldl);
+}
+
+// Nearest hit of a ray on an entity light's own primitives, with azimuth's
+// arithmetic (sphere :64-146; mesh instance :244-281 over the mesh's
+// `triangle` array, whose vertices are the triangle entities' vertices).
+// Returns 1 with the world t, 0 if the light is not hit, -1 if the light is
+// too large to test here (the caller then runs a full nearest-hit query).
+__device__ int light_entity_hit(const DevScene &S, const DevLight &L, const Ray &wr, float &t_world) {
+    if (L.ent_index == 0xFFFFFFFFu) return -1;
+    if (L.entity_type == ENT_SPHERE) {
+        float tl;
+        return sphere_test(S.ents[L.ent_index], wr, 0.0f, t_world, tl) ? 1 : 0;
+    }
+    if (L.tri_count > 64) return -1;
+    f3 motion = wr.time * mk(L.motion[0], L.motion[1], L.motion[2]);
+    Ray m = wr;
+    m.o = wr.o - motion;
+    Ray lr = local_ray(m, L.inv);
+    float best = FLT_MAX;
+    for (uint32_t k = 0; k < L.tri_count; k++) {
+        const DevLightTri &T = S.light_tris[L.tri_offset + k];
+        DevTri tr;
+        tr.a = make_float4(T.p0n.x, T.p0n.y, T.p0n.z, T.p0n.x - T.p1n.x);
+        tr.b = make_float4(T.p0n.y - T.p1n.y, T.p0n.z - T.p1n.z, T.p0n.x - T.p2n.x, T.p0n.y - T.p2n.y);
+        tr.c = make_float4(T.p0n.z - T.p2n.z, T.p0n.w, T.p1n.w, T.p2n.w);
+        float t, b, g;
+        if (tri_test(tr, lr, false, 0.0f, best, t, b, g)) best = t;
+    }
+    if (best == FLT_MAX) return 0;
+    f3 lp = lr.o + (lr.d * best);
+    f3 wp = point_xf(L.xf, lp) + motion;
+    float wt = length(wp - m.o - motion) / length(wr.d);
+    if (!(wt > 0.0f && wt < FLT_MAX)) return 0;
+    t_world = wt;
+    return 1;
 }
 
 // Background of a primary miss, SampleBackgroundColor (:1180-1207).

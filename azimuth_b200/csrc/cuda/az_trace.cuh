@@ -5,10 +5,10 @@
 // (src/azimuth_main.cpp:147-243), the transformed, moving sphere
 // (:64-146) and the mesh-instance path (:244-281: motion, GetLocalRay with a
 // re-normalised direction, world t recomputed from the local hit point).
-// The hierarchy is this library's own BVH, traversed near-first with
-// t-pruning on conservative boxes; it finds the same nearest primitive as
-// azimuth's exhaustive BVH walk except for exact ties and rays that graze a
-// box azimuth's slab test rejects.
+// The hierarchy is this library's own 8-wide compressed BVH, traversed
+// near-first with t-pruning on conservative boxes; it finds the same nearest
+// primitive as azimuth's exhaustive BVH walk except for exact ties and rays
+// that graze a box azimuth's slab test rejects.
 #pragma once
 #include <cfloat>
 
@@ -83,14 +83,25 @@ __device__ __forceinline__ bool tri_test(const DevTri &tr, const Ray &r, bool cu
     float K = p0x - r.o.x, M = p0y - r.o.y, N = p0z - r.o.z;
     float detB = (K * E * I) + (M * H * C) + (N * B * F) - (C * E * N) - (F * H * K) - (I * B * M);
     const float lower = -0.000001f;
+    // Division-free pre-rejects: only cases where azimuth's test is certain to
+    // fail (the quotient is out of range by far more than its rounding), so
+    // every accepted hit still comes from azimuth's exact divisions below.
+    const float am = fabsf(detM);
+    const float sb = detM < 0.0f ? -detB : detB;
+    if (!(sb > -0.001f * am && sb <= 1.001f * am)) return false;
     float beta = detB / detM;
     if (!(beta > lower && beta <= 1.0f)) return false;
     float detG = (A * M * I) + (D * N * C) + (G * K * F) - (C * M * G) - (F * N * A) - (I * K * D);
+    const float sg = detM < 0.0f ? -detG : detG;
+    if (!(sg > -0.001f * am && sg <= 1.001f * am)) return false;
     float gamma = detG / detM;
     if (!(gamma > lower && gamma <= 1.0f)) return false;
     float alpha = 1.0f - beta - gamma;
     if (!(alpha > lower)) return false;
     float detT = (A * E * N) + (D * H * K) + (G * B * M) - (K * E * G) - (M * H * A) - (N * B * D);
+    const float st = detM < 0.0f ? -detT : detT;
+    if (eps >= 0.0f && !(st > 0.0f)) return false;                // t <= 0 <= eps
+    if (st >= tmax * 1.0001f * am) return false;                   // t >= tmax
     float t = detT / detM;
     if (!(t > eps && t < tmax)) return false;
     t_out = t;
@@ -99,45 +110,14 @@ __device__ __forceinline__ bool tri_test(const DevTri &tr, const Ray &r, bool cu
     return true;
 }
 
-// Conservative slab test of both children of a node (explicit FMAs; boxes are
-// stored slightly enlarged).  Returns a 2-bit mask and the entry distances.
-__device__ __forceinline__ uint32_t node_test(const BVHNode &n, f3 oinv, f3 inv, float tmin, float tmax,
-                                              float &t0, float &t1) {
-    const float l0x = __fmaf_rn(n.bx.x, inv.x, -oinv.x), h0x = __fmaf_rn(n.bx.y, inv.x, -oinv.x);
-    const float l1x = __fmaf_rn(n.bx.z, inv.x, -oinv.x), h1x = __fmaf_rn(n.bx.w, inv.x, -oinv.x);
-    const float l0y = __fmaf_rn(n.by.x, inv.y, -oinv.y), h0y = __fmaf_rn(n.by.y, inv.y, -oinv.y);
-    const float l1y = __fmaf_rn(n.by.z, inv.y, -oinv.y), h1y = __fmaf_rn(n.by.w, inv.y, -oinv.y);
-    const float l0z = __fmaf_rn(n.bz.x, inv.z, -oinv.z), h0z = __fmaf_rn(n.bz.y, inv.z, -oinv.z);
-    const float l1z = __fmaf_rn(n.bz.z, inv.z, -oinv.z), h1z = __fmaf_rn(n.bz.w, inv.z, -oinv.z);
-    float n0 = fmaxf(fmaxf(fminf(l0x, h0x), fminf(l0y, h0y)), fmaxf(fminf(l0z, h0z), tmin));
-    float f0 = fminf(fminf(fmaxf(l0x, h0x), fmaxf(l0y, h0y)), fminf(fmaxf(l0z, h0z), tmax));
-    float n1 = fmaxf(fmaxf(fminf(l1x, h1x), fminf(l1y, h1y)), fmaxf(fminf(l1z, h1z), tmin));
-    float f1 = fminf(fminf(fmaxf(l1x, h1x), fmaxf(l1y, h1y)), fminf(fmaxf(l1z, h1z), tmax));
-    // 1 + 2^-20 absorbs the rounding of the slab distances (cf. Ize 2013)
-    f0 *= 1.00000095367431640625f;
-    f1 *= 1.00000095367431640625f;
-    t0 = n0;
-    t1 = n1;
-    return (n0 <= f0 ? 1u : 0u) | (n1 <= f1 ? 2u : 0u);
-}
-
+// Reciprocal direction for the box tests; components are kept at most 1e18
+// in magnitude so that 2^23 * grid step * 1/d stays finite.
 __device__ __forceinline__ f3 safe_inv(f3 d) {
-    const float tiny = 1e-30f;
+    const float tiny = 1e-18f;
     float x = fabsf(d.x) < tiny ? copysignf(tiny, d.x) : d.x;
     float y = fabsf(d.y) < tiny ? copysignf(tiny, d.y) : d.y;
     float z = fabsf(d.z) < tiny ? copysignf(tiny, d.z) : d.z;
     return mk(1.0f / x, 1.0f / y, 1.0f / z);
-}
-
-__device__ __forceinline__ BVHNode load_node(const BVHNode *nodes, uint32_t i) {
-    const float4 *p = reinterpret_cast<const float4 *>(nodes + i);
-    BVHNode n;
-    n.bx = __ldg(p + 0);
-    n.by = __ldg(p + 1);
-    n.bz = __ldg(p + 2);
-    float4 c = __ldg(p + 3);
-    n.ch = make_uint4(__float_as_uint(c.x), __float_as_uint(c.y), __float_as_uint(c.z), __float_as_uint(c.w));
-    return n;
 }
 
 __device__ __forceinline__ DevTri load_tri(const DevTri *tris, uint32_t i) {
@@ -149,223 +129,275 @@ __device__ __forceinline__ DevTri load_tri(const DevTri *tris, uint32_t i) {
     return t;
 }
 
-// Stack entries: inner node index, leaf range or the BLAS-exit marker.
-#define AZD_ENT_LEAF 0x80000000u
-#define AZD_ENT_EXIT 0xFFFFFFFFu
-#define AZD_STACK 64
-
-// leaf entry: flag, 3 bits of count-1 (leaves hold at most 8 primitives), 27 bits of start
-__device__ __forceinline__ uint32_t leaf_entry(uint32_t start, uint32_t count) {
-    return AZD_ENT_LEAF | (((count - 1u) & 7u) << 27) | (start & 0x07FFFFFFu);
-}
-
 enum QueryKind : uint32_t {
     Q_CLOSEST = 0,   // nearest hit
     Q_ANY = 1        // any hit with world t < tmax (early exit)
 };
 
-// Two-level traversal.  For Q_CLOSEST returns the nearest hit in `best`
-// (best.ent == 0xFFFFFFFF: none).  For Q_ANY returns true as soon as a
-// primitive's world t < tmax.  `counts` (optional) accumulates node and
-// primitive visits.
-// A valid BVH needs far fewer steps; the cap only guards against a corrupt
-// tree looping forever.  When hit, the query stops and sets *err.
+// A valid hierarchy needs far fewer steps; the cap only guards against a
+// corrupt one looping forever.  When hit, the query stops and sets *err.
 #define AZD_MAX_STEPS (1u << 22)
+#define AZD_WSTACK 48
 
+// Stack entries (uint2): .x a base index, .y the kind in its top two bits
+//   node group      .y = imask << 8 | hit bits (bit = slot ^ octant)
+//   primitive group .y = AZD_E_PRIMS | 24-bit mask of untested primitives after .x
+//   BLAS exit       .y = AZD_E_EXIT
+//   BLAS entry      .y = AZD_E_GROUP, .x = group index
+#define AZD_E_EXIT 0xFFFFFFFFu
+#define AZD_E_GROUP 0xFFFFFFFEu
+#define AZD_E_PRIMS 0x40000000u
+
+// 8-bit grid value to float without the conversion pipe: PRMT places the byte
+// in the low mantissa bits of 2^23, and one subtraction removes 2^23 (exact).
+// (Folding the 2^23 into the slab test's FMA constant instead would cost a
+// rounding of |origin offset| + 2^23 grid steps, which exceeds the one-step
+// box margin for thin nodes far from the ray origin.)
+__device__ __forceinline__ float qbyte(uint32_t w, uint32_t k) {
+    return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u | k)) - 8388608.0f;
+}
+
+struct WideHits {
+    uint32_t inner;   // hit inner children, bit = slot ^ octant
+    uint32_t prims;   // hit leaf primitives, bit = offset from prim_base
+};
+
+// Slab test of the 8 quantised child boxes of a wide node.
+__device__ __forceinline__ WideHits wide_test(const uint4 w0, const uint4 w1, const uint4 w2, const uint4 w3,
+                                              const uint4 w4, f3 o, f3 inv, uint32_t oct, float tmax) {
+    const float px = __uint_as_float(w0.x), py = __uint_as_float(w0.y), pz = __uint_as_float(w0.z);
+    const uint32_t ex = w0.w & 0xFFu, ey = (w0.w >> 8) & 0xFFu, ez = (w0.w >> 16) & 0xFFu, imask = w0.w >> 24;
+    const float sx = __uint_as_float(ex << 23) * inv.x, sy = __uint_as_float(ey << 23) * inv.y,
+                sz = __uint_as_float(ez << 23) * inv.z;
+    const float ox = (px - o.x) * inv.x, oy = (py - o.y) * inv.y, oz = (pz - o.z) * inv.z;
+    // near/far planes: swap lo and hi when the direction is negative
+    const bool nx = inv.x < 0.0f, ny = inv.y < 0.0f, nz = inv.z < 0.0f;
+    const uint32_t nx0 = nx ? w3.z : w2.x, nx1 = nx ? w3.w : w2.y, fx0 = nx ? w2.x : w3.z, fx1 = nx ? w2.y : w3.w;
+    const uint32_t ny0 = ny ? w4.x : w2.z, ny1 = ny ? w4.y : w2.w, fy0 = ny ? w2.z : w4.x, fy1 = ny ? w2.w : w4.y;
+    const uint32_t nz0 = nz ? w4.z : w3.x, nz1 = nz ? w4.w : w3.y, fz0 = nz ? w3.x : w4.z, fz1 = nz ? w3.y : w4.w;
+    WideHits h{0u, 0u};
+#pragma unroll
+    for (int s = 0; s < 8; s++) {
+        const uint32_t k = s & 3;
+        const float tnx = __fmaf_rn(qbyte(s < 4 ? nx0 : nx1, k), sx, ox);
+        const float tfx = __fmaf_rn(qbyte(s < 4 ? fx0 : fx1, k), sx, ox);
+        const float tny = __fmaf_rn(qbyte(s < 4 ? ny0 : ny1, k), sy, oy);
+        const float tfy = __fmaf_rn(qbyte(s < 4 ? fy0 : fy1, k), sy, oy);
+        const float tnz = __fmaf_rn(qbyte(s < 4 ? nz0 : nz1, k), sz, oz);
+        const float tfz = __fmaf_rn(qbyte(s < 4 ? fz0 : fz1, k), sz, oz);
+        const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f));
+        const float tf = fminf(fminf(tfx, tfy), fminf(tfz, tmax)) * 1.00000095367431640625f;
+        if (tn <= tf) {
+            if ((imask >> s) & 1u) {
+                h.inner |= 1u << (s ^ oct);
+            } else {
+                const uint32_t meta = ((s < 4 ? w1.z : w1.w) >> (8 * k)) & 0xFFu;
+                h.prims |= ((1u << (meta >> 5)) - 1u) << (meta & 31u);   // empty slot: meta 0, no bits
+            }
+        }
+    }
+    return h;
+}
+
+__device__ __forceinline__ uint32_t octant_of(f3 d) {
+    return (d.x < 0.0f ? 1u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 4u : 0u);
+}
+
+// World t of a triangle hit of group g at local t (azimuth's instance path,
+// src/azimuth_main.cpp:256-262).
+__device__ __forceinline__ float group_world_t(const DevGroup &g, const Ray &wr, const Ray &lr, float t) {
+    if (g.raw) return t;
+    f3 motion = wr.time * mk(g.motion[0], g.motion[1], g.motion[2]);
+    f3 o2 = wr.o - motion;
+    f3 lp = lr.o + (lr.d * t);
+    f3 wp = point_xf(g.xf, lp) + motion;
+    return length(wp - o2 - motion) / length(wr.d);
+}
+
+// Two-level traversal of the 8-wide hierarchy, after the node-group /
+// primitive-group scheme of Ylitie, Karras, Laine, "Efficient Incoherent Ray
+// Traversal on GPUs Through Compressed Wide BVHs" (HPG 2017): each step
+// visits the nearest node of the current group, then tests the primitives its
+// leaves hit, postponing them onto the stack while few lanes of the warp have
+// primitives to test.  For Q_CLOSEST returns the nearest hit in `best`
+// (best.ent == 0xFFFFFFFF: none).  For Q_ANY returns true as soon as a
+// primitive's world t < tmax.  `skip_ent` (optional) is an entity whose
+// primitives are ignored.  `counts` accumulates node and primitive visits.
 template <QueryKind KIND>
 __device__ bool trace(const DevScene &S, const Ray &wr, bool cull, float eps, float tmax, Hit &best,
-                      uint32_t *counts = nullptr, uint32_t *err = nullptr) {
+                      uint32_t *counts = nullptr, uint32_t *err = nullptr, uint32_t skip_ent = 0xFFFFFFFFu) {
     best.t = FLT_MAX;
     best.tl = 0.0f;
     best.prim = 0xFFFFFFFFu;
     best.ent = 0xFFFFFFFFu;
     if (S.tlas_root == 0xFFFFFFFFu) return false;
 
-    uint32_t stack_node[AZD_STACK];
-    float stack_t[AZD_STACK];
+    uint2 stack[AZD_WSTACK];
     int sp = 0;
 
-    // current ray space
-    Ray r = wr;
+    Ray r = wr;                                    // current ray space
     f3 inv = safe_inv(r.d);
-    f3 oinv = had(r.o, inv);
+    uint32_t oct = octant_of(r.d);
     float tcur = KIND == Q_ANY ? tmax : FLT_MAX;   // pruning distance in the current space
     bool in_blas = false;
     uint32_t g_idx = 0;
-    float blas_scale = 1.0f;                        // local t per world t (upper bound)
-    float bl_t = FLT_MAX, bl_b = 0.0f;              // nearest local hit of this BLAS visit
+    float bl_t = FLT_MAX;                          // nearest local hit of this BLAS visit
     uint32_t bl_prim = 0xFFFFFFFFu;
-    uint32_t nodes_visited = 0, prims_visited = 0;
+    uint32_t nodes_visited = 0, prims_visited = 0, steps = 0;
+    bool hit_any = false;
 
-    uint32_t cur = S.tlas_root;  // inner node index or an entry
-    uint32_t steps = 0;
+    // current node group: the root alone (imask bit 0, hit bit 0 ^ oct)
+    uint32_t ng_base = S.tlas_root, ng_bits = (1u << 8) | (1u << oct);
+    uint32_t pg_base = 0, pg_mask = 0;             // current primitive group
+
     while (true) {
         if (++steps > AZD_MAX_STEPS) {
             if (err) atomicOr(err, 1u);
             break;
         }
-        if (cur == AZD_ENT_EXIT) {
-            // leaving a BLAS: azimuth's instance path keeps the nearest local hit
-            // and recomputes its world t (src/azimuth_main.cpp:256-276)
-            const DevGroup &g = S.groups[g_idx];
-            if (bl_prim != 0xFFFFFFFFu) {
-                float wt;
-                if (g.raw) {
-                    wt = bl_t;
-                } else {
-                    f3 motion = wr.time * mk(g.motion[0], g.motion[1], g.motion[2]);
-                    f3 o2 = wr.o - motion;
-                    f3 lp = r.o + (r.d * bl_t);
-                    f3 wp = point_xf(g.xf, lp) + motion;
-                    wt = length(wp - o2 - motion) / length(wr.d);
-                }
-                if (wt > eps && wt < best.t) {
-                    if (KIND == Q_ANY) {
-                        if (wt < tmax) return true;
-                    } else {
-                        best.t = wt;
-                        best.tl = bl_t;
-                        best.prim = bl_prim;
-                        best.ent = S.tri_attr[bl_prim].entity;
-                    }
-                }
+        if (ng_bits & 0xFFu) {
+            // visit the nearest node of the group; the rest of the group waits on the stack
+            const uint32_t hits = ng_bits & 0xFFu, imask = (ng_bits >> 8) & 0xFFu;
+            const uint32_t key = __ffs(hits) - 1u;
+            const uint32_t slot = key ^ oct;
+            const uint32_t node = ng_base + __popc(imask & ((1u << slot) - 1u));
+            ng_bits &= ~(1u << key);
+            if (ng_bits & 0xFFu) {
+                if (sp < AZD_WSTACK) stack[sp++] = make_uint2(ng_base, ng_bits);
+                else if (err) atomicOr(err, 2u);
             }
-            (void)bl_b;
-            r = wr;
-            inv = safe_inv(r.d);
-            oinv = had(r.o, inv);
-            tcur = KIND == Q_ANY ? tmax : best.t;
-            in_blas = false;
-            cur = 0xFFFFFFFEu;  // pop next
-        } else if (cur & AZD_ENT_LEAF) {
-            uint32_t start = cur & 0x07FFFFFFu, count = ((cur >> 27) & 7u) + 1u;
-            cur = 0xFFFFFFFEu;
-            if (in_blas) {
-                for (uint32_t i = 0; i < count; i++) {
-                    uint32_t pi = start + i;
-                    DevTri tr = load_tri(S.tris, pi);
-                    float t, b, gm;
-                    prims_visited++;
-                    if (tri_test(tr, r, cull, eps, bl_t, t, b, gm)) {
-                        bl_t = t;
-                        bl_b = b;
-                        bl_prim = pi;
-                        if (KIND == Q_ANY) {
-                            // early exit as soon as one hit of this group is in range
-                            const DevGroup &g = S.groups[g_idx];
-                            float wt;
-                            if (g.raw) {
-                                wt = t;
-                            } else {
-                                f3 motion = wr.time * mk(g.motion[0], g.motion[1], g.motion[2]);
-                                f3 o2 = wr.o - motion;
-                                f3 lp = r.o + (r.d * t);
-                                f3 wp = point_xf(g.xf, lp) + motion;
-                                wt = length(wp - o2 - motion) / length(wr.d);
-                            }
-                            if (wt > eps && wt < tmax) return true;
-                        } else {
-                            tcur = fminf(tcur, t);
-                        }
-                    }
-                }
-            } else {
-                for (uint32_t i = 0; i < count; i++) {
-                    uint32_t p = __ldg(S.tlas_prims + start + i);
-                    prims_visited++;
-                    if (p & AZD_TLAS_GROUP) {
-                        // enter the group's BLAS (azimuth: GetLocalRay of the
-                        // motion-shifted ray, src/azimuth_main.cpp:246-250)
-                        g_idx = p & ~AZD_TLAS_GROUP;
-                        const DevGroup &g = S.groups[g_idx];
-                        if (g.root == 0xFFFFFFFFu) continue;
-                        if (sp >= AZD_STACK) break;
-                        stack_node[sp] = AZD_ENT_EXIT;
-                        stack_t[sp] = -FLT_MAX;
-                        sp++;
-                        if (g.raw) {
-                            r = wr;
-                            blas_scale = 1.0f;
-                        } else {
-                            Ray m = wr;
-                            m.o = wr.o - wr.time * mk(g.motion[0], g.motion[1], g.motion[2]);
-                            r = local_ray(m, g.inv);
-                            // local t = world t * |inv * d| / |d| (up to rounding)
-                            f3 ld = vector_xf(g.inv, wr.d);
-                            blas_scale = length(ld) / length(wr.d) * 1.0001f;
-                        }
-                        inv = safe_inv(r.d);
-                        oinv = had(r.o, inv);
-                        float wlim = KIND == Q_ANY ? tmax : best.t;
-                        tcur = wlim < FLT_MAX ? wlim * blas_scale + 1e-30f : FLT_MAX;
-                        bl_t = FLT_MAX;
-                        bl_prim = 0xFFFFFFFFu;
-                        in_blas = true;
-                        cur = g.root;
-                        break;  // TLAS leaves hold one primitive
-                    } else {
-                        const DevEntity &e = S.ents[p];
-                        float wt, tl;
-                        if (e.type == ENT_SPHERE && sphere_test(e, wr, eps, wt, tl)) {
-                            if (KIND == Q_ANY) {
-                                if (wt < tmax) return true;
-                            } else if (wt < best.t) {
-                                best.t = wt;
-                                best.tl = tl;
-                                best.prim = 0xFFFFFFFFu;
-                                best.ent = p;
-                                tcur = wt;
-                            }
-                        }
-                    }
-                }
-            }
-        } else if (cur != 0xFFFFFFFEu) {
-            // inner node: test both children, continue with the nearer one
-            BVHNode n = load_node(S.nodes, cur);
+            const uint4 *np = reinterpret_cast<const uint4 *>(S.wnodes + node);
+            const uint4 w0 = __ldg(np + 0), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3),
+                        w4 = __ldg(np + 4);
             nodes_visited++;
-            float t0, t1;
-            uint32_t mask = node_test(n, oinv, inv, 0.0f, tcur, t0, t1);
-            uint32_t e0 = n.ch.z ? leaf_entry(n.ch.x, n.ch.z) : n.ch.x;
-            uint32_t e1 = n.ch.w ? leaf_entry(n.ch.y, n.ch.w) : n.ch.y;
-            if (mask == 3u) {
-                uint32_t nearE = e0, farE = e1;
-                float farT = t1;
-                if (t1 < t0) { nearE = e1; farE = e0; farT = t0; }
-                if (sp < AZD_STACK) {
-                    stack_node[sp] = farE;
-                    stack_t[sp] = farT;
-                    sp++;
+            const WideHits h = wide_test(w0, w1, w2, w3, w4, r.o, inv, oct, tcur);
+            ng_base = w1.x;
+            ng_bits = h.inner | ((w0.w >> 24) << 8);
+            if (h.prims) {
+                if (pg_mask) {   // still holding primitives: keep them for later
+                    if (sp < AZD_WSTACK) stack[sp++] = make_uint2(pg_base, AZD_E_PRIMS | pg_mask);
+                    else if (err) atomicOr(err, 2u);
                 }
-                cur = nearE;
-            } else if (mask == 1u) {
-                cur = e0;
-            } else if (mask == 2u) {
-                cur = e1;
-            } else {
-                cur = 0xFFFFFFFEu;
+                pg_base = w1.y;
+                pg_mask = h.prims;
             }
         }
-        if (cur == 0xFFFFFFFEu) {
-            // pop, skipping entries beyond the current pruning distance
-            bool found = false;
-            while (sp > 0) {
-                sp--;
-                uint32_t e = stack_node[sp];
-                if (e == AZD_ENT_EXIT || !(stack_t[sp] > tcur)) {
-                    cur = e;
-                    found = true;
-                    break;
+        // primitives, postponed while few lanes of the warp have any
+        while (pg_mask) {
+            if (__popc(__activemask()) < 6u && (ng_bits & 0xFFu) && sp < AZD_WSTACK) {
+                stack[sp++] = make_uint2(pg_base, AZD_E_PRIMS | pg_mask);
+                pg_mask = 0;
+                break;
+            }
+            const uint32_t bit = __ffs(pg_mask) - 1u;
+            pg_mask &= pg_mask - 1u;
+            const uint32_t pi = pg_base + bit;
+            prims_visited++;
+            if (in_blas) {
+                if (skip_ent != 0xFFFFFFFFu && __ldg(&S.tri_attr[pi].entity) == skip_ent) continue;
+                DevTri tr = load_tri(S.tris, pi);
+                float t, b, gm;
+                if (tri_test(tr, r, cull, eps, bl_t, t, b, gm)) {
+                    bl_t = t;
+                    bl_prim = pi;
+                    if (KIND == Q_ANY) {
+                        // exit as soon as one hit of this group is in range
+                        float wt = group_world_t(S.groups[g_idx], wr, r, t);
+                        if (wt > eps && wt < tmax) {
+                            hit_any = true;
+                            break;
+                        }
+                    } else {
+                        tcur = fminf(tcur, t);
+                    }
+                }
+            } else {
+                const uint32_t p = __ldg(S.tlas_prims + pi);
+                if (p & AZD_TLAS_GROUP) {
+                    // entered when popped; leave room for its exit marker
+                    if (sp + 1 < AZD_WSTACK) stack[sp++] = make_uint2(p & ~AZD_TLAS_GROUP, AZD_E_GROUP);
+                    else if (err) atomicOr(err, 2u);
+                } else if (p != skip_ent) {
+                    const DevEntity &e = S.ents[p];
+                    float wt, tl;
+                    if (e.type == ENT_SPHERE && sphere_test(e, wr, eps, wt, tl)) {
+                        if (KIND == Q_ANY) {
+                            if (wt < tmax) {
+                                hit_any = true;
+                                break;
+                            }
+                        } else if (wt < best.t) {
+                            best.t = wt;
+                            best.tl = tl;
+                            best.prim = 0xFFFFFFFFu;
+                            best.ent = p;
+                            tcur = wt;
+                        }
+                    }
                 }
             }
-            if (!found) break;
+        }
+        if (KIND == Q_ANY && hit_any) break;
+        if ((ng_bits & 0xFFu) || pg_mask) continue;
+        // nothing left in the current groups: pop
+        if (sp == 0) break;
+        const uint2 e = stack[--sp];
+        if (e.y == AZD_E_EXIT) {
+            // leaving a BLAS: azimuth's instance path keeps the nearest local hit
+            // and recomputes its world t (src/azimuth_main.cpp:256-276)
+            if (KIND == Q_CLOSEST && bl_prim != 0xFFFFFFFFu) {
+                float wt = group_world_t(S.groups[g_idx], wr, r, bl_t);
+                if (wt > eps && wt < best.t) {
+                    best.t = wt;
+                    best.tl = bl_t;
+                    best.prim = bl_prim;
+                    best.ent = S.tri_attr[bl_prim].entity;
+                }
+            }
+            r = wr;
+            inv = safe_inv(r.d);
+            oct = octant_of(r.d);
+            tcur = KIND == Q_ANY ? tmax : best.t;
+            in_blas = false;
+        } else if (e.y == AZD_E_GROUP) {
+            // enter the group's BLAS (azimuth: GetLocalRay of the motion-shifted
+            // ray, src/azimuth_main.cpp:246-250)
+            g_idx = e.x;
+            const DevGroup &g = S.groups[g_idx];
+            if (g.root == 0xFFFFFFFFu) continue;
+            stack[sp++] = make_uint2(0u, AZD_E_EXIT);   // room was kept when the entry was pushed
+            float blas_scale = 1.0f;
+            if (g.raw) {
+                r = wr;
+            } else {
+                Ray m = wr;
+                m.o = wr.o - wr.time * mk(g.motion[0], g.motion[1], g.motion[2]);
+                r = local_ray(m, g.inv);
+                // local t = world t * |inv * d| / |d| (up to rounding)
+                blas_scale = length(vector_xf(g.inv, wr.d)) / length(wr.d) * 1.0001f;
+            }
+            inv = safe_inv(r.d);
+            oct = octant_of(r.d);
+            float wlim = KIND == Q_ANY ? tmax : best.t;
+            tcur = wlim < FLT_MAX ? wlim * blas_scale + 1e-30f : FLT_MAX;
+            bl_t = FLT_MAX;
+            bl_prim = 0xFFFFFFFFu;
+            in_blas = true;
+            ng_base = g.root;
+            ng_bits = (1u << 8) | (1u << oct);
+        } else if ((e.y & 0xC0000000u) == AZD_E_PRIMS) {
+            pg_base = e.x;
+            pg_mask = e.y & 0x00FFFFFFu;
+        } else {
+            ng_base = e.x;
+            ng_bits = e.y;
         }
     }
     if (counts) {
         atomicAdd(counts + 0, nodes_visited);
         atomicAdd(counts + 1, prims_visited);
     }
-    if (KIND == Q_ANY) return false;
+    if (KIND == Q_ANY) return hit_any;
     return best.ent != 0xFFFFFFFFu;
 }
 

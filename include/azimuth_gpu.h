@@ -55,8 +55,11 @@ typedef struct az_render_opts {
     uint32_t flags;                 /* AZ_FLAG_* */
     uint32_t chunk_samples;         /* camera samples in flight per wave; 0 = automatic */
     uint32_t bvh_width;             /* 0 or 2 (binary BVH) */
-    uint32_t block_size;            /* threads per block for the wavefront kernels; 0 = automatic */
-    uint32_t reserved[5];
+    uint32_t block_size;            /* reserved (0) */
+    uint32_t variant;               /* traversal launch configuration 1..7 (threads per block and register
+                                       cap); 0 = the scene's choice: 3 (128 threads, at most 64 registers)
+                                       until az_gpu_autotune picks another */
+    uint32_t reserved[4];
 } az_render_opts;
 
 typedef struct az_render_stats {
@@ -104,6 +107,14 @@ int az_gpu_render(az_gpu_scene *scene, az_pixel *film, const az_camera *camera,
 int az_gpu_render_host(az_gpu_scene *scene, az_pixel *pixels, const az_camera *camera,
                        const az_epsilon_values *epsilons, az_scissor scissor, int32_t filter_type,
                        uint32_t backface_culling, const az_render_opts *opts, az_render_stats *stats);
+
+/* Autotuner: renders a band of the frame (the middle eighth of the scissor's
+ * rows, every sample) with each traversal launch configuration and keeps the
+ * fastest as the scene's default.  Writes the chosen variant (1-based) and its
+ * time in ms.  Synchronous. */
+int az_gpu_autotune(az_gpu_scene *scene, const az_camera *camera, const az_epsilon_values *epsilons,
+                    az_scissor scissor, int32_t filter_type, uint32_t backface_culling,
+                    const az_render_opts *opts, uint32_t *variant_out, float *ms_out);
 
 /* Allocation-free variant of az_gpu_render; it has no counterpart in azimuth.
  *

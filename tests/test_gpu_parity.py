@@ -87,3 +87,18 @@ def test_seed_changes_the_image(gpu):
     assert not np.array_equal(a, b)
     assert np.array_equal(a, az.produce_image(scene, seed=1)) or ol.film_compare(
         a, az.produce_image(scene, seed=1), 1e-6)[0] > 0.999
+
+
+def test_autotune_picks_a_variant_and_renders_the_same(gpu):
+    import torch
+    scene = az.generate_scene(az.SCENE_DENSE_MESH, seed=1, width=64, height=64, spp=4, detail=4)
+    w, h = scene.resolution()
+    with az.GpuScene(scene) as g:
+        a = torch.zeros((h, w, 4), device="cuda")
+        g.render_device(a.data_ptr(), seed=3, stats=True)
+        v, ms = g.autotune(seed=3)
+        assert 1 <= v <= 7 and ms > 0
+        b = torch.zeros((h, w, 4), device="cuda")
+        g.render_device(b.data_ptr(), seed=3, stats=True)
+        # launch configuration changes scheduling only: same samples, same sums up to atomic order
+        assert ol.film_compare(b.cpu().numpy(), a.cpu().numpy(), 1e-4)[0] == 1.0
