@@ -1,7 +1,8 @@
 // GPU LBVH construction (Karras, "Maximizing Parallelism in the Construction
-// of BVHs, Octrees, and k-d Trees", HPG 2012): 30-bit Morton codes of the box
-// centroids with the primitive index as tie-break, a radix sort, one thread
-// per internal node to find its range and split, and a bottom-up pass that
+// of BVHs, Octrees, and k-d Trees", HPG 2012): 63-bit Morton codes (21 bits per
+// axis) of the box centroids, a radix sort of (code, primitive) pairs, one
+// thread per internal node to find its range and split (equal codes are told
+// apart by their sorted position, as in the paper), and a bottom-up pass that
 // fills each node with the (slightly enlarged) boxes of both children.
 #include <cub/cub.cuh>
 
@@ -12,11 +13,14 @@
 namespace az {
 namespace {
 
-__device__ __forceinline__ uint32_t expand_bits(uint32_t v) {
-    v = (v * 0x00010001u) & 0xFF0000FFu;
-    v = (v * 0x00000101u) & 0x0F00F00Fu;
-    v = (v * 0x00000011u) & 0xC30C30C3u;
-    v = (v * 0x00000005u) & 0x49249249u;
+// 21 bits spread to every third bit of a 63-bit word.
+__device__ __forceinline__ unsigned long long spread3(unsigned long long v) {
+    v &= 0x1FFFFFull;
+    v = (v | (v << 32)) & 0x001F00000000FFFFull;
+    v = (v | (v << 16)) & 0x001F0000FF0000FFull;
+    v = (v | (v << 8)) & 0x100F00F00F00F00Full;
+    v = (v | (v << 4)) & 0x10C30C30C30C30C3ull;
+    v = (v | (v << 2)) & 0x1249249249249249ull;
     return v;
 }
 
@@ -49,25 +53,29 @@ __global__ void k_bounds_reduce(const float4 *lo, const float4 *hi, uint32_t n, 
 }
 
 __global__ void k_morton(const float4 *lo, const float4 *hi, uint32_t n, const float *bounds6,
-                         unsigned long long *keys) {
+                         unsigned long long *keys, uint32_t *vals) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float4 a = lo[i], b = hi[i];
-    float c[3] = {0.5f * (a.x + b.x), 0.5f * (a.y + b.y), 0.5f * (a.z + b.z)};
-    uint32_t q[3];
+    double c[3] = {0.5 * ((double)a.x + b.x), 0.5 * ((double)a.y + b.y), 0.5 * ((double)a.z + b.z)};
+    unsigned long long q[3];
     for (int k = 0; k < 3; k++) {
-        float ext = bounds6[3 + k] - bounds6[k];
-        float u = ext > 0.0f ? (c[k] - bounds6[k]) / ext : 0.5f;
-        u = fminf(fmaxf(u, 0.0f), 1.0f);
-        q[k] = min((uint32_t)(u * 1024.0f), 1023u);
+        double ext = (double)bounds6[3 + k] - bounds6[k];
+        double u = ext > 0.0 ? (c[k] - bounds6[k]) / ext : 0.5;
+        u = fmin(fmax(u, 0.0), 1.0);
+        q[k] = (unsigned long long)fmin(u * 2097152.0, 2097151.0);
     }
-    uint32_t m = (expand_bits(q[0]) << 2) | (expand_bits(q[1]) << 1) | expand_bits(q[2]);
-    keys[i] = ((unsigned long long)m << 32) | i;
+    keys[i] = (spread3(q[0]) << 2) | (spread3(q[1]) << 1) | spread3(q[2]);
+    vals[i] = i;
 }
 
+// Common-prefix length of sorted keys i and j; equal keys continue with the
+// bits of their positions (Karras 2012, section 4).
 __device__ __forceinline__ int delta(const unsigned long long *k, int n, int i, int j) {
     if (j < 0 || j >= n) return -1;
-    return __clzll(k[i] ^ k[j]);
+    unsigned long long a = k[i], b = k[j];
+    if (a == b) return 64 + __clz((uint32_t)(i ^ j));
+    return __clzll(a ^ b);
 }
 
 // One thread per internal node i in [0, n-2]: children (internal index or
@@ -124,7 +132,7 @@ __device__ __forceinline__ void pad_box(float4 &lo, float4 &hi) {
 
 // Bottom-up: one thread per leaf walks to the root; the second child to
 // arrive at a node writes it.
-__global__ void k_fill(const unsigned long long *keys, const float4 *plo, const float4 *phi, int n,
+__global__ void k_fill(const uint32_t *order, const float4 *plo, const float4 *phi, int n,
                        const uint32_t *left, const uint32_t *right, const int *parent_int, const int *parent_leaf,
                        float4 *ilo, float4 *ihi, unsigned int *visits, azd::BVHNode *nodes, uint32_t node_base,
                        uint32_t leaf_base) {
@@ -141,7 +149,7 @@ __global__ void k_fill(const unsigned long long *keys, const float4 *plo, const 
         for (int s = 0; s < 2; s++) {
             if (c[s] & 0x80000000u) {
                 uint32_t li = c[s] & 0x7FFFFFFFu;
-                uint32_t prim = (uint32_t)(keys[li] & 0xFFFFFFFFull);
+                uint32_t prim = order[li];
                 blo[s] = plo[prim];
                 bhi[s] = phi[prim];
                 ref[s] = leaf_base + li;
@@ -169,9 +177,9 @@ __global__ void k_fill(const unsigned long long *keys, const float4 *plo, const 
     }
 }
 
-__global__ void k_extract_perm(const unsigned long long *keys, uint32_t n, uint32_t *perm) {
+__global__ void k_copy_u32(const uint32_t *src, uint32_t n, uint32_t *dst) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) perm[i] = (uint32_t)(keys[i] & 0xFFFFFFFFull);
+    if (i < n) dst[i] = src[i];
 }
 
 __global__ void k_single(const float4 *lo, const float4 *hi, azd::BVHNode *nodes, uint32_t node_base,
@@ -213,6 +221,7 @@ int BuildLBVH(const float4 *d_lo, const float4 *d_hi, uint32_t n, azd::BVHNode *
     }
     Scratch<float> bounds;
     Scratch<unsigned long long> keys, keys_sorted;
+    Scratch<uint32_t> vals, vals_sorted;
     Scratch<uint32_t> left, right;
     Scratch<int> parent_int, parent_leaf;
     Scratch<float4> ilo, ihi;
@@ -221,6 +230,8 @@ int BuildLBVH(const float4 *d_lo, const float4 *d_hi, uint32_t n, azd::BVHNode *
     AZ_CUDA_TRY(bounds.alloc(6));
     AZ_CUDA_TRY(keys.alloc(n));
     AZ_CUDA_TRY(keys_sorted.alloc(n));
+    AZ_CUDA_TRY(vals.alloc(n));
+    AZ_CUDA_TRY(vals_sorted.alloc(n));
     AZ_CUDA_TRY(left.alloc(n));
     AZ_CUDA_TRY(right.alloc(n));
     AZ_CUDA_TRY(parent_int.alloc(n));
@@ -229,20 +240,22 @@ int BuildLBVH(const float4 *d_lo, const float4 *d_hi, uint32_t n, azd::BVHNode *
     AZ_CUDA_TRY(ihi.alloc(n));
     AZ_CUDA_TRY(visits.alloc(n));
     size_t temp_bytes = 0;
-    AZ_CUDA_TRY(cub::DeviceRadixSort::SortKeys(nullptr, temp_bytes, keys.p, keys_sorted.p, (int)n, 0, 62, stream));
+    AZ_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, keys.p, keys_sorted.p, vals.p, vals_sorted.p,
+                                                (int)n, 0, 63, stream));
     AZ_CUDA_TRY(temp.alloc(temp_bytes));
     const int B = 256;
     uint32_t grid = (n + B - 1) / B;
     k_bounds_reduce<<<1, 256, 0, stream>>>(d_lo, d_hi, n, bounds.p);
-    k_morton<<<grid, B, 0, stream>>>(d_lo, d_hi, n, bounds.p, keys.p);
+    k_morton<<<grid, B, 0, stream>>>(d_lo, d_hi, n, bounds.p, keys.p, vals.p);
     AZ_CUDA_TRY(cudaGetLastError());
-    AZ_CUDA_TRY(cub::DeviceRadixSort::SortKeys(temp.p, temp_bytes, keys.p, keys_sorted.p, (int)n, 0, 62, stream));
+    AZ_CUDA_TRY(cub::DeviceRadixSort::SortPairs(temp.p, temp_bytes, keys.p, keys_sorted.p, vals.p, vals_sorted.p,
+                                                (int)n, 0, 63, stream));
     AZ_CUDA_TRY(cudaMemsetAsync(parent_int.p, 0xFF, n * sizeof(int), stream));   // root's parent = -1
     AZ_CUDA_TRY(cudaMemsetAsync(visits.p, 0, n * sizeof(unsigned int), stream));
     k_karras<<<grid, B, 0, stream>>>(keys_sorted.p, (int)n, left.p, right.p, parent_int.p, parent_leaf.p);
-    k_fill<<<grid, B, 0, stream>>>(keys_sorted.p, d_lo, d_hi, (int)n, left.p, right.p, parent_int.p, parent_leaf.p,
+    k_fill<<<grid, B, 0, stream>>>(vals_sorted.p, d_lo, d_hi, (int)n, left.p, right.p, parent_int.p, parent_leaf.p,
                                    ilo.p, ihi.p, visits.p, d_nodes, node_base, leaf_base);
-    k_extract_perm<<<grid, B, 0, stream>>>(keys_sorted.p, n, d_perm);
+    k_copy_u32<<<grid, B, 0, stream>>>(vals_sorted.p, n, d_perm);
     AZ_CUDA_TRY(cudaGetLastError());
     // scratch is freed when this returns: finish the work that uses it
     AZ_CUDA_TRY(cudaStreamSynchronize(stream));

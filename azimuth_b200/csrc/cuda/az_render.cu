@@ -128,20 +128,90 @@ __global__ void k_camera(CameraParams cam, WaveQueues Q, uint64_t wave_start, ui
     Q.accum[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 }
 
-template <int BLOCK, int MINB>
+// Persistent traversal kernels.  Each warp reserves rays of the level's queue
+// in batches; a lane whose query has finished takes the next reserved ray at
+// its next step, so no lane idles until its warp's slowest ray is done.
+constexpr uint32_t kFetchBatch = 64;
+constexpr uint32_t kLaneIdle = 0xFFFFFFFFu, kLaneDone = 0xFFFFFFFEu;
+
+struct WarpFetch {
+    uint32_t next = 0, end = 0;
+    bool exhausted = false;
+
+    // Hands the idle lanes of the warp new indices below n (kLaneDone when the
+    // queue is exhausted).  Called by all 32 lanes.
+    __device__ __forceinline__ bool refill(uint32_t *counter, uint32_t n, uint32_t &idx) {
+        const uint32_t lane = threadIdx.x & 31u;
+        const uint32_t idle = __ballot_sync(0xFFFFFFFFu, idx == kLaneIdle);
+        if (!idle) return false;
+        if (next >= end && !exhausted) {
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(counter, kFetchBatch);
+            base = __shfl_sync(0xFFFFFFFFu, base, 0);
+            if (base >= n) {
+                exhausted = true;
+            } else {
+                next = base;
+                end = min(base + kFetchBatch, n);
+            }
+        }
+        const uint32_t avail = end - next;
+        bool got = false;
+        if (idx == kLaneIdle) {
+            const uint32_t rank = __popc(idle & ((1u << lane) - 1u));
+            if (rank < avail) {
+                idx = next + rank;
+                got = true;
+            } else if (exhausted) {
+                idx = kLaneDone;
+            }
+        }
+        next += min(avail, (uint32_t)__popc(idle));
+        return got;
+    }
+};
+
+template <int BLOCK, int MINB, bool PERSIST>
 __global__ void __launch_bounds__(BLOCK, MINB) k_extend(DevScene S, CameraParams cam, WaveQueues Q, uint32_t level) {
     const int buf = level & 1;
     const uint32_t n = min(Q.counts[level], Q.cap_q);
     uint32_t *cnt = cam.count_traversal ? Q.counts + AZ_COUNT_NODES : nullptr;
-    for (uint32_t i = blockIdx.x * BLOCK + threadIdx.x; i < n; i += gridDim.x * BLOCK) {
-        float4 o = Q.o[buf][i], d = Q.d[buf][i];
-        Ray r;
-        r.o = mk(o.x, o.y, o.z);
-        r.d = mk(d.x, d.y, d.z);
-        r.time = o.w;
-        Hit h;
-        trace<Q_CLOSEST>(S, r, cam.cull != 0, cam.eps_isect, FLT_MAX, h, cnt, Q.counts + AZ_COUNT_ERROR);
-        Q.hit[i] = make_uint4(__float_as_uint(h.t), __float_as_uint(h.tl), h.prim, h.ent);
+    uint32_t *err = Q.counts + AZ_COUNT_ERROR;
+    if (!PERSIST) {
+        // one query per thread at a time, grid-stride over the queue
+        for (uint32_t i = blockIdx.x * BLOCK + threadIdx.x; i < n; i += gridDim.x * BLOCK) {
+            const float4 o = Q.o[buf][i], d = Q.d[buf][i];
+            Ray r;
+            r.o = mk(o.x, o.y, o.z);
+            r.d = mk(d.x, d.y, d.z);
+            r.time = o.w;
+            Hit h;
+            trace<Q_CLOSEST>(S, r, cam.cull != 0, cam.eps_isect, FLT_MAX, h, cnt, err);
+            Q.hit[i] = make_uint4(__float_as_uint(h.t), __float_as_uint(h.tl), h.prim, h.ent);
+        }
+        return;
+    }
+    uint32_t *fetch = Q.counts + AZ_COUNT_FETCH + level;
+    Tracer<Q_CLOSEST> T;
+    uint2 stack[AZD_WSTACK];
+    WarpFetch wf;
+    uint32_t idx = kLaneIdle;
+    while (true) {
+        if (wf.refill(fetch, n, idx)) {
+            const float4 o = Q.o[buf][idx], d = Q.d[buf][idx];
+            Ray r;
+            r.o = mk(o.x, o.y, o.z);
+            r.d = mk(d.x, d.y, d.z);
+            r.time = o.w;
+            T.init(S, r, cam.cull != 0, cam.eps_isect, FLT_MAX);
+        }
+        if (__all_sync(0xFFFFFFFFu, idx == kLaneDone)) break;
+        if (idx < n && T.step(S, stack, err)) {
+            const Hit &h = T.best;
+            Q.hit[idx] = make_uint4(__float_as_uint(h.t), __float_as_uint(h.tl), h.prim, h.ent);
+            T.flush_counts(cnt);
+            idx = kLaneIdle;
+        }
     }
 }
 
@@ -391,39 +461,82 @@ __global__ void __launch_bounds__(BLOCK) k_shade(DevScene S, CameraParams cam, W
     }
 }
 
-// Visibility of the queued light samples; unoccluded ones are added to their sample.
-template <int BLOCK, int MINB>
+// Visibility of the queued light samples; unoccluded ones are added to their
+// sample.  Entity lights: occluded unless the nearest hit is the light's
+// entity, so the light's own nearest hit is found exactly first and the query
+// looks for anything else before it.
+template <int BLOCK, int MINB, bool PERSIST>
 __global__ void __launch_bounds__(BLOCK, MINB) k_shadow(DevScene S, CameraParams cam, WaveQueues Q, uint32_t level) {
     const uint32_t n = min(Q.counts[AZ_COUNT_SHADOW + level], Q.cap_s);
     uint32_t *cnt = cam.count_traversal ? Q.counts + AZ_COUNT_NODES : nullptr;
-    for (uint32_t i = blockIdx.x * BLOCK + threadIdx.x; i < n; i += gridDim.x * BLOCK) {
-        float4 o = Q.so[i], d = Q.sd[i], c = Q.sc[i];
-        uint32_t meta = Q.smeta[i];
-        uint32_t kind = meta >> 30, uid = meta & 0x3FFFFFFFu;
-        Ray r;
-        r.o = mk(o.x, o.y, o.z);
-        r.d = mk(d.x, d.y, d.z);
-        r.time = o.w;
-        Hit h;
-        bool visible;
-        if (kind == SHADOW_ENTITY) {
-            // occluded unless the nearest hit is the light's entity: find the
-            // light's own nearest hit exactly, then look for anything else before it
-            const DevLight &L = S.lights[uid];
-            float tl;
-            int lh = light_entity_hit(S, L, r, tl);
-            if (lh < 0) {
-                bool any = trace<Q_CLOSEST>(S, r, false, 0.0f, FLT_MAX, h, cnt, Q.counts + AZ_COUNT_ERROR);
-                visible = !any || S.ents[h.ent].uid == L.uid;
+    uint32_t *err = Q.counts + AZ_COUNT_ERROR;
+    if (!PERSIST) {
+        for (uint32_t i = blockIdx.x * BLOCK + threadIdx.x; i < n; i += gridDim.x * BLOCK) {
+            const float4 o = Q.so[i], d = Q.sd[i], c = Q.sc[i];
+            const uint32_t meta = Q.smeta[i];
+            const uint32_t kind = meta >> 30, li = meta & 0x3FFFFFFFu;
+            Ray r;
+            r.o = mk(o.x, o.y, o.z);
+            r.d = mk(d.x, d.y, d.z);
+            r.time = o.w;
+            Hit h;
+            bool visible;
+            if (kind == SHADOW_ENTITY) {
+                const DevLight &L = S.lights[li];
+                float tl = FLT_MAX;
+                const int lh = light_entity_hit(S, L, r, tl);
+                if (lh < 0) {
+                    bool any = trace<Q_CLOSEST>(S, r, false, 0.0f, FLT_MAX, h, cnt, err);
+                    visible = !any || S.ents[h.ent].uid == L.uid;
+                } else {
+                    visible = !trace<Q_ANY>(S, r, false, 0.0f, lh ? tl : FLT_MAX, h, cnt, err, L.ent_index);
+                }
             } else {
-                visible = !trace<Q_ANY>(S, r, false, 0.0f, lh ? tl : FLT_MAX, h, cnt, Q.counts + AZ_COUNT_ERROR,
-                                        L.ent_index);
+                visible = !trace<Q_ANY>(S, r, false, 0.0f, kind == SHADOW_ANY ? FLT_MAX : d.w, h, cnt, err);
             }
-        } else {
-            visible = !trace<Q_ANY>(S, r, false, 0.0f, kind == SHADOW_ANY ? FLT_MAX : d.w, h, cnt,
-                                    Q.counts + AZ_COUNT_ERROR);
+            if (visible) add_accum(Q.accum, __float_as_uint(c.w), mk(c.x, c.y, c.z));
         }
-        if (visible) add_accum(Q.accum, __float_as_uint(c.w), mk(c.x, c.y, c.z));
+        return;
+    }
+    uint32_t *fetch = Q.counts + AZ_COUNT_FETCH + AZ_MAX_LEVELS + level;
+    Tracer<Q_ANY> T;
+    uint2 stack[AZD_WSTACK];
+    WarpFetch wf;
+    uint32_t idx = kLaneIdle;
+    float4 c = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    while (true) {
+        if (wf.refill(fetch, n, idx)) {
+            const float4 o = Q.so[idx], d = Q.sd[idx];
+            c = Q.sc[idx];
+            const uint32_t meta = Q.smeta[idx];
+            const uint32_t kind = meta >> 30, li = meta & 0x3FFFFFFFu;
+            Ray r;
+            r.o = mk(o.x, o.y, o.z);
+            r.d = mk(d.x, d.y, d.z);
+            r.time = o.w;
+            if (kind == SHADOW_ENTITY) {
+                const DevLight &L = S.lights[li];
+                float tl = FLT_MAX;
+                const int lh = light_entity_hit(S, L, r, tl);
+                if (lh < 0) {
+                    // a light too large to test alone: one full nearest-hit query
+                    Hit h;
+                    bool any = trace<Q_CLOSEST>(S, r, false, 0.0f, FLT_MAX, h, cnt, err);
+                    if (!any || S.ents[h.ent].uid == L.uid) add_accum(Q.accum, __float_as_uint(c.w), mk(c.x, c.y, c.z));
+                    idx = kLaneIdle;
+                } else {
+                    T.init(S, r, false, 0.0f, lh ? tl : FLT_MAX, L.ent_index);
+                }
+            } else {
+                T.init(S, r, false, 0.0f, kind == SHADOW_ANY ? FLT_MAX : d.w);
+            }
+        }
+        if (__all_sync(0xFFFFFFFFu, idx == kLaneDone)) break;
+        if (idx < n && T.step(S, stack, err)) {
+            if (!T.hit_any) add_accum(Q.accum, __float_as_uint(c.w), mk(c.x, c.y, c.z));
+            T.flush_counts(cnt);
+            idx = kLaneIdle;
+        }
     }
 }
 
@@ -456,13 +569,18 @@ __global__ void k_splat(CameraParams cam, WaveQueues Q, uint64_t wave_start, uin
 
 constexpr int kBlock = 128;
 
-// Launch configurations of the two traversal kernels (threads per block,
-// minimum resident blocks per SM, which caps registers); chosen per scene by
+// Launch configurations of the two traversal kernels: threads per block,
+// minimum resident blocks per SM (which caps registers), and whether warps
+// fetch rays persistently (a lane takes a new ray as soon as its query ends)
+// or one query per thread in a grid-stride loop; chosen per scene by
 // az_gpu_autotune.
 struct Variant {
     int block, minb;
+    bool persist;
 };
-constexpr Variant kVariants[] = {{128, 1}, {128, 6}, {128, 8}, {256, 1}, {256, 3}, {64, 1}, {64, 12}};
+constexpr Variant kVariants[] = {{128, 1, false}, {128, 6, false}, {128, 8, false}, {256, 1, false},
+                                 {256, 3, false}, {64, 1, false},  {64, 12, false}, {128, 8, true},
+                                 {128, 6, true},  {256, 3, true}};
 constexpr uint32_t kVariantCount = sizeof(kVariants) / sizeof(kVariants[0]);
 
 template <uint32_t F>
@@ -493,24 +611,27 @@ void LaunchShade(int grid, const DevScene &S, const CameraParams &cam, const Wav
     }
 }
 
-template <int B, int M>
+template <int B, int M, bool P>
 void LaunchTraversal(bool shadow, int sms, const DevScene &S, const CameraParams &cam, const WaveQueues &Q,
                      uint32_t L, cudaStream_t st) {
     const int grid = sms * (2048 / B);
-    if (shadow) k_shadow<B, M><<<grid, B, 0, st>>>(S, cam, Q, L);
-    else k_extend<B, M><<<grid, B, 0, st>>>(S, cam, Q, L);
+    if (shadow) k_shadow<B, M, P><<<grid, B, 0, st>>>(S, cam, Q, L);
+    else k_extend<B, M, P><<<grid, B, 0, st>>>(S, cam, Q, L);
 }
 
 void LaunchTraversalVariant(uint32_t v, bool shadow, int sms, const DevScene &S, const CameraParams &cam,
                             const WaveQueues &Q, uint32_t L, cudaStream_t st) {
     switch (v) {
-        case 1: LaunchTraversal<128, 6>(shadow, sms, S, cam, Q, L, st); break;
-        case 2: LaunchTraversal<128, 8>(shadow, sms, S, cam, Q, L, st); break;
-        case 3: LaunchTraversal<256, 1>(shadow, sms, S, cam, Q, L, st); break;
-        case 4: LaunchTraversal<256, 3>(shadow, sms, S, cam, Q, L, st); break;
-        case 5: LaunchTraversal<64, 1>(shadow, sms, S, cam, Q, L, st); break;
-        case 6: LaunchTraversal<64, 12>(shadow, sms, S, cam, Q, L, st); break;
-        default: LaunchTraversal<128, 1>(shadow, sms, S, cam, Q, L, st); break;
+        case 0: LaunchTraversal<128, 1, false>(shadow, sms, S, cam, Q, L, st); break;
+        case 1: LaunchTraversal<128, 6, false>(shadow, sms, S, cam, Q, L, st); break;
+        case 3: LaunchTraversal<256, 1, false>(shadow, sms, S, cam, Q, L, st); break;
+        case 4: LaunchTraversal<256, 3, false>(shadow, sms, S, cam, Q, L, st); break;
+        case 5: LaunchTraversal<64, 1, false>(shadow, sms, S, cam, Q, L, st); break;
+        case 6: LaunchTraversal<64, 12, false>(shadow, sms, S, cam, Q, L, st); break;
+        case 7: LaunchTraversal<128, 8, true>(shadow, sms, S, cam, Q, L, st); break;
+        case 8: LaunchTraversal<128, 6, true>(shadow, sms, S, cam, Q, L, st); break;
+        case 9: LaunchTraversal<256, 3, true>(shadow, sms, S, cam, Q, L, st); break;
+        default: LaunchTraversal<128, 8, false>(shadow, sms, S, cam, Q, L, st); break;
     }
 }
 
@@ -772,7 +893,10 @@ int Autotune(GpuScene &G, const az_camera *camera, const az_epsilon_values *eps,
     CameraParams cam;
     int rc = SetupCamera(camera, sc, filter, cull, eps, opts ? opts->seed : 0, cam);
     if (rc != AZ_OK) return rc;
-    uint32_t rows = std::max<uint32_t>(1, cam.hsc / 8);
+    // at least ~2^20 samples so that the timing is not dominated by launch overhead
+    const uint64_t per_row = (uint64_t)cam.wsc * cam.sqrt_spp * cam.sqrt_spp;
+    uint32_t rows = std::max<uint32_t>(cam.hsc / 8, (uint32_t)std::min<uint64_t>(cam.hsc, (1u << 20) / std::max<uint64_t>(per_row, 1) + 1));
+    rows = std::max<uint32_t>(1, std::min(rows, cam.hsc));
     az_scissor band = sc;
     band.Min.y = cam.r0 + (cam.hsc - rows) / 2;
     band.Max.y = band.Min.y + rows;
@@ -790,10 +914,13 @@ int Autotune(GpuScene &G, const az_camera *camera, const az_epsilon_values *eps,
         o.variant = v + 1;
         o.flags &= ~(uint32_t)AZ_FLAG_TIME_STAGES;
         az_render_stats stats;
-        for (int rep = 0; rep < 2 && rc == AZ_OK; rep++)   // the first run warms caches and allocates queues
+        float vms = FLT_MAX;
+        for (int rep = 0; rep < 3 && rc == AZ_OK; rep++) {   // the first run warms caches and allocates queues
             rc = Render(G, film, camera, eps, band, filter, cull, &o, st, &stats);
-        if (rc == AZ_OK && stats.gpu_ms < best_ms) {
-            best_ms = stats.gpu_ms;
+            if (rep > 0) vms = std::min(vms, stats.gpu_ms);
+        }
+        if (rc == AZ_OK && vms < best_ms) {
+            best_ms = vms;
             best = v;
         }
     }
@@ -870,7 +997,7 @@ constexpr size_t Align256(size_t x) { return (x + 255) & ~(size_t)255; }
 constexpr size_t kQ16 = Align256((size_t)kStaticCapQ * 16), kQ4 = Align256((size_t)kStaticCapQ * 4);
 constexpr size_t kS16 = Align256((size_t)kStaticCapS * 16), kS4 = Align256((size_t)kStaticCapS * 4);
 constexpr size_t kA16 = Align256((size_t)kStaticWave * 16), kC4 = Align256((size_t)AZ_COUNT_TOTAL * 4);
-constexpr size_t kStaticBytes = 2 * (4 * kQ16 + kQ4) + kQ16 + 3 * kS16 + kS4 + kA16 + kC4;  // 9,110,272 B
+constexpr size_t kStaticBytes = 2 * (4 * kQ16 + kQ4) + kQ16 + 3 * kS16 + kS4 + kA16 + kC4;  // 9,110,784 B
 
 // One copy per GPU that loads this library, held until the process exits.
 // Host code must not use this name as an address: it resolves the device

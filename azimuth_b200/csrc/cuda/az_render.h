@@ -14,7 +14,8 @@ constexpr uint32_t AZ_COUNT_SHADOW = AZ_MAX_LEVELS;      // shadow-queue sizes p
 constexpr uint32_t AZ_COUNT_OVERFLOW = 2 * AZ_MAX_LEVELS;
 constexpr uint32_t AZ_COUNT_NODES = 2 * AZ_MAX_LEVELS + 2;  // node visits, primitive visits
 constexpr uint32_t AZ_COUNT_ERROR = 2 * AZ_MAX_LEVELS + 4;  // traversal step limit reached
-constexpr uint32_t AZ_COUNT_TOTAL = 2 * AZ_MAX_LEVELS + 8;
+constexpr uint32_t AZ_COUNT_FETCH = 2 * AZ_MAX_LEVELS + 8;  // per level: extend, then shadow work counters
+constexpr uint32_t AZ_COUNT_TOTAL = 4 * AZ_MAX_LEVELS + 8;
 
 // Camera and film parameters of one render call (ProduceImageInLinearSpace's
 // locals, src/azimuth_main.cpp:1265-1347).

@@ -219,13 +219,225 @@ __device__ __forceinline__ float group_world_t(const DevGroup &g, const Ray &wr,
 // Traversal on GPUs Through Compressed Wide BVHs" (HPG 2017): each step
 // visits the nearest node of the current group, then tests the primitives its
 // leaves hit, postponing them onto the stack while few lanes of the warp have
-// primitives to test.  For Q_CLOSEST returns the nearest hit in `best`
-// (best.ent == 0xFFFFFFFF: none).  For Q_ANY returns true as soon as a
-// primitive's world t < tmax.  `skip_ent` (optional) is an entity whose
-// primitives are ignored.  `counts` accumulates node and primitive visits.
+// primitives to test.  The traversal is a resumable state machine (init, then
+// step() until it reports the query finished) so that persistent kernels can
+// hand a lane a new ray as soon as its query ends.
+//
+// Q_CLOSEST: nearest hit in `best` (best.ent == 0xFFFFFFFF: none).
+// Q_ANY: `hit_any` is set as soon as a primitive's world t < tmax.
+// `skip_ent` is an entity whose primitives are ignored (0xFFFFFFFF: none).
 template <QueryKind KIND>
 __device__ bool trace(const DevScene &S, const Ray &wr, bool cull, float eps, float tmax, Hit &best,
-                      uint32_t *counts = nullptr, uint32_t *err = nullptr, uint32_t skip_ent = 0xFFFFFFFFu) {
+                      uint32_t *counts = nullptr, uint32_t *err = nullptr, uint32_t skip_ent = 0xFFFFFFFFu);
+
+template <QueryKind KIND>
+struct Tracer {
+    Ray wr;                    // world ray
+    Ray r;                     // ray in the current space (world or a group's local space)
+    f3 inv;
+    uint32_t oct;
+    float tcur;                // pruning distance in the current space
+    float tmax, eps;
+    bool cull, in_blas, hit_any;
+    uint32_t skip_ent, g_idx;
+    float bl_t;                // nearest local hit of this BLAS visit
+    uint32_t bl_prim;
+    uint32_t ng_base, ng_bits; // current node group
+    uint32_t pg_base, pg_mask; // current primitive group
+    uint32_t steps, nodes_visited, prims_visited;
+    int sp;
+    Hit best;
+
+    __device__ __forceinline__ void init(const DevScene &S, const Ray &ray, bool cull_, float eps_, float tmax_,
+                                         uint32_t skip = 0xFFFFFFFFu) {
+        wr = ray;
+        r = ray;
+        inv = safe_inv(r.d);
+        oct = octant_of(r.d);
+        tmax = tmax_;
+        eps = eps_;
+        cull = cull_;
+        tcur = KIND == Q_ANY ? tmax_ : FLT_MAX;
+        in_blas = false;
+        hit_any = false;
+        skip_ent = skip;
+        g_idx = 0;
+        bl_t = FLT_MAX;
+        bl_prim = 0xFFFFFFFFu;
+        pg_base = 0;
+        pg_mask = 0;
+        steps = nodes_visited = prims_visited = 0;
+        sp = 0;
+        best.t = FLT_MAX;
+        best.tl = 0.0f;
+        best.prim = 0xFFFFFFFFu;
+        best.ent = 0xFFFFFFFFu;
+        // current node group: the root alone (imask bit 0, hit bit 0 ^ oct)
+        ng_base = S.tlas_root;
+        ng_bits = S.tlas_root == 0xFFFFFFFFu ? 0u : ((1u << 8) | (1u << oct));
+    }
+
+    __device__ __forceinline__ void push(uint2 *stack, uint32_t x, uint32_t y, uint32_t *err) {
+        if (sp < AZD_WSTACK) stack[sp++] = make_uint2(x, y);
+        else if (err) atomicOr(err, 2u);
+    }
+
+    // One step: visit the nearest node of the current group and test the
+    // primitives it hits, or pop the stack.  Returns true when finished.  The
+    // stack (AZD_WSTACK entries) is a separate array of the caller so that the
+    // state above stays in registers.
+    __device__ __forceinline__ bool step(const DevScene &S, uint2 *stack, uint32_t *err) {
+        if (++steps > AZD_MAX_STEPS) {
+            if (err) atomicOr(err, 1u);
+            return true;
+        }
+        if (ng_bits & 0xFFu) {
+            const uint32_t hits = ng_bits & 0xFFu, imask = (ng_bits >> 8) & 0xFFu;
+            const uint32_t key = __ffs(hits) - 1u;
+            const uint32_t slot = key ^ oct;
+            const uint32_t node = ng_base + __popc(imask & ((1u << slot) - 1u));
+            ng_bits &= ~(1u << key);
+            if (ng_bits & 0xFFu) push(stack, ng_base, ng_bits, err);
+            const uint4 *np = reinterpret_cast<const uint4 *>(S.wnodes + node);
+            const uint4 w0 = __ldg(np + 0), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3),
+                        w4 = __ldg(np + 4);
+            nodes_visited++;
+            const WideHits h = wide_test(w0, w1, w2, w3, w4, r.o, inv, oct, tcur);
+            ng_base = w1.x;
+            ng_bits = h.inner | ((w0.w >> 24) << 8);
+            if (h.prims) {
+                if (pg_mask) push(stack, pg_base, AZD_E_PRIMS | pg_mask, err);   // keep the older group for later
+                pg_base = w1.y;
+                pg_mask = h.prims;
+            }
+        }
+        // primitives, postponed while few lanes of the warp have any
+        while (pg_mask) {
+            if (__popc(__activemask()) < 6u && (ng_bits & 0xFFu) && sp < AZD_WSTACK) {
+                stack[sp++] = make_uint2(pg_base, AZD_E_PRIMS | pg_mask);
+                pg_mask = 0;
+                break;
+            }
+            const uint32_t bit = __ffs(pg_mask) - 1u;
+            pg_mask &= pg_mask - 1u;
+            const uint32_t pi = pg_base + bit;
+            prims_visited++;
+            if (in_blas) {
+                if (skip_ent != 0xFFFFFFFFu && __ldg(&S.tri_attr[pi].entity) == skip_ent) continue;
+                DevTri tr = load_tri(S.tris, pi);
+                float t, b, gm;
+                if (tri_test(tr, r, cull, eps, bl_t, t, b, gm)) {
+                    bl_t = t;
+                    bl_prim = pi;
+                    if (KIND == Q_ANY) {
+                        // finished as soon as one hit of this group is in range
+                        float wt = group_world_t(S.groups[g_idx], wr, r, t);
+                        if (wt > eps && wt < tmax) {
+                            hit_any = true;
+                            return true;
+                        }
+                    } else {
+                        tcur = fminf(tcur, t);
+                    }
+                }
+            } else {
+                const uint32_t p = __ldg(S.tlas_prims + pi);
+                if (p & AZD_TLAS_GROUP) {
+                    push(stack, p & ~AZD_TLAS_GROUP, AZD_E_GROUP, err);   // entered when popped
+                } else if (p != skip_ent) {
+                    const DevEntity &e = S.ents[p];
+                    float wt, tl;
+                    if (e.type == ENT_SPHERE && sphere_test(e, wr, eps, wt, tl)) {
+                        if (KIND == Q_ANY) {
+                            if (wt < tmax) {
+                                hit_any = true;
+                                return true;
+                            }
+                        } else if (wt < best.t) {
+                            best.t = wt;
+                            best.tl = tl;
+                            best.prim = 0xFFFFFFFFu;
+                            best.ent = p;
+                            tcur = wt;
+                        }
+                    }
+                }
+            }
+        }
+        if ((ng_bits & 0xFFu) || pg_mask) return false;
+        // nothing left in the current groups: pop
+        if (sp == 0) return true;
+        const uint2 e = stack[--sp];
+        if (e.y == AZD_E_EXIT) {
+            // leaving a BLAS: azimuth's instance path keeps the nearest local hit
+            // and recomputes its world t (src/azimuth_main.cpp:256-276)
+            if (KIND == Q_CLOSEST && bl_prim != 0xFFFFFFFFu) {
+                float wt = group_world_t(S.groups[g_idx], wr, r, bl_t);
+                if (wt > eps && wt < best.t) {
+                    best.t = wt;
+                    best.tl = bl_t;
+                    best.prim = bl_prim;
+                    best.ent = S.tri_attr[bl_prim].entity;
+                }
+            }
+            r = wr;
+            inv = safe_inv(r.d);
+            oct = octant_of(r.d);
+            tcur = KIND == Q_ANY ? tmax : best.t;
+            in_blas = false;
+        } else if (e.y == AZD_E_GROUP) {
+            // enter the group's BLAS (azimuth: GetLocalRay of the motion-shifted
+            // ray, src/azimuth_main.cpp:246-250)
+            g_idx = e.x;
+            const DevGroup &g = S.groups[g_idx];
+            if (g.root == 0xFFFFFFFFu) return false;
+            stack[sp++] = make_uint2(0u, AZD_E_EXIT);   // reuses the popped entry's slot
+            float blas_scale = 1.0f;
+            if (g.raw) {
+                r = wr;
+            } else {
+                Ray m = wr;
+                m.o = wr.o - wr.time * mk(g.motion[0], g.motion[1], g.motion[2]);
+                r = local_ray(m, g.inv);
+                // local t = world t * |inv * d| / |d| (up to rounding)
+                blas_scale = length(vector_xf(g.inv, wr.d)) / length(wr.d) * 1.0001f;
+            }
+            inv = safe_inv(r.d);
+            oct = octant_of(r.d);
+            float wlim = KIND == Q_ANY ? tmax : best.t;
+            tcur = wlim < FLT_MAX ? wlim * blas_scale + 1e-30f : FLT_MAX;
+            bl_t = FLT_MAX;
+            bl_prim = 0xFFFFFFFFu;
+            in_blas = true;
+            ng_base = g.root;
+            ng_bits = (1u << 8) | (1u << oct);
+        } else if ((e.y & 0xC0000000u) == AZD_E_PRIMS) {
+            pg_base = e.x;
+            pg_mask = e.y & 0x00FFFFFFu;
+        } else {
+            ng_base = e.x;
+            ng_bits = e.y;
+        }
+        return false;
+    }
+
+    __device__ __forceinline__ void flush_counts(uint32_t *counts) const {
+        if (counts) {
+            atomicAdd(counts + 0, nodes_visited);
+            atomicAdd(counts + 1, prims_visited);
+        }
+    }
+};
+
+// A whole query in one loop: the same traversal as Tracer written as a single
+// function, which the compiler schedules better when one thread runs one
+// query to its end (grid-stride kernels).  For Q_CLOSEST returns whether
+// something was hit and the nearest hit in `best`; for Q_ANY returns whether a
+// primitive lies closer than tmax.  `skip_ent` is an entity whose primitives
+// are ignored; `counts` accumulates node and primitive visits.
+template <QueryKind KIND>
+__device__ bool trace(const DevScene &S, const Ray &wr, bool cull, float eps, float tmax, Hit &best,
+                      uint32_t *counts, uint32_t *err, uint32_t skip_ent) {
     best.t = FLT_MAX;
     best.tl = 0.0f;
     best.prim = 0xFFFFFFFFu;

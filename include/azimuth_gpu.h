@@ -56,9 +56,9 @@ typedef struct az_render_opts {
     uint32_t chunk_samples;         /* camera samples in flight per wave; 0 = automatic */
     uint32_t bvh_width;             /* 0 or 2 (binary BVH) */
     uint32_t block_size;            /* reserved (0) */
-    uint32_t variant;               /* traversal launch configuration 1..7 (threads per block and register
-                                       cap); 0 = the scene's choice: 3 (128 threads, at most 64 registers)
-                                       until az_gpu_autotune picks another */
+    uint32_t variant;               /* traversal launch configuration 1..10 (threads per block, register
+                                       cap, persistent ray fetching); 0 = the scene's choice: 3 (128
+                                       threads, at most 64 registers) until az_gpu_autotune picks another */
     uint32_t reserved[4];
 } az_render_opts;
 
@@ -108,9 +108,9 @@ int az_gpu_render_host(az_gpu_scene *scene, az_pixel *pixels, const az_camera *c
                        const az_epsilon_values *epsilons, az_scissor scissor, int32_t filter_type,
                        uint32_t backface_culling, const az_render_opts *opts, az_render_stats *stats);
 
-/* Autotuner: renders a band of the frame (the middle eighth of the scissor's
- * rows, every sample) with each traversal launch configuration and keeps the
- * fastest as the scene's default.  Writes the chosen variant (1-based) and its
+/* Autotuner: renders a band of the frame (the middle rows of the scissor: an
+ * eighth of them, or enough for about 2^20 samples) with each traversal launch
+ * configuration and keeps the fastest as the scene's default.  Writes the chosen variant (1-based) and its
  * time in ms.  Synchronous. */
 int az_gpu_autotune(az_gpu_scene *scene, const az_camera *camera, const az_epsilon_values *epsilons,
                     az_scissor scissor, int32_t filter_type, uint32_t backface_culling,
@@ -123,7 +123,7 @@ int az_gpu_autotune(az_gpu_scene *scene, const az_camera *camera, const az_epsil
  * hosts whose caching allocator owns all device memory, and real-time loops
  * that keep a fixed memory budget.  The scene (created earlier with
  * az_gpu_scene_create) and the DEVICE film are passed in as usual; the wave
- * queues live in one static device array of 9,110,272 bytes (8.7 MiB) that
+ * queues live in one static device array of 9,110,784 bytes (8.7 MiB) that
  * every GPU loading this library holds until the process exits, which caps a
  * wave at 16384 camera samples: opts->chunk_samples above 16384 is rejected
  * with AZ_ERR_INVALID_ARGUMENT.  The first call on a device looks up the
