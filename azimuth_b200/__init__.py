@@ -31,6 +31,7 @@ FILTER_GAUSSIAN = 1
 FLAG_COUNT_TRAVERSAL = 1
 FLAG_NO_GRAPH = 2
 FLAG_TIME_STAGES = 4
+LAUNCH_VARIANTS = 14   # AZ_LAUNCH_VARIANTS
 
 STATUS = {0: "AZ_OK", 1: "AZ_ERR_INVALID_ARGUMENT", 2: "AZ_ERR_INVALID_SCENE", 3: "AZ_ERR_OUT_OF_MEMORY",
           4: "AZ_ERR_CUDA", 5: "AZ_ERR_TIMEOUT", 6: "AZ_ERR_UNSUPPORTED", 7: "AZ_ERR_NO_DEVICE"}
@@ -120,9 +121,11 @@ def full_scissor(scene):
     return Scissor(Vec2u(w, h), Vec2u(0, 0))
 
 
-def make_opts(scene=None, seed=0, stream=None, device=0, flags=0, chunk_samples=0, block_size=0, variant=0):
+def make_opts(scene=None, seed=0, stream=None, device=0, flags=0, chunk_samples=0, block_size=0, variant=0,
+              bvh_width=0):
     o = RenderOpts()
     o.variant = variant
+    o.bvh_width = bvh_width
     o.seed = seed
     o.perlin_gradients = scene.perlin_gradients if scene is not None else None
     o.stream = stream
@@ -150,11 +153,11 @@ def produce_image(scene, pixels=None, scissor=None, filter_type=None, backface_c
 class GpuScene:
     """A device-resident scene (az_gpu_scene_create / az_gpu_scene_destroy)."""
 
-    def __init__(self, scene, device=0):
+    def __init__(self, scene, device=0, bvh_width=0):
         self.scene = scene
         self.device = device
         self._h = C.c_void_p()
-        o = make_opts(scene, device=device)
+        o = make_opts(scene, device=device, bvh_width=bvh_width)
         _check(lib().az_gpu_scene_create(scene.scene_ptr, C.byref(o), C.byref(self._h)), "az_gpu_scene_create")
 
     def autotune(self, seed=0, stream=None):
@@ -166,6 +169,19 @@ class GpuScene:
                                      self.scene.filter_type, 0, C.byref(o), C.byref(v), C.byref(ms)),
                "az_gpu_autotune")
         return v.value, ms.value
+
+    def autotune_scene(self, seed=0, stream=None):
+        """az_gpu_autotune_scene: sweeps BVH width (8, 4, 2) and launch variant, keeps the fastest build;
+        returns (width, variant, ms)."""
+        o = make_opts(self.scene, seed=seed, stream=stream, device=self.device)
+        w = C.c_uint32()
+        v = C.c_uint32()
+        ms = C.c_float()
+        _check(lib().az_gpu_autotune_scene(self.scene.scene_ptr, self._h, self.scene.camera_ptr,
+                                           self.scene.epsilons_ptr, full_scissor(self.scene), self.scene.filter_type,
+                                           0, C.byref(o), C.byref(w), C.byref(v), C.byref(ms)),
+               "az_gpu_autotune_scene")
+        return w.value, v.value, ms.value
 
     def render_device(self, film_ptr, camera_ptr=None, scissor=None, filter_type=None, seed=0, stream=None,
                       stats=False, flags=0, chunk_samples=0, variant=0):

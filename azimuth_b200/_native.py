@@ -96,6 +96,8 @@ def _declare(L):
         L.az_gpu_render_host.restype = i32
         L.az_gpu_autotune.argtypes = [vp, vp, vp, Scissor, i32, u32, C.POINTER(RenderOpts), vp, vp]
         L.az_gpu_autotune.restype = i32
+        L.az_gpu_autotune_scene.argtypes = [vp, vp, vp, vp, Scissor, i32, u32, C.POINTER(RenderOpts), vp, vp, vp]
+        L.az_gpu_autotune_scene.restype = i32
         L.az_gpu_render_noalloc.argtypes = [vp, vp, vp, vp, Scissor, i32, u32, C.POINTER(RenderOpts)]
         L.az_gpu_render_noalloc.restype = i32
         L.az_gpu_closest_hit.argtypes = [vp, vp, u32, i32, C.c_float, vp, vp, vp, vp, vp]

@@ -2,6 +2,7 @@
 //
 // Each call selects opts->device, runs on opts->stream (or a private stream),
 // catches every CUDA error into an AZ_* status and never throws across the ABI.
+#include <cfloat>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -184,6 +185,57 @@ extern "C" int az_gpu_autotune(az_gpu_scene *scene, const az_camera *camera, con
     if (rc != AZ_OK) return rc;
     return Autotune(*scene->impl, camera, epsilons, scissor, filter_type, backface_culling, opts, ctx.stream,
                     variant_out, ms_out);
+}
+
+extern "C" int az_gpu_autotune_scene(const az_scene *host_scene, az_gpu_scene *scene, const az_camera *camera,
+                                     const az_epsilon_values *epsilons, az_scissor scissor, int32_t filter_type,
+                                     uint32_t backface_culling, const az_render_opts *opts, uint32_t *width_out,
+                                     uint32_t *variant_out, float *ms_out) {
+    if (!host_scene || !scene || !scene->impl || !camera) return SetError(AZ_ERR_INVALID_ARGUMENT, "null argument");
+    CallContext ctx;
+    int rc = ctx.begin(opts);
+    if (rc != AZ_OK) return rc;
+    az_render_opts o;
+    if (opts) o = *opts;
+    else memset(&o, 0, sizeof(o));
+    o.device = scene->impl->device;
+    GpuScene *best = nullptr;
+    uint32_t best_v = 0;
+    float best_ms = FLT_MAX;
+    for (uint32_t width : {8u, 4u, 2u}) {
+        GpuScene *g = scene->impl;
+        if (width != g->bvh_width) {
+            o.bvh_width = width;
+            g = nullptr;
+            rc = BuildGpuScene(host_scene, &o, ctx.stream, &g);
+            if (rc != AZ_OK) break;
+        }
+        uint32_t v = 0;
+        float ms = FLT_MAX;
+        rc = Autotune(*g, camera, epsilons, scissor, filter_type, backface_culling, opts, ctx.stream, &v, &ms);
+        if (rc == AZ_OK && ms < best_ms) {
+            if (best && best != scene->impl) delete best;
+            best = g;
+            best_v = v;
+            best_ms = ms;
+        } else if (g != scene->impl) {
+            delete g;
+        }
+        if (rc != AZ_OK) break;
+    }
+    if (rc != AZ_OK) {
+        if (best && best != scene->impl) delete best;
+        return rc;
+    }
+    if (best != scene->impl) {
+        cudaStreamSynchronize(ctx.stream);
+        delete scene->impl;
+        scene->impl = best;
+    }
+    if (width_out) *width_out = best->bvh_width;
+    if (variant_out) *variant_out = best_v;
+    if (ms_out) *ms_out = best_ms;
+    return AZ_OK;
 }
 
 extern "C" int az_gpu_closest_hit(az_gpu_scene *scene, const az_ray3 *rays, uint32_t count, int32_t cull,

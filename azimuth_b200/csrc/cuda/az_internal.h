@@ -36,9 +36,11 @@ struct GpuScene {
     uint64_t sphere_count = 0;
     uint64_t node_count = 0;
     uint32_t max_bvh_depth = 0;
+    uint32_t bvh_width = 8;      // children per wide node (2, 4 or 8)
     size_t device_bytes = 0;
     WaveBuffers waves;           // reused across render calls on this scene
-    uint32_t variant = 2;        // traversal launch configuration (128 threads, 8 blocks/SM; az_gpu_autotune)
+    uint32_t variant = 7;        // traversal launch configuration, 0-based (128 threads, 8 blocks/SM,
+                                 // persistent fetching; az_gpu_autotune picks per scene)
     az_pixel *host_film_dev = nullptr;   // device film of az_gpu_render_host
     size_t host_film_bytes = 0;
     ~GpuScene();
@@ -56,11 +58,12 @@ int BuildLBVH(const float4 *d_lo, const float4 *d_hi, uint32_t n, azd::BVHNode *
               uint32_t leaf_base, uint32_t *d_perm, cudaStream_t stream, uint32_t *root_out);
 
 // Collapse of a binary BVH (nodes `bin`, global index of bin[0] = bin_base)
-// into 8-wide nodes appended to `out`; `prim_order[j]` receives the sorted
-// primitive position of output slot prim_out_base + j.
+// into wide nodes of at most `width` (2, 4 or 8) children appended to `out`;
+// `prim_order[j]` receives the sorted primitive position of output slot
+// prim_out_base + j.
 int CollapseToWide(const std::vector<azd::BVHNode> &bin, uint32_t bin_base, uint32_t bin_root, uint32_t max_leaf,
-                   std::vector<azd::WideNode> &out, std::vector<uint32_t> &prim_order, uint32_t prim_out_base,
-                   uint32_t *root_out, uint32_t *depth_out);
+                   uint32_t width, std::vector<azd::WideNode> &out, std::vector<uint32_t> &prim_order,
+                   uint32_t prim_out_base, uint32_t *root_out, uint32_t *depth_out);
 
 int SetupCamera(const az_camera *c, az_scissor sc, int32_t filter, uint32_t cull, const az_epsilon_values *eps,
                 uint64_t seed, CameraParams &cam);

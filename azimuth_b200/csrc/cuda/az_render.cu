@@ -40,7 +40,8 @@ using namespace azd;
 enum : uint32_t {
     SHADOW_TMAX = 0,     // point/area/spot: occluded by a hit with t < 1 - ShadowRay epsilon
     SHADOW_ANY = 1,      // directional light and environment ray: occluded by any hit
-    SHADOW_ENTITY = 2    // entity light: occluded unless the nearest hit is the light's entity
+    SHADOW_ENTITY = 2,   // entity light: occluded unless the nearest hit is the light's entity
+    SHADOW_ENTITY_FULL = 3   // the same for a light too large for the two-phase test: k_shadow_full
 };
 
 // flags packed into d.w of a path entry
@@ -171,13 +172,49 @@ struct WarpFetch {
     }
 };
 
-template <int BLOCK, int MINB, bool PERSIST>
+// How a traversal kernel maps queries to threads:
+//   MODE_LOOP     one query per thread at a time in a grid-stride loop, each
+//                 thread running its query to the end in one loop
+//   MODE_LOCKSTEP the same assignment, but the warp advances its 32 queries
+//                 one traversal step at a time and reconverges after every
+//                 step
+//   MODE_FETCH    persistent warps: a lane takes the next query of the queue
+//                 as soon as its own ends (batches of kFetchBatch per warp)
+enum : int { MODE_LOOP = 0, MODE_LOCKSTEP = 1, MODE_FETCH = 2 };
+
+template <int BLOCK, int MINB, int MODE>
 __global__ void __launch_bounds__(BLOCK, MINB) k_extend(DevScene S, CameraParams cam, WaveQueues Q, uint32_t level) {
     const int buf = level & 1;
     const uint32_t n = min(Q.counts[level], Q.cap_q);
     uint32_t *cnt = cam.count_traversal ? Q.counts + AZ_COUNT_NODES : nullptr;
     uint32_t *err = Q.counts + AZ_COUNT_ERROR;
-    if (!PERSIST) {
+    if (MODE == MODE_LOCKSTEP) {
+        Tracer<Q_CLOSEST> T;
+        uint2 stack[AZD_WSTACK];
+        // warp-uniform loop bound: every lane of a warp sees the same base
+        for (uint32_t base = blockIdx.x * BLOCK + (threadIdx.x & ~31u); base < n; base += gridDim.x * BLOCK) {
+            const uint32_t i = base + (threadIdx.x & 31u);
+            bool live = i < n;
+            if (live) {
+                const float4 o = Q.o[buf][i], d = Q.d[buf][i];
+                Ray r;
+                r.o = mk(o.x, o.y, o.z);
+                r.d = mk(d.x, d.y, d.z);
+                r.time = o.w;
+                T.init(S, r, cam.cull != 0, cam.eps_isect, FLT_MAX);
+            }
+            while (__any_sync(0xFFFFFFFFu, live)) {
+                if (live && T.step(S, stack, err)) {
+                    const Hit &h = T.best;
+                    Q.hit[i] = make_uint4(__float_as_uint(h.t), __float_as_uint(h.tl), h.prim, h.ent);
+                    T.flush_counts(cnt);
+                    live = false;
+                }
+            }
+        }
+        return;
+    }
+    if (MODE == MODE_LOOP) {
         // one query per thread at a time, grid-stride over the queue
         for (uint32_t i = blockIdx.x * BLOCK + threadIdx.x; i < n; i += gridDim.x * BLOCK) {
             const float4 o = Q.o[buf][i], d = Q.d[buf][i];
@@ -297,7 +334,7 @@ __global__ void __launch_bounds__(BLOCK) k_shade(DevScene S, CameraParams cam, W
             if (!LIGHTS || L.type == LIGHT_ENTITY) {
                 sample_entity_light(S, L, s.p, rng, ldir, invpdf);
                 I = ld3(L.intensity);
-                kind = SHADOW_ENTITY;
+                kind = entity_light_needs_full_query(L) ? SHADOW_ENTITY_FULL : SHADOW_ENTITY;
             } else if (L.type == LIGHT_POINT) {
                 ldir = ld3(L.position) - s.p;
                 ldist = length(ldir);
@@ -336,7 +373,7 @@ __global__ void __launch_bounds__(BLOCK) k_shade(DevScene S, CameraParams cam, W
             if (is_zero(c)) continue;
             // entity lights carry the light index (their identity test needs the light)
             push_shadow(Q, level, s.p + (ldir * seps), r.time, ldir, 1.0f - seps, c, slot, kind,
-                        kind == SHADOW_ENTITY ? li : 0u);
+                        kind >= SHADOW_ENTITY ? li : 0u);
         }
         if (ENV && S.use_env_map) {
             // cosine-sampled environment ray (:724-778); not gated by InsideDielectric
@@ -465,12 +502,72 @@ __global__ void __launch_bounds__(BLOCK) k_shade(DevScene S, CameraParams cam, W
 // sample.  Entity lights: occluded unless the nearest hit is the light's
 // entity, so the light's own nearest hit is found exactly first and the query
 // looks for anything else before it.
-template <int BLOCK, int MINB, bool PERSIST>
+// Visibility of the SHADOW_ENTITY_FULL queries of the shadow queue (entity
+// lights too large for the two-phase test): one full nearest-hit query each,
+// visible when the nearest hit is the light's entity (src/azimuth_main.cpp:694-712).
+// Launched only for scenes that have such a light.
+__global__ void __launch_bounds__(128) k_shadow_full(DevScene S, CameraParams cam, WaveQueues Q, uint32_t level) {
+    const uint32_t n = min(Q.counts[AZ_COUNT_SHADOW + level], Q.cap_s);
+    uint32_t *cnt = cam.count_traversal ? Q.counts + AZ_COUNT_NODES : nullptr;
+    uint32_t *err = Q.counts + AZ_COUNT_ERROR;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t meta = Q.smeta[i];
+        if ((meta >> 30) != SHADOW_ENTITY_FULL) continue;
+        const float4 o = Q.so[i], d = Q.sd[i], c = Q.sc[i];
+        const DevLight &L = S.lights[meta & 0x3FFFFFFFu];
+        Ray r;
+        r.o = mk(o.x, o.y, o.z);
+        r.d = mk(d.x, d.y, d.z);
+        r.time = o.w;
+        Hit h;
+        const bool any = trace<Q_CLOSEST>(S, r, false, 0.0f, FLT_MAX, h, cnt, err);
+        if (!any || S.ents[h.ent].uid == L.uid) add_accum(Q.accum, __float_as_uint(c.w), mk(c.x, c.y, c.z));
+    }
+}
+
+template <int BLOCK, int MINB, int MODE>
 __global__ void __launch_bounds__(BLOCK, MINB) k_shadow(DevScene S, CameraParams cam, WaveQueues Q, uint32_t level) {
     const uint32_t n = min(Q.counts[AZ_COUNT_SHADOW + level], Q.cap_s);
     uint32_t *cnt = cam.count_traversal ? Q.counts + AZ_COUNT_NODES : nullptr;
     uint32_t *err = Q.counts + AZ_COUNT_ERROR;
-    if (!PERSIST) {
+    if (MODE == MODE_LOCKSTEP) {
+        Tracer<Q_ANY> T;
+        uint2 stack[AZD_WSTACK];
+        for (uint32_t base = blockIdx.x * BLOCK + (threadIdx.x & ~31u); base < n; base += gridDim.x * BLOCK) {
+            const uint32_t i = base + (threadIdx.x & 31u);
+            bool live = i < n;
+            float4 c = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            if (live) {
+                const float4 o = Q.so[i], d = Q.sd[i];
+                c = Q.sc[i];
+                const uint32_t meta = Q.smeta[i];
+                const uint32_t kind = meta >> 30, li = meta & 0x3FFFFFFFu;
+                Ray r;
+                r.o = mk(o.x, o.y, o.z);
+                r.d = mk(d.x, d.y, d.z);
+                r.time = o.w;
+                if (kind == SHADOW_ENTITY_FULL) {
+                    live = false;   // k_shadow_full
+                } else if (kind == SHADOW_ENTITY) {
+                    const DevLight &L = S.lights[li];
+                    float tl = FLT_MAX;
+                    const int lh = light_entity_hit(S, L, r, tl);
+                    T.init(S, r, false, 0.0f, lh ? tl : FLT_MAX, L.ent_index);
+                } else {
+                    T.init(S, r, false, 0.0f, kind == SHADOW_ANY ? FLT_MAX : d.w);
+                }
+            }
+            while (__any_sync(0xFFFFFFFFu, live)) {
+                if (live && T.step(S, stack, err)) {
+                    if (!T.hit_any) add_accum(Q.accum, __float_as_uint(c.w), mk(c.x, c.y, c.z));
+                    T.flush_counts(cnt);
+                    live = false;
+                }
+            }
+        }
+        return;
+    }
+    if (MODE == MODE_LOOP) {
         for (uint32_t i = blockIdx.x * BLOCK + threadIdx.x; i < n; i += gridDim.x * BLOCK) {
             const float4 o = Q.so[i], d = Q.sd[i], c = Q.sc[i];
             const uint32_t meta = Q.smeta[i];
@@ -481,16 +578,13 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_shadow(DevScene S, CameraParams
             r.time = o.w;
             Hit h;
             bool visible;
-            if (kind == SHADOW_ENTITY) {
+            if (kind == SHADOW_ENTITY_FULL) {
+                continue;   // k_shadow_full
+            } else if (kind == SHADOW_ENTITY) {
                 const DevLight &L = S.lights[li];
                 float tl = FLT_MAX;
                 const int lh = light_entity_hit(S, L, r, tl);
-                if (lh < 0) {
-                    bool any = trace<Q_CLOSEST>(S, r, false, 0.0f, FLT_MAX, h, cnt, err);
-                    visible = !any || S.ents[h.ent].uid == L.uid;
-                } else {
-                    visible = !trace<Q_ANY>(S, r, false, 0.0f, lh ? tl : FLT_MAX, h, cnt, err, L.ent_index);
-                }
+                visible = !trace<Q_ANY>(S, r, false, 0.0f, lh ? tl : FLT_MAX, h, cnt, err, L.ent_index);
             } else {
                 visible = !trace<Q_ANY>(S, r, false, 0.0f, kind == SHADOW_ANY ? FLT_MAX : d.w, h, cnt, err);
             }
@@ -514,19 +608,13 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_shadow(DevScene S, CameraParams
             r.o = mk(o.x, o.y, o.z);
             r.d = mk(d.x, d.y, d.z);
             r.time = o.w;
-            if (kind == SHADOW_ENTITY) {
+            if (kind == SHADOW_ENTITY_FULL) {
+                idx = kLaneIdle;   // k_shadow_full
+            } else if (kind == SHADOW_ENTITY) {
                 const DevLight &L = S.lights[li];
                 float tl = FLT_MAX;
                 const int lh = light_entity_hit(S, L, r, tl);
-                if (lh < 0) {
-                    // a light too large to test alone: one full nearest-hit query
-                    Hit h;
-                    bool any = trace<Q_CLOSEST>(S, r, false, 0.0f, FLT_MAX, h, cnt, err);
-                    if (!any || S.ents[h.ent].uid == L.uid) add_accum(Q.accum, __float_as_uint(c.w), mk(c.x, c.y, c.z));
-                    idx = kLaneIdle;
-                } else {
-                    T.init(S, r, false, 0.0f, lh ? tl : FLT_MAX, L.ent_index);
-                }
+                T.init(S, r, false, 0.0f, lh ? tl : FLT_MAX, L.ent_index);
             } else {
                 T.init(S, r, false, 0.0f, kind == SHADOW_ANY ? FLT_MAX : d.w);
             }
@@ -575,13 +663,15 @@ constexpr int kBlock = 128;
 // or one query per thread in a grid-stride loop; chosen per scene by
 // az_gpu_autotune.
 struct Variant {
-    int block, minb;
-    bool persist;
+    int block, minb, mode;
 };
-constexpr Variant kVariants[] = {{128, 1, false}, {128, 6, false}, {128, 8, false}, {256, 1, false},
-                                 {256, 3, false}, {64, 1, false},  {64, 12, false}, {128, 8, true},
-                                 {128, 6, true},  {256, 3, true}};
+constexpr Variant kVariants[] = {{128, 1, MODE_LOOP},     {128, 6, MODE_LOOP},     {128, 8, MODE_LOOP},
+                                 {256, 1, MODE_LOOP},     {256, 3, MODE_LOOP},     {64, 1, MODE_LOOP},
+                                 {64, 12, MODE_LOOP},     {128, 8, MODE_FETCH},    {128, 6, MODE_FETCH},
+                                 {256, 3, MODE_FETCH},    {128, 8, MODE_LOCKSTEP}, {128, 6, MODE_LOCKSTEP},
+                                 {256, 3, MODE_LOCKSTEP}, {64, 12, MODE_LOCKSTEP}};
 constexpr uint32_t kVariantCount = sizeof(kVariants) / sizeof(kVariants[0]);
+static_assert(kVariantCount == AZ_LAUNCH_VARIANTS, "variant table and header disagree");
 
 template <uint32_t F>
 void LaunchShadeF(int grid, const DevScene &S, const CameraParams &cam, const WaveQueues &Q, uint64_t start,
@@ -611,7 +701,7 @@ void LaunchShade(int grid, const DevScene &S, const CameraParams &cam, const Wav
     }
 }
 
-template <int B, int M, bool P>
+template <int B, int M, int P>
 void LaunchTraversal(bool shadow, int sms, const DevScene &S, const CameraParams &cam, const WaveQueues &Q,
                      uint32_t L, cudaStream_t st) {
     const int grid = sms * (2048 / B);
@@ -621,17 +711,22 @@ void LaunchTraversal(bool shadow, int sms, const DevScene &S, const CameraParams
 
 void LaunchTraversalVariant(uint32_t v, bool shadow, int sms, const DevScene &S, const CameraParams &cam,
                             const WaveQueues &Q, uint32_t L, cudaStream_t st) {
+    if (shadow && S.full_light_queries) k_shadow_full<<<sms * 16, 128, 0, st>>>(S, cam, Q, L);
     switch (v) {
-        case 0: LaunchTraversal<128, 1, false>(shadow, sms, S, cam, Q, L, st); break;
-        case 1: LaunchTraversal<128, 6, false>(shadow, sms, S, cam, Q, L, st); break;
-        case 3: LaunchTraversal<256, 1, false>(shadow, sms, S, cam, Q, L, st); break;
-        case 4: LaunchTraversal<256, 3, false>(shadow, sms, S, cam, Q, L, st); break;
-        case 5: LaunchTraversal<64, 1, false>(shadow, sms, S, cam, Q, L, st); break;
-        case 6: LaunchTraversal<64, 12, false>(shadow, sms, S, cam, Q, L, st); break;
-        case 7: LaunchTraversal<128, 8, true>(shadow, sms, S, cam, Q, L, st); break;
-        case 8: LaunchTraversal<128, 6, true>(shadow, sms, S, cam, Q, L, st); break;
-        case 9: LaunchTraversal<256, 3, true>(shadow, sms, S, cam, Q, L, st); break;
-        default: LaunchTraversal<128, 8, false>(shadow, sms, S, cam, Q, L, st); break;
+        case 0: LaunchTraversal<128, 1, MODE_LOOP>(shadow, sms, S, cam, Q, L, st); break;
+        case 1: LaunchTraversal<128, 6, MODE_LOOP>(shadow, sms, S, cam, Q, L, st); break;
+        case 3: LaunchTraversal<256, 1, MODE_LOOP>(shadow, sms, S, cam, Q, L, st); break;
+        case 4: LaunchTraversal<256, 3, MODE_LOOP>(shadow, sms, S, cam, Q, L, st); break;
+        case 5: LaunchTraversal<64, 1, MODE_LOOP>(shadow, sms, S, cam, Q, L, st); break;
+        case 6: LaunchTraversal<64, 12, MODE_LOOP>(shadow, sms, S, cam, Q, L, st); break;
+        case 7: LaunchTraversal<128, 8, MODE_FETCH>(shadow, sms, S, cam, Q, L, st); break;
+        case 8: LaunchTraversal<128, 6, MODE_FETCH>(shadow, sms, S, cam, Q, L, st); break;
+        case 9: LaunchTraversal<256, 3, MODE_FETCH>(shadow, sms, S, cam, Q, L, st); break;
+        case 10: LaunchTraversal<128, 8, MODE_LOCKSTEP>(shadow, sms, S, cam, Q, L, st); break;
+        case 11: LaunchTraversal<128, 6, MODE_LOCKSTEP>(shadow, sms, S, cam, Q, L, st); break;
+        case 12: LaunchTraversal<256, 3, MODE_LOCKSTEP>(shadow, sms, S, cam, Q, L, st); break;
+        case 13: LaunchTraversal<64, 12, MODE_LOCKSTEP>(shadow, sms, S, cam, Q, L, st); break;
+        default: LaunchTraversal<128, 8, MODE_LOOP>(shadow, sms, S, cam, Q, L, st); break;
     }
 }
 
@@ -791,7 +886,7 @@ static int RenderWave(const GpuScene &G, const CameraParams &cam, WaveBuffers &W
         if (timer) timer->Mark(st, 2);
         LaunchTraversalVariant(v, true, sms, G.dev, cam, Q, L, st);
         if (timer) timer->Mark(st, 3);
-        rc.launches += 3;
+        rc.launches += G.dev.full_light_queries ? 4 : 3;
         rc.extend_launches++;
     }
     k_splat<<<(n + 255) / 256, 256, 0, st>>>(cam, Q, start, n, film);

@@ -130,6 +130,13 @@ struct __align__(16) DevLight {
     uint32_t ent_index;       // dense index of the light's entity in ents[], or 0xFFFFFFFF
 };
 
+// An entity light whose visibility needs a full nearest-hit query: its entity
+// is not among the scene's top-level entities, or its mesh is too large to
+// test on its own.
+__host__ __device__ __forceinline__ bool entity_light_needs_full_query(const DevLight &L) {
+    return L.ent_index == 0xFFFFFFFFu || (L.entity_type != ENT_SPHERE && L.tri_count > 64);
+}
+
 struct __align__(16) DevLightTri {
     float4 p0n;  // P0.xyz, N.x
     float4 p1n;  // P1.xyz, N.y
@@ -164,6 +171,7 @@ struct DevScene {
     uint32_t max_depth, path_trace, importance_sampling;
     uint32_t light_draws;           // RNG draws made by the light loop at every vertex
     uint32_t features;              // FEAT_* bits
+    uint32_t full_light_queries;    // 1: an entity light needs full nearest-hit visibility queries
 };
 
 }  // namespace azd

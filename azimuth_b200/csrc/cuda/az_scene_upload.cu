@@ -350,6 +350,9 @@ int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_
     *out = nullptr;
     std::unique_ptr<GpuScene> G(new GpuScene());
     G->device = opts ? opts->device : 0;
+    const uint32_t width = opts && opts->bvh_width ? opts->bvh_width : 8u;
+    if (width != 2 && width != 4 && width != 8) return SetError(AZ_ERR_INVALID_ARGUMENT, "bvh_width must be 0, 2, 4 or 8");
+    G->bvh_width = width;
     Flattener F;
     F.s = scene;
     if (!scene->BVHRoot) return SetError(AZ_ERR_INVALID_SCENE, "scene has no BVHRoot");
@@ -544,7 +547,7 @@ int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_
         std::vector<uint32_t> order;
         order.reserve(n);
         uint32_t depth = 0;
-        int rc2 = CollapseToWide(bin, node_base, bin_root, max_leaf, wide, order, prim_base, wroot, &depth);
+        int rc2 = CollapseToWide(bin, node_base, bin_root, max_leaf, width, wide, order, prim_base, wroot, &depth);
         if (rc2 != AZ_OK) return rc2;
         if (order.size() != n) return SetError(AZ_ERR_CUDA, "BVH collapse lost primitives");
         wide_depth = std::max(wide_depth, depth);
@@ -655,8 +658,11 @@ int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_
     if (scene->UseEnvironmentMap) D.features |= azd::FEAT_ENV;
     for (const azd::DevMaterial &m : mats)
         if (m.transparent || m.is_mirror) D.features |= azd::FEAT_SPECIAL;
-    for (const azd::DevLight &l : lights)
+    D.full_light_queries = 0;
+    for (const azd::DevLight &l : lights) {
         if (l.type != azd::LIGHT_ENTITY) D.features |= azd::FEAT_ANALYTIC_LIGHTS;
+        else if (azd::entity_light_needs_full_query(l)) D.full_light_queries = 1;
+    }
     AZ_CUDA_TRY(cudaStreamSynchronize(st));
     // the unsorted copies and build scratch are no longer needed
     for (auto &b : G->bufs) {

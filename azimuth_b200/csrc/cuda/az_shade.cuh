@@ -334,15 +334,14 @@ __device__ void sample_entity_light(const DevScene &S, const DevLight &L, f3 hp,
 // Nearest hit of a ray on an entity light's own primitives, with azimuth's
 // arithmetic (sphere :64-146; mesh instance :244-281 over the mesh's
 // `triangle` array, whose vertices are the triangle entities' vertices).
-// Returns 1 with the world t, 0 if the light is not hit, -1 if the light is
-// too large to test here (the caller then runs a full nearest-hit query).
+// Returns 1 with the world t, 0 if the light is not hit, -1 if the light
+// needs a full nearest-hit query instead (entity_light_needs_full_query).
 __device__ int light_entity_hit(const DevScene &S, const DevLight &L, const Ray &wr, float &t_world) {
-    if (L.ent_index == 0xFFFFFFFFu) return -1;
+    if (entity_light_needs_full_query(L)) return -1;
     if (L.entity_type == ENT_SPHERE) {
         float tl;
         return sphere_test(S.ents[L.ent_index], wr, 0.0f, t_world, tl) ? 1 : 0;
     }
-    if (L.tri_count > 64) return -1;
     f3 motion = wr.time * mk(L.motion[0], L.motion[1], L.motion[2]);
     Ray m = wr;
     m.o = wr.o - motion;

@@ -148,13 +148,11 @@ enum QueryKind : uint32_t {
 #define AZD_E_GROUP 0xFFFFFFFEu
 #define AZD_E_PRIMS 0x40000000u
 
-// 8-bit grid value to float without the conversion pipe: PRMT places the byte
-// in the low mantissa bits of 2^23, and one subtraction removes 2^23 (exact).
-// (Folding the 2^23 into the slab test's FMA constant instead would cost a
-// rounding of |origin offset| + 2^23 grid steps, which exceeds the one-step
-// box margin for thin nodes far from the ray origin.)
-__device__ __forceinline__ float qbyte(uint32_t w, uint32_t k) {
-    return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u | k)) - 8388608.0f;
+// 8-bit grid value q as the float 2^23 + q: PRMT places the byte in the low
+// mantissa bits of 2^23 (exact).  The slab test subtracts the 2^23 inside its
+// FMA (see wide_test).
+__device__ __forceinline__ float qbyte_biased(uint32_t w, uint32_t k) {
+    return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u | k));
 }
 
 struct WideHits {
@@ -169,7 +167,14 @@ __device__ __forceinline__ WideHits wide_test(const uint4 w0, const uint4 w1, co
     const uint32_t ex = w0.w & 0xFFu, ey = (w0.w >> 8) & 0xFFu, ez = (w0.w >> 16) & 0xFFu, imask = w0.w >> 24;
     const float sx = __uint_as_float(ex << 23) * inv.x, sy = __uint_as_float(ey << 23) * inv.y,
                 sz = __uint_as_float(ez << 23) * inv.z;
-    const float ox = (px - o.x) * inv.x, oy = (py - o.y) * inv.y, oz = (pz - o.z) * inv.z;
+    // Plane distance (p + q * step - o) * inv = q * s + o', computed as
+    // fma(2^23 + q, s, o' - 2^23 * s): the 2^23 * s terms cancel exactly (the
+    // same rounded s in both), so the only cost of the fold is the rounding of
+    // o' - 2^23 * s, at most half a grid step in t; the collapse leaves a full
+    // step of slack around every child box (az_wide_bvh.cu).
+    const float ox = __fmaf_rn(-8388608.0f, sx, (px - o.x) * inv.x);
+    const float oy = __fmaf_rn(-8388608.0f, sy, (py - o.y) * inv.y);
+    const float oz = __fmaf_rn(-8388608.0f, sz, (pz - o.z) * inv.z);
     // near/far planes: swap lo and hi when the direction is negative
     const bool nx = inv.x < 0.0f, ny = inv.y < 0.0f, nz = inv.z < 0.0f;
     const uint32_t nx0 = nx ? w3.z : w2.x, nx1 = nx ? w3.w : w2.y, fx0 = nx ? w2.x : w3.z, fx1 = nx ? w2.y : w3.w;
@@ -179,12 +184,12 @@ __device__ __forceinline__ WideHits wide_test(const uint4 w0, const uint4 w1, co
 #pragma unroll
     for (int s = 0; s < 8; s++) {
         const uint32_t k = s & 3;
-        const float tnx = __fmaf_rn(qbyte(s < 4 ? nx0 : nx1, k), sx, ox);
-        const float tfx = __fmaf_rn(qbyte(s < 4 ? fx0 : fx1, k), sx, ox);
-        const float tny = __fmaf_rn(qbyte(s < 4 ? ny0 : ny1, k), sy, oy);
-        const float tfy = __fmaf_rn(qbyte(s < 4 ? fy0 : fy1, k), sy, oy);
-        const float tnz = __fmaf_rn(qbyte(s < 4 ? nz0 : nz1, k), sz, oz);
-        const float tfz = __fmaf_rn(qbyte(s < 4 ? fz0 : fz1, k), sz, oz);
+        const float tnx = __fmaf_rn(qbyte_biased(s < 4 ? nx0 : nx1, k), sx, ox);
+        const float tfx = __fmaf_rn(qbyte_biased(s < 4 ? fx0 : fx1, k), sx, ox);
+        const float tny = __fmaf_rn(qbyte_biased(s < 4 ? ny0 : ny1, k), sy, oy);
+        const float tfy = __fmaf_rn(qbyte_biased(s < 4 ? fy0 : fy1, k), sy, oy);
+        const float tnz = __fmaf_rn(qbyte_biased(s < 4 ? nz0 : nz1, k), sz, oz);
+        const float tfz = __fmaf_rn(qbyte_biased(s < 4 ? fz0 : fz1, k), sz, oz);
         const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f));
         const float tf = fminf(fminf(tfx, tfy), fminf(tfz, tmax)) * 1.00000095367431640625f;
         if (tn <= tf) {

@@ -2,7 +2,8 @@
 //
 // The binary LBVH built on the GPU (az_bvh_build.cu) is read back and turned
 // into WideNode records: every wide node takes a binary node and repeatedly
-// opens the child with the largest surface area until it has 8 children;
+// opens the child with the largest surface area until it has `width` (2, 4
+// or 8) children;
 // subtrees of at most `max_leaf` primitives become leaf children.  Children
 // are placed in the slot matching the octant of their centre relative to the
 // node centre, so a ray visits slots near-first by XOR-ing with its direction
@@ -42,6 +43,7 @@ struct Collapser {
     uint32_t node_base;                  // global index of bin[0]
     std::vector<Range> range;            // per binary node (local index)
     uint32_t max_leaf;
+    uint32_t width = 8;                  // children per wide node: 2, 4 or 8
     std::vector<azd::WideNode> &out;
     uint32_t wide_base;                  // global index of out[0]
     std::vector<uint32_t> &prim_order;   // output slot -> sorted primitive position
@@ -109,23 +111,29 @@ struct Collapser {
                 lo[a] = std::min(lo[a], kids[i].lo[a]);
                 hi[a] = std::max(hi[a], kids[i].hi[a]);
             }
+        // Per axis a grid origin p and a power-of-two step with at least one
+        // full step of slack on both sides of every child box, including the
+        // ones on the node's own bounds: the device folds the byte-to-float
+        // bias into its slab-test FMA at a cost of up to half a step.
         float p[3];
         int e[3];
         for (int a = 0; a < 3; a++) {
-            // the grid origin sits one step-size of slack below the box
             double mag = std::max(std::fabs((double)lo[a]), std::fabs((double)hi[a]));
             double ext = std::max((double)hi[a] - lo[a], std::max(mag * 1e-6, 1e-30));
-            int ex = (int)std::ceil(std::log2(ext / 253.0));
+            int ex = (int)std::ceil(std::log2(ext / 251.0));
             ex = std::max(-126, std::min(127, ex));
-            double step = std::ldexp(1.0, ex);
-            // origin: rounded down onto a float no larger than lo
-            float pa = (float)lo[a];
-            p[a] = nextafterf(pa, -FLT_MAX);
-            e[a] = ex;
-            // grow the step until every upper bound fits in 255 steps
-            while ((double)hi[a] - p[a] > 255.0 * step && e[a] < 127) {
-                e[a]++;
-                step *= 2.0;
+            while (true) {
+                const double step = std::ldexp(1.0, ex);
+                // origin: a float at least one step below lo
+                float pa = (float)((double)lo[a] - step);
+                while ((double)pa > (double)lo[a] - step) pa = nextafterf(pa, -FLT_MAX);
+                const double top = std::ceil(((double)hi[a] - pa) / step) + 1.0;   // hi's byte, with slack
+                if (top <= 255.0 || ex >= 127) {
+                    p[a] = pa;
+                    e[a] = ex;
+                    break;
+                }
+                ex++;
             }
         }
         w.px = p[0]; w.py = p[1]; w.pz = p[2];
@@ -141,8 +149,9 @@ struct Collapser {
                 double h = std::ceil(((double)kids[i].hi[a] - p[a]) / step) + 1.0;
                 qlo[a][s] = (uint8_t)std::max(0.0, std::min(255.0, l));
                 qhi[a][s] = (uint8_t)std::max(0.0, std::min(255.0, h));
-                if ((double)p[a] + qlo[a][s] * step > (double)kids[i].lo[a] ||
-                    (double)p[a] + qhi[a][s] * step < (double)kids[i].hi[a])
+                // the decoded box must hold the child with a full step to spare on both sides
+                if ((double)p[a] + qlo[a][s] * step > (double)kids[i].lo[a] - step ||
+                    (double)p[a] + qhi[a][s] * step < (double)kids[i].hi[a] + step)
                     bad_box = true;
             }
         }
@@ -160,7 +169,7 @@ struct Collapser {
             kids[nk++] = ChildItem(n, 0);
             kids[nk++] = ChildItem(n, 1);
         }
-        while (nk < 8) {
+        while (nk < (int)width) {
             int best = -1;
             double best_area = -1.0;
             for (int i = 0; i < nk; i++) {
@@ -241,11 +250,13 @@ struct Collapser {
 }  // namespace
 
 int CollapseToWide(const std::vector<azd::BVHNode> &bin, uint32_t bin_base, uint32_t bin_root, uint32_t max_leaf,
-                   std::vector<azd::WideNode> &out, std::vector<uint32_t> &prim_order, uint32_t prim_out_base,
-                   uint32_t *root_out, uint32_t *depth_out) {
+                   uint32_t width, std::vector<azd::WideNode> &out, std::vector<uint32_t> &prim_order,
+                   uint32_t prim_out_base, uint32_t *root_out, uint32_t *depth_out) {
     if (max_leaf < 1 || max_leaf > 3) return SetError(AZ_ERR_INVALID_ARGUMENT, "leaf size must be 1..3");
+    if (width != 2 && width != 4 && width != 8) return SetError(AZ_ERR_INVALID_ARGUMENT, "BVH width must be 2, 4 or 8");
     // `out` may already hold the nodes of earlier hierarchies: indices are global
     Collapser C(bin, bin_base, max_leaf, out, 0, prim_order, prim_out_base);
+    C.width = width;
     uint32_t self = (uint32_t)out.size();
     C.Ranges(bin_root);
     Item root;

@@ -1,4 +1,5 @@
 // Seeded procedural scenes in azimuth's structs (see include/azimuth_scenes.h).
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -445,6 +446,130 @@ bool GenMotionEnv(Generated &G, const az_gen_params &p, uint64_t seed) {
     return true;
 }
 
+// Tessellated panel: origin o, edge vectors eu (nu cells) and ev (nv cells),
+// every interior vertex displaced along nrm by amp * fbm(position * freq);
+// faces wound so that the face normal is cross(eu, ev).  Cells whose centre
+// lies inside `hole` (fractions of the two edges) are left out (doorways).
+struct Hole {
+    float u0, u1, v0, v1;   // u0 >= u1: none
+};
+
+uint64_t TessPanel(Generated &G, MeshDesc &M, az_vec3 o, az_vec3 eu, az_vec3 ev, uint32_t nu, uint32_t nv,
+                   az_vec3 nrm, const GeoNoise &noise, double amp, double freq, Hole hole = Hole{1, 0, 1, 0}) {
+    const uint32_t base = (uint32_t)G.B.Vertices.size();
+    for (uint32_t j = 0; j <= nv; j++)
+        for (uint32_t i = 0; i <= nu; i++) {
+            const double fu = (double)i / nu, fv = (double)j / nv;
+            double px = o.x + eu.x * fu + ev.x * fv, py = o.y + eu.y * fu + ev.y * fv, pz = o.z + eu.z * fu + ev.z * fv;
+            // panel edges stay put so that neighbouring panels meet without cracks
+            const bool edge = i == 0 || j == 0 || i == nu || j == nv;
+            const double d = edge ? 0.0 : amp * noise.fbm(px * freq + 3.1, py * freq + 7.7, pz * freq + 1.3, 3);
+            AddV(G, V3((float)(px + nrm.x * d), (float)(py + nrm.y * d), (float)(pz + nrm.z * d)),
+                 az_vec2{(float)fu, (float)fv});
+        }
+    uint64_t tris = 0;
+    for (uint32_t j = 0; j < nv; j++)
+        for (uint32_t i = 0; i < nu; i++) {
+            const float cu = (i + 0.5f) / nu, cv = (j + 0.5f) / nv;
+            if (cu > hole.u0 && cu < hole.u1 && cv > hole.v0 && cv < hole.v1) continue;
+            const uint32_t a = base + j * (nu + 1) + i, b = a + 1, c = a + (nu + 1) + 1, d = a + (nu + 1);
+            M.Faces.push_back(az_vec3u{a, b, c});
+            M.Faces.push_back(az_vec3u{a, c, d});
+            tris += 2;
+        }
+    return tris;
+}
+
+// Axis-aligned box with outward faces, each face a panel of n x n cells.
+uint64_t TessBox(Generated &G, MeshDesc &M, const Box &b, uint32_t n, const GeoNoise &noise, double amp) {
+    const float dx = b.x1 - b.x0, dy = b.y1 - b.y0, dz = b.z1 - b.z0;
+    uint64_t t = 0;
+    t += TessPanel(G, M, V3(b.x0, b.y1, b.z0), V3(0, 0, dz), V3(dx, 0, 0), n, n, V3(0, 1, 0), noise, amp, 6.0);   // top
+    t += TessPanel(G, M, V3(b.x0, b.y0, b.z0), V3(dx, 0, 0), V3(0, 0, dz), n, n, V3(0, -1, 0), noise, amp, 6.0);  // bottom
+    t += TessPanel(G, M, V3(b.x0, b.y0, b.z1), V3(dx, 0, 0), V3(0, dy, 0), n, n, V3(0, 0, 1), noise, amp, 6.0);   // +z
+    t += TessPanel(G, M, V3(b.x1, b.y0, b.z0), V3(-dx, 0, 0), V3(0, dy, 0), n, n, V3(0, 0, -1), noise, amp, 6.0); // -z
+    t += TessPanel(G, M, V3(b.x1, b.y0, b.z1), V3(0, 0, -dz), V3(0, dy, 0), n, n, V3(1, 0, 0), noise, amp, 6.0);  // +x
+    t += TessPanel(G, M, V3(b.x0, b.y0, b.z0), V3(0, 0, dz), V3(0, dy, 0), n, n, V3(-1, 0, 0), noise, amp, 6.0);  // -x
+    return t;
+}
+
+// Interior: three 8 x 4 x 8 rooms in a row along x, joined by 1 x 2 doorways
+// in 0.2-thick inner walls, every surface a Perlin-displaced panel tessellated
+// at `detail` cells per metre (default 49: about 4 M triangles with the
+// clutter), 12 clutter boxes per room, one 1 x 1 area light under the ceiling
+// of room 1 and the camera in room 3 looking back through the doorways.
+bool GenInterior(Generated &G, const az_gen_params &p, uint64_t seed) {
+    Rng r(seed + 3);
+    GeoNoise noise(seed + 33);
+    const uint32_t cpm = Def(p.detail, 49);
+    const double amp = 0.015, freq = 2.5;
+    uint32_t wall = G.B.AddMaterial(Lambert(0.75f, 0.73f, 0.70f));
+    uint32_t floorm = G.B.AddMaterial(Lambert(0.55f, 0.45f, 0.35f));
+    uint32_t ceil = G.B.AddMaterial(Lambert(0.80f, 0.80f, 0.80f));
+    uint32_t clutter[4] = {G.B.AddMaterial(Lambert(0.65f, 0.20f, 0.15f)), G.B.AddMaterial(Lambert(0.20f, 0.50f, 0.25f)),
+                           G.B.AddMaterial(Lambert(0.20f, 0.30f, 0.65f)), G.B.AddMaterial(Lambert(0.70f, 0.65f, 0.30f))};
+    const float W = 8.0f, H = 4.0f, D = 8.0f, T = 0.2f;   // room width (x), height, depth (z); wall thickness
+    auto cells = [&](float len) { return std::max<uint32_t>(1u, (uint32_t)std::lround(len * cpm)); };
+    uint64_t tris = 0;
+    MeshDesc Walls, Floor, Ceil;
+    Walls.MaterialIndex = wall;
+    Floor.MaterialIndex = floorm;
+    Ceil.MaterialIndex = ceil;
+    const float X1 = 3 * W + 2 * T;     // total length along x
+    // floor (normal +y) and ceiling (normal -y) over the whole length
+    tris += TessPanel(G, Floor, V3(0, 0, 0), V3(0, 0, D), V3(X1, 0, 0), cells(D), cells(X1), V3(0, 1, 0), noise, amp, freq);
+    tris += TessPanel(G, Ceil, V3(0, H, 0), V3(X1, 0, 0), V3(0, 0, D), cells(X1), cells(D), V3(0, -1, 0), noise, amp, freq);
+    // long walls z = 0 (normal +z) and z = D (normal -z)
+    tris += TessPanel(G, Walls, V3(0, 0, 0), V3(X1, 0, 0), V3(0, H, 0), cells(X1), cells(H), V3(0, 0, 1), noise, amp, freq);
+    tris += TessPanel(G, Walls, V3(X1, 0, D), V3(-X1, 0, 0), V3(0, H, 0), cells(X1), cells(H), V3(0, 0, -1), noise, amp, freq);
+    // end walls x = 0 (normal +x) and x = X1 (normal -x)
+    tris += TessPanel(G, Walls, V3(0, 0, D), V3(0, 0, -D), V3(0, H, 0), cells(D), cells(H), V3(1, 0, 0), noise, amp, freq);
+    tris += TessPanel(G, Walls, V3(X1, 0, 0), V3(0, 0, D), V3(0, H, 0), cells(D), cells(H), V3(-1, 0, 0), noise, amp, freq);
+    // inner walls with a 1 x 2 doorway centred in z: two faces, the doorway's jambs and lintel
+    const Hole door{(D * 0.5f - 0.5f) / D, (D * 0.5f + 0.5f) / D, 0.0f, 2.0f / H};
+    for (int k = 1; k <= 2; k++) {
+        const float xa = k * W + (k - 1) * T, xb = xa + T;   // the wall spans x in [xa, xb]
+        tris += TessPanel(G, Walls, V3(xa, 0, 0), V3(0, 0, D), V3(0, H, 0), cells(D), cells(H), V3(-1, 0, 0), noise,
+                          amp, freq, door);   // face toward room k (normal -x)
+        const Hole doorb{1.0f - door.u1, 1.0f - door.u0, door.v0, door.v1};
+        tris += TessPanel(G, Walls, V3(xb, 0, D), V3(0, 0, -D), V3(0, H, 0), cells(D), cells(H), V3(1, 0, 0), noise,
+                          amp, freq, doorb);  // face toward room k+1 (normal +x)
+        const float z0 = D * 0.5f - 0.5f, z1 = D * 0.5f + 0.5f;
+        tris += TessPanel(G, Walls, V3(xb, 0, z0), V3(-T, 0, 0), V3(0, 2, 0), cells(T), cells(2), V3(0, 0, 1), noise, 0.0, freq);
+        tris += TessPanel(G, Walls, V3(xa, 0, z1), V3(T, 0, 0), V3(0, 2, 0), cells(T), cells(2), V3(0, 0, -1), noise, 0.0, freq);
+        tris += TessPanel(G, Walls, V3(xa, 2, z0), V3(T, 0, 0), V3(0, 0, 1), cells(T), cells(1), V3(0, -1, 0), noise, 0.0, freq);
+    }
+    // clutter boxes on the floor, off the aisle through the doorways
+    MeshDesc Clutter[4];
+    for (int k = 0; k < 4; k++) Clutter[k].MaterialIndex = clutter[k];
+    for (int room = 0; room < 3; room++) {
+        const float rx = room * (W + T);
+        for (int i = 0; i < 12; i++) {
+            const float sx = r.uniform(0.3f, 1.2f), sy = r.uniform(0.2f, 1.5f), sz = r.uniform(0.3f, 1.2f);
+            float cx = rx + r.uniform(0.8f, W - 0.8f), cz = r.uniform(0.8f, D - 0.8f);
+            if (fabsf(cz - D * 0.5f) < 1.6f) cz = cz < D * 0.5f ? cz - 1.6f : cz + 1.6f;
+            const Box b{cx - sx * 0.5f, cx + sx * 0.5f, 0.0f, sy, cz - sz * 0.5f, cz + sz * 0.5f};
+            tris += TessBox(G, Clutter[r.next() % 4], b, std::max<uint32_t>(2u, cpm / 2), noise, 0.01);
+        }
+    }
+    G.B.AddMesh(Floor);
+    G.B.AddMesh(Ceil);
+    G.B.AddMesh(Walls);
+    for (int k = 0; k < 4; k++)
+        if (!Clutter[k].Faces.empty()) G.B.AddMesh(Clutter[k]);
+    G.Triangles += tris;
+    // the only light: 1 x 1 under the ceiling of room 1, facing down
+    CeilingLight(G, W * 0.5f, D * 0.5f, 1.0f, H - 0.02f, 60.0f, ceil);
+    az_scene &S = G.B.Scene;
+    S.MaxRecursionDepth = Def(p.max_depth, 10);
+    S.PathTrace = 1;
+    S.ImportanceSampling = p.importance_sampling >= 0 ? (uint32_t)p.importance_sampling : 1u;
+    // room 3, looking toward -x through both doorways
+    SimpleCamera(G, V3(X1 - 1.0f, 1.6f, D * 0.5f + 0.6f), V3(-1.0f, -0.08f, -0.12f), 60.0f, Def(p.width, 1920),
+                 Def(p.height, 1080), Def(p.spp, 16));
+    return true;
+}
+
 bool GenFeatures(Generated &G, const az_gen_params &p, uint64_t seed) {
     Rng r(seed + 100);
     az_scene &S = G.B.Scene;
@@ -663,6 +788,7 @@ extern "C" int az_scene_generate(int32_t scene_id, uint64_t seed, const az_gen_p
         case AZ_SCENE_CORNELL: ok = GenCornell(*G, p, seed); break;
         case AZ_SCENE_DENSE_MESH: ok = GenDenseMesh(*G, p, seed); filter = AZ_Filter_Gaussian; break;
         case AZ_SCENE_MOTION_ENV: ok = GenMotionEnv(*G, p, seed); break;
+        case AZ_SCENE_INTERIOR: ok = GenInterior(*G, p, seed); break;
         case AZ_SCENE_FEATURES: ok = GenFeatures(*G, p, seed); filter = AZ_Filter_Gaussian; break;
         case AZ_SCENE_ENV_SPHERES: ok = GenEnvSpheres(*G, p, seed); break;
         default: delete G; return 1;

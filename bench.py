@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--chunk", type=int, default=0, help="camera samples per wave (0 = library default)")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="skip az_gpu_autotune_scene (BVH width and traversal launch variant) before timing")
     return ap.parse_args()
 
 
@@ -166,6 +168,10 @@ def reference_arm(args):
     return 0
 
 
+def seed_base(rank):
+    return 1000 * rank
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -193,11 +199,17 @@ def main():
     gs = az.GpuScene(scene, device=local)
     torch.cuda.synchronize()
     upload_s = time.time() - t0
+    tune = None
+    if not args.no_autotune:
+        # the autotuner's sweep (BVH width 8/4/2 x launch variants) on a band of the frame
+        t0 = time.time()
+        tw, tv, tms = gs.autotune_scene(seed=seed_base(rank))
+        tune = {"bvh_width": tw, "variant": tv, "band_ms": tms, "seconds": time.time() - t0}
 
     stream = torch.cuda.current_stream()
     sptr = stream.cuda_stream
     film = torch.zeros((h, w, 4), device="cuda", dtype=torch.float32)
-    seed = 1000 * rank
+    seed = seed_base(rank)
 
     def step(i, flags=0, stats=False):
         return gs.render_device(film.data_ptr(), seed=seed + i, stream=sptr, flags=flags, stats=stats,
@@ -273,7 +285,8 @@ def main():
     frac_ext = cnt["extend_rays"] / max(1, cnt["extend_rays"] + cnt["shadow_rays"])
     ext_nodes = cnt["node_visits"] * frac_ext
     ext_prims = cnt["prim_visits"] * frac_ext
-    bytes_per_frame = cnt["extend_rays"] * (32 + 16) + ext_nodes * 64 + ext_prims * 48
+    # per query: ray read (32 B) + hit written (16 B); 80 B per wide node, 48 B per triangle
+    bytes_per_frame = cnt["extend_rays"] * (32 + 16) + ext_nodes * 80 + ext_prims * 48
     per_launch_bytes = bytes_per_frame / max(1, cnt["extend_launches"])
     per_launch_ms = extend_ms / max(1, extend_launches)
     achieved = per_launch_bytes / (per_launch_ms / 1000.0) / 1e9
@@ -305,7 +318,7 @@ def main():
                           "parallelism": "dp%d (one frame per GPU, own seed)" % world,
                           "l2": "inputs larger than L2 (scene ~%.0f MB on device)" % (
                               (scene.triangle_count * (48 + 80 + 64)) / 1e6),
-                          "scene_upload_s": upload_s},
+                          "scene_upload_s": upload_s, "autotune": tune},
                "segments_per_s": world * seg / (ms / 1000.0), "rays_per_s": world * (seg + shadow) / (ms / 1000.0),
                "gpu_launches": int(launches), "e2e": e2e, "roofline": roofline, "clocks": clk}
         if cpu:

@@ -46,6 +46,9 @@ enum {
     AZ_FLAG_TIME_STAGES = 1u << 2       /* time each stage with CUDA events (az_render_stats *_ms) */
 };
 
+/* Number of traversal launch configurations (az_render_opts.variant). */
+#define AZ_LAUNCH_VARIANTS 14
+
 typedef struct az_render_opts {
     uint64_t seed;                  /* counter-RNG key */
     const float *perlin_gradients;  /* azimuth's PerlinGradient[256] (src/azimuth_texture.h:17-18),
@@ -54,11 +57,13 @@ typedef struct az_render_opts {
     int32_t device;                 /* CUDA device ordinal */
     uint32_t flags;                 /* AZ_FLAG_* */
     uint32_t chunk_samples;         /* camera samples in flight per wave; 0 = automatic */
-    uint32_t bvh_width;             /* 0 or 2 (binary BVH) */
+    uint32_t bvh_width;             /* az_gpu_scene_create: children per BVH node, 2, 4 or 8 (0 = 8) */
     uint32_t block_size;            /* reserved (0) */
-    uint32_t variant;               /* traversal launch configuration 1..10 (threads per block, register
-                                       cap, persistent ray fetching); 0 = the scene's choice: 3 (128
-                                       threads, at most 64 registers) until az_gpu_autotune picks another */
+    uint32_t variant;               /* traversal launch configuration 1..AZ_LAUNCH_VARIANTS (threads per
+                                       block, register cap, how queries map to threads: one per thread
+                                       to its end, warp lockstep per traversal step, or persistent
+                                       fetching); 0 = the scene's choice: 8 (128 threads, at most 64
+                                       registers, persistent fetching) until az_gpu_autotune picks another */
     uint32_t reserved[4];
 } az_render_opts;
 
@@ -115,6 +120,16 @@ int az_gpu_render_host(az_gpu_scene *scene, az_pixel *pixels, const az_camera *c
 int az_gpu_autotune(az_gpu_scene *scene, const az_camera *camera, const az_epsilon_values *epsilons,
                     az_scissor scissor, int32_t filter_type, uint32_t backface_culling,
                     const az_render_opts *opts, uint32_t *variant_out, float *ms_out);
+
+/* Autotuner over the BVH width as well: rebuilds the device hierarchy of
+ * `host_scene` (the scene `scene` was created from) with 8, 4 and 2 children
+ * per node, runs az_gpu_autotune on each and keeps the fastest build (and its
+ * launch configuration) in `scene`.  Writes the width, the variant (1-based)
+ * and its time in ms.  Synchronous; `scene` must not be rendering meanwhile. */
+int az_gpu_autotune_scene(const az_scene *host_scene, az_gpu_scene *scene, const az_camera *camera,
+                          const az_epsilon_values *epsilons, az_scissor scissor, int32_t filter_type,
+                          uint32_t backface_culling, const az_render_opts *opts, uint32_t *width_out,
+                          uint32_t *variant_out, float *ms_out);
 
 /* Allocation-free variant of az_gpu_render; it has no counterpart in azimuth.
  *

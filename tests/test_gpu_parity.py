@@ -97,7 +97,7 @@ def test_autotune_picks_a_variant_and_renders_the_same(gpu):
         a = torch.zeros((h, w, 4), device="cuda")
         g.render_device(a.data_ptr(), seed=3, stats=True)
         v, ms = g.autotune(seed=3)
-        assert 1 <= v <= 10 and ms > 0
+        assert 1 <= v <= az.LAUNCH_VARIANTS and ms > 0
         b = torch.zeros((h, w, 4), device="cuda")
         g.render_device(b.data_ptr(), seed=3, stats=True)
         # launch configuration changes scheduling only: same samples, same sums up to atomic order
@@ -106,13 +106,45 @@ def test_autotune_picks_a_variant_and_renders_the_same(gpu):
 
 def test_every_launch_variant_renders_the_same_film(gpu):
     import torch
-    scene = az.generate_scene(az.SCENE_FEATURES, seed=2, width=48, height=40, spp=4)
+    # the features scene reaches every shading path; the dense mesh exercises deep
+    # bottom-level traversal (where launch configurations differ the most)
+    cases = [(az.SCENE_FEATURES, dict(width=48, height=40, spp=4), 1.0),
+             (az.SCENE_DENSE_MESH, dict(width=40, height=40, spp=4, detail=5), 0.999)]
+    for sid, kw, need in cases:
+        scene = az.generate_scene(sid, seed=2, **kw)
+        w, h = scene.resolution()
+        films = []
+        with az.GpuScene(scene) as g:
+            for v in range(1, az.LAUNCH_VARIANTS + 1):
+                f = torch.zeros((h, w, 4), device="cuda")
+                g.render_device(f.data_ptr(), seed=5, stats=True, variant=v)
+                films.append(f.cpu().numpy())
+        for v, f in enumerate(films[1:], start=2):
+            # same samples, same nearest hits: equal up to the order of the film atomics
+            # (on the mesh an exact-tie primitive may be picked in another order)
+            assert ol.film_compare(f, films[0], 1e-4)[0] >= need, (sid, v)
+
+
+def test_bvh_widths_render_the_same_film_and_autotune_scene(gpu):
+    import torch
+    scene = az.generate_scene(az.SCENE_DENSE_MESH, seed=1, width=48, height=48, spp=4, detail=4)
     w, h = scene.resolution()
     films = []
-    with az.GpuScene(scene) as g:
-        for v in range(1, 11):
+    for width in (8, 4, 2):
+        with az.GpuScene(scene, bvh_width=width) as g:
             f = torch.zeros((h, w, 4), device="cuda")
-            g.render_device(f.data_ptr(), seed=5, stats=True, variant=v)
+            g.render_device(f.data_ptr(), seed=7, stats=True)
             films.append(f.cpu().numpy())
-    for v, f in enumerate(films[1:], start=2):
-        assert ol.film_compare(f, films[0], 1e-4)[0] == 1.0, v
+    # a different hierarchy finds the same nearest primitives except at exact ties
+    # (a ray through an edge shared by two faces of different BRDFs may take the
+    # other face), so a few paths diverge
+    for f in films[1:]:
+        ok, _, rel = ol.film_compare(f, films[0], 1e-4)
+        assert ok >= 0.98 and rel < 1e-3, (ok, rel)
+    with az.GpuScene(scene) as g:
+        width, v, ms = g.autotune_scene(seed=7)
+        assert width in (2, 4, 8) and 1 <= v <= az.LAUNCH_VARIANTS and ms > 0
+        f = torch.zeros((h, w, 4), device="cuda")
+        g.render_device(f.data_ptr(), seed=7, stats=True)
+        ok, _, rel = ol.film_compare(f.cpu().numpy(), films[0], 1e-4)
+        assert ok >= 0.98 and rel < 1e-3, (ok, rel)
