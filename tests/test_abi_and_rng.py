@@ -81,3 +81,15 @@ def test_generated_scene_shapes():
     c0 = az.generate_scene(az.SCENE_CORNELL)
     assert c0.resolution() == (256, 256) and c0.sample_count() == 16 and c0.max_depth() == 5
     assert c0.triangle_count == 12 and c0.sphere_count == 2
+    # interior: three rooms, every surface tessellated at `detail` cells per metre
+    # (panels of two triangles per cell), 36 clutter boxes and the 2-triangle light
+    it = az.generate_scene(az.SCENE_INTERIOR, width=32, height=18, spp=4, detail=4)
+    assert it.resolution() == (32, 18) and it.max_depth() == 10
+    assert 20000 < it.triangle_count < 40000
+    assert it.triangle_count % 2 == 0
+
+
+def test_launch_variant_count_matches_header():
+    import re
+    hdr = open(os.path.join(REPO, "include", "azimuth_gpu.h")).read()
+    assert int(re.search(r"#define AZ_LAUNCH_VARIANTS (\d+)", hdr).group(1)) == az.LAUNCH_VARIANTS

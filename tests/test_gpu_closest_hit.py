@@ -31,6 +31,7 @@ CASES = [
     ("dense_mesh", az.SCENE_DENSE_MESH, dict(detail=5), (-0.45, 0.05, -0.45), (0.45, 0.95, 0.45)),
     ("motion_env", az.SCENE_MOTION_ENV, dict(detail=2000), (0.0, 0.0, 0.0), (10.0, 10.0, 10.0)),
     ("env_spheres", az.SCENE_ENV_SPHERES, {}, (-2.0, 0.05, -2.0), (2.0, 2.0, 2.0)),
+    ("interior", az.SCENE_INTERIOR, dict(detail=8), (0.5, 0.2, 0.5), (24.0, 3.8, 7.5)),
 ]
 
 

@@ -26,6 +26,7 @@ CASES = [
     ("dense_mesh", az.SCENE_DENSE_MESH, dict(width=40, height=40, spp=4, detail=3)),
     ("motion_env", az.SCENE_MOTION_ENV, dict(width=48, height=32, spp=4, detail=400, env_width=128,
                                              env_height=64)),
+    ("interior", az.SCENE_INTERIOR, dict(width=48, height=27, spp=4, detail=6)),
 ]
 
 
