@@ -16,7 +16,7 @@ import ctypes as C
 import numpy as np
 
 from . import _native
-from ._native import GenParams, GeneratedScene, RenderOpts, RenderStats, Scissor, Vec2u, Ray3, lib
+from ._native import GenParams, GeneratedScene, GuideConfig, RenderOpts, RenderStats, Scissor, Vec2u, Ray3, lib
 
 SCENE_CORNELL = 0
 SCENE_DENSE_MESH = 1
@@ -225,6 +225,94 @@ class GpuScene:
     def close(self):
         if self._h:
             lib().az_gpu_scene_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Guide:
+    """A neural path guide for one GpuScene (az_guide_create / az_guide_destroy)."""
+
+    LEVELS = 16
+    TABLE = 1 << 19
+
+    def __init__(self, gpu_scene, seed=0, learning_rate=0.0, train_batch=0, record_samples=0):
+        self.gs = gpu_scene
+        cfg = GuideConfig()
+        cfg.learning_rate = learning_rate
+        cfg.train_batch = train_batch
+        cfg.record_samples = record_samples
+        cfg.seed = seed
+        self._h = C.c_void_p()
+        _check(lib().az_guide_create(gpu_scene._h, C.byref(cfg), C.byref(self._h)), "az_guide_create")
+
+    def render(self, film_ptr, train=False, seed=0, stream=None, stats=True, flags=0, chunk_samples=0,
+               camera_ptr=None, scissor=None):
+        """az_gpu_render_guided into a DEVICE film pointer; returns az_render_stats as a dict if stats."""
+        sc_ = self.gs.scene
+        o = make_opts(sc_, seed=seed, stream=stream, device=self.gs.device, flags=flags, chunk_samples=chunk_samples)
+        st = RenderStats() if stats else None
+        _check(lib().az_gpu_render_guided(self.gs._h, self._h, film_ptr, camera_ptr or sc_.camera_ptr,
+                                          sc_.epsilons_ptr, scissor or full_scissor(sc_), sc_.filter_type, 0,
+                                          1 if train else 0, C.byref(o), C.byref(st) if st is not None else None),
+               "az_gpu_render_guided")
+        return _stats(st)
+
+    def info(self):
+        res = np.zeros(16, np.uint32)
+        lo = np.zeros(3, np.float32)
+        inv = np.zeros(3, np.float32)
+        steps = C.c_uint32()
+        _check(lib().az_guide_info(self._h, res.ctypes.data, lo.ctypes.data, inv.ctypes.data, C.byref(steps)),
+               "az_guide_info")
+        return {"res": res, "lo": lo, "inv_ext": inv, "steps": steps.value}
+
+    def params(self, grid=True):
+        mlp = np.zeros((4, 64, 64), np.float32)
+        bias = np.zeros(64, np.float32)
+        g = np.zeros((self.LEVELS, self.TABLE, 2), np.float32) if grid else None
+        _check(lib().az_guide_get_params(self._h, mlp.ctypes.data, bias.ctypes.data,
+                                         g.ctypes.data if grid else None), "az_guide_get_params")
+        return mlp, bias, g
+
+    def set_params(self, mlp=None, bias=None, grid=None):
+        arrs = [None if a is None else np.ascontiguousarray(a, np.float32) for a in (mlp, bias, grid)]
+        _check(lib().az_guide_set_params(self._h, *[None if a is None else a.ctypes.data for a in arrs]),
+               "az_guide_set_params")
+
+    def eval(self, rows):
+        """rows: (N, 16) float32 [pos, weight, normal, 0, wo, 0, wi, 0]; outputs, loss and gradients."""
+        rows = np.ascontiguousarray(rows, np.float32)
+        n = rows.shape[0]
+        out = np.zeros((n, 64), np.float32)
+        loss = np.zeros(1, np.float32)
+        mg = np.zeros((4, 64, 64), np.float32)
+        bg = np.zeros(64, np.float32)
+        eg = np.zeros((n, 32), np.float32)
+        _check(lib().az_guide_eval(self._h, rows.ctypes.data, n, out.ctypes.data, loss.ctypes.data, mg.ctypes.data,
+                                   bg.ctypes.data, eg.ctypes.data), "az_guide_eval")
+        return {"outputs": out, "loss": float(loss[0]), "mlp_grad": mg, "bias_grad": bg, "enc_grad": eg}
+
+    def train(self, rows, steps):
+        rows = np.ascontiguousarray(rows, np.float32)
+        losses = np.zeros(steps, np.float32)
+        _check(lib().az_guide_train(self._h, rows.ctypes.data, rows.shape[0], steps, losses.ctypes.data),
+               "az_guide_train")
+        return losses
+
+    def close(self):
+        if self._h:
+            lib().az_guide_destroy(self._h)
             self._h = C.c_void_p()
 
     def __enter__(self):

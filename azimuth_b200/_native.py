@@ -49,6 +49,11 @@ class RenderOpts(C.Structure):
                 ("reserved", C.c_uint32 * 4)]
 
 
+class GuideConfig(C.Structure):
+    _fields_ = [("learning_rate", C.c_float), ("train_batch", C.c_uint32), ("record_samples", C.c_uint32),
+                ("reserved0", C.c_uint32), ("seed", C.c_uint64), ("reserved", C.c_uint32 * 6)]
+
+
 class RenderStats(C.Structure):
     _fields_ = [("samples", C.c_uint64), ("extend_rays", C.c_uint64), ("shadow_rays", C.c_uint64),
                 ("chunks", C.c_uint32), ("retries", C.c_uint32), ("kernel_launches", C.c_uint64),
@@ -99,6 +104,22 @@ def _declare(L):
         L.az_gpu_autotune_scene.argtypes = [vp, vp, vp, vp, Scissor, i32, u32, C.POINTER(RenderOpts), vp, vp, vp]
         L.az_gpu_autotune_scene.restype = i32
         L.az_gpu_render_noalloc.argtypes = [vp, vp, vp, vp, Scissor, i32, u32, C.POINTER(RenderOpts)]
+        L.az_guide_create.argtypes = [vp, C.POINTER(GuideConfig), C.POINTER(vp)]
+        L.az_guide_create.restype = i32
+        L.az_guide_destroy.argtypes = [vp]
+        L.az_guide_destroy.restype = None
+        L.az_gpu_render_guided.argtypes = [vp, vp, vp, vp, vp, Scissor, i32, u32, u32, C.POINTER(RenderOpts), vp]
+        L.az_gpu_render_guided.restype = i32
+        L.az_guide_get_params.argtypes = [vp, vp, vp, vp]
+        L.az_guide_get_params.restype = i32
+        L.az_guide_set_params.argtypes = [vp, vp, vp, vp]
+        L.az_guide_set_params.restype = i32
+        L.az_guide_info.argtypes = [vp, vp, vp, vp, vp]
+        L.az_guide_info.restype = i32
+        L.az_guide_eval.argtypes = [vp, vp, u32, vp, vp, vp, vp, vp]
+        L.az_guide_eval.restype = i32
+        L.az_guide_train.argtypes = [vp, vp, u32, u32, vp]
+        L.az_guide_train.restype = i32
         L.az_gpu_render_noalloc.restype = i32
         L.az_gpu_closest_hit.argtypes = [vp, vp, u32, i32, C.c_float, vp, vp, vp, vp, vp]
         L.az_gpu_closest_hit.restype = i32

@@ -238,6 +238,20 @@ extern "C" int az_gpu_autotune_scene(const az_scene *host_scene, az_gpu_scene *s
     return AZ_OK;
 }
 
+extern "C" int az_gpu_render_guided(az_gpu_scene *scene, az_guide *guide, az_pixel *film, const az_camera *camera,
+                                    const az_epsilon_values *epsilons, az_scissor scissor, int32_t filter_type,
+                                    uint32_t backface_culling, uint32_t train, const az_render_opts *opts,
+                                    az_render_stats *stats) {
+    if (!scene || !scene->impl || !guide || !film || !camera) return SetError(AZ_ERR_INVALID_ARGUMENT, "null argument");
+    GuideState *g = GuideOf(guide);
+    if (!g) return SetError(AZ_ERR_INVALID_ARGUMENT, "null guide");
+    CallContext ctx;
+    int rc = ctx.begin(opts);
+    if (rc != AZ_OK) return rc;
+    return Render(*scene->impl, film, camera, epsilons, scissor, filter_type, backface_culling, opts, ctx.stream, stats,
+                  g, train != 0);
+}
+
 extern "C" int az_gpu_closest_hit(az_gpu_scene *scene, const az_ray3 *rays, uint32_t count, int32_t cull,
                                   float hit_epsilon, uint32_t *out_hit, uint32_t *out_uid, uint32_t *out_face,
                                   float *out_t, const az_render_opts *opts) {

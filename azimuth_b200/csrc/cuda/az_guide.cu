@@ -1,0 +1,1005 @@
+// Neural path guiding: the network's kernels (hash-grid encoding, fully
+// fused MLP forward and backward on BF16 tensor cores, loss, Adam) and the
+// guided render driver.  Network and proposal are described in az_guide.cuh.
+//
+// The MLP runs warp-synchronously on 16 rows at a time with
+// mma.sync.m16n8k16 (BF16 inputs, FP32 accumulation): the accumulator
+// fragments of one layer are, after ReLU and conversion, exactly the A
+// fragments of the next, so activations stay in registers; weights sit in
+// shared memory already arranged as B fragments (one 8-byte load per lane
+// per 16x8 tile).  Training keeps each layer's input in shared memory for the
+// backward pass: dX = dY W^T on the tensor cores with a second, transposed
+// copy of the fragments, dW = X^T dY on the tensor cores with operands
+// gathered from the row-major copies and accumulated per block in shared
+// memory, and the encoding gradient scattered into the hash grid with
+// atomics.  Adam keeps FP32 master weights and refreshes the BF16 fragments
+// and the FP16 grid after every step.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "az_guide.cuh"
+#include "az_internal.h"
+#include "az_render.h"
+#include "az_shade.cuh"
+#include "azimuth_gpu.h"
+
+namespace az {
+namespace {
+
+using namespace azd;
+
+constexpr int W = GUIDE_WIDTH;
+constexpr int NW = GUIDE_LAYERS * W * W;             // MLP weights
+constexpr int NFRAG = GUIDE_LAYERS * 4 * 8 * 32;     // B fragments (uint2) per copy
+constexpr int XS = W + 8;                            // row stride (bf16) of the shared activation copies
+constexpr int OS = W + 4;                            // row stride (fp32) of the shared output rows
+constexpr int kWarps = 4;                            // warps per block of the network kernels
+
+// Parameters of the network as the kernels see them.
+struct GuideNetDev {
+    const uint2 *wf;          // forward B fragments [layer][kk][nn][lane]
+    const uint2 *wt;          // transposed B fragments for dX = dY W^T
+    const float *bias;        // output-layer bias [64]
+    const __half2 *grid;      // [level][GUIDE_T] features
+    uint32_t res[GUIDE_LEVELS];
+    float lo[3], inv_ext[3];  // position normalisation onto [0, 1]^3
+};
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+    __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<uint32_t *>(&v);
+}
+
+__device__ __forceinline__ float2 unpack_bf16(uint32_t u) {
+    __nv_bfloat162 v = *reinterpret_cast<__nv_bfloat162 *>(&u);
+    return __bfloat1622float2(v);
+}
+
+__device__ __forceinline__ void mma16816(float (&c)[4], const uint32_t *a, uint2 b) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b.x), "r"(b.y));
+}
+
+__device__ __forceinline__ f3 normalise_pos(const GuideNetDev &N, f3 p) {
+    return mk(fminf(1.0f, fmaxf(0.0f, (p.x - N.lo[0]) * N.inv_ext[0])),
+              fminf(1.0f, fmaxf(0.0f, (p.y - N.lo[1]) * N.inv_ext[1])),
+              fminf(1.0f, fmaxf(0.0f, (p.z - N.lo[2]) * N.inv_ext[2])));
+}
+
+// Trilinear corners of level l at normalised position p.
+struct Corners {
+    uint32_t idx[8];
+    float w[8];
+};
+
+__device__ __forceinline__ void grid_corners(const GuideNetDev &N, int l, f3 p, Corners &c) {
+    const uint32_t res = N.res[l];
+    const float fr = (float)res;
+    const float x = p.x * fr, y = p.y * fr, z = p.z * fr;
+    const uint32_t ix = min((uint32_t)x, res - 1u), iy = min((uint32_t)y, res - 1u), iz = min((uint32_t)z, res - 1u);
+    const float fx = x - (float)ix, fy = y - (float)iy, fz = z - (float)iz;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        const uint32_t dx = k & 1, dy = (k >> 1) & 1, dz = (k >> 2) & 1;
+        c.w[k] = (dx ? fx : 1.0f - fx) * (dy ? fy : 1.0f - fy) * (dz ? fz : 1.0f - fz);
+        c.idx[k] = (uint32_t)l * GUIDE_T + guide_index(ix + dx, iy + dy, iz + dz, res);
+    }
+}
+
+__device__ __forceinline__ float2 grid_feature(const GuideNetDev &N, int l, f3 p) {
+    Corners c;
+    grid_corners(N, l, p, c);
+    float2 f = make_float2(0.0f, 0.0f);
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        const float2 v = __half22float2(N.grid[c.idx[k]]);
+        f.x += c.w[k] * v.x;
+        f.y += c.w[k] * v.y;
+    }
+    return f;
+}
+
+// Network inputs of rows g and g + 8 of the warp's 16-row tile as the A
+// fragments of the first layer.  Input columns: 0..31 the hash-grid features
+// (level l at 2l, 2l+1), 32..34 the normal, 35..37 the outgoing direction,
+// 38 a constant 1, the rest 0.  Lane (g, t) holds, per row, columns 2t, 2t+1,
+// 2t+8, 2t+9 of each 16-column tile: grid levels t, t+4, t+8, t+12.
+__device__ __forceinline__ void encode_rows(const GuideNetDev &N, f3 p0, f3 n0, f3 o0, f3 p1, f3 n1, f3 o1,
+                                            uint32_t t, uint32_t (&act)[16]) {
+#pragma unroll
+    for (int kk = 0; kk < 2; kk++)
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int l = (int)t + 4 * h + 8 * kk;
+            const float2 a = grid_feature(N, l, p0), b = grid_feature(N, l, p1);
+            act[kk * 4 + 2 * h + 0] = pack_bf16(a.x, a.y);
+            act[kk * 4 + 2 * h + 1] = pack_bf16(b.x, b.y);
+        }
+    const float e0[8] = {n0.x, n0.y, n0.z, o0.x, o0.y, o0.z, 1.0f, 0.0f};
+    const float e1[8] = {n1.x, n1.y, n1.z, o1.x, o1.y, o1.z, 1.0f, 0.0f};
+    act[8] = pack_bf16(e0[2 * t], e0[2 * t + 1]);
+    act[9] = pack_bf16(e1[2 * t], e1[2 * t + 1]);
+    act[10] = act[11] = 0u;
+    act[12] = act[13] = act[14] = act[15] = 0u;
+}
+
+// One layer: acc (8 column tiles of 16x8) = A (16x64) * B (64x64).
+__device__ __forceinline__ void layer_mma(const uint32_t (&act)[16], const uint2 *frag, uint32_t lane,
+                                          float (&acc)[8][4]) {
+#pragma unroll
+    for (int nn = 0; nn < 8; nn++) {
+        acc[nn][0] = acc[nn][1] = acc[nn][2] = acc[nn][3] = 0.0f;
+#pragma unroll
+        for (int kk = 0; kk < 4; kk++) mma16816(acc[nn], &act[kk * 4], frag[(kk * 8 + nn) * 32 + lane]);
+    }
+}
+
+// Accumulators (D fragments) to the next layer's A fragments, after ReLU.
+__device__ __forceinline__ void relu_to_act(const float (&acc)[8][4], uint32_t (&act)[16]) {
+#pragma unroll
+    for (int kk = 0; kk < 4; kk++) {
+        act[kk * 4 + 0] = pack_bf16(fmaxf(acc[2 * kk][0], 0.0f), fmaxf(acc[2 * kk][1], 0.0f));
+        act[kk * 4 + 1] = pack_bf16(fmaxf(acc[2 * kk][2], 0.0f), fmaxf(acc[2 * kk][3], 0.0f));
+        act[kk * 4 + 2] = pack_bf16(fmaxf(acc[2 * kk + 1][0], 0.0f), fmaxf(acc[2 * kk + 1][1], 0.0f));
+        act[kk * 4 + 3] = pack_bf16(fmaxf(acc[2 * kk + 1][2], 0.0f), fmaxf(acc[2 * kk + 1][3], 0.0f));
+    }
+}
+
+// A fragments of a 16x64 tile to its row-major BF16 copy (row stride XS).
+__device__ __forceinline__ void store_act(const uint32_t (&act)[16], __nv_bfloat16 *X, uint32_t g, uint32_t t) {
+#pragma unroll
+    for (int kk = 0; kk < 4; kk++) {
+        *reinterpret_cast<uint32_t *>(X + g * XS + 16 * kk + 2 * t) = act[kk * 4 + 0];
+        *reinterpret_cast<uint32_t *>(X + (g + 8) * XS + 16 * kk + 2 * t) = act[kk * 4 + 1];
+        *reinterpret_cast<uint32_t *>(X + g * XS + 16 * kk + 2 * t + 8) = act[kk * 4 + 2];
+        *reinterpret_cast<uint32_t *>(X + (g + 8) * XS + 16 * kk + 2 * t + 8) = act[kk * 4 + 3];
+    }
+}
+
+// Output-layer accumulators plus bias to rows of `out` (row stride OS).
+__device__ __forceinline__ void store_out(const float (&acc)[8][4], const float *bias, float *out, uint32_t g,
+                                          uint32_t t) {
+#pragma unroll
+    for (int nn = 0; nn < 8; nn++) {
+        const int c = 8 * nn + 2 * t;
+        out[g * OS + c] = acc[nn][0] + bias[c];
+        out[g * OS + c + 1] = acc[nn][1] + bias[c + 1];
+        out[(g + 8) * OS + c] = acc[nn][2] + bias[c];
+        out[(g + 8) * OS + c + 1] = acc[nn][3] + bias[c + 1];
+    }
+}
+
+// Raw outputs of one row to the proposal (az_guide.cuh).
+__device__ void decode_lobes(const float *o, GuideLobes &G) {
+    float mx = -FLT_MAX;
+#pragma unroll
+    for (int k = 0; k < GUIDE_LOBES; k++) mx = fmaxf(mx, o[5 * k + 4]);
+    float e[GUIDE_LOBES], se = 0.0f;
+#pragma unroll
+    for (int k = 0; k < GUIDE_LOBES; k++) {
+        e[k] = __expf(o[5 * k + 4] - mx);
+        se += e[k];
+    }
+    float cum = 0.0f;
+#pragma unroll
+    for (int k = 0; k < GUIDE_LOBES; k++) {
+        const float m0 = o[5 * k], m1 = o[5 * k + 1], m2 = o[5 * k + 2];
+        const float inv = rsqrtf(m0 * m0 + m1 * m1 + m2 * m2 + 1e-12f);
+        const float kap = __expf(fminf(GUIDE_LOGK_MAX, fmaxf(GUIDE_LOGK_MIN, o[5 * k + 3])));
+        const float pk = e[k] / se;
+        G.mk[k] = make_float4(m0 * inv, m1 * inv, m2 * inv, kap);
+        G.c[k] = pk * kap / (2.0f * GUIDE_PI * -expm1f(-2.0f * kap));
+        cum += pk;
+        G.cdf[k] = cum;
+    }
+    G.cdf[GUIDE_LOBES - 1] = 1.0f;
+    const float s = 1.0f / (1.0f + __expf(-o[40]));
+    G.alpha = GUIDE_ALPHA_MIN + GUIDE_ALPHA_SPAN * s;
+    G.pad[0] = G.pad[1] = G.pad[2] = 0.0f;
+}
+
+// Loss -w log q(wi) of one row and its gradient with respect to the 41 raw
+// outputs (written to d[0..63], zeros past 40).
+__device__ float loss_grad(const float *o, f3 n, f3 wi, float w, float *d) {
+    float mx = -FLT_MAX;
+    for (int k = 0; k < GUIDE_LOBES; k++) mx = fmaxf(mx, o[5 * k + 4]);
+    float pi[GUIDE_LOBES], f[GUIDE_LOBES], mu[GUIDE_LOBES][3], len[GUIDE_LOBES], kap[GUIDE_LOBES], cw[GUIDE_LOBES];
+    bool inside[GUIDE_LOBES];
+    float se = 0.0f;
+    for (int k = 0; k < GUIDE_LOBES; k++) {
+        pi[k] = expf(o[5 * k + 4] - mx);
+        se += pi[k];
+    }
+    float qv = 0.0f;
+    for (int k = 0; k < GUIDE_LOBES; k++) {
+        pi[k] /= se;
+        const float m0 = o[5 * k], m1 = o[5 * k + 1], m2 = o[5 * k + 2];
+        len[k] = sqrtf(m0 * m0 + m1 * m1 + m2 * m2 + 1e-12f);
+        mu[k][0] = m0 / len[k];
+        mu[k][1] = m1 / len[k];
+        mu[k][2] = m2 / len[k];
+        const float lk = o[5 * k + 3];
+        inside[k] = lk > GUIDE_LOGK_MIN && lk < GUIDE_LOGK_MAX;
+        kap[k] = expf(fminf(GUIDE_LOGK_MAX, fmaxf(GUIDE_LOGK_MIN, lk)));
+        cw[k] = mu[k][0] * wi.x + mu[k][1] * wi.y + mu[k][2] * wi.z;
+        f[k] = kap[k] / (2.0f * GUIDE_PI * -expm1f(-2.0f * kap[k])) * expf(kap[k] * (cw[k] - 1.0f));
+        qv += pi[k] * f[k];
+    }
+    const float s = 1.0f / (1.0f + expf(-o[40]));
+    const float alpha = GUIDE_ALPHA_MIN + GUIDE_ALPHA_SPAN * s;
+    const float pc = fmaxf(0.0f, dot(n, wi)) / GUIDE_PI;
+    const float q = fmaxf(alpha * qv + (1.0f - alpha) * pc, 1e-30f);
+    const float g = -w / q;
+    for (int j = 0; j < W; j++) d[j] = 0.0f;
+    d[40] = g * (qv - pc) * GUIDE_ALPHA_SPAN * s * (1.0f - s);
+    float dotp = 0.0f;
+    float gp[GUIDE_LOBES];
+    for (int k = 0; k < GUIDE_LOBES; k++) {
+        gp[k] = g * alpha * f[k];
+        dotp += pi[k] * gp[k];
+    }
+    for (int k = 0; k < GUIDE_LOBES; k++) {
+        d[5 * k + 4] = pi[k] * (gp[k] - dotp);
+        const float gf = g * alpha * pi[k] * f[k];   // d loss / d log f_k
+        const float dlk = 1.0f / kap[k] - 2.0f / expm1f(2.0f * kap[k]) + (cw[k] - 1.0f);
+        d[5 * k + 3] = inside[k] ? gf * dlk * kap[k] : 0.0f;
+        const float gm0 = gf * kap[k] * wi.x, gm1 = gf * kap[k] * wi.y, gm2 = gf * kap[k] * wi.z;
+        const float pr = gm0 * mu[k][0] + gm1 * mu[k][1] + gm2 * mu[k][2];
+        d[5 * k + 0] = (gm0 - pr * mu[k][0]) / len[k];
+        d[5 * k + 1] = (gm1 - pr * mu[k][1]) / len[k];
+        d[5 * k + 2] = (gm2 - pr * mu[k][2]) / len[k];
+    }
+    return -w * logf(q);
+}
+
+// Column c of rows r0 and r1 of a row-major BF16 tile, packed (r0 in the low half).
+__device__ __forceinline__ uint32_t pack2(const __nv_bfloat16 *X, int r0, int r1, int c) {
+    const uint32_t a = *reinterpret_cast<const unsigned short *>(X + r0 * XS + c);
+    const uint32_t b = *reinterpret_cast<const unsigned short *>(X + r1 * XS + c);
+    return a | (b << 16);
+}
+
+__device__ __forceinline__ void load_frags(uint2 *dst, const uint2 *src) {
+    for (int i = threadIdx.x; i < NFRAG; i += blockDim.x) dst[i] = src[i];
+}
+
+// ---- inference over the extension queue of one level ----
+constexpr size_t kInferSmem = NFRAG * sizeof(uint2) + (size_t)kWarps * 16 * OS * sizeof(float) + W * sizeof(float);
+
+__global__ void __launch_bounds__(kWarps * 32) k_guide_infer(DevScene S, WaveQueues Q, uint32_t level, GuideNetDev N,
+                                                             GuideLobes *out) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    uint2 *s_wf = reinterpret_cast<uint2 *>(smem);
+    float *s_outs = reinterpret_cast<float *>(s_wf + NFRAG);
+    float *s_bias = s_outs + kWarps * 16 * OS;
+    load_frags(s_wf, N.wf);
+    for (int i = threadIdx.x; i < W; i += blockDim.x) s_bias[i] = N.bias[i];
+    __syncthreads();
+    const int buf = level & 1;
+    const uint32_t n = min(Q.counts[level], Q.cap_q);
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3u;
+    float *out_rows = s_outs + warp * 16 * OS;
+    const uint32_t tiles = (n + 15u) / 16u;
+    for (uint32_t tile = blockIdx.x * kWarps + warp; tile < tiles; tile += gridDim.x * kWarps) {
+        f3 p[2], nr[2], wo[2];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const uint32_t i = tile * 16u + g + 8u * h;
+            p[h] = nr[h] = wo[h] = mk(0.0f, 0.0f, 1.0f);
+            if (i < n) {
+                const uint4 hh = Q.hit[i];
+                const float4 o4 = Q.o[buf][i], d4 = Q.d[buf][i];
+                if (hh.w != 0xFFFFFFFFu) {
+                    Ray r;
+                    r.o = mk(o4.x, o4.y, o4.z);
+                    r.d = mk(d4.x, d4.y, d4.z);
+                    r.time = o4.w;
+                    Hit hit;
+                    hit.t = __uint_as_float(hh.x);
+                    hit.tl = __uint_as_float(hh.y);
+                    hit.prim = hh.z;
+                    hit.ent = hh.w;
+                    guide_query(S, r, hit, p[h], nr[h]);
+                    p[h] = normalise_pos(N, p[h]);
+                    wo[h] = -r.d;
+                }
+            }
+        }
+        uint32_t act[16];
+        encode_rows(N, p[0], nr[0], wo[0], p[1], nr[1], wo[1], t, act);
+        float acc[8][4];
+#pragma unroll
+        for (int l = 0; l < GUIDE_LAYERS; l++) {
+            layer_mma(act, s_wf + l * 4 * 8 * 32, lane, acc);
+            if (l + 1 < GUIDE_LAYERS) relu_to_act(acc, act);
+        }
+        store_out(acc, s_bias, out_rows, g, t);
+        __syncwarp();
+        if (lane < 16) {
+            const uint32_t i = tile * 16u + lane;
+            if (i < n) {
+                GuideLobes G;
+                decode_lobes(out_rows + lane * OS, G);
+                float4 *dst = reinterpret_cast<float4 *>(out + i);
+                const float4 *src = reinterpret_cast<const float4 *>(&G);
+#pragma unroll
+                for (int j = 0; j < 13; j++) dst[j] = src[j];
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// ---- training targets from the recorded vertices of a finished wave ----
+__global__ void k_guide_targets(const GuideRecord *rec, uint32_t n_rec, uint32_t levels, const float4 *accum,
+                                GuideRow *rows, uint32_t cap, uint32_t *count, float *wsum) {
+    const uint32_t total = n_rec * levels;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x) {
+        const GuideRecord R = rec[k];
+        if (R.tpc.w != 1.0f || R.snap.w != 1.0f || !(R.pos_q.w > 0.0f)) continue;
+        const float4 a = accum[k % n_rec];
+        // radiance along wi: what the child's subtree added, divided by its throughput
+        const float lx = R.tpc.x > 1e-20f ? (a.x - R.snap.x) / R.tpc.x : 0.0f;
+        const float ly = R.tpc.y > 1e-20f ? (a.y - R.snap.y) / R.tpc.y : 0.0f;
+        const float lz = R.tpc.z > 1e-20f ? (a.z - R.snap.z) / R.tpc.z : 0.0f;
+        const float lum = fmaxf(0.0f, 0.2126f * lx + 0.7152f * ly + 0.0722f * lz);
+        const float cs = fmaxf(0.0f, R.n.x * R.wi.x + R.n.y * R.wi.y + R.n.z * R.wi.z);
+        // KL objective toward the density proportional to L(wi) cos: weight F / q
+        const float w = lum * cs / R.pos_q.w;
+        if (!(w > 0.0f) || !isfinite(w)) continue;
+        const uint32_t j = atomicAdd(count, 1u);
+        if (j >= cap) continue;
+        atomicAdd(wsum, w);
+        GuideRow r;
+        r.pos_w = make_float4(R.pos_q.x, R.pos_q.y, R.pos_q.z, w);
+        r.n = R.n;
+        r.wo = R.wo;
+        r.wi = R.wi;
+        rows[j] = r;
+    }
+}
+
+// ---- forward, loss and backward over training rows ----
+// Gradients accumulate into w_grad (MLP), b_grad (output bias) and
+// grid_grad; the loss sum into *loss.  Weights are scaled by
+// count / wsum (mean weight 1).  Optional outputs for tests: raw outputs
+// (n x 64) and encoding gradients (n x 32).
+struct TrainArgs {
+    const GuideRow *rows;
+    const uint32_t *count;    // rows used: min(*count, cap)
+    uint32_t cap;
+    const float *wsum;        // null: weights used as given
+    float *w_grad, *b_grad;
+    float2 *grid_grad;
+    float *loss;
+    float *dbg_out, *dbg_enc;
+};
+
+constexpr size_t kTrainSmem = 2 * NFRAG * sizeof(uint2) + (size_t)GUIDE_LAYERS * W * W * sizeof(float) +
+                              W * sizeof(float) * 2 +
+                              (size_t)kWarps * ((GUIDE_LAYERS + 1) * 16 * XS * sizeof(__nv_bfloat16) +
+                                                16 * OS * sizeof(float));
+
+__global__ void __launch_bounds__(kWarps * 32) k_guide_train(GuideNetDev N, TrainArgs A) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    uint2 *s_wf = reinterpret_cast<uint2 *>(smem);
+    uint2 *s_wt = s_wf + NFRAG;
+    float *s_dw = reinterpret_cast<float *>(s_wt + NFRAG);
+    float *s_bias = s_dw + GUIDE_LAYERS * W * W;
+    float *s_db = s_bias + W;
+    unsigned char *per_warp = reinterpret_cast<unsigned char *>(s_db + W);
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3u;
+    const size_t warp_bytes = (GUIDE_LAYERS + 1) * 16 * XS * sizeof(__nv_bfloat16) + 16 * OS * sizeof(float);
+    __nv_bfloat16 *s_x = reinterpret_cast<__nv_bfloat16 *>(per_warp + warp * warp_bytes);   // [layer][16][XS]
+    __nv_bfloat16 *s_dy = s_x + GUIDE_LAYERS * 16 * XS;                                    // [16][XS]
+    float *s_o = reinterpret_cast<float *>(s_dy + 16 * XS);                                 // [16][OS]
+    load_frags(s_wf, N.wf);
+    load_frags(s_wt, N.wt);
+    for (int i = threadIdx.x; i < GUIDE_LAYERS * W * W; i += blockDim.x) s_dw[i] = 0.0f;
+    for (int i = threadIdx.x; i < W; i += blockDim.x) {
+        s_bias[i] = N.bias[i];
+        s_db[i] = 0.0f;
+    }
+    __syncthreads();
+    const uint32_t n = min(*A.count, A.cap);
+    const float wscale = A.wsum ? (float)n / fmaxf(*A.wsum, 1e-30f) : 1.0f;
+    float loss_acc = 0.0f;
+    const uint32_t tiles = (n + 15u) / 16u;
+    for (uint32_t tile = blockIdx.x * kWarps + warp; tile < tiles; tile += gridDim.x * kWarps) {
+        // ---- forward, keeping each layer's input ----
+        f3 p[2], nr[2], wo[2];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const uint32_t i = tile * 16u + g + 8u * h;
+            p[h] = nr[h] = wo[h] = mk(0.0f, 0.0f, 1.0f);
+            if (i < n) {
+                const GuideRow r = A.rows[i];
+                p[h] = normalise_pos(N, mk(r.pos_w.x, r.pos_w.y, r.pos_w.z));
+                nr[h] = mk(r.n.x, r.n.y, r.n.z);
+                wo[h] = mk(r.wo.x, r.wo.y, r.wo.z);
+            }
+        }
+        uint32_t act[16];
+        encode_rows(N, p[0], nr[0], wo[0], p[1], nr[1], wo[1], t, act);
+        float acc[8][4];
+#pragma unroll
+        for (int l = 0; l < GUIDE_LAYERS; l++) {
+            store_act(act, s_x + l * 16 * XS, g, t);
+            layer_mma(act, s_wf + l * 4 * 8 * 32, lane, acc);
+            if (l + 1 < GUIDE_LAYERS) relu_to_act(acc, act);
+        }
+        store_out(acc, s_bias, s_o, g, t);
+        __syncwarp();
+        // ---- loss and output gradient, one row per lane ----
+        if (lane < 16) {
+            const uint32_t i = tile * 16u + lane;
+            float *o = s_o + lane * OS;
+            if (A.dbg_out && i < n)
+                for (int j = 0; j < W; j++) A.dbg_out[(size_t)i * W + j] = o[j];
+            float d[W];
+            if (i < n) {
+                const GuideRow r = A.rows[i];
+                loss_acc += loss_grad(o, mk(r.n.x, r.n.y, r.n.z), mk(r.wi.x, r.wi.y, r.wi.z), r.pos_w.w * wscale, d);
+            } else {
+                for (int j = 0; j < W; j++) d[j] = 0.0f;
+            }
+            for (int j = 0; j < W; j++) o[j] = d[j];
+        }
+        __syncwarp();
+        // output-bias gradient and the BF16 row-major copy of dY
+        for (int j = lane; j < W; j += 32) {
+            float sacc = 0.0f;
+            for (int r = 0; r < 16; r++) sacc += s_o[r * OS + j];
+            atomicAdd(&s_db[j], sacc);
+        }
+        for (int e = lane; e < 16 * W; e += 32) {
+            const int r = e / W, c = e % W;
+            s_dy[r * XS + c] = __float2bfloat16_rn(s_o[r * OS + c]);
+        }
+        __syncwarp();
+        // dY of the output layer as A fragments
+        uint32_t dya[16];
+#pragma unroll
+        for (int kk = 0; kk < 4; kk++) {
+            dya[kk * 4 + 0] = *reinterpret_cast<const uint32_t *>(s_dy + g * XS + 16 * kk + 2 * t);
+            dya[kk * 4 + 1] = *reinterpret_cast<const uint32_t *>(s_dy + (g + 8) * XS + 16 * kk + 2 * t);
+            dya[kk * 4 + 2] = *reinterpret_cast<const uint32_t *>(s_dy + g * XS + 16 * kk + 2 * t + 8);
+            dya[kk * 4 + 3] = *reinterpret_cast<const uint32_t *>(s_dy + (g + 8) * XS + 16 * kk + 2 * t + 8);
+        }
+        // ---- backward through the layers ----
+        for (int l = GUIDE_LAYERS - 1; l >= 0; l--) {
+            const __nv_bfloat16 *X = s_x + l * 16 * XS;
+            // dW_l += X_l^T dY_l: M = input unit, K = row, N = output unit
+#pragma unroll
+            for (int mt = 0; mt < 4; mt++) {
+                const int c0 = 16 * mt + (int)g;
+                uint32_t a[4];
+                a[0] = pack2(X, 2 * t, 2 * t + 1, c0);
+                a[1] = pack2(X, 2 * t, 2 * t + 1, c0 + 8);
+                a[2] = pack2(X, 2 * t + 8, 2 * t + 9, c0);
+                a[3] = pack2(X, 2 * t + 8, 2 * t + 9, c0 + 8);
+#pragma unroll
+                for (int nn = 0; nn < 8; nn++) {
+                    const int oc = 8 * nn + (int)g;
+                    uint2 b;
+                    b.x = pack2(s_dy, 2 * t, 2 * t + 1, oc);
+                    b.y = pack2(s_dy, 2 * t + 8, 2 * t + 9, oc);
+                    float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+                    mma16816(c, a, b);
+                    float *dw = s_dw + l * W * W;
+                    const int col = 8 * nn + 2 * (int)t;
+                    atomicAdd(&dw[c0 * W + col], c[0]);
+                    atomicAdd(&dw[c0 * W + col + 1], c[1]);
+                    atomicAdd(&dw[(c0 + 8) * W + col], c[2]);
+                    atomicAdd(&dw[(c0 + 8) * W + col + 1], c[3]);
+                }
+            }
+            // dX_l = dY_l W_l^T
+            float dx[8][4];
+            layer_mma(dya, s_wt + l * 4 * 8 * 32, lane, dx);
+            __syncwarp();
+            if (l > 0) {
+                // through the ReLU that produced X_l: dY_{l-1} = dX_l where X_l > 0
+#pragma unroll
+                for (int kk = 0; kk < 4; kk++) {
+                    const float2 x00 = unpack_bf16(*reinterpret_cast<const uint32_t *>(X + g * XS + 16 * kk + 2 * t));
+                    const float2 x01 = unpack_bf16(*reinterpret_cast<const uint32_t *>(X + (g + 8) * XS + 16 * kk + 2 * t));
+                    const float2 x10 = unpack_bf16(*reinterpret_cast<const uint32_t *>(X + g * XS + 16 * kk + 2 * t + 8));
+                    const float2 x11 = unpack_bf16(*reinterpret_cast<const uint32_t *>(X + (g + 8) * XS + 16 * kk + 2 * t + 8));
+                    dya[kk * 4 + 0] = pack_bf16(x00.x > 0.0f ? dx[2 * kk][0] : 0.0f, x00.y > 0.0f ? dx[2 * kk][1] : 0.0f);
+                    dya[kk * 4 + 1] = pack_bf16(x01.x > 0.0f ? dx[2 * kk][2] : 0.0f, x01.y > 0.0f ? dx[2 * kk][3] : 0.0f);
+                    dya[kk * 4 + 2] = pack_bf16(x10.x > 0.0f ? dx[2 * kk + 1][0] : 0.0f, x10.y > 0.0f ? dx[2 * kk + 1][1] : 0.0f);
+                    dya[kk * 4 + 3] = pack_bf16(x11.x > 0.0f ? dx[2 * kk + 1][2] : 0.0f, x11.y > 0.0f ? dx[2 * kk + 1][3] : 0.0f);
+                }
+                store_act(dya, s_dy, g, t);
+                __syncwarp();
+            } else {
+                // encoding gradient: columns 0..31, level 4 nn + t at 8 nn + 2t
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const uint32_t i = tile * 16u + g + 8u * h;
+                    if (i >= n) continue;
+#pragma unroll
+                    for (int nn = 0; nn < 4; nn++) {
+                        const int lv = 4 * nn + (int)t;
+                        const float gx = dx[nn][2 * h], gy = dx[nn][2 * h + 1];
+                        if (A.dbg_enc) {
+                            A.dbg_enc[(size_t)i * 32 + 2 * lv] = gx;
+                            A.dbg_enc[(size_t)i * 32 + 2 * lv + 1] = gy;
+                        }
+                        if (A.grid_grad) {
+                            Corners c;
+                            grid_corners(N, lv, p[h], c);
+#pragma unroll
+                            for (int k = 0; k < 8; k++)
+                                atomicAdd(&A.grid_grad[c.idx[k]], make_float2(c.w[k] * gx, c.w[k] * gy));
+                        }
+                    }
+                }
+            }
+        }
+        __syncwarp();
+    }
+    if (lane < 16 && loss_acc != 0.0f) atomicAdd(A.loss, loss_acc);
+    __syncthreads();
+    for (int i = threadIdx.x; i < GUIDE_LAYERS * W * W; i += blockDim.x)
+        if (s_dw[i] != 0.0f) atomicAdd(&A.w_grad[i], s_dw[i]);
+    for (int i = threadIdx.x; i < W; i += blockDim.x)
+        if (s_db[i] != 0.0f) atomicAdd(&A.b_grad[i], s_db[i]);
+}
+
+// ---- Adam (Kingma, Ba 2015) with FP32 master weights; gradients are cleared ----
+struct AdamStep {
+    float lr, b1, b2, eps, c1, c2;   // c1, c2: bias corrections 1 / (1 - b^t)
+};
+
+__global__ void k_adam(float *w, float *g, float *m, float *v, uint32_t n, AdamStep a) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float gi = g[i];
+        g[i] = 0.0f;
+        const float mi = a.b1 * m[i] + (1.0f - a.b1) * gi, vi = a.b2 * v[i] + (1.0f - a.b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        w[i] -= a.lr * (mi * a.c1) / (sqrtf(vi * a.c2) + a.eps);
+    }
+}
+
+__global__ void k_adam_grid(float2 *w, float2 *g, float2 *m, float2 *v, __half2 *feat, uint32_t n, AdamStep a) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float2 gi = g[i];
+        if (gi.x == 0.0f && gi.y == 0.0f && m[i].x == 0.0f && m[i].y == 0.0f) continue;   // never touched
+        g[i] = make_float2(0.0f, 0.0f);
+        float2 mi = m[i], vi = v[i], wi = w[i];
+        mi.x = a.b1 * mi.x + (1.0f - a.b1) * gi.x;
+        mi.y = a.b1 * mi.y + (1.0f - a.b1) * gi.y;
+        vi.x = a.b2 * vi.x + (1.0f - a.b2) * gi.x * gi.x;
+        vi.y = a.b2 * vi.y + (1.0f - a.b2) * gi.y * gi.y;
+        wi.x -= a.lr * (mi.x * a.c1) / (sqrtf(vi.x * a.c2) + a.eps);
+        wi.y -= a.lr * (mi.y * a.c1) / (sqrtf(vi.y * a.c2) + a.eps);
+        m[i] = mi;
+        v[i] = vi;
+        w[i] = wi;
+        feat[i] = __float22half2_rn(wi);
+    }
+}
+
+// BF16 B fragments of every layer from the FP32 master weights W[l][k][n]:
+// forward (k = input unit, n = output unit) and transposed (for dY W^T).
+__global__ void k_frags(const float *w, uint2 *wf, uint2 *wt) {
+    const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (uint32_t)NFRAG) return;
+    const uint32_t lane = idx & 31u, nn = (idx >> 5) & 7u, kk = (idx >> 8) & 3u, l = idx >> 10;
+    const uint32_t g = lane >> 2, t = lane & 3u;
+    const float *Wl = w + l * W * W;
+    const uint32_t k0 = 16 * kk + 2 * t, c = 8 * nn + g;
+    wf[idx] = make_uint2(pack_bf16(Wl[k0 * W + c], Wl[(k0 + 1) * W + c]),
+                         pack_bf16(Wl[(k0 + 8) * W + c], Wl[(k0 + 9) * W + c]));
+    wt[idx] = make_uint2(pack_bf16(Wl[c * W + k0], Wl[c * W + k0 + 1]), pack_bf16(Wl[c * W + k0 + 8], Wl[c * W + k0 + 9]));
+}
+
+__global__ void k_half_grid(const float2 *w, __half2 *feat, uint32_t n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        feat[i] = __float22half2_rn(w[i]);
+}
+
+constexpr uint32_t kGridN = GUIDE_LEVELS * GUIDE_T;   // float2 entries of the grid
+
+// SplitMix64 for the seeded initialisation.
+struct InitRng {
+    uint64_t s;
+    uint64_t next() {
+        uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        return z ^ (z >> 31);
+    }
+    float uniform(float a, float b) { return a + (b - a) * (float)((next() >> 11) * (1.0 / 9007199254740992.0)); }
+};
+
+}  // namespace
+
+struct GuideState {
+    int device = 0;
+    GuideNetDev net{};
+    float *w = nullptr, *w_grad = nullptr, *w_m = nullptr, *w_v = nullptr;
+    float *bias = nullptr, *b_grad = nullptr, *b_m = nullptr, *b_v = nullptr;
+    uint2 *wf = nullptr, *wt = nullptr;
+    __half2 *feat = nullptr;
+    float2 *grid = nullptr, *grid_grad = nullptr, *grid_m = nullptr, *grid_v = nullptr;
+    GuideLobes *lobes = nullptr;
+    size_t lobes_cap = 0;
+    GuideRecord *rec = nullptr;
+    uint32_t n_rec = 0, rec_levels = 0;
+    GuideRow *rows = nullptr;
+    uint32_t rows_cap = 0;
+    uint32_t *count = nullptr;      // [0] rows, then scratch
+    float *wsum = nullptr, *loss = nullptr;
+    float lr = 1e-2f;
+    uint32_t step = 0;
+    uint64_t trained_rows = 0;
+    float last_loss = 0.0f;
+    std::vector<void *> allocs;
+    int sms = 148;
+
+    ~GuideState() {
+        for (void *p : allocs)
+            if (p) cudaFree(p);
+        if (lobes) cudaFree(lobes);
+        if (rec) cudaFree(rec);
+    }
+    template <typename T>
+    T *Alloc(size_t n) {
+        void *p = nullptr;
+        if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) return nullptr;
+        allocs.push_back(p);
+        return (T *)p;
+    }
+};
+
+namespace {
+
+// World bounds of the scene from its top-level root node.
+void SceneBounds(const GpuScene &G, float lo[3], float hi[3]) {
+    for (int a = 0; a < 3; a++) {
+        lo[a] = -1.0f;
+        hi[a] = 1.0f;
+    }
+    if (G.dev.tlas_root == 0xFFFFFFFFu) return;
+    WideNode n;
+    if (cudaMemcpy(&n, G.dev.wnodes + G.dev.tlas_root, sizeof(n), cudaMemcpyDeviceToHost) != cudaSuccess) return;
+    const float p[3] = {n.px, n.py, n.pz};
+    const uint8_t e[3] = {n.ex, n.ey, n.ez};
+    const uint8_t *ql[3] = {n.qlo_x, n.qlo_y, n.qlo_z}, *qh[3] = {n.qhi_x, n.qhi_y, n.qhi_z};
+    double l[3] = {1e30, 1e30, 1e30}, h[3] = {-1e30, -1e30, -1e30};
+    for (int s = 0; s < 8; s++) {
+        if (!((n.imask >> s) & 1u) && n.meta[s] == 0) continue;   // empty slot
+        for (int a = 0; a < 3; a++) {
+            const double step = std::ldexp(1.0, (int)e[a] - 127);
+            l[a] = std::min(l[a], (double)p[a] + ql[a][s] * step);
+            h[a] = std::max(h[a], (double)p[a] + qh[a][s] * step);
+        }
+    }
+    for (int a = 0; a < 3; a++)
+        if (l[a] < h[a]) {
+            lo[a] = (float)l[a];
+            hi[a] = (float)h[a];
+        }
+}
+
+int RefreshFragments(GuideState &g, cudaStream_t st) {
+    k_frags<<<(NFRAG + 255) / 256, 256, 0, st>>>(g.w, g.wf, g.wt);
+    AZ_CUDA_TRY(cudaGetLastError());
+    return AZ_OK;
+}
+
+// One training step over rows[0 .. min(*count, cap)): gradients, then Adam.
+int TrainStep(GuideState &g, const GuideRow *rows, const uint32_t *count, uint32_t cap, const float *wsum,
+              cudaStream_t st, float *dbg_out = nullptr, float *dbg_enc = nullptr, bool apply = true) {
+    TrainArgs A;
+    A.rows = rows;
+    A.count = count;
+    A.cap = cap;
+    A.wsum = wsum;
+    A.w_grad = g.w_grad;
+    A.b_grad = g.b_grad;
+    A.grid_grad = g.grid_grad;
+    A.loss = g.loss;
+    A.dbg_out = dbg_out;
+    A.dbg_enc = dbg_enc;
+    AZ_CUDA_TRY(cudaMemsetAsync(g.loss, 0, sizeof(float), st));
+    k_guide_train<<<g.sms, kWarps * 32, kTrainSmem, st>>>(g.net, A);
+    AZ_CUDA_TRY(cudaGetLastError());
+    if (!apply) return AZ_OK;
+    g.step++;
+    AdamStep a;
+    a.lr = g.lr;
+    a.b1 = 0.9f;
+    a.b2 = 0.99f;
+    a.eps = 1e-8f;
+    a.c1 = (float)(1.0 / (1.0 - std::pow(0.9, (double)g.step)));
+    a.c2 = (float)(1.0 / (1.0 - std::pow(0.99, (double)g.step)));
+    k_adam<<<16, 256, 0, st>>>(g.w, g.w_grad, g.w_m, g.w_v, NW, a);
+    k_adam<<<1, 64, 0, st>>>(g.bias, g.b_grad, g.b_m, g.b_v, W, a);
+    k_adam_grid<<<g.sms * 8, 256, 0, st>>>(g.grid, g.grid_grad, g.grid_m, g.grid_v, g.feat, kGridN, a);
+    AZ_CUDA_TRY(cudaGetLastError());
+    return RefreshFragments(g, st);
+}
+
+}  // namespace
+
+int CreateGuide(const GpuScene &G, const az_guide_config *cfg, GuideState **out) {
+    std::unique_ptr<GuideState> g(new GuideState());
+    g->device = G.device;
+    cudaDeviceGetAttribute(&g->sms, cudaDevAttrMultiProcessorCount, G.device);
+    g->lr = cfg && cfg->learning_rate > 0.0f ? cfg->learning_rate : 1e-2f;
+    g->n_rec = cfg && cfg->record_samples ? cfg->record_samples : (1u << 16);
+    g->rows_cap = cfg && cfg->train_batch ? cfg->train_batch : (1u << 18);
+    const uint64_t seed = cfg ? cfg->seed : 0;
+    g->w = g->Alloc<float>(NW);
+    g->w_grad = g->Alloc<float>(NW);
+    g->w_m = g->Alloc<float>(NW);
+    g->w_v = g->Alloc<float>(NW);
+    g->bias = g->Alloc<float>(W);
+    g->b_grad = g->Alloc<float>(W);
+    g->b_m = g->Alloc<float>(W);
+    g->b_v = g->Alloc<float>(W);
+    g->wf = g->Alloc<uint2>(NFRAG);
+    g->wt = g->Alloc<uint2>(NFRAG);
+    g->feat = g->Alloc<__half2>(kGridN);
+    g->grid = g->Alloc<float2>(kGridN);
+    g->grid_grad = g->Alloc<float2>(kGridN);
+    g->grid_m = g->Alloc<float2>(kGridN);
+    g->grid_v = g->Alloc<float2>(kGridN);
+    g->rows = g->Alloc<GuideRow>(g->rows_cap);
+    g->count = g->Alloc<uint32_t>(4);
+    g->wsum = g->Alloc<float>(1);
+    g->loss = g->Alloc<float>(1);
+    for (void *p : g->allocs)
+        if (!p) return SetError(AZ_ERR_OUT_OF_MEMORY, "path guide parameters");
+    // Xavier-uniform weights, small uniform grid features; output biases
+    // start at kappa = e and alpha = 0.05 + 0.9 sigmoid(-2) (mostly cosine
+    // sampling until the network has learned something)
+    InitRng r{seed * 0x2545F4914F6CDD1Dull + 0x1234567ull};
+    std::vector<float> w(NW), b(W, 0.0f);
+    const float lim = std::sqrt(6.0f / (W + W));
+    for (int i = 0; i < NW; i++) w[i] = r.uniform(-lim, lim);
+    for (int k = 0; k < GUIDE_LOBES; k++) b[5 * k + 3] = 1.0f;
+    b[40] = -2.0f;
+    std::vector<float2> grid(kGridN);
+    for (uint32_t i = 0; i < kGridN; i++) grid[i] = make_float2(r.uniform(-1e-4f, 1e-4f), r.uniform(-1e-4f, 1e-4f));
+    AZ_CUDA_TRY(cudaMemcpy(g->w, w.data(), NW * sizeof(float), cudaMemcpyHostToDevice));
+    AZ_CUDA_TRY(cudaMemcpy(g->bias, b.data(), W * sizeof(float), cudaMemcpyHostToDevice));
+    AZ_CUDA_TRY(cudaMemcpy(g->grid, grid.data(), kGridN * sizeof(float2), cudaMemcpyHostToDevice));
+    AZ_CUDA_TRY(cudaMemset(g->w_grad, 0, NW * sizeof(float)));
+    AZ_CUDA_TRY(cudaMemset(g->w_m, 0, NW * sizeof(float)));
+    AZ_CUDA_TRY(cudaMemset(g->w_v, 0, NW * sizeof(float)));
+    AZ_CUDA_TRY(cudaMemset(g->b_grad, 0, W * sizeof(float)));
+    AZ_CUDA_TRY(cudaMemset(g->b_m, 0, W * sizeof(float)));
+    AZ_CUDA_TRY(cudaMemset(g->b_v, 0, W * sizeof(float)));
+    AZ_CUDA_TRY(cudaMemset(g->grid_grad, 0, kGridN * sizeof(float2)));
+    AZ_CUDA_TRY(cudaMemset(g->grid_m, 0, kGridN * sizeof(float2)));
+    AZ_CUDA_TRY(cudaMemset(g->grid_v, 0, kGridN * sizeof(float2)));
+    k_half_grid<<<g->sms * 8, 256>>>(g->grid, g->feat, kGridN);
+    int rc = RefreshFragments(*g, nullptr);
+    if (rc != AZ_OK) return rc;
+    AZ_CUDA_TRY(cudaFuncSetAttribute(k_guide_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrainSmem));
+    AZ_CUDA_TRY(cudaFuncSetAttribute(k_guide_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInferSmem));
+    // network view
+    g->net.wf = g->wf;
+    g->net.wt = g->wt;
+    g->net.bias = g->bias;
+    g->net.grid = g->feat;
+    for (int l = 0; l < GUIDE_LEVELS; l++) g->net.res[l] = (uint32_t)std::floor(16.0 * std::pow(2.0, 7.0 * l / 15.0));
+    float lo[3], hi[3];
+    SceneBounds(G, lo, hi);
+    for (int a = 0; a < 3; a++) {
+        const float ext = std::max(hi[a] - lo[a], 1e-6f);
+        g->net.lo[a] = lo[a];
+        g->net.inv_ext[a] = 1.0f / ext;
+    }
+    AZ_CUDA_TRY(cudaDeviceSynchronize());
+    *out = g.release();
+    return AZ_OK;
+}
+
+void DestroyGuide(GuideState *g) { delete g; }
+
+int GuidePrepareWave(GuideState &g, WaveQueues &Q, uint32_t cap_q, uint32_t levels, cudaStream_t st) {
+    if (g.lobes_cap < cap_q) {
+        if (g.lobes) cudaFree(g.lobes);
+        g.lobes = nullptr;
+        g.lobes_cap = 0;
+        if (cudaMalloc((void **)&g.lobes, (size_t)cap_q * sizeof(GuideLobes)) != cudaSuccess)
+            return SetError(AZ_ERR_OUT_OF_MEMORY, "path guide proposals");
+        g.lobes_cap = cap_q;
+    }
+    Q.lobes = g.lobes;
+    Q.rec = nullptr;
+    Q.n_rec = 0;
+    Q.rec_levels = 0;
+    if (levels == 0) return AZ_OK;   // not training: no records
+    if (g.rec_levels < levels) {
+        if (g.rec) cudaFree(g.rec);
+        g.rec = nullptr;
+        g.rec_levels = 0;
+        if (cudaMalloc((void **)&g.rec, (size_t)levels * g.n_rec * sizeof(GuideRecord)) != cudaSuccess)
+            return SetError(AZ_ERR_OUT_OF_MEMORY, "path guide records");
+        g.rec_levels = levels;
+    }
+    // records of earlier waves must not be mistaken for this wave's
+    AZ_CUDA_TRY(cudaMemsetAsync(g.rec, 0, (size_t)g.rec_levels * g.n_rec * sizeof(GuideRecord), st));
+    Q.rec = g.rec;
+    Q.n_rec = g.n_rec;
+    Q.rec_levels = g.rec_levels;
+    return AZ_OK;
+}
+
+int GuideInfer(GuideState &g, const GpuScene &G, const WaveQueues &Q, uint32_t level, cudaStream_t st) {
+    k_guide_infer<<<g.sms * 4, kWarps * 32, kInferSmem, st>>>(G.dev, Q, level, g.net, g.lobes);
+    AZ_CUDA_TRY(cudaGetLastError());
+    return AZ_OK;
+}
+
+int GuideTrainWave(GuideState &g, const WaveQueues &Q, cudaStream_t st) {
+    AZ_CUDA_TRY(cudaMemsetAsync(g.count, 0, 4 * sizeof(uint32_t), st));
+    AZ_CUDA_TRY(cudaMemsetAsync(g.wsum, 0, sizeof(float), st));
+    k_guide_targets<<<g.sms * 4, 256, 0, st>>>(g.rec, g.n_rec, g.rec_levels, Q.accum, g.rows, g.rows_cap, g.count,
+                                               g.wsum);
+    AZ_CUDA_TRY(cudaGetLastError());
+    return TrainStep(g, g.rows, g.count, g.rows_cap, g.wsum, st);
+}
+
+}  // namespace az
+
+using namespace az;
+
+struct az_guide {
+    GuideState *impl;
+};
+
+namespace az {
+GuideState *GuideOf(az_guide *g) { return g ? g->impl : nullptr; }
+}  // namespace az
+
+extern "C" int az_guide_create(az_gpu_scene *scene, const az_guide_config *cfg, az_guide **out) {
+    if (!scene || !scene->impl || !out) return SetError(AZ_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    AZ_CUDA_TRY(cudaSetDevice(scene->impl->device));
+    GuideState *g = nullptr;
+    int rc = CreateGuide(*scene->impl, cfg, &g);
+    if (rc != AZ_OK) return rc;
+    *out = new az_guide{g};
+    return AZ_OK;
+}
+
+extern "C" void az_guide_destroy(az_guide *g) {
+    if (!g) return;
+    cudaSetDevice(g->impl->device);
+    cudaDeviceSynchronize();
+    DestroyGuide(g->impl);
+    delete g;
+}
+
+extern "C" int az_guide_info(az_guide *g, uint32_t *res, float *lo, float *inv_ext, uint32_t *steps) {
+    if (!g) return SetError(AZ_ERR_INVALID_ARGUMENT, "null guide");
+    for (int l = 0; l < GUIDE_LEVELS && res; l++) res[l] = g->impl->net.res[l];
+    for (int a = 0; a < 3; a++) {
+        if (lo) lo[a] = g->impl->net.lo[a];
+        if (inv_ext) inv_ext[a] = g->impl->net.inv_ext[a];
+    }
+    if (steps) *steps = g->impl->step;
+    return AZ_OK;
+}
+
+extern "C" int az_guide_get_params(az_guide *g, float *mlp, float *bias, float *grid) {
+    if (!g) return SetError(AZ_ERR_INVALID_ARGUMENT, "null guide");
+    GuideState &s = *g->impl;
+    AZ_CUDA_TRY(cudaSetDevice(s.device));
+    AZ_CUDA_TRY(cudaDeviceSynchronize());
+    if (mlp) AZ_CUDA_TRY(cudaMemcpy(mlp, s.w, NW * sizeof(float), cudaMemcpyDeviceToHost));
+    if (bias) AZ_CUDA_TRY(cudaMemcpy(bias, s.bias, W * sizeof(float), cudaMemcpyDeviceToHost));
+    if (grid) AZ_CUDA_TRY(cudaMemcpy(grid, s.grid, kGridN * sizeof(float2), cudaMemcpyDeviceToHost));
+    return AZ_OK;
+}
+
+extern "C" int az_guide_set_params(az_guide *g, const float *mlp, const float *bias, const float *grid) {
+    if (!g) return SetError(AZ_ERR_INVALID_ARGUMENT, "null guide");
+    GuideState &s = *g->impl;
+    AZ_CUDA_TRY(cudaSetDevice(s.device));
+    AZ_CUDA_TRY(cudaDeviceSynchronize());
+    if (mlp) AZ_CUDA_TRY(cudaMemcpy(s.w, mlp, NW * sizeof(float), cudaMemcpyHostToDevice));
+    if (bias) AZ_CUDA_TRY(cudaMemcpy(s.bias, bias, W * sizeof(float), cudaMemcpyHostToDevice));
+    if (grid) {
+        AZ_CUDA_TRY(cudaMemcpy(s.grid, grid, kGridN * sizeof(float2), cudaMemcpyHostToDevice));
+        k_half_grid<<<s.sms * 8, 256>>>(s.grid, s.feat, kGridN);
+    }
+    int rc = RefreshFragments(s, nullptr);
+    if (rc != AZ_OK) return rc;
+    AZ_CUDA_TRY(cudaDeviceSynchronize());
+    return AZ_OK;
+}
+
+// Rows are host arrays of 16 floats: position, weight, normal, 0, outgoing
+// direction, 0, incident direction, 0 (the GuideRow layout).
+static int UploadRows(GuideState &s, const float *rows, uint32_t n, GuideRow **d_rows, uint32_t **d_count) {
+    *d_rows = nullptr;
+    *d_count = nullptr;
+    AZ_CUDA_TRY(cudaMalloc((void **)d_rows, std::max<size_t>(n, 1) * sizeof(GuideRow)));
+    AZ_CUDA_TRY(cudaMalloc((void **)d_count, sizeof(uint32_t)));
+    AZ_CUDA_TRY(cudaMemcpy(*d_rows, rows, (size_t)n * sizeof(GuideRow), cudaMemcpyHostToDevice));
+    AZ_CUDA_TRY(cudaMemcpy(*d_count, &n, sizeof(uint32_t), cudaMemcpyHostToDevice));
+    return AZ_OK;
+}
+
+extern "C" int az_guide_eval(az_guide *g, const float *rows, uint32_t n, float *outputs, float *loss,
+                             float *mlp_grad, float *bias_grad, float *enc_grad) {
+    if (!g || (n && !rows)) return SetError(AZ_ERR_INVALID_ARGUMENT, "null argument");
+    GuideState &s = *g->impl;
+    AZ_CUDA_TRY(cudaSetDevice(s.device));
+    GuideRow *d_rows = nullptr;
+    uint32_t *d_count = nullptr;
+    float *d_out = nullptr, *d_enc = nullptr;
+    int rc = UploadRows(s, rows, n, &d_rows, &d_count);
+    if (rc == AZ_OK && outputs && cudaMalloc((void **)&d_out, std::max<size_t>(n, 1) * W * sizeof(float)) != cudaSuccess)
+        rc = SetError(AZ_ERR_OUT_OF_MEMORY, "eval outputs");
+    if (rc == AZ_OK && enc_grad && cudaMalloc((void **)&d_enc, std::max<size_t>(n, 1) * 32 * sizeof(float)) != cudaSuccess)
+        rc = SetError(AZ_ERR_OUT_OF_MEMORY, "eval gradients");
+    if (rc == AZ_OK) {
+        cudaMemset(s.w_grad, 0, NW * sizeof(float));
+        cudaMemset(s.b_grad, 0, W * sizeof(float));
+        // the grid gradient is not needed here: pass none
+        float2 *gg = s.grid_grad;
+        s.grid_grad = nullptr;
+        rc = TrainStep(s, d_rows, d_count, n, nullptr, nullptr, d_out, d_enc, false);
+        s.grid_grad = gg;
+    }
+    if (rc == AZ_OK) {
+        cudaError_t e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) rc = CudaError(e, "guide eval");
+    }
+    if (rc == AZ_OK && outputs) cudaMemcpy(outputs, d_out, (size_t)n * W * sizeof(float), cudaMemcpyDeviceToHost);
+    if (rc == AZ_OK && enc_grad) cudaMemcpy(enc_grad, d_enc, (size_t)n * 32 * sizeof(float), cudaMemcpyDeviceToHost);
+    if (rc == AZ_OK && loss) cudaMemcpy(loss, s.loss, sizeof(float), cudaMemcpyDeviceToHost);
+    if (rc == AZ_OK && mlp_grad) cudaMemcpy(mlp_grad, s.w_grad, NW * sizeof(float), cudaMemcpyDeviceToHost);
+    if (rc == AZ_OK && bias_grad) cudaMemcpy(bias_grad, s.b_grad, W * sizeof(float), cudaMemcpyDeviceToHost);
+    cudaMemset(s.w_grad, 0, NW * sizeof(float));
+    cudaMemset(s.b_grad, 0, W * sizeof(float));
+    cudaFree(d_rows);
+    cudaFree(d_count);
+    if (d_out) cudaFree(d_out);
+    if (d_enc) cudaFree(d_enc);
+    return rc;
+}
+
+extern "C" int az_guide_train(az_guide *g, const float *rows, uint32_t n, uint32_t steps, float *losses) {
+    if (!g || (n && !rows)) return SetError(AZ_ERR_INVALID_ARGUMENT, "null argument");
+    GuideState &s = *g->impl;
+    AZ_CUDA_TRY(cudaSetDevice(s.device));
+    GuideRow *d_rows = nullptr;
+    uint32_t *d_count = nullptr;
+    int rc = UploadRows(s, rows, n, &d_rows, &d_count);
+    for (uint32_t k = 0; k < steps && rc == AZ_OK; k++) {
+        rc = TrainStep(s, d_rows, d_count, n, nullptr, nullptr);
+        if (rc == AZ_OK && losses) {
+            cudaError_t e = cudaMemcpy(&losses[k], s.loss, sizeof(float), cudaMemcpyDeviceToHost);
+            if (e != cudaSuccess) rc = CudaError(e, "guide train");
+        }
+    }
+    if (rc == AZ_OK) {
+        cudaError_t e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) rc = CudaError(e, "guide train");
+    }
+    cudaFree(d_rows);
+    cudaFree(d_count);
+    return rc;
+}

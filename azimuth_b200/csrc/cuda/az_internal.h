@@ -67,8 +67,24 @@ int CollapseToWide(const std::vector<azd::BVHNode> &bin, uint32_t bin_base, uint
 
 int SetupCamera(const az_camera *c, az_scissor sc, int32_t filter, uint32_t cull, const az_epsilon_values *eps,
                 uint64_t seed, CameraParams &cam);
+// Path guide (az_guide.cu): network state and the hooks of a guided render.
+struct GuideState;
+int CreateGuide(const GpuScene &G, const az_guide_config *cfg, GuideState **out);
+void DestroyGuide(GuideState *g);
+// Proposal and training-record buffers of a wave with `cap_q` queue entries
+// and `levels` tree levels; sets the guide fields of Q.
+int GuidePrepareWave(GuideState &g, WaveQueues &Q, uint32_t cap_q, uint32_t levels, cudaStream_t st);
+// Proposals for the extension queue of `level` (between extend and shade).
+int GuideInfer(GuideState &g, const GpuScene &G, const WaveQueues &Q, uint32_t level, cudaStream_t st);
+// Training targets of the finished wave and one Adam step.
+int GuideTrainWave(GuideState &g, const WaveQueues &Q, cudaStream_t st);
+GuideState *GuideOf(az_guide *g);
+
+// `guide` (may be null) steers the scattering direction; `train` also
+// updates the network after every wave.
 int Render(GpuScene &G, az_pixel *film, const az_camera *camera, const az_epsilon_values *eps, az_scissor sc,
-           int32_t filter, uint32_t cull, const az_render_opts *opts, cudaStream_t st, az_render_stats *stats);
+           int32_t filter, uint32_t cull, const az_render_opts *opts, cudaStream_t st, az_render_stats *stats,
+           GuideState *guide = nullptr, bool train = false);
 int Autotune(GpuScene &G, const az_camera *camera, const az_epsilon_values *eps, az_scissor sc, int32_t filter,
              uint32_t cull, const az_render_opts *opts, cudaStream_t st, uint32_t *best_out, float *ms_out);
 int ClosestHit(GpuScene &G, const az_ray3 *rays, uint32_t n, int32_t cull, float eps, uint32_t *out_hit,

@@ -45,7 +45,9 @@ enum : uint32_t {
 };
 
 // flags packed into d.w of a path entry
-enum : uint32_t { PF_INSIDE = 1u, PF_ATTEN = 2u };
+// PF_BRANCHED: an ancestor vertex spawned more than one child (its
+// descendants are not used for training the path guide)
+enum : uint32_t { PF_INSIDE = 1u, PF_ATTEN = 2u, PF_BRANCHED = 4u };
 
 __host__ __device__ __forceinline__ void sample_of(const CameraParams &cam, uint64_t s, uint32_t &row,
                                                    uint32_t &col, uint32_t &sx, uint32_t &sy) {
@@ -284,6 +286,14 @@ __global__ void __launch_bounds__(BLOCK) k_shade(DevScene S, CameraParams cam, W
         h.ent = hh.w;
         uint32_t row, col, sx, sy;
         sample_of(cam, wave_start + slot, row, col, sx, sy);
+        // path-guide training: this node is the only child of the vertex recorded
+        // one level up, so the sample's sum now holds everything up to that
+        // vertex's level
+        const bool recordable = Q.rec && slot < Q.n_rec && !(flags & PF_BRANCHED);
+        if (recordable && level >= 2 && level - 2 < Q.rec_levels) {
+            const float4 a = Q.accum[slot];
+            Q.rec[(size_t)(level - 2) * Q.n_rec + slot].snap = make_float4(a.x, a.y, a.z, 1.0f);
+        }
         if (h.ent == 0xFFFFFFFFu) {
             // a miss returns 0, except for the primary ray, whose sample then takes
             // the background (RayTravelDistance == 0, src/azimuth_main.cpp:1374-1384)
@@ -395,29 +405,67 @@ __global__ void __launch_bounds__(BLOCK) k_shade(DevScene S, CameraParams cam, W
             }
         }
         uint32_t next_child = 0;
+        // a vertex that may spawn more than one child marks its subtree
+        const bool multi = SPECIAL && S.path_trace && (m.is_mirror || m.transparent);
+        const uint32_t bflag = ((flags & PF_BRANCHED) || multi) ? PF_BRANCHED : 0u;
         if (S.path_trace) {
             // diffuse scatter ray (:1029-1083): child 0
-            float theta = S.importance_sampling ? asinf(sqrtf(rng.next())) : acosf(rng.next());
-            float ct = cosf(theta), st = sinf(theta);
-            float phi = 2.0f * AZD_PI_F32 * rng.next();
-            float cp = cosf(phi), sp = sinf(phi);
-            f3 U, V;
-            onb(s.n, U, V);
-            f3 Sd = normalize(U * st * cp + V * st * sp + s.n * ct);
-            float invpdf;
-            if (S.importance_sampling) {
-                float cs = dot(Sd, s.n);
-                if (cs == 0.0f) cs = 0.000001f;
-                invpdf = AZD_PI_F32 / cs;
+            f3 Sd;
+            float invpdf, qpdf = 0.0f;
+            if (Q.lobes) {
+                // path guiding: one-sample MIS of the learned vMF mixture and
+                // cosine sampling, weighted by the mixture density
+                const GuideLobes &G = Q.lobes[i];
+                const float us = rng.next();
+                if (us < G.alpha) {
+                    const int k = guide_pick_lobe(G, rng.next());
+                    const float u1 = rng.next();
+                    Sd = guide_sample_lobe(G, k, u1, rng.next());
+                } else {
+                    const float theta = asinf(sqrtf(rng.next()));
+                    const float phi = 2.0f * AZD_PI_F32 * rng.next();
+                    f3 U, V;
+                    onb(s.n, U, V);
+                    Sd = normalize(U * (sinf(theta) * cosf(phi)) + V * (sinf(theta) * sinf(phi)) + s.n * cosf(theta));
+                }
+                qpdf = guide_mixture_pdf(G, s.n, Sd);
+                invpdf = qpdf > 0.0f ? 1.0f / qpdf : 0.0f;
             } else {
-                invpdf = AZD_PI_F32 * 2.0f;
+                float theta = S.importance_sampling ? asinf(sqrtf(rng.next())) : acosf(rng.next());
+                float ct = cosf(theta), st = sinf(theta);
+                float phi = 2.0f * AZD_PI_F32 * rng.next();
+                float cp = cosf(phi), sp = sinf(phi);
+                f3 U, V;
+                onb(s.n, U, V);
+                Sd = normalize(U * st * cp + V * st * sp + s.n * ct);
+                if (S.importance_sampling) {
+                    float cs = dot(Sd, s.n);
+                    if (cs == 0.0f) cs = 0.000001f;
+                    invpdf = AZD_PI_F32 / cs;
+                } else {
+                    invpdf = AZD_PI_F32 * 2.0f;
+                }
             }
-            f3 dc, sc;
-            if (can_spawn && light_contribution(dc, sc, m, mk(1.0f, 1.0f, 1.0f), Sd, r.d, s.n, 1.0f, 1.0f, invpdf)) {
-                f3 ctp = had(tp, had(dcol, dc) + had(scol, sc));
-                if (!is_zero(ctp))
-                    push_path(Q, nbuf, level + 1, s.p + (Sd * seps), r.time, Sd, flags & PF_INSIDE, ctp, slot,
-                              mk(0.0f, 0.0f, 0.0f), child_digits(digits, level, 0));
+            f3 dc, sc, ctp = mk(0.0f, 0.0f, 0.0f);
+            bool queued = false;
+            if (can_spawn && invpdf > 0.0f &&
+                light_contribution(dc, sc, m, mk(1.0f, 1.0f, 1.0f), Sd, r.d, s.n, 1.0f, 1.0f, invpdf)) {
+                ctp = had(tp, had(dcol, dc) + had(scol, sc));
+                if (!is_zero(ctp)) {
+                    push_path(Q, nbuf, level + 1, s.p + (Sd * seps), r.time, Sd, (flags & PF_INSIDE) | bflag, ctp,
+                              slot, mk(0.0f, 0.0f, 0.0f), child_digits(digits, level, 0));
+                    queued = true;
+                }
+            }
+            if (recordable && !multi && level - 1 < Q.rec_levels) {
+                f3 gp, gn;
+                guide_query(S, r, h, gp, gn);
+                GuideRecord &R = Q.rec[(size_t)(level - 1) * Q.n_rec + slot];
+                R.pos_q = make_float4(gp.x, gp.y, gp.z, qpdf);
+                R.n = make_float4(gn.x, gn.y, gn.z, 0.0f);
+                R.wo = make_float4(-r.d.x, -r.d.y, -r.d.z, 0.0f);
+                R.wi = make_float4(Sd.x, Sd.y, Sd.z, 0.0f);
+                R.tpc = make_float4(ctp.x, ctp.y, ctp.z, queued ? 1.0f : 0.0f);
             }
             next_child = 1;
         }
@@ -448,8 +496,8 @@ __global__ void __launch_bounds__(BLOCK) k_shade(DevScene S, CameraParams cam, W
             }
             f3 ctp = had(tp, ld3(m.mirror));
             if (can_spawn && !is_zero(ctp))
-                push_path(Q, nbuf, level + 1, s.p + (rd * 0.000825f), r.time, rd, flags & PF_INSIDE, ctp, slot,
-                          mk(0.0f, 0.0f, 0.0f), child_digits(digits, level, next_child));
+                push_path(Q, nbuf, level + 1, s.p + (rd * 0.000825f), r.time, rd, (flags & PF_INSIDE) | bflag, ctp,
+                          slot, mk(0.0f, 0.0f, 0.0f), child_digits(digits, level, next_child));
             next_child++;
         }
         if (m.transparent) {
@@ -484,7 +532,7 @@ __global__ void __launch_bounds__(BLOCK) k_shade(DevScene S, CameraParams cam, W
                 f3 ctp = tp * (1.0f - refl);
                 if (can_spawn && !is_zero(ctp))
                     push_path(Q, nbuf, level + 1, s.p + (td * 0.0001f), r.time, td,
-                              (inside ? 0u : PF_INSIDE) | (inside ? 0u : PF_ATTEN), ctp, slot, att,
+                              (inside ? 0u : PF_INSIDE) | (inside ? 0u : PF_ATTEN) | bflag, ctp, slot, att,
                               child_digits(digits, level, next_child));
                 next_child++;
             }
@@ -492,7 +540,7 @@ __global__ void __launch_bounds__(BLOCK) k_shade(DevScene S, CameraParams cam, W
             f3 ctp = tp * refl;
             if (can_spawn && !is_zero(ctp))
                 push_path(Q, nbuf, level + 1, s.p + (rd * 0.0001f), r.time, rd,
-                          (inside ? PF_INSIDE : 0u) | (inside ? PF_ATTEN : 0u), ctp, slot, att,
+                          (inside ? PF_INSIDE : 0u) | (inside ? PF_ATTEN : 0u) | bflag, ctp, slot, att,
                           child_digits(digits, level, next_child));
         }
     }
@@ -868,19 +916,29 @@ struct StageTimer {
 // Renders samples [start, start+n) of the scissor into `film`; returns the
 // per-wave counters (path and shadow queue sizes per level, overflow flag).
 static int RenderWave(const GpuScene &G, const CameraParams &cam, WaveBuffers &W, uint64_t start, uint32_t n,
-                      az_pixel *film, cudaStream_t st, int sms, RenderCounters &rc, StageTimer *timer) {
+                      az_pixel *film, cudaStream_t st, int sms, RenderCounters &rc, StageTimer *timer,
+                      GuideState *guide, bool train) {
     WaveQueues Q = W.q;
+    const uint32_t levels = std::min<uint32_t>(G.dev.max_depth + 1, AZ_MAX_LEVELS - 2);
+    if (guide) {
+        int grc = GuidePrepareWave(*guide, Q, Q.cap_q, train ? levels : 0u, st);
+        if (grc != AZ_OK) return grc;
+    }
     AZ_CUDA_TRY(cudaMemsetAsync(Q.counts, 0, AZ_COUNT_TOTAL * sizeof(uint32_t), st));
     uint32_t first = n;
     AZ_CUDA_TRY(cudaMemcpyAsync(Q.counts + 1, &first, sizeof(uint32_t), cudaMemcpyHostToDevice, st));
     k_camera<<<(n + 255) / 256, 256, 0, st>>>(cam, Q, start, n);
     rc.launches++;
-    const uint32_t levels = std::min<uint32_t>(G.dev.max_depth + 1, AZ_MAX_LEVELS - 2);
     const int grid = sms * 16;
     const uint32_t v = cam.variant;
     for (uint32_t L = 1; L <= levels; L++) {
         if (timer) timer->Mark(st, 0);
         LaunchTraversalVariant(v, false, sms, G.dev, cam, Q, L, st);
+        if (guide) {
+            int grc = GuideInfer(*guide, G, Q, L, st);
+            if (grc != AZ_OK) return grc;
+            rc.launches++;
+        }
         if (timer) timer->Mark(st, 1);
         LaunchShade(grid, G.dev, cam, Q, start, L, st);
         if (timer) timer->Mark(st, 2);
@@ -889,6 +947,11 @@ static int RenderWave(const GpuScene &G, const CameraParams &cam, WaveBuffers &W
         rc.launches += G.dev.full_light_queries ? 4 : 3;
         rc.extend_launches++;
     }
+    if (guide && train) {
+        int grc = GuideTrainWave(*guide, Q, st);
+        if (grc != AZ_OK) return grc;
+        rc.launches += 7;
+    }
     k_splat<<<(n + 255) / 256, 256, 0, st>>>(cam, Q, start, n, film);
     rc.launches++;
     AZ_CUDA_TRY(cudaGetLastError());
@@ -896,7 +959,8 @@ static int RenderWave(const GpuScene &G, const CameraParams &cam, WaveBuffers &W
 }
 
 int Render(GpuScene &G, az_pixel *film, const az_camera *camera, const az_epsilon_values *eps, az_scissor sc,
-           int32_t filter, uint32_t cull, const az_render_opts *opts, cudaStream_t st, az_render_stats *stats) {
+           int32_t filter, uint32_t cull, const az_render_opts *opts, cudaStream_t st, az_render_stats *stats,
+           GuideState *guide, bool train) {
     CameraParams cam;
     int rc = SetupCamera(camera, sc, filter, cull, eps, opts ? opts->seed : 0, cam);
     if (rc != AZ_OK) return rc;
@@ -910,6 +974,7 @@ int Render(GpuScene &G, az_pixel *film, const az_camera *camera, const az_epsilo
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, G.device);
     uint32_t chunk = opts && opts->chunk_samples ? opts->chunk_samples : (1u << 22);
+    if (guide) chunk = std::min<uint32_t>(chunk, 1u << 20);   // proposals are kept per queue entry
     chunk = (uint32_t)std::min<uint64_t>(chunk, total);
     uint32_t per_node_shadow = G.dev.light_count + (G.dev.use_env_map ? 1u : 0u);
     WaveBuffers &W = G.waves;
@@ -931,7 +996,7 @@ int Render(GpuScene &G, az_pixel *film, const az_camera *camera, const az_epsilo
                                                                          (uint64_t)n * 4), 1024);
         rc = W.Ensure(n, cap_q, cap_s);
         if (rc != AZ_OK) return rc;
-        rc = RenderWave(G, cam, W, pos, n, film, st, sms, counters, timer.get());
+        rc = RenderWave(G, cam, W, pos, n, film, st, sms, counters, timer.get(), guide, train);
         if (rc != AZ_OK) return rc;
         AZ_CUDA_TRY(cudaMemcpyAsync(host_counts.data(), W.q.counts, AZ_COUNT_TOTAL * sizeof(uint32_t),
                                     cudaMemcpyDeviceToHost, st));

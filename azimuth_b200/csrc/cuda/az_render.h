@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "az_device_math.cuh"
+#include "az_guide.cuh"
 
 namespace az {
 
@@ -46,6 +47,10 @@ struct WaveQueues {
     uint32_t cap_s;
     float4 *accum;                          // per-sample radiance sums
     uint32_t *counts;                       // see AZ_COUNT_*
+    // path guiding (null when rendering without a guide)
+    const azd::GuideLobes *lobes;           // per extension-queue entry of the current level
+    azd::GuideRecord *rec;                  // [level][n_rec] training vertices
+    uint32_t n_rec, rec_levels;
 };
 
 struct WaveBuffers {

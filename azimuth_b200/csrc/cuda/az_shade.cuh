@@ -22,7 +22,7 @@ __device__ __forceinline__ uint32_t perlin_hash(const uint32_t *P, int32_t i, in
     return __ldg(P + (((uint32_t)i + b) & 255u));
 }
 
-__device__ float sample_perlin(const DevScene &S, const DevTexture &t, f3 p) {  // :156-195
+static __device__ float sample_perlin(const DevScene &S, const DevTexture &t, f3 p) {  // :156-195
     float r = 0.0f;
     p = p * t.scaling;
     int32_t I = (int32_t)floorf(p.x), J = (int32_t)floorf(p.y), K = (int32_t)floorf(p.z);
@@ -50,7 +50,7 @@ __device__ __forceinline__ f3 fetch_texel(const DevScene &S, const DevTexture &t
     return mk(__ldg(p + idx), __ldg(p + idx + 1), __ldg(p + idx + 2));
 }
 
-__device__ f3 sample_tex2d(const DevScene &S, const DevTexture &t, float u, float v, bool normalize_) {  // :239-339
+static __device__ f3 sample_tex2d(const DevScene &S, const DevTexture &t, float u, float v, bool normalize_) {  // :239-339
     f3 r;
     if (t.wrap == 0) {
         float a = u < 1.0f ? u : 1.0f;
@@ -225,10 +225,29 @@ __device__ Surface surface_at(const DevScene &S, const Ray &wr, const Hit &h) {
     return s;
 }
 
+// Inputs of the path-guiding network at a hit: the world position o + t d
+// and the geometric normal (face normal of the triangle, or centre-to-hit
+// direction of the sphere), normalised.
+__device__ __forceinline__ void guide_query(const DevScene &S, const Ray &wr, const Hit &h, f3 &p, f3 &n) {
+    p = wr.o + wr.d * h.t;
+    const DevEntity &e = S.ents[h.ent];
+    if (h.prim == 0xFFFFFFFFu) {
+        const f3 c = point_xf(e.xf, mk(e.center[0], e.center[1], e.center[2])) +
+                     wr.time * mk(e.motion[0], e.motion[1], e.motion[2]);
+        n = normalize(p - c);
+    } else {
+        const float4 c4 = S.tris[h.prim].c;
+        f3 fn = mk(c4.y, c4.z, c4.w);
+        const DevGroup &g = S.groups[e.group];
+        if (!g.raw) fn = normal_xf(g.inv, fn);
+        n = normalize(fn);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // BRDFs and light contribution, src/azimuth_main.cpp:461-603
 // ---------------------------------------------------------------------------
-__device__ void eval_brdf(float &diffuse, float &specular, const DevMaterial &m, f3 L, f3 N, f3 V, float cti) {
+static __device__ void eval_brdf(float &diffuse, float &specular, const DevMaterial &m, f3 L, f3 N, f3 V, float cti) {
     const float e = m.exponent;
     switch (m.brdf_type) {
         case 0: {  // Phong
@@ -295,7 +314,7 @@ __device__ __forceinline__ bool light_contribution(f3 &dc, f3 &sc, const DevMate
 }
 
 // SampleEntityLight (:392-459): direction and inverse pdf.
-__device__ void sample_entity_light(const DevScene &S, const DevLight &L, f3 hp, NodeRng &rng, f3 &dir, float &invpdf) {
+static __device__ void sample_entity_light(const DevScene &S, const DevLight &L, f3 hp, NodeRng &rng, f3 &dir, float &invpdf) {
     f3 hpl = point_xf(L.inv, hp);
     f3 ldl = mk(0.0f, 0.0f, 0.0f);
     invpdf = 0.0f;
@@ -336,7 +355,7 @@ __device__ void sample_entity_light(const DevScene &S, const DevLight &L, f3 hp,
 // `triangle` array, whose vertices are the triangle entities' vertices).
 // Returns 1 with the world t, 0 if the light is not hit, -1 if the light
 // needs a full nearest-hit query instead (entity_light_needs_full_query).
-__device__ int light_entity_hit(const DevScene &S, const DevLight &L, const Ray &wr, float &t_world) {
+static __device__ int light_entity_hit(const DevScene &S, const DevLight &L, const Ray &wr, float &t_world) {
     if (entity_light_needs_full_query(L)) return -1;
     if (L.entity_type == ENT_SPHERE) {
         float tl;
@@ -366,7 +385,7 @@ __device__ int light_entity_hit(const DevScene &S, const DevLight &L, const Ray 
 }
 
 // Background of a primary miss, SampleBackgroundColor (:1180-1207).
-__device__ f3 background(const DevScene &S, f3 d, int32_t w1, int32_t h1, uint32_t row, uint32_t col) {
+static __device__ f3 background(const DevScene &S, f3 d, int32_t w1, int32_t h1, uint32_t row, uint32_t col) {
     if (S.use_env_map) {
         float theta = acosf(d.y), phi = atan2f(d.z, d.x);
         float u = (-phi + AZD_PI_F32) / (2.0f * AZD_PI_F32), v = theta / AZD_PI_F32;

@@ -1,0 +1,137 @@
+"""Equal-time comparison of the guided and the plain GPU renderer.
+
+    python -m azimuth_b200.guiding_eval [--width 480 --height 270 --detail 49 --ref-spp 4096 --pass-spp 4]
+
+Workload: the interior scene (three 8x4x8 rooms joined by 1x2 doorways,
+Perlin-displaced panels and clutter, ~4 M triangles at the default detail,
+one 1x1 light in room 1, camera in room 3, depth 10).  A converged reference
+is accumulated in FP64 from plain renders (`--ref-spp` samples per pixel).
+Then each renderer runs passes of `--pass-spp` samples per pixel until
+`--passes`; after every pass the running average's relMSE against the
+reference, mean over pixels and channels of (x - ref)^2 / (ref^2 + 1e-2), is
+recorded with the GPU time spent so far (CUDA events; the guide's inference,
+recording and training included).  The guided renderer trains during the
+first `--train-passes` passes and keeps every pass in its average (all are
+unbiased).  Reported: both curves and the time the guided renderer needs to
+reach the plain renderer's final relMSE, as a fraction of the plain time.
+"""
+import argparse
+import json
+import sys
+import time
+
+import numpy as np
+
+
+def _relmse(img, ref):
+    return float(np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2)))
+
+
+def _time_to(curve, target):
+    """First time (linear interpolation in log relMSE) at which curve reaches target."""
+    prev_t, prev_e = 0.0, None
+    for t, e in curve:
+        if e <= target:
+            if prev_e is None or prev_e <= e:
+                return t
+            a = (np.log(prev_e) - np.log(target)) / (np.log(prev_e) - np.log(e))
+            return prev_t + a * (t - prev_t)
+        prev_t, prev_e = t, e
+    return None
+
+
+def _log(msg):
+    print(msg, file=sys.stderr, flush=True)
+
+
+def run(width=480, height=270, detail=49, ref_spp=4096, pass_spp=4, passes=64, train_passes=16, seed=0,
+        log=_log):
+    import torch
+    import azimuth_b200 as az
+    t0 = time.time()
+    scene = az.generate_scene(az.SCENE_INTERIOR, seed=seed, width=width, height=height, spp=pass_spp, detail=detail)
+    gen_s = time.time() - t0
+    w, h = scene.resolution()
+    spp = int(int(scene.sample_count() ** 0.5) ** 2)
+    film = torch.zeros((h, w, 4), device="cuda")
+    out = {"workload": "interior (3 rooms, %d triangles), %dx%d, depth %d" % (scene.triangle_count, w, h,
+                                                                                scene.max_depth()),
+           "pass_spp": spp, "passes": passes, "train_passes": train_passes, "generate_s": gen_s}
+    with az.GpuScene(scene) as g:
+        stream = torch.cuda.current_stream()
+
+        def one(render):
+            film.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            render()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            f = film.cpu().numpy().astype(np.float64)
+            return f[..., :3] / np.maximum(f[..., 3:4], 1e-30), e0.elapsed_time(e1) / 1000.0
+
+        # converged reference, FP64 accumulation of plain passes
+        ref = np.zeros((h, w, 3))
+        n_ref = max(1, ref_spp // spp)
+        t_ref = 0.0
+        for k in range(n_ref):
+            img, dt = one(lambda: g.render_device(film.data_ptr(), seed=100000 + k, stream=stream.cuda_stream))
+            ref += img
+            t_ref += dt
+        ref /= n_ref
+        out["reference"] = {"spp": n_ref * spp, "gpu_s": t_ref, "mean": float(ref.mean())}
+        log("reference: %d spp in %.1f s GPU" % (n_ref * spp, t_ref))
+
+        curves = {}
+        # plain
+        acc = np.zeros_like(ref)
+        t, curve = 0.0, []
+        for k in range(passes):
+            img, dt = one(lambda: g.render_device(film.data_ptr(), seed=k, stream=stream.cuda_stream))
+            acc += img
+            t += dt
+            curve.append((t, _relmse(acc / (k + 1), ref)))
+        curves["plain"] = curve
+        # guided (trains during the first passes)
+        with az.Guide(g, seed=seed) as guide:
+            acc = np.zeros_like(ref)
+            t, curve = 0.0, []
+            for k in range(passes):
+                tr = k < train_passes
+                img, dt = one(lambda: guide.render(film.data_ptr(), train=tr, seed=k, stream=stream.cuda_stream,
+                                                   stats=False))
+                acc += img
+                t += dt
+                curve.append((t, _relmse(acc / (k + 1), ref)))
+            curves["guided"] = curve
+            out["guide_steps"] = guide.info()["steps"]
+    target = curves["plain"][-1][1]
+    t_plain = curves["plain"][-1][0]
+    t_guided = _time_to(curves["guided"], target)
+    out["plain"] = {"gpu_s": t_plain, "relmse": target, "s_per_pass": t_plain / passes}
+    out["guided"] = {"gpu_s": curves["guided"][-1][0], "relmse": curves["guided"][-1][1],
+                     "s_per_pass": curves["guided"][-1][0] / passes,
+                     "time_to_plain_relmse_s": t_guided}
+    out["time_ratio_at_equal_relmse"] = (t_guided / t_plain) if t_guided is not None else None
+    out["relmse_ratio_at_equal_passes"] = curves["guided"][-1][1] / target
+    out["curves"] = {k: [[round(a, 5), b] for a, b in v] for k, v in curves.items()}
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--width", type=int, default=480)
+    ap.add_argument("--height", type=int, default=270)
+    ap.add_argument("--detail", type=int, default=49)
+    ap.add_argument("--ref-spp", type=int, default=4096)
+    ap.add_argument("--pass-spp", type=int, default=4)
+    ap.add_argument("--passes", type=int, default=64)
+    ap.add_argument("--train-passes", type=int, default=16)
+    ap.add_argument("--seed", type=int, default=0)
+    a = ap.parse_args()
+    res = run(a.width, a.height, a.detail, a.ref_spp, a.pass_spp, a.passes, a.train_passes, a.seed)
+    print(json.dumps(res), flush=True)
+
+
+if __name__ == "__main__":
+    main()

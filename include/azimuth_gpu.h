@@ -131,6 +131,54 @@ int az_gpu_autotune_scene(const az_scene *host_scene, az_gpu_scene *scene, const
                           uint32_t backface_culling, const az_render_opts *opts, uint32_t *width_out,
                           uint32_t *variant_out, float *ms_out);
 
+/* ---- Neural path guiding (the learned proposal; no counterpart in azimuth) ----
+ *
+ * A guide belongs to one device scene.  Rendered with az_gpu_render_guided,
+ * the scattering direction of every diffuse vertex is drawn by one-sample
+ * MIS from a learned mixture of 8 von Mises-Fisher lobes (a hash-grid encoded
+ * MLP of position, normal and outgoing direction) and cosine sampling, with a
+ * learned selection probability; the mixture density weights the sample, so
+ * the estimate stays unbiased.  With `train` set, every wave also trains the
+ * network (one Adam step) on the radiance its own paths brought back. */
+typedef struct az_guide az_guide;
+
+typedef struct az_guide_config {
+    float learning_rate;            /* Adam step size; 0 = 1e-2 */
+    uint32_t train_batch;           /* training rows per step at most; 0 = 2^18 */
+    uint32_t record_samples;        /* camera samples per wave whose vertices are recorded; 0 = 2^16 */
+    uint32_t reserved0;
+    uint64_t seed;                  /* weight initialisation */
+    uint32_t reserved[6];
+} az_guide_config;
+
+int az_guide_create(az_gpu_scene *scene, const az_guide_config *cfg, az_guide **out);
+void az_guide_destroy(az_guide *guide);
+
+/* az_gpu_render with the guide's proposal for the scattering direction (waves
+ * of at most 2^20 camera samples); `train` != 0 trains after every wave.
+ * Pass the scene the guide was created for. */
+int az_gpu_render_guided(az_gpu_scene *scene, az_guide *guide, az_pixel *film, const az_camera *camera,
+                         const az_epsilon_values *epsilons, az_scissor scissor, int32_t filter_type,
+                         uint32_t backface_culling, uint32_t train, const az_render_opts *opts,
+                         az_render_stats *stats);
+
+/* Network access for tests and tools (host arrays, synchronous).
+ * mlp: 4 x 64 x 64 weights W[layer][input][output]; bias: 64 output-layer
+ * biases; grid: 16 x 2^19 x 2 hash-grid features.  NULL skips an array. */
+int az_guide_get_params(az_guide *guide, float *mlp, float *bias, float *grid);
+int az_guide_set_params(az_guide *guide, const float *mlp, const float *bias, const float *grid);
+/* Level resolutions (16), position normalisation (lo, 1/extent) and Adam steps taken. */
+int az_guide_info(az_guide *guide, uint32_t *res, float *lo, float *inv_ext, uint32_t *steps);
+/* Rows: n x 16 floats (position, weight, normal, 0, outgoing direction, 0,
+ * incident direction, 0).  Evaluates the network and the loss
+ * sum_i -w_i log q_i(wi_i) without updating it: raw outputs (n x 64), the
+ * loss, its gradient with respect to the MLP weights, the output biases and
+ * the encoded grid features (n x 32).  Any output may be NULL. */
+int az_guide_eval(az_guide *guide, const float *rows, uint32_t n, float *outputs, float *loss, float *mlp_grad,
+                  float *bias_grad, float *enc_grad);
+/* `steps` Adam steps on the given rows; per-step loss (before the step) in losses. */
+int az_guide_train(az_guide *guide, const float *rows, uint32_t n, uint32_t steps, float *losses);
+
 /* Allocation-free variant of az_gpu_render; it has no counterpart in azimuth.
  *
  * For callers that must not allocate device memory while rendering: code

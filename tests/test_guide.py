@@ -1,0 +1,229 @@
+"""Neural path guiding: the CPU oracle against finite differences and Monte
+Carlo, the CUDA network against the oracle, training, and the guided render
+(unbiased, and better than plain cosine sampling at equal samples)."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+import azimuth_b200 as az
+
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle"))
+import guide_oracle as go  # noqa: E402
+
+
+def _unit(rng, n):
+    v = rng.normal(size=(n, 3))
+    return v / np.linalg.norm(v, axis=1, keepdims=True)
+
+
+def _rows(rng, n, lo, hi):
+    pos = lo + (hi - lo) * rng.random((n, 3))
+    nrm = _unit(rng, n)
+    wo = _unit(rng, n)
+    wi = _unit(rng, n)
+    wi = np.where(((wi * nrm).sum(1) < 0)[:, None] & (rng.random((n, 1)) < 0.7), -wi, wi)
+    w = rng.uniform(0.1, 2.0, n)
+    rows = np.zeros((n, 16), np.float32)
+    rows[:, 0:3] = pos
+    rows[:, 3] = w
+    rows[:, 4:7] = nrm
+    rows[:, 8:11] = wo
+    rows[:, 12:15] = wi
+    return rows
+
+
+def _small_params(rng, scale=0.25):
+    return {"mlp": rng.normal(scale=scale, size=(4, 64, 64)), "bias": rng.normal(scale=0.5, size=64)}
+
+
+# ---------------------------------------------------------------- CPU: oracle
+def test_oracle_loss_gradient_matches_finite_differences():
+    rng = np.random.default_rng(0)
+    n = 6
+    o = rng.normal(size=(n, 64))
+    nrm = _unit(rng, n)
+    wi = _unit(rng, n)
+    w = rng.uniform(0.5, 1.5, n)
+    _, do = go.loss_and_grad(o, nrm, wi, w)
+    eps = 1e-6
+    for j in list(range(41)):
+        op, om = o.copy(), o.copy()
+        op[:, j] += eps
+        om[:, j] -= eps
+        fd = (go.loss_and_grad(op, nrm, wi, w)[0] - go.loss_and_grad(om, nrm, wi, w)[0]) / (2 * eps)
+        assert abs(fd - do[:, j].sum()) <= 1e-5 * max(1.0, abs(fd)), j
+
+
+def test_oracle_network_gradient_matches_finite_differences():
+    rng = np.random.default_rng(1)
+    n = 5
+    p = _small_params(rng)
+    x = np.zeros((n, 64))
+    x[:, :39] = rng.normal(size=(n, 39))
+    nrm, wi, w = _unit(rng, n), _unit(rng, n), rng.uniform(0.5, 1.5, n)
+
+    def loss(params, xx):
+        o, _ = go.forward(params, xx, bf=False)
+        return go.loss_and_grad(o, nrm, wi, w)[0]
+
+    o, inputs = go.forward(p, x, bf=False)
+    _, do = go.loss_and_grad(o, nrm, wi, w)
+    dmlp, dbias, enc = go.backward(p, inputs, do, bf=False)
+    eps = 1e-6
+    for (l, i, j) in [(0, 3, 5), (1, 10, 20), (2, 63, 0), (3, 7, 40), (3, 12, 4)]:
+        q = {"mlp": p["mlp"].copy(), "bias": p["bias"]}
+        q["mlp"][l, i, j] += eps
+        up = loss(q, x)
+        q["mlp"][l, i, j] -= 2 * eps
+        fd = (up - loss(q, x)) / (2 * eps)
+        assert abs(fd - dmlp[l, i, j]) <= 1e-5 * max(1.0, abs(fd)), (l, i, j)
+    for j in [0, 17, 31]:
+        xp, xm = x.copy(), x.copy()
+        xp[2, j] += eps
+        xm[2, j] -= eps
+        fd = (loss(p, xp) - loss(p, xm)) / (2 * eps)
+        assert abs(fd - enc[2, j]) <= 1e-5 * max(1.0, abs(fd)), j
+
+
+def test_vmf_mixture_density_integrates_to_one_and_sampler_follows_it():
+    rng = np.random.default_rng(2)
+    o = rng.normal(size=(1, 64))
+    o[0, 3:40:5] = np.log([0.5, 2.0, 5.0, 20.0, 1.0, 8.0, 3.0, 50.0])
+    nrm = np.array([[0.0, 0.0, 1.0]])
+    m = 400000
+    w = _unit(rng, m)
+    q = go.mixture_pdf(np.repeat(o, m, 0), np.repeat(nrm, m, 0), w)
+    assert abs(q.mean() * 4 * np.pi - 1.0) < 0.02
+    # the lobe sampler: mean cosine to the lobe axis matches coth(kappa) - 1/kappa
+    mu = np.repeat(np.array([[0.0, 0.6, 0.8]]), m, 0)
+    for kap in (0.3, 4.0, 60.0):
+        d = go.sample_vmf(mu, kap, rng.random(m), rng.random(m))
+        assert np.allclose(np.linalg.norm(d, axis=1), 1.0, atol=1e-9)
+        mean_cos = (d * mu).sum(1).mean()
+        assert abs(mean_cos - (1.0 / np.tanh(kap) - 1.0 / kap)) < 5e-3
+
+
+# ---------------------------------------------------------------- GPU
+def _guide(gpu_scene, seed=0, **kw):
+    return az.Guide(gpu_scene, seed=seed, **kw)
+
+
+def _bounds(info):
+    lo = info["lo"].astype(np.float64)
+    return lo, lo + 1.0 / info["inv_ext"].astype(np.float64)
+
+
+@pytest.mark.gpu
+def test_guide_forward_and_gradients_match_oracle(gpu):
+    rng = np.random.default_rng(3)
+    scene = az.generate_scene(az.SCENE_CORNELL, width=8, height=8, spp=1)
+    with az.GpuScene(scene) as g, _guide(g) as guide:
+        info = guide.info()
+        assert list(info["res"]) == list(go.level_res())
+        mlp = rng.normal(scale=0.2, size=(4, 64, 64)).astype(np.float32)
+        bias = rng.normal(scale=0.5, size=64).astype(np.float32)
+        grid = rng.uniform(-1.0, 1.0, size=(16, 1 << 19, 2)).astype(np.float32)
+        guide.set_params(mlp, bias, grid)
+        lo, hi = _bounds(info)
+        rows = _rows(rng, 512, lo, hi)
+        got = guide.eval(rows)
+        ref = go.evaluate({"mlp": mlp.astype(np.float64), "bias": bias.astype(np.float64)},
+                          grid.astype(np.float16).astype(np.float64), rows, info["lo"], info["inv_ext"])
+    o_gpu, o_ref = got["outputs"][:, :41], ref["outputs"][:, :41]
+    scale = np.abs(o_ref).max()
+    assert np.abs(o_gpu - o_ref).max() <= 1e-2 * scale, np.abs(o_gpu - o_ref).max()
+    assert abs(got["loss"] - ref["loss"]) <= 2e-3 * abs(ref["loss"])
+
+    def rel(a, b):
+        return np.linalg.norm(np.asarray(a, np.float64) - b) / np.linalg.norm(b)
+    assert rel(got["bias_grad"], ref["bias_grad"]) < 2e-2
+    assert rel(got["mlp_grad"], ref["mlp_grad"]) < 3e-2
+    assert rel(got["enc_grad"], ref["enc_grad"]) < 3e-2
+
+
+@pytest.mark.gpu
+def test_guide_training_fits_a_direction_field(gpu):
+    """Maximum-likelihood fit (unit weights) of directions scattered around an
+    axis that depends on the position (16 surface points, 512 directions each):
+    the loss drops and the learned density peaks on the axis."""
+    rng = np.random.default_rng(4)
+    scene = az.generate_scene(az.SCENE_CORNELL, width=8, height=8, spp=1)
+    with az.GpuScene(scene) as g, _guide(g, seed=1) as guide:
+        lo, hi = _bounds(guide.info())
+        n = 8192
+        rows = _rows(rng, n, lo, hi)
+        points = lo + (hi - lo) * rng.random((16, 3))
+        rows[:, 0:3] = points[np.arange(n) % 16]
+        axis = np.where((rows[:, 0:1] < (lo[0] + hi[0]) / 2), [[0.0, 1.0, 0.0]], [[0.0, 0.0, 1.0]])
+        rows[:, 12:15] = go.sample_vmf(axis, 30.0, rng.random(n), rng.random(n))
+        rows[:, 4:7] = axis          # normal along the axis: the cosine part can help too
+        rows[:, 3] = 1.0
+        losses = guide.train(rows, 300)
+        after = guide.eval(rows)
+    per_row = losses / n
+    assert per_row[-1] < per_row[0] - 1.0, (per_row[0], per_row[-1])
+    q = go.mixture_pdf(after["outputs"].astype(np.float64), rows[:, 4:7].astype(np.float64), axis)
+    assert np.median(q) > 2.0     # cosine alone gives 1/pi at the axis
+
+
+def _relmse(img, ref):
+    return float(np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2)))
+
+
+@pytest.mark.gpu
+def test_guided_render_is_unbiased_and_beats_cosine_sampling(gpu):
+    """Interior (light in room 1, camera in room 3): against an FP64-accumulated
+    converged plain render, the trained guide's image at equal samples has the
+    same mean and a lower relMSE than plain cosine sampling."""
+    import torch
+    scene = az.generate_scene(az.SCENE_INTERIOR, seed=0, width=64, height=36, spp=16, detail=4)
+    w, h = scene.resolution()
+    with az.GpuScene(scene) as g:
+        film = torch.zeros((h, w, 4), device="cuda")
+        acc = np.zeros((h, w, 3))
+        passes = 48
+        for k in range(passes):                     # converged reference: 48 x 16 spp, FP64 sums
+            film.zero_()
+            g.render_device(film.data_ptr(), seed=1000 + k)
+            f = film.cpu().numpy().astype(np.float64)
+            acc += f[..., :3] / f[..., 3:4]
+        ref = acc / passes
+        film.zero_()
+        g.render_device(film.data_ptr(), seed=7)
+        f = film.cpu().numpy().astype(np.float64)
+        plain = f[..., :3] / f[..., 3:4]
+        with _guide(g, seed=2) as guide:
+            for k in range(24):
+                film.zero_()
+                guide.render(film.data_ptr(), train=True, seed=2000 + k)
+            assert guide.info()["steps"] >= 24
+            film.zero_()
+            guide.render(film.data_ptr(), train=False, seed=7)
+            f = film.cpu().numpy().astype(np.float64)
+            guided = f[..., :3] / f[..., 3:4]
+            # unbiasedness: many guided renders average to the reference
+            passes_g = 32
+            gacc = np.zeros_like(ref)
+            for k in range(passes_g):
+                film.zero_()
+                guide.render(film.data_ptr(), train=False, seed=3000 + k)
+                f = film.cpu().numpy().astype(np.float64)
+                gacc += f[..., :3] / f[..., 3:4]
+            gmean = gacc / passes_g
+        # control: as many plain renders, for the size of the noise on the mean
+        pacc = np.zeros_like(ref)
+        for k in range(passes_g):
+            film.zero_()
+            g.render_device(film.data_ptr(), seed=3000 + k)
+            f = film.cpu().numpy().astype(np.float64)
+            pacc += f[..., :3] / f[..., 3:4]
+        pmean = pacc / passes_g
+    e_plain, e_guided = _relmse(plain, ref), _relmse(guided, ref)
+    print("interior 64x36, 16 spp: relMSE plain %.4g, guided %.4g; image mean: reference %.5g, "
+          "%d guided renders %.5g, %d plain renders %.5g" % (e_plain, e_guided, ref.mean(), passes_g, gmean.mean(),
+                                                             passes_g, pmean.mean()))
+    assert np.isfinite(guided).all()
+    assert abs(gmean.mean() - ref.mean()) <= 0.05 * ref.mean()
+    assert e_guided < e_plain
