@@ -16,7 +16,8 @@ import ctypes as C
 import numpy as np
 
 from . import _native
-from ._native import GenParams, GeneratedScene, GuideConfig, RenderOpts, RenderStats, Scissor, Vec2u, Ray3, lib
+from ._native import (BatchOpts, BatchStats, GenParams, GeneratedScene, GuideConfig, Job, RenderOpts, RenderStats,
+                      Scissor, Vec2u, Ray3, lib)
 
 SCENE_CORNELL = 0
 SCENE_DENSE_MESH = 1
@@ -326,6 +327,38 @@ class Guide:
             self.close()
         except Exception:
             pass
+
+
+def render_batch(jobs, streams=0, flags=0, chunk_samples=0, device=0):
+    """az_gpu_render_batch.  jobs: list of dicts with keys gpu_scene (GpuScene), film_ptr (device film of
+    the scene's camera resolution) and optionally guide (Guide), train, seed, scissor.  Returns
+    (per-job list of dicts done_ms/status/samples, batch stats dict)."""
+    arr = (Job * len(jobs))()
+    for k, j in enumerate(jobs):
+        gs = j["gpu_scene"]
+        sc_ = gs.scene
+        a = arr[k]
+        a.scene = gs._h
+        a.guide = j["guide"]._h if j.get("guide") is not None else None
+        a.film = j["film_ptr"]
+        a.camera = sc_.camera_ptr
+        a.epsilons = sc_.epsilons_ptr
+        a.scissor = j.get("scissor") or full_scissor(sc_)
+        a.filter_type = sc_.filter_type
+        a.backface_culling = 0
+        a.train = 1 if j.get("train") else 0
+        a.seed = j.get("seed", 0)
+    o = BatchOpts()
+    o.device = device
+    o.streams = streams
+    o.flags = flags
+    o.chunk_samples = chunk_samples
+    st = BatchStats()
+    rc = lib().az_gpu_render_batch(arr, len(jobs), C.byref(o), C.byref(st))
+    per = [{"done_ms": arr[k].done_ms, "status": arr[k].status, "samples": arr[k].samples} for k in range(len(jobs))]
+    _check(rc, "az_gpu_render_batch")
+    return per, {"samples": st.samples, "gpu_ms": st.gpu_ms, "p50_ms": st.p50_ms, "p99_ms": st.p99_ms,
+                 "jobs": st.jobs, "failed": st.failed, "streams": st.streams}
 
 
 def _stats(st):

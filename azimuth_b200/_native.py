@@ -49,6 +49,23 @@ class RenderOpts(C.Structure):
                 ("reserved", C.c_uint32 * 4)]
 
 
+class Job(C.Structure):
+    _fields_ = [("scene", C.c_void_p), ("guide", C.c_void_p), ("film", C.c_void_p), ("camera", C.c_void_p),
+                ("epsilons", C.c_void_p), ("scissor", Scissor), ("filter_type", C.c_int32),
+                ("backface_culling", C.c_uint32), ("train", C.c_uint32), ("reserved0", C.c_uint32),
+                ("seed", C.c_uint64), ("done_ms", C.c_float), ("status", C.c_int32), ("samples", C.c_uint64)]
+
+
+class BatchOpts(C.Structure):
+    _fields_ = [("device", C.c_int32), ("streams", C.c_uint32), ("flags", C.c_uint32), ("chunk_samples", C.c_uint32),
+                ("reserved", C.c_uint32 * 4)]
+
+
+class BatchStats(C.Structure):
+    _fields_ = [("samples", C.c_uint64), ("gpu_ms", C.c_float), ("p50_ms", C.c_float), ("p99_ms", C.c_float),
+                ("jobs", C.c_uint32), ("failed", C.c_uint32), ("streams", C.c_uint32), ("reserved", C.c_uint32 * 3)]
+
+
 class GuideConfig(C.Structure):
     _fields_ = [("learning_rate", C.c_float), ("train_batch", C.c_uint32), ("record_samples", C.c_uint32),
                 ("reserved0", C.c_uint32), ("seed", C.c_uint64), ("reserved", C.c_uint32 * 6)]
@@ -104,6 +121,8 @@ def _declare(L):
         L.az_gpu_autotune_scene.argtypes = [vp, vp, vp, vp, Scissor, i32, u32, C.POINTER(RenderOpts), vp, vp, vp]
         L.az_gpu_autotune_scene.restype = i32
         L.az_gpu_render_noalloc.argtypes = [vp, vp, vp, vp, Scissor, i32, u32, C.POINTER(RenderOpts)]
+        L.az_gpu_render_batch.argtypes = [vp, u32, C.POINTER(BatchOpts), C.POINTER(BatchStats)]
+        L.az_gpu_render_batch.restype = i32
         L.az_guide_create.argtypes = [vp, C.POINTER(GuideConfig), C.POINTER(vp)]
         L.az_guide_create.restype = i32
         L.az_guide_destroy.argtypes = [vp]

@@ -45,7 +45,9 @@ struct CallContext {
         if (opts && opts->stream) {
             stream = (cudaStream_t)opts->stream;
         } else {
-            AZ_CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+            // a blocking stream: ordered after earlier work on the legacy default
+            // stream (a film zeroed there, for instance)
+            AZ_CUDA_TRY(cudaStreamCreate(&stream));
             own = true;
         }
         return AZ_OK;
@@ -248,6 +250,7 @@ extern "C" int az_gpu_render_guided(az_gpu_scene *scene, az_guide *guide, az_pix
     CallContext ctx;
     int rc = ctx.begin(opts);
     if (rc != AZ_OK) return rc;
+    std::lock_guard<std::mutex> lock(GuideLock(*g));
     return Render(*scene->impl, film, camera, epsilons, scissor, filter_type, backface_culling, opts, ctx.stream, stats,
                   g, train != 0);
 }

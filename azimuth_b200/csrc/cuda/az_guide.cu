@@ -650,6 +650,7 @@ struct GuideState {
     float last_loss = 0.0f;
     std::vector<void *> allocs;
     int sms = 148;
+    std::mutex mu;
 
     ~GuideState() {
         for (void *p : allocs)
@@ -869,6 +870,7 @@ struct az_guide {
 
 namespace az {
 GuideState *GuideOf(az_guide *g) { return g ? g->impl : nullptr; }
+std::mutex &GuideLock(GuideState &g) { return g.mu; }
 }  // namespace az
 
 extern "C" int az_guide_create(az_gpu_scene *scene, const az_guide_config *cfg, az_guide **out) {

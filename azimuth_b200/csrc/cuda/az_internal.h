@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -79,12 +80,16 @@ int GuideInfer(GuideState &g, const GpuScene &G, const WaveQueues &Q, uint32_t l
 // Training targets of the finished wave and one Adam step.
 int GuideTrainWave(GuideState &g, const WaveQueues &Q, cudaStream_t st);
 GuideState *GuideOf(az_guide *g);
+// Serialises the renders that use one guide (its proposal and record buffers).
+std::mutex &GuideLock(GuideState &g);
 
 // `guide` (may be null) steers the scattering direction; `train` also
 // updates the network after every wave.
+// `wave_buffers`: the queues to use (null: the scene's own); concurrent
+// renders of one scene need their own.
 int Render(GpuScene &G, az_pixel *film, const az_camera *camera, const az_epsilon_values *eps, az_scissor sc,
            int32_t filter, uint32_t cull, const az_render_opts *opts, cudaStream_t st, az_render_stats *stats,
-           GuideState *guide = nullptr, bool train = false);
+           GuideState *guide = nullptr, bool train = false, WaveBuffers *wave_buffers = nullptr);
 int Autotune(GpuScene &G, const az_camera *camera, const az_epsilon_values *eps, az_scissor sc, int32_t filter,
              uint32_t cull, const az_render_opts *opts, cudaStream_t st, uint32_t *best_out, float *ms_out);
 int ClosestHit(GpuScene &G, const az_ray3 *rays, uint32_t n, int32_t cull, float eps, uint32_t *out_hit,

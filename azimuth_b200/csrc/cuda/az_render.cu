@@ -106,6 +106,12 @@ __device__ __forceinline__ void push_shadow(const WaveQueues &Q, uint32_t level,
 // GetSampleCoord + GetRayForPixel (src/azimuth_main.cpp:1135-1178).
 __global__ void k_camera(CameraParams cam, WaveQueues Q, uint64_t wave_start, uint32_t n) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (Q.wave) {
+        wave_start = Q.wave[0];
+        n = (uint32_t)Q.wave[1];
+        cam.seed = Q.wave[2];
+        if (i == 0) Q.counts[1] = n;   // the level-1 queue is the wave itself
+    }
     if (i >= n) return;
     uint32_t row, col, sx, sy;
     sample_of(cam, wave_start + i, row, col, sx, sy);
@@ -269,6 +275,10 @@ __global__ void __launch_bounds__(BLOCK) k_shade(DevScene S, CameraParams cam, W
     const uint32_t n = min(Q.counts[level], Q.cap_q);
     const bool can_spawn = level + 1 <= S.max_depth + 1;   // child's RecursionDepth <= MaxRecursionDepth
     const float seps = cam.eps_shadow;
+    if (Q.wave) {
+        wave_start = Q.wave[0];
+        cam.seed = Q.wave[2];
+    }
     for (uint32_t i = blockIdx.x * BLOCK + threadIdx.x; i < n; i += gridDim.x * BLOCK) {
         const float4 o4 = Q.o[buf][i], d4 = Q.d[buf][i], tp4 = Q.tp[buf][i];
         const uint4 hh = Q.hit[i];
@@ -679,6 +689,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_shadow(DevScene S, CameraParams
 // ComputeSampleWeight (src/azimuth_main.cpp:1209-1254) for every sample of the wave.
 __global__ void k_splat(CameraParams cam, WaveQueues Q, uint64_t wave_start, uint32_t n, az_pixel *film) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (Q.wave) {
+        wave_start = Q.wave[0];
+        n = (uint32_t)Q.wave[1];
+    }
     if (i >= n) return;
     if (Q.counts[AZ_COUNT_OVERFLOW]) return;   // the wave is re-run
     uint32_t row, col, sx, sy;
@@ -845,12 +859,21 @@ int SetupCamera(const az_camera *c, az_scissor sc, int32_t filter, uint32_t cull
 }
 
 WaveBuffers::~WaveBuffers() {
+    DropGraph();
     for (void *p : ptrs)
         if (p) cudaFree(p);
+    if (wave_host) cudaFreeHost(wave_host);
+}
+
+void WaveBuffers::DropGraph() {
+    if (graph) cudaGraphExecDestroy(graph);
+    graph = nullptr;
+    graph_key.clear();
 }
 
 int WaveBuffers::Ensure(uint32_t chunk, uint32_t cap_q, uint32_t cap_s) {
     if (chunk <= this->chunk && cap_q <= q.cap_q && cap_s <= q.cap_s && !ptrs.empty()) return AZ_OK;
+    DropGraph();   // it refers to the buffers freed below
     for (void *p : ptrs)
         if (p) cudaFree(p);
     ptrs.clear();
@@ -876,8 +899,13 @@ int WaveBuffers::Ensure(uint32_t chunk, uint32_t cap_q, uint32_t cap_s) {
     q.smeta = (uint32_t *)alloc((size_t)cap_s * sizeof(uint32_t));
     q.accum = (float4 *)alloc((size_t)chunk * sizeof(float4));
     q.counts = (uint32_t *)alloc(AZ_COUNT_TOTAL * sizeof(uint32_t));
-    if (!q.hit || !q.so || !q.sd || !q.sc || !q.smeta || !q.accum || !q.counts)
+    wave_dev = (uint64_t *)alloc(4 * sizeof(uint64_t));
+    if (!q.hit || !q.so || !q.sd || !q.sc || !q.smeta || !q.accum || !q.counts || !wave_dev)
         return SetError(AZ_ERR_OUT_OF_MEMORY, "wave queues");
+    if (!wave_host && cudaMallocHost((void **)&wave_host, 4 * sizeof(uint64_t)) != cudaSuccess) {
+        wave_host = nullptr;
+        return SetError(AZ_ERR_OUT_OF_MEMORY, "wave descriptor");
+    }
     q.cap_q = cap_q;
     q.cap_s = cap_s;
     this->chunk = chunk;
@@ -915,18 +943,24 @@ struct StageTimer {
 
 // Renders samples [start, start+n) of the scissor into `film`; returns the
 // per-wave counters (path and shadow queue sizes per level, overflow flag).
+// Launches of one wave.  With `capture`, the launches read the wave's first
+// sample, size and seed from W.wave_dev (set before every replay of the
+// captured graph) and size their grids for `n` = the largest wave.
 static int RenderWave(const GpuScene &G, const CameraParams &cam, WaveBuffers &W, uint64_t start, uint32_t n,
                       az_pixel *film, cudaStream_t st, int sms, RenderCounters &rc, StageTimer *timer,
-                      GuideState *guide, bool train) {
+                      GuideState *guide, bool train, bool capture = false) {
     WaveQueues Q = W.q;
+    if (capture) Q.wave = W.wave_dev;
     const uint32_t levels = std::min<uint32_t>(G.dev.max_depth + 1, AZ_MAX_LEVELS - 2);
     if (guide) {
         int grc = GuidePrepareWave(*guide, Q, Q.cap_q, train ? levels : 0u, st);
         if (grc != AZ_OK) return grc;
     }
     AZ_CUDA_TRY(cudaMemsetAsync(Q.counts, 0, AZ_COUNT_TOTAL * sizeof(uint32_t), st));
-    uint32_t first = n;
-    AZ_CUDA_TRY(cudaMemcpyAsync(Q.counts + 1, &first, sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    if (!capture) {
+        uint32_t first = n;
+        AZ_CUDA_TRY(cudaMemcpyAsync(Q.counts + 1, &first, sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    }
     k_camera<<<(n + 255) / 256, 256, 0, st>>>(cam, Q, start, n);
     rc.launches++;
     const int grid = sms * 16;
@@ -958,9 +992,64 @@ static int RenderWave(const GpuScene &G, const CameraParams &cam, WaveBuffers &W
     return AZ_OK;
 }
 
+// One wave through the captured graph of W (capturing it first when the
+// scene, camera, film, launch configuration or largest wave changed).
+static int ReplayWave(const GpuScene &G, const CameraParams &cam, WaveBuffers &W, uint64_t start, uint32_t n,
+                      uint32_t n_max, az_pixel *film, cudaStream_t st, int sms, RenderCounters &rc) {
+    struct Key {
+        const GpuScene *g;
+        az_pixel *film;
+        CameraParams cam;
+        uint32_t n_max, cap_q, cap_s;
+        int sms;
+        const void *q0;
+    } key;
+    memset(&key, 0, sizeof(key));
+    key.g = &G;
+    key.film = film;
+    key.cam = cam;
+    key.cam.seed = 0;   // read from the descriptor
+    key.n_max = n_max;
+    key.cap_q = W.q.cap_q;
+    key.cap_s = W.q.cap_s;
+    key.sms = sms;
+    key.q0 = W.q.o[0];
+    const unsigned char *kb = reinterpret_cast<const unsigned char *>(&key);
+    RenderCounters launches{};
+    if (!W.graph || W.graph_key.size() != sizeof(key) || memcmp(W.graph_key.data(), kb, sizeof(key)) != 0) {
+        W.DropGraph();
+        AZ_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        int crc = RenderWave(G, cam, W, 0, n_max, film, st, sms, launches, nullptr, nullptr, false, true);
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamEndCapture(st, &graph);
+        if (crc != AZ_OK) {
+            if (graph) cudaGraphDestroy(graph);
+            return crc;
+        }
+        if (e != cudaSuccess) return CudaError(e, "capturing the wave launches");
+        e = cudaGraphInstantiate(&W.graph, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+            W.graph = nullptr;
+            return CudaError(e, "instantiating the wave graph");
+        }
+        W.graph_key.assign(kb, kb + sizeof(key));
+        W.graph_launches = launches.launches;
+        W.graph_extend_launches = launches.extend_launches;
+    }
+    W.wave_host[0] = start;
+    W.wave_host[1] = n;
+    W.wave_host[2] = cam.seed;
+    AZ_CUDA_TRY(cudaMemcpyAsync(W.wave_dev, W.wave_host, 3 * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+    AZ_CUDA_TRY(cudaGraphLaunch(W.graph, st));
+    rc.launches += W.graph_launches;
+    rc.extend_launches += W.graph_extend_launches;
+    return AZ_OK;
+}
+
 int Render(GpuScene &G, az_pixel *film, const az_camera *camera, const az_epsilon_values *eps, az_scissor sc,
            int32_t filter, uint32_t cull, const az_render_opts *opts, cudaStream_t st, az_render_stats *stats,
-           GuideState *guide, bool train) {
+           GuideState *guide, bool train, WaveBuffers *wave_buffers) {
     CameraParams cam;
     int rc = SetupCamera(camera, sc, filter, cull, eps, opts ? opts->seed : 0, cam);
     if (rc != AZ_OK) return rc;
@@ -977,7 +1066,7 @@ int Render(GpuScene &G, az_pixel *film, const az_camera *camera, const az_epsilo
     if (guide) chunk = std::min<uint32_t>(chunk, 1u << 20);   // proposals are kept per queue entry
     chunk = (uint32_t)std::min<uint64_t>(chunk, total);
     uint32_t per_node_shadow = G.dev.light_count + (G.dev.use_env_map ? 1u : 0u);
-    WaveBuffers &W = G.waves;
+    WaveBuffers &W = wave_buffers ? *wave_buffers : G.waves;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (stats) {
         AZ_CUDA_TRY(cudaEventCreate(&e0));
@@ -988,6 +1077,13 @@ int Render(GpuScene &G, az_pixel *film, const az_camera *camera, const az_epsilo
     std::vector<uint32_t> host_counts(AZ_COUNT_TOTAL);
     std::unique_ptr<StageTimer> timer;
     if (stats && opts && (opts->flags & AZ_FLAG_TIME_STAGES)) timer.reset(new StageTimer());
+    // The launches of a wave run as one CUDA graph, captured once per scene,
+    // camera, film and launch configuration and replayed for every wave with
+    // its first sample, size and seed in a 24-byte descriptor.  Not for stage
+    // timing, guided renders, or a legacy default stream (which cannot be
+    // captured).
+    const bool use_graph = !(opts && (opts->flags & AZ_FLAG_NO_GRAPH)) && !timer && !guide && st != nullptr &&
+                           st != cudaStreamLegacy && st != cudaStreamPerThread;
     uint64_t pos = 0;
     while (pos < total) {
         uint32_t n = (uint32_t)std::min<uint64_t>(chunk, total - pos);
@@ -996,7 +1092,11 @@ int Render(GpuScene &G, az_pixel *film, const az_camera *camera, const az_epsilo
                                                                          (uint64_t)n * 4), 1024);
         rc = W.Ensure(n, cap_q, cap_s);
         if (rc != AZ_OK) return rc;
-        rc = RenderWave(G, cam, W, pos, n, film, st, sms, counters, timer.get(), guide, train);
+        if (use_graph) {
+            rc = ReplayWave(G, cam, W, pos, n, chunk, film, st, sms, counters);
+        } else {
+            rc = RenderWave(G, cam, W, pos, n, film, st, sms, counters, timer.get(), guide, train);
+        }
         if (rc != AZ_OK) return rc;
         AZ_CUDA_TRY(cudaMemcpyAsync(host_counts.data(), W.q.counts, AZ_COUNT_TOTAL * sizeof(uint32_t),
                                     cudaMemcpyDeviceToHost, st));

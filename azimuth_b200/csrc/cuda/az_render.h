@@ -47,6 +47,10 @@ struct WaveQueues {
     uint32_t cap_s;
     float4 *accum;                          // per-sample radiance sums
     uint32_t *counts;                       // see AZ_COUNT_*
+    // [first sample, sample count, seed] of the current wave when set: a
+    // captured CUDA graph replays the same launches for every wave and reads
+    // them here; null: the kernels' arguments and cam.seed
+    const uint64_t *wave;
     // path guiding (null when rendering without a guide)
     const azd::GuideLobes *lobes;           // per extension-queue entry of the current level
     azd::GuideRecord *rec;                  // [level][n_rec] training vertices
@@ -57,7 +61,14 @@ struct WaveBuffers {
     WaveQueues q{};
     uint32_t chunk = 0;
     std::vector<void *> ptrs;
+    // the per-wave launches captured as a CUDA graph, with what they were captured for
+    uint64_t *wave_dev = nullptr;          // device copy of the wave descriptor
+    uint64_t *wave_host = nullptr;         // pinned staging for it
+    cudaGraphExec_t graph = nullptr;
+    std::vector<unsigned char> graph_key;
+    uint64_t graph_launches = 0, graph_extend_launches = 0;   // kernels in the graph
     ~WaveBuffers();
+    void DropGraph();
     int Ensure(uint32_t chunk, uint32_t cap_q, uint32_t cap_s);
 };
 

@@ -131,6 +131,52 @@ int az_gpu_autotune_scene(const az_scene *host_scene, az_gpu_scene *scene, const
                           uint32_t backface_culling, const az_render_opts *opts, uint32_t *width_out,
                           uint32_t *variant_out, float *ms_out);
 
+/* ---- Batched render jobs (no counterpart in azimuth, which renders one camera per call) ----
+ *
+ * Many render jobs of uneven size, scene and settings in one call: the jobs
+ * run concurrently on `streams` CUDA streams (default 4), largest first, each
+ * stream with its own wave queues; a job of several waves replays its wave
+ * launches as one CUDA graph.  Each job is az_gpu_render (or, with a guide,
+ * az_gpu_render_guided) of its own scene, camera and DEVICE film.  Jobs that
+ * share a guide run one after another. */
+typedef struct az_job {
+    az_gpu_scene *scene;
+    struct az_guide *guide;         /* NULL: plain render */
+    az_pixel *film;                 /* DEVICE film, W*H of the job's camera, accumulated into */
+    const az_camera *camera;
+    const az_epsilon_values *epsilons;
+    az_scissor scissor;
+    int32_t filter_type;
+    uint32_t backface_culling;
+    uint32_t train;                 /* guided jobs: train the guide while rendering */
+    uint32_t reserved0;
+    uint64_t seed;
+    /* written by az_gpu_render_batch */
+    float done_ms;                  /* completion time after the batch started (device clock) */
+    int32_t status;                 /* AZ_OK or the job's error */
+    uint64_t samples;
+} az_job;
+
+typedef struct az_batch_opts {
+    int32_t device;
+    uint32_t streams;               /* concurrent jobs; 0 = 4 */
+    uint32_t flags;                 /* AZ_FLAG_* applied to every job */
+    uint32_t chunk_samples;         /* 0 = library default */
+    uint32_t reserved[4];
+} az_batch_opts;
+
+typedef struct az_batch_stats {
+    uint64_t samples;               /* camera samples of all jobs */
+    float gpu_ms;                   /* batch start to the last job's completion */
+    float p50_ms, p99_ms;           /* job completion times */
+    uint32_t jobs, failed, streams;
+    uint32_t reserved[3];
+} az_batch_stats;
+
+/* Returns AZ_OK when every job succeeded, else the first failing job's status
+ * (see each job's `status`). Synchronous. */
+int az_gpu_render_batch(az_job *jobs, uint32_t n, const az_batch_opts *opts, az_batch_stats *stats);
+
 /* ---- Neural path guiding (the learned proposal; no counterpart in azimuth) ----
  *
  * A guide belongs to one device scene.  Rendered with az_gpu_render_guided,
