@@ -329,9 +329,10 @@ class Guide:
             pass
 
 
-def render_batch(jobs, streams=0, flags=0, chunk_samples=0, device=0):
+def render_batch(jobs, streams=0, flags=0, chunk_samples=0, device=0, largest_first=False):
     """az_gpu_render_batch.  jobs: list of dicts with keys gpu_scene (GpuScene), film_ptr (device film of
-    the scene's camera resolution) and optionally guide (Guide), train, seed, scissor.  Returns
+    the scene's camera resolution) and optionally guide (Guide), train, seed, scissor, and camera_ptr,
+    epsilons_ptr, filter_type (default: those of the GpuScene's host scene).  Returns
     (per-job list of dicts done_ms/status/samples, batch stats dict)."""
     arr = (Job * len(jobs))()
     for k, j in enumerate(jobs):
@@ -341,10 +342,10 @@ def render_batch(jobs, streams=0, flags=0, chunk_samples=0, device=0):
         a.scene = gs._h
         a.guide = j["guide"]._h if j.get("guide") is not None else None
         a.film = j["film_ptr"]
-        a.camera = sc_.camera_ptr
-        a.epsilons = sc_.epsilons_ptr
+        a.camera = j.get("camera_ptr") or sc_.camera_ptr
+        a.epsilons = j.get("epsilons_ptr") or sc_.epsilons_ptr
         a.scissor = j.get("scissor") or full_scissor(sc_)
-        a.filter_type = sc_.filter_type
+        a.filter_type = j["filter_type"] if "filter_type" in j else sc_.filter_type
         a.backface_culling = 0
         a.train = 1 if j.get("train") else 0
         a.seed = j.get("seed", 0)
@@ -353,6 +354,7 @@ def render_batch(jobs, streams=0, flags=0, chunk_samples=0, device=0):
     o.streams = streams
     o.flags = flags
     o.chunk_samples = chunk_samples
+    o.largest_first = 1 if largest_first else 0
     st = BatchStats()
     rc = lib().az_gpu_render_batch(arr, len(jobs), C.byref(o), C.byref(st))
     per = [{"done_ms": arr[k].done_ms, "status": arr[k].status, "samples": arr[k].samples} for k in range(len(jobs))]

@@ -58,7 +58,7 @@ class Job(C.Structure):
 
 class BatchOpts(C.Structure):
     _fields_ = [("device", C.c_int32), ("streams", C.c_uint32), ("flags", C.c_uint32), ("chunk_samples", C.c_uint32),
-                ("reserved", C.c_uint32 * 4)]
+                ("largest_first", C.c_uint32), ("reserved", C.c_uint32 * 3)]
 
 
 class BatchStats(C.Structure):

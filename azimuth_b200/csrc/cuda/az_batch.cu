@@ -2,9 +2,10 @@
 // and scene in one call (az_gpu_render_batch, include/azimuth_gpu.h).
 //
 // One host worker per CUDA stream pulls the next job from a shared queue
-// ordered by estimated cost (samples x tree levels, largest first, so that
-// the long jobs do not end up alone at the tail) and renders it with its own
-// wave queues; the streams run concurrently on the device, so small jobs fill
+// ordered by estimated cost (samples x tree levels): shortest first by
+// default, which minimises the jobs' completion times (a large job's waves
+// fill the GPU on their own, so it loses little by starting late), or
+// largest first; each worker renders with its own wave queues; the streams run concurrently on the device, so small jobs fill
 // the SMs that a large job's waves leave idle.  A job of three or more waves
 // replays its per-wave launches as one CUDA graph.  Completion times are
 // device times between an event recorded before any job and each job's end
@@ -64,8 +65,8 @@ extern "C" int az_gpu_render_batch(az_job *jobs, uint32_t n, const az_batch_opts
     const uint32_t S = std::max(1u, std::min(opts && opts->streams ? opts->streams : 4u, n));
     const uint32_t chunk = opts && opts->chunk_samples ? opts->chunk_samples : (1u << 22);
 
-    // largest first
     std::vector<uint32_t> order(n);
+    const bool largest_first = opts && opts->largest_first;
     std::vector<double> cost(n);
     for (uint32_t i = 0; i < n; i++) {
         order[i] = i;
@@ -74,7 +75,8 @@ extern "C" int az_gpu_render_batch(az_job *jobs, uint32_t n, const az_batch_opts
         jobs[i].status = AZ_OK;
         jobs[i].done_ms = 0.0f;
     }
-    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return cost[a] > cost[b]; });
+    std::stable_sort(order.begin(), order.end(),
+                     [&](uint32_t a, uint32_t b) { return largest_first ? cost[a] > cost[b] : cost[a] < cost[b]; });
 
     std::vector<std::unique_ptr<Worker>> workers;
     std::vector<cudaEvent_t> done(n, nullptr);

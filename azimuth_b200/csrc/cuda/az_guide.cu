@@ -636,10 +636,7 @@ struct GuideState {
     uint2 *wf = nullptr, *wt = nullptr;
     __half2 *feat = nullptr;
     float2 *grid = nullptr, *grid_grad = nullptr, *grid_m = nullptr, *grid_v = nullptr;
-    GuideLobes *lobes = nullptr;
-    size_t lobes_cap = 0;
-    GuideRecord *rec = nullptr;
-    uint32_t n_rec = 0, rec_levels = 0;
+    uint32_t n_rec = 0;             // samples per wave whose vertices are recorded
     GuideRow *rows = nullptr;
     uint32_t rows_cap = 0;
     uint32_t *count = nullptr;      // [0] rows, then scratch
@@ -655,8 +652,6 @@ struct GuideState {
     ~GuideState() {
         for (void *p : allocs)
             if (p) cudaFree(p);
-        if (lobes) cudaFree(lobes);
-        if (rec) cudaFree(rec);
     }
     template <typename T>
     T *Alloc(size_t n) {
@@ -815,38 +810,40 @@ int CreateGuide(const GpuScene &G, const az_guide_config *cfg, GuideState **out)
 
 void DestroyGuide(GuideState *g) { delete g; }
 
-int GuidePrepareWave(GuideState &g, WaveQueues &Q, uint32_t cap_q, uint32_t levels, cudaStream_t st) {
-    if (g.lobes_cap < cap_q) {
-        if (g.lobes) cudaFree(g.lobes);
-        g.lobes = nullptr;
-        g.lobes_cap = 0;
-        if (cudaMalloc((void **)&g.lobes, (size_t)cap_q * sizeof(GuideLobes)) != cudaSuccess)
+int GuidePrepareWave(GuideState &g, WaveBuffers &W, WaveQueues &Q, uint32_t cap_q, uint32_t levels, cudaStream_t st) {
+    if (W.guide_lobes_cap < cap_q) {
+        if (W.guide_lobes) cudaFree(W.guide_lobes);
+        W.guide_lobes = nullptr;
+        W.guide_lobes_cap = 0;
+        if (cudaMalloc((void **)&W.guide_lobes, (size_t)cap_q * sizeof(GuideLobes)) != cudaSuccess)
             return SetError(AZ_ERR_OUT_OF_MEMORY, "path guide proposals");
-        g.lobes_cap = cap_q;
+        W.guide_lobes_cap = cap_q;
     }
-    Q.lobes = g.lobes;
+    Q.lobes = W.guide_lobes;
+    Q.cap_q = std::min<uint32_t>(Q.cap_q, (uint32_t)W.guide_lobes_cap);
     Q.rec = nullptr;
     Q.n_rec = 0;
     Q.rec_levels = 0;
     if (levels == 0) return AZ_OK;   // not training: no records
-    if (g.rec_levels < levels) {
-        if (g.rec) cudaFree(g.rec);
-        g.rec = nullptr;
-        g.rec_levels = 0;
-        if (cudaMalloc((void **)&g.rec, (size_t)levels * g.n_rec * sizeof(GuideRecord)) != cudaSuccess)
+    const size_t need = (size_t)levels * g.n_rec;
+    if (W.guide_rec_cap < need) {
+        if (W.guide_rec) cudaFree(W.guide_rec);
+        W.guide_rec = nullptr;
+        W.guide_rec_cap = 0;
+        if (cudaMalloc((void **)&W.guide_rec, need * sizeof(GuideRecord)) != cudaSuccess)
             return SetError(AZ_ERR_OUT_OF_MEMORY, "path guide records");
-        g.rec_levels = levels;
+        W.guide_rec_cap = need;
     }
     // records of earlier waves must not be mistaken for this wave's
-    AZ_CUDA_TRY(cudaMemsetAsync(g.rec, 0, (size_t)g.rec_levels * g.n_rec * sizeof(GuideRecord), st));
-    Q.rec = g.rec;
+    AZ_CUDA_TRY(cudaMemsetAsync(W.guide_rec, 0, need * sizeof(GuideRecord), st));
+    Q.rec = W.guide_rec;
     Q.n_rec = g.n_rec;
-    Q.rec_levels = g.rec_levels;
+    Q.rec_levels = levels;
     return AZ_OK;
 }
 
 int GuideInfer(GuideState &g, const GpuScene &G, const WaveQueues &Q, uint32_t level, cudaStream_t st) {
-    k_guide_infer<<<g.sms * 4, kWarps * 32, kInferSmem, st>>>(G.dev, Q, level, g.net, g.lobes);
+    k_guide_infer<<<g.sms * 4, kWarps * 32, kInferSmem, st>>>(G.dev, Q, level, g.net, Q.lobes);
     AZ_CUDA_TRY(cudaGetLastError());
     return AZ_OK;
 }
@@ -854,7 +851,7 @@ int GuideInfer(GuideState &g, const GpuScene &G, const WaveQueues &Q, uint32_t l
 int GuideTrainWave(GuideState &g, const WaveQueues &Q, cudaStream_t st) {
     AZ_CUDA_TRY(cudaMemsetAsync(g.count, 0, 4 * sizeof(uint32_t), st));
     AZ_CUDA_TRY(cudaMemsetAsync(g.wsum, 0, sizeof(float), st));
-    k_guide_targets<<<g.sms * 4, 256, 0, st>>>(g.rec, g.n_rec, g.rec_levels, Q.accum, g.rows, g.rows_cap, g.count,
+    k_guide_targets<<<g.sms * 4, 256, 0, st>>>(Q.rec, Q.n_rec, Q.rec_levels, Q.accum, g.rows, g.rows_cap, g.count,
                                                g.wsum);
     AZ_CUDA_TRY(cudaGetLastError());
     return TrainStep(g, g.rows, g.count, g.rows_cap, g.wsum, st);

@@ -72,9 +72,10 @@ int SetupCamera(const az_camera *c, az_scissor sc, int32_t filter, uint32_t cull
 struct GuideState;
 int CreateGuide(const GpuScene &G, const az_guide_config *cfg, GuideState **out);
 void DestroyGuide(GuideState *g);
-// Proposal and training-record buffers of a wave with `cap_q` queue entries
-// and `levels` tree levels; sets the guide fields of Q.
-int GuidePrepareWave(GuideState &g, WaveQueues &Q, uint32_t cap_q, uint32_t levels, cudaStream_t st);
+// Proposal and training-record buffers (in W) of a wave whose queues hold at
+// most `cap_q` entries and `levels` tree levels; sets the guide fields of Q and
+// lowers Q.cap_q to the proposals' capacity.
+int GuidePrepareWave(GuideState &g, WaveBuffers &W, WaveQueues &Q, uint32_t cap_q, uint32_t levels, cudaStream_t st);
 // Proposals for the extension queue of `level` (between extend and shade).
 int GuideInfer(GuideState &g, const GpuScene &G, const WaveQueues &Q, uint32_t level, cudaStream_t st);
 // Training targets of the finished wave and one Adam step.

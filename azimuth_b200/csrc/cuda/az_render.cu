@@ -863,6 +863,8 @@ WaveBuffers::~WaveBuffers() {
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (wave_host) cudaFreeHost(wave_host);
+    if (guide_lobes) cudaFree(guide_lobes);
+    if (guide_rec) cudaFree(guide_rec);
 }
 
 void WaveBuffers::DropGraph() {
@@ -953,7 +955,8 @@ static int RenderWave(const GpuScene &G, const CameraParams &cam, WaveBuffers &W
     if (capture) Q.wave = W.wave_dev;
     const uint32_t levels = std::min<uint32_t>(G.dev.max_depth + 1, AZ_MAX_LEVELS - 2);
     if (guide) {
-        int grc = GuidePrepareWave(*guide, Q, Q.cap_q, train ? levels : 0u, st);
+        // proposals for every queue entry this wave can hold (the queue is capped to match)
+        int grc = GuidePrepareWave(*guide, W, Q, std::min<uint32_t>(Q.cap_q, n + n / 2 + 1024), train ? levels : 0u, st);
         if (grc != AZ_OK) return grc;
     }
     AZ_CUDA_TRY(cudaMemsetAsync(Q.counts, 0, AZ_COUNT_TOTAL * sizeof(uint32_t), st));

@@ -52,7 +52,7 @@ struct WaveQueues {
     // them here; null: the kernels' arguments and cam.seed
     const uint64_t *wave;
     // path guiding (null when rendering without a guide)
-    const azd::GuideLobes *lobes;           // per extension-queue entry of the current level
+    azd::GuideLobes *lobes;                 // per extension-queue entry of the current level
     azd::GuideRecord *rec;                  // [level][n_rec] training vertices
     uint32_t n_rec, rec_levels;
 };
@@ -67,6 +67,11 @@ struct WaveBuffers {
     cudaGraphExec_t graph = nullptr;
     std::vector<unsigned char> graph_key;
     uint64_t graph_launches = 0, graph_extend_launches = 0;   // kernels in the graph
+    // scratch of guided waves: proposals per queue entry, training records
+    azd::GuideLobes *guide_lobes = nullptr;
+    size_t guide_lobes_cap = 0;
+    azd::GuideRecord *guide_rec = nullptr;
+    size_t guide_rec_cap = 0;
     ~WaveBuffers();
     void DropGraph();
     int Ensure(uint32_t chunk, uint32_t cap_q, uint32_t cap_s);

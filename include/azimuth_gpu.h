@@ -134,9 +134,9 @@ int az_gpu_autotune_scene(const az_scene *host_scene, az_gpu_scene *scene, const
 /* ---- Batched render jobs (no counterpart in azimuth, which renders one camera per call) ----
  *
  * Many render jobs of uneven size, scene and settings in one call: the jobs
- * run concurrently on `streams` CUDA streams (default 4), largest first, each
- * stream with its own wave queues; a job of several waves replays its wave
- * launches as one CUDA graph.  Each job is az_gpu_render (or, with a guide,
+ * run concurrently on `streams` CUDA streams (default 4), shortest first (or
+ * largest first), each stream with its own wave queues; a job of several
+ * waves replays its wave launches as one CUDA graph.  Each job is az_gpu_render (or, with a guide,
  * az_gpu_render_guided) of its own scene, camera and DEVICE film.  Jobs that
  * share a guide run one after another. */
 typedef struct az_job {
@@ -162,7 +162,8 @@ typedef struct az_batch_opts {
     uint32_t streams;               /* concurrent jobs; 0 = 4 */
     uint32_t flags;                 /* AZ_FLAG_* applied to every job */
     uint32_t chunk_samples;         /* 0 = library default */
-    uint32_t reserved[4];
+    uint32_t largest_first;         /* 0: shortest jobs first (low completion times); 1: largest first */
+    uint32_t reserved[3];
 } az_batch_opts;
 
 typedef struct az_batch_stats {
