@@ -32,6 +32,7 @@ FILTER_GAUSSIAN = 1
 FLAG_COUNT_TRAVERSAL = 1
 FLAG_NO_GRAPH = 2
 FLAG_TIME_STAGES = 4
+FLAG_ENV_IMPORTANCE = 8
 LAUNCH_VARIANTS = 14   # AZ_LAUNCH_VARIANTS
 
 STATUS = {0: "AZ_OK", 1: "AZ_ERR_INVALID_ARGUMENT", 2: "AZ_ERR_INVALID_SCENE", 3: "AZ_ERR_OUT_OF_MEMORY",

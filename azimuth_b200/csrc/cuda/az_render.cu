@@ -106,17 +106,18 @@ __device__ __forceinline__ void push_shadow(const WaveQueues &Q, uint32_t level,
 // GetSampleCoord + GetRayForPixel (src/azimuth_main.cpp:1135-1178).
 __global__ void k_camera(CameraParams cam, WaveQueues Q, uint64_t wave_start, uint32_t n) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint64_t seed = cam.seed;
     if (Q.wave) {
         wave_start = Q.wave[0];
         n = (uint32_t)Q.wave[1];
-        cam.seed = Q.wave[2];
+        seed = Q.wave[2];
         if (i == 0) Q.counts[1] = n;   // the level-1 queue is the wave itself
     }
     if (i >= n) return;
     uint32_t row, col, sx, sy;
     sample_of(cam, wave_start + i, row, col, sx, sy);
     NodeRng rng;
-    rng.init(cam.seed, (row << 16) | col, (sy << 16) | sx, 0u, 0u);
+    rng.init(seed, (row << 16) | col, (sy << 16) | sx, 0u, 0u);
     float cx = (float)col + (0.5f * cam.inv_sqrt + (float)sx * cam.inv_sqrt);
     float cy = (float)row + (0.5f * cam.inv_sqrt + (float)sy * cam.inv_sqrt);
     // the lens pair is drawn y first: GCC evaluates the two Random01()
@@ -266,7 +267,7 @@ __device__ __forceinline__ f3 ld3(const float *p) { return mk(p[0], p[1], p[2]);
 // src/azimuth_main.cpp:974-1130).  FEAT (DevScene.features) compiles out the
 // parts a scene cannot reach: textures, environment map, mirror/dielectric
 // branches, point/area/directional/spot lights.
-template <int BLOCK, uint32_t FEAT>
+template <int BLOCK, uint32_t FEAT, bool GUIDED>
 __global__ void __launch_bounds__(BLOCK) k_shade(DevScene S, CameraParams cam, WaveQueues Q, uint64_t wave_start,
                                                  uint32_t level) {
     constexpr bool TEX = FEAT & FEAT_TEXTURES, ENV = FEAT & FEAT_ENV, SPECIAL = FEAT & FEAT_SPECIAL,
@@ -275,9 +276,10 @@ __global__ void __launch_bounds__(BLOCK) k_shade(DevScene S, CameraParams cam, W
     const uint32_t n = min(Q.counts[level], Q.cap_q);
     const bool can_spawn = level + 1 <= S.max_depth + 1;   // child's RecursionDepth <= MaxRecursionDepth
     const float seps = cam.eps_shadow;
+    uint64_t seed = cam.seed;
     if (Q.wave) {
         wave_start = Q.wave[0];
-        cam.seed = Q.wave[2];
+        seed = Q.wave[2];
     }
     for (uint32_t i = blockIdx.x * BLOCK + threadIdx.x; i < n; i += gridDim.x * BLOCK) {
         const float4 o4 = Q.o[buf][i], d4 = Q.d[buf][i], tp4 = Q.tp[buf][i];
@@ -299,7 +301,7 @@ __global__ void __launch_bounds__(BLOCK) k_shade(DevScene S, CameraParams cam, W
         // path-guide training: this node is the only child of the vertex recorded
         // one level up, so the sample's sum now holds everything up to that
         // vertex's level
-        const bool recordable = Q.rec && slot < Q.n_rec && !(flags & PF_BRANCHED);
+        const bool recordable = GUIDED && Q.rec && slot < Q.n_rec && !(flags & PF_BRANCHED);
         if (recordable && level >= 2 && level - 2 < Q.rec_levels) {
             const float4 a = Q.accum[slot];
             Q.rec[(size_t)(level - 2) * Q.n_rec + slot].snap = make_float4(a.x, a.y, a.z, 1.0f);
@@ -325,7 +327,7 @@ __global__ void __launch_bounds__(BLOCK) k_shade(DevScene S, CameraParams cam, W
         }
         NodeRng rng;
         const uint32_t digits = Q.digits[buf][i];
-        rng.init(cam.seed, (row << 16) | col, (sy << 16) | sx, digits, level);
+        rng.init(seed, (row << 16) | col, (sy << 16) | sx, digits, level);
         const Surface s = surface_at<TEX>(S, r, h);
         const DevMaterial &m = S.materials[e.material];
         f3 dcol = ld3(m.diffuse), scol = ld3(m.specular);
@@ -397,19 +399,28 @@ __global__ void __launch_bounds__(BLOCK) k_shade(DevScene S, CameraParams cam, W
         }
         if (ENV && S.use_env_map) {
             // cosine-sampled environment ray (:724-778); not gated by InsideDielectric
-            float phi = 2.0f * AZD_PI_F32 * rng.next();
-            float cp = cosf(phi), sp = sinf(phi);
-            float theta = asinf(sqrtf(rng.next()));
-            float ct = cosf(theta), st = sinf(theta);
-            f3 U, V;
-            onb(s.n, U, V);
-            f3 Ld = normalize(U * st * cp + V * st * sp + s.n * ct);
+            f3 Ld;
+            float env_invpdf;
+            if (cam.env_importance) {
+                // the same two draws, through one-sample MIS of the map's luminance CDF and cosine sampling
+                const float u1 = rng.next(), u2 = rng.next();
+                env_invpdf = sample_env_mis(S, s.n, u1, u2, Ld);
+            } else {
+                float phi = 2.0f * AZD_PI_F32 * rng.next();
+                float cp = cosf(phi), sp = sinf(phi);
+                float theta = asinf(sqrtf(rng.next()));
+                float ct = cosf(theta), st = sinf(theta);
+                f3 U, V;
+                onb(s.n, U, V);
+                Ld = normalize(U * st * cp + V * st * sp + s.n * ct);
+                float ca = dot(Ld, s.n);
+                if (ca == 0.0f) ca = 0.000001f;
+                env_invpdf = AZD_PI_F32 / ca;
+            }
             float u = (-atan2f(Ld.z, Ld.x) + AZD_PI_F32) / (2.0f * AZD_PI_F32), v = acosf(Ld.y) / AZD_PI_F32;
             f3 I = sample_texture(S, S.textures[S.env_texture], mk(u, v, 1.0f), u, v);
-            float ca = dot(Ld, s.n);
-            if (ca == 0.0f) ca = 0.000001f;
             f3 dc, sc;
-            if (light_contribution(dc, sc, m, I, Ld, r.d, s.n, 1.0f, 1.0f, AZD_PI_F32 / ca)) {
+            if (env_invpdf > 0.0f && light_contribution(dc, sc, m, I, Ld, r.d, s.n, 1.0f, 1.0f, env_invpdf)) {
                 f3 c = had(tp, had(dcol, dc) + had(scol, sc));
                 if (!is_zero(c)) push_shadow(Q, level, s.p + (Ld * seps), r.time, Ld, FLT_MAX, c, slot, SHADOW_ANY, 0u);
             }
@@ -422,7 +433,7 @@ __global__ void __launch_bounds__(BLOCK) k_shade(DevScene S, CameraParams cam, W
             // diffuse scatter ray (:1029-1083): child 0
             f3 Sd;
             float invpdf, qpdf = 0.0f;
-            if (Q.lobes) {
+            if (GUIDED) {
                 // path guiding: one-sample MIS of the learned vMF mixture and
                 // cosine sampling, weighted by the mixture density
                 const GuideLobes &G = Q.lobes[i];
@@ -737,29 +748,33 @@ static_assert(kVariantCount == AZ_LAUNCH_VARIANTS, "variant table and header dis
 
 template <uint32_t F>
 void LaunchShadeF(int grid, const DevScene &S, const CameraParams &cam, const WaveQueues &Q, uint64_t start,
-                  uint32_t L, cudaStream_t st) {
-    k_shade<kBlock, F><<<grid, kBlock, 0, st>>>(S, cam, Q, start, L);
+                  uint32_t L, cudaStream_t st, bool guided) {
+    if (guided) k_shade<kBlock, F, true><<<grid, kBlock, 0, st>>>(S, cam, Q, start, L);
+    else k_shade<kBlock, F, false><<<grid, kBlock, 0, st>>>(S, cam, Q, start, L);
 }
 
+// The shading kernel specialised for the scene's features (DevScene.features)
+// and for guided scattering (Q.lobes set).
 void LaunchShade(int grid, const DevScene &S, const CameraParams &cam, const WaveQueues &Q, uint64_t start,
                  uint32_t L, cudaStream_t st) {
+    const bool guided = Q.lobes != nullptr;
     switch (S.features & 15u) {
-        case 0: LaunchShadeF<0>(grid, S, cam, Q, start, L, st); break;
-        case 1: LaunchShadeF<1>(grid, S, cam, Q, start, L, st); break;
-        case 2: LaunchShadeF<2>(grid, S, cam, Q, start, L, st); break;
-        case 3: LaunchShadeF<3>(grid, S, cam, Q, start, L, st); break;
-        case 4: LaunchShadeF<4>(grid, S, cam, Q, start, L, st); break;
-        case 5: LaunchShadeF<5>(grid, S, cam, Q, start, L, st); break;
-        case 6: LaunchShadeF<6>(grid, S, cam, Q, start, L, st); break;
-        case 7: LaunchShadeF<7>(grid, S, cam, Q, start, L, st); break;
-        case 8: LaunchShadeF<8>(grid, S, cam, Q, start, L, st); break;
-        case 9: LaunchShadeF<9>(grid, S, cam, Q, start, L, st); break;
-        case 10: LaunchShadeF<10>(grid, S, cam, Q, start, L, st); break;
-        case 11: LaunchShadeF<11>(grid, S, cam, Q, start, L, st); break;
-        case 12: LaunchShadeF<12>(grid, S, cam, Q, start, L, st); break;
-        case 13: LaunchShadeF<13>(grid, S, cam, Q, start, L, st); break;
-        case 14: LaunchShadeF<14>(grid, S, cam, Q, start, L, st); break;
-        default: LaunchShadeF<15>(grid, S, cam, Q, start, L, st); break;
+        case 0: LaunchShadeF<0>(grid, S, cam, Q, start, L, st, guided); break;
+        case 1: LaunchShadeF<1>(grid, S, cam, Q, start, L, st, guided); break;
+        case 2: LaunchShadeF<2>(grid, S, cam, Q, start, L, st, guided); break;
+        case 3: LaunchShadeF<3>(grid, S, cam, Q, start, L, st, guided); break;
+        case 4: LaunchShadeF<4>(grid, S, cam, Q, start, L, st, guided); break;
+        case 5: LaunchShadeF<5>(grid, S, cam, Q, start, L, st, guided); break;
+        case 6: LaunchShadeF<6>(grid, S, cam, Q, start, L, st, guided); break;
+        case 7: LaunchShadeF<7>(grid, S, cam, Q, start, L, st, guided); break;
+        case 8: LaunchShadeF<8>(grid, S, cam, Q, start, L, st, guided); break;
+        case 9: LaunchShadeF<9>(grid, S, cam, Q, start, L, st, guided); break;
+        case 10: LaunchShadeF<10>(grid, S, cam, Q, start, L, st, guided); break;
+        case 11: LaunchShadeF<11>(grid, S, cam, Q, start, L, st, guided); break;
+        case 12: LaunchShadeF<12>(grid, S, cam, Q, start, L, st, guided); break;
+        case 13: LaunchShadeF<13>(grid, S, cam, Q, start, L, st, guided); break;
+        case 14: LaunchShadeF<14>(grid, S, cam, Q, start, L, st, guided); break;
+        default: LaunchShadeF<15>(grid, S, cam, Q, start, L, st, guided); break;
     }
 }
 
@@ -1057,6 +1072,7 @@ int Render(GpuScene &G, az_pixel *film, const az_camera *camera, const az_epsilo
     int rc = SetupCamera(camera, sc, filter, cull, eps, opts ? opts->seed : 0, cam);
     if (rc != AZ_OK) return rc;
     cam.count_traversal = opts && (opts->flags & AZ_FLAG_COUNT_TRAVERSAL) ? 1u : 0u;
+    cam.env_importance = opts && (opts->flags & AZ_FLAG_ENV_IMPORTANCE) && G.dev.env_rows ? 1u : 0u;
     cam.variant = opts && opts->variant ? opts->variant - 1 : G.variant;
     if (cam.variant >= kVariantCount) return SetError(AZ_ERR_INVALID_ARGUMENT, "unknown launch variant");
     if (G.dev.max_depth + 1 > AZ_MAX_LEVELS - 2) return SetError(AZ_ERR_UNSUPPORTED, "MaxRecursionDepth above 60");

@@ -34,6 +34,7 @@ struct CameraParams {
     uint32_t cull;
     uint32_t count_traversal;
     uint32_t variant;              // launch configuration of the traversal kernels
+    uint32_t env_importance;       // AZ_FLAG_ENV_IMPORTANCE
 };
 
 // Device queues of one wave of camera samples (structure of arrays).

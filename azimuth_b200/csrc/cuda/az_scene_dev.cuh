@@ -172,6 +172,11 @@ struct DevScene {
     uint32_t light_draws;           // RNG draws made by the light loop at every vertex
     uint32_t features;              // FEAT_* bits
     uint32_t full_light_queries;    // 1: an entity light needs full nearest-hit visibility queries
+    // luminance CDF of a 2D environment map (null when the scene has none):
+    // env_rows[0..H] over rows (weighted by sin theta), env_cols[r * (W + 1) + 0..W] within row r
+    const float *env_rows;
+    const float *env_cols;
+    uint32_t env_cdf_w, env_cdf_h;
 };
 
 }  // namespace azd

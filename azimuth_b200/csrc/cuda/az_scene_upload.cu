@@ -645,6 +645,79 @@ int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_
     D.light_count = (uint32_t)lights.size();
     D.bg_texture = bg_idx;
     D.env_texture = env_idx;
+    // luminance CDF of a 2D environment map for AZ_FLAG_ENV_IMPORTANCE: per
+    // texel the largest luminance of its 3 x 3 neighbourhood (the lookup's
+    // nearest texel is round(u (W - 1)), up to one texel off this CDF's
+    // floor(u W) cells, and a bilinear lookup blends neighbours), times
+    // sin(theta) of its row centre, plus a small floor
+    D.env_rows = D.env_cols = nullptr;
+    D.env_cdf_w = D.env_cdf_h = 0;
+    {
+        const az_texture &E = scene->EnvironmentMap;
+        if (scene->UseEnvironmentMap && E.Type != AZ_TextureType_PerlinNoise && E.Pixels && E.Width && E.Height) {
+            const uint32_t W = E.Width, H = E.Height;
+            std::vector<double> lum((size_t)W * H);
+            double total_l = 0.0;
+            for (uint32_t y = 0; y < H; y++)
+                for (uint32_t x = 0; x < W; x++) {
+                    double rgb[3];
+                    const size_t i = (size_t)y * W + x;
+                    for (int c = 0; c < 3; c++)
+                        rgb[c] = E.PixelFormat == AZ_PixelFormat_RGB_F32 ? (double)((const float *)E.Pixels)[3 * i + c]
+                                                                          : (double)((const uint8_t *)E.Pixels)[3 * i + c];
+                    const double l = std::max(0.0, 0.2126 * rgb[0] + 0.7152 * rgb[1] + 0.0722 * rgb[2]);
+                    lum[i] = l;
+                    total_l += l;
+                }
+            const double floor_l = 1e-3 * total_l / ((double)W * H) + 1e-30;
+            {
+                std::vector<double> dil(lum.size());
+                for (uint32_t y = 0; y < H; y++)
+                    for (uint32_t x = 0; x < W; x++) {
+                        double m = 0.0;
+                        for (int dy = -1; dy <= 1; dy++) {
+                            const int yy = std::min<int>((int)H - 1, std::max<int>(0, (int)y + dy));
+                            for (int dx = -1; dx <= 1; dx++) {
+                                const int xx = ((int)x + dx + (int)W) % (int)W;
+                                m = std::max(m, lum[(size_t)yy * W + xx]);
+                            }
+                        }
+                        dil[(size_t)y * W + x] = m;
+                    }
+                lum.swap(dil);
+            }
+            std::vector<float> rows(H + 1), cols((size_t)H * (W + 1));
+            std::vector<double> row_w(H);
+            double tot = 0.0;
+            for (uint32_t y = 0; y < H; y++) {
+                const double st = std::sin(3.14159265358979323846 * (y + 0.5) / H);
+                double acc = 0.0;
+                for (uint32_t x = 0; x < W; x++) acc += lum[(size_t)y * W + x] + floor_l;
+                double run = 0.0;
+                cols[(size_t)y * (W + 1)] = 0.0f;
+                for (uint32_t x = 0; x < W; x++) {
+                    run += lum[(size_t)y * W + x] + floor_l;
+                    cols[(size_t)y * (W + 1) + x + 1] = (float)(run / acc);
+                }
+                cols[(size_t)y * (W + 1) + W] = 1.0f;
+                row_w[y] = acc * st;
+                tot += row_w[y];
+            }
+            double run = 0.0;
+            rows[0] = 0.0f;
+            for (uint32_t y = 0; y < H; y++) {
+                run += row_w[y];
+                rows[y + 1] = (float)(run / tot);
+            }
+            rows[H] = 1.0f;
+            int urc = AZ_OK;
+            D.env_rows = Upload(*G, rows, st, urc);
+            if (urc == AZ_OK) D.env_cols = Upload(*G, cols, st, urc);
+            if (urc != AZ_OK) return urc;
+            D.env_cdf_w = W;
+            D.env_cdf_h = H;
+        }
+    }
     memcpy(D.ambient, &scene->AmbientLight, 12);
     memcpy(D.background, &scene->BackgroundColor, 12);
     D.use_bg_texture = scene->UseBackgroundTexture ? 1u : 0u;

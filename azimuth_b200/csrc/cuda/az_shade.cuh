@@ -225,6 +225,67 @@ __device__ Surface surface_at(const DevScene &S, const Ray &wr, const Hit &h) {
     return s;
 }
 
+// Density over solid angle of the environment map's luminance CDF
+// (DevScene.env_rows / env_cols) at direction d: p(u, v) / (2 pi^2 sin theta)
+// with the equirectangular mapping of background().
+__device__ __forceinline__ float env_cdf_pdf(const DevScene &S, f3 d) {
+    const uint32_t H = S.env_cdf_h, W = S.env_cdf_w;
+    const float theta = acosf(fminf(1.0f, fmaxf(-1.0f, d.y)));
+    const float u = (-atan2f(d.z, d.x) + AZD_PI_F32) / (2.0f * AZD_PI_F32), v = theta / AZD_PI_F32;
+    const uint32_t r = min((uint32_t)fmaxf(0.0f, v * (float)H), H - 1u);
+    const uint32_t c = min((uint32_t)fmaxf(0.0f, u * (float)W), W - 1u);
+    const float *cc = S.env_cols + (size_t)r * (W + 1);
+    const float pdf_uv = (S.env_rows[r + 1] - S.env_rows[r]) * (cc[c + 1] - cc[c]) * (float)H * (float)W;
+    const float st = sinf(theta);
+    return st > 0.0f ? pdf_uv / (2.0f * AZD_PI_F32 * AZD_PI_F32 * st) : 0.0f;
+}
+
+// Environment light direction for AZ_FLAG_ENV_IMPORTANCE: one-sample MIS of
+// the map's luminance CDF (row by the marginal over rows, column by the row's
+// conditional, uniform within the texel, then the inverse equirectangular
+// mapping theta = v pi, phi = pi - 2 pi u) and cosine sampling about n, half
+// each (u1 < 1/2 picks the CDF; u1 is then rescaled), so that directions the
+// CDF rarely proposes (sky behind an occluded sun) keep the cosine density.
+// Returns 1 / (0.5 p_cdf + 0.5 p_cos), or 0 for a degenerate sample.
+__device__ __forceinline__ float sample_env_mis(const DevScene &S, f3 n, float u1, float u2, f3 &dir) {
+    if (u1 < 0.5f) {
+        u1 = 2.0f * u1;
+        const uint32_t H = S.env_cdf_h, W = S.env_cdf_w;
+        uint32_t lo = 0, hi = H;   // largest r with rows[r] <= u1
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (S.env_rows[mid] <= u1) lo = mid;
+            else hi = mid;
+        }
+        const uint32_t r = lo;
+        const float pr = S.env_rows[r + 1] - S.env_rows[r];
+        const float fr = pr > 0.0f ? fminf(0.99999994f, fmaxf(0.0f, (u1 - S.env_rows[r]) / pr)) : 0.5f;
+        const float *cc = S.env_cols + (size_t)r * (W + 1);
+        lo = 0;
+        hi = W;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (cc[mid] <= u2) lo = mid;
+            else hi = mid;
+        }
+        const uint32_t c = lo;
+        const float pc = cc[c + 1] - cc[c];
+        const float fc = pc > 0.0f ? fminf(0.99999994f, fmaxf(0.0f, (u2 - cc[c]) / pc)) : 0.5f;
+        const float u = ((float)c + fc) / (float)W, v = ((float)r + fr) / (float)H;
+        const float theta = v * AZD_PI_F32, phi = AZD_PI_F32 - 2.0f * AZD_PI_F32 * u;
+        const float st = sinf(theta);
+        dir = mk(st * cosf(phi), cosf(theta), st * sinf(phi));
+    } else {
+        u1 = 2.0f * u1 - 1.0f;
+        const float theta = asinf(sqrtf(u1)), phi = 2.0f * AZD_PI_F32 * u2;
+        f3 U, V;
+        onb(n, U, V);
+        dir = normalize(U * (sinf(theta) * cosf(phi)) + V * (sinf(theta) * sinf(phi)) + n * cosf(theta));
+    }
+    const float q = 0.5f * env_cdf_pdf(S, dir) + 0.5f * fmaxf(0.0f, dot(n, dir)) * (1.0f / AZD_PI_F32);
+    return q > 0.0f ? 1.0f / q : 0.0f;
+}
+
 // Inputs of the path-guiding network at a hit: the world position o + t d
 // and the geometric normal (face normal of the triangle, or centre-to-hit
 // direction of the sphere), normalised.

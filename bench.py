@@ -172,6 +172,21 @@ def seed_base(rank):
     return 1000 * rank
 
 
+def max_over_ranks(dist, value, device):
+    """The largest of every rank's `value` (a time), on every rank; `value` itself without a process group."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate(world, units_per_rank, steps, seconds):
+    """Whole-job throughput: every rank's units over the slowest rank's time (weak scaling)."""
+    return world * units_per_rank * steps / seconds
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -250,13 +265,11 @@ def main():
     extend_launches = stg["extend_launches"] * args.steps
     stages = {"extend_ms": stg["extend_ms"], "shade_ms": stg["shade_ms"], "shadow_ms": stg["shadow_ms"],
               "frame_ms": stg["gpu_ms"]}
+    ms = max_over_ranks(dist, ms, "cuda")
     if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
     ms_per_step = ms / args.steps
-    value = world * paths_per_frame * args.steps / (ms / 1000.0) / 1e6
+    value = aggregate(world, paths_per_frame, args.steps, ms / 1000.0) / 1e6
 
     # end to end through the host-film entry point (film in and out every step)
     host_film = torch.zeros((h, w, 4), dtype=torch.float32).pin_memory()
@@ -270,11 +283,8 @@ def main():
     for i in range(e_steps):
         gs.render_host(hf, seed=seed + i, stream=sptr, chunk_samples=args.chunk)
     e2e_s = time.monotonic() - t0
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = {"value": world * paths_per_frame * e_steps / e2e_s / 1e6, "unit": "Mpaths/s",
+    e2e_s = max_over_ranks(dist, e2e_s, "cuda")
+    e2e = {"value": aggregate(world, paths_per_frame, e_steps, e2e_s) / 1e6, "unit": "Mpaths/s",
            "h2d_bytes_per_step": int(w * h * 16), "d2h_bytes_per_step": int(w * h * 16),
            "api": "az_gpu_render_host (device scene resident, host film copied in and out)"}
 

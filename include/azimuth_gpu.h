@@ -43,7 +43,11 @@ enum {
     AZ_FLAG_NONE = 0,
     AZ_FLAG_COUNT_TRAVERSAL = 1u << 0,  /* fill az_render_stats node/primitive visit counters */
     AZ_FLAG_NO_GRAPH = 1u << 1,         /* launch the per-bounce stages directly, not as a CUDA graph */
-    AZ_FLAG_TIME_STAGES = 1u << 2       /* time each stage with CUDA events (az_render_stats *_ms) */
+    AZ_FLAG_TIME_STAGES = 1u << 2,      /* time each stage with CUDA events (az_render_stats *_ms) */
+    AZ_FLAG_ENV_IMPORTANCE = 1u << 3    /* environment light samples by one-sample MIS of a luminance CDF of
+                                           the 2D environment map and cosine sampling, instead of azimuth's
+                                           cosine sampling alone (same estimate, lower variance for peaked
+                                           maps; not a parity mode) */
 };
 
 /* Number of traversal launch configurations (az_render_opts.variant). */
