@@ -124,10 +124,11 @@ def full_scissor(scene):
 
 
 def make_opts(scene=None, seed=0, stream=None, device=0, flags=0, chunk_samples=0, block_size=0, variant=0,
-              bvh_width=0):
+              bvh_width=0, bvh_leaf=0):
     o = RenderOpts()
     o.variant = variant
     o.bvh_width = bvh_width
+    o.bvh_leaf = bvh_leaf
     o.seed = seed
     o.perlin_gradients = scene.perlin_gradients if scene is not None else None
     o.stream = stream
@@ -155,11 +156,11 @@ def produce_image(scene, pixels=None, scissor=None, filter_type=None, backface_c
 class GpuScene:
     """A device-resident scene (az_gpu_scene_create / az_gpu_scene_destroy)."""
 
-    def __init__(self, scene, device=0, bvh_width=0):
+    def __init__(self, scene, device=0, bvh_width=0, bvh_leaf=0):
         self.scene = scene
         self.device = device
         self._h = C.c_void_p()
-        o = make_opts(scene, device=device, bvh_width=bvh_width)
+        o = make_opts(scene, device=device, bvh_width=bvh_width, bvh_leaf=bvh_leaf)
         _check(lib().az_gpu_scene_create(scene.scene_ptr, C.byref(o), C.byref(self._h)), "az_gpu_scene_create")
 
     def autotune(self, seed=0, stream=None):
@@ -173,8 +174,8 @@ class GpuScene:
         return v.value, ms.value
 
     def autotune_scene(self, seed=0, stream=None):
-        """az_gpu_autotune_scene: sweeps BVH width (8, 4, 2) and launch variant, keeps the fastest build;
-        returns (width, variant, ms)."""
+        """az_gpu_autotune_scene: sweeps the hierarchy's shape (width 8/4/2, 1-3 triangles per leaf) and the
+        launch variant, keeps the fastest build; returns (width, variant, ms)."""
         o = make_opts(self.scene, seed=seed, stream=stream, device=self.device)
         w = C.c_uint32()
         v = C.c_uint32()

@@ -46,7 +46,7 @@ class RenderOpts(C.Structure):
     _fields_ = [("seed", C.c_uint64), ("perlin_gradients", C.c_void_p), ("stream", C.c_void_p),
                 ("device", C.c_int32), ("flags", C.c_uint32), ("chunk_samples", C.c_uint32),
                 ("bvh_width", C.c_uint32), ("block_size", C.c_uint32), ("variant", C.c_uint32),
-                ("reserved", C.c_uint32 * 4)]
+                ("bvh_leaf", C.c_uint32), ("reserved", C.c_uint32 * 3)]
 
 
 class Job(C.Structure):

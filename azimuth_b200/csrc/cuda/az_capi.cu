@@ -204,10 +204,14 @@ extern "C" int az_gpu_autotune_scene(const az_scene *host_scene, az_gpu_scene *s
     GpuScene *best = nullptr;
     uint32_t best_v = 0;
     float best_ms = FLT_MAX;
-    for (uint32_t width : {8u, 4u, 2u}) {
+    // hierarchy shapes: children per node x triangles per leaf
+    const uint32_t shapes[][2] = {{8, 2}, {8, 1}, {8, 3}, {4, 2}, {4, 3}, {2, 2}};
+    for (const auto &shape : shapes) {
+        const uint32_t width = shape[0], leaf = shape[1];
         GpuScene *g = scene->impl;
-        if (width != g->bvh_width) {
+        if (width != g->bvh_width || leaf != g->bvh_leaf) {
             o.bvh_width = width;
+            o.bvh_leaf = leaf;
             g = nullptr;
             rc = BuildGpuScene(host_scene, &o, ctx.stream, &g);
             if (rc != AZ_OK) break;

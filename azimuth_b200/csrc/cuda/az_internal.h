@@ -38,6 +38,7 @@ struct GpuScene {
     uint64_t node_count = 0;
     uint32_t max_bvh_depth = 0;
     uint32_t bvh_width = 8;      // children per wide node (2, 4 or 8)
+    uint32_t bvh_leaf = 2;       // triangles per bottom-level leaf at most
     size_t device_bytes = 0;
     WaveBuffers waves;           // reused across render calls on this scene
     uint32_t variant = 7;        // traversal launch configuration, 0-based (128 threads, 8 blocks/SM,

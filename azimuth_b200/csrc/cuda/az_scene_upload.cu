@@ -353,6 +353,9 @@ int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_
     const uint32_t width = opts && opts->bvh_width ? opts->bvh_width : 8u;
     if (width != 2 && width != 4 && width != 8) return SetError(AZ_ERR_INVALID_ARGUMENT, "bvh_width must be 0, 2, 4 or 8");
     G->bvh_width = width;
+    const uint32_t leaf = opts && opts->bvh_leaf ? opts->bvh_leaf : 2u;
+    if (leaf < 1 || leaf > 3) return SetError(AZ_ERR_INVALID_ARGUMENT, "bvh_leaf must be 0..3");
+    G->bvh_leaf = leaf;
     Flattener F;
     F.s = scene;
     if (!scene->BVHRoot) return SetError(AZ_ERR_INVALID_SCENE, "scene has no BVHRoot");
@@ -577,7 +580,7 @@ int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_
         uint32_t root, wroot;
         rc = BuildLBVH(d_lo, d_hi, n, d_nodes, node_base, g.g.tri_begin, d_perm, st, &root);
         if (rc != AZ_OK) return rc;
-        rc = collapse(n, node_base, root, g.g.tri_begin, 2, comp, &wroot);
+        rc = collapse(n, node_base, root, g.g.tri_begin, leaf, comp, &wroot);
         if (rc != AZ_OK) return rc;
         g.g.root = wroot;
         node_base += n > 1 ? n - 1 : 1;

@@ -120,6 +120,19 @@ __device__ __forceinline__ f3 safe_inv(f3 d) {
     return mk(1.0f / x, 1.0f / y, 1.0f / z);
 }
 
+// Three-input max and min (exact, order-independent like fmaxf / fminf).
+__device__ __forceinline__ float max3f(float a, float b, float c) {
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
+__device__ __forceinline__ float min3f(float a, float b, float c) {
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
 __device__ __forceinline__ DevTri load_tri(const DevTri *tris, uint32_t i) {
     const float4 *p = reinterpret_cast<const float4 *>(tris + i);
     DevTri t;
@@ -190,8 +203,8 @@ __device__ __forceinline__ WideHits wide_test(const uint4 w0, const uint4 w1, co
         const float tfy = __fmaf_rn(qbyte_biased(s < 4 ? fy0 : fy1, k), sy, oy);
         const float tnz = __fmaf_rn(qbyte_biased(s < 4 ? nz0 : nz1, k), sz, oz);
         const float tfz = __fmaf_rn(qbyte_biased(s < 4 ? fz0 : fz1, k), sz, oz);
-        const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f));
-        const float tf = fminf(fminf(tfx, tfy), fminf(tfz, tmax)) * 1.00000095367431640625f;
+        const float tn = fmaxf(max3f(tnx, tny, tnz), 0.0f);
+        const float tf = fminf(min3f(tfx, tfy, tfz), tmax) * 1.00000095367431640625f;
         if (tn <= tf) {
             if ((imask >> s) & 1u) {
                 h.inner |= 1u << (s ^ oct);

@@ -68,7 +68,8 @@ typedef struct az_render_opts {
                                        to its end, warp lockstep per traversal step, or persistent
                                        fetching); 0 = the scene's choice: 8 (128 threads, at most 64
                                        registers, persistent fetching) until az_gpu_autotune picks another */
-    uint32_t reserved[4];
+    uint32_t bvh_leaf;              /* az_gpu_scene_create: triangles per bottom-level leaf at most, 1..3 (0 = 2) */
+    uint32_t reserved[3];
 } az_render_opts;
 
 typedef struct az_render_stats {
@@ -125,11 +126,12 @@ int az_gpu_autotune(az_gpu_scene *scene, const az_camera *camera, const az_epsil
                     az_scissor scissor, int32_t filter_type, uint32_t backface_culling,
                     const az_render_opts *opts, uint32_t *variant_out, float *ms_out);
 
-/* Autotuner over the BVH width as well: rebuilds the device hierarchy of
- * `host_scene` (the scene `scene` was created from) with 8, 4 and 2 children
- * per node, runs az_gpu_autotune on each and keeps the fastest build (and its
- * launch configuration) in `scene`.  Writes the width, the variant (1-based)
- * and its time in ms.  Synchronous; `scene` must not be rendering meanwhile. */
+/* Autotuner over the hierarchy's shape as well: rebuilds the device
+ * hierarchy of `host_scene` (the scene `scene` was created from) with 8, 4 and
+ * 2 children per node and 1 to 3 triangles per bottom-level leaf, runs
+ * az_gpu_autotune on each and keeps the fastest build (and its launch
+ * configuration) in `scene`.  Writes the width, the variant (1-based) and its
+ * time in ms.  Synchronous; `scene` must not be rendering meanwhile. */
 int az_gpu_autotune_scene(const az_scene *host_scene, az_gpu_scene *scene, const az_camera *camera,
                           const az_epsilon_values *epsilons, az_scissor scissor, int32_t filter_type,
                           uint32_t backface_culling, const az_render_opts *opts, uint32_t *width_out,

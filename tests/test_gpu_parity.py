@@ -131,8 +131,8 @@ def test_bvh_widths_render_the_same_film_and_autotune_scene(gpu):
     scene = az.generate_scene(az.SCENE_DENSE_MESH, seed=1, width=48, height=48, spp=4, detail=4)
     w, h = scene.resolution()
     films = []
-    for width in (8, 4, 2):
-        with az.GpuScene(scene, bvh_width=width) as g:
+    for width, leaf in ((8, 2), (4, 2), (2, 2), (8, 1), (8, 3)):
+        with az.GpuScene(scene, bvh_width=width, bvh_leaf=leaf) as g:
             f = torch.zeros((h, w, 4), device="cuda")
             g.render_device(f.data_ptr(), seed=7, stats=True)
             films.append(f.cpu().numpy())
