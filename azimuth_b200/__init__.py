@@ -17,7 +17,7 @@ import numpy as np
 
 from . import _native
 from ._native import (BatchOpts, BatchStats, GenParams, GeneratedScene, GuideConfig, Job, RenderOpts, RenderStats,
-                      Scissor, Vec2u, Ray3, lib)
+                      Scissor, Tonemap, Vec2u, Ray3, lib)
 
 SCENE_CORNELL = 0
 SCENE_DENSE_MESH = 1
@@ -329,6 +329,20 @@ class Guide:
             self.close()
         except Exception:
             pass
+
+
+def postprocess(film_ptr, width, height, key_value=0.18, burnout=1.0, saturation=1.0, photographic=True,
+                inv_gamma=1.0 / 2.2, srgb=True, linear=False, rgb_ptr=None, rgb8_ptr=None, stream=None, device=0):
+    """az_gpu_postprocess: azimuth's normalisation, tone mapping and gamma of a DEVICE film into DEVICE
+    outputs (rgb_ptr: width*height*3 float32; rgb8_ptr: width*height*3 uint8)."""
+    tm = Tonemap()
+    tm.KeyValue = key_value
+    tm.BurnoutPercentage = burnout
+    tm.Saturation = saturation
+    tm.Operator = 1 if photographic else 0
+    o = make_opts(stream=stream, device=device)
+    _check(lib().az_gpu_postprocess(film_ptr, width, height, C.byref(tm), inv_gamma, 1 if srgb else 0,
+                                    1 if linear else 0, rgb_ptr, rgb8_ptr, C.byref(o)), "az_gpu_postprocess")
 
 
 def render_batch(jobs, streams=0, flags=0, chunk_samples=0, device=0, largest_first=False):

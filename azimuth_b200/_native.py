@@ -49,6 +49,11 @@ class RenderOpts(C.Structure):
                 ("bvh_leaf", C.c_uint32), ("reserved", C.c_uint32 * 3)]
 
 
+class Tonemap(C.Structure):
+    _fields_ = [("KeyValue", C.c_float), ("BurnoutPercentage", C.c_float), ("Saturation", C.c_float),
+                ("Operator", C.c_uint32)]
+
+
 class Job(C.Structure):
     _fields_ = [("scene", C.c_void_p), ("guide", C.c_void_p), ("film", C.c_void_p), ("camera", C.c_void_p),
                 ("epsilons", C.c_void_p), ("scissor", Scissor), ("filter_type", C.c_int32),
@@ -121,6 +126,9 @@ def _declare(L):
         L.az_gpu_autotune_scene.argtypes = [vp, vp, vp, vp, Scissor, i32, u32, C.POINTER(RenderOpts), vp, vp, vp]
         L.az_gpu_autotune_scene.restype = i32
         L.az_gpu_render_noalloc.argtypes = [vp, vp, vp, vp, Scissor, i32, u32, C.POINTER(RenderOpts)]
+        L.az_gpu_postprocess.argtypes = [vp, u32, u32, C.POINTER(Tonemap), C.c_float, u32, u32, vp, vp,
+                                         C.POINTER(RenderOpts)]
+        L.az_gpu_postprocess.restype = i32
         L.az_gpu_render_batch.argtypes = [vp, u32, C.POINTER(BatchOpts), C.POINTER(BatchStats)]
         L.az_gpu_render_batch.restype = i32
         L.az_guide_create.argtypes = [vp, C.POINTER(GuideConfig), C.POINTER(vp)]

@@ -259,6 +259,18 @@ extern "C" int az_gpu_render_guided(az_gpu_scene *scene, az_guide *guide, az_pix
                   g, train != 0);
 }
 
+extern "C" int az_gpu_postprocess(const az_pixel *film, uint32_t width, uint32_t height, const az_tonemap *tonemap,
+                                  float inv_gamma, uint32_t srgb, uint32_t linear, float *rgb_out, uint8_t *rgb8_out,
+                                  const az_render_opts *opts) {
+    if ((width && height) && (!film || (!rgb_out && !rgb8_out)))
+        return SetError(AZ_ERR_INVALID_ARGUMENT, "null film or no output");
+    if ((uint64_t)width * height > 0x7FFFFFFFull) return SetError(AZ_ERR_INVALID_ARGUMENT, "film too large");
+    CallContext ctx;
+    int rc = ctx.begin(opts);
+    if (rc != AZ_OK) return rc;
+    return PostProcess(film, width, height, tonemap, inv_gamma, srgb, linear, rgb_out, rgb8_out, ctx.stream);
+}
+
 extern "C" int az_gpu_closest_hit(az_gpu_scene *scene, const az_ray3 *rays, uint32_t count, int32_t cull,
                                   float hit_epsilon, uint32_t *out_hit, uint32_t *out_uid, uint32_t *out_face,
                                   float *out_t, const az_render_opts *opts) {

@@ -94,6 +94,9 @@ int Render(GpuScene &G, az_pixel *film, const az_camera *camera, const az_epsilo
            GuideState *guide = nullptr, bool train = false, WaveBuffers *wave_buffers = nullptr);
 int Autotune(GpuScene &G, const az_camera *camera, const az_epsilon_values *eps, az_scissor sc, int32_t filter,
              uint32_t cull, const az_render_opts *opts, cudaStream_t st, uint32_t *best_out, float *ms_out);
+// OutputPixelsToFile's post-processing of a device film (az_post.cu).
+int PostProcess(const az_pixel *film, uint32_t w, uint32_t h, const az_tonemap *tm, float inv_gamma, uint32_t srgb,
+                uint32_t linear, float *rgb_out, uint8_t *rgb8_out, cudaStream_t st);
 int ClosestHit(GpuScene &G, const az_ray3 *rays, uint32_t n, int32_t cull, float eps, uint32_t *out_hit,
                uint32_t *out_uid, uint32_t *out_face, float *out_t, cudaStream_t st);
 

@@ -137,6 +137,21 @@ int az_gpu_autotune_scene(const az_scene *host_scene, az_gpu_scene *scene, const
                           uint32_t backface_culling, const az_render_opts *opts, uint32_t *width_out,
                           uint32_t *variant_out, float *ms_out);
 
+/* OutputPixelsToFile's image post-processing (src/azimuth_main.cpp:1620-1760)
+ * on the GPU, for a DEVICE film of width x height az_pixel that is left
+ * untouched: colour / TotalWeight; with tonemap->Operator == Photographic
+ * (and not `linear`) azimuth's photographic operator (log-average luminance,
+ * burn-out percentile of the sorted luminances, saturation); then, unless
+ * `linear` (azimuth's EXR output), sRGB (`srgb`) or 1/gamma (`inv_gamma`)
+ * correction.  Writes the resulting colours (width*height*3 floats) to the
+ * DEVICE buffer rgb_out and/or the bytes azimuth's PNG/BMP/TGA/JPG writers
+ * store, (uint8)(clamp01(c) * 255), to the DEVICE buffer rgb8_out (either may
+ * be NULL).  Synchronous.  The log-average is summed in double (azimuth: a
+ * serial float sum), so results can differ from azimuth's in the last bits. */
+int az_gpu_postprocess(const az_pixel *film, uint32_t width, uint32_t height, const az_tonemap *tonemap,
+                       float inv_gamma, uint32_t srgb, uint32_t linear, float *rgb_out, uint8_t *rgb8_out,
+                       const az_render_opts *opts);
+
 /* ---- Batched render jobs (no counterpart in azimuth, which renders one camera per call) ----
  *
  * Many render jobs of uneven size, scene and settings in one call: the jobs

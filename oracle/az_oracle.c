@@ -950,3 +950,67 @@ void azo_philox(const uint32_t *ctr4, uint32_t k0, uint32_t k1, uint32_t *out4) 
 }
 
 float azo_sample_perlin(const az_texture *t, float x, float y, float z) { return sample_perlin(t, mk(x, y, z)); }
+
+/* OutputPixelsToFile's post-processing (src/azimuth_main.cpp:1620-1760) for an
+ * 8-bit file: normalise by TotalWeight; photographic tone mapping with the
+ * log-average luminance (f32 running sum of log(L + 1e-5)), the burn-out
+ * luminance at index round((1 - burnout/100) (N - 1)) of the sorted
+ * luminances, Ld = Ls (1 + Ls / Lwhite^2) / (1 + Ls), colour (C/L)^saturation
+ * Ld clamped; then sRGB or 1/gamma; the writers' bytes are
+ * (u8)(clamp01(C) * 255) (:1473-1475).  Luminance 0.27 R + 0.67 G + 0.06 B
+ * (src/azimuth_math.cpp:1866-1880).  rgb: N x 3 floats out; rgb8: N x 3 bytes out. */
+static int cmp_f32(const void *a, const void *b) {
+    float x = *(const float *)a, y = *(const float *)b;
+    return x < y ? -1 : (x > y ? 1 : 0);
+}
+
+static float lum3(float r, float g, float b) { return r * 0.27f + g * 0.67f + b * 0.06f; }
+static float clamp01(float v) { return v < 0.0f ? 0.0f : (v > 1.0f ? 1.0f : v); }
+
+int azo_output_pixels(const float *film4, uint32_t w, uint32_t h, const az_tonemap *tm, float inv_gamma,
+                      uint32_t srgb, float *rgb, uint8_t *rgb8) {
+    const uint32_t n = w * h;
+    const int tonemapped = tm->Operator != AZ_Tonemap_None;
+    float *lums = tonemapped ? (float *)malloc(sizeof(float) * (n ? n : 1)) : NULL;
+    float logavg = 0.0f;
+    for (uint32_t i = 0; i < n; i++) {
+        const float wt = film4[4 * i + 3];
+        float r = film4[4 * i + 0] / wt, g = film4[4 * i + 1] / wt, b = film4[4 * i + 2] / wt;
+        rgb[3 * i + 0] = r;
+        rgb[3 * i + 1] = g;
+        rgb[3 * i + 2] = b;
+        if (tonemapped) {
+            const float l = lum3(r, g, b);
+            lums[i] = l;
+            logavg += logf(l + 0.00001f);
+        }
+    }
+    if (tonemapped) {
+        logavg = expf(logavg / (float)n);
+        const float factor = tm->KeyValue / logavg;
+        qsort(lums, n, sizeof(float), cmp_f32);
+        const uint32_t li = (uint32_t)((1.0f - tm->BurnoutPercentage * 0.01f) * (float)(n - 1) + 0.5f);
+        float lw2 = lums[li] * factor;
+        lw2 = lw2 * lw2;
+        for (uint32_t i = 0; i < n; i++) {
+            const float r = rgb[3 * i + 0], g = rgb[3 * i + 1], b = rgb[3 * i + 2];
+            const float l = lum3(r, g, b);
+            if (l != 0.0f) {
+                const float ls = l * factor;
+                const float ld = (ls * (1.0f + (ls / lw2))) / (1.0f + ls);
+                rgb[3 * i + 0] = clamp01(powf(r / l, tm->Saturation) * ld);
+                rgb[3 * i + 1] = clamp01(powf(g / l, tm->Saturation) * ld);
+                rgb[3 * i + 2] = clamp01(powf(b / l, tm->Saturation) * ld);
+            }
+        }
+        free(lums);
+    }
+    for (uint32_t i = 0; i < 3 * n; i++) {
+        float v = rgb[i];
+        if (srgb) v = v > 0.0031308f ? 1.055f * powf(v, inv_gamma) - 0.055f : v * 12.92f;
+        else v = powf(v, inv_gamma);
+        rgb[i] = v;
+        if (rgb8) rgb8[i] = (uint8_t)(clamp01(v) * 255.0f);
+    }
+    return 1;
+}

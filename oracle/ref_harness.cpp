@@ -272,4 +272,18 @@ void azref_light_contribution(az_brdf *Brdf, const float *Intensity3, const floa
 
 uint32_t azref_sizeof_entity(void) { return (uint32_t)sizeof(entity); }
 
+/* OutputPixelsToFile (src/azimuth_main.cpp:1620-1797) as azimuth calls it for a
+ * BMP (SaveFormat BMP, no EXR copy): normalises, tone maps and gamma-corrects
+ * `Pixels` in place and writes the file to BmpPath.  The 8-bit values azimuth
+ * writes are (u8)(Clamp01(C) * 255.0f) of the resulting colours. */
+int azref_output_pixels(az_pixel *Pixels, uint32_t Width, uint32_t Height, const az_tonemap *Tonemap,
+                        float InvGamma, uint32_t SRGB, const char *BmpPath) {
+    tonemap T;
+    memcpy(&T, Tonemap, sizeof(T));
+    char Path[256] = {0};
+    strncpy(Path, BmpPath, sizeof(Path) - 1);
+    return OutputPixelsToFile(Path, (pixel *)Pixels, Vec2u(Width, Height), &T, InvGamma, (b32)SRGB,
+                              FileFormat_BMP, false) ? 1 : 0;
+}
+
 }  /* extern "C" */

@@ -40,6 +40,8 @@ def ref(fast=False):
         L = C.CDLL(path)
         vp, u32, i32, u64 = C.c_void_p, C.c_uint32, C.c_int32, C.c_uint64
         L.azref_set_seed.argtypes = [u64]
+        L.azref_output_pixels.argtypes = [vp, u32, u32, vp, C.c_float, u32, C.c_char_p]
+        L.azref_output_pixels.restype = i32
         L.azref_produce_image.argtypes = [vp, vp, vp, vp, Scissor, i32, i32, u32]
         L.azref_closest_hit.argtypes = [vp, vp, u32, i32, C.c_float, vp, vp, vp, vp, vp, i32]
         L.azref_set_perlin_gradients.argtypes = [vp]
@@ -64,6 +66,8 @@ def port():
         L = C.CDLL(PORT_SO)
         vp, u32, i32, u64 = C.c_void_p, C.c_uint32, C.c_int32, C.c_uint64
         L.azo_set_order.argtypes = [i32]
+        L.azo_output_pixels.argtypes = [vp, u32, u32, vp, C.c_float, u32, vp, vp]
+        L.azo_output_pixels.restype = i32
         L.azo_set_gradients.argtypes = [vp]
         L.azo_produce_image.argtypes = [vp, vp, vp, vp, Scissor, i32, i32, u64, i32]
         L.azo_render_samples.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, u32, i32, u64]
@@ -85,6 +89,34 @@ def scissor_of(scene, rows=None, cols=None):
     r0, r1 = rows if rows else (0, h)
     c0, c1 = cols if cols else (0, w)
     return Scissor(Vec2u(c1, r1), Vec2u(c0, r0))
+
+
+def output_pixels(film, tonemap, inv_gamma, srgb, kind="ref", tmpdir="/tmp"):
+    """azimuth's OutputPixelsToFile post-processing of a film (H, W, 4): (colours (H, W, 3) float32, the
+    8-bit values azimuth writes).  kind "ref" runs azimuth's own function (writing a BMP it then
+    discards), "port" the C restatement."""
+    import tempfile
+    from azimuth_b200._native import Tonemap
+    h, w = film.shape[:2]
+    tm = Tonemap()
+    tm.KeyValue, tm.BurnoutPercentage, tm.Saturation, tm.Operator = tonemap
+    if kind == "ref":
+        px = np.ascontiguousarray(film, np.float32).copy()
+        fd, path = tempfile.mkstemp(suffix=".bmp", dir=tmpdir)
+        os.close(fd)
+        try:
+            ok = ref().azref_output_pixels(px.ctypes.data, w, h, C.byref(tm), inv_gamma, srgb, path.encode())
+        finally:
+            os.unlink(path)
+        assert ok == 1
+        rgb = np.ascontiguousarray(px[..., :3])
+        rgb8 = (np.clip(rgb, 0.0, 1.0) * np.float32(255.0)).astype(np.float32).astype(np.uint8)
+        return rgb, rgb8
+    rgb = np.zeros((h, w, 3), np.float32)
+    rgb8 = np.zeros((h, w, 3), np.uint8)
+    port().azo_output_pixels(np.ascontiguousarray(film, np.float32).ctypes.data, w, h, C.byref(tm), inv_gamma, srgb,
+                             rgb.ctypes.data, rgb8.ctypes.data)
+    return rgb, rgb8
 
 
 def ref_film(scene, seed=0, threads=None, scissor=None, fast=False, filter_type=None):
