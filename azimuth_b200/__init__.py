@@ -249,12 +249,13 @@ class Guide:
     LEVELS = 16
     TABLE = 1 << 19
 
-    def __init__(self, gpu_scene, seed=0, learning_rate=0.0, train_batch=0, record_samples=0):
+    def __init__(self, gpu_scene, seed=0, learning_rate=0.0, train_batch=0, record_samples=0, steps_per_wave=0):
         self.gs = gpu_scene
         cfg = GuideConfig()
         cfg.learning_rate = learning_rate
         cfg.train_batch = train_batch
         cfg.record_samples = record_samples
+        cfg.steps_per_wave = steps_per_wave
         cfg.seed = seed
         self._h = C.c_void_p()
         _check(lib().az_guide_create(gpu_scene._h, C.byref(cfg), C.byref(self._h)), "az_guide_create")

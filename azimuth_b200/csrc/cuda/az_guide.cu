@@ -40,7 +40,8 @@ constexpr int NW = GUIDE_LAYERS * W * W;             // MLP weights
 constexpr int NFRAG = GUIDE_LAYERS * 4 * 8 * 32;     // B fragments (uint2) per copy
 constexpr int XS = W + 8;                            // row stride (bf16) of the shared activation copies
 constexpr int OS = W + 4;                            // row stride (fp32) of the shared output rows
-constexpr int kWarps = 4;                            // warps per block of the network kernels
+constexpr int kWarps = 4;                            // warps per block of the training kernel
+constexpr int kInferWarps = 8;                       // warps per block of the inference kernel
 
 // Parameters of the network as the kernels see them.
 struct GuideNetDev {
@@ -274,14 +275,14 @@ __device__ __forceinline__ void load_frags(uint2 *dst, const uint2 *src) {
 }
 
 // ---- inference over the extension queue of one level ----
-constexpr size_t kInferSmem = NFRAG * sizeof(uint2) + (size_t)kWarps * 16 * OS * sizeof(float) + W * sizeof(float);
+constexpr size_t kInferSmem = NFRAG * sizeof(uint2) + (size_t)kInferWarps * 16 * OS * sizeof(float) + W * sizeof(float);
 
-__global__ void __launch_bounds__(kWarps * 32) k_guide_infer(DevScene S, WaveQueues Q, uint32_t level, GuideNetDev N,
+__global__ void __launch_bounds__(kInferWarps * 32) k_guide_infer(DevScene S, WaveQueues Q, uint32_t level, GuideNetDev N,
                                                              GuideLobes *out) {
     extern __shared__ __align__(16) unsigned char smem[];
     uint2 *s_wf = reinterpret_cast<uint2 *>(smem);
     float *s_outs = reinterpret_cast<float *>(s_wf + NFRAG);
-    float *s_bias = s_outs + kWarps * 16 * OS;
+    float *s_bias = s_outs + kInferWarps * 16 * OS;
     load_frags(s_wf, N.wf);
     for (int i = threadIdx.x; i < W; i += blockDim.x) s_bias[i] = N.bias[i];
     __syncthreads();
@@ -290,7 +291,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_guide_infer(DevScene S, WaveQue
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3u;
     float *out_rows = s_outs + warp * 16 * OS;
     const uint32_t tiles = (n + 15u) / 16u;
-    for (uint32_t tile = blockIdx.x * kWarps + warp; tile < tiles; tile += gridDim.x * kWarps) {
+    for (uint32_t tile = blockIdx.x * kInferWarps + warp; tile < tiles; tile += gridDim.x * kInferWarps) {
         f3 p[2], nr[2], wo[2];
 #pragma unroll
         for (int h = 0; h < 2; h++) {
@@ -637,6 +638,7 @@ struct GuideState {
     __half2 *feat = nullptr;
     float2 *grid = nullptr, *grid_grad = nullptr, *grid_m = nullptr, *grid_v = nullptr;
     uint32_t n_rec = 0;             // samples per wave whose vertices are recorded
+    uint32_t steps_per_wave = 1;    // Adam steps on each wave's rows
     GuideRow *rows = nullptr;
     uint32_t rows_cap = 0;
     uint32_t *count = nullptr;      // [0] rows, then scratch
@@ -738,7 +740,8 @@ int CreateGuide(const GpuScene &G, const az_guide_config *cfg, GuideState **out)
     g->device = G.device;
     cudaDeviceGetAttribute(&g->sms, cudaDevAttrMultiProcessorCount, G.device);
     g->lr = cfg && cfg->learning_rate > 0.0f ? cfg->learning_rate : 1e-2f;
-    g->n_rec = cfg && cfg->record_samples ? cfg->record_samples : (1u << 16);
+    g->n_rec = cfg && cfg->record_samples ? cfg->record_samples : (1u << 17);
+    g->steps_per_wave = cfg && cfg->steps_per_wave ? cfg->steps_per_wave : 1u;
     g->rows_cap = cfg && cfg->train_batch ? cfg->train_batch : (1u << 18);
     const uint64_t seed = cfg ? cfg->seed : 0;
     g->w = g->Alloc<float>(NW);
@@ -843,7 +846,7 @@ int GuidePrepareWave(GuideState &g, WaveBuffers &W, WaveQueues &Q, uint32_t cap_
 }
 
 int GuideInfer(GuideState &g, const GpuScene &G, const WaveQueues &Q, uint32_t level, cudaStream_t st) {
-    k_guide_infer<<<g.sms * 4, kWarps * 32, kInferSmem, st>>>(G.dev, Q, level, g.net, Q.lobes);
+    k_guide_infer<<<g.sms * 3, kInferWarps * 32, kInferSmem, st>>>(G.dev, Q, level, g.net, Q.lobes);
     AZ_CUDA_TRY(cudaGetLastError());
     return AZ_OK;
 }
@@ -854,7 +857,11 @@ int GuideTrainWave(GuideState &g, const WaveQueues &Q, cudaStream_t st) {
     k_guide_targets<<<g.sms * 4, 256, 0, st>>>(Q.rec, Q.n_rec, Q.rec_levels, Q.accum, g.rows, g.rows_cap, g.count,
                                                g.wsum);
     AZ_CUDA_TRY(cudaGetLastError());
-    return TrainStep(g, g.rows, g.count, g.rows_cap, g.wsum, st);
+    for (uint32_t k = 0; k < g.steps_per_wave; k++) {
+        int rc = TrainStep(g, g.rows, g.count, g.rows_cap, g.wsum, st);
+        if (rc != AZ_OK) return rc;
+    }
+    return AZ_OK;
 }
 
 }  // namespace az

@@ -1075,14 +1075,15 @@ int Render(GpuScene &G, az_pixel *film, const az_camera *camera, const az_epsilo
     cam.env_importance = opts && (opts->flags & AZ_FLAG_ENV_IMPORTANCE) && G.dev.env_rows ? 1u : 0u;
     cam.variant = opts && opts->variant ? opts->variant - 1 : G.variant;
     if (cam.variant >= kVariantCount) return SetError(AZ_ERR_INVALID_ARGUMENT, "unknown launch variant");
-    if (G.dev.max_depth + 1 > AZ_MAX_LEVELS - 2) return SetError(AZ_ERR_UNSUPPORTED, "MaxRecursionDepth above 60");
+    if (G.dev.max_depth + 1 > AZ_MAX_LEVELS - 2) return SetError(AZ_ERR_UNSUPPORTED, "MaxRecursionDepth above 61");
     uint64_t total = cam.npix * (uint64_t)cam.sqrt_spp * cam.sqrt_spp;
     if (stats) memset(stats, 0, sizeof(*stats));
     if (total == 0) return AZ_OK;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, G.device);
     uint32_t chunk = opts && opts->chunk_samples ? opts->chunk_samples : (1u << 22);
-    if (guide) chunk = std::min<uint32_t>(chunk, 1u << 20);   // proposals are kept per queue entry
+    // a training render updates the guide after every wave: smaller waves, more updates
+    if (guide && train && !(opts && opts->chunk_samples)) chunk = 1u << 20;
     chunk = (uint32_t)std::min<uint64_t>(chunk, total);
     uint32_t per_node_shadow = G.dev.light_count + (G.dev.use_env_map ? 1u : 0u);
     WaveBuffers &W = wave_buffers ? *wave_buffers : G.waves;
@@ -1337,7 +1338,7 @@ extern "C" int az_gpu_render_noalloc(az_gpu_scene *scene, az_pixel *film, const 
         return SetError(AZ_ERR_INVALID_ARGUMENT,
                         "chunk_samples " + std::to_string(wave) + " exceeds the static wave scratch of " +
                             std::to_string(kStaticWave) + " camera samples");
-    if (G.dev.max_depth + 1 > AZ_MAX_LEVELS - 2) return SetError(AZ_ERR_UNSUPPORTED, "MaxRecursionDepth above 60");
+    if (G.dev.max_depth + 1 > AZ_MAX_LEVELS - 2) return SetError(AZ_ERR_UNSUPPORTED, "MaxRecursionDepth above 61");
     AZ_CUDA_TRY(cudaSetDevice(device));
     cudaStream_t st = opts && opts->stream ? (cudaStream_t)opts->stream : cudaStreamPerThread;
     void *base = nullptr;

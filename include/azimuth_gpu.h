@@ -213,8 +213,8 @@ typedef struct az_guide az_guide;
 typedef struct az_guide_config {
     float learning_rate;            /* Adam step size; 0 = 1e-2 */
     uint32_t train_batch;           /* training rows per step at most; 0 = 2^18 */
-    uint32_t record_samples;        /* camera samples per wave whose vertices are recorded; 0 = 2^16 */
-    uint32_t reserved0;
+    uint32_t record_samples;        /* camera samples per wave whose vertices are recorded; 0 = 2^17 */
+    uint32_t steps_per_wave;        /* Adam steps on each wave's rows when training; 0 = 1 */
     uint64_t seed;                  /* weight initialisation */
     uint32_t reserved[6];
 } az_guide_config;
@@ -222,8 +222,9 @@ typedef struct az_guide_config {
 int az_guide_create(az_gpu_scene *scene, const az_guide_config *cfg, az_guide **out);
 void az_guide_destroy(az_guide *guide);
 
-/* az_gpu_render with the guide's proposal for the scattering direction (waves
- * of at most 2^20 camera samples); `train` != 0 trains after every wave.
+/* az_gpu_render with the guide's proposal for the scattering direction;
+ * `train` != 0 trains after every wave (waves of 2^20 camera samples unless
+ * opts->chunk_samples says otherwise).
  * Pass the scene the guide was created for. */
 int az_gpu_render_guided(az_gpu_scene *scene, az_guide *guide, az_pixel *film, const az_camera *camera,
                          const az_epsilon_values *epsilons, az_scissor scissor, int32_t filter_type,
