@@ -17,7 +17,7 @@ import numpy as np
 
 from . import _native
 from ._native import (BatchOpts, BatchStats, GenParams, GeneratedScene, GuideConfig, Job, RenderOpts, RenderStats,
-                      Scissor, Tonemap, Vec2u, Ray3, lib)
+                      SceneInfo, Scissor, Tonemap, Vec2u, Ray3, lib)
 
 SCENE_CORNELL = 0
 SCENE_DENSE_MESH = 1
@@ -162,6 +162,13 @@ class GpuScene:
         self._h = C.c_void_p()
         o = make_opts(scene, device=device, bvh_width=bvh_width, bvh_leaf=bvh_leaf)
         _check(lib().az_gpu_scene_create(scene.scene_ptr, C.byref(o), C.byref(self._h)), "az_gpu_scene_create")
+
+    def info(self):
+        """az_gpu_scene_info: what the build made (triangles, spheres, wide nodes, depth, device bytes) and
+        the time of its parts (host flattening, uploads, GPU BVH build) in ms."""
+        si = SceneInfo()
+        _check(lib().az_gpu_scene_info(self._h, C.byref(si)), "az_gpu_scene_info")
+        return {k: getattr(si, k) for k, _ in SceneInfo._fields_ if k != "reserved"}
 
     def autotune(self, seed=0, stream=None):
         """az_gpu_autotune: picks the traversal launch variant for this scene; returns (variant, ms)."""

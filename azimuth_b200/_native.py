@@ -84,6 +84,14 @@ class RenderStats(C.Structure):
                 ("extend_launches", C.c_uint32), ("reserved", C.c_uint32 * 3)]
 
 
+class SceneInfo(C.Structure):
+    _fields_ = [("triangles", C.c_uint64), ("spheres", C.c_uint64), ("wide_nodes", C.c_uint64),
+                ("device_bytes", C.c_uint64), ("bvh_width", C.c_uint32), ("bvh_leaf", C.c_uint32),
+                ("bvh_depth", C.c_uint32), ("hierarchies", C.c_uint32), ("flatten_ms", C.c_float),
+                ("upload_ms", C.c_float), ("bvh_ms", C.c_float), ("total_ms", C.c_float),
+                ("reserved", C.c_uint32 * 4)]
+
+
 def lib():
     """Load (once) and return the native library; raises if it was not built."""
     global _lib
@@ -115,6 +123,8 @@ def _declare(L):
         L.az_gpu_scene_create.restype = i32
         L.az_gpu_scene_destroy.argtypes = [vp]
         L.az_gpu_scene_destroy.restype = None
+        L.az_gpu_scene_info.argtypes = [vp, C.POINTER(SceneInfo)]
+        L.az_gpu_scene_info.restype = i32
         L.az_gpu_render.argtypes = [vp, vp, vp, vp, Scissor, i32, u32, C.POINTER(RenderOpts),
                                     C.POINTER(RenderStats)]
         L.az_gpu_render.restype = i32

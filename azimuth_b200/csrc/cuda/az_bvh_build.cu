@@ -79,9 +79,9 @@ __device__ __forceinline__ int delta(const unsigned long long *k, int n, int i, 
 }
 
 // One thread per internal node i in [0, n-2]: children (internal index or
-// leaf flagged with bit 31) and parents.
+// leaf flagged with bit 31), parents, and the node's sorted primitive range.
 __global__ void k_karras(const unsigned long long *k, int n, uint32_t *left, uint32_t *right, int *parent_int,
-                         int *parent_leaf) {
+                         int *parent_leaf, uint2 *range, uint32_t leaf_base) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n - 1) return;
     int d = (delta(k, n, i, i + 1) - delta(k, n, i, i - 1)) > 0 ? 1 : -1;
@@ -101,6 +101,7 @@ __global__ void k_karras(const unsigned long long *k, int n, uint32_t *left, uin
     } while (t > 1);
     int gamma = i + s * d + min(d, 0);
     int lo = min(i, j), hi = max(i, j);
+    range[i] = make_uint2(leaf_base + (uint32_t)lo, (uint32_t)(hi - lo + 1));
     uint32_t lc, rc;
     if (lo == gamma) {
         lc = 0x80000000u | (uint32_t)gamma;
@@ -182,7 +183,7 @@ __global__ void k_copy_u32(const uint32_t *src, uint32_t n, uint32_t *dst) {
     if (i < n) dst[i] = src[i];
 }
 
-__global__ void k_single(const float4 *lo, const float4 *hi, azd::BVHNode *nodes, uint32_t node_base,
+__global__ void k_single(const float4 *lo, const float4 *hi, azd::BVHNode *nodes, uint2 *range, uint32_t node_base,
                          uint32_t leaf_base, uint32_t *perm) {
     float4 a = lo[0], b = hi[0];
     pad_box(a, b);
@@ -193,6 +194,7 @@ __global__ void k_single(const float4 *lo, const float4 *hi, azd::BVHNode *nodes
     out.bz = make_float4(a.z, b.z, FLT_MAX, -FLT_MAX);
     out.ch = make_uint4(leaf_base, leaf_base, 1u, 1u);
     nodes[node_base] = out;
+    range[node_base] = make_uint2(leaf_base, 1u);
     perm[0] = 0;
 }
 
@@ -207,15 +209,15 @@ struct Scratch {
 
 }  // namespace
 
-int BuildLBVH(const float4 *d_lo, const float4 *d_hi, uint32_t n, azd::BVHNode *d_nodes, uint32_t node_base,
-              uint32_t leaf_base, uint32_t *d_perm, cudaStream_t stream, uint32_t *root_out) {
+int BuildLBVH(const float4 *d_lo, const float4 *d_hi, uint32_t n, azd::BVHNode *d_nodes, uint2 *d_range,
+              uint32_t node_base, uint32_t leaf_base, uint32_t *d_perm, cudaStream_t stream, uint32_t *root_out) {
     if (n == 0) {
         *root_out = 0xFFFFFFFFu;
         return AZ_OK;
     }
     *root_out = node_base;
     if (n == 1) {
-        k_single<<<1, 1, 0, stream>>>(d_lo, d_hi, d_nodes, node_base, leaf_base, d_perm);
+        k_single<<<1, 1, 0, stream>>>(d_lo, d_hi, d_nodes, d_range, node_base, leaf_base, d_perm);
         AZ_CUDA_TRY(cudaGetLastError());
         return AZ_OK;
     }
@@ -252,7 +254,8 @@ int BuildLBVH(const float4 *d_lo, const float4 *d_hi, uint32_t n, azd::BVHNode *
                                                 (int)n, 0, 63, stream));
     AZ_CUDA_TRY(cudaMemsetAsync(parent_int.p, 0xFF, n * sizeof(int), stream));   // root's parent = -1
     AZ_CUDA_TRY(cudaMemsetAsync(visits.p, 0, n * sizeof(unsigned int), stream));
-    k_karras<<<grid, B, 0, stream>>>(keys_sorted.p, (int)n, left.p, right.p, parent_int.p, parent_leaf.p);
+    k_karras<<<grid, B, 0, stream>>>(keys_sorted.p, (int)n, left.p, right.p, parent_int.p, parent_leaf.p,
+                                     d_range + node_base, leaf_base);
     k_fill<<<grid, B, 0, stream>>>(vals_sorted.p, d_lo, d_hi, (int)n, left.p, right.p, parent_int.p, parent_leaf.p,
                                    ilo.p, ihi.p, visits.p, d_nodes, node_base, leaf_base);
     k_copy_u32<<<grid, B, 0, stream>>>(vals_sorted.p, n, d_perm);

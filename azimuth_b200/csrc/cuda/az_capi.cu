@@ -101,6 +101,25 @@ extern "C" int az_gpu_scene_create(const az_scene *scene, const az_render_opts *
     return AZ_OK;
 }
 
+extern "C" int az_gpu_scene_info(const az_gpu_scene *scene, az_scene_info *out) {
+    if (!scene || !scene->impl || !out) return SetError(AZ_ERR_INVALID_ARGUMENT, "null scene or output");
+    const GpuScene &G = *scene->impl;
+    memset(out, 0, sizeof(*out));
+    out->triangles = G.triangle_count;
+    out->spheres = G.sphere_count;
+    out->wide_nodes = G.node_count;
+    out->device_bytes = G.device_bytes;
+    out->bvh_width = G.bvh_width;
+    out->bvh_leaf = G.bvh_leaf;
+    out->bvh_depth = G.max_bvh_depth;
+    out->hierarchies = G.hierarchies;
+    out->flatten_ms = G.flatten_ms;
+    out->upload_ms = G.upload_ms;
+    out->bvh_ms = G.bvh_ms;
+    out->total_ms = G.total_ms;
+    return AZ_OK;
+}
+
 extern "C" void az_gpu_scene_destroy(az_gpu_scene *s) {
     if (!s) return;
     if (s->impl) {

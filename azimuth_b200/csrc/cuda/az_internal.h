@@ -37,6 +37,11 @@ struct GpuScene {
     uint64_t sphere_count = 0;
     uint64_t node_count = 0;
     uint32_t max_bvh_depth = 0;
+    uint32_t hierarchies = 0;    // bottom-level hierarchies plus the top level
+    float flatten_ms = 0.0f;     // host: azimuth's structs walked into device records
+    float upload_ms = 0.0f;      // host-to-device copies of the primitives
+    float bvh_ms = 0.0f;         // GPU: LBVH builds, wide collapse, primitive gather
+    float total_ms = 0.0f;       // the whole az_gpu_scene_create
     uint32_t bvh_width = 8;      // children per wide node (2, 4 or 8)
     uint32_t bvh_leaf = 2;       // triangles per bottom-level leaf at most
     size_t device_bytes = 0;
@@ -53,19 +58,25 @@ struct GpuScene {
 int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_t stream, GpuScene **out);
 
 // LBVH over `n` boxes (device arrays lo/hi of float4).  Writes nodes into
-// `nodes` starting at `node_base` (n-1 nodes, or 1 for n == 1) and the sorted
-// primitive order into `perm`.  Leaf child references are `leaf_base + sorted
-// position`.  Returns the root node index.
-int BuildLBVH(const float4 *d_lo, const float4 *d_hi, uint32_t n, azd::BVHNode *d_nodes, uint32_t node_base,
-              uint32_t leaf_base, uint32_t *d_perm, cudaStream_t stream, uint32_t *root_out);
+// `nodes` starting at `node_base` (n-1 nodes, or 1 for n == 1), each inner
+// node's primitive range (first sorted position + leaf_base, count) into
+// `range` at the same index, and the sorted primitive order into `perm`.  Leaf
+// child references are `leaf_base + sorted position`.  Returns the root node
+// index.
+int BuildLBVH(const float4 *d_lo, const float4 *d_hi, uint32_t n, azd::BVHNode *d_nodes, uint2 *d_range,
+              uint32_t node_base, uint32_t leaf_base, uint32_t *d_perm, cudaStream_t stream, uint32_t *root_out);
 
-// Collapse of a binary BVH (nodes `bin`, global index of bin[0] = bin_base)
-// into wide nodes of at most `width` (2, 4 or 8) children appended to `out`;
-// `prim_order[j]` receives the sorted primitive position of output slot
-// prim_out_base + j.
-int CollapseToWide(const std::vector<azd::BVHNode> &bin, uint32_t bin_base, uint32_t bin_root, uint32_t max_leaf,
-                   uint32_t width, std::vector<azd::WideNode> &out, std::vector<uint32_t> &prim_order,
-                   uint32_t prim_out_base, uint32_t *root_out, uint32_t *depth_out);
+// Collapse, on the GPU, of the binary LBVH of `n` primitives rooted at
+// `bin_root` (device nodes and ranges as BuildLBVH writes them) into wide nodes
+// of at most `width` (2, 4 or 8) children and leaves of at most `max_leaf`
+// primitives, written to d_wide from index *wide_count on (at most wide_cap
+// nodes in all; *wide_count is advanced).  Leaf primitives are numbered
+// leaf_base + [0, n): d_out_perm[j] receives the unsorted local index of the
+// primitive placed at j (d_sorted_perm maps sorted positions to those).
+int CollapseToWide(const azd::BVHNode *d_nodes, const uint2 *d_range, uint32_t bin_root, uint32_t n,
+                   uint32_t leaf_base, const uint32_t *d_sorted_perm, uint32_t max_leaf, uint32_t width,
+                   azd::WideNode *d_wide, uint32_t wide_cap, uint32_t *wide_count, uint32_t *d_out_perm,
+                   cudaStream_t st, uint32_t *root_out, uint32_t *depth_out);
 
 int SetupCamera(const az_camera *c, az_scissor sc, int32_t filter, uint32_t cull, const az_epsilon_values *eps,
                 uint64_t seed, CameraParams &cam);

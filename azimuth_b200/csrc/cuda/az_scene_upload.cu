@@ -8,6 +8,7 @@
 // quantity azimuth computes (local ray, world t) is then the same for all of
 // them, so only the choice between exactly tied hits can differ.
 #include <algorithm>
+#include <chrono>
 #include <cfloat>
 #include <cmath>
 #include <cstring>
@@ -313,6 +314,16 @@ T *Upload(GpuScene &G, const std::vector<T> &v, cudaStream_t st, int &rc) {
     return p;
 }
 
+// A device buffer that lives only while the scene is built.
+template <typename T>
+struct TempBuf {
+    T *p = nullptr;
+    ~TempBuf() {
+        if (p) cudaFree(p);
+    }
+    bool alloc(size_t n) { return cudaMalloc((void **)&p, (n ? n : 1) * sizeof(T)) != cudaSuccess; }   // true on failure
+};
+
 __global__ void k_gather_tris(const azd::DevTri *src, const azd::DevTriAttr *src_attr, const uint32_t *perm,
                               uint32_t n, azd::DevTri *dst, azd::DevTriAttr *dst_attr) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -348,6 +359,7 @@ __global__ void k_tri_boxes(const azd::DevTri *t, uint32_t n, float4 *lo, float4
 int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_t st, GpuScene **out) {
     if (!scene || !out) return SetError(AZ_ERR_INVALID_ARGUMENT, "null scene");
     *out = nullptr;
+    const auto t_start = std::chrono::steady_clock::now();
     std::unique_ptr<GpuScene> G(new GpuScene());
     G->device = opts ? opts->device : 0;
     const uint32_t width = opts && opts->bvh_width ? opts->bvh_width : 8u;
@@ -518,104 +530,90 @@ int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_
     }
     node_total += tlas.size() > 1 ? (uint32_t)tlas.size() - 1 : (uint32_t)tlas.size();
 
-    azd::DevTri *d_tris_unsorted = (azd::DevTri *)G->Alloc(all_tris.size() * sizeof(azd::DevTri));
-    azd::DevTriAttr *d_attr_unsorted = (azd::DevTriAttr *)G->Alloc(all_attr.size() * sizeof(azd::DevTriAttr));
+    G->flatten_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+    // Build-only buffers are freed when the build ends; the scene keeps the
+    // sorted primitives, the wide nodes and the top-level primitive list.
+    const size_t nmax = std::max(all_tris.size(), tlas.size()) + 1;
+    TempBuf<azd::DevTri> d_tris_unsorted;
+    TempBuf<azd::DevTriAttr> d_attr_unsorted;
+    TempBuf<azd::BVHNode> d_nodes;
+    TempBuf<uint2> d_range;
+    TempBuf<float4> d_lo, d_hi;
+    TempBuf<uint32_t> d_perm, d_comp, d_tlas_unsorted;
+    TempBuf<azd::WideNode> d_wide_tmp;
     azd::DevTri *d_tris = (azd::DevTri *)G->Alloc(all_tris.size() * sizeof(azd::DevTri));
     azd::DevTriAttr *d_attr = (azd::DevTriAttr *)G->Alloc(all_attr.size() * sizeof(azd::DevTriAttr));
-    azd::BVHNode *d_nodes = (azd::BVHNode *)G->Alloc((size_t)node_total * sizeof(azd::BVHNode));
-    float4 *d_lo = (float4 *)G->Alloc((std::max(all_tris.size(), tlas.size()) + 1) * sizeof(float4));
-    float4 *d_hi = (float4 *)G->Alloc((std::max(all_tris.size(), tlas.size()) + 1) * sizeof(float4));
-    uint32_t *d_perm = (uint32_t *)G->Alloc((std::max(all_tris.size(), tlas.size()) + 1) * sizeof(uint32_t));
-    if (!d_tris_unsorted || !d_attr_unsorted || !d_tris || !d_attr || !d_nodes || !d_lo || !d_hi || !d_perm)
+    uint32_t *d_tlas = (uint32_t *)G->Alloc((tlas.size() + 1) * sizeof(uint32_t));
+    if (!d_tris || !d_attr || !d_tlas || d_tris_unsorted.alloc(all_tris.size()) ||
+        d_attr_unsorted.alloc(all_attr.size()) || d_nodes.alloc(node_total) || d_range.alloc(node_total) ||
+        d_lo.alloc(nmax) || d_hi.alloc(nmax) || d_perm.alloc(nmax) || d_comp.alloc(nmax) ||
+        d_tlas_unsorted.alloc(tlas.size() + 1) || d_wide_tmp.alloc(node_total))
         return SetError(AZ_ERR_OUT_OF_MEMORY, "device allocation failed");
+    const auto t_up0 = std::chrono::steady_clock::now();
     if (!all_tris.empty()) {
-        AZ_CUDA_TRY(cudaMemcpyAsync(d_tris_unsorted, all_tris.data(), all_tris.size() * sizeof(azd::DevTri),
+        AZ_CUDA_TRY(cudaMemcpyAsync(d_tris_unsorted.p, all_tris.data(), all_tris.size() * sizeof(azd::DevTri),
                                     cudaMemcpyHostToDevice, st));
-        AZ_CUDA_TRY(cudaMemcpyAsync(d_attr_unsorted, all_attr.data(), all_attr.size() * sizeof(azd::DevTriAttr),
+        AZ_CUDA_TRY(cudaMemcpyAsync(d_attr_unsorted.p, all_attr.data(), all_attr.size() * sizeof(azd::DevTriAttr),
                                     cudaMemcpyHostToDevice, st));
     }
-    // Per hierarchy: LBVH on the GPU, read back, collapse to 8-wide nodes on the
-    // host, then gather the primitives once into wide-leaf order.
-    std::vector<azd::WideNode> wide;
-    uint32_t wide_depth = 0;
-    auto collapse = [&](uint32_t n, uint32_t node_base, uint32_t bin_root, uint32_t prim_base, uint32_t max_leaf,
-                        std::vector<uint32_t> &comp, uint32_t *wroot) -> int {
-        uint32_t nb = n > 1 ? n - 1 : 1;
-        std::vector<azd::BVHNode> bin(nb);
-        std::vector<uint32_t> perm(n);
-        AZ_CUDA_TRY(cudaMemcpyAsync(bin.data(), d_nodes + node_base, nb * sizeof(azd::BVHNode),
-                                    cudaMemcpyDeviceToHost, st));
-        AZ_CUDA_TRY(cudaMemcpyAsync(perm.data(), d_perm, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-        AZ_CUDA_TRY(cudaStreamSynchronize(st));
-        std::vector<uint32_t> order;
-        order.reserve(n);
-        uint32_t depth = 0;
-        int rc2 = CollapseToWide(bin, node_base, bin_root, max_leaf, width, wide, order, prim_base, wroot, &depth);
-        if (rc2 != AZ_OK) return rc2;
-        if (order.size() != n) return SetError(AZ_ERR_CUDA, "BVH collapse lost primitives");
-        wide_depth = std::max(wide_depth, depth);
-        // output slot j holds sorted position order[j], i.e. unsorted primitive perm[order[j] - prim_base]
-        comp.resize(n);
-        std::vector<uint8_t> seen(n, 0);
-        for (uint32_t j = 0; j < n; j++) {
-            uint32_t sp = order[j] - prim_base;
-            if (sp >= n || perm[sp] >= n || seen[perm[sp]])
-                return SetError(AZ_ERR_CUDA, "BVH collapse did not produce a permutation of the primitives");
-            seen[perm[sp]] = 1;
-            comp[j] = perm[sp];
-        }
-        return AZ_OK;
-    };
-    uint32_t node_base = 0;
-    std::vector<uint32_t> comp;
+    if (!tlas.empty())
+        AZ_CUDA_TRY(cudaMemcpyAsync(d_tlas_unsorted.p, tlas.data(), tlas.size() * sizeof(uint32_t),
+                                    cudaMemcpyHostToDevice, st));
+    AZ_CUDA_TRY(cudaStreamSynchronize(st));
+    const auto t_up1 = std::chrono::steady_clock::now();
+    G->upload_ms += std::chrono::duration<float, std::milli>(t_up1 - t_up0).count();
+    // Per hierarchy on the GPU: LBVH, collapse to wide nodes, then the
+    // primitives gathered once into wide-leaf order.
+    uint32_t wide_count = 0, wide_depth = 0, node_base = 0;
+    const int B = 256;
     for (auto &g : F.groups) {
         uint32_t n = g.g.tri_end - g.g.tri_begin;
         if (n == 0) {
             g.g.root = 0xFFFFFFFFu;
             continue;
         }
-        const int B = 256;
-        k_tri_boxes<<<(n + B - 1) / B, B, 0, st>>>(d_tris_unsorted + g.g.tri_begin, n, d_lo, d_hi);
+        k_tri_boxes<<<(n + B - 1) / B, B, 0, st>>>(d_tris_unsorted.p + g.g.tri_begin, n, d_lo.p, d_hi.p);
         AZ_CUDA_TRY(cudaGetLastError());
-        uint32_t root, wroot;
-        rc = BuildLBVH(d_lo, d_hi, n, d_nodes, node_base, g.g.tri_begin, d_perm, st, &root);
+        uint32_t root, wroot, depth = 0;
+        rc = BuildLBVH(d_lo.p, d_hi.p, n, d_nodes.p, d_range.p, node_base, g.g.tri_begin, d_perm.p, st, &root);
         if (rc != AZ_OK) return rc;
-        rc = collapse(n, node_base, root, g.g.tri_begin, leaf, comp, &wroot);
+        rc = CollapseToWide(d_nodes.p, d_range.p, root, n, g.g.tri_begin, d_perm.p, leaf, width, d_wide_tmp.p,
+                            node_total, &wide_count, d_comp.p, st, &wroot, &depth);
         if (rc != AZ_OK) return rc;
+        wide_depth = std::max(wide_depth, depth);
         g.g.root = wroot;
         node_base += n > 1 ? n - 1 : 1;
-        AZ_CUDA_TRY(cudaMemcpyAsync(d_perm, comp.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
-        k_gather_tris<<<(n + B - 1) / B, B, 0, st>>>(d_tris_unsorted + g.g.tri_begin, d_attr_unsorted + g.g.tri_begin,
-                                                     d_perm, n, d_tris + g.g.tri_begin, d_attr + g.g.tri_begin);
+        k_gather_tris<<<(n + B - 1) / B, B, 0, st>>>(d_tris_unsorted.p + g.g.tri_begin,
+                                                     d_attr_unsorted.p + g.g.tri_begin, d_comp.p, n,
+                                                     d_tris + g.g.tri_begin, d_attr + g.g.tri_begin);
         AZ_CUDA_TRY(cudaGetLastError());
-        AZ_CUDA_TRY(cudaStreamSynchronize(st));
+        G->hierarchies++;
     }
-    uint32_t *d_tlas = (uint32_t *)G->Alloc((tlas.size() + 1) * sizeof(uint32_t));
-    uint32_t *d_tlas_unsorted = (uint32_t *)G->Alloc((tlas.size() + 1) * sizeof(uint32_t));
-    if (!d_tlas || !d_tlas_unsorted) return SetError(AZ_ERR_OUT_OF_MEMORY, "device allocation failed");
     uint32_t tlas_root = 0xFFFFFFFFu;
     if (!tlas.empty()) {
         uint32_t n = (uint32_t)tlas.size();
-        AZ_CUDA_TRY(cudaMemcpyAsync(d_lo, tlo.data(), tlo.size() * sizeof(float4), cudaMemcpyHostToDevice, st));
-        AZ_CUDA_TRY(cudaMemcpyAsync(d_hi, thi.data(), thi.size() * sizeof(float4), cudaMemcpyHostToDevice, st));
-        AZ_CUDA_TRY(cudaMemcpyAsync(d_tlas_unsorted, tlas.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
-        uint32_t root;
-        rc = BuildLBVH(d_lo, d_hi, n, d_nodes, node_base, 0, d_perm, st, &root);
+        AZ_CUDA_TRY(cudaMemcpyAsync(d_lo.p, tlo.data(), tlo.size() * sizeof(float4), cudaMemcpyHostToDevice, st));
+        AZ_CUDA_TRY(cudaMemcpyAsync(d_hi.p, thi.data(), thi.size() * sizeof(float4), cudaMemcpyHostToDevice, st));
+        uint32_t root, depth = 0;
+        rc = BuildLBVH(d_lo.p, d_hi.p, n, d_nodes.p, d_range.p, node_base, 0, d_perm.p, st, &root);
         if (rc != AZ_OK) return rc;
         // top-level leaves hold one primitive each (a group is entered from its leaf)
-        rc = collapse(n, node_base, root, 0, 1, comp, &tlas_root);
+        rc = CollapseToWide(d_nodes.p, d_range.p, root, n, 0, d_perm.p, 1, width, d_wide_tmp.p, node_total,
+                            &wide_count, d_comp.p, st, &tlas_root, &depth);
         if (rc != AZ_OK) return rc;
+        wide_depth = std::max(wide_depth, depth);
         node_base += n > 1 ? n - 1 : 1;
-        const int B = 256;
-        AZ_CUDA_TRY(cudaMemcpyAsync(d_perm, comp.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
-        k_gather_u32<<<(n + B - 1) / B, B, 0, st>>>(d_tlas_unsorted, d_perm, n, d_tlas);
+        k_gather_u32<<<(n + B - 1) / B, B, 0, st>>>(d_tlas_unsorted.p, d_comp.p, n, d_tlas);
         AZ_CUDA_TRY(cudaGetLastError());
+        G->hierarchies++;
     }
-    azd::WideNode *d_wide = (azd::WideNode *)G->Alloc((wide.size() + 1) * sizeof(azd::WideNode));
+    azd::WideNode *d_wide = (azd::WideNode *)G->Alloc(((size_t)wide_count + 1) * sizeof(azd::WideNode));
     if (!d_wide) return SetError(AZ_ERR_OUT_OF_MEMORY, "device allocation failed");
-    if (!wide.empty())
-        AZ_CUDA_TRY(cudaMemcpyAsync(d_wide, wide.data(), wide.size() * sizeof(azd::WideNode), cudaMemcpyHostToDevice,
-                                    st));
+    if (wide_count)
+        AZ_CUDA_TRY(cudaMemcpyAsync(d_wide, d_wide_tmp.p, (size_t)wide_count * sizeof(azd::WideNode),
+                                    cudaMemcpyDeviceToDevice, st));
+    AZ_CUDA_TRY(cudaStreamSynchronize(st));
+    G->bvh_ms += std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t_up1).count();
 
     std::vector<azd::DevGroup> dgroups;
     for (auto &g : F.groups) dgroups.push_back(g.g);
@@ -740,19 +738,11 @@ int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_
         else if (azd::entity_light_needs_full_query(l)) D.full_light_queries = 1;
     }
     AZ_CUDA_TRY(cudaStreamSynchronize(st));
-    // the unsorted copies and build scratch are no longer needed
-    for (auto &b : G->bufs) {
-        if (b.ptr == d_tris_unsorted || b.ptr == d_attr_unsorted || b.ptr == d_lo || b.ptr == d_hi ||
-            b.ptr == d_perm || b.ptr == d_tlas_unsorted || b.ptr == d_nodes) {
-            cudaFree(b.ptr);
-            G->device_bytes -= b.bytes;
-            b.ptr = nullptr;
-        }
-    }
     G->triangle_count = total_tris;
     G->sphere_count = tlas.size() - dgroups.size();
-    G->node_count = wide.size();
+    G->node_count = wide_count;
     G->max_bvh_depth = wide_depth;
+    G->total_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t_start).count();
     *out = G.release();
     return AZ_OK;
 }

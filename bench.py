@@ -214,6 +214,8 @@ def main():
     gs = az.GpuScene(scene, device=local)
     torch.cuda.synchronize()
     upload_s = time.time() - t0
+    # az_gpu_scene_info: host flattening, uploads and the GPU BVH build of this first build
+    build = {k: (round(v, 2) if isinstance(v, float) else v) for k, v in gs.info().items()}
     tune = None
     if not args.no_autotune:
         # the autotuner's sweep (BVH width 8/4/2 x launch variants) on a band of the frame
@@ -334,9 +336,9 @@ def main():
                "config": {"workload": WORKLOAD, "triangles": int(scene.triangle_count), "width": w, "height": h,
                           "spp": spp, "max_depth": scene.max_depth(), "paths_per_step_per_gpu": paths_per_frame,
                           "parallelism": "dp%d (one frame per GPU, own seed)" % world,
-                          "l2": "inputs larger than L2 (scene ~%.0f MB on device)" % (
-                              (scene.triangle_count * (48 + 80 + 64)) / 1e6),
-                          "scene_upload_s": upload_s, "autotune": tune},
+                          "l2": "inputs larger than L2 (scene %.0f MB on device)" % (
+                              gs.info()["device_bytes"] / 1e6),
+                          "scene_upload_s": upload_s, "scene_build": build, "autotune": tune},
                "segments_per_s": world * seg / (ms / 1000.0), "rays_per_s": world * (seg + shadow) / (ms / 1000.0),
                "gpu_launches": int(launches), "stages_one_frame": stages, "e2e": e2e, "roofline": roofline,
                "clocks": clk}

@@ -96,6 +96,26 @@ typedef struct az_gpu_scene az_gpu_scene;
 int az_gpu_scene_create(const az_scene *scene, const az_render_opts *opts, az_gpu_scene **out);
 void az_gpu_scene_destroy(az_gpu_scene *scene);
 
+/* What az_gpu_scene_create built and how long its parts took (no counterpart
+ * in azimuth, whose ImportXML builds its BVHs on the host,
+ * src/azimuth_xml.cpp:3632-3875 and src/azimuth_bvh.cpp:1-328). */
+typedef struct az_scene_info {
+    uint64_t triangles;          /* triangles of all meshes, after flattening */
+    uint64_t spheres;
+    uint64_t wide_nodes;         /* compressed wide BVH nodes of all hierarchies */
+    uint64_t device_bytes;       /* device memory the scene holds */
+    uint32_t bvh_width, bvh_leaf;
+    uint32_t bvh_depth;          /* deepest wide-node level (root = 0) */
+    uint32_t hierarchies;        /* bottom-level hierarchies plus the top level */
+    float flatten_ms;            /* host: azimuth's entity trees walked into device records */
+    float upload_ms;             /* host-to-device copies of the primitives */
+    float bvh_ms;                /* GPU: LBVH builds, wide collapse and primitive gather */
+    float total_ms;              /* the whole az_gpu_scene_create call */
+    uint32_t reserved[4];
+} az_scene_info;
+
+int az_gpu_scene_info(const az_gpu_scene *scene, az_scene_info *out);
+
 /* ProduceImageInLinearSpace (src/azimuth_main.cpp:1256-1263) on the GPU:
  * accumulates every camera sample of the scissor rectangle into the HOST film
  * `pixels` (W*H entries, caller-zeroed or holding earlier sums), with
