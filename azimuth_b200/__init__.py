@@ -12,6 +12,7 @@ Typical use::
         film = g.render(sc)              # numpy (H, W, 4): rgb sum, weight sum
 """
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -343,14 +344,58 @@ def postprocess(film_ptr, width, height, key_value=0.18, burnout=1.0, saturation
                 inv_gamma=1.0 / 2.2, srgb=True, linear=False, rgb_ptr=None, rgb8_ptr=None, stream=None, device=0):
     """az_gpu_postprocess: azimuth's normalisation, tone mapping and gamma of a DEVICE film into DEVICE
     outputs (rgb_ptr: width*height*3 float32; rgb8_ptr: width*height*3 uint8)."""
+    tm = _tonemap(key_value, burnout, saturation, photographic)
+    o = make_opts(stream=stream, device=device)
+    _check(lib().az_gpu_postprocess(film_ptr, width, height, C.byref(tm), inv_gamma, 1 if srgb else 0,
+                                    1 if linear else 0, rgb_ptr, rgb8_ptr, C.byref(o)), "az_gpu_postprocess")
+
+
+FILE_PNG, FILE_BMP, FILE_TGA, FILE_JPG, FILE_EXR = 0, 1, 2, 3, 4   # azimuth's file_format values
+
+
+def _tonemap(key_value, burnout, saturation, photographic):
     tm = Tonemap()
     tm.KeyValue = key_value
     tm.BurnoutPercentage = burnout
     tm.Saturation = saturation
     tm.Operator = 1 if photographic else 0
+    return tm
+
+
+def output_pixels_to_file(path, film_ptr, width, height, file_format=FILE_PNG, key_value=0.18, burnout=1.0,
+                          saturation=1.0, photographic=True, inv_gamma=1.0 / 2.2, srgb=True, save_exr=False,
+                          stream=None, device=0):
+    """az_gpu_output_pixels_to_file: azimuth's OutputPixelsToFile for a DEVICE film (post-process on the
+    GPU, then this library's PNG/BMP/TGA/JPG/EXR writer)."""
+    tm = _tonemap(key_value, burnout, saturation, photographic)
     o = make_opts(stream=stream, device=device)
-    _check(lib().az_gpu_postprocess(film_ptr, width, height, C.byref(tm), inv_gamma, 1 if srgb else 0,
-                                    1 if linear else 0, rgb_ptr, rgb8_ptr, C.byref(o)), "az_gpu_postprocess")
+    _check(lib().az_gpu_output_pixels_to_file(os.fsencode(path), film_ptr, width, height, C.byref(tm), inv_gamma,
+                                              1 if srgb else 0, file_format, 1 if save_exr else 0, C.byref(o)),
+           "az_gpu_output_pixels_to_file")
+
+
+def write_image(path, rgb8, file_format=FILE_PNG, quality=None):
+    """az_write_image (az_write_jpg_quality with quality): uint8 array (H, W, 3) to a file."""
+    a = np.ascontiguousarray(rgb8, np.uint8)
+    h, w = a.shape[:2]
+    if quality is not None:
+        _check(lib().az_write_jpg_quality(os.fsencode(path), a.ctypes.data, w, h, int(quality)), "az_write_jpg_quality")
+    else:
+        _check(lib().az_write_image(os.fsencode(path), a.ctypes.data, w, h, file_format), "az_write_image")
+
+
+def write_exr(path, rgb):
+    """az_write_exr: float array (H, W, 3) to an uncompressed half-float OpenEXR file."""
+    a = np.ascontiguousarray(rgb, np.float32)
+    h, w = a.shape[:2]
+    _check(lib().az_write_exr(os.fsencode(path), a.ctypes.data, w, h), "az_write_exr")
+
+
+def exr_sibling_path(path):
+    """az_exr_sibling_path: the EXR name OutputPixelsToFile derives from `path`, or None."""
+    buf = C.create_string_buffer(256)
+    rc = lib().az_exr_sibling_path(os.fsencode(path), buf, 256)
+    return buf.value.decode() if rc == 0 else None
 
 
 def render_batch(jobs, streams=0, flags=0, chunk_samples=0, device=0, largest_first=False):

@@ -139,6 +139,17 @@ def _declare(L):
         L.az_gpu_postprocess.argtypes = [vp, u32, u32, C.POINTER(Tonemap), C.c_float, u32, u32, vp, vp,
                                          C.POINTER(RenderOpts)]
         L.az_gpu_postprocess.restype = i32
+        L.az_gpu_output_pixels_to_file.argtypes = [C.c_char_p, vp, u32, u32, C.POINTER(Tonemap), C.c_float, u32,
+                                                    i32, u32, C.POINTER(RenderOpts)]
+        L.az_gpu_output_pixels_to_file.restype = i32
+        L.az_write_image.argtypes = [C.c_char_p, vp, u32, u32, i32]
+        L.az_write_image.restype = i32
+        L.az_write_jpg_quality.argtypes = [C.c_char_p, vp, u32, u32, i32]
+        L.az_write_jpg_quality.restype = i32
+        L.az_write_exr.argtypes = [C.c_char_p, vp, u32, u32]
+        L.az_write_exr.restype = i32
+        L.az_exr_sibling_path.argtypes = [C.c_char_p, C.c_char_p, u32]
+        L.az_exr_sibling_path.restype = i32
         L.az_gpu_render_batch.argtypes = [vp, u32, C.POINTER(BatchOpts), C.POINTER(BatchStats)]
         L.az_gpu_render_batch.restype = i32
         L.az_guide_create.argtypes = [vp, C.POINTER(GuideConfig), C.POINTER(vp)]

@@ -4,7 +4,8 @@ Host C++ (scene assembly, generators, the RenderScene-style host API) is
 compiled with g++ and ``-ffp-contract=off`` so its float sums round like
 azimuth's; CUDA sources are compiled by nvcc for sm_100a only
 (``-gencode arch=compute_100a,code=sm_100a``).  The result links the CUDA
-runtime statically, so the library needs only the driver at run time.
+runtime statically, so the library needs only the driver and the system zlib
+at run time.
 
 Usage: python -m azimuth_b200.build [--force] [--debug]
 """
@@ -76,9 +77,9 @@ def build(force=False, debug=False, verbose=False):
         objs.append(obj)
     if force or not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
         if cu_srcs:
-            _run([NVCC, "-shared", "-cudart", "static"] + ARCH + objs + ["-o", LIB, "-lpthread"])
+            _run([NVCC, "-shared", "-cudart", "static"] + ARCH + objs + ["-o", LIB, "-lpthread", "-lz"])
         else:
-            _run(["g++", "-shared"] + objs + ["-o", LIB])
+            _run(["g++", "-shared"] + objs + ["-o", LIB, "-lz"])
     return LIB
 
 

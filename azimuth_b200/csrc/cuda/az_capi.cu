@@ -8,8 +8,10 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "az_internal.h"
+#include "azimuth_io.h"
 
 namespace az {
 
@@ -288,6 +290,57 @@ extern "C" int az_gpu_postprocess(const az_pixel *film, uint32_t width, uint32_t
     int rc = ctx.begin(opts);
     if (rc != AZ_OK) return rc;
     return PostProcess(film, width, height, tonemap, inv_gamma, srgb, linear, rgb_out, rgb8_out, ctx.stream);
+}
+
+extern "C" int az_gpu_output_pixels_to_file(const char *path, const az_pixel *film, uint32_t width, uint32_t height,
+                                            const az_tonemap *tonemap, float inv_gamma, uint32_t srgb, int32_t format,
+                                            uint32_t save_exr, const az_render_opts *opts) {
+    if (!path || !film || width == 0 || height == 0) return SetError(AZ_ERR_INVALID_ARGUMENT, "null path or film");
+    if (format < AZ_FileFormat_PNG || format > AZ_FileFormat_EXR)
+        return SetError(AZ_ERR_INVALID_ARGUMENT, "unknown file format");
+    if ((uint64_t)width * height > 0x7FFFFFFFull) return SetError(AZ_ERR_INVALID_ARGUMENT, "film too large");
+    CallContext ctx;
+    int rc = ctx.begin(opts);
+    if (rc != AZ_OK) return rc;
+    const size_t n = (size_t)width * height;
+    if (format == AZ_FileFormat_EXR || save_exr) {
+        // the normalised colours times 255, before tone mapping and gamma
+        // (OutputPixelsToEXR, src/azimuth_main.cpp:1426-1458)
+        std::string exr_path = path;
+        if (format != AZ_FileFormat_EXR) {
+            char sib[256];
+            exr_path = az_exr_sibling_path(path, sib, sizeof(sib)) == AZ_OK ? std::string(sib) : std::string();
+        }
+        if (!exr_path.empty()) {
+            float *d_rgb = nullptr;
+            AZ_CUDA_TRY(cudaMalloc((void **)&d_rgb, n * 3 * sizeof(float)));
+            rc = PostProcess(film, width, height, tonemap, inv_gamma, srgb, 1, d_rgb, nullptr, ctx.stream);
+            std::vector<float> rgb(n * 3);
+            if (rc == AZ_OK) {
+                cudaError_t e = cudaMemcpy(rgb.data(), d_rgb, n * 3 * sizeof(float), cudaMemcpyDeviceToHost);
+                if (e != cudaSuccess) rc = CudaError(e, "cudaMemcpy(EXR colours)");
+            }
+            cudaFree(d_rgb);
+            if (rc != AZ_OK) return rc;
+            for (float &c : rgb) c = c * 255.0f;
+            if (az_write_exr(exr_path.c_str(), rgb.data(), width, height) != AZ_OK)
+                return SetError(AZ_ERR_IO, "cannot write " + exr_path);
+        }
+        if (format == AZ_FileFormat_EXR) return AZ_OK;
+    }
+    uint8_t *d_rgb8 = nullptr;
+    AZ_CUDA_TRY(cudaMalloc((void **)&d_rgb8, n * 3));
+    rc = PostProcess(film, width, height, tonemap, inv_gamma, srgb, 0, nullptr, d_rgb8, ctx.stream);
+    std::vector<uint8_t> rgb8(n * 3);
+    if (rc == AZ_OK) {
+        cudaError_t e = cudaMemcpy(rgb8.data(), d_rgb8, n * 3, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) rc = CudaError(e, "cudaMemcpy(8-bit colours)");
+    }
+    cudaFree(d_rgb8);
+    if (rc != AZ_OK) return rc;
+    if (az_write_image(path, rgb8.data(), width, height, format) != AZ_OK)
+        return SetError(AZ_ERR_IO, std::string("cannot write ") + path);
+    return AZ_OK;
 }
 
 extern "C" int az_gpu_closest_hit(az_gpu_scene *scene, const az_ray3 *rays, uint32_t count, int32_t cull,

@@ -35,7 +35,8 @@ enum {
     AZ_ERR_CUDA = 4,
     AZ_ERR_TIMEOUT = 5,
     AZ_ERR_UNSUPPORTED = 6,
-    AZ_ERR_NO_DEVICE = 7
+    AZ_ERR_NO_DEVICE = 7,
+    AZ_ERR_IO = 8
 };
 
 /* az_render_opts.flags */

@@ -24,6 +24,7 @@
 #include "azimuth_main.cpp"
 
 #include <omp.h>
+#include <vector>
 #include "az_abi.h"
 #include "az_rng_oracle.h"
 
@@ -284,6 +285,40 @@ int azref_output_pixels(az_pixel *Pixels, uint32_t Width, uint32_t Height, const
     strncpy(Path, BmpPath, sizeof(Path) - 1);
     return OutputPixelsToFile(Path, (pixel *)Pixels, Vec2u(Width, Height), &T, InvGamma, (b32)SRGB,
                               FileFormat_BMP, false) ? 1 : 0;
+}
+
+/* OutputPixelsToFile (src/azimuth_main.cpp:1620-1797) with any of the four
+ * 8-bit formats (file_format values, src/azimuth_io.h:1-7); no EXR (OpenEXR
+ * is stubbed in this build). */
+int azref_output_pixels_fmt(az_pixel *Pixels, uint32_t Width, uint32_t Height, const az_tonemap *Tonemap,
+                            float InvGamma, uint32_t SRGB, int32_t Format, const char *FilePath) {
+    if (Format < FileFormat_PNG || Format > FileFormat_JPG) return 0;
+    tonemap T;
+    memcpy(&T, Tonemap, sizeof(T));
+    char Path[256] = {0};
+    strncpy(Path, FilePath, sizeof(Path) - 1);
+    return OutputPixelsToFile(Path, (pixel *)Pixels, Vec2u(Width, Height), &T, InvGamma, (b32)SRGB,
+                              (file_format)Format, false) ? 1 : 0;
+}
+
+/* OutputPixelsToPNG / BMP / TGA / JPG (src/azimuth_main.cpp:1460-1618)
+ * alone, on colours rgb (W*H*3 floats, top row first). */
+int azref_write_image(const float *Rgb, uint32_t Width, uint32_t Height, int32_t Format, const char *FilePath) {
+    std::vector<pixel> Px((size_t)Width * Height);
+    for (size_t i = 0; i < Px.size(); i++) {
+        Px[i].Color = Vec3(Rgb[3 * i + 0], Rgb[3 * i + 1], Rgb[3 * i + 2]);
+        Px[i].TotalWeight = 1.0f;
+    }
+    char Path[256] = {0};
+    strncpy(Path, FilePath, sizeof(Path) - 1);
+    vec2u Size = Vec2u(Width, Height);
+    switch (Format) {
+        case FileFormat_PNG: return OutputPixelsToPNG(Path, Px.data(), Size) ? 1 : 0;
+        case FileFormat_BMP: return OutputPixelsToBMP(Path, Px.data(), Size) ? 1 : 0;
+        case FileFormat_TGA: return OutputPixelsToTGA(Path, Px.data(), Size) ? 1 : 0;
+        case FileFormat_JPG: return OutputPixelsToJPG(Path, Px.data(), Size) ? 1 : 0;
+        default: return 0;
+    }
 }
 
 }  /* extern "C" */

@@ -42,6 +42,10 @@ def ref(fast=False):
         L.azref_set_seed.argtypes = [u64]
         L.azref_output_pixels.argtypes = [vp, u32, u32, vp, C.c_float, u32, C.c_char_p]
         L.azref_output_pixels.restype = i32
+        L.azref_output_pixels_fmt.argtypes = [vp, u32, u32, vp, C.c_float, u32, i32, C.c_char_p]
+        L.azref_output_pixels_fmt.restype = i32
+        L.azref_write_image.argtypes = [vp, u32, u32, i32, C.c_char_p]
+        L.azref_write_image.restype = i32
         L.azref_produce_image.argtypes = [vp, vp, vp, vp, Scissor, i32, i32, u32]
         L.azref_closest_hit.argtypes = [vp, vp, u32, i32, C.c_float, vp, vp, vp, vp, vp, i32]
         L.azref_set_perlin_gradients.argtypes = [vp]

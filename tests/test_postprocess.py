@@ -63,3 +63,32 @@ def test_gpu_postprocess_linear_output_is_the_normalised_film(gpu):
     rgb = torch.zeros((h, w, 3), device="cuda")
     az.postprocess(d_film.data_ptr(), w, h, linear=True, rgb_ptr=rgb.data_ptr())
     assert np.array_equal(rgb.cpu().numpy(), (film[..., :3] / film[..., 3:4]).astype(np.float32))
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not ol.have_ref(), reason="azimuth's compiled reference is not built here")
+@pytest.mark.parametrize("fmt,ext", [(az.FILE_PNG, "png"), (az.FILE_BMP, "bmp"), (az.FILE_TGA, "tga")])
+def test_gpu_output_pixels_to_file_matches_azimuths_file(gpu, tmp_path, fmt, ext):
+    """az_gpu_output_pixels_to_file against azimuth's OutputPixelsToFile writing the same format."""
+    import ctypes as C
+    import torch
+    from PIL import Image
+    from azimuth_b200._native import Tonemap
+    film = _film()
+    h, w = film.shape[:2]
+    ours, ref = str(tmp_path / ("ours." + ext)), str(tmp_path / ("ref." + ext))
+    d_film = torch.from_numpy(film).cuda()
+    az.output_pixels_to_file(ours, d_film.data_ptr(), w, h, fmt, save_exr=True)
+    tm = Tonemap()
+    tm.KeyValue, tm.BurnoutPercentage, tm.Saturation, tm.Operator = 0.18, 1.0, 1.0, 1
+    px = np.ascontiguousarray(film, np.float32).copy()
+    assert ol.ref().azref_output_pixels_fmt(px.ctypes.data, w, h, C.byref(tm), 1.0 / 2.2, 1, fmt, ref.encode()) == 1
+    a = np.asarray(Image.open(ours).convert("RGB")).astype(np.int32)
+    b = np.asarray(Image.open(ref).convert("RGB")).astype(np.int32)
+    diff = np.abs(a - b)
+    assert diff.max() <= 1 and (diff == 0).mean() >= 0.995
+    # the EXR beside it: the normalised colours times 255 as halves
+    from test_image_io import _read_exr
+    _, got = _read_exr(str(tmp_path / "ours.exr"))
+    want = ((film[..., :3] / film[..., 3:4]).astype(np.float32) * np.float32(255.0)).astype(np.float16)
+    assert np.array_equal(got.view(np.uint16), want.view(np.uint16))
