@@ -17,8 +17,10 @@ import os
 import numpy as np
 
 from . import _native
-from ._native import (BatchOpts, BatchStats, GenParams, GeneratedScene, GuideConfig, Job, RenderOpts, RenderStats,
-                      SceneInfo, Scissor, Tonemap, Vec2u, Ray3, lib)
+from ._native import (BatchOpts, BatchStats, GenParams, GeneratedScene, GuideConfig, Job, MeshDesc, MeshSoup,
+                      RenderOpts, RenderStats, SceneInfo, Scissor, Tonemap, Vec2u, Ray3, lib)
+
+GEN_SOUP_ONLY = 1   # az_gen_params.flags: meshes left as the importer's soup
 
 SCENE_CORNELL = 0
 SCENE_DENSE_MESH = 1
@@ -56,9 +58,10 @@ class Scene:
     """A generated azimuth scene (azimuth structs owned by the native library)."""
 
     def __init__(self, scene_id, seed=0, width=0, height=0, spp=0, max_depth=0, detail=0, filter=-1,
-                 importance_sampling=-1, env_width=0, env_height=0):
+                 importance_sampling=-1, env_width=0, env_height=0, soup_only=False):
         self._g = GeneratedScene()
-        p = GenParams(width, height, spp, max_depth, detail, filter, importance_sampling, env_width, env_height)
+        p = GenParams(width, height, spp, max_depth, detail, filter, importance_sampling, env_width, env_height,
+                      GEN_SOUP_ONLY if soup_only else 0)
         rc = lib().az_scene_generate(int(scene_id), int(seed), C.byref(p), C.byref(self._g))
         if rc != 0:
             raise RuntimeError("az_scene_generate(%d) failed with %d" % (scene_id, rc))
@@ -68,6 +71,26 @@ class Scene:
     @property
     def scene_ptr(self):
         return self._g.scene
+
+    @property
+    def soup_ptr(self):
+        """The meshes before the importer's post-processing (az_mesh_soup*)."""
+        return self._g.soup
+
+    def soup_arrays(self):
+        """Copies of the soup: (vertices (V, 3) f32, faces (F, 3) u32, uvs (U, 2) f32, mesh descs list)."""
+        s = MeshSoup.from_address(self._g.soup)
+
+        def arr(ptr, n, k, dt):
+            if n == 0:
+                return np.zeros((0, k), dt)
+            return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(C.c_float if dt == np.float32 else C.c_uint32)),
+                                         (n * k,)).reshape(n, k).copy()
+        descs = [MeshDesc.from_address(s.meshes + i * C.sizeof(MeshDesc)) for i in range(s.mesh_count)]
+        descs = [{k: (list(getattr(d, k)) if not isinstance(getattr(d, k), int) else getattr(d, k))
+                  for k, _ in MeshDesc._fields_} for d in descs]
+        return (arr(s.vertices, s.vertex_count, 3, np.float32), arr(s.faces, s.face_count, 3, np.uint32),
+                arr(s.uvs, s.uv_count, 2, np.float32), descs)
 
     @property
     def camera_ptr(self):
@@ -157,12 +180,18 @@ def produce_image(scene, pixels=None, scissor=None, filter_type=None, backface_c
 class GpuScene:
     """A device-resident scene (az_gpu_scene_create / az_gpu_scene_destroy)."""
 
-    def __init__(self, scene, device=0, bvh_width=0, bvh_leaf=0):
+    def __init__(self, scene, device=0, bvh_width=0, bvh_leaf=0, from_soup=False):
+        """from_soup: build through az_gpu_scene_create_from_meshes from the scene's mesh soup (the meshes
+        post-processed on the GPU) instead of azimuth's finished structs."""
         self.scene = scene
         self.device = device
         self._h = C.c_void_p()
         o = make_opts(scene, device=device, bvh_width=bvh_width, bvh_leaf=bvh_leaf)
-        _check(lib().az_gpu_scene_create(scene.scene_ptr, C.byref(o), C.byref(self._h)), "az_gpu_scene_create")
+        if from_soup:
+            _check(lib().az_gpu_scene_create_from_meshes(scene.scene_ptr, scene.soup_ptr, C.byref(o),
+                                                         C.byref(self._h)), "az_gpu_scene_create_from_meshes")
+        else:
+            _check(lib().az_gpu_scene_create(scene.scene_ptr, C.byref(o), C.byref(self._h)), "az_gpu_scene_create")
 
     def info(self):
         """az_gpu_scene_info: what the build made (triangles, spheres, wide nodes, depth, device bytes) and
@@ -351,6 +380,20 @@ def postprocess(film_ptr, width, height, key_value=0.18, burnout=1.0, saturation
 
 
 FILE_PNG, FILE_BMP, FILE_TGA, FILE_JPG, FILE_EXR = 0, 1, 2, 3, 4   # azimuth's file_format values
+
+
+def mesh_postprocess(scene, device=0):
+    """az_gpu_mesh_postprocess of a generated scene's soup: dict of vertex_normals (V, 3), triangles (F, 12:
+    P0, P1, P2, N), attrs (F, 15: N0, N1, N2, UV0, UV1, UV2), total_area (M,), all float32."""
+    s = MeshSoup.from_address(scene.soup_ptr)
+    vn = np.zeros((s.vertex_count, 3), np.float32)
+    tris = np.zeros((s.face_count, 12), np.float32)
+    attrs = np.zeros((s.face_count, 15), np.float32)
+    area = np.zeros(s.mesh_count, np.float32)
+    o = make_opts(device=device)
+    _check(lib().az_gpu_mesh_postprocess(scene.soup_ptr, vn.ctypes.data, tris.ctypes.data, attrs.ctypes.data,
+                                         area.ctypes.data, C.byref(o)), "az_gpu_mesh_postprocess")
+    return {"vertex_normals": vn, "triangles": tris, "attrs": attrs, "total_area": area}
 
 
 def _tonemap(key_value, burnout, saturation, photographic):

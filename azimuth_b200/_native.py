@@ -32,14 +32,14 @@ class GenParams(C.Structure):
     _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("spp", C.c_uint32),
                 ("max_depth", C.c_uint32), ("detail", C.c_uint32), ("filter", C.c_int32),
                 ("importance_sampling", C.c_int32), ("env_width", C.c_uint32),
-                ("env_height", C.c_uint32)]
+                ("env_height", C.c_uint32), ("flags", C.c_uint32)]
 
 
 class GeneratedScene(C.Structure):
     _fields_ = [("scene", C.c_void_p), ("camera", C.c_void_p), ("epsilons", C.c_void_p),
                 ("filter_type", C.c_int32), ("backface_culling", C.c_uint32),
                 ("perlin_gradients", C.c_void_p), ("triangle_count", C.c_uint64),
-                ("sphere_count", C.c_uint64), ("owner", C.c_void_p)]
+                ("sphere_count", C.c_uint64), ("owner", C.c_void_p), ("soup", C.c_void_p)]
 
 
 class RenderOpts(C.Structure):
@@ -89,7 +89,20 @@ class SceneInfo(C.Structure):
                 ("device_bytes", C.c_uint64), ("bvh_width", C.c_uint32), ("bvh_leaf", C.c_uint32),
                 ("bvh_depth", C.c_uint32), ("hierarchies", C.c_uint32), ("flatten_ms", C.c_float),
                 ("upload_ms", C.c_float), ("bvh_ms", C.c_float), ("total_ms", C.c_float),
-                ("reserved", C.c_uint32 * 4)]
+                ("ingest_ms", C.c_float), ("reserved", C.c_uint32 * 3)]
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [("face_base", C.c_uint32), ("face_count", C.c_uint32), ("uv_offset", C.c_int32),
+                ("shading_mode", C.c_uint32), ("material_index", C.c_uint32), ("texture_index", C.c_uint32),
+                ("is_emitter", C.c_uint32), ("unique_entity_id", C.c_uint32), ("motion", C.c_float * 3),
+                ("radiance", C.c_float * 3), ("transform", C.c_float * 16), ("inv_transform", C.c_float * 16)]
+
+
+class MeshSoup(C.Structure):
+    _fields_ = [("vertices", C.c_void_p), ("faces", C.c_void_p), ("uvs", C.c_void_p), ("meshes", C.c_void_p),
+                ("vertex_count", C.c_uint32), ("face_count", C.c_uint32), ("uv_count", C.c_uint32),
+                ("mesh_count", C.c_uint32)]
 
 
 def lib():
@@ -125,6 +138,10 @@ def _declare(L):
         L.az_gpu_scene_destroy.restype = None
         L.az_gpu_scene_info.argtypes = [vp, C.POINTER(SceneInfo)]
         L.az_gpu_scene_info.restype = i32
+        L.az_gpu_scene_create_from_meshes.argtypes = [vp, vp, C.POINTER(RenderOpts), C.POINTER(vp)]
+        L.az_gpu_scene_create_from_meshes.restype = i32
+        L.az_gpu_mesh_postprocess.argtypes = [vp, vp, vp, vp, vp, C.POINTER(RenderOpts)]
+        L.az_gpu_mesh_postprocess.restype = i32
         L.az_gpu_render.argtypes = [vp, vp, vp, vp, Scissor, i32, u32, C.POINTER(RenderOpts),
                                     C.POINTER(RenderStats)]
         L.az_gpu_render.restype = i32

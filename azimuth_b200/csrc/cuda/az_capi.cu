@@ -103,6 +103,43 @@ extern "C" int az_gpu_scene_create(const az_scene *scene, const az_render_opts *
     return AZ_OK;
 }
 
+extern "C" int az_gpu_scene_create_from_meshes(const az_scene *scene, const az_mesh_soup *soup,
+                                               const az_render_opts *opts, az_gpu_scene **out) {
+    if (!scene || !soup || !out) return SetError(AZ_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    CallContext ctx;
+    int rc = ctx.begin(opts);
+    if (rc != AZ_OK) return rc;
+    GpuScene *g = nullptr;
+    rc = BuildGpuScene(scene, opts, ctx.stream, &g, soup);
+    if (rc != AZ_OK) return rc;
+    az_gpu_scene *h = new (std::nothrow) az_gpu_scene{g};
+    if (!h) {
+        delete g;
+        return SetError(AZ_ERR_OUT_OF_MEMORY, "host allocation failed");
+    }
+    *out = h;
+    return AZ_OK;
+}
+
+extern "C" int az_gpu_mesh_postprocess(const az_mesh_soup *soup, az_vec3 *vertex_normals, az_triangle *triangles,
+                                       az_face_attr *attrs, float *total_area, const az_render_opts *opts) {
+    if (!soup) return SetError(AZ_ERR_INVALID_ARGUMENT, "null mesh soup");
+    CallContext ctx;
+    int rc = ctx.begin(opts);
+    if (rc != AZ_OK) return rc;
+    SoupWork *w = nullptr;
+    rc = IngestSoup(soup, ctx.stream, &w);
+    if (rc != AZ_OK) return rc;
+    std::unique_ptr<SoupWork, void (*)(SoupWork *)> hold(w, FreeSoupWork);
+    if (total_area) {
+        std::vector<float> a;
+        if ((rc = SoupAreas(*w, a)) != AZ_OK) return rc;
+        if (!a.empty()) memcpy(total_area, a.data(), a.size() * sizeof(float));
+    }
+    return SoupRecords(*w, triangles, attrs, vertex_normals, ctx.stream);
+}
+
 extern "C" int az_gpu_scene_info(const az_gpu_scene *scene, az_scene_info *out) {
     if (!scene || !scene->impl || !out) return SetError(AZ_ERR_INVALID_ARGUMENT, "null scene or output");
     const GpuScene &G = *scene->impl;
@@ -119,6 +156,7 @@ extern "C" int az_gpu_scene_info(const az_gpu_scene *scene, az_scene_info *out) 
     out->upload_ms = G.upload_ms;
     out->bvh_ms = G.bvh_ms;
     out->total_ms = G.total_ms;
+    out->ingest_ms = G.ingest_ms;
     return AZ_OK;
 }
 

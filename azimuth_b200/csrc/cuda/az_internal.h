@@ -42,6 +42,7 @@ struct GpuScene {
     float upload_ms = 0.0f;      // host-to-device copies of the primitives
     float bvh_ms = 0.0f;         // GPU: LBVH builds, wide collapse, primitive gather
     float total_ms = 0.0f;       // the whole az_gpu_scene_create
+    float ingest_ms = 0.0f;      // GPU post-processing of a mesh soup (az_gpu_scene_create_from_meshes)
     uint32_t bvh_width = 8;      // children per wide node (2, 4 or 8)
     uint32_t bvh_leaf = 2;       // triangles per bottom-level leaf at most
     size_t device_bytes = 0;
@@ -54,8 +55,27 @@ struct GpuScene {
     void *Alloc(size_t bytes);   // nullptr on failure
 };
 
-// Builds the device scene from azimuth's structs (az_scene_upload.cu).
-int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_t stream, GpuScene **out);
+// Builds the device scene from azimuth's structs (az_scene_upload.cu); with
+// `soup` the meshes come from it instead (post-processed on the GPU).
+int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_t stream, GpuScene **out,
+                  const az_mesh_soup *soup = nullptr);
+
+// The importer's mesh post-processing on the GPU (az_mesh_ingest.cu).
+struct SoupWork;
+struct IngestMesh {
+    uint32_t out_base;           // first slot of the mesh's triangles in the device primitive arrays
+    uint32_t entity;             // dense index of its instance entity
+    uint32_t shading_mode, texture_index;
+};
+int IngestSoup(const az_mesh_soup *soup, cudaStream_t st, SoupWork **out);
+void FreeSoupWork(SoupWork *w);
+int SoupAreas(const SoupWork &w, std::vector<float> &areas);
+// Per mesh (soup order): lo.xyz, hi.xyz of its faces' vertices.
+int SoupBoxes(const SoupWork &w, std::vector<float> &boxes, cudaStream_t st);
+int SoupRecords(const SoupWork &w, az_triangle *tris, az_face_attr *attrs, az_vec3 *vertex_normals, cudaStream_t st);
+int SoupTriangles(const SoupWork &w, uint32_t face_base, uint32_t count, az_triangle *tris, cudaStream_t st);
+int SoupEmitScene(const SoupWork &w, const std::vector<IngestMesh> &meshes, azd::DevTri *d_tris,
+                  azd::DevTriAttr *d_attr, cudaStream_t st);
 
 // LBVH over `n` boxes (device arrays lo/hi of float4).  Writes nodes into
 // `nodes` starting at `node_base` (n-1 nodes, or 1 for n == 1), each inner

@@ -17,6 +17,7 @@
 #include <string>
 
 #include "az_internal.h"
+#include "az_scene_build.h"
 
 namespace az {
 
@@ -99,6 +100,8 @@ struct HostGroup {
     azd::DevGroup g{};
     std::vector<azd::DevTri> tris;
     std::vector<azd::DevTriAttr> attr;
+    std::vector<uint32_t> soup_meshes;   // meshes of the soup whose triangles follow `tris` on the device
+    uint32_t soup_tris = 0;
     Box local;
 };
 
@@ -109,7 +112,30 @@ struct Flattener {
     std::vector<HostGroup> groups;
     std::map<GroupKey, uint32_t> group_of;
     int raw_group = -1;
+    bool skip_meshes = false;            // mesh instances come from a soup instead
     std::string err;
+
+    // The group of an instance with these matrices and motion (one BLAS per
+    // distinct transform).
+    uint32_t GroupFor(const azd::DevEntity &d) {
+        GroupKey key;
+        memcpy(key.bytes, &d.inv, sizeof(m34));
+        memcpy(key.bytes + sizeof(m34), &d.xf, sizeof(m34));
+        memcpy(key.bytes + 2 * sizeof(m34), d.motion, 12);
+        memset(key.bytes + 2 * sizeof(m34) + 12, 0, 4);
+        auto it = group_of.find(key);
+        if (it != group_of.end()) return it->second;
+        const uint32_t gi = (uint32_t)groups.size();
+        group_of.emplace(key, gi);
+        groups.emplace_back();
+        HostGroup &g = groups.back();
+        g.g.inv = d.inv;
+        g.g.xf = d.xf;
+        memcpy(g.g.motion, d.motion, 12);
+        g.g.identity = IsIdentity(d.inv) && IsIdentity(d.xf) && d.motion[0] == 0.0f && d.motion[1] == 0.0f &&
+                       d.motion[2] == 0.0f;
+        return gi;
+    }
 
     azd::DevEntity BaseEntity(const az_entity *e) {
         azd::DevEntity d;
@@ -183,6 +209,7 @@ struct Flattener {
     }
 
     bool Run() {
+        if (!s->BVHRoot && skip_meshes) return true;   // every entity is a mesh of the soup
         return Walk(s->BVHRoot, [&](const az_entity *e) -> bool {
             uint32_t idx = (uint32_t)ents.size();
             azd::DevEntity d = BaseEntity(e);
@@ -217,31 +244,13 @@ struct Flattener {
                     return AddTriangle(groups[raw_group], e, idx);
                 }
                 case AZ_Entity_MeshInstance: {
+                    if (skip_meshes) return true;
                     d.type = azd::ENT_INSTANCE;
                     if (!e->Mesh) {
                         err = "mesh instance without mesh";
                         return false;
                     }
-                    GroupKey key;
-                    memcpy(key.bytes, &d.inv, sizeof(m34));
-                    memcpy(key.bytes + sizeof(m34), &d.xf, sizeof(m34));
-                    memcpy(key.bytes + 2 * sizeof(m34), d.motion, 12);
-                    memset(key.bytes + 2 * sizeof(m34) + 12, 0, 4);
-                    auto it = group_of.find(key);
-                    uint32_t gi;
-                    if (it == group_of.end()) {
-                        gi = (uint32_t)groups.size();
-                        group_of.emplace(key, gi);
-                        groups.emplace_back();
-                        HostGroup &g = groups.back();
-                        g.g.inv = d.inv;
-                        g.g.xf = d.xf;
-                        memcpy(g.g.motion, d.motion, 12);
-                        g.g.identity = IsIdentity(d.inv) && IsIdentity(d.xf) && d.motion[0] == 0.0f &&
-                                       d.motion[1] == 0.0f && d.motion[2] == 0.0f;
-                    } else {
-                        gi = it->second;
-                    }
+                    const uint32_t gi = GroupFor(d);
                     d.group = gi;
                     ents.push_back(d);
                     ent_box.push_back(Box());
@@ -356,7 +365,8 @@ __global__ void k_tri_boxes(const azd::DevTri *t, uint32_t n, float4 *lo, float4
 
 }  // namespace
 
-int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_t st, GpuScene **out) {
+int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_t st, GpuScene **out,
+                  const az_mesh_soup *soup) {
     if (!scene || !out) return SetError(AZ_ERR_INVALID_ARGUMENT, "null scene");
     *out = nullptr;
     const auto t_start = std::chrono::steady_clock::now();
@@ -370,8 +380,57 @@ int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_
     G->bvh_leaf = leaf;
     Flattener F;
     F.s = scene;
-    if (!scene->BVHRoot) return SetError(AZ_ERR_INVALID_SCENE, "scene has no BVHRoot");
+    F.skip_meshes = soup != nullptr;
+    if (!scene->BVHRoot && !soup) return SetError(AZ_ERR_INVALID_SCENE, "scene has no BVHRoot");
     if (!F.Run()) return SetError(AZ_ERR_INVALID_SCENE, F.err);
+
+    // ---- meshes of a soup: post-processed on the GPU, one instance entity each ----
+    std::unique_ptr<SoupWork, void (*)(SoupWork *)> soupw(nullptr, FreeSoupWork);
+    std::vector<IngestMesh> ingest;
+    std::vector<float> soup_area;
+    if (soup) {
+        const auto t_in = std::chrono::steady_clock::now();
+        SoupWork *w = nullptr;
+        int r = IngestSoup(soup, st, &w);
+        if (r != AZ_OK) return r;
+        soupw.reset(w);
+        if ((r = SoupAreas(*w, soup_area)) != AZ_OK) return r;
+        // per-mesh bounds for the top-level boxes of their groups
+        std::vector<float> boxes;
+        if ((r = SoupBoxes(*w, boxes, st)) != AZ_OK) return r;
+        const az_mat4 I = Mat4Identity();
+        ingest.resize(soup->mesh_count);
+        for (uint32_t m = 0; m < soup->mesh_count; m++) {
+            const az_mesh_desc &md = soup->meshes[m];
+            if (md.face_count == 0) return SetError(AZ_ERR_INVALID_SCENE, "a mesh of the soup has no faces");
+            // the instance entity the importer appends for the mesh
+            // (src/azimuth_xml.cpp:3753-3766), transform composed as in :3785-3791
+            azd::DevEntity d;
+            memset(&d, 0, sizeof(d));
+            d.type = azd::ENT_INSTANCE;
+            d.xf = ToM34(Mat4Mul(I, md.transform));
+            d.inv = ToM34(Mat4Mul(md.inv_transform, I));
+            d.motion[0] = md.motion.x; d.motion[1] = md.motion.y; d.motion[2] = md.motion.z;
+            d.radiance[0] = md.radiance.x; d.radiance[1] = md.radiance.y; d.radiance[2] = md.radiance.z;
+            d.is_emitter = md.is_emitter ? 1u : 0u;
+            d.texture_index = md.texture_index;
+            d.material = md.material_index;
+            d.uid = md.unique_entity_id;
+            const uint32_t gi = F.GroupFor(d);
+            d.group = gi;
+            ingest[m].entity = (uint32_t)F.ents.size();
+            ingest[m].shading_mode = md.shading_mode;
+            ingest[m].texture_index = md.texture_index;
+            F.ents.push_back(d);
+            F.ent_box.push_back(Box());
+            HostGroup &g = F.groups[gi];
+            g.soup_meshes.push_back(m);
+            g.soup_tris += md.face_count;
+            g.local.grow(boxes[6 * m + 0], boxes[6 * m + 1], boxes[6 * m + 2]);
+            g.local.grow(boxes[6 * m + 3], boxes[6 * m + 4], boxes[6 * m + 5]);
+        }
+        G->ingest_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t_in).count();
+    }
 
     // ---- materials, textures, lights, validation ----
     std::vector<azd::DevMaterial> mats(scene->MaterialCount);
@@ -421,6 +480,9 @@ int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_
         for (const azd::DevTriAttr &a : g.attr)
             if (a.texture_index && (a.texture_index > scene->TextureCount || !tex_ok(a.texture_index - 1)))
                 return SetError(AZ_ERR_INVALID_SCENE, "triangle texture index out of range or texture not loaded");
+    for (const IngestMesh &m : ingest)
+        if (m.texture_index && (m.texture_index > scene->TextureCount || !tex_ok(m.texture_index - 1)))
+            return SetError(AZ_ERR_INVALID_SCENE, "mesh texture index out of range or texture not loaded");
     for (const azd::DevEntity &e : F.ents) {
         if (!e.is_emitter && e.material >= scene->MaterialCount)
             return SetError(AZ_ERR_INVALID_SCENE, "entity material index out of range");
@@ -467,6 +529,23 @@ int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_
                 memcpy(d.center, &E.Center, 12);
                 d.radius = E.Radius;
                 light_draws += 2;
+            } else if (E.Type == AZ_Entity_MeshInstance && soup) {
+                // the mesh's triangles and TotalArea from the GPU post-processing
+                if (E.BaseMeshID >= soup->mesh_count)
+                    return SetError(AZ_ERR_INVALID_SCENE, "entity light's BaseMeshID is not a mesh of the soup");
+                const az_mesh_desc &md = soup->meshes[E.BaseMeshID];
+                std::vector<az_triangle> tr(md.face_count);
+                int r = SoupTriangles(*soupw, md.face_base, md.face_count, tr.data(), st);
+                if (r != AZ_OK) return r;
+                d.entity_type = azd::ENT_INSTANCE;
+                d.tri_offset = (uint32_t)light_tris.size();
+                d.tri_count = md.face_count;
+                d.total_area = soup_area[E.BaseMeshID];
+                for (const az_triangle &T : tr)
+                    light_tris.push_back(azd::DevLightTri{make_float4(T.P0.x, T.P0.y, T.P0.z, T.N.x),
+                                                          make_float4(T.P1.x, T.P1.y, T.P1.z, T.N.y),
+                                                          make_float4(T.P2.x, T.P2.y, T.P2.z, T.N.z)});
+                light_draws += 3;
             } else if (E.Type == AZ_Entity_MeshInstance && E.Mesh && E.Mesh->Triangles && E.Mesh->TriangleCount) {
                 d.entity_type = azd::ENT_INSTANCE;
                 d.tri_offset = (uint32_t)light_tris.size();
@@ -491,19 +570,18 @@ int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_
     // ---- upload primitives, build BLAS per group and the TLAS ----
     int rc = AZ_OK;
     uint64_t total_tris = 0;
-    for (auto &g : F.groups) total_tris += g.tris.size();
+    for (auto &g : F.groups) total_tris += g.tris.size() + g.soup_tris;
     if (total_tris >= (1ull << 27)) return SetError(AZ_ERR_UNSUPPORTED, "more than 2^27 triangles");
-    std::vector<azd::DevTri> all_tris;
-    std::vector<azd::DevTriAttr> all_attr;
-    all_tris.reserve(total_tris);
-    all_attr.reserve(total_tris);
+    // per group: the flattened triangles, then those of its soup meshes
+    uint32_t cursor = 0;
     for (auto &g : F.groups) {
-        g.g.tri_begin = (uint32_t)all_tris.size();
-        all_tris.insert(all_tris.end(), g.tris.begin(), g.tris.end());
-        all_attr.insert(all_attr.end(), g.attr.begin(), g.attr.end());
-        g.g.tri_end = (uint32_t)all_tris.size();
-        std::vector<azd::DevTri>().swap(g.tris);
-        std::vector<azd::DevTriAttr>().swap(g.attr);
+        g.g.tri_begin = cursor;
+        cursor += (uint32_t)g.tris.size();
+        for (uint32_t m : g.soup_meshes) {
+            ingest[m].out_base = cursor;
+            cursor += soup->meshes[m].face_count;
+        }
+        g.g.tri_end = cursor;
     }
     // TLAS primitives: spheres and groups
     std::vector<uint32_t> tlas;
@@ -530,10 +608,11 @@ int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_
     }
     node_total += tlas.size() > 1 ? (uint32_t)tlas.size() - 1 : (uint32_t)tlas.size();
 
-    G->flatten_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+    G->flatten_ms =
+        std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t_start).count() - G->ingest_ms;
     // Build-only buffers are freed when the build ends; the scene keeps the
     // sorted primitives, the wide nodes and the top-level primitive list.
-    const size_t nmax = std::max(all_tris.size(), tlas.size()) + 1;
+    const size_t nmax = std::max((size_t)total_tris, tlas.size()) + 1;
     TempBuf<azd::DevTri> d_tris_unsorted;
     TempBuf<azd::DevTriAttr> d_attr_unsorted;
     TempBuf<azd::BVHNode> d_nodes;
@@ -541,25 +620,35 @@ int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_
     TempBuf<float4> d_lo, d_hi;
     TempBuf<uint32_t> d_perm, d_comp, d_tlas_unsorted;
     TempBuf<azd::WideNode> d_wide_tmp;
-    azd::DevTri *d_tris = (azd::DevTri *)G->Alloc(all_tris.size() * sizeof(azd::DevTri));
-    azd::DevTriAttr *d_attr = (azd::DevTriAttr *)G->Alloc(all_attr.size() * sizeof(azd::DevTriAttr));
+    azd::DevTri *d_tris = (azd::DevTri *)G->Alloc(total_tris * sizeof(azd::DevTri));
+    azd::DevTriAttr *d_attr = (azd::DevTriAttr *)G->Alloc(total_tris * sizeof(azd::DevTriAttr));
     uint32_t *d_tlas = (uint32_t *)G->Alloc((tlas.size() + 1) * sizeof(uint32_t));
-    if (!d_tris || !d_attr || !d_tlas || d_tris_unsorted.alloc(all_tris.size()) ||
-        d_attr_unsorted.alloc(all_attr.size()) || d_nodes.alloc(node_total) || d_range.alloc(node_total) ||
+    if (!d_tris || !d_attr || !d_tlas || d_tris_unsorted.alloc(total_tris) ||
+        d_attr_unsorted.alloc(total_tris) || d_nodes.alloc(node_total) || d_range.alloc(node_total) ||
         d_lo.alloc(nmax) || d_hi.alloc(nmax) || d_perm.alloc(nmax) || d_comp.alloc(nmax) ||
         d_tlas_unsorted.alloc(tlas.size() + 1) || d_wide_tmp.alloc(node_total))
         return SetError(AZ_ERR_OUT_OF_MEMORY, "device allocation failed");
     const auto t_up0 = std::chrono::steady_clock::now();
-    if (!all_tris.empty()) {
-        AZ_CUDA_TRY(cudaMemcpyAsync(d_tris_unsorted.p, all_tris.data(), all_tris.size() * sizeof(azd::DevTri),
+    for (auto &g : F.groups) {
+        if (g.tris.empty()) continue;
+        AZ_CUDA_TRY(cudaMemcpyAsync(d_tris_unsorted.p + g.g.tri_begin, g.tris.data(), g.tris.size() * sizeof(azd::DevTri),
                                     cudaMemcpyHostToDevice, st));
-        AZ_CUDA_TRY(cudaMemcpyAsync(d_attr_unsorted.p, all_attr.data(), all_attr.size() * sizeof(azd::DevTriAttr),
-                                    cudaMemcpyHostToDevice, st));
+        AZ_CUDA_TRY(cudaMemcpyAsync(d_attr_unsorted.p + g.g.tri_begin, g.attr.data(),
+                                    g.attr.size() * sizeof(azd::DevTriAttr), cudaMemcpyHostToDevice, st));
+    }
+    if (soupw) {
+        int r = SoupEmitScene(*soupw, ingest, d_tris_unsorted.p, d_attr_unsorted.p, st);
+        if (r != AZ_OK) return r;
+        soupw.reset();   // its device arrays are no longer needed
     }
     if (!tlas.empty())
         AZ_CUDA_TRY(cudaMemcpyAsync(d_tlas_unsorted.p, tlas.data(), tlas.size() * sizeof(uint32_t),
                                     cudaMemcpyHostToDevice, st));
     AZ_CUDA_TRY(cudaStreamSynchronize(st));
+    for (auto &g : F.groups) {
+        std::vector<azd::DevTri>().swap(g.tris);
+        std::vector<azd::DevTriAttr>().swap(g.attr);
+    }
     const auto t_up1 = std::chrono::steady_clock::now();
     G->upload_ms += std::chrono::duration<float, std::milli>(t_up1 - t_up0).count();
     // Per hierarchy on the GPU: LBVH, collapse to wide nodes, then the

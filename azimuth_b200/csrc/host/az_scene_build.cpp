@@ -292,11 +292,14 @@ struct SceneBuilder::Storage {
     std::vector<std::unique_ptr<az_entity[]>> TriEntities;
     std::vector<std::unique_ptr<az_triangle[]>> Triangles;
     std::unique_ptr<az_entity[]> Entities;
+    std::unique_ptr<az_entity[]> RootEntities;   // soup-only scenes: the entities other than mesh instances
+    std::vector<az_vec3u> SoupFaces;
+    std::vector<az_mesh_desc> SoupDescs;
     std::vector<std::unique_ptr<uint8_t[]>> Texels;
     EntityPool Pool;
 };
 
-SceneBuilder::SceneBuilder() : Scene(DefaultScene()), S(new Storage) {}
+SceneBuilder::SceneBuilder() : Scene(DefaultScene()), S(new Storage) { memset(&Soup, 0, sizeof(Soup)); }
 SceneBuilder::~SceneBuilder() = default;
 
 uint32_t SceneBuilder::AddVertex(az_vec3 P) {
@@ -335,7 +338,7 @@ void *SceneBuilder::AllocTexels(size_t Bytes) {
     return S->Texels.back().get();
 }
 
-bool SceneBuilder::Finalize() {
+bool SceneBuilder::Finalize(bool soup_only) {
     Storage &St = *S;
     // Entities in importer order: parsed objects first (spheres here), mesh
     // instances appended while meshes are processed (src/azimuth_xml.cpp:3753-3776).
@@ -344,9 +347,42 @@ bool SceneBuilder::Finalize() {
     for (size_t i = 0; i < St.Spheres.size(); i++)
         if (St.SphereIsLight[i]) EntityLightIdx.push_back((uint32_t)i);
 
+    // The importer's shared arrays before its post-processing: faces of all
+    // meshes in mesh order, each mesh a range of them
+    St.SoupFaces.clear();
+    St.SoupDescs.clear();
+    for (size_t mi = 0; mi < St.MeshDescs.size(); mi++) {
+        const MeshDesc &D = St.MeshDescs[mi];
+        az_mesh_desc d;
+        memset(&d, 0, sizeof(d));
+        d.face_base = (uint32_t)St.SoupFaces.size();
+        d.face_count = (uint32_t)D.Faces.size();
+        d.uv_offset = D.UVOffset;
+        d.shading_mode = D.ShadingMode;
+        d.material_index = D.MaterialIndex;
+        d.texture_index = D.TextureIndex;
+        d.is_emitter = D.IsEmitter ? 1u : 0u;
+        d.unique_entity_id = (uint32_t)(St.Spheres.size() + mi);
+        d.motion = D.Motion;
+        d.radiance = D.Radiance;
+        d.transform = D.Transform;
+        d.inv_transform = D.InvTransform;
+        St.SoupFaces.insert(St.SoupFaces.end(), D.Faces.begin(), D.Faces.end());
+        St.SoupDescs.push_back(d);
+    }
+    Soup.vertices = Vertices.empty() ? nullptr : Vertices.data();
+    Soup.faces = St.SoupFaces.empty() ? nullptr : St.SoupFaces.data();
+    Soup.uvs = UVs.empty() ? nullptr : UVs.data();
+    Soup.meshes = St.SoupDescs.empty() ? nullptr : St.SoupDescs.data();
+    Soup.vertex_count = (uint32_t)Vertices.size();
+    Soup.face_count = (uint32_t)St.SoupFaces.size();
+    Soup.uv_count = (uint32_t)UVs.size();
+    Soup.mesh_count = (uint32_t)St.SoupDescs.size();
+
     // Per-vertex normals: normalised sum of unnormalised face normals over every
     // face that uses the vertex (src/azimuth_xml.cpp:3632-3667).
-    std::vector<az_vec3> VN(Vertices.size(), V3(0, 0, 0));
+    std::vector<az_vec3> VN(soup_only ? 0 : Vertices.size(), V3(0, 0, 0));
+    if (!soup_only)
     for (const MeshDesc &M : St.MeshDescs)
         for (const az_vec3u &F : M.Faces) {
             az_vec3 P0 = Vertices[F.x], P1 = Vertices[F.y], P2 = Vertices[F.z];
@@ -374,6 +410,21 @@ bool SceneBuilder::Finalize() {
         Mesh.UVOffset = D.UVOffset;
         Mesh.ID = (uint32_t)mi + 1;
         Mesh.ShadingMode = D.ShadingMode;
+        Mesh.TriangleCount = FaceCount;
+        if (soup_only) {
+            az_entity Inst = DefaultEntity();
+            Inst.BaseMeshID = (uint32_t)mi;
+            Inst.ResetTransform = 0;
+            Inst.MotionVector = D.Motion;
+            Inst.Radiance = D.Radiance;
+            Inst.IsEmitter = Mesh.IsEmitter;
+            Inst.TextureIndex = D.TextureIndex;
+            Inst.MaterialIndex = D.MaterialIndex;
+            Inst.Type = AZ_Entity_MeshInstance;
+            Ents.push_back(Inst);
+            if (D.IsLight) EntityLightIdx.push_back((uint32_t)Ents.size() - 1);
+            continue;
+        }
 
         // Triangle entities and the `triangle` array (src/azimuth_xml.cpp:3669-3750).
         // The face index is stamped into the (otherwise unused) entity ID.
@@ -430,11 +481,12 @@ bool SceneBuilder::Finalize() {
     for (az_entity &E : Ents) {
         if (E.Type != AZ_Entity_MeshInstance) continue;
         E.Mesh = &St.Meshes[E.BaseMeshID];
-        E.AABB = E.Mesh->BVH->AABB;  // a 1-triangle mesh reads the triangle's bytes here
         if (!E.ResetTransform) {
             E.TransformationMatrix = Mat4Mul(E.TransformationMatrix, E.Mesh->TransformationMatrix);
             E.InvTransformationMatrix = Mat4Mul(E.Mesh->InvTransformationMatrix, E.InvTransformationMatrix);
         }
+        if (soup_only) continue;   // no mesh BVH to bound
+        E.AABB = E.Mesh->BVH->AABB;  // a 1-triangle mesh reads the triangle's bytes here
         const az_aabb A = E.AABB;
         const az_vec3 Corners[8] = {
             V3(A.Min.x, A.Min.y, A.Min.z), V3(A.Min.x, A.Min.y, A.Max.z), V3(A.Min.x, A.Max.y, A.Min.z),
@@ -483,6 +535,14 @@ bool SceneBuilder::Finalize() {
     Scene.LightCount = (uint32_t)St.Lights.size();
     Scene.Textures = St.Textures.empty() ? nullptr : St.Textures.data();
     Scene.TextureCount = (uint32_t)St.Textures.size();
+    if (soup_only) {
+        uint32_t n = 0;
+        St.RootEntities.reset(new az_entity[EntityCount]);
+        for (uint32_t i = 0; i < EntityCount; i++)
+            if (St.Entities[i].Type != AZ_Entity_MeshInstance) St.RootEntities[n++] = St.Entities[i];
+        Scene.BVHRoot = nullptr;
+        return n == 0 || ConstructBVH(&Scene.BVHRoot, St.RootEntities.get(), n, 0, St.Pool);
+    }
     return ConstructBVH(&Scene.BVHRoot, St.Entities.get(), EntityCount, 0, St.Pool);
 }
 

@@ -13,7 +13,7 @@
 #include <memory>
 #include <vector>
 
-#include "az_abi.h"
+#include "azimuth_gpu.h"
 
 namespace az {
 
@@ -63,10 +63,13 @@ public:
     void *AllocTexels(size_t Bytes);
 
     // Runs the importer's post-processing and both BVH builds.  Returns false
-    // on an empty mesh or a failed allocation.
-    bool Finalize();
+    // on an empty mesh or a failed allocation.  With `soup_only` the meshes
+    // are left as the importer holds them before its post-processing (no
+    // triangles, areas or mesh BVHs; BVHRoot over the other entities only).
+    bool Finalize(bool soup_only = false);
 
     az_scene Scene;                  // valid after Finalize()
+    az_mesh_soup Soup;               // the meshes before post-processing, valid after Finalize()
     std::vector<az_vec3> Vertices;
     std::vector<az_vec2> UVs;
 

@@ -793,7 +793,7 @@ extern "C" int az_scene_generate(int32_t scene_id, uint64_t seed, const az_gen_p
         case AZ_SCENE_ENV_SPHERES: ok = GenEnvSpheres(*G, p, seed); break;
         default: delete G; return 1;
     }
-    if (!ok || !G->B.Finalize()) {
+    if (!ok || !G->B.Finalize((p.flags & AZ_GEN_SOUP_ONLY) != 0)) {
         delete G;
         return 2;
     }
@@ -806,6 +806,7 @@ extern "C" int az_scene_generate(int32_t scene_id, uint64_t seed, const az_gen_p
     out->triangle_count = G->Triangles;
     out->sphere_count = G->Spheres;
     out->owner = G;
+    out->soup = &G->B.Soup;
     return 0;
 }
 

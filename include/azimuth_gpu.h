@@ -108,14 +108,69 @@ typedef struct az_scene_info {
     uint32_t bvh_width, bvh_leaf;
     uint32_t bvh_depth;          /* deepest wide-node level (root = 0) */
     uint32_t hierarchies;        /* bottom-level hierarchies plus the top level */
-    float flatten_ms;            /* host: azimuth's entity trees walked into device records */
+    float flatten_ms;            /* host: azimuth's entity trees walked into device records (and the
+                                    lights, materials and textures) */
     float upload_ms;             /* host-to-device copies of the primitives */
     float bvh_ms;                /* GPU: LBVH builds, wide collapse and primitive gather */
     float total_ms;              /* the whole az_gpu_scene_create call */
-    uint32_t reserved[4];
+    float ingest_ms;             /* GPU post-processing of a mesh soup (az_gpu_scene_create_from_meshes) */
+    uint32_t reserved[3];
 } az_scene_info;
 
 int az_gpu_scene_info(const az_gpu_scene *scene, az_scene_info *out);
+
+/* ---- Scene ingestion on the GPU ----
+ * azimuth's importer collects every mesh's vertices, faces and UVs into shared
+ * arrays, then post-processes them on the host (src/azimuth_xml.cpp:3632-3776:
+ * per-vertex normals as the normalised sum of the unnormalised normals of the
+ * faces using the vertex, in face order; face normals; TotalArea; UVs through
+ * UVOffset) and builds a 288-byte entity BVH per mesh.  The two calls below
+ * take those arrays as they are before the post-processing and do it on the
+ * GPU with the same float arithmetic (per-vertex sums in face order, so the
+ * results are bit for bit azimuth's). */
+typedef struct az_mesh_desc {
+    uint32_t face_base, face_count;   /* the mesh's faces: faces[face_base, face_base + face_count) */
+    int32_t uv_offset;                /* Mesh->UVOffset: vertex i's UV is uvs[i + uv_offset] when in range */
+    uint32_t shading_mode;            /* AZ_Shading_* */
+    uint32_t material_index, texture_index;
+    uint32_t is_emitter;
+    uint32_t unique_entity_id;        /* UniqueEntityID of the mesh's instance entity */
+    az_vec3 motion, radiance;
+    az_mat4 transform, inv_transform; /* Mesh->TransformationMatrix / InvTransformationMatrix */
+} az_mesh_desc;
+
+typedef struct az_mesh_soup {
+    const az_vec3 *vertices;          /* host arrays */
+    const az_vec3u *faces;            /* vertex indices */
+    const az_vec2 *uvs;               /* may be NULL when uv_count is 0 */
+    const az_mesh_desc *meshes;       /* face ranges must not overlap */
+    uint32_t vertex_count, face_count, uv_count, mesh_count;
+} az_mesh_soup;
+
+/* Per-face shading data of the importer's triangle entities (entity.N0-N2, UV0-UV2). */
+typedef struct az_face_attr {
+    az_vec3 N0, N1, N2;
+    az_vec2 UV0, UV1, UV2;
+} az_face_attr;
+
+/* The importer's mesh post-processing on the GPU, results copied to the HOST
+ * arrays given (any may be NULL): vertex_normals[vertex_count], triangles
+ * and attrs[face_count] (azimuth's triangle {P0, P1, P2, unit face normal}
+ * and the entity fields, for every face; a face outside every mesh gets UVs
+ * 0), total_area[mesh_count] (Mesh->TotalArea: the float sum of |N|/2 over the
+ * mesh's faces in order).  Synchronous. */
+int az_gpu_mesh_postprocess(const az_mesh_soup *soup, az_vec3 *vertex_normals, az_triangle *triangles,
+                            az_face_attr *attrs, float *total_area, const az_render_opts *opts);
+
+/* az_gpu_scene_create for a scene whose meshes come as `soup`: the meshes are
+ * post-processed on the GPU and go straight into the device scene, with no
+ * host triangles or entity BVHs.  Everything else comes from `scene`:
+ * materials, textures, lights, environment and settings, and the other
+ * entities found under scene->BVHRoot (mesh instances there are ignored;
+ * BVHRoot may be NULL).  An entity light whose entity is a mesh instance
+ * takes its triangles and area from soup mesh Entity.BaseMeshID. */
+int az_gpu_scene_create_from_meshes(const az_scene *scene, const az_mesh_soup *soup, const az_render_opts *opts,
+                                    az_gpu_scene **out);
 
 /* ProduceImageInLinearSpace (src/azimuth_main.cpp:1256-1263) on the GPU:
  * accumulates every camera sample of the scissor rectangle into the HOST film

@@ -12,7 +12,7 @@
 #ifndef AZIMUTH_SCENES_H
 #define AZIMUTH_SCENES_H
 
-#include "az_abi.h"
+#include "azimuth_gpu.h"
 
 #ifdef __cplusplus
 extern "C" {
@@ -37,7 +37,16 @@ typedef struct az_gen_params {
     int32_t  filter;             /* -1 = default, else AZ_Filter_* */
     int32_t  importance_sampling;/* -1 = default, 0 = uniform hemisphere, 1 = cosine */
     uint32_t env_width, env_height; /* environment map size; 0 = default */
+    uint32_t flags;              /* AZ_GEN_* */
 } az_gen_params;
+
+enum {
+    /* Leave the meshes as the importer has them before its post-processing:
+     * no triangles, areas or entity BVHs (BVHRoot holds the other entities
+     * only); az_generated_scene.soup is then the only copy of the geometry,
+     * for az_gpu_scene_create_from_meshes. */
+    AZ_GEN_SOUP_ONLY = 1
+};
 
 typedef struct az_generated_scene {
     az_scene *scene;
@@ -49,6 +58,7 @@ typedef struct az_generated_scene {
     uint64_t triangle_count;
     uint64_t sphere_count;
     void *owner;                 /* internal */
+    const az_mesh_soup *soup;    /* the meshes before post-processing (vertices, faces, UVs, descriptions) */
 } az_generated_scene;
 
 /* Returns 0 on success. `params` may be NULL. */
