@@ -147,9 +147,13 @@ def full_scissor(scene):
     return Scissor(Vec2u(w, h), Vec2u(0, 0))
 
 
+BVH_LBVH, BVH_PLOC = 1, 2   # az_render_opts.bvh_builder
+
+
 def make_opts(scene=None, seed=0, stream=None, device=0, flags=0, chunk_samples=0, block_size=0, variant=0,
-              bvh_width=0, bvh_leaf=0):
+              bvh_width=0, bvh_leaf=0, bvh_builder=0):
     o = RenderOpts()
+    o.bvh_builder = bvh_builder
     o.variant = variant
     o.bvh_width = bvh_width
     o.bvh_leaf = bvh_leaf
@@ -180,13 +184,13 @@ def produce_image(scene, pixels=None, scissor=None, filter_type=None, backface_c
 class GpuScene:
     """A device-resident scene (az_gpu_scene_create / az_gpu_scene_destroy)."""
 
-    def __init__(self, scene, device=0, bvh_width=0, bvh_leaf=0, from_soup=False):
+    def __init__(self, scene, device=0, bvh_width=0, bvh_leaf=0, from_soup=False, bvh_builder=0):
         """from_soup: build through az_gpu_scene_create_from_meshes from the scene's mesh soup (the meshes
         post-processed on the GPU) instead of azimuth's finished structs."""
         self.scene = scene
         self.device = device
         self._h = C.c_void_p()
-        o = make_opts(scene, device=device, bvh_width=bvh_width, bvh_leaf=bvh_leaf)
+        o = make_opts(scene, device=device, bvh_width=bvh_width, bvh_leaf=bvh_leaf, bvh_builder=bvh_builder)
         if from_soup:
             _check(lib().az_gpu_scene_create_from_meshes(scene.scene_ptr, scene.soup_ptr, C.byref(o),
                                                          C.byref(self._h)), "az_gpu_scene_create_from_meshes")

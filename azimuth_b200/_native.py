@@ -46,7 +46,7 @@ class RenderOpts(C.Structure):
     _fields_ = [("seed", C.c_uint64), ("perlin_gradients", C.c_void_p), ("stream", C.c_void_p),
                 ("device", C.c_int32), ("flags", C.c_uint32), ("chunk_samples", C.c_uint32),
                 ("bvh_width", C.c_uint32), ("block_size", C.c_uint32), ("variant", C.c_uint32),
-                ("bvh_leaf", C.c_uint32), ("reserved", C.c_uint32 * 3)]
+                ("bvh_leaf", C.c_uint32), ("bvh_builder", C.c_uint32), ("reserved", C.c_uint32 * 2)]
 
 
 class Tonemap(C.Structure):
@@ -89,7 +89,7 @@ class SceneInfo(C.Structure):
                 ("device_bytes", C.c_uint64), ("bvh_width", C.c_uint32), ("bvh_leaf", C.c_uint32),
                 ("bvh_depth", C.c_uint32), ("hierarchies", C.c_uint32), ("flatten_ms", C.c_float),
                 ("upload_ms", C.c_float), ("bvh_ms", C.c_float), ("total_ms", C.c_float),
-                ("ingest_ms", C.c_float), ("reserved", C.c_uint32 * 3)]
+                ("ingest_ms", C.c_float), ("bvh_builder", C.c_uint32), ("reserved", C.c_uint32 * 2)]
 
 
 class MeshDesc(C.Structure):

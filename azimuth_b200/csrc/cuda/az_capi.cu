@@ -157,6 +157,7 @@ extern "C" int az_gpu_scene_info(const az_gpu_scene *scene, az_scene_info *out) 
     out->bvh_ms = G.bvh_ms;
     out->total_ms = G.total_ms;
     out->ingest_ms = G.ingest_ms;
+    out->bvh_builder = G.bvh_builder;
     return AZ_OK;
 }
 
@@ -260,6 +261,10 @@ extern "C" int az_gpu_autotune_scene(const az_scene *host_scene, az_gpu_scene *s
     if (opts) o = *opts;
     else memset(&o, 0, sizeof(o));
     o.device = scene->impl->device;
+    o.bvh_builder = scene->impl->bvh_builder;
+    if (scene->impl->from_soup)
+        return SetError(AZ_ERR_UNSUPPORTED, "a scene built from a mesh soup cannot be rebuilt from host_scene; "
+                                            "use az_gpu_autotune or create it with the shape wanted");
     GpuScene *best = nullptr;
     uint32_t best_v = 0;
     float best_ms = FLT_MAX;

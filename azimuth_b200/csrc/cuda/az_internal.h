@@ -45,6 +45,8 @@ struct GpuScene {
     float ingest_ms = 0.0f;      // GPU post-processing of a mesh soup (az_gpu_scene_create_from_meshes)
     uint32_t bvh_width = 8;      // children per wide node (2, 4 or 8)
     uint32_t bvh_leaf = 2;       // triangles per bottom-level leaf at most
+    uint32_t bvh_builder = AZ_BVH_PLOC;   // binary hierarchy under the wide collapse
+    bool from_soup = false;      // meshes came from az_gpu_scene_create_from_meshes
     size_t device_bytes = 0;
     WaveBuffers waves;           // reused across render calls on this scene
     uint32_t variant = 7;        // traversal launch configuration, 0-based (128 threads, 8 blocks/SM,
@@ -84,6 +86,10 @@ int SoupEmitScene(const SoupWork &w, const std::vector<IngestMesh> &meshes, azd:
 // child references are `leaf_base + sorted position`.  Returns the root node
 // index.
 int BuildLBVH(const float4 *d_lo, const float4 *d_hi, uint32_t n, azd::BVHNode *d_nodes, uint2 *d_range,
+              uint32_t node_base, uint32_t leaf_base, uint32_t *d_perm, cudaStream_t stream, uint32_t *root_out);
+// The same outputs from PLOC clustering (az_bvh_build.cu); primitive order is
+// then the tree's depth-first leaf order, so every node's range is contiguous.
+int BuildPLOC(const float4 *d_lo, const float4 *d_hi, uint32_t n, azd::BVHNode *d_nodes, uint2 *d_range,
               uint32_t node_base, uint32_t leaf_base, uint32_t *d_perm, cudaStream_t stream, uint32_t *root_out);
 
 // Collapse, on the GPU, of the binary LBVH of `n` primitives rooted at

@@ -378,9 +378,15 @@ int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_
     const uint32_t leaf = opts && opts->bvh_leaf ? opts->bvh_leaf : 2u;
     if (leaf < 1 || leaf > 3) return SetError(AZ_ERR_INVALID_ARGUMENT, "bvh_leaf must be 0..3");
     G->bvh_leaf = leaf;
+    const uint32_t builder = opts && opts->bvh_builder ? opts->bvh_builder : (uint32_t)AZ_BVH_PLOC;
+    if (builder != AZ_BVH_LBVH && builder != AZ_BVH_PLOC)
+        return SetError(AZ_ERR_INVALID_ARGUMENT, "bvh_builder must be 0, AZ_BVH_LBVH or AZ_BVH_PLOC");
+    G->bvh_builder = builder;
+    auto build_binary = builder == AZ_BVH_PLOC ? BuildPLOC : BuildLBVH;
     Flattener F;
     F.s = scene;
     F.skip_meshes = soup != nullptr;
+    G->from_soup = soup != nullptr;
     if (!scene->BVHRoot && !soup) return SetError(AZ_ERR_INVALID_SCENE, "scene has no BVHRoot");
     if (!F.Run()) return SetError(AZ_ERR_INVALID_SCENE, F.err);
 
@@ -664,7 +670,7 @@ int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_
         k_tri_boxes<<<(n + B - 1) / B, B, 0, st>>>(d_tris_unsorted.p + g.g.tri_begin, n, d_lo.p, d_hi.p);
         AZ_CUDA_TRY(cudaGetLastError());
         uint32_t root, wroot, depth = 0;
-        rc = BuildLBVH(d_lo.p, d_hi.p, n, d_nodes.p, d_range.p, node_base, g.g.tri_begin, d_perm.p, st, &root);
+        rc = build_binary(d_lo.p, d_hi.p, n, d_nodes.p, d_range.p, node_base, g.g.tri_begin, d_perm.p, st, &root);
         if (rc != AZ_OK) return rc;
         rc = CollapseToWide(d_nodes.p, d_range.p, root, n, g.g.tri_begin, d_perm.p, leaf, width, d_wide_tmp.p,
                             node_total, &wide_count, d_comp.p, st, &wroot, &depth);
@@ -684,7 +690,7 @@ int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_
         AZ_CUDA_TRY(cudaMemcpyAsync(d_lo.p, tlo.data(), tlo.size() * sizeof(float4), cudaMemcpyHostToDevice, st));
         AZ_CUDA_TRY(cudaMemcpyAsync(d_hi.p, thi.data(), thi.size() * sizeof(float4), cudaMemcpyHostToDevice, st));
         uint32_t root, depth = 0;
-        rc = BuildLBVH(d_lo.p, d_hi.p, n, d_nodes.p, d_range.p, node_base, 0, d_perm.p, st, &root);
+        rc = build_binary(d_lo.p, d_hi.p, n, d_nodes.p, d_range.p, node_base, 0, d_perm.p, st, &root);
         if (rc != AZ_OK) return rc;
         // top-level leaves hold one primitive each (a group is entered from its leaf)
         rc = CollapseToWide(d_nodes.p, d_range.p, root, n, 0, d_perm.p, 1, width, d_wide_tmp.p, node_total,

@@ -70,8 +70,15 @@ typedef struct az_render_opts {
                                        fetching); 0 = the scene's choice: 8 (128 threads, at most 64
                                        registers, persistent fetching) until az_gpu_autotune picks another */
     uint32_t bvh_leaf;              /* az_gpu_scene_create: triangles per bottom-level leaf at most, 1..3 (0 = 2) */
-    uint32_t reserved[3];
+    uint32_t bvh_builder;           /* az_gpu_scene_create: binary hierarchy before the wide collapse,
+                                       AZ_BVH_LBVH or AZ_BVH_PLOC (0 = the default, AZ_BVH_PLOC) */
+    uint32_t reserved[2];
 } az_render_opts;
+
+enum {
+    AZ_BVH_LBVH = 1,   /* Morton-order radix tree (Karras 2012): fastest build */
+    AZ_BVH_PLOC = 2    /* locally-ordered clustering (Meister, Bittner 2018): fewer nodes visited per ray */
+};
 
 typedef struct az_render_stats {
     uint64_t samples;               /* camera samples rendered */
@@ -114,7 +121,8 @@ typedef struct az_scene_info {
     float bvh_ms;                /* GPU: LBVH builds, wide collapse and primitive gather */
     float total_ms;              /* the whole az_gpu_scene_create call */
     float ingest_ms;             /* GPU post-processing of a mesh soup (az_gpu_scene_create_from_meshes) */
-    uint32_t reserved[3];
+    uint32_t bvh_builder;        /* AZ_BVH_LBVH or AZ_BVH_PLOC */
+    uint32_t reserved[2];
 } az_scene_info;
 
 int az_gpu_scene_info(const az_gpu_scene *scene, az_scene_info *out);
@@ -206,8 +214,10 @@ int az_gpu_autotune(az_gpu_scene *scene, const az_camera *camera, const az_epsil
  * hierarchy of `host_scene` (the scene `scene` was created from) with 8, 4 and
  * 2 children per node and 1 to 3 triangles per bottom-level leaf, runs
  * az_gpu_autotune on each and keeps the fastest build (and its launch
- * configuration) in `scene`.  Writes the width, the variant (1-based) and its
- * time in ms.  Synchronous; `scene` must not be rendering meanwhile. */
+ * configuration) in `scene`; the binary builder stays the scene's.  Writes the
+ * width, the variant (1-based) and its time in ms.  Synchronous; `scene` must
+ * not be rendering meanwhile.  A scene made by az_gpu_scene_create_from_meshes
+ * has no host_scene to rebuild from: AZ_ERR_UNSUPPORTED. */
 int az_gpu_autotune_scene(const az_scene *host_scene, az_gpu_scene *scene, const az_camera *camera,
                           const az_epsilon_values *epsilons, az_scissor scissor, int32_t filter_type,
                           uint32_t backface_culling, const az_render_opts *opts, uint32_t *width_out,

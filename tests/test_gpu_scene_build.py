@@ -72,3 +72,32 @@ def test_two_builds_give_identical_hits(gpu, scene_id):
         assert outs[0][1].any()   # the rays do hit something
     finally:
         sc.close()
+
+
+@pytest.mark.parametrize("scene_id", [az.SCENE_DENSE_MESH, az.SCENE_MOTION_ENV])
+def test_ploc_and_lbvh_find_the_same_hits(gpu, scene_id):
+    kw = {"detail": 5} if scene_id == az.SCENE_DENSE_MESH else {}
+    sc = az.generate_scene(scene_id, seed=5, width=32, height=32, spp=1, **kw)
+    try:
+        span = (0.0, 10.0) if scene_id == az.SCENE_MOTION_ENV else (-1.0, 1.0)
+        rays = _rays(1 << 15, seed=11, lo=span[0], hi=span[1])
+        with az.GpuScene(sc, bvh_builder=az.BVH_LBVH) as a, az.GpuScene(sc, bvh_builder=az.BVH_PLOC) as b:
+            assert a.info()["bvh_builder"] == az.BVH_LBVH and b.info()["bvh_builder"] == az.BVH_PLOC
+            ha, hb = a.closest_hit(rays), b.closest_hit(rays)
+        same = (ha[0] == hb[0]) & (ha[1] == hb[1]) & (ha[2] == hb[2]) & (ha[3] == hb[3])
+        assert same.mean() >= 0.999
+        assert np.array_equal(ha[3][~same], hb[3][~same])   # exact-distance ties only
+    finally:
+        sc.close()
+
+
+def test_ploc_visits_fewer_nodes(gpu, dense):
+    import torch
+    w, h = dense.resolution()
+    film = torch.zeros((h, w, 4), device="cuda")
+    visits = {}
+    for builder in (az.BVH_LBVH, az.BVH_PLOC):
+        with az.GpuScene(dense, bvh_builder=builder) as g:
+            st = g.render_device(film.data_ptr(), seed=1, stats=True, flags=az.FLAG_COUNT_TRAVERSAL)
+            visits[builder] = (st["node_visits"] + st["prim_visits"]) / (st["extend_rays"] + st["shadow_rays"])
+    assert visits[az.BVH_PLOC] < visits[az.BVH_LBVH]
