@@ -71,9 +71,7 @@ __device__ __forceinline__ uint32_t push_slot(uint32_t *counter) {
 
 __device__ __forceinline__ void add_accum(float4 *accum, uint32_t slot, f3 v) {
     if (is_zero(v)) return;
-    atomicAdd(&accum[slot].x, v.x);
-    atomicAdd(&accum[slot].y, v.y);
-    atomicAdd(&accum[slot].z, v.z);
+    atomicAdd(&accum[slot], make_float4(v.x, v.y, v.z, 0.0f));   // one vector atomic (sm_90 and later)
 }
 
 __device__ __forceinline__ void push_path(const WaveQueues &Q, int buf, uint32_t level, f3 o, float time, f3 d,
@@ -210,7 +208,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_extend(DevScene S, CameraParams
                 r.o = mk(o.x, o.y, o.z);
                 r.d = mk(d.x, d.y, d.z);
                 r.time = o.w;
-                T.init(S, r, cam.cull != 0, cam.eps_isect, FLT_MAX);
+                T.init(S, r, cam.cull != 0, cam.eps_isect, FLT_MAX, stack);
             }
             while (__any_sync(0xFFFFFFFFu, live)) {
                 if (live && T.step(S, stack, err)) {
@@ -249,7 +247,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_extend(DevScene S, CameraParams
             r.o = mk(o.x, o.y, o.z);
             r.d = mk(d.x, d.y, d.z);
             r.time = o.w;
-            T.init(S, r, cam.cull != 0, cam.eps_isect, FLT_MAX);
+            T.init(S, r, cam.cull != 0, cam.eps_isect, FLT_MAX, stack);
         }
         if (__all_sync(0xFFFFFFFFu, idx == kLaneDone)) break;
         if (idx < n && T.step(S, stack, err)) {
@@ -621,9 +619,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_shadow(DevScene S, CameraParams
                     const DevLight &L = S.lights[li];
                     float tl = FLT_MAX;
                     const int lh = light_entity_hit(S, L, r, tl);
-                    T.init(S, r, false, 0.0f, lh ? tl : FLT_MAX, L.ent_index);
+                    T.init(S, r, false, 0.0f, lh ? tl : FLT_MAX, stack, L.ent_index);
                 } else {
-                    T.init(S, r, false, 0.0f, kind == SHADOW_ANY ? FLT_MAX : d.w);
+                    T.init(S, r, false, 0.0f, kind == SHADOW_ANY ? FLT_MAX : d.w, stack);
                 }
             }
             while (__any_sync(0xFFFFFFFFu, live)) {
@@ -683,9 +681,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_shadow(DevScene S, CameraParams
                 const DevLight &L = S.lights[li];
                 float tl = FLT_MAX;
                 const int lh = light_entity_hit(S, L, r, tl);
-                T.init(S, r, false, 0.0f, lh ? tl : FLT_MAX, L.ent_index);
+                T.init(S, r, false, 0.0f, lh ? tl : FLT_MAX, stack, L.ent_index);
             } else {
-                T.init(S, r, false, 0.0f, kind == SHADOW_ANY ? FLT_MAX : d.w);
+                T.init(S, r, false, 0.0f, kind == SHADOW_ANY ? FLT_MAX : d.w, stack);
             }
         }
         if (__all_sync(0xFFFFFFFFu, idx == kLaneDone)) break;

@@ -163,6 +163,8 @@ struct DevScene {
     const float *perlin_grad;       // 256 * 3
     const unsigned char *texels;
     uint32_t tlas_root;             // 0xFFFFFFFF: empty scene
+    uint32_t tlas_single_group;     // the top level's only primitive when it is a group (its hierarchy
+                                    // is entered directly), else 0xFFFFFFFF
     uint32_t ent_count, group_count, material_count, texture_count, light_count;
     uint32_t bg_texture, env_texture;  // indices into textures[] (appended after scene.Textures)
     float ambient[3];

@@ -734,6 +734,7 @@ int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_
     D.texels = Upload(*G, texels, st, rc);
     if (rc != AZ_OK) return rc;
     D.tlas_root = tlas_root;
+    D.tlas_single_group = tlas.size() == 1 && (tlas[0] & AZD_TLAS_GROUP) ? (tlas[0] & ~AZD_TLAS_GROUP) : 0xFFFFFFFFu;
     D.ent_count = (uint32_t)F.ents.size();
     D.group_count = (uint32_t)dgroups.size();
     D.material_count = scene->MaterialCount;

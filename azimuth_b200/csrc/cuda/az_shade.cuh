@@ -308,41 +308,48 @@ __device__ __forceinline__ void guide_query(const DevScene &S, const Ray &wr, co
 // ---------------------------------------------------------------------------
 // BRDFs and light contribution, src/azimuth_main.cpp:461-603
 // ---------------------------------------------------------------------------
+// The seven models share one powf(cos alpha, exponent): Phong-type models take
+// cos alpha from the reflected light direction, Blinn-type models and
+// Torrance-Sparrow from the half vector.  Each model's expression is azimuth's
+// (same operations on the same values), so results are unchanged; warps whose
+// lanes hold different models evaluate the power once instead of once per model.
 static __device__ void eval_brdf(float &diffuse, float &specular, const DevMaterial &m, f3 L, f3 N, f3 V, float cti) {
     const float e = m.exponent;
-    switch (m.brdf_type) {
-        case 0: {  // Phong
-            float ca = dot(-V, reflect(L, N));
-            specular = ca > 0.0f ? powf(ca, e) / cti : 0.0f;
-        } break;
-        case 1: {  // Modified Phong
-            float ca = dot(-V, reflect(L, N));
-            specular = ca > 0.0f ? powf(ca, e) : 0.0f;
-        } break;
-        case 2: {  // Normalized Modified Phong
+    const uint32_t type = m.brdf_type;
+    f3 hv = mk(0.0f, 0.0f, 0.0f);
+    float ca;
+    if (type <= 2) {
+        ca = dot(-V, reflect(L, N));
+    } else {
+        hv = normalize(-V + L);
+        ca = dot(N, hv);
+    }
+    const float p = ca > 0.0f ? powf(ca, e) : 0.0f;
+    switch (type) {
+        case 0:  // Phong
+            specular = ca > 0.0f ? p / cti : 0.0f;
+            break;
+        case 1:  // Modified Phong
+            specular = ca > 0.0f ? p : 0.0f;
+            break;
+        case 2:  // Normalized Modified Phong
             diffuse = (float)(1.0 / 3.14159265359);
-            float ca = dot(-V, reflect(L, N));
-            specular = ca > 0.0f ? ((e + 2.0f) / (2.0f * AZD_PI_F32)) * powf(ca, e) : 0.0f;
-        } break;
-        case 3: {  // Blinn-Phong
-            float ca = dot(N, normalize(-V + L));
-            specular = ca > 0.0f ? powf(ca, e) / cti : 0.0f;
-        } break;
-        case 4: {  // Modified Blinn-Phong
-            float ca = dot(N, normalize(-V + L));
-            specular = ca > 0.0f ? powf(ca, e) : 0.0f;
-        } break;
-        case 5: {  // Normalized Modified Blinn-Phong
+            specular = ca > 0.0f ? ((e + 2.0f) / (2.0f * AZD_PI_F32)) * p : 0.0f;
+            break;
+        case 3:  // Blinn-Phong
+            specular = ca > 0.0f ? p / cti : 0.0f;
+            break;
+        case 4:  // Modified Blinn-Phong
+            specular = ca > 0.0f ? p : 0.0f;
+            break;
+        case 5:  // Normalized Modified Blinn-Phong
             diffuse = (float)(1.0 / 3.14159265359);
-            float ca = dot(N, normalize(-V + L));
-            specular = ca > 0.0f ? ((e + 8.0f) / (8.0f * AZD_PI_F32)) * powf(ca, e) : 0.0f;
-        } break;
+            specular = ca > 0.0f ? ((e + 8.0f) / (8.0f * AZD_PI_F32)) * p : 0.0f;
+            break;
         default: {  // Torrance-Sparrow
             diffuse = (float)(1.0 / 3.14159265359);
-            f3 hv = normalize(-V + L);
-            float ca = dot(N, hv);
             if (ca > 0.0f) {
-                float D = ((e + 2.0f) / (2.0f * AZD_PI_F32)) * powf(ca, e);
+                float D = ((e + 2.0f) / (2.0f * AZD_PI_F32)) * p;
                 float nw0 = dot(N, -V), w0wh = dot(-V, hv);
                 float G = nw0 < cti ? nw0 : cti;
                 G = (2.0f * G * ca) / w0wh;

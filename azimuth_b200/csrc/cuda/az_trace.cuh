@@ -266,8 +266,10 @@ struct Tracer {
     int sp;
     Hit best;
 
+    // `stack`: the query's stack (AZD_WSTACK entries), which a scene whose top
+    // level is a single group starts with that group's exit marker.
     __device__ __forceinline__ void init(const DevScene &S, const Ray &ray, bool cull_, float eps_, float tmax_,
-                                         uint32_t skip = 0xFFFFFFFFu) {
+                                         uint2 *stack, uint32_t skip = 0xFFFFFFFFu) {
         wr = ray;
         r = ray;
         inv = safe_inv(r.d);
@@ -293,6 +295,41 @@ struct Tracer {
         // current node group: the root alone (imask bit 0, hit bit 0 ^ oct)
         ng_base = S.tlas_root;
         ng_bits = S.tlas_root == 0xFFFFFFFFu ? 0u : ((1u << 8) | (1u << oct));
+        // a top level holding one group only: enter its hierarchy directly (the
+        // top-level root test and the group's leaf would only lead there)
+        if (S.tlas_single_group != 0xFFFFFFFFu) {
+            ng_bits = 0u;
+            enter_group(S, stack, S.tlas_single_group);
+        }
+    }
+
+    // Enters group gi's bottom-level hierarchy (azimuth: GetLocalRay of the
+    // motion-shifted ray, src/azimuth_main.cpp:246-250); its exit marker goes on
+    // the stack (room for it is kept when a group entry is pushed).
+    __device__ __forceinline__ void enter_group(const DevScene &S, uint2 *stack, uint32_t gi) {
+        g_idx = gi;
+        const DevGroup &g = S.groups[g_idx];
+        if (g.root == 0xFFFFFFFFu) return;
+        stack[sp++] = make_uint2(0u, AZD_E_EXIT);
+        float blas_scale = 1.0f;
+        if (g.raw) {
+            r = wr;
+        } else {
+            Ray m = wr;
+            m.o = wr.o - wr.time * mk(g.motion[0], g.motion[1], g.motion[2]);
+            r = local_ray(m, g.inv);
+            // local t = world t * |inv * d| / |d| (up to rounding)
+            blas_scale = length(vector_xf(g.inv, wr.d)) / length(wr.d) * 1.0001f;
+        }
+        inv = safe_inv(r.d);
+        oct = octant_of(r.d);
+        float wlim = KIND == Q_ANY ? tmax : best.t;
+        tcur = wlim < FLT_MAX ? wlim * blas_scale + 1e-30f : FLT_MAX;
+        bl_t = FLT_MAX;
+        bl_prim = 0xFFFFFFFFu;
+        in_blas = true;
+        ng_base = g.root;
+        ng_bits = (1u << 8) | (1u << oct);
     }
 
     __device__ __forceinline__ void push(uint2 *stack, uint32_t x, uint32_t y, uint32_t *err) {
@@ -341,10 +378,12 @@ struct Tracer {
             const uint32_t pi = pg_base + bit;
             prims_visited++;
             if (in_blas) {
-                if (skip_ent != 0xFFFFFFFFu && __ldg(&S.tri_attr[pi].entity) == skip_ent) continue;
                 DevTri tr = load_tri(S.tris, pi);
                 float t, b, gm;
                 if (tri_test(tr, r, cull, eps, bl_t, t, b, gm)) {
+                    // a primitive of the skipped entity is ignored; its owner is
+                    // looked up only for the few primitives that are hit
+                    if (skip_ent != 0xFFFFFFFFu && __ldg(&S.tri_attr[pi].entity) == skip_ent) continue;
                     bl_t = t;
                     bl_prim = pi;
                     if (KIND == Q_ANY) {
@@ -404,31 +443,7 @@ struct Tracer {
             tcur = KIND == Q_ANY ? tmax : best.t;
             in_blas = false;
         } else if (e.y == AZD_E_GROUP) {
-            // enter the group's BLAS (azimuth: GetLocalRay of the motion-shifted
-            // ray, src/azimuth_main.cpp:246-250)
-            g_idx = e.x;
-            const DevGroup &g = S.groups[g_idx];
-            if (g.root == 0xFFFFFFFFu) return false;
-            stack[sp++] = make_uint2(0u, AZD_E_EXIT);   // reuses the popped entry's slot
-            float blas_scale = 1.0f;
-            if (g.raw) {
-                r = wr;
-            } else {
-                Ray m = wr;
-                m.o = wr.o - wr.time * mk(g.motion[0], g.motion[1], g.motion[2]);
-                r = local_ray(m, g.inv);
-                // local t = world t * |inv * d| / |d| (up to rounding)
-                blas_scale = length(vector_xf(g.inv, wr.d)) / length(wr.d) * 1.0001f;
-            }
-            inv = safe_inv(r.d);
-            oct = octant_of(r.d);
-            float wlim = KIND == Q_ANY ? tmax : best.t;
-            tcur = wlim < FLT_MAX ? wlim * blas_scale + 1e-30f : FLT_MAX;
-            bl_t = FLT_MAX;
-            bl_prim = 0xFFFFFFFFu;
-            in_blas = true;
-            ng_base = g.root;
-            ng_bits = (1u << 8) | (1u << oct);
+            enter_group(S, stack, e.x);   // its exit marker reuses the popped entry's slot
         } else if ((e.y & 0xC0000000u) == AZD_E_PRIMS) {
             pg_base = e.x;
             pg_mask = e.y & 0x00FFFFFFu;
@@ -479,6 +494,11 @@ __device__ bool trace(const DevScene &S, const Ray &wr, bool cull, float eps, fl
     // current node group: the root alone (imask bit 0, hit bit 0 ^ oct)
     uint32_t ng_base = S.tlas_root, ng_bits = (1u << 8) | (1u << oct);
     uint32_t pg_base = 0, pg_mask = 0;             // current primitive group
+    if (S.tlas_single_group != 0xFFFFFFFFu) {
+        // a top level holding one group only: start with its entry on the stack
+        ng_bits = 0u;
+        stack[sp++] = make_uint2(S.tlas_single_group, AZD_E_GROUP);
+    }
 
     while (true) {
         if (++steps > AZD_MAX_STEPS) {
@@ -524,10 +544,12 @@ __device__ bool trace(const DevScene &S, const Ray &wr, bool cull, float eps, fl
             const uint32_t pi = pg_base + bit;
             prims_visited++;
             if (in_blas) {
-                if (skip_ent != 0xFFFFFFFFu && __ldg(&S.tri_attr[pi].entity) == skip_ent) continue;
                 DevTri tr = load_tri(S.tris, pi);
                 float t, b, gm;
                 if (tri_test(tr, r, cull, eps, bl_t, t, b, gm)) {
+                    // a primitive of the skipped entity is ignored; its owner is
+                    // looked up only for the few primitives that are hit
+                    if (skip_ent != 0xFFFFFFFFu && __ldg(&S.tri_attr[pi].entity) == skip_ent) continue;
                     bl_t = t;
                     bl_prim = pi;
                     if (KIND == Q_ANY) {
