@@ -36,6 +36,9 @@ FLAG_COUNT_TRAVERSAL = 1
 FLAG_NO_GRAPH = 2
 FLAG_TIME_STAGES = 4
 FLAG_ENV_IMPORTANCE = 8
+FLAG_ORDER_SHADOW = 16     # visit shadow queues by origin cell
+FLAG_ORDER_EXTEND = 32     # visit extension queues by origin cell and direction octant
+FLAG_ORDER_NONE = 64       # queues in fill order
 LAUNCH_VARIANTS = 14   # AZ_LAUNCH_VARIANTS
 
 STATUS = {0: "AZ_OK", 1: "AZ_ERR_INVALID_ARGUMENT", 2: "AZ_ERR_INVALID_SCENE", 3: "AZ_ERR_OUT_OF_MEMORY",
@@ -202,7 +205,7 @@ class GpuScene:
         the time of its parts (host flattening, uploads, GPU BVH build) in ms."""
         si = SceneInfo()
         _check(lib().az_gpu_scene_info(self._h, C.byref(si)), "az_gpu_scene_info")
-        return {k: getattr(si, k) for k, _ in SceneInfo._fields_ if k != "reserved"}
+        return {k: getattr(si, k) for k, _ in SceneInfo._fields_}
 
     def autotune(self, seed=0, stream=None):
         """az_gpu_autotune: picks the traversal launch variant for this scene; returns (variant, ms)."""

@@ -89,7 +89,8 @@ class SceneInfo(C.Structure):
                 ("device_bytes", C.c_uint64), ("bvh_width", C.c_uint32), ("bvh_leaf", C.c_uint32),
                 ("bvh_depth", C.c_uint32), ("hierarchies", C.c_uint32), ("flatten_ms", C.c_float),
                 ("upload_ms", C.c_float), ("bvh_ms", C.c_float), ("total_ms", C.c_float),
-                ("ingest_ms", C.c_float), ("bvh_builder", C.c_uint32), ("reserved", C.c_uint32 * 2)]
+                ("ingest_ms", C.c_float), ("bvh_builder", C.c_uint32), ("queue_order", C.c_uint32),
+                ("variant", C.c_uint32)]
 
 
 class MeshDesc(C.Structure):

@@ -158,6 +158,9 @@ extern "C" int az_gpu_scene_info(const az_gpu_scene *scene, az_scene_info *out) 
     out->total_ms = G.total_ms;
     out->ingest_ms = G.ingest_ms;
     out->bvh_builder = G.bvh_builder;
+    out->queue_order = ((G.order & kOrderShadow) ? (uint32_t)AZ_FLAG_ORDER_SHADOW : 0u) |
+                       ((G.order & kOrderExtend) ? (uint32_t)AZ_FLAG_ORDER_EXTEND : 0u);
+    out->variant = G.variant + 1;
     return AZ_OK;
 }
 

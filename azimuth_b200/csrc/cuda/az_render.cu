@@ -19,6 +19,8 @@
 // own tree up to float summation order.  Child nodes whose weight is exactly
 // zero (e.g. the scatter ray of a pure mirror) are not traced; azimuth traces
 // them and multiplies their radiance by zero.
+#include <cub/cub.cuh>
+
 #include <algorithm>
 #include <cfloat>
 #include <cstring>
@@ -179,6 +181,41 @@ struct WarpFetch {
     }
 };
 
+// Sort keys that group a level's queue by where its rays start: a 15-bit
+// Morton code of the origin's cell in a 32^3 grid over the scene bounds, for
+// extension rays the top 13 bits of it and the direction octant.  Entries past
+// the queue's size get the largest key, so after a stable sort the first
+// `size` indices are the queue's own.
+__global__ void k_order_keys(DevScene S, WaveQueues Q, uint32_t level, int shadow, uint32_t cap, uint32_t *keys,
+                             uint32_t *vals) {
+    const uint32_t n = shadow ? min(Q.counts[AZ_COUNT_SHADOW + level], Q.cap_s) : min(Q.counts[level], Q.cap_q);
+    const int buf = level & 1;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cap; i += gridDim.x * blockDim.x) {
+        uint32_t key = 0xFFFFu;
+        if (i < n) {
+            const float4 o = shadow ? Q.so[i] : Q.o[buf][i];
+            uint32_t c[3];
+            const float p[3] = {o.x, o.y, o.z};
+            for (int a = 0; a < 3; a++) {
+                const float u = (p[a] - S.box_lo[a]) * S.box_scale[a] * 32.0f;
+                c[a] = u > 0.0f ? min((uint32_t)u, 31u) : 0u;   // NaN and below the box: cell 0
+            }
+            uint32_t m = 0;
+            for (int b = 4; b >= 0; b--)
+                m = (m << 3) | (((c[0] >> b) & 1u) << 2) | (((c[1] >> b) & 1u) << 1) | ((c[2] >> b) & 1u);
+            if (shadow) {
+                key = m;
+            } else {
+                const float4 d = Q.d[buf][i];
+                const uint32_t oct = (d.x < 0.0f ? 4u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 1u : 0u);
+                key = ((m >> 2) << 3) | oct;
+            }
+        }
+        keys[i] = key;
+        vals[i] = i;
+    }
+}
+
 // How a traversal kernel maps queries to threads:
 //   MODE_LOOP     one query per thread at a time in a grid-stride loop, each
 //                 thread running its query to the end in one loop
@@ -200,8 +237,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_extend(DevScene S, CameraParams
         uint2 stack[AZD_WSTACK];
         // warp-uniform loop bound: every lane of a warp sees the same base
         for (uint32_t base = blockIdx.x * BLOCK + (threadIdx.x & ~31u); base < n; base += gridDim.x * BLOCK) {
-            const uint32_t i = base + (threadIdx.x & 31u);
-            bool live = i < n;
+            const uint32_t k = base + (threadIdx.x & 31u);
+            bool live = k < n;
+            const uint32_t i = live && Q.eorder ? Q.eorder[k] : k;
             if (live) {
                 const float4 o = Q.o[buf][i], d = Q.d[buf][i];
                 Ray r;
@@ -223,7 +261,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_extend(DevScene S, CameraParams
     }
     if (MODE == MODE_LOOP) {
         // one query per thread at a time, grid-stride over the queue
-        for (uint32_t i = blockIdx.x * BLOCK + threadIdx.x; i < n; i += gridDim.x * BLOCK) {
+        for (uint32_t k = blockIdx.x * BLOCK + threadIdx.x; k < n; k += gridDim.x * BLOCK) {
+            const uint32_t i = Q.eorder ? Q.eorder[k] : k;
             const float4 o = Q.o[buf][i], d = Q.d[buf][i];
             Ray r;
             r.o = mk(o.x, o.y, o.z);
@@ -239,10 +278,11 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_extend(DevScene S, CameraParams
     Tracer<Q_CLOSEST> T;
     uint2 stack[AZD_WSTACK];
     WarpFetch wf;
-    uint32_t idx = kLaneIdle;
+    uint32_t idx = kLaneIdle, qi = 0;   // work item and its queue entry
     while (true) {
         if (wf.refill(fetch, n, idx)) {
-            const float4 o = Q.o[buf][idx], d = Q.d[buf][idx];
+            qi = Q.eorder ? Q.eorder[idx] : idx;
+            const float4 o = Q.o[buf][qi], d = Q.d[buf][qi];
             Ray r;
             r.o = mk(o.x, o.y, o.z);
             r.d = mk(d.x, d.y, d.z);
@@ -252,7 +292,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_extend(DevScene S, CameraParams
         if (__all_sync(0xFFFFFFFFu, idx == kLaneDone)) break;
         if (idx < n && T.step(S, stack, err)) {
             const Hit &h = T.best;
-            Q.hit[idx] = make_uint4(__float_as_uint(h.t), __float_as_uint(h.tl), h.prim, h.ent);
+            Q.hit[qi] = make_uint4(__float_as_uint(h.t), __float_as_uint(h.tl), h.prim, h.ent);
             T.flush_counts(cnt);
             idx = kLaneIdle;
         }
@@ -601,8 +641,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_shadow(DevScene S, CameraParams
         Tracer<Q_ANY> T;
         uint2 stack[AZD_WSTACK];
         for (uint32_t base = blockIdx.x * BLOCK + (threadIdx.x & ~31u); base < n; base += gridDim.x * BLOCK) {
-            const uint32_t i = base + (threadIdx.x & 31u);
-            bool live = i < n;
+            const uint32_t k = base + (threadIdx.x & 31u);
+            bool live = k < n;
+            const uint32_t i = live && Q.sorder ? Q.sorder[k] : k;
             float4 c = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             if (live) {
                 const float4 o = Q.so[i], d = Q.sd[i];
@@ -635,7 +676,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_shadow(DevScene S, CameraParams
         return;
     }
     if (MODE == MODE_LOOP) {
-        for (uint32_t i = blockIdx.x * BLOCK + threadIdx.x; i < n; i += gridDim.x * BLOCK) {
+        for (uint32_t k = blockIdx.x * BLOCK + threadIdx.x; k < n; k += gridDim.x * BLOCK) {
+            const uint32_t i = Q.sorder ? Q.sorder[k] : k;
             const float4 o = Q.so[i], d = Q.sd[i], c = Q.sc[i];
             const uint32_t meta = Q.smeta[i];
             const uint32_t kind = meta >> 30, li = meta & 0x3FFFFFFFu;
@@ -667,9 +709,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_shadow(DevScene S, CameraParams
     float4 c = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     while (true) {
         if (wf.refill(fetch, n, idx)) {
-            const float4 o = Q.so[idx], d = Q.sd[idx];
-            c = Q.sc[idx];
-            const uint32_t meta = Q.smeta[idx];
+            const uint32_t qi = Q.sorder ? Q.sorder[idx] : idx;
+            const float4 o = Q.so[qi], d = Q.sd[qi];
+            c = Q.sc[qi];
+            const uint32_t meta = Q.smeta[qi];
             const uint32_t kind = meta >> 30, li = meta & 0x3FFFFFFFu;
             Ray r;
             r.o = mk(o.x, o.y, o.z);
@@ -878,6 +921,34 @@ WaveBuffers::~WaveBuffers() {
     if (wave_host) cudaFreeHost(wave_host);
     if (guide_lobes) cudaFree(guide_lobes);
     if (guide_rec) cudaFree(guide_rec);
+    for (void *p : {(void *)okey[0], (void *)okey[1], (void *)oval, (void *)oidx_e, (void *)oidx_s, otemp})
+        if (p) cudaFree(p);
+}
+
+int WaveBuffers::EnsureOrder(uint32_t cap) {
+    if (cap <= ocap && otemp) return AZ_OK;
+    DropGraph();   // it refers to the buffers replaced below
+    for (uint32_t **p : {&okey[0], &okey[1], &oval, &oidx_e, &oidx_s}) {
+        if (*p) cudaFree(*p);
+        *p = nullptr;
+    }
+    if (otemp) cudaFree(otemp);
+    otemp = nullptr;
+    ocap = 0;
+    for (uint32_t **p : {&okey[0], &okey[1], &oval, &oidx_e, &oidx_s})
+        if (cudaMalloc((void **)p, (size_t)cap * sizeof(uint32_t)) != cudaSuccess) {
+            *p = nullptr;
+            return SetError(AZ_ERR_OUT_OF_MEMORY, "queue ordering buffers");
+        }
+    size_t bytes = 0;
+    AZ_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, bytes, okey[0], okey[1], oval, oidx_e, (int)cap, 0, 16));
+    if (cudaMalloc(&otemp, bytes) != cudaSuccess) {
+        otemp = nullptr;
+        return SetError(AZ_ERR_OUT_OF_MEMORY, "queue ordering scratch");
+    }
+    otemp_bytes = bytes;
+    ocap = cap;
+    return AZ_OK;
 }
 
 void WaveBuffers::DropGraph() {
@@ -961,11 +1032,25 @@ struct StageTimer {
 // Launches of one wave.  With `capture`, the launches read the wave's first
 // sample, size and seed from W.wave_dev (set before every replay of the
 // captured graph) and size their grids for `n` = the largest wave.
+// Sorts the extension (shadow = 0) or shadow queue of `level` by origin cell
+// into its visiting order (k_order_keys + a 16-bit radix sort).
+static int OrderQueue(const GpuScene &G, const WaveQueues &Q, WaveBuffers &W, uint32_t level, int shadow, int sms,
+                      cudaStream_t st, RenderCounters &rc) {
+    const uint32_t cap = shadow ? Q.cap_s : Q.cap_q;
+    k_order_keys<<<sms * 8, 256, 0, st>>>(G.dev, Q, level, shadow, cap, W.okey[0], W.oval);
+    rc.launches++;
+    AZ_CUDA_TRY(cub::DeviceRadixSort::SortPairs(W.otemp, W.otemp_bytes, W.okey[0], W.okey[1], W.oval,
+                                                shadow ? W.oidx_s : W.oidx_e, (int)cap, 0, 16, st));
+    return AZ_OK;
+}
+
 static int RenderWave(const GpuScene &G, const CameraParams &cam, WaveBuffers &W, uint64_t start, uint32_t n,
                       az_pixel *film, cudaStream_t st, int sms, RenderCounters &rc, StageTimer *timer,
                       GuideState *guide, bool train, bool capture = false) {
     WaveQueues Q = W.q;
     if (capture) Q.wave = W.wave_dev;
+    if (cam.order & kOrderExtend) Q.eorder = W.oidx_e;
+    if (cam.order & kOrderShadow) Q.sorder = W.oidx_s;
     const uint32_t levels = std::min<uint32_t>(G.dev.max_depth + 1, AZ_MAX_LEVELS - 2);
     if (guide) {
         // proposals for every queue entry this wave can hold (the queue is capped to match)
@@ -983,6 +1068,10 @@ static int RenderWave(const GpuScene &G, const CameraParams &cam, WaveBuffers &W
     const uint32_t v = cam.variant;
     for (uint32_t L = 1; L <= levels; L++) {
         if (timer) timer->Mark(st, 0);
+        if (cam.order & kOrderExtend) {
+            int orc = OrderQueue(G, Q, W, L, 0, sms, st, rc);
+            if (orc != AZ_OK) return orc;
+        }
         LaunchTraversalVariant(v, false, sms, G.dev, cam, Q, L, st);
         if (guide) {
             int grc = GuideInfer(*guide, G, Q, L, st);
@@ -992,6 +1081,10 @@ static int RenderWave(const GpuScene &G, const CameraParams &cam, WaveBuffers &W
         if (timer) timer->Mark(st, 1);
         LaunchShade(grid, G.dev, cam, Q, start, L, st);
         if (timer) timer->Mark(st, 2);
+        if (cam.order & kOrderShadow) {
+            int orc = OrderQueue(G, Q, W, L, 1, sms, st, rc);
+            if (orc != AZ_OK) return orc;
+        }
         LaunchTraversalVariant(v, true, sms, G.dev, cam, Q, L, st);
         if (timer) timer->Mark(st, 3);
         rc.launches += G.dev.full_light_queries ? 4 : 3;
@@ -1063,6 +1156,15 @@ static int ReplayWave(const GpuScene &G, const CameraParams &cam, WaveBuffers &W
     return AZ_OK;
 }
 
+// The queue ordering of a render: the flags', else the scene's choice.
+static uint32_t QueueOrder(const GpuScene &G, const az_render_opts *opts) {
+    const uint32_t f = opts ? opts->flags : 0u;
+    if (f & AZ_FLAG_ORDER_NONE) return 0u;
+    if (f & (AZ_FLAG_ORDER_SHADOW | AZ_FLAG_ORDER_EXTEND))
+        return ((f & AZ_FLAG_ORDER_SHADOW) ? kOrderShadow : 0u) | ((f & AZ_FLAG_ORDER_EXTEND) ? kOrderExtend : 0u);
+    return G.order;
+}
+
 int Render(GpuScene &G, az_pixel *film, const az_camera *camera, const az_epsilon_values *eps, az_scissor sc,
            int32_t filter, uint32_t cull, const az_render_opts *opts, cudaStream_t st, az_render_stats *stats,
            GuideState *guide, bool train, WaveBuffers *wave_buffers) {
@@ -1073,6 +1175,7 @@ int Render(GpuScene &G, az_pixel *film, const az_camera *camera, const az_epsilo
     cam.env_importance = opts && (opts->flags & AZ_FLAG_ENV_IMPORTANCE) && G.dev.env_rows ? 1u : 0u;
     cam.variant = opts && opts->variant ? opts->variant - 1 : G.variant;
     if (cam.variant >= kVariantCount) return SetError(AZ_ERR_INVALID_ARGUMENT, "unknown launch variant");
+    cam.order = QueueOrder(G, opts);
     if (G.dev.max_depth + 1 > AZ_MAX_LEVELS - 2) return SetError(AZ_ERR_UNSUPPORTED, "MaxRecursionDepth above 61");
     uint64_t total = cam.npix * (uint64_t)cam.sqrt_spp * cam.sqrt_spp;
     if (stats) memset(stats, 0, sizeof(*stats));
@@ -1110,6 +1213,7 @@ int Render(GpuScene &G, az_pixel *film, const az_camera *camera, const az_epsilo
                                                                          (uint64_t)n * 4), 1024);
         rc = W.Ensure(n, cap_q, cap_s);
         if (rc != AZ_OK) return rc;
+        if (cam.order && (rc = W.EnsureOrder(std::max(W.q.cap_q, W.q.cap_s))) != AZ_OK) return rc;
         if (use_graph) {
             rc = ReplayWave(G, cam, W, pos, n, chunk, film, st, sms, counters);
         } else {
@@ -1202,9 +1306,33 @@ int Autotune(GpuScene &G, const az_camera *camera, const az_epsilon_values *eps,
             best = v;
         }
     }
+    // then the queue ordering with that launch configuration, unless the caller fixed it
+    const uint32_t order_flags = AZ_FLAG_ORDER_SHADOW | AZ_FLAG_ORDER_EXTEND | AZ_FLAG_ORDER_NONE;
+    uint32_t best_order = QueueOrder(G, opts);
+    if (rc == AZ_OK && !(opts && (opts->flags & order_flags))) {
+        o.variant = best + 1;
+        for (uint32_t ord : {0u, kOrderShadow, kOrderExtend, kOrderShadow | kOrderExtend}) {
+            if (ord == best_order || rc != AZ_OK) continue;
+            o.flags = (o.flags & ~(order_flags | (uint32_t)AZ_FLAG_TIME_STAGES)) |
+                      (ord == 0 ? (uint32_t)AZ_FLAG_ORDER_NONE
+                                : ((ord & kOrderShadow) ? (uint32_t)AZ_FLAG_ORDER_SHADOW : 0u) |
+                                      ((ord & kOrderExtend) ? (uint32_t)AZ_FLAG_ORDER_EXTEND : 0u));
+            az_render_stats stats;
+            float oms = FLT_MAX;
+            for (int rep = 0; rep < 3 && rc == AZ_OK; rep++) {
+                rc = Render(G, film, camera, eps, band, filter, cull, &o, st, &stats);
+                if (rep > 0) oms = std::min(oms, stats.gpu_ms);
+            }
+            if (rc == AZ_OK && oms < best_ms) {
+                best_ms = oms;
+                best_order = ord;
+            }
+        }
+    }
     cudaFree(film);
     if (rc != AZ_OK) return rc;
     G.variant = best;
+    G.order = best_order;
     if (best_out) *best_out = best + 1;
     if (ms_out) *ms_out = best_ms;
     return AZ_OK;

@@ -35,7 +35,10 @@ struct CameraParams {
     uint32_t count_traversal;
     uint32_t variant;              // launch configuration of the traversal kernels
     uint32_t env_importance;       // AZ_FLAG_ENV_IMPORTANCE
+    uint32_t order;                // kOrderShadow | kOrderExtend: queues visited in sorted order
 };
+
+constexpr uint32_t kOrderShadow = 1, kOrderExtend = 2;
 
 // Device queues of one wave of camera samples (structure of arrays).
 struct WaveQueues {
@@ -46,6 +49,9 @@ struct WaveQueues {
     float4 *so, *sd, *sc;                   // shadow queue
     uint32_t *smeta;
     uint32_t cap_s;
+    // visiting orders of the extension and shadow queues (null: queue order);
+    // entry k of the stage's work is queue entry order[k]
+    const uint32_t *eorder, *sorder;
     float4 *accum;                          // per-sample radiance sums
     uint32_t *counts;                       // see AZ_COUNT_*
     // [first sample, sample count, seed] of the current wave when set: a
@@ -73,7 +79,14 @@ struct WaveBuffers {
     size_t guide_lobes_cap = 0;
     azd::GuideRecord *guide_rec = nullptr;
     size_t guide_rec_cap = 0;
+    // queue ordering: cell keys (double-buffered), identity indices, the two
+    // visiting orders and the radix sort's scratch
+    uint32_t *okey[2] = {nullptr, nullptr}, *oval = nullptr, *oidx_e = nullptr, *oidx_s = nullptr;
+    void *otemp = nullptr;
+    size_t otemp_bytes = 0;
+    uint32_t ocap = 0;
     ~WaveBuffers();
+    int EnsureOrder(uint32_t cap);
     void DropGraph();
     int Ensure(uint32_t chunk, uint32_t cap_q, uint32_t cap_s);
 };

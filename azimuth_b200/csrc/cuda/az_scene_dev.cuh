@@ -165,6 +165,7 @@ struct DevScene {
     uint32_t tlas_root;             // 0xFFFFFFFF: empty scene
     uint32_t tlas_single_group;     // the top level's only primitive when it is a group (its hierarchy
                                     // is entered directly), else 0xFFFFFFFF
+    float box_lo[3], box_scale[3];  // scene bounds: cell = (p - box_lo) * box_scale in [0, 1)
     uint32_t ent_count, group_count, material_count, texture_count, light_count;
     uint32_t bg_texture, env_texture;  // indices into textures[] (appended after scene.Textures)
     float ambient[3];

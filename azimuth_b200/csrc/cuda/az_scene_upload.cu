@@ -734,6 +734,18 @@ int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_
     D.texels = Upload(*G, texels, st, rc);
     if (rc != AZ_OK) return rc;
     D.tlas_root = tlas_root;
+    {
+        Box sb;
+        for (size_t k = 0; k < tlo.size(); k++) {
+            sb.grow(tlo[k].x, tlo[k].y, tlo[k].z);
+            sb.grow(thi[k].x, thi[k].y, thi[k].z);
+        }
+        for (int a = 0; a < 3; a++) {
+            const float ext = sb.hi[a] > sb.lo[a] ? sb.hi[a] - sb.lo[a] : 1.0f;
+            D.box_lo[a] = tlo.empty() ? 0.0f : sb.lo[a];
+            D.box_scale[a] = 1.0f / ext;
+        }
+    }
     D.tlas_single_group = tlas.size() == 1 && (tlas[0] & AZD_TLAS_GROUP) ? (tlas[0] & ~AZD_TLAS_GROUP) : 0xFFFFFFFFu;
     D.ent_count = (uint32_t)F.ents.size();
     D.group_count = (uint32_t)dgroups.size();

@@ -45,10 +45,15 @@ enum {
     AZ_FLAG_COUNT_TRAVERSAL = 1u << 0,  /* fill az_render_stats node/primitive visit counters */
     AZ_FLAG_NO_GRAPH = 1u << 1,         /* launch the per-bounce stages directly, not as a CUDA graph */
     AZ_FLAG_TIME_STAGES = 1u << 2,      /* time each stage with CUDA events (az_render_stats *_ms) */
-    AZ_FLAG_ENV_IMPORTANCE = 1u << 3    /* environment light samples by one-sample MIS of a luminance CDF of
+    AZ_FLAG_ENV_IMPORTANCE = 1u << 3,   /* environment light samples by one-sample MIS of a luminance CDF of
                                            the 2D environment map and cosine sampling, instead of azimuth's
                                            cosine sampling alone (same estimate, lower variance for peaked
                                            maps; not a parity mode) */
+    /* Queue ordering (the results do not change, only which rays share a warp):
+     * by default the scene's choice (az_gpu_autotune picks it). */
+    AZ_FLAG_ORDER_SHADOW = 1u << 4,     /* visit each level's shadow queue in the order of the rays' origin cells */
+    AZ_FLAG_ORDER_EXTEND = 1u << 5,     /* visit each level's extension queue by origin cell and direction octant */
+    AZ_FLAG_ORDER_NONE = 1u << 6        /* queues in the order they were filled */
 };
 
 /* Number of traversal launch configurations (az_render_opts.variant). */
@@ -122,7 +127,9 @@ typedef struct az_scene_info {
     float total_ms;              /* the whole az_gpu_scene_create call */
     float ingest_ms;             /* GPU post-processing of a mesh soup (az_gpu_scene_create_from_meshes) */
     uint32_t bvh_builder;        /* AZ_BVH_LBVH or AZ_BVH_PLOC */
-    uint32_t reserved[2];
+    uint32_t queue_order;        /* the scene's queue ordering: AZ_FLAG_ORDER_SHADOW | AZ_FLAG_ORDER_EXTEND bits
+                                    (0: queue order); az_gpu_autotune sets it */
+    uint32_t variant;            /* the scene's traversal launch configuration, 1-based */
 } az_scene_info;
 
 int az_gpu_scene_info(const az_gpu_scene *scene, az_scene_info *out);

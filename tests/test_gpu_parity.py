@@ -149,3 +149,30 @@ def test_bvh_widths_render_the_same_film_and_autotune_scene(gpu):
         g.render_device(f.data_ptr(), seed=7, stats=True)
         ok, _, rel = ol.film_compare(f.cpu().numpy(), films[0], 1e-4)
         assert ok >= 0.98 and rel < 1e-3, (ok, rel)
+
+
+def test_queue_orderings_render_the_same_film(gpu):
+    """Visiting the extension and shadow queues in origin-cell order (AZ_FLAG_ORDER_*) changes only which
+    rays share a warp: the same samples, hits and sums up to the order of the atomics.  Every launch mode
+    reads through the order."""
+    import torch
+    cases = [(az.SCENE_FEATURES, dict(width=48, height=40, spp=4), 1.0),
+             (az.SCENE_DENSE_MESH, dict(width=40, height=40, spp=4, detail=5), 0.999),
+             (az.SCENE_MOTION_ENV, dict(width=48, height=32, spp=4), 1.0)]
+    orders = [az.FLAG_ORDER_NONE, az.FLAG_ORDER_SHADOW, az.FLAG_ORDER_EXTEND,
+              az.FLAG_ORDER_SHADOW | az.FLAG_ORDER_EXTEND]
+    for sid, kw, need in cases:
+        scene = az.generate_scene(sid, seed=3, **kw)
+        w, h = scene.resolution()
+        with az.GpuScene(scene) as g:
+            base = torch.zeros((h, w, 4), device="cuda")
+            g.render_device(base.data_ptr(), seed=4, flags=az.FLAG_ORDER_NONE)
+            base = base.cpu().numpy()
+            for fl in orders[1:]:
+                for v in (1, 8, 11):   # grid-stride, persistent fetching, warp lockstep
+                    f = torch.zeros((h, w, 4), device="cuda")
+                    g.render_device(f.data_ptr(), seed=4, flags=fl, variant=v)
+                    assert ol.film_compare(f.cpu().numpy(), base, 1e-4)[0] >= need, (sid, fl, v)
+            v, ms = g.autotune(seed=4)
+            info = g.info()
+            assert info["variant"] == v and info["queue_order"] & ~(az.FLAG_ORDER_SHADOW | az.FLAG_ORDER_EXTEND) == 0
