@@ -79,6 +79,13 @@ __device__ __forceinline__ float guide_mixture_pdf(const GuideLobes &G, f3 n, f3
     return G.alpha * guide_vmf_mixture_pdf(G, w) + (1.0f - G.alpha) * cs * (1.0f / GUIDE_PI);
 }
 
+// The same mixture with the selection probability `alpha` given (any alpha
+// in [0, 1] gives an unbiased one-sample MIS estimator).
+__device__ __forceinline__ float guide_mixture_pdf_alpha(const GuideLobes &G, float alpha, f3 n, f3 w) {
+    const float cs = fmaxf(0.0f, dot(n, w));
+    return alpha * guide_vmf_mixture_pdf(G, w) + (1.0f - alpha) * cs * (1.0f / GUIDE_PI);
+}
+
 // Direction from lobe `k` (Wood 1994 / Jakob 2012 closed form for the vMF
 // on the sphere): cos theta = 1 + log(u1 + (1 - u1) exp(-2 kappa)) / kappa.
 __device__ __forceinline__ f3 guide_sample_lobe(const GuideLobes &G, int k, float u1, float u2) {

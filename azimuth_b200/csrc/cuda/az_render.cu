@@ -471,12 +471,15 @@ __global__ void __launch_bounds__(BLOCK) k_shade(DevScene S, CameraParams cam, W
             // diffuse scatter ray (:1029-1083): child 0
             f3 Sd;
             float invpdf, qpdf = 0.0f;
-            if (GUIDED) {
+            if (GUIDED && can_spawn) {
                 // path guiding: one-sample MIS of the learned vMF mixture and
-                // cosine sampling, weighted by the mixture density
+                // cosine sampling, weighted by the mixture density (the deepest
+                // level spawns no child: it has no proposals, and its records
+                // keep density 0, which training skips)
                 const GuideLobes &G = Q.lobes[i];
+                const float alpha = fminf(G.alpha, Q.guide_alpha_max);
                 const float us = rng.next();
-                if (us < G.alpha) {
+                if (us < alpha) {
                     const int k = guide_pick_lobe(G, rng.next());
                     const float u1 = rng.next();
                     Sd = guide_sample_lobe(G, k, u1, rng.next());
@@ -487,7 +490,7 @@ __global__ void __launch_bounds__(BLOCK) k_shade(DevScene S, CameraParams cam, W
                     onb(s.n, U, V);
                     Sd = normalize(U * (sinf(theta) * cosf(phi)) + V * (sinf(theta) * sinf(phi)) + s.n * cosf(theta));
                 }
-                qpdf = guide_mixture_pdf(G, s.n, Sd);
+                qpdf = guide_mixture_pdf_alpha(G, alpha, s.n, Sd);
                 invpdf = qpdf > 0.0f ? 1.0f / qpdf : 0.0f;
             } else {
                 float theta = S.importance_sampling ? asinf(sqrtf(rng.next())) : acosf(rng.next());
@@ -1051,6 +1054,11 @@ static int RenderWave(const GpuScene &G, const CameraParams &cam, WaveBuffers &W
     if (capture) Q.wave = W.wave_dev;
     if (cam.order & kOrderExtend) Q.eorder = W.oidx_e;
     if (cam.order & kOrderShadow) Q.sorder = W.oidx_s;
+    // While the guide trains, its early proposals can be far from the light
+    // field; capping the chance of sampling them at one half keeps every
+    // sample's weight within twice cosine sampling's (the estimate stays
+    // unbiased for any cap).  Inference-only renders use the learned value.
+    Q.guide_alpha_max = train ? 0.5f : 1.0f;
     const uint32_t levels = std::min<uint32_t>(G.dev.max_depth + 1, AZ_MAX_LEVELS - 2);
     if (guide) {
         // proposals for every queue entry this wave can hold (the queue is capped to match)
@@ -1073,7 +1081,7 @@ static int RenderWave(const GpuScene &G, const CameraParams &cam, WaveBuffers &W
             if (orc != AZ_OK) return orc;
         }
         LaunchTraversalVariant(v, false, sms, G.dev, cam, Q, L, st);
-        if (guide) {
+        if (guide && L + 1 <= G.dev.max_depth + 1) {   // the deepest level spawns nothing to guide
             int grc = GuideInfer(*guide, G, Q, L, st);
             if (grc != AZ_OK) return grc;
             rc.launches++;

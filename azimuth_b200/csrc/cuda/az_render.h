@@ -62,6 +62,7 @@ struct WaveQueues {
     azd::GuideLobes *lobes;                 // per extension-queue entry of the current level
     azd::GuideRecord *rec;                  // [level][n_rec] training vertices
     uint32_t n_rec, rec_levels;
+    float guide_alpha_max;                  // cap on the learned selection probability (1: none)
 };
 
 struct WaveBuffers {
