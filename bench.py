@@ -39,6 +39,9 @@ METRIC = "Mpaths/s on 1 B200; equal-time relMSE guided vs plain GPU vs FP64 conv
 WORKLOAD = "dense mesh + importance sampling: 1,310,720-triangle Perlin-displaced icosphere in a Cornell box, " \
            "7 BRDFs, 1024x1024, 64 spp, depth 8, cosine sampling + area-light NEE, Gaussian filter"
 SCENE_ARGS = dict(scene_id=1, seed=0)
+# mean DRAM read + write of three k_extend launches of this workload's timed
+# frame (levels 5-7 of wave 5), measured with ncu (see the roofline below)
+EXTEND_DRAM_BYTES_PER_LAUNCH = (451426560 + 387705344 + 341759488) / 3.0
 
 
 def parse():
@@ -310,8 +313,15 @@ def main():
     per_launch_bytes = bytes_per_frame / max(1, cnt["extend_launches"])
     per_launch_ms = extend_ms / max(1, extend_launches)
     achieved = per_launch_bytes / (per_launch_ms / 1000.0) / 1e9
+    # DRAM bytes (read + write) per k_extend launch of this workload, from one
+    # ncu capture of three launches of the timed frame (dram__bytes_read.sum +
+    # dram__bytes_write.sum, a single-pass capture of the full-size run; see
+    # profiles/k_extend_traffic_dense_mesh_1024x1024_64spp.md).  ncu flushes the
+    # caches before each captured launch, so this is the cold-cache figure.
+    traffic = EXTEND_DRAM_BYTES_PER_LAUNCH if SCENE_ARGS["scene_id"] == az.SCENE_DENSE_MESH else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                "traffic": None, "kernel": "k_extend (closest-hit traversal)",
+                "traffic": traffic, "traffic_unit": "bytes per launch (ncu capture)",
+                "algorithmic_bytes_per_launch": per_launch_bytes, "kernel": "k_extend (closest-hit traversal)",
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650",
                 "bytes_per_segment": bytes_per_frame / max(1, cnt["extend_rays"]),
                 "node_visits_per_segment": ext_nodes / max(1, cnt["extend_rays"]),
