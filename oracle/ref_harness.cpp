@@ -321,4 +321,57 @@ int azref_write_image(const float *Rgb, uint32_t Width, uint32_t Height, int32_t
     }
 }
 
+/* ImportXML (src/azimuth_xml.cpp:3021-3930) as azimuth's main calls it
+ * (src/azimuth_main.cpp:2026-2036): a default scene, epsilons 0 and 0.000275,
+ * then the scene file, PLY meshes included.  In this build
+ * libxml/xmlreader.h is the header-only reader of include/az_xmlreader.h.
+ * Returns 1 on success with heap copies of the scene, the cameras and the
+ * epsilons (kept for the life of the process), 0 when ImportXML fails. */
+int azref_import_xml(const char *FilePath, az_scene **SceneOut, az_camera **CamerasOut, uint32_t *CameraCount,
+                     az_epsilon_values **EpsilonsOut) {
+    scene *S = (scene *)calloc(1, sizeof(scene));
+    epsilon_values *E = (epsilon_values *)calloc(1, sizeof(epsilon_values));
+    if (!S || !E) { free(S); free(E); return 0; }
+    *S = DefaultScene();
+    E->Intersection = 0.0f;
+    E->ShadowRay = 0.000275f;
+    camera *Cameras = 0;
+    u32 Count = 0;
+    std::vector<char> Path(FilePath, FilePath + strlen(FilePath) + 1);
+    if (!ImportXML(S, &Cameras, &Count, E, Path.data())) return 0;
+    *SceneOut = (az_scene *)S;
+    *CamerasOut = (az_camera *)Cameras;
+    *CameraCount = Count;
+    *EpsilonsOut = (az_epsilon_values *)E;
+    return 1;
+}
+
+static void CountLeaves(const entity *E, uint32_t *Spheres, uint32_t *Instances) {
+    if (!E) return;
+    if (E->Type == EntityType_BVHNode) {
+        CountLeaves(E->Left, Spheres, Instances);
+        CountLeaves(E->Right, Spheres, Instances);
+    } else if (E->Type == EntityType_Sphere) {
+        (*Spheres)++;
+    } else if (E->Type == EntityType_MeshInstance) {
+        (*Instances)++;
+    }
+}
+
+/* Counts of an imported scene: Out[0..8] = meshes, materials, lights,
+ * triangles over all meshes, spheres and mesh instances under the top-level
+ * BVH, emitting meshes, PathTrace, MaxRecursionDepth. */
+void azref_scene_summary(const az_scene *AScene, uint32_t *Out9) {
+    const scene *S = (const scene *)AScene;
+    uint32_t Tris = 0, Emitters = 0, Spheres = 0, Instances = 0;
+    for (u32 M = 0; M < S->MeshCount; M++) {
+        Tris += S->Meshes[M].TriangleCount;
+        Emitters += S->Meshes[M].IsEmitter ? 1u : 0u;
+    }
+    CountLeaves(S->BVHRoot, &Spheres, &Instances);
+    uint32_t V[9] = {S->MeshCount, S->MaterialCount, S->LightCount, Tris, Spheres, Instances, Emitters,
+                     S->PathTrace, S->MaxRecursionDepth};
+    memcpy(Out9, V, sizeof(V));
+}
+
 }  /* extern "C" */

@@ -1,0 +1,151 @@
+"""azimuth's own scene importer, ImportXML with its PLY loader
+(src/azimuth_xml.cpp:3021-3930), run on a hand-written scene through the
+header-only reader (include/az_xmlreader.h) in place of libxml2, then the
+imported structs rendered and intersected by the GPU path against azimuth's
+own render code.  tests/scenes/box.xml holds an inline mesh, a light mesh, a
+point light, spheres, a smooth mesh from an ASCII PLY file with a quad face, a
+transformed instance of it, and a cube from a binary PLY file with motion."""
+import ctypes as C
+import os
+import shutil
+import struct
+
+import numpy as np
+import pytest
+
+import azimuth_b200 as az
+import oracle_lib as ol
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SCENES = os.path.join(HERE, "scenes")
+
+pytestmark = pytest.mark.skipif(not ol.have_ref(), reason="reference harness not built")
+
+
+def _cube_ply(path, half=0.15):
+    """A cube as a binary little-endian PLY file: 8 vertices of x y z nx ny nz u v, 6 quads."""
+    v = np.array([[x, y, z] for x in (-half, half) for y in (-half, half) for z in (-half, half)], np.float32)
+    quads = [(0, 1, 3, 2), (4, 6, 7, 5), (0, 4, 5, 1), (2, 3, 7, 6), (0, 2, 6, 4), (1, 5, 7, 3)]
+    for a, b, c, d in quads:   # outward windings, checked on both halves of the split
+        for tri in ((a, b, c), (a, c, d)):
+            n = np.cross(v[tri[1]] - v[tri[0]], v[tri[2]] - v[tri[0]])
+            assert np.dot(n, v[list(tri)].mean(0)) > 0
+    head = ("ply\nformat binary_little_endian 1.0\ncomment a cube for azimuth's PLY loader\n"
+            "element vertex 8\nproperty float x\nproperty float y\nproperty float z\n"
+            "property float nx\nproperty float ny\nproperty float nz\nproperty float u\nproperty float v\n"
+            "element face 6\nproperty list uchar int vertex_indices\nend_header\n").encode()
+    body = b"".join(struct.pack("<8f", *p, *(p / np.linalg.norm(p)), 0.5, 0.5) for p in v)
+    body += b"".join(struct.pack("<B4i", 4, *q) for q in quads)
+    with open(path, "wb") as f:
+        f.write(head + body)
+
+
+def write_box_scene(dirpath, xml_text=None):
+    ascii_ply = os.path.join(dirpath, "pyramid.ply")
+    binary_ply = os.path.join(dirpath, "cube.ply")
+    shutil.copy(os.path.join(SCENES, "pyramid.ply"), ascii_ply)
+    _cube_ply(binary_ply)
+    text = xml_text if xml_text is not None else open(os.path.join(SCENES, "box.xml")).read()
+    text = text.replace("@PLY_ASCII@", ascii_ply).replace("@PLY_BINARY@", binary_ply)
+    path = os.path.join(dirpath, "box.xml")
+    with open(path, "w") as f:
+        f.write(text)
+    return path
+
+
+class ImportedScene:
+    """The scene, first camera and epsilons that ImportXML produced (azimuth's own structs)."""
+
+    filter_type = az.FILTER_BOX       # RenderScene's filter (src/azimuth_main.cpp:1847)
+    perlin_gradients = None
+
+    def __init__(self, path):
+        L = ol.ref()
+        L.azref_import_xml.argtypes = [C.c_char_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.azref_import_xml.restype = C.c_int
+        L.azref_scene_summary.argtypes = [C.c_void_p, C.c_void_p]
+        s, cams, eps = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        n = C.c_uint32()
+        self.ok = L.azref_import_xml(os.fsencode(path), C.byref(s), C.byref(cams), C.byref(n), C.byref(eps)) == 1
+        self.scene_ptr, self.camera_ptr, self.epsilons_ptr = s.value, cams.value, eps.value
+        self.camera_count = n.value
+
+    def resolution(self):
+        buf = (C.c_uint32 * 2).from_address(self.camera_ptr + 340)   # az_camera.Resolution
+        return int(buf[0]), int(buf[1])
+
+    def sample_count(self):
+        return int(C.c_uint32.from_address(self.camera_ptr + 384).value)
+
+    def summary(self):
+        out = (C.c_uint32 * 9)()
+        ol.ref().azref_scene_summary(self.scene_ptr, out)
+        keys = ("meshes", "materials", "lights", "triangles", "spheres", "instances", "emitters", "path_trace",
+                "max_depth")
+        return dict(zip(keys, (int(x) for x in out)))
+
+
+@pytest.fixture(scope="module")
+def box(tmp_path_factory):
+    sc = ImportedScene(write_box_scene(str(tmp_path_factory.mktemp("box"))))
+    assert sc.ok
+    return sc
+
+
+def test_importer_reads_the_scene(box):
+    assert box.camera_count == 1
+    assert box.resolution() == (48, 40) and box.sample_count() == 4
+    # meshes 1-3, the light mesh, the PLY pyramid (4 triangles + a quad split in two), the PLY cube
+    # (6 quads); one instance per mesh plus the explicit MeshInstance; lights: the point light and
+    # the light mesh as an entity light
+    assert box.summary() == {"meshes": 6, "materials": 4, "lights": 2, "triangles": 6 + 2 + 2 + 2 + 6 + 12,
+                             "spheres": 2, "instances": 7, "emitters": 1, "path_trace": 1, "max_depth": 4}
+
+
+def test_restatement_renders_the_imported_scene_like_azimuth(box):
+    ref = ol.ref_film(box, seed=5, threads=1)
+    port = ol.port_film(box, seed=5, threads=1)
+    assert np.array_equal(ref.view(np.uint32), port.view(np.uint32))
+    assert (ref[..., :3] > 0).mean() > 0.5     # the box is lit
+
+
+@pytest.mark.parametrize("edit", [
+    ("<Radius>0.3</Radius>", "<Radius>0.3</Radius><Bogus/>"),            # an element the importer does not know
+    ("<Faces>1 4 8   1 8 5</Faces>", "<Faces>1 4 8   1 8 5</Mesh>"),      # mismatched end tag
+    ('<Mesh id="1">', "<Mesh id=1>"),                                    # unquoted attribute value
+    ("<Objects>", "<Objects><Radius>1</Radius>"),                        # an element out of place
+])
+def test_import_failures_are_reported(tmp_path, edit):
+    text = open(os.path.join(SCENES, "box.xml")).read()
+    assert edit[0] in text
+    sc = ImportedScene(write_box_scene(str(tmp_path), text.replace(edit[0], edit[1], 1)))
+    assert not sc.ok
+
+
+@pytest.mark.gpu
+def test_gpu_renders_the_imported_scene(gpu, box):
+    ref = ol.ref_film(box, seed=9)
+    film = az.produce_image(box, seed=9)
+    other = az.produce_image(box, seed=10)
+    ok, _, relmse = ol.film_compare(film, ref, 1e-4)
+    _, _, noise = ol.film_compare(other, ref, 1e-4)
+    assert np.allclose(film[..., 3], ref[..., 3], rtol=1e-5, atol=1e-6)
+    assert ok >= 0.95 and relmse <= 0.05 * noise
+
+
+@pytest.mark.gpu
+def test_gpu_hits_on_the_imported_scene(gpu, box):
+    rng = np.random.default_rng(4)
+    n = 1 << 14
+    o = rng.uniform((-0.95, 0.05, -0.95), (0.95, 1.95, 0.95), (n, 3)).astype(np.float32)
+    d = rng.normal(size=(n, 3)).astype(np.float32)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    t = rng.uniform(0.0, 1.0, (n, 1)).astype(np.float32)
+    rays = np.concatenate([o, d, t], axis=1)
+    want = ol.closest_hit("ref", box, rays)
+    with az.GpuScene(box) as g:
+        got = g.closest_hit(rays)
+    same = (got[0] == want[0]) & (got[1] == want[1]) & (got[2] == want[2])
+    assert want[0].mean() > 0.99                 # a closed box: nearly every ray hits
+    assert same.mean() >= 0.999
+    assert np.array_equal(got[3][same].view(np.uint32), want[3][same].view(np.uint32))
