@@ -58,7 +58,8 @@ def build_reference(reference=DEFAULT_REFERENCE, force=False):
     harness = os.path.join(HERE, "ref_harness.cpp")
     shim = os.path.join(HERE, "shim")
     deps = [harness, os.path.join(HERE, "patch_reference.py"), os.path.join(HERE, "az_rng_oracle.h"),
-            os.path.join(REPO, "include", "az_abi.h"), os.path.join(REPO, "include", "az_xmlreader.h")]
+            os.path.join(REPO, "include", "az_abi.h"), os.path.join(REPO, "include", "az_xmlreader.h"),
+            os.path.join(REPO, "include", "azimuth_gpu.h")]
     deps += [os.path.join(d, f) for d, _, files in os.walk(shim) for f in files]
     outputs = {"libazref.so": PARITY_FLAGS, "libazref_fast.so": SPEED_FLAGS}
     if not force and not any(_stale(os.path.join(REF_OUT, o), deps) for o in outputs):

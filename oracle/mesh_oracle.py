@@ -14,10 +14,11 @@ numpy float32, with every operation rounded as azimuth's IEEE build rounds it
     divisions, N0-N2 from the vertex normals, UVk = UVs[index_k + UVOffset]
     when 0 <= index_k + UVOffset < len(UVs), else 0.
 
-The reference's importer itself cannot run here (it needs libxml2), so this
-restatement is pinned against the library's host scene builder, whose
-finished azimuth structs are what azimuth's own renderer consumes in the
-render parity tests.
+Pinned two ways: against azimuth's own ImportXML, run through the
+header-only reader of include/az_xmlreader.h on tests/scenes/box.xml (inline,
+ASCII PLY and binary PLY meshes; tests/test_xml_import.py), bit for bit; and
+against the library's host scene builder, whose finished azimuth structs are
+what azimuth's own renderer consumes in the render parity tests.
 """
 import numpy as np
 

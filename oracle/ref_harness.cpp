@@ -17,6 +17,10 @@
  *                         (src/azimuth_bvh.cpp:1-328)
  *   azref_*perlin*, azref_sample_texture, azref_eval_brdf
  *                         per-routine known-answer access
+ *   azref_import_xml      ImportXML (src/azimuth_xml.cpp:3021-3930) through
+ *                         the reader of include/az_xmlreader.h, with
+ *                         azref_scene_summary / azref_mesh_arrays to read
+ *                         back what it built
  *
  * It also defines the counter-RNG hooks that the patched Random01,
  * GetSampleCoord and TraceRay call (see oracle/shim/az_oracle_compat.h).
@@ -26,6 +30,7 @@
 #include <omp.h>
 #include <vector>
 #include "az_abi.h"
+#include "azimuth_gpu.h"
 #include "az_rng_oracle.h"
 
 /* ---- the reference structs and the C mirror must share one layout ---- */
@@ -372,6 +377,53 @@ void azref_scene_summary(const az_scene *AScene, uint32_t *Out9) {
     uint32_t V[9] = {S->MeshCount, S->MaterialCount, S->LightCount, Tris, Spheres, Instances, Emitters,
                      S->PathTrace, S->MaxRecursionDepth};
     memcpy(Out9, V, sizeof(V));
+}
+
+static void CollectTriangles(const entity *E, std::vector<const entity *> *Out) {
+    if (!E) return;
+    if (E->Type == EntityType_BVHNode) {
+        CollectTriangles(E->Left, Out);
+        CollectTriangles(E->Right, Out);
+    } else if (E->Type == EntityType_Triangle) {
+        Out->push_back(E);
+    }
+}
+
+/* What the importer's mesh loop (src/azimuth_xml.cpp:3669-3776) left in mesh
+ * M of an imported scene: Tris12 = Mesh->Triangles (P0, P1, P2, N per face,
+ * face order), Ents24 = the triangle entities under Mesh->BVH (P0, P1, P2,
+ * N0, N1, N2, UV0, UV1, UV2; BVH leaf order), *TotalArea, and the fields of
+ * the mesh's az_mesh_desc that come from the mesh itself.  Both arrays hold
+ * Mesh->TriangleCount rows; returns that count, or -1 when the BVH holds a
+ * different number of triangles. */
+int azref_mesh_arrays(const az_scene *AScene, uint32_t M, float *Tris12, float *Ents24, float *TotalArea,
+                      az_mesh_desc *Desc) {
+    const scene *S = (const scene *)AScene;
+    if (M >= S->MeshCount) return -1;
+    const mesh *Me = S->Meshes + M;
+    memcpy(Tris12, Me->Triangles, sizeof(triangle) * Me->TriangleCount);
+    std::vector<const entity *> Leaves;
+    CollectTriangles(Me->BVH, &Leaves);
+    if (Leaves.size() != Me->TriangleCount) return -1;
+    for (size_t I = 0; I < Leaves.size(); I++) {
+        const entity *E = Leaves[I];
+        const vec3 *V[6] = {&E->P0, &E->P1, &E->P2, &E->N0, &E->N1, &E->N2};
+        float *O = Ents24 + 24 * I;
+        for (int K = 0; K < 6; K++) { O[3 * K] = V[K]->x; O[3 * K + 1] = V[K]->y; O[3 * K + 2] = V[K]->z; }
+        const vec2 *U[3] = {&E->UV0, &E->UV1, &E->UV2};
+        for (int K = 0; K < 3; K++) { O[18 + 2 * K] = U[K]->x; O[19 + 2 * K] = U[K]->y; }
+    }
+    *TotalArea = Me->TotalArea;
+    Desc->uv_offset = Me->UVOffset;
+    Desc->shading_mode = (uint32_t)Me->ShadingMode;
+    Desc->material_index = Me->MaterialIndex;
+    Desc->texture_index = Me->TextureIndex;
+    Desc->is_emitter = Me->IsEmitter;
+    memcpy(&Desc->motion, &Me->MotionVector, sizeof(Desc->motion));
+    memcpy(&Desc->radiance, &Me->Radiance, sizeof(Desc->radiance));
+    memcpy(&Desc->transform, &Me->TransformationMatrix, sizeof(Desc->transform));
+    memcpy(&Desc->inv_transform, &Me->InvTransformationMatrix, sizeof(Desc->inv_transform));
+    return (int)Me->TriangleCount;
 }
 
 }  /* extern "C" */

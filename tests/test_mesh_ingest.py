@@ -2,7 +2,8 @@
 (src/azimuth_xml.cpp:3632-3750) as az_gpu_mesh_postprocess, bit for bit
 against the numpy restatement in oracle/mesh_oracle.py, which is itself pinned
 against the host scene builder's finished azimuth structs (the input of
-azimuth's renderer in the render parity tests); and a device scene built from
+azimuth's renderer in the render parity tests) and against azimuth's own
+importer (tests/test_xml_import.py); and a device scene built from
 the raw mesh soup (az_gpu_scene_create_from_meshes) against one built from
 the finished structs."""
 import ctypes as C
