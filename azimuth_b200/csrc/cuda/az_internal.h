@@ -79,6 +79,14 @@ int SoupRecords(const SoupWork &w, az_triangle *tris, az_face_attr *attrs, az_ve
 int SoupTriangles(const SoupWork &w, uint32_t face_base, uint32_t count, az_triangle *tris, cudaStream_t st);
 int SoupEmitScene(const SoupWork &w, const std::vector<IngestMesh> &meshes, azd::DevTri *d_tris,
                   azd::DevTriAttr *d_attr, cudaStream_t st);
+// A further placement of a soup mesh (a mesh instance besides the importer's
+// own one): `count` primitives copied from slot `src` to slot `dst` of the
+// device primitive arrays, with their instance entity set to `entity`.
+struct IngestCopy {
+    uint32_t src, dst, count, entity;
+};
+int SoupCopyPlacements(const std::vector<IngestCopy> &copies, azd::DevTri *d_tris, azd::DevTriAttr *d_attr,
+                       cudaStream_t st);
 
 // LBVH over `n` boxes (device arrays lo/hi of float4).  Writes nodes into
 // `nodes` starting at `node_base` (n-1 nodes, or 1 for n == 1), each inner

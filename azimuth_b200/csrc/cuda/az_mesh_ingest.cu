@@ -206,6 +206,31 @@ __global__ void k_ingest_emit_scene(const float *v, const uint32_t *faces, uint3
     attrs[o] = a;
 }
 
+// One thread per copied primitive; `start` holds each copy's first thread
+// (exclusive prefix of the counts), so a thread finds its copy by bisection.
+__global__ void k_ingest_copy(const IngestCopy *copies, const uint32_t *start, uint32_t nc, uint32_t total,
+                              azd::DevTri *tris, azd::DevTriAttr *attrs) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    int lo = 0, hi = (int)nc - 1, c = 0;
+    while (lo <= hi) {
+        const int mid = (lo + hi) >> 1;
+        if (start[mid] <= t) {
+            c = mid;
+            lo = mid + 1;
+        } else {
+            hi = mid - 1;
+        }
+    }
+    const IngestCopy &C = copies[c];
+    const uint32_t k = t - start[c];
+    if (k >= C.count) return;
+    tris[C.dst + k] = tris[C.src + k];
+    azd::DevTriAttr a = attrs[C.src + k];
+    a.entity = C.entity;
+    attrs[C.dst + k] = a;
+}
+
 template <typename T>
 struct Dev {
     T *p = nullptr;
@@ -401,6 +426,30 @@ int SoupEmitScene(const SoupWork &w, const std::vector<IngestMesh> &meshes, azd:
     AZ_CUDA_TRY(cudaMemcpyAsync(dm.p, meshes.data(), meshes.size() * sizeof(IngestMesh), cudaMemcpyHostToDevice, st));
     k_ingest_emit_scene<<<(w.nf + 255) / 256, 256, 0, st>>>(w.v.p, w.faces.p, w.nf, w.fn_unit.p, w.vn.p, w.uv.p, w.nuv,
                                                            w.ranges.p, w.nm, dm.p, d_tris, d_attr);
+    AZ_CUDA_TRY(cudaGetLastError());
+    AZ_CUDA_TRY(cudaStreamSynchronize(st));
+    return AZ_OK;
+}
+
+int SoupCopyPlacements(const std::vector<IngestCopy> &copies, azd::DevTri *d_tris, azd::DevTriAttr *d_attr,
+                       cudaStream_t st) {
+    if (copies.empty()) return AZ_OK;
+    std::vector<uint32_t> start(copies.size());
+    uint64_t total = 0;
+    for (size_t i = 0; i < copies.size(); i++) {
+        start[i] = (uint32_t)total;
+        total += copies[i].count;
+    }
+    if (total >= (1ull << 31)) return SetError(AZ_ERR_UNSUPPORTED, "more than 2^31 instanced primitives");
+    if (total == 0) return AZ_OK;
+    Dev<IngestCopy> dc;
+    Dev<uint32_t> ds;
+    AZ_CUDA_TRY(dc.alloc(copies.size()));
+    AZ_CUDA_TRY(ds.alloc(copies.size()));
+    AZ_CUDA_TRY(cudaMemcpyAsync(dc.p, copies.data(), copies.size() * sizeof(IngestCopy), cudaMemcpyHostToDevice, st));
+    AZ_CUDA_TRY(cudaMemcpyAsync(ds.p, start.data(), start.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    k_ingest_copy<<<(uint32_t)((total + 255) / 256), 256, 0, st>>>(dc.p, ds.p, (uint32_t)copies.size(),
+                                                                    (uint32_t)total, d_tris, d_attr);
     AZ_CUDA_TRY(cudaGetLastError());
     AZ_CUDA_TRY(cudaStreamSynchronize(st));
     return AZ_OK;

@@ -14,6 +14,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <set>
 #include <string>
 
 #include "az_internal.h"
@@ -101,6 +102,7 @@ struct HostGroup {
     std::vector<azd::DevTri> tris;
     std::vector<azd::DevTriAttr> attr;
     std::vector<uint32_t> soup_meshes;   // meshes of the soup whose triangles follow `tris` on the device
+    std::vector<uint32_t> soup_extra;    // then further placements of soup meshes (Flattener::extra)
     uint32_t soup_tris = 0;
     Box local;
 };
@@ -113,6 +115,14 @@ struct Flattener {
     std::map<GroupKey, uint32_t> group_of;
     int raw_group = -1;
     bool skip_meshes = false;            // mesh instances come from a soup instead
+    const az_mesh_soup *soup = nullptr;
+    std::set<uint32_t> soup_uids;        // UniqueEntityIDs of the soup meshes' own instances
+    // A mesh instance under BVHRoot that is not a soup mesh's own instance (a
+    // MeshInstance element of the scene file): soup mesh `mesh` placed again.
+    struct Extra {
+        uint32_t mesh, entity, group, out_base;
+    };
+    std::vector<Extra> extra;
     std::string err;
 
     // The group of an instance with these matrices and motion (one BLAS per
@@ -244,7 +254,22 @@ struct Flattener {
                     return AddTriangle(groups[raw_group], e, idx);
                 }
                 case AZ_Entity_MeshInstance: {
-                    if (skip_meshes) return true;
+                    if (skip_meshes) {
+                        // a soup mesh's own instance is made from the soup; any other
+                        // instance places soup mesh BaseMeshID again, with its own
+                        // (already composed) transform, motion and material
+                        if (soup_uids.count(e->UniqueEntityID)) return true;
+                        if (e->BaseMeshID >= soup->mesh_count) {
+                            err = "mesh instance's BaseMeshID is not a mesh of the soup";
+                            return false;
+                        }
+                        d.type = azd::ENT_INSTANCE;
+                        d.group = GroupFor(d);
+                        extra.push_back(Extra{e->BaseMeshID, idx, d.group, 0});
+                        ents.push_back(d);
+                        ent_box.push_back(Box());
+                        return true;
+                    }
                     d.type = azd::ENT_INSTANCE;
                     if (!e->Mesh) {
                         err = "mesh instance without mesh";
@@ -386,6 +411,10 @@ int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_
     Flattener F;
     F.s = scene;
     F.skip_meshes = soup != nullptr;
+    F.soup = soup;
+    if (soup && soup->mesh_count && !soup->meshes)
+        return SetError(AZ_ERR_INVALID_ARGUMENT, "mesh soup array missing");
+    for (uint32_t m = 0; soup && m < soup->mesh_count; m++) F.soup_uids.insert(soup->meshes[m].unique_entity_id);
     G->from_soup = soup != nullptr;
     if (!scene->BVHRoot && !soup) return SetError(AZ_ERR_INVALID_SCENE, "scene has no BVHRoot");
     if (!F.Run()) return SetError(AZ_ERR_INVALID_SCENE, F.err);
@@ -432,6 +461,14 @@ int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_
             HostGroup &g = F.groups[gi];
             g.soup_meshes.push_back(m);
             g.soup_tris += md.face_count;
+            g.local.grow(boxes[6 * m + 0], boxes[6 * m + 1], boxes[6 * m + 2]);
+            g.local.grow(boxes[6 * m + 3], boxes[6 * m + 4], boxes[6 * m + 5]);
+        }
+        for (uint32_t x = 0; x < F.extra.size(); x++) {
+            const uint32_t m = F.extra[x].mesh;
+            HostGroup &g = F.groups[F.extra[x].group];
+            g.soup_extra.push_back(x);
+            g.soup_tris += soup->meshes[m].face_count;
             g.local.grow(boxes[6 * m + 0], boxes[6 * m + 1], boxes[6 * m + 2]);
             g.local.grow(boxes[6 * m + 3], boxes[6 * m + 4], boxes[6 * m + 5]);
         }
@@ -587,6 +624,10 @@ int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_
             ingest[m].out_base = cursor;
             cursor += soup->meshes[m].face_count;
         }
+        for (uint32_t x : g.soup_extra) {
+            F.extra[x].out_base = cursor;
+            cursor += soup->meshes[F.extra[x].mesh].face_count;
+        }
         g.g.tri_end = cursor;
     }
     // TLAS primitives: spheres and groups
@@ -645,6 +686,10 @@ int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_
     if (soupw) {
         int r = SoupEmitScene(*soupw, ingest, d_tris_unsorted.p, d_attr_unsorted.p, st);
         if (r != AZ_OK) return r;
+        std::vector<IngestCopy> copies;
+        for (const auto &x : F.extra)
+            copies.push_back(IngestCopy{ingest[x.mesh].out_base, x.out_base, soup->meshes[x.mesh].face_count, x.entity});
+        if ((r = SoupCopyPlacements(copies, d_tris_unsorted.p, d_attr_unsorted.p, st)) != AZ_OK) return r;
         soupw.reset();   // its device arrays are no longer needed
     }
     if (!tlas.empty())

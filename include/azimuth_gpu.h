@@ -181,9 +181,13 @@ int az_gpu_mesh_postprocess(const az_mesh_soup *soup, az_vec3 *vertex_normals, a
  * post-processed on the GPU and go straight into the device scene, with no
  * host triangles or entity BVHs.  Everything else comes from `scene`:
  * materials, textures, lights, environment and settings, and the other
- * entities found under scene->BVHRoot (mesh instances there are ignored;
- * BVHRoot may be NULL).  An entity light whose entity is a mesh instance
- * takes its triangles and area from soup mesh Entity.BaseMeshID. */
+ * entities found under scene->BVHRoot (BVHRoot may be NULL).  A mesh instance
+ * there whose UniqueEntityID is a soup mesh's unique_entity_id is that mesh's
+ * own instance and comes from the soup; any other mesh instance (a
+ * MeshInstance element, src/azimuth_xml.cpp:2743-2797) places soup mesh
+ * BaseMeshID again with the instance's transform, motion and material.  An
+ * entity light whose entity is a mesh instance takes its triangles and area
+ * from soup mesh Entity.BaseMeshID. */
 int az_gpu_scene_create_from_meshes(const az_scene *scene, const az_mesh_soup *soup, const az_render_opts *opts,
                                     az_gpu_scene **out);
 

@@ -262,7 +262,7 @@ def test_gpu_mesh_postprocess_matches_the_importer(gpu, box):
 @pytest.mark.gpu
 def test_gpu_scene_from_the_importers_arrays(gpu, box):
     # az_gpu_scene_create_from_meshes: the importer's arrays post-processed on the GPU, the rest of
-    # the scene (materials, lights, spheres) from azimuth's structs
+    # the scene (materials, lights, spheres, the MeshInstance element) from azimuth's structs
     ref = ol.ref_film(box, seed=9)
     w, h = box.resolution()
     film, other = np.zeros((h, w, 4), np.float32), np.zeros((h, w, 4), np.float32)
@@ -275,7 +275,8 @@ def test_gpu_scene_from_the_importers_arrays(gpu, box):
 
 
 @pytest.mark.gpu
-def test_gpu_hits_on_the_imported_scene(gpu, box):
+@pytest.mark.parametrize("from_soup", [False, True], ids=["structs", "soup"])
+def test_gpu_hits_on_the_imported_scene(gpu, box, from_soup):
     rng = np.random.default_rng(4)
     n = 1 << 14
     o = rng.uniform((-0.95, 0.05, -0.95), (0.95, 1.95, 0.95), (n, 3)).astype(np.float32)
@@ -284,7 +285,7 @@ def test_gpu_hits_on_the_imported_scene(gpu, box):
     t = rng.uniform(0.0, 1.0, (n, 1)).astype(np.float32)
     rays = np.concatenate([o, d, t], axis=1)
     want = ol.closest_hit("ref", box, rays)
-    with az.GpuScene(box) as g:
+    with az.GpuScene(box, from_soup=from_soup) as g:
         got = g.closest_hit(rays)
     same = (got[0] == want[0]) & (got[1] == want[1]) & (got[2] == want[2])
     assert want[0].mean() > 0.75                 # the box is open only at the front (+z)
