@@ -368,7 +368,9 @@ int az_gpu_render_noalloc(az_gpu_scene *scene, az_pixel *film, const az_camera *
 /* Closest hit for `count` HOST rays (azimuth's RayEntityIntersection on the
  * scene root, src/azimuth_main.cpp:53-385).  Per ray: hit flag, UniqueEntityID
  * of the top-level entity, face id (entity.ID of the triangle hit inside a
- * mesh instance, else 0xFFFFFFFF) and world t.  Synchronous. */
+ * mesh instance, else 0xFFFFFFFF; in a scene built from a mesh soup, the
+ * face's index within its mesh, as azimuth's importer keeps no face id of its
+ * own, src/azimuth_xml.cpp:3695) and world t.  Synchronous. */
 int az_gpu_closest_hit(az_gpu_scene *scene, const az_ray3 *rays, uint32_t count, int32_t cull,
                        float hit_epsilon, uint32_t *out_hit, uint32_t *out_uid, uint32_t *out_face,
                        float *out_t, const az_render_opts *opts);
