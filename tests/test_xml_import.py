@@ -4,7 +4,9 @@ header-only reader (include/az_xmlreader.h) in place of libxml2, then the
 imported structs rendered and intersected by the GPU path against azimuth's
 own render code.  tests/scenes/box.xml holds an inline mesh, a light mesh, a
 point light, spheres, a smooth mesh from an ASCII PLY file with a quad face, a
-transformed instance of it, and a cube from a binary PLY file with motion."""
+transformed instance of it, and a cube from a binary PLY file with motion;
+tests/scenes/features.xml the lights, materials, textures and indexing
+options that box.xml leaves out."""
 import ctypes as C
 import os
 import shutil
@@ -57,11 +59,23 @@ def write_box_scene(dirpath, xml_text=None):
     return path
 
 
+def write_features_scene(dirpath):
+    """tests/scenes/features.xml with its image texture, a 16x12 PNG written by the library's writer."""
+    y, x = np.mgrid[0:12, 0:16]
+    rgb8 = np.stack([x * 16, y * 20, ((x // 4 + y // 4) % 2) * 200 + 30], -1).astype(np.uint8)
+    image = os.path.join(dirpath, "checker.png")
+    az.write_image(image, rgb8, az.FILE_PNG)
+    text = open(os.path.join(SCENES, "features.xml")).read().replace("@IMAGE@", image)
+    path = os.path.join(dirpath, "features.xml")
+    with open(path, "w") as f:
+        f.write(text)
+    return path
+
+
 class ImportedScene:
     """The scene, first camera and epsilons that ImportXML produced (azimuth's own structs)."""
 
     filter_type = az.FILTER_BOX       # RenderScene's filter (src/azimuth_main.cpp:1847)
-    perlin_gradients = None
 
     def __init__(self, path):
         L = ol.ref()
@@ -75,6 +89,11 @@ class ImportedScene:
         self.camera_count = n.value
         self.path = path
         self._soup = None
+        # the Perlin gradient table the import filled (a process-wide table in azimuth)
+        self._grad = np.zeros(768, np.float32)
+        L.azref_get_perlin_gradients.argtypes = [C.c_void_p]
+        L.azref_get_perlin_gradients(self._grad.ctypes.data)
+        self.perlin_gradients = self._grad.ctypes.data if self.ok else None
 
     def resolution(self):
         buf = (C.c_uint32 * 2).from_address(self.camera_ptr + 340)   # az_camera.Resolution
@@ -111,15 +130,20 @@ class ImportedScene:
         uvs, descs) with the other desc fields from azimuth's finished meshes."""
         root = ET.parse(self.path).getroot()
         verts = [np.array(root.find("VertexData").text.split(), np.float32).reshape(-1, 3)]
-        faces, uvs, ranges, plys = [], [np.zeros((0, 2), np.float32)], [], []
+        zb = root.find("ZeroBasedIndexing")
+        one_based = zb is None or zb.text.strip() != "true"
+        tc = root.find("TexCoordData")
+        faces, ranges, plys = [], [], []
+        uvs = [np.array(tc.text.split(), np.float32).reshape(-1, 2) if tc is not None else np.zeros((0, 2), np.float32)]
         for m in (e for e in root.find("Objects") if e.tag in ("Mesh", "LightMesh")):
             fe = m.find("Faces")
             if fe.get("plyFile"):
                 plys.append((len(ranges), fe.get("plyFile")))
                 ranges.append(None)
             else:
-                f = np.array(fe.text.split(), np.int64).reshape(-1, 3) - 1
-                ranges.append((sum(len(x) for x in faces), len(f), 0))
+                voff = int(fe.get("vertexOffset", 0))
+                f = np.array(fe.text.split(), np.int64).reshape(-1, 3) + voff - (1 if one_based else 0)
+                ranges.append((sum(len(x) for x in faces), len(f), int(fe.get("textureOffset", 0)) - voff))
                 faces.append(f)
         nverts = len(verts[0])
         for mi, path in plys:
@@ -181,11 +205,11 @@ def read_ply(path):
     return v8[:, :3].copy(), np.array(tris, np.int64), v8[:, 6:8].copy()
 
 
-def check_mesh_results(box, tris, attrs, areas):
+def check_mesh_results(scene, tris, attrs, areas):
     """The post-processed soup (face order) against azimuth's finished meshes, bit for bit."""
-    _, _, _, descs = box.soup()
+    _, _, _, descs = scene.soup()
     for mi, d in enumerate(descs):
-        want_tris, ents, want_area, _ = box.mesh_arrays(mi)
+        want_tris, ents, want_area, _ = scene.mesh_arrays(mi)
         b, n = d.face_base, d.face_count
         assert len(want_tris) == n
         assert np.array_equal(tris[b:b + n].view(np.uint32), want_tris.view(np.uint32))
@@ -205,6 +229,18 @@ def box(tmp_path_factory):
     return sc
 
 
+@pytest.fixture(scope="module")
+def features(tmp_path_factory):
+    sc = ImportedScene(write_features_scene(str(tmp_path_factory.mktemp("features"))))
+    assert sc.ok
+    return sc
+
+
+@pytest.fixture(params=["box", "features"])
+def imported(request):
+    return request.getfixturevalue(request.param)
+
+
 def test_importer_reads_the_scene(box):
     assert box.camera_count == 1
     assert box.resolution() == (48, 40) and box.sample_count() == 4
@@ -215,18 +251,27 @@ def test_importer_reads_the_scene(box):
                              "spheres": 2, "instances": 7, "emitters": 1, "path_trace": 1, "max_depth": 4}
 
 
-def test_restatement_renders_the_imported_scene_like_azimuth(box):
-    ref = ol.ref_film(box, seed=5, threads=1)
-    port = ol.port_film(box, seed=5, threads=1)
+def test_importer_reads_the_feature_scene(features):
+    assert features.camera_count == 1 and features.resolution() == (40, 32)
+    # lights: area, spot, directional, then the light sphere as an entity light (ambient is a
+    # scene colour); one instance per mesh plus the explicit MeshInstance
+    assert features.summary() == {"meshes": 5, "materials": 6, "lights": 4, "triangles": 10, "spheres": 3,
+                                  "instances": 6, "emitters": 0, "path_trace": 1, "max_depth": 5}
+    assert np.abs(features._grad).max() > 0     # the Perlin textures filled the gradient table
+
+
+def test_restatement_renders_the_imported_scene_like_azimuth(imported):
+    ref = ol.ref_film(imported, seed=5, threads=1)
+    port = ol.port_film(imported, seed=5, threads=1)
     assert np.array_equal(ref.view(np.uint32), port.view(np.uint32))
-    assert (ref[..., :3] > 0).mean() > 0.5     # the box is lit
+    assert (ref[..., :3] > 0).mean() > 0.5     # the scene is lit
 
 
-def test_mesh_restatement_matches_the_importer(box):
-    v, f, uv, descs = box.soup()
+def test_mesh_restatement_matches_the_importer(imported):
+    v, f, uv, descs = imported.soup()
     out = mo.postprocess(v, f, uv, [{"face_base": d.face_base, "face_count": d.face_count,
                                      "uv_offset": d.uv_offset} for d in descs])
-    check_mesh_results(box, out["triangles"], out["attrs"], out["total_area"])
+    check_mesh_results(imported, out["triangles"], out["attrs"], out["total_area"])
 
 
 @pytest.mark.parametrize("edit", [
@@ -243,10 +288,10 @@ def test_import_failures_are_reported(tmp_path, edit):
 
 
 @pytest.mark.gpu
-def test_gpu_renders_the_imported_scene(gpu, box):
-    ref = ol.ref_film(box, seed=9)
-    film = az.produce_image(box, seed=9)
-    other = az.produce_image(box, seed=10)
+def test_gpu_renders_the_imported_scene(gpu, imported):
+    ref = ol.ref_film(imported, seed=9)
+    film = az.produce_image(imported, seed=9)
+    other = az.produce_image(imported, seed=10)
     ok, _, relmse = ol.film_compare(film, ref, 1e-4)
     _, _, noise = ol.film_compare(other, ref, 1e-4)
     assert np.allclose(film[..., 3], ref[..., 3], rtol=1e-5, atol=1e-6)
@@ -254,19 +299,19 @@ def test_gpu_renders_the_imported_scene(gpu, box):
 
 
 @pytest.mark.gpu
-def test_gpu_mesh_postprocess_matches_the_importer(gpu, box):
-    out = az.mesh_postprocess(box)
-    check_mesh_results(box, out["triangles"], out["attrs"], out["total_area"])
+def test_gpu_mesh_postprocess_matches_the_importer(gpu, imported):
+    out = az.mesh_postprocess(imported)
+    check_mesh_results(imported, out["triangles"], out["attrs"], out["total_area"])
 
 
 @pytest.mark.gpu
-def test_gpu_scene_from_the_importers_arrays(gpu, box):
+def test_gpu_scene_from_the_importers_arrays(gpu, imported):
     # az_gpu_scene_create_from_meshes: the importer's arrays post-processed on the GPU, the rest of
     # the scene (materials, lights, spheres, the MeshInstance element) from azimuth's structs
-    ref = ol.ref_film(box, seed=9)
-    w, h = box.resolution()
+    ref = ol.ref_film(imported, seed=9)
+    w, h = imported.resolution()
     film, other = np.zeros((h, w, 4), np.float32), np.zeros((h, w, 4), np.float32)
-    with az.GpuScene(box, from_soup=True) as g:
+    with az.GpuScene(imported, from_soup=True) as g:
         g.render_host(film, seed=9)
         g.render_host(other, seed=10)
     ok, _, relmse = ol.film_compare(film, ref, 1e-4)
@@ -276,7 +321,7 @@ def test_gpu_scene_from_the_importers_arrays(gpu, box):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("from_soup", [False, True], ids=["structs", "soup"])
-def test_gpu_hits_on_the_imported_scene(gpu, box, from_soup):
+def test_gpu_hits_on_the_imported_scene(gpu, imported, from_soup):
     rng = np.random.default_rng(4)
     n = 1 << 14
     o = rng.uniform((-0.95, 0.05, -0.95), (0.95, 1.95, 0.95), (n, 3)).astype(np.float32)
@@ -284,8 +329,8 @@ def test_gpu_hits_on_the_imported_scene(gpu, box, from_soup):
     d /= np.linalg.norm(d, axis=1, keepdims=True)
     t = rng.uniform(0.0, 1.0, (n, 1)).astype(np.float32)
     rays = np.concatenate([o, d, t], axis=1)
-    want = ol.closest_hit("ref", box, rays)
-    with az.GpuScene(box, from_soup=from_soup) as g:
+    want = ol.closest_hit("ref", imported, rays)
+    with az.GpuScene(imported, from_soup=from_soup) as g:
         got = g.closest_hit(rays)
     # the importer sets every triangle entity's ID to 0 (src/azimuth_xml.cpp:3695); a soup-built
     # scene reports the face's index within its mesh instead
@@ -293,6 +338,6 @@ def test_gpu_hits_on_the_imported_scene(gpu, box, from_soup):
     if from_soup:
         mesh_hit = want[2][same] != 0xFFFFFFFF
         assert np.array_equal(got[2][same] == 0xFFFFFFFF, ~mesh_hit) and (got[2][same][mesh_hit] < 12).all()
-    assert want[0].mean() > 0.75                 # the box is open only at the front (+z)
+    assert want[0].mean() > 0.75                 # both boxes are open only at the front (+z)
     assert same.mean() >= 0.999
     assert np.array_equal(got[3][same].view(np.uint32), want[3][same].view(np.uint32))
