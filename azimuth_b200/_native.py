@@ -90,7 +90,7 @@ class SceneInfo(C.Structure):
                 ("bvh_depth", C.c_uint32), ("hierarchies", C.c_uint32), ("flatten_ms", C.c_float),
                 ("upload_ms", C.c_float), ("bvh_ms", C.c_float), ("total_ms", C.c_float),
                 ("ingest_ms", C.c_float), ("bvh_builder", C.c_uint32), ("queue_order", C.c_uint32),
-                ("variant", C.c_uint32)]
+                ("variant", C.c_uint32), ("shadow_variant", C.c_uint32)]
 
 
 class MeshDesc(C.Structure):

@@ -161,6 +161,7 @@ extern "C" int az_gpu_scene_info(const az_gpu_scene *scene, az_scene_info *out) 
     out->queue_order = ((G.order & kOrderShadow) ? (uint32_t)AZ_FLAG_ORDER_SHADOW : 0u) |
                        ((G.order & kOrderExtend) ? (uint32_t)AZ_FLAG_ORDER_EXTEND : 0u);
     out->variant = G.variant + 1;
+    out->shadow_variant = (G.shadow_variant < AZ_LAUNCH_VARIANTS ? G.shadow_variant : G.variant) + 1;
     return AZ_OK;
 }
 

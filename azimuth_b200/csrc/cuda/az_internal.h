@@ -51,6 +51,8 @@ struct GpuScene {
     WaveBuffers waves;           // reused across render calls on this scene
     uint32_t variant = 7;        // traversal launch configuration, 0-based (128 threads, 8 blocks/SM,
                                  // persistent fetching; az_gpu_autotune picks per scene)
+    uint32_t shadow_variant = 0xFFFFFFFFu;   // the shadow queries' own configuration (az_gpu_autotune;
+                                             // 0xFFFFFFFF: `variant`)
     uint32_t order = 0;          // queue ordering (kOrderShadow | kOrderExtend); az_gpu_autotune picks
     az_pixel *host_film_dev = nullptr;   // device film of az_gpu_render_host
     size_t host_film_bytes = 0;

@@ -1093,7 +1093,7 @@ static int RenderWave(const GpuScene &G, const CameraParams &cam, WaveBuffers &W
             int orc = OrderQueue(G, Q, W, L, 1, sms, st, rc);
             if (orc != AZ_OK) return orc;
         }
-        LaunchTraversalVariant(v, true, sms, G.dev, cam, Q, L, st);
+        LaunchTraversalVariant(cam.shadow_variant, true, sms, G.dev, cam, Q, L, st);
         if (timer) timer->Mark(st, 3);
         rc.launches += G.dev.full_light_queries ? 4 : 3;
         rc.extend_launches++;
@@ -1183,6 +1183,8 @@ int Render(GpuScene &G, az_pixel *film, const az_camera *camera, const az_epsilo
     cam.env_importance = opts && (opts->flags & AZ_FLAG_ENV_IMPORTANCE) && G.dev.env_rows ? 1u : 0u;
     cam.variant = opts && opts->variant ? opts->variant - 1 : G.variant;
     if (cam.variant >= kVariantCount) return SetError(AZ_ERR_INVALID_ARGUMENT, "unknown launch variant");
+    // a variant the caller names applies to both traversal kernels
+    cam.shadow_variant = (opts && opts->variant) || G.shadow_variant >= kVariantCount ? cam.variant : G.shadow_variant;
     cam.order = QueueOrder(G, opts);
     if (G.dev.max_depth + 1 > AZ_MAX_LEVELS - 2) return SetError(AZ_ERR_UNSUPPORTED, "MaxRecursionDepth above 61");
     uint64_t total = cam.npix * (uint64_t)cam.sqrt_spp * cam.sqrt_spp;
@@ -1337,9 +1339,37 @@ int Autotune(GpuScene &G, const az_camera *camera, const az_epsilon_values *eps,
             }
         }
     }
+    // then the shadow queries' configuration alone, with the extension's fixed
+    uint32_t best_shadow = best;
+    if (rc == AZ_OK) {
+        const uint32_t keep_variant = G.variant, keep_order = G.order, keep_shadow = G.shadow_variant;
+        G.variant = best;
+        G.order = best_order;
+        o.variant = 0;   // the scene's configuration, with the shadow variant under test
+        o.flags &= ~(uint32_t)AZ_FLAG_TIME_STAGES;
+        if (!(opts && (opts->flags & order_flags))) o.flags &= ~order_flags;
+        for (uint32_t v = 0; v < kVariantCount && rc == AZ_OK; v++) {
+            if (v == best) continue;
+            G.shadow_variant = v;
+            az_render_stats stats;
+            float vms = FLT_MAX;
+            for (int rep = 0; rep < 3 && rc == AZ_OK; rep++) {
+                rc = Render(G, film, camera, eps, band, filter, cull, &o, st, &stats);
+                if (rep > 0) vms = std::min(vms, stats.gpu_ms);
+            }
+            if (rc == AZ_OK && vms < best_ms) {
+                best_ms = vms;
+                best_shadow = v;
+            }
+        }
+        G.variant = keep_variant;
+        G.order = keep_order;
+        G.shadow_variant = keep_shadow;
+    }
     cudaFree(film);
     if (rc != AZ_OK) return rc;
     G.variant = best;
+    G.shadow_variant = best_shadow;
     G.order = best_order;
     if (best_out) *best_out = best + 1;
     if (ms_out) *ms_out = best_ms;
@@ -1483,6 +1513,8 @@ extern "C" int az_gpu_render_noalloc(az_gpu_scene *scene, az_pixel *film, const 
     if (rc != AZ_OK) return rc;
     cam.variant = opts && opts->variant ? opts->variant - 1 : G.variant;
     if (cam.variant >= kVariantCount) return SetError(AZ_ERR_INVALID_ARGUMENT, "unknown launch variant");
+    // a variant the caller names applies to both traversal kernels
+    cam.shadow_variant = (opts && opts->variant) || G.shadow_variant >= kVariantCount ? cam.variant : G.shadow_variant;
     const uint64_t total = cam.npix * (uint64_t)cam.sqrt_spp * cam.sqrt_spp;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -1501,7 +1533,7 @@ extern "C" int az_gpu_render_noalloc(az_gpu_scene *scene, az_pixel *film, const 
         for (uint32_t L = 1; L <= levels; L++) {
             LaunchTraversalVariant(cam.variant, false, sms, G.dev, cam, Q, L, st);
             LaunchShade(grid, G.dev, cam, Q, pos, L, st);
-            LaunchTraversalVariant(cam.variant, true, sms, G.dev, cam, Q, L, st);
+            LaunchTraversalVariant(cam.shadow_variant, true, sms, G.dev, cam, Q, L, st);
         }
         k_splat<<<(n + 255) / 256, 256, 0, st>>>(cam, Q, pos, n, film);
         AZ_CUDA_TRY(cudaGetLastError());

@@ -33,7 +33,8 @@ struct CameraParams {
     float eps_isect, eps_shadow;
     uint32_t cull;
     uint32_t count_traversal;
-    uint32_t variant;              // launch configuration of the traversal kernels
+    uint32_t variant;              // launch configuration of the extension queries
+    uint32_t shadow_variant;       // launch configuration of the shadow queries
     uint32_t env_importance;       // AZ_FLAG_ENV_IMPORTANCE
     uint32_t order;                // kOrderShadow | kOrderExtend: queues visited in sorted order
 };

@@ -224,7 +224,8 @@ def main():
         # the autotuner's sweep (BVH width 8/4/2 x launch variants) on a band of the frame
         t0 = time.time()
         tw, tv, tms = gs.autotune_scene(seed=seed_base(rank))
-        tune = {"bvh_width": tw, "variant": tv, "band_ms": tms, "seconds": time.time() - t0}
+        tune = {"bvh_width": tw, "variant": tv, "shadow_variant": gs.info()["shadow_variant"], "band_ms": tms,
+                "seconds": time.time() - t0}
 
     # a stream of our own: the wave launches are captured and replayed as CUDA
     # graphs, which the legacy default stream does not allow

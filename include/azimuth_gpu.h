@@ -130,6 +130,8 @@ typedef struct az_scene_info {
     uint32_t queue_order;        /* the scene's queue ordering: AZ_FLAG_ORDER_SHADOW | AZ_FLAG_ORDER_EXTEND bits
                                     (0: queue order); az_gpu_autotune sets it */
     uint32_t variant;            /* the scene's traversal launch configuration, 1-based */
+    uint32_t shadow_variant;     /* the shadow queries' launch configuration, 1-based (az_gpu_autotune
+                                    times it separately; a variant named in az_render_opts applies to both) */
 } az_scene_info;
 
 int az_gpu_scene_info(const az_gpu_scene *scene, az_scene_info *out);

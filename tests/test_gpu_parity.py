@@ -99,6 +99,9 @@ def test_autotune_picks_a_variant_and_renders_the_same(gpu):
         g.render_device(a.data_ptr(), seed=3, stats=True)
         v, ms = g.autotune(seed=3)
         assert 1 <= v <= az.LAUNCH_VARIANTS and ms > 0
+        info = g.info()
+        # the shadow queries are timed apart and may keep another configuration
+        assert info["variant"] == v and 1 <= info["shadow_variant"] <= az.LAUNCH_VARIANTS
         b = torch.zeros((h, w, 4), device="cuda")
         g.render_device(b.data_ptr(), seed=3, stats=True)
         # launch configuration changes scheduling only: same samples, same sums up to atomic order
