@@ -448,11 +448,18 @@ def exr_sibling_path(path):
     return buf.value.decode() if rc == 0 else None
 
 
-def render_batch(jobs, streams=0, flags=0, chunk_samples=0, device=0, largest_first=False):
-    """az_gpu_render_batch.  jobs: list of dicts with keys gpu_scene (GpuScene), film_ptr (device film of
-    the scene's camera resolution) and optionally guide (Guide), train, seed, scissor, and camera_ptr,
-    epsilons_ptr, filter_type (default: those of the GpuScene's host scene).  Returns
-    (per-job list of dicts done_ms/status/samples, batch stats dict)."""
+def render_tiles(jobs, flags=0, chunk_samples=0, device=0):
+    """az_gpu_render_tiles: jobs of ONE GpuScene (same dict keys as render_batch, no guide) rendered
+    together in shared waves of 4096-sample tiles.  Returns (per-job list, stats dict)."""
+    arr, o, st = _batch_args(jobs, 0, flags, chunk_samples, device, False)
+    rc = lib().az_gpu_render_tiles(arr, len(jobs), C.byref(o), C.byref(st))
+    per = [{"done_ms": arr[k].done_ms, "status": arr[k].status, "samples": arr[k].samples} for k in range(len(jobs))]
+    _check(rc, "az_gpu_render_tiles")
+    return per, {"samples": st.samples, "gpu_ms": st.gpu_ms, "p50_ms": st.p50_ms, "p99_ms": st.p99_ms,
+                 "jobs": st.jobs, "failed": st.failed, "streams": st.streams}
+
+
+def _batch_args(jobs, streams, flags, chunk_samples, device, largest_first):
     arr = (Job * len(jobs))()
     for k, j in enumerate(jobs):
         gs = j["gpu_scene"]
@@ -474,7 +481,15 @@ def render_batch(jobs, streams=0, flags=0, chunk_samples=0, device=0, largest_fi
     o.flags = flags
     o.chunk_samples = chunk_samples
     o.largest_first = 1 if largest_first else 0
-    st = BatchStats()
+    return arr, o, BatchStats()
+
+
+def render_batch(jobs, streams=0, flags=0, chunk_samples=0, device=0, largest_first=False):
+    """az_gpu_render_batch.  jobs: list of dicts with keys gpu_scene (GpuScene), film_ptr (device film of
+    the scene's camera resolution) and optionally guide (Guide), train, seed, scissor, and camera_ptr,
+    epsilons_ptr, filter_type (default: those of the GpuScene's host scene).  Returns
+    (per-job list of dicts done_ms/status/samples, batch stats dict)."""
+    arr, o, st = _batch_args(jobs, streams, flags, chunk_samples, device, largest_first)
     rc = lib().az_gpu_render_batch(arr, len(jobs), C.byref(o), C.byref(st))
     per = [{"done_ms": arr[k].done_ms, "status": arr[k].status, "samples": arr[k].samples} for k in range(len(jobs))]
     _check(rc, "az_gpu_render_batch")

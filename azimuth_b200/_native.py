@@ -170,6 +170,8 @@ def _declare(L):
         L.az_exr_sibling_path.restype = i32
         L.az_gpu_render_batch.argtypes = [vp, u32, C.POINTER(BatchOpts), C.POINTER(BatchStats)]
         L.az_gpu_render_batch.restype = i32
+        L.az_gpu_render_tiles.argtypes = [vp, u32, C.POINTER(BatchOpts), C.POINTER(BatchStats)]
+        L.az_gpu_render_tiles.restype = i32
         L.az_guide_create.argtypes = [vp, C.POINTER(GuideConfig), C.POINTER(vp)]
         L.az_guide_create.restype = i32
         L.az_guide_destroy.argtypes = [vp]

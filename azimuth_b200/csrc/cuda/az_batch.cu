@@ -181,3 +181,62 @@ extern "C" int az_gpu_render_batch(az_job *jobs, uint32_t n, const az_batch_opts
     if (first_rc != AZ_OK) return SetError(first_rc, first_msg);
     return AZ_OK;
 }
+
+extern "C" int az_gpu_render_tiles(az_job *jobs, uint32_t n, const az_batch_opts *opts, az_batch_stats *stats) {
+    if (stats) memset(stats, 0, sizeof(*stats));
+    if (n && !jobs) return SetError(AZ_ERR_INVALID_ARGUMENT, "null job array");
+    if (n == 0) return AZ_OK;
+    GpuScene *G = jobs[0].scene && jobs[0].scene->impl ? jobs[0].scene->impl : nullptr;
+    std::vector<TileJob> tj(n);
+    for (uint32_t i = 0; i < n; i++) {
+        const az_job &j = jobs[i];
+        if (!j.scene || j.scene->impl != G || !G)
+            return SetError(AZ_ERR_INVALID_ARGUMENT, "job " + std::to_string(i) + ": every job needs the same scene");
+        if (!j.film || !j.camera)
+            return SetError(AZ_ERR_INVALID_ARGUMENT, "job " + std::to_string(i) + ": null film or camera");
+        if (j.guide) return SetError(AZ_ERR_UNSUPPORTED, "job " + std::to_string(i) + ": guided jobs are not tiled");
+        tj[i].film = j.film;
+        tj[i].camera = j.camera;
+        tj[i].eps = j.epsilons;
+        tj[i].scissor = j.scissor;
+        tj[i].filter = j.filter_type;
+        tj[i].cull = j.backface_culling;
+        tj[i].seed = j.seed;
+    }
+    const int device = opts ? opts->device : 0;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return SetError(AZ_ERR_NO_DEVICE, "no CUDA device available");
+    if (device < 0 || device >= count || G->device != device)
+        return SetError(AZ_ERR_INVALID_ARGUMENT, "device ordinal out of range or not the scene's");
+    AZ_CUDA_TRY(cudaSetDevice(device));
+    az_render_opts ro;
+    memset(&ro, 0, sizeof(ro));
+    ro.device = device;
+    ro.flags = opts ? opts->flags : 0u;
+    ro.chunk_samples = opts ? opts->chunk_samples : 0u;
+    // a blocking stream: ordered after earlier work on the legacy default stream (films zeroed there)
+    cudaStream_t st = nullptr;
+    if (cudaStreamCreate(&st) != cudaSuccess) return SetError(AZ_ERR_CUDA, "stream creation");
+    az_render_stats rs;
+    int rc = RenderTiles(*G, tj, &ro, st, &rs);
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+    std::vector<float> done;
+    for (uint32_t i = 0; i < n; i++) {
+        jobs[i].status = rc;
+        jobs[i].samples = tj[i].samples;
+        jobs[i].done_ms = tj[i].done_ms;
+        done.push_back(tj[i].done_ms);
+    }
+    if (stats) {
+        std::sort(done.begin(), done.end());
+        stats->samples = rc == AZ_OK ? rs.samples : 0;
+        stats->gpu_ms = rc == AZ_OK ? rs.gpu_ms : 0.0f;
+        stats->p50_ms = done[(n - 1) / 2];
+        stats->p99_ms = done[std::min<size_t>(n - 1, (size_t)(0.99 * n))];
+        stats->jobs = n;
+        stats->failed = rc == AZ_OK ? 0u : n;
+        stats->streams = 1;
+    }
+    return rc;
+}

@@ -142,6 +142,23 @@ int Render(GpuScene &G, az_pixel *film, const az_camera *camera, const az_epsilo
            GuideState *guide = nullptr, bool train = false, WaveBuffers *wave_buffers = nullptr);
 int Autotune(GpuScene &G, const az_camera *camera, const az_epsilon_values *eps, az_scissor sc, int32_t filter,
              uint32_t cull, const az_render_opts *opts, cudaStream_t st, uint32_t *best_out, float *ms_out);
+// One render job of a tile render (az_gpu_render_tiles).
+struct TileJob {
+    az_pixel *film;              // device film of the job's camera
+    const az_camera *camera;
+    const az_epsilon_values *eps;
+    az_scissor scissor;
+    int32_t filter;
+    uint32_t cull;
+    uint64_t seed;
+    uint64_t samples = 0;        // written: the job's camera samples
+    float done_ms = 0.0f;        // written: device time from the call's start to its last wave's end
+};
+// Renders jobs of one scene together: their samples are cut into tiles, and
+// every wave takes the next tiles of all jobs from a device work queue, so one
+// chain of launches serves every job.  The jobs must share epsilons and culling.
+int RenderTiles(GpuScene &G, std::vector<TileJob> &jobs, const az_render_opts *opts, cudaStream_t st,
+                az_render_stats *stats);
 // OutputPixelsToFile's post-processing of a device film (az_post.cu).
 int PostProcess(const az_pixel *film, uint32_t w, uint32_t h, const az_tonemap *tm, float inv_gamma, uint32_t srgb,
                 uint32_t linear, float *rgb_out, uint8_t *rgb8_out, cudaStream_t st);

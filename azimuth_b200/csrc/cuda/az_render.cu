@@ -103,19 +103,12 @@ __device__ __forceinline__ void push_shadow(const WaveQueues &Q, uint32_t level,
     Q.smeta[i] = (kind << 30) | (uid & 0x3FFFFFFFu);
 }
 
-// GetSampleCoord + GetRayForPixel (src/azimuth_main.cpp:1135-1178).
-__global__ void k_camera(CameraParams cam, WaveQueues Q, uint64_t wave_start, uint32_t n) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    uint64_t seed = cam.seed;
-    if (Q.wave) {
-        wave_start = Q.wave[0];
-        n = (uint32_t)Q.wave[1];
-        seed = Q.wave[2];
-        if (i == 0) Q.counts[1] = n;   // the level-1 queue is the wave itself
-    }
-    if (i >= n) return;
+// GetSampleCoord + GetRayForPixel (src/azimuth_main.cpp:1135-1178) of camera
+// sample s into wave slot i.
+__device__ __forceinline__ void camera_node(const CameraParams &cam, const WaveQueues &Q, uint64_t s, uint64_t seed,
+                                            uint32_t i) {
     uint32_t row, col, sx, sy;
-    sample_of(cam, wave_start + i, row, col, sx, sy);
+    sample_of(cam, s, row, col, sx, sy);
     NodeRng rng;
     rng.init(seed, (row << 16) | col, (sy << 16) | sx, 0u, 0u);
     float cx = (float)col + (0.5f * cam.inv_sqrt + (float)sx * cam.inv_sqrt);
@@ -136,6 +129,38 @@ __global__ void k_camera(CameraParams cam, WaveQueues Q, uint64_t wave_start, ui
     Q.att[1][i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     Q.digits[1][i] = 0u;
     Q.accum[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+}
+
+__global__ void k_camera(CameraParams cam, WaveQueues Q, uint64_t wave_start, uint32_t n) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint64_t seed = cam.seed;
+    if (Q.wave) {
+        wave_start = Q.wave[0];
+        n = (uint32_t)Q.wave[1];
+        seed = Q.wave[2];
+        if (i == 0) Q.counts[1] = n;   // the level-1 queue is the wave itself
+    }
+    if (i >= n) return;
+    camera_node(cam, Q, wave_start + i, seed, i);
+}
+
+// Camera samples of a tile wave: each block takes the next tile of the wave's
+// work queue (`next`, zeroed before the launch) until the queue is empty.
+__global__ void k_camera_tiles(const Tile *tiles, uint32_t ntiles, uint32_t *next, WaveQueues Q, uint2 *slot_map) {
+    __shared__ uint32_t taken;
+    for (;;) {
+        if (threadIdx.x == 0) taken = atomicAdd(next, 1u);
+        __syncthreads();
+        const uint32_t t = taken;
+        __syncthreads();   // every thread has read `taken` before it is overwritten
+        if (t >= ntiles) return;
+        const Tile T = tiles[t];
+        const CameraParams &cam = Q.job_cams[T.job];
+        for (uint32_t k = threadIdx.x; k < T.count; k += blockDim.x) {
+            camera_node(cam, Q, (uint64_t)T.first + k, cam.seed, T.slot + k);
+            slot_map[T.slot + k] = make_uint2(T.job, T.first + k);
+        }
+    }
 }
 
 // Persistent traversal kernels.  Each warp reserves rays of the level's queue
@@ -305,7 +330,7 @@ __device__ __forceinline__ f3 ld3(const float *p) { return mk(p[0], p[1], p[2]);
 // src/azimuth_main.cpp:974-1130).  FEAT (DevScene.features) compiles out the
 // parts a scene cannot reach: textures, environment map, mirror/dielectric
 // branches, point/area/directional/spot lights.
-template <int BLOCK, uint32_t FEAT, bool GUIDED>
+template <int BLOCK, uint32_t FEAT, bool GUIDED, bool TILES = false>
 __global__ void __launch_bounds__(BLOCK) k_shade(DevScene S, CameraParams cam, WaveQueues Q, uint64_t wave_start,
                                                  uint32_t level) {
     constexpr bool TEX = FEAT & FEAT_TEXTURES, ENV = FEAT & FEAT_ENV, SPECIAL = FEAT & FEAT_SPECIAL,
@@ -334,8 +359,17 @@ __global__ void __launch_bounds__(BLOCK) k_shade(DevScene S, CameraParams cam, W
         h.tl = __uint_as_float(hh.y);
         h.prim = hh.z;
         h.ent = hh.w;
+        // the sample's pixel; in a tile wave (TILES) its own job's camera,
+        // whose seed and film size are read again where they are needed
         uint32_t row, col, sx, sy;
-        sample_of(cam, wave_start + slot, row, col, sx, sy);
+        uint32_t job = 0;
+        if (TILES) {
+            const uint2 js = Q.slot_map[slot];
+            job = js.x;
+            sample_of(Q.job_cams[job], js.y, row, col, sx, sy);
+        } else {
+            sample_of(cam, wave_start + slot, row, col, sx, sy);
+        }
         // path-guide training: this node is the only child of the vertex recorded
         // one level up, so the sample's sum now holds everything up to that
         // vertex's level
@@ -347,8 +381,11 @@ __global__ void __launch_bounds__(BLOCK) k_shade(DevScene S, CameraParams cam, W
         if (h.ent == 0xFFFFFFFFu) {
             // a miss returns 0, except for the primary ray, whose sample then takes
             // the background (RayTravelDistance == 0, src/azimuth_main.cpp:1374-1384)
-            if (level == 1)
-                add_accum(Q.accum, slot, background(S, r.d, (int32_t)cam.width - 1, (int32_t)cam.height - 1, row, col));
+            if (level == 1) {
+                const uint32_t fw = TILES ? Q.job_cams[job].width : cam.width;
+                const uint32_t fh = TILES ? Q.job_cams[job].height : cam.height;
+                add_accum(Q.accum, slot, background(S, r.d, (int32_t)fw - 1, (int32_t)fh - 1, row, col));
+            }
             continue;
         }
         const bool inside = (flags & PF_INSIDE) != 0;
@@ -365,7 +402,7 @@ __global__ void __launch_bounds__(BLOCK) k_shade(DevScene S, CameraParams cam, W
         }
         NodeRng rng;
         const uint32_t digits = Q.digits[buf][i];
-        rng.init(seed, (row << 16) | col, (sy << 16) | sx, digits, level);
+        rng.init(TILES ? Q.job_cams[job].seed : seed, (row << 16) | col, (sy << 16) | sx, digits, level);
         const Surface s = surface_at<TEX>(S, r, h);
         const DevMaterial &m = S.materials[e.material];
         f3 dcol = ld3(m.diffuse), scol = ld3(m.specular);
@@ -742,17 +779,11 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_shadow(DevScene S, CameraParams
 }
 
 // ComputeSampleWeight (src/azimuth_main.cpp:1209-1254) for every sample of the wave.
-__global__ void k_splat(CameraParams cam, WaveQueues Q, uint64_t wave_start, uint32_t n, az_pixel *film) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (Q.wave) {
-        wave_start = Q.wave[0];
-        n = (uint32_t)Q.wave[1];
-    }
-    if (i >= n) return;
-    if (Q.counts[AZ_COUNT_OVERFLOW]) return;   // the wave is re-run
+// ComputeSampleWeight (src/azimuth_main.cpp:1209-1254): sample s's sum `a`
+// into the film, box or Gaussian footprint.
+__device__ __forceinline__ void splat_sample(const CameraParams &cam, az_pixel *film, uint64_t s, float4 a) {
     uint32_t row, col, sx, sy;
-    sample_of(cam, wave_start + i, row, col, sx, sy);
-    float4 a = Q.accum[i];
+    sample_of(cam, s, row, col, sx, sy);
     float4 *f = reinterpret_cast<float4 *>(film);
     if (cam.filter == AZ_Filter_Box) {
         atomicAdd(&f[(size_t)row * cam.width + col], make_float4(a.x, a.y, a.z, 1.0f));
@@ -770,6 +801,26 @@ __global__ void k_splat(CameraParams cam, WaveQueues Q, uint64_t wave_start, uin
             float g = cam.g_norm * expf(cam.g_neg * d2);
             atomicAdd(&f[(size_t)gy * cam.width + gx], make_float4(a.x * g, a.y * g, a.z * g, g));
         }
+}
+
+__global__ void k_splat(CameraParams cam, WaveQueues Q, uint64_t wave_start, uint32_t n, az_pixel *film) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (Q.wave) {
+        wave_start = Q.wave[0];
+        n = (uint32_t)Q.wave[1];
+    }
+    if (i >= n) return;
+    if (Q.counts[AZ_COUNT_OVERFLOW]) return;   // the wave is re-run
+    splat_sample(cam, film, wave_start + i, Q.accum[i]);
+}
+
+// The samples of a tile wave, each into its own job's film.
+__global__ void k_splat_tiles(WaveQueues Q, uint32_t n, az_pixel *const *films) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (Q.counts[AZ_COUNT_OVERFLOW]) return;   // the wave is re-run
+    const uint2 js = Q.slot_map[i];
+    splat_sample(Q.job_cams[js.x], films[js.x], js.y, Q.accum[i]);
 }
 
 constexpr int kBlock = 128;
@@ -793,7 +844,8 @@ static_assert(kVariantCount == AZ_LAUNCH_VARIANTS, "variant table and header dis
 template <uint32_t F>
 void LaunchShadeF(int grid, const DevScene &S, const CameraParams &cam, const WaveQueues &Q, uint64_t start,
                   uint32_t L, cudaStream_t st, bool guided) {
-    if (guided) k_shade<kBlock, F, true><<<grid, kBlock, 0, st>>>(S, cam, Q, start, L);
+    if (Q.slot_map) k_shade<kBlock, F, false, true><<<grid, kBlock, 0, st>>>(S, cam, Q, start, L);   // tile wave
+    else if (guided) k_shade<kBlock, F, true><<<grid, kBlock, 0, st>>>(S, cam, Q, start, L);
     else k_shade<kBlock, F, false><<<grid, kBlock, 0, st>>>(S, cam, Q, start, L);
 }
 
@@ -1047,10 +1099,25 @@ static int OrderQueue(const GpuScene &G, const WaveQueues &Q, WaveBuffers &W, ui
     return AZ_OK;
 }
 
+// The device side of a tile wave (az_gpu_render_tiles): the wave's tiles, the
+// counter its camera kernel pulls them with, and the jobs' cameras and films.
+struct TileWave {
+    const Tile *tiles;
+    uint32_t ntiles;
+    uint32_t *next;
+    uint2 *slot_map;
+    const CameraParams *cams;
+    az_pixel *const *films;
+};
+
 static int RenderWave(const GpuScene &G, const CameraParams &cam, WaveBuffers &W, uint64_t start, uint32_t n,
                       az_pixel *film, cudaStream_t st, int sms, RenderCounters &rc, StageTimer *timer,
-                      GuideState *guide, bool train, bool capture = false) {
+                      GuideState *guide, bool train, bool capture = false, const TileWave *tw = nullptr) {
     WaveQueues Q = W.q;
+    if (tw) {
+        Q.slot_map = tw->slot_map;
+        Q.job_cams = tw->cams;
+    }
     if (capture) Q.wave = W.wave_dev;
     if (cam.order & kOrderExtend) Q.eorder = W.oidx_e;
     if (cam.order & kOrderShadow) Q.sorder = W.oidx_s;
@@ -1070,7 +1137,13 @@ static int RenderWave(const GpuScene &G, const CameraParams &cam, WaveBuffers &W
         uint32_t first = n;
         AZ_CUDA_TRY(cudaMemcpyAsync(Q.counts + 1, &first, sizeof(uint32_t), cudaMemcpyHostToDevice, st));
     }
-    k_camera<<<(n + 255) / 256, 256, 0, st>>>(cam, Q, start, n);
+    if (tw) {
+        AZ_CUDA_TRY(cudaMemsetAsync(tw->next, 0, sizeof(uint32_t), st));
+        k_camera_tiles<<<std::min<uint32_t>(tw->ntiles, (uint32_t)sms * 8), 256, 0, st>>>(tw->tiles, tw->ntiles,
+                                                                                          tw->next, Q, tw->slot_map);
+    } else {
+        k_camera<<<(n + 255) / 256, 256, 0, st>>>(cam, Q, start, n);
+    }
     rc.launches++;
     const int grid = sms * 16;
     const uint32_t v = cam.variant;
@@ -1103,7 +1176,8 @@ static int RenderWave(const GpuScene &G, const CameraParams &cam, WaveBuffers &W
         if (grc != AZ_OK) return grc;
         rc.launches += 7;
     }
-    k_splat<<<(n + 255) / 256, 256, 0, st>>>(cam, Q, start, n, film);
+    if (tw) k_splat_tiles<<<(n + 255) / 256, 256, 0, st>>>(Q, n, tw->films);
+    else k_splat<<<(n + 255) / 256, 256, 0, st>>>(cam, Q, start, n, film);
     rc.launches++;
     AZ_CUDA_TRY(cudaGetLastError());
     return AZ_OK;
@@ -1274,6 +1348,146 @@ int Render(GpuScene &G, az_pixel *film, const az_camera *camera, const az_epsilo
             stats->shade_ms = timer->ms[1];
             stats->shadow_ms = timer->ms[2];
         }
+    }
+    return AZ_OK;
+}
+
+int RenderTiles(GpuScene &G, std::vector<TileJob> &jobs, const az_render_opts *opts, cudaStream_t st,
+                az_render_stats *stats) {
+    if (stats) memset(stats, 0, sizeof(*stats));
+    if (jobs.empty()) return AZ_OK;
+    if (G.dev.max_depth + 1 > AZ_MAX_LEVELS - 2) return SetError(AZ_ERR_UNSUPPORTED, "MaxRecursionDepth above 61");
+    const uint32_t nj = (uint32_t)jobs.size();
+    std::vector<CameraParams> cams(nj);
+    uint64_t total = 0;
+    for (uint32_t j = 0; j < nj; j++) {
+        const TileJob &J = jobs[j];
+        if (!J.film || !J.camera) return SetError(AZ_ERR_INVALID_ARGUMENT, "tile job without film or camera");
+        CameraParams &c = cams[j];
+        int rc = SetupCamera(J.camera, J.scissor, J.filter, J.cull, J.eps, J.seed, c);
+        if (rc != AZ_OK) return rc;
+        c.count_traversal = opts && (opts->flags & AZ_FLAG_COUNT_TRAVERSAL) ? 1u : 0u;
+        c.env_importance = opts && (opts->flags & AZ_FLAG_ENV_IMPORTANCE) && G.dev.env_rows ? 1u : 0u;
+        c.variant = opts && opts->variant ? opts->variant - 1 : G.variant;
+        if (c.variant >= kVariantCount) return SetError(AZ_ERR_INVALID_ARGUMENT, "unknown launch variant");
+        c.shadow_variant = (opts && opts->variant) || G.shadow_variant >= kVariantCount ? c.variant : G.shadow_variant;
+        c.order = QueueOrder(G, opts);
+        // the traversal and shading kernels take these from the wave's first job
+        if (c.eps_isect != cams[0].eps_isect || c.eps_shadow != cams[0].eps_shadow || c.cull != cams[0].cull)
+            return SetError(AZ_ERR_INVALID_ARGUMENT, "the jobs of a tile render need the same epsilons and culling");
+        const uint64_t samples = c.npix * (uint64_t)c.sqrt_spp * c.sqrt_spp;
+        if (samples >= (1ull << 32)) return SetError(AZ_ERR_UNSUPPORTED, "a tile job with 2^32 samples or more");
+        jobs[j].samples = samples;
+        jobs[j].done_ms = 0.0f;
+        total += samples;
+    }
+    if (total == 0) return AZ_OK;
+    // every job's samples in runs of kTile consecutive sample indices (one
+    // sample number over a run of pixels: coherent camera rays), jobs in order
+    constexpr uint32_t kTile = 4096;
+    std::vector<Tile> tiles;
+    std::vector<size_t> last_tile(nj, 0);
+    for (uint32_t j = 0; j < nj; j++) {
+        for (uint64_t first = 0; first < jobs[j].samples; first += kTile)
+            tiles.push_back(Tile{j, (uint32_t)first, (uint32_t)std::min<uint64_t>(kTile, jobs[j].samples - first), 0u});
+        last_tile[j] = tiles.size();   // one past the job's last tile
+    }
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, G.device);
+    uint32_t chunk = opts && opts->chunk_samples ? opts->chunk_samples : (1u << 22);
+    chunk = std::max<uint32_t>(chunk, kTile);
+    const uint32_t per_node_shadow = G.dev.light_count + (G.dev.use_env_map ? 1u : 0u);
+    WaveBuffers &W = G.waves;
+    // device tables: cameras, films, this wave's tiles, the work-queue counter, slot -> (job, sample)
+    struct DevBuf {
+        void *p = nullptr;
+        ~DevBuf() {
+            if (p) cudaFree(p);
+        }
+    } d_cams, d_films, d_tiles, d_next, d_slots;
+    std::vector<az_pixel *> films(nj);
+    for (uint32_t j = 0; j < nj; j++) films[j] = jobs[j].film;
+    AZ_CUDA_TRY(cudaMalloc(&d_cams.p, nj * sizeof(CameraParams)));
+    AZ_CUDA_TRY(cudaMalloc(&d_films.p, nj * sizeof(az_pixel *)));
+    AZ_CUDA_TRY(cudaMalloc(&d_tiles.p, (chunk / kTile + 2 + nj) * sizeof(Tile)));
+    AZ_CUDA_TRY(cudaMalloc(&d_next.p, sizeof(uint32_t)));
+    AZ_CUDA_TRY(cudaMalloc(&d_slots.p, (size_t)chunk * sizeof(uint2)));
+    AZ_CUDA_TRY(cudaMemcpyAsync(d_cams.p, cams.data(), nj * sizeof(CameraParams), cudaMemcpyHostToDevice, st));
+    AZ_CUDA_TRY(cudaMemcpyAsync(d_films.p, films.data(), nj * sizeof(az_pixel *), cudaMemcpyHostToDevice, st));
+    struct Events {
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        ~Events() {
+            if (e0) cudaEventDestroy(e0);
+            if (e1) cudaEventDestroy(e1);
+        }
+    } ev;
+    AZ_CUDA_TRY(cudaEventCreate(&ev.e0));
+    AZ_CUDA_TRY(cudaEventCreate(&ev.e1));
+    AZ_CUDA_TRY(cudaEventRecord(ev.e0, st));
+    RenderCounters counters{};
+    std::vector<uint32_t> host_counts(AZ_COUNT_TOTAL);
+    size_t ti = 0;
+    while (ti < tiles.size()) {
+        // the wave: the next tiles while they fit in `chunk` samples (the
+        // tile table holds at most chunk / kTile + 2 + nj of them)
+        uint32_t n = 0;
+        size_t te = ti;
+        while (te < tiles.size() && n + tiles[te].count <= chunk) {
+            tiles[te].slot = n;
+            n += tiles[te].count;
+            te++;
+        }
+        const uint32_t ntiles = (uint32_t)(te - ti);
+        const uint32_t cap_q = std::max<uint32_t>(n + n / 2, 1024);
+        const uint32_t cap_s = std::max<uint32_t>(
+            (uint32_t)std::min<uint64_t>((uint64_t)cap_q * std::max(per_node_shadow, 1u), (uint64_t)n * 4), 1024);
+        int rc = W.Ensure(n, cap_q, cap_s);
+        if (rc != AZ_OK) return rc;
+        if (cams[0].order && (rc = W.EnsureOrder(std::max(W.q.cap_q, W.q.cap_s))) != AZ_OK) return rc;
+        AZ_CUDA_TRY(cudaMemcpyAsync(d_tiles.p, tiles.data() + ti, ntiles * sizeof(Tile), cudaMemcpyHostToDevice, st));
+        TileWave tw{(const Tile *)d_tiles.p, ntiles, (uint32_t *)d_next.p, (uint2 *)d_slots.p,
+                    (const CameraParams *)d_cams.p, (az_pixel *const *)d_films.p};
+        rc = RenderWave(G, cams[0], W, 0, n, nullptr, st, sms, counters, nullptr, nullptr, false, false, &tw);
+        if (rc != AZ_OK) return rc;
+        AZ_CUDA_TRY(cudaMemcpyAsync(host_counts.data(), W.q.counts, AZ_COUNT_TOTAL * sizeof(uint32_t),
+                                    cudaMemcpyDeviceToHost, st));
+        AZ_CUDA_TRY(cudaEventRecord(ev.e1, st));
+        AZ_CUDA_TRY(cudaEventSynchronize(ev.e1));
+        if (host_counts[AZ_COUNT_ERROR])
+            return SetError(AZ_ERR_CUDA, "BVH traversal exceeded its step limit (corrupt hierarchy)");
+        if (host_counts[AZ_COUNT_OVERFLOW]) {
+            // a queue overflowed: this wave wrote nothing; retry it with half the samples
+            if (n <= kTile) return SetError(AZ_ERR_OUT_OF_MEMORY, "wave queue overflow with one tile");
+            chunk = std::max<uint32_t>(n / 2, kTile);
+            counters.retries++;
+            continue;
+        }
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, ev.e0, ev.e1);
+        for (uint32_t j = 0; j < nj; j++)
+            if (last_tile[j] > ti && last_tile[j] <= te) jobs[j].done_ms = ms;
+        for (uint32_t L = 1; L < AZ_MAX_LEVELS; L++) {
+            counters.extend += host_counts[L];
+            counters.shadow += host_counts[AZ_COUNT_SHADOW + L];
+        }
+        counters.nodes += host_counts[AZ_COUNT_NODES];
+        counters.prims += host_counts[AZ_COUNT_NODES + 1];
+        counters.chunks++;
+        ti = te;
+    }
+    if (stats) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, ev.e0, ev.e1);
+        stats->samples = total;
+        stats->extend_rays = counters.extend;
+        stats->shadow_rays = counters.shadow;
+        stats->chunks = counters.chunks;
+        stats->retries = counters.retries;
+        stats->kernel_launches = counters.launches;
+        stats->gpu_ms = ms;
+        stats->node_visits = counters.nodes;
+        stats->prim_visits = counters.prims;
+        stats->extend_launches = (uint32_t)counters.extend_launches;
     }
     return AZ_OK;
 }

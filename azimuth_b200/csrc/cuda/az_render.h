@@ -64,6 +64,17 @@ struct WaveQueues {
     azd::GuideRecord *rec;                  // [level][n_rec] training vertices
     uint32_t n_rec, rec_levels;
     float guide_alpha_max;                  // cap on the learned selection probability (1: none)
+    // a tile wave (az_gpu_render_tiles) holds samples of several jobs of one
+    // scene: per wave slot its (job, sample index in the job), and each job's
+    // camera; null: every sample belongs to the kernels' `cam`
+    const uint2 *slot_map;
+    const CameraParams *job_cams;
+};
+
+// One tile of a tile wave: samples [first, first + count) of job `job`, at
+// wave slots [slot, slot + count).
+struct Tile {
+    uint32_t job, first, count, slot;
 };
 
 struct WaveBuffers {

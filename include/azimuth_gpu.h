@@ -298,6 +298,19 @@ typedef struct az_batch_stats {
  * (see each job's `status`). Synchronous. */
 int az_gpu_render_batch(az_job *jobs, uint32_t n, const az_batch_opts *opts, az_batch_stats *stats);
 
+/* The jobs of ONE device scene rendered together: every job's camera samples
+ * are cut into tiles of 4096, and each wave of the render takes the next tiles
+ * of all jobs from a device work queue (a camera kernel whose blocks pull
+ * tiles), so one chain of extend/shade/shadow launches per wave serves every
+ * job and small jobs share waves instead of running their own.  The jobs may
+ * differ in camera, resolution, spp, scissor, filter, seed and film; they
+ * must share the scene, the epsilon values and culling, and be plain renders
+ * (guide NULL).  Each job's film gets exactly what az_gpu_render with the
+ * job's seed would add (up to the order of float atomics).  opts->streams and
+ * largest_first are ignored; a job's done_ms is the end of the wave holding
+ * its last tile.  Synchronous. */
+int az_gpu_render_tiles(az_job *jobs, uint32_t n, const az_batch_opts *opts, az_batch_stats *stats);
+
 /* ---- Neural path guiding (the learned proposal; no counterpart in azimuth) ----
  *
  * A guide belongs to one device scene.  Rendered with az_gpu_render_guided,
