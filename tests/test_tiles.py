@@ -38,9 +38,10 @@ def test_tile_render_gives_every_job_its_own_render(gpu, scene_id):
     try:
         cams = [None, camera_copy(sc, 57, 21, 9), camera_copy(sc, 8, 8, 1), camera_copy(sc, 96, 70, 16)]
         specs = []   # (camera buffer or None, width, height, scissor or None, filter, seed)
+        full = lambda w, h: az.Scissor(az.Vec2u(w, h), az.Vec2u(0, 0))   # noqa: E731
         specs.append((None, 40, 30, None, sc.filter_type, 11))
-        specs.append((cams[1], 57, 21, None, az.FILTER_GAUSSIAN, 12))
-        specs.append((cams[2], 8, 8, None, az.FILTER_BOX, 13))
+        specs.append((cams[1], 57, 21, full(57, 21), az.FILTER_GAUSSIAN, 12))
+        specs.append((cams[2], 8, 8, full(8, 8), az.FILTER_BOX, 13))
         specs.append((cams[3], 96, 70, az.Scissor(az.Vec2u(90, 61), az.Vec2u(5, 3)), az.FILTER_BOX, 14))
         specs.append((None, 40, 30, az.Scissor(az.Vec2u(40, 12), az.Vec2u(0, 0)), az.FILTER_GAUSSIAN, 15))
         with az.GpuScene(sc) as g:
