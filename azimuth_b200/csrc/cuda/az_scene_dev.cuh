@@ -96,7 +96,7 @@ struct __align__(16) DevTexture {
     uint32_t wrap, filter, blend, bump;
     float scaling;            // Perlin ScalingFactor
     uint32_t appearance;
-    uint32_t perm_offset;     // into perlin_perm (256 entries)
+    uint32_t perm_offset;     // into perlin_perm (256 entries after the 256 words azimuth reads before them)
     uint32_t pad;
     unsigned long long texel_offset;  // bytes into texels
     unsigned long long pad2;

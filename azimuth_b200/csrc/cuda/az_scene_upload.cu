@@ -296,8 +296,10 @@ struct Flattener {
     }
 };
 
+// `valid_from`: the first host byte before `t` that may be read (the start of
+// the array holding `t`), for the words a Perlin hash reads before the table.
 azd::DevTexture ToDevTexture(const az_texture &t, std::vector<unsigned char> &texels, std::vector<uint32_t> &perms,
-                             std::string &err) {
+                             std::string &err, const void *valid_from = nullptr) {
     azd::DevTexture d;
     memset(&d, 0, sizeof(d));
     d.type = t.Type;
@@ -315,6 +317,20 @@ azd::DevTexture ToDevTexture(const az_texture &t, std::vector<unsigned char> &te
     if (t.Type == AZ_TextureType_PerlinNoise) {
         d.scaling = t.ScalingFactor;
         d.appearance = t.PerlinAppearance;
+        // azimuth's PerlinHash indexes the table with the signed K % 256, so a
+        // lattice point with K < 0 reads one of the 255 words in memory before
+        // Perm (src/azimuth_texture.h:134-144): the texture's own ImagePath, then
+        // the texture before it in the array.  The device table repeats those
+        // words before the table itself; words outside the caller's array (the
+        // reference reads whatever memory lies there) are 0.
+        const unsigned char *perm0 = reinterpret_cast<const unsigned char *>(&t.Perm[0]);
+        const unsigned char *lo = valid_from ? static_cast<const unsigned char *>(valid_from)
+                                             : reinterpret_cast<const unsigned char *>(&t);
+        for (int n = AZ_PERLIN_GRADIENT_SIZE; n >= 1; n--) {
+            uint32_t w = 0;
+            if (perm0 - lo >= (ptrdiff_t)(4 * n)) memcpy(&w, perm0 - 4 * n, 4);
+            perms.push_back(w);
+        }
         d.perm_offset = (uint32_t)perms.size();
         for (int i = 0; i < AZ_PERLIN_GRADIENT_SIZE; i++) perms.push_back(t.Perm[i]);
     } else if (t.Pixels && t.Width && t.Height) {
@@ -504,7 +520,7 @@ int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_
     std::vector<azd::DevTexture> texs;
     std::string err;
     for (uint32_t i = 0; i < scene->TextureCount; i++) {
-        texs.push_back(ToDevTexture(scene->Textures[i], texels, perms, err));
+        texs.push_back(ToDevTexture(scene->Textures[i], texels, perms, err, scene->Textures));
         uses_perlin |= scene->Textures[i].Type == AZ_TextureType_PerlinNoise;
     }
     uint32_t bg_idx = (uint32_t)texs.size();

@@ -15,9 +15,10 @@ __device__ __forceinline__ float perlin_weight(float v) {  // :146-154
 
 // PerlinHash (:134-144).  azimuth adds s32 lattice coordinates to u32 table
 // entries, so only the innermost K % 256 is a signed remainder; for K < 0 it
-// indexes before the table.  Here that remainder is taken modulo 256 instead.
+// indexes before the table, and the device table holds the 255 words azimuth
+// reads there (az_scene_upload.cu, ToDevTexture).
 __device__ __forceinline__ uint32_t perlin_hash(const uint32_t *P, int32_t i, int32_t j, int32_t k) {
-    uint32_t a = __ldg(P + (((k % 256) + 256) & 255));
+    uint32_t a = __ldg(P + (k % 256));
     uint32_t b = __ldg(P + (((uint32_t)j + a) & 255u));
     return __ldg(P + (((uint32_t)i + b) & 255u));
 }
