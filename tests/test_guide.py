@@ -213,8 +213,8 @@ def test_guided_render_is_unbiased(gpu):
 @pytest.mark.gpu
 def test_guided_render_beats_cosine_sampling(gpu):
     """Interior (light in room 1, camera in room 3): against an FP64-accumulated
-    converged plain render, the trained guide's images at equal samples have a
-    lower relMSE than plain cosine sampling (median of five renders each: one
+    converged plain render, trained guides' images at equal samples have a
+    lower relMSE than plain cosine sampling (medians over five renders each: one
     16-spp image's error is dominated by a few rare paths)."""
     import torch
     scene = az.generate_scene(az.SCENE_INTERIOR, seed=0, width=64, height=36, spp=16, detail=4)
@@ -234,17 +234,21 @@ def test_guided_render_beats_cosine_sampling(gpu):
             g.render_device(film.data_ptr(), seed=7 + s)
             e_plain.append(_relmse(_film_image(film), ref))
         e_guided = []
-        with _guide(g, seed=2) as guide:
-            for k in range(24):
-                film.zero_()
-                guide.render(film.data_ptr(), train=True, seed=2000 + k)
-            assert guide.info()["steps"] >= 24
-            for s in range(5):
-                film.zero_()
-                guide.render(film.data_ptr(), train=False, seed=7 + s)
-                guided = _film_image(film)
-                assert np.isfinite(guided).all()
-                e_guided.append(_relmse(guided, ref))
+        # training sums gradients with float atomics, so a trained network varies
+        # from run to run: three guides, 64 training renders each, and the median
+        # over all their renders
+        for gseed in (2, 3, 4):
+            with _guide(g, seed=gseed) as guide:
+                for k in range(64):
+                    film.zero_()
+                    guide.render(film.data_ptr(), train=True, seed=2000 + 100 * gseed + k)
+                assert guide.info()["steps"] >= 64
+                for s in range(5):
+                    film.zero_()
+                    guide.render(film.data_ptr(), train=False, seed=7 + s)
+                    guided = _film_image(film)
+                    assert np.isfinite(guided).all()
+                    e_guided.append(_relmse(guided, ref))
     e_plain, e_guided = float(np.median(e_plain)), float(np.median(e_guided))
     print("interior 64x36, 16 spp: median relMSE plain %.4g, guided %.4g" % (e_plain, e_guided))
     assert e_guided < e_plain
