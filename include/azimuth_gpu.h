@@ -66,7 +66,10 @@ typedef struct az_render_opts {
     void *stream;                   /* cudaStream_t to run on, or NULL for the library's own stream */
     int32_t device;                 /* CUDA device ordinal */
     uint32_t flags;                 /* AZ_FLAG_* */
-    uint32_t chunk_samples;         /* camera samples in flight per wave; 0 = automatic */
+    uint32_t chunk_samples;         /* camera samples in flight per wave; 0 = automatic: the power of two
+                                       from 2^22 to 2^26 whose wave queues (~350 bytes a sample) fit in a
+                                       quarter of the free device memory; they stay allocated with the
+                                       scene for its next render */
     uint32_t bvh_width;             /* az_gpu_scene_create: children per BVH node, 2, 4 or 8 (0 = 8) */
     uint32_t block_size;            /* reserved (0) */
     uint32_t variant;               /* traversal launch configuration 1..AZ_LAUNCH_VARIANTS (threads per
@@ -281,7 +284,8 @@ typedef struct az_batch_opts {
     int32_t device;
     uint32_t streams;               /* concurrent jobs; 0 = 4 */
     uint32_t flags;                 /* AZ_FLAG_* applied to every job */
-    uint32_t chunk_samples;         /* 0 = library default */
+    uint32_t chunk_samples;         /* 0 = 2^22 per job in az_gpu_render_batch; az_gpu_render_tiles as
+                                       az_render_opts.chunk_samples */
     uint32_t largest_first;         /* 0: shortest jobs first (low completion times); 1: largest first */
     uint32_t reserved[3];
 } az_batch_opts;
