@@ -1251,7 +1251,9 @@ static uint32_t QueueOrder(const GpuScene &G, const az_render_opts *opts) {
 // free device memory holds in wave queues, a power of two from 2^22 to 2^26.
 // Bigger waves keep the launches of the deep tree levels, where most paths
 // have ended, full (C1: 427 ms per frame at 2^22, 393 at 2^24, 383 at 2^26).
-static uint32_t DefaultWave(uint32_t per_node_shadow) {
+// The queues `W` already holds count as free, so that repeated renders of a
+// scene keep their wave size.
+static uint32_t DefaultWave(uint32_t per_node_shadow, const WaveBuffers &W) {
     uint64_t n = 1u << 22;
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
@@ -1262,7 +1264,9 @@ static uint32_t DefaultWave(uint32_t per_node_shadow) {
     // float4, digits, hit), shadow entries of 52 bytes, one float4 sum
     const double shadow_entries = std::min(1.5 * std::max(per_node_shadow, 1u), 4.0);
     const double per_sample = 1.5 * 168.0 + shadow_entries * 52.0 + 16.0;
-    const uint64_t fit = (uint64_t)((double)free_b / 4.0 / per_sample);
+    const double held = W.ptrs.empty() ? 0.0
+                                       : (double)W.q.cap_q * 168.0 + (double)W.q.cap_s * 52.0 + (double)W.chunk * 16.0;
+    const uint64_t fit = (uint64_t)(((double)free_b + held) / 4.0 / per_sample);
     while (n * 2 <= fit && n < (1u << 26)) n *= 2;
     return (uint32_t)n;
 }
@@ -1287,11 +1291,11 @@ int Render(GpuScene &G, az_pixel *film, const az_camera *camera, const az_epsilo
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, G.device);
     uint32_t per_node_shadow = G.dev.light_count + (G.dev.use_env_map ? 1u : 0u);
-    uint32_t chunk = opts && opts->chunk_samples ? opts->chunk_samples : DefaultWave(per_node_shadow);
+    WaveBuffers &W = wave_buffers ? *wave_buffers : G.waves;
+    uint32_t chunk = opts && opts->chunk_samples ? opts->chunk_samples : DefaultWave(per_node_shadow, W);
     // a training render updates the guide after every wave: smaller waves, more updates
     if (guide && train && !(opts && opts->chunk_samples)) chunk = 1u << 20;
     chunk = (uint32_t)std::min<uint64_t>(chunk, total);
-    WaveBuffers &W = wave_buffers ? *wave_buffers : G.waves;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (stats) {
         AZ_CUDA_TRY(cudaEventCreate(&e0));
@@ -1415,7 +1419,7 @@ int RenderTiles(GpuScene &G, std::vector<TileJob> &jobs, const az_render_opts *o
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, G.device);
     const uint32_t per_node_shadow = G.dev.light_count + (G.dev.use_env_map ? 1u : 0u);
-    uint32_t chunk = opts && opts->chunk_samples ? opts->chunk_samples : DefaultWave(per_node_shadow);
+    uint32_t chunk = opts && opts->chunk_samples ? opts->chunk_samples : DefaultWave(per_node_shadow, G.waves);
     chunk = std::max<uint32_t>(chunk, kTile);
     WaveBuffers &W = G.waves;
     // device tables: cameras, films, this wave's tiles, the work-queue counter, slot -> (job, sample)

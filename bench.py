@@ -311,7 +311,9 @@ def main():
     ext_prims = cnt["prim_visits"] * frac_ext
     # per query: ray read (32 B) + hit written (16 B); 80 B per wide node, 48 B per triangle
     bytes_per_frame = cnt["extend_rays"] * (32 + 16) + ext_nodes * 80 + ext_prims * 48
-    per_launch_bytes = bytes_per_frame / max(1, cnt["extend_launches"])
+    # one frame's bytes over the timed frame's extend launches (the counting pass
+    # renders the same frame, whatever its wave size)
+    per_launch_bytes = bytes_per_frame / max(1, stg["extend_launches"])
     per_launch_ms = extend_ms / max(1, extend_launches)
     achieved = per_launch_bytes / (per_launch_ms / 1000.0) / 1e9
     # DRAM bytes (read + write) per k_extend launch of this workload, from one
