@@ -1295,6 +1295,8 @@ int Render(GpuScene &G, az_pixel *film, const az_camera *camera, const az_epsilo
     uint32_t chunk = opts && opts->chunk_samples ? opts->chunk_samples : DefaultWave(per_node_shadow, W);
     // a training render updates the guide after every wave: smaller waves, more updates
     if (guide && train && !(opts && opts->chunk_samples)) chunk = 1u << 20;
+    // the visit counters are 32-bit per wave: counting renders keep 2^22-sample waves
+    if (cam.count_traversal && !(opts && opts->chunk_samples)) chunk = std::min(chunk, 1u << 22);
     chunk = (uint32_t)std::min<uint64_t>(chunk, total);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (stats) {

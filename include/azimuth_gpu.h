@@ -42,7 +42,8 @@ enum {
 /* az_render_opts.flags */
 enum {
     AZ_FLAG_NONE = 0,
-    AZ_FLAG_COUNT_TRAVERSAL = 1u << 0,  /* fill az_render_stats node/primitive visit counters */
+    AZ_FLAG_COUNT_TRAVERSAL = 1u << 0,  /* fill az_render_stats node/primitive visit counters (waves of at
+                                           most 2^22 samples unless chunk_samples is set) */
     AZ_FLAG_NO_GRAPH = 1u << 1,         /* launch the per-bounce stages directly, not as a CUDA graph */
     AZ_FLAG_TIME_STAGES = 1u << 2,      /* time each stage with CUDA events (az_render_stats *_ms) */
     AZ_FLAG_ENV_IMPORTANCE = 1u << 3,   /* environment light samples by one-sample MIS of a luminance CDF of
