@@ -39,9 +39,10 @@ METRIC = "Mpaths/s on 1 B200; equal-time relMSE guided vs plain GPU vs FP64 conv
 WORKLOAD = "dense mesh + importance sampling: 1,310,720-triangle Perlin-displaced icosphere in a Cornell box, " \
            "7 BRDFs, 1024x1024, 64 spp, depth 8, cosine sampling + area-light NEE, Gaussian filter"
 SCENE_ARGS = dict(scene_id=1, seed=0)
-# mean DRAM read + write of three k_extend launches of this workload's warm-up
-# frame (levels 5-7 of its fifth wave), measured with ncu (see the roofline below)
-EXTEND_DRAM_BYTES_PER_LAUNCH = (451426560 + 387705344 + 341759488) / 3.0
+# mean DRAM read + write of the nine k_extend launches (tree levels 1-9) of this
+# workload's first frame, one 2^26-sample wave, measured with ncu (see the
+# roofline below)
+EXTEND_DRAM_BYTES_PER_LAUNCH = 6610635235.6
 
 
 def parse():
@@ -317,7 +318,7 @@ def main():
     per_launch_ms = extend_ms / max(1, extend_launches)
     achieved = per_launch_bytes / (per_launch_ms / 1000.0) / 1e9
     # DRAM bytes (read + write) per k_extend launch of this workload, from one
-    # ncu capture of three launches of the warm-up frame (dram__bytes_read.sum +
+    # ncu capture of the nine launches of the first frame (dram__bytes_read.sum +
     # dram__bytes_write.sum, a single-pass capture of the full-size run; see
     # profiles/k_extend_traffic_dense_mesh_1024x1024_64spp.md).  ncu flushes the
     # caches before each captured launch, so this is the cold-cache figure.
