@@ -282,6 +282,10 @@ static inline int xmlTextReaderRead(xmlTextReaderPtr r) {
                 return -1;
             }
             std::string raw = d.substr(p, ve - p), val;
+            if (raw.find('<') != std::string::npos) {   // not allowed unescaped in an attribute value
+                r->failed = true;
+                return -1;
+            }
             for (char &c : raw)
                 if (c == '\t' || c == '\n' || c == '\r') c = ' ';   // attribute-value normalisation
             if (!az_xml_decode(raw, val)) {

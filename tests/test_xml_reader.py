@@ -87,6 +87,7 @@ def test_prolog_forms_are_skipped(walker, tmp_path):
     "<a b=1/>",                   # unquoted attribute value
     "<a><!-- open comment</a>",   # comment never closed
     "<a>&#0;</a>",                # character reference to NUL
+    "<a b='<c/>'/>",              # '<' inside an attribute value
 ])
 def test_malformed_input_is_an_error(walker, tmp_path, text):
     _, rc = walk(walker, tmp_path, text)
@@ -96,3 +97,19 @@ def test_malformed_input_is_an_error(walker, tmp_path, text):
 def test_missing_file_gives_no_reader(walker, tmp_path):
     res = subprocess.run([walker, str(tmp_path / "absent.xml")], capture_output=True, text=True)
     assert res.returncode == 1 and "open failed" in res.stdout
+
+
+def test_markup_inside_values_and_nesting(walker, tmp_path):
+    text = ('<a k = "x>y" j=\'z/\'><a><!--c--><b/></a>t<a/></a>')
+    nodes, rc = walk(walker, tmp_path, text, ["k", "j"])
+    assert nodes == [
+        (1, "a", 0, "-", "x>y", "z/"),
+        (1, "a", 0, "-", "-", "-"),
+        (8, "#comment", 1, "c", "-", "-"),
+        (1, "b", 0, "-", "-", "-"),
+        (15, "a", 0, "-", "-", "-"),
+        (3, "#text", 1, "t", "-", "-"),
+        (1, "a", 0, "-", "-", "-"),
+        (15, "a", 0, "-", "-", "-"),
+    ]
+    assert rc == 0
