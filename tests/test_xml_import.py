@@ -341,3 +341,30 @@ def test_gpu_hits_on_the_imported_scene(gpu, imported, from_soup):
     assert want[0].mean() > 0.75                 # both boxes are open only at the front (+z)
     assert same.mean() >= 0.999
     assert np.array_equal(got[3][same].view(np.uint32), want[3][same].view(np.uint32))
+
+
+def test_binary_vertex_and_face_files_import_like_inline(tmp_path, box):
+    # the importer's binaryFile forms (src/azimuth_xml.cpp:2397-2430, 2653-2697): a u32 count, then
+    # float xyz per vertex or u32 index triples per face
+    text = open(os.path.join(SCENES, "box.xml")).read()
+    v0, v1 = text.index("<VertexData>"), text.index("</VertexData>") + len("</VertexData>")
+    verts = np.array(text[v0 + len("<VertexData>"):v1 - len("</VertexData>")].split(), np.float32)
+    vpath = str(tmp_path / "verts.bin")
+    with open(vpath, "wb") as f:
+        f.write(struct.pack("<I", len(verts) // 3) + verts.tobytes())
+    text = text[:v0] + '<VertexData binaryFile="%s"/>' % vpath + text[v1:]
+    f0 = text.index("<Faces>")
+    f1 = text.index("</Faces>", f0) + len("</Faces>")
+    faces = np.array(text[f0 + len("<Faces>"):f1 - len("</Faces>")].split(), np.uint32)
+    fpath = str(tmp_path / "faces.bin")
+    with open(fpath, "wb") as f:
+        f.write(struct.pack("<I", len(faces) // 3) + faces.tobytes())
+    text = text[:f0] + '<Faces binaryFile="%s"/>' % fpath + text[f1:]
+    sc = ImportedScene(write_box_scene(str(tmp_path), text))
+    assert sc.ok
+    assert sc.summary() == box.summary()
+    for m in range(box.summary()["meshes"]):
+        a, b = sc.mesh_arrays(m), box.mesh_arrays(m)
+        assert np.array_equal(a[0].view(np.uint32), b[0].view(np.uint32))
+        assert np.array_equal(a[1].view(np.uint32), b[1].view(np.uint32))
+        assert a[2].view(np.uint32) == b[2].view(np.uint32)
