@@ -92,3 +92,12 @@ def test_tile_render_rejects_mixed_scenes_and_guides(gpu):
     finally:
         a.close()
         b.close()
+
+
+def test_tile_entry_checks_its_arguments_before_the_device():
+    lib = az.lib()
+    st = az.BatchStats()
+    assert lib.az_gpu_render_tiles(None, 0, None, C.byref(st)) == 0          # nothing to render
+    assert lib.az_gpu_render_tiles(None, 3, None, C.byref(st)) != 0          # jobs missing
+    jobs = (az.Job * 1)()                                                    # a job without a scene
+    assert lib.az_gpu_render_tiles(jobs, 1, None, C.byref(st)) != 0
