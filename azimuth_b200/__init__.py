@@ -18,7 +18,7 @@ import numpy as np
 
 from . import _native
 from ._native import (BatchOpts, BatchStats, GenParams, GeneratedScene, GuideConfig, Job, MeshDesc, MeshSoup,
-                      RenderOpts, RenderStats, SceneInfo, Scissor, Tonemap, Vec2u, Ray3, lib)
+                      RenderOpts, RenderStats, SceneArrays, SceneInfo, Scissor, Tonemap, Vec2u, Ray3, lib)
 
 GEN_SOUP_ONLY = 1   # az_gen_params.flags: meshes left as the importer's soup
 
@@ -39,7 +39,9 @@ FLAG_ENV_IMPORTANCE = 8
 FLAG_ORDER_SHADOW = 16     # visit shadow queues by origin cell
 FLAG_ORDER_EXTEND = 32     # visit extension queues by origin cell and direction octant
 FLAG_ORDER_NONE = 64       # queues in fill order
-LAUNCH_VARIANTS = 14   # AZ_LAUNCH_VARIANTS
+FLAG_SERIAL_LEVELS = 128   # visibility queries of a level before the next level's closest-hit queries
+FLAG_WATERTIGHT = 256      # triangles by the watertight test (production mode) instead of azimuth's Cramer test
+LAUNCH_VARIANTS = 18   # AZ_LAUNCH_VARIANTS
 
 STATUS = {0: "AZ_OK", 1: "AZ_ERR_INVALID_ARGUMENT", 2: "AZ_ERR_INVALID_SCENE", 3: "AZ_ERR_OUT_OF_MEMORY",
           4: "AZ_ERR_CUDA", 5: "AZ_ERR_TIMEOUT", 6: "AZ_ERR_UNSUPPORTED", 7: "AZ_ERR_NO_DEVICE"}
@@ -154,8 +156,10 @@ BVH_LBVH, BVH_PLOC = 1, 2   # az_render_opts.bvh_builder
 
 
 def make_opts(scene=None, seed=0, stream=None, device=0, flags=0, chunk_samples=0, block_size=0, variant=0,
-              bvh_width=0, bvh_leaf=0, bvh_builder=0):
+              bvh_width=0, bvh_leaf=0, bvh_builder=0, sample_part=0, sample_parts=0):
     o = RenderOpts()
+    o.sample_part = sample_part
+    o.sample_parts = sample_parts
     o.bvh_builder = bvh_builder
     o.variant = variant
     o.bvh_width = bvh_width
@@ -207,6 +211,13 @@ class GpuScene:
         _check(lib().az_gpu_scene_info(self._h, C.byref(si)), "az_gpu_scene_info")
         return {k: getattr(si, k) for k, _ in SceneInfo._fields_}
 
+    def arrays(self):
+        """az_gpu_scene_arrays: device addresses and counts of the wide nodes and triangles, the top-level
+        root and the root of a single top-level group."""
+        sa = SceneArrays()
+        _check(lib().az_gpu_scene_arrays(self._h, C.byref(sa)), "az_gpu_scene_arrays")
+        return {k: getattr(sa, k) for k, _ in SceneArrays._fields_ if k != "reserved"}
+
     def autotune(self, seed=0, stream=None):
         """az_gpu_autotune: picks the traversal launch variant for this scene; returns (variant, ms)."""
         o = make_opts(self.scene, seed=seed, stream=stream, device=self.device)
@@ -231,16 +242,31 @@ class GpuScene:
         return w.value, v.value, ms.value
 
     def render_device(self, film_ptr, camera_ptr=None, scissor=None, filter_type=None, seed=0, stream=None,
-                      stats=False, flags=0, chunk_samples=0, variant=0):
-        """az_gpu_render into a DEVICE film pointer; returns az_render_stats as a dict if stats."""
+                      stats=False, flags=0, chunk_samples=0, variant=0, sample_part=0, sample_parts=0):
+        """az_gpu_render into a DEVICE film pointer; returns az_render_stats as a dict if stats.
+        sample_part / sample_parts: render one of that many equal ranges of the camera-sample sequence."""
         sc = scissor or full_scissor(self.scene)
         ft = self.scene.filter_type if filter_type is None else filter_type
         o = make_opts(self.scene, seed=seed, stream=stream, device=self.device, flags=flags,
-                      chunk_samples=chunk_samples, variant=variant)
+                      chunk_samples=chunk_samples, variant=variant, sample_part=sample_part,
+                      sample_parts=sample_parts)
         st = RenderStats() if stats else None
         _check(lib().az_gpu_render(self._h, film_ptr, camera_ptr or self.scene.camera_ptr, self.scene.epsilons_ptr,
                                    sc, ft, 0, C.byref(o), C.byref(st) if st is not None else None),
                "az_gpu_render")
+        return _stats(st)
+
+    def render_samples(self, samples_ptr, camera_ptr=None, scissor=None, seed=0, stream=None, stats=False, flags=0,
+                       chunk_samples=0, variant=0):
+        """az_gpu_render_samples: every camera sample's radiance (4 floats, DEVICE pointer) in the scissor's
+        sample order (sample number * scissor pixels + pixel) instead of a film."""
+        sc = scissor or full_scissor(self.scene)
+        o = make_opts(self.scene, seed=seed, stream=stream, device=self.device, flags=flags,
+                      chunk_samples=chunk_samples, variant=variant)
+        st = RenderStats() if stats else None
+        _check(lib().az_gpu_render_samples(self._h, samples_ptr, camera_ptr or self.scene.camera_ptr,
+                                           self.scene.epsilons_ptr, sc, 0, C.byref(o),
+                                           C.byref(st) if st is not None else None), "az_gpu_render_samples")
         return _stats(st)
 
     def render_host(self, pixels, camera_ptr=None, scissor=None, filter_type=None, seed=0, stream=None,
@@ -256,15 +282,16 @@ class GpuScene:
                                         sc, ft, 0, C.byref(o), C.byref(st)), "az_gpu_render_host")
         return _stats(st)
 
-    def closest_hit(self, rays, cull=0, eps=0.0):
-        """rays: numpy (N, 7) float32 [origin, direction, T]; returns (hit, uid, face, t)."""
+    def closest_hit(self, rays, cull=0, eps=0.0, flags=0):
+        """rays: numpy (N, 7) float32 [origin, direction, T]; returns (hit, uid, face, t).
+        flags: FLAG_WATERTIGHT for the watertight triangle test."""
         rays = np.ascontiguousarray(rays, np.float32)
         n = rays.shape[0]
         hit = np.zeros(n, np.uint32)
         uid = np.zeros(n, np.uint32)
         face = np.zeros(n, np.uint32)
         t = np.zeros(n, np.float32)
-        o = make_opts(self.scene, device=self.device)
+        o = make_opts(self.scene, device=self.device, flags=flags)
         _check(lib().az_gpu_closest_hit(self._h, rays.ctypes.data, n, cull, eps, hit.ctypes.data, uid.ctypes.data,
                                         face.ctypes.data, t.ctypes.data, C.byref(o)), "az_gpu_closest_hit")
         return hit, uid, face, t
@@ -449,8 +476,8 @@ def exr_sibling_path(path):
 
 
 def render_tiles(jobs, flags=0, chunk_samples=0, device=0):
-    """az_gpu_render_tiles: jobs of ONE GpuScene (same dict keys as render_batch, no guide) rendered
-    together in shared waves of 4096-sample tiles.  Returns (per-job list, stats dict)."""
+    """az_gpu_render_tiles: jobs (same dict keys as render_batch, no guide; any GpuScenes of one device)
+    rendered together in shared waves of 4096-sample tiles.  Returns (per-job list, stats dict)."""
     arr, o, st = _batch_args(jobs, 0, flags, chunk_samples, device, False)
     rc = lib().az_gpu_render_tiles(arr, len(jobs), C.byref(o), C.byref(st))
     per = [{"done_ms": arr[k].done_ms, "status": arr[k].status, "samples": arr[k].samples} for k in range(len(jobs))]
@@ -459,7 +486,7 @@ def render_tiles(jobs, flags=0, chunk_samples=0, device=0):
                  "jobs": st.jobs, "failed": st.failed, "streams": st.streams}
 
 
-def _batch_args(jobs, streams, flags, chunk_samples, device, largest_first):
+def _batch_args(jobs, streams, flags, chunk_samples, device, largest_first, tiles=False):
     arr = (Job * len(jobs))()
     for k, j in enumerate(jobs):
         gs = j["gpu_scene"]
@@ -481,15 +508,17 @@ def _batch_args(jobs, streams, flags, chunk_samples, device, largest_first):
     o.flags = flags
     o.chunk_samples = chunk_samples
     o.largest_first = 1 if largest_first else 0
+    o.tiles = 1 if tiles else 0
     return arr, o, BatchStats()
 
 
-def render_batch(jobs, streams=0, flags=0, chunk_samples=0, device=0, largest_first=False):
+def render_batch(jobs, streams=0, flags=0, chunk_samples=0, device=0, largest_first=False, tiles=False):
     """az_gpu_render_batch.  jobs: list of dicts with keys gpu_scene (GpuScene), film_ptr (device film of
     the scene's camera resolution) and optionally guide (Guide), train, seed, scissor, and camera_ptr,
-    epsilons_ptr, filter_type (default: those of the GpuScene's host scene).  Returns
+    epsilons_ptr, filter_type (default: those of the GpuScene's host scene).  tiles: the plain jobs
+    render together in tile waves on one stream while the other streams take the guided jobs.  Returns
     (per-job list of dicts done_ms/status/samples, batch stats dict)."""
-    arr, o, st = _batch_args(jobs, streams, flags, chunk_samples, device, largest_first)
+    arr, o, st = _batch_args(jobs, streams, flags, chunk_samples, device, largest_first, tiles)
     rc = lib().az_gpu_render_batch(arr, len(jobs), C.byref(o), C.byref(st))
     per = [{"done_ms": arr[k].done_ms, "status": arr[k].status, "samples": arr[k].samples} for k in range(len(jobs))]
     _check(rc, "az_gpu_render_batch")
@@ -503,7 +532,8 @@ def _stats(st):
     return {"samples": st.samples, "extend_rays": st.extend_rays, "shadow_rays": st.shadow_rays,
             "chunks": st.chunks, "retries": st.retries, "kernel_launches": st.kernel_launches,
             "gpu_ms": st.gpu_ms, "extend_ms": st.extend_ms, "shade_ms": st.shade_ms, "shadow_ms": st.shadow_ms,
-            "node_visits": st.node_visits, "prim_visits": st.prim_visits, "extend_launches": st.extend_launches}
+            "node_visits": st.node_visits, "prim_visits": st.prim_visits, "extend_launches": st.extend_launches,
+            "shadow_node_visits": st.shadow_node_visits, "shadow_prim_visits": st.shadow_prim_visits}
 
 
 def device_info(device=0):

@@ -46,7 +46,8 @@ class RenderOpts(C.Structure):
     _fields_ = [("seed", C.c_uint64), ("perlin_gradients", C.c_void_p), ("stream", C.c_void_p),
                 ("device", C.c_int32), ("flags", C.c_uint32), ("chunk_samples", C.c_uint32),
                 ("bvh_width", C.c_uint32), ("block_size", C.c_uint32), ("variant", C.c_uint32),
-                ("bvh_leaf", C.c_uint32), ("bvh_builder", C.c_uint32), ("reserved", C.c_uint32 * 2)]
+                ("bvh_leaf", C.c_uint32), ("bvh_builder", C.c_uint32), ("sample_part", C.c_uint32),
+                ("sample_parts", C.c_uint32)]
 
 
 class Tonemap(C.Structure):
@@ -63,7 +64,7 @@ class Job(C.Structure):
 
 class BatchOpts(C.Structure):
     _fields_ = [("device", C.c_int32), ("streams", C.c_uint32), ("flags", C.c_uint32), ("chunk_samples", C.c_uint32),
-                ("largest_first", C.c_uint32), ("reserved", C.c_uint32 * 3)]
+                ("largest_first", C.c_uint32), ("tiles", C.c_uint32), ("reserved", C.c_uint32 * 2)]
 
 
 class BatchStats(C.Structure):
@@ -81,7 +82,9 @@ class RenderStats(C.Structure):
                 ("chunks", C.c_uint32), ("retries", C.c_uint32), ("kernel_launches", C.c_uint64),
                 ("gpu_ms", C.c_float), ("extend_ms", C.c_float), ("shade_ms", C.c_float),
                 ("shadow_ms", C.c_float), ("node_visits", C.c_uint64), ("prim_visits", C.c_uint64),
-                ("extend_launches", C.c_uint32), ("reserved", C.c_uint32 * 3)]
+                ("extend_launches", C.c_uint32), ("reserved0", C.c_uint32),
+                ("shadow_node_visits", C.c_uint64), ("shadow_prim_visits", C.c_uint64),
+                ("reserved", C.c_uint32 * 2)]
 
 
 class SceneInfo(C.Structure):
@@ -91,6 +94,12 @@ class SceneInfo(C.Structure):
                 ("upload_ms", C.c_float), ("bvh_ms", C.c_float), ("total_ms", C.c_float),
                 ("ingest_ms", C.c_float), ("bvh_builder", C.c_uint32), ("queue_order", C.c_uint32),
                 ("variant", C.c_uint32), ("shadow_variant", C.c_uint32)]
+
+
+class SceneArrays(C.Structure):
+    _fields_ = [("wide_nodes", C.c_void_p), ("wide_node_count", C.c_uint64), ("triangles", C.c_void_p),
+                ("triangle_count", C.c_uint64), ("tlas_root", C.c_uint32), ("single_group_root", C.c_uint32),
+                ("reserved", C.c_uint32 * 4)]
 
 
 class MeshDesc(C.Structure):
@@ -137,6 +146,8 @@ def _declare(L):
         L.az_gpu_scene_create.restype = i32
         L.az_gpu_scene_destroy.argtypes = [vp]
         L.az_gpu_scene_destroy.restype = None
+        L.az_gpu_scene_arrays.argtypes = [vp, C.POINTER(SceneArrays)]
+        L.az_gpu_scene_arrays.restype = i32
         L.az_gpu_scene_info.argtypes = [vp, C.POINTER(SceneInfo)]
         L.az_gpu_scene_info.restype = i32
         L.az_gpu_scene_create_from_meshes.argtypes = [vp, vp, C.POINTER(RenderOpts), C.POINTER(vp)]
@@ -149,6 +160,9 @@ def _declare(L):
         L.az_gpu_render_host.argtypes = [vp, vp, vp, vp, Scissor, i32, u32, C.POINTER(RenderOpts),
                                          C.POINTER(RenderStats)]
         L.az_gpu_render_host.restype = i32
+        L.az_gpu_render_samples.argtypes = [vp, vp, vp, vp, Scissor, u32, C.POINTER(RenderOpts),
+                                            C.POINTER(RenderStats)]
+        L.az_gpu_render_samples.restype = i32
         L.az_gpu_autotune.argtypes = [vp, vp, vp, Scissor, i32, u32, C.POINTER(RenderOpts), vp, vp]
         L.az_gpu_autotune.restype = i32
         L.az_gpu_autotune_scene.argtypes = [vp, vp, vp, vp, Scissor, i32, u32, C.POINTER(RenderOpts), vp, vp, vp]

@@ -3,13 +3,19 @@
 Host C++ (scene assembly, generators, the RenderScene-style host API) is
 compiled with g++ and ``-ffp-contract=off`` so its float sums round like
 azimuth's; CUDA sources are compiled by nvcc for sm_100a only
-(``-gencode arch=compute_100a,code=sm_100a``).  The result links the CUDA
+(``-gencode arch=compute_100a,code=sm_100a``), side by side.  CUDA files are
+compiled without FMA contraction (``--fmad=false``: primitive tests, mesh
+ingestion, BVH quantisation and the post-process round like azimuth's scalar
+code), except the ones in ``CONTRACTED``, whose results are compared within a
+tolerance and feed no bit-exact distance: the shading stage and the path
+guide.  The result links the CUDA
 runtime statically, so the library needs only the driver and the system zlib
 at run time.
 
 Usage: python -m azimuth_b200.build [--force] [--debug]
 """
 import argparse
+import concurrent.futures
 import glob
 import os
 import subprocess
@@ -22,6 +28,8 @@ OBJ = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libazimuth_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# CUDA files compiled with FMA contraction (see above)
+CONTRACTED = {"az_shade_kernel.cu", "az_guide.cu"}
 INCLUDES = ["-I", os.path.join(REPO, "include"), "-I", os.path.join(CSRC, "host"), "-I", os.path.join(CSRC, "cuda")]
 
 
@@ -64,17 +72,22 @@ def build(force=False, debug=False, verbose=False):
                  + opt + INCLUDES + ["-I", "/usr/local/cuda/include", src, "-o", obj])
         objs.append(obj)
     cu_srcs = sorted(glob.glob(os.path.join(CSRC, "cuda", "*.cu")))
+    jobs = []
     for src in cu_srcs:
         obj = os.path.join(OBJ, os.path.basename(src) + ".o")
         if force or _newer(src, obj, headers):
+            fmad = "--fmad=true" if os.path.basename(src) in CONTRACTED else "--fmad=false"
             cmd = [NVCC, "-std=c++17", "-c", "-Xcompiler", "-fPIC,-ffp-contract=off", "-lineinfo", "-O3",
-                   "--fmad=false"] + ARCH + INCLUDES
+                   fmad] + ARCH + INCLUDES
             cmd += ["-Xptxas", "-v"] if verbose else []
             cmd += ["-DAZ_DEBUG_CHECKS=1"] if debug else []
-            out = _run(cmd + [src, "-o", obj])
+            jobs.append(cmd + [src, "-o", obj])
+        objs.append(obj)
+    # the CUDA files compile independently: one nvcc per file, side by side
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for out in ex.map(_run, jobs):
             if verbose:
                 sys.stdout.write(out)
-        objs.append(obj)
     if force or not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
         if cu_srcs:
             _run([NVCC, "-shared", "-cudart", "static"] + ARCH + objs + ["-o", LIB, "-lpthread", "-lz"])

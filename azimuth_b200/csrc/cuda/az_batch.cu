@@ -7,9 +7,12 @@
 // fill the GPU on their own, so it loses little by starting late), or
 // largest first; each worker renders with its own wave queues; the streams run concurrently on the device, so small jobs fill
 // the SMs that a large job's waves leave idle.  A job of three or more waves
-// replays its per-wave launches as one CUDA graph.  Completion times are
-// device times between an event recorded before any job and each job's end
-// event.
+// replays its per-wave launches as one CUDA graph.  With opts->tiles the
+// plain jobs, whatever their scenes, render together in tile waves pulled
+// from a device work queue (RenderTiles) on the first stream, while the other
+// streams take the guided jobs.  Completion times are device times between an
+// event recorded before any job and each job's end event (for tiled jobs, the
+// end of the wave holding their last tile).
 #include <algorithm>
 #include <atomic>
 #include <cmath>
@@ -65,16 +68,20 @@ extern "C" int az_gpu_render_batch(az_job *jobs, uint32_t n, const az_batch_opts
     const uint32_t S = std::max(1u, std::min(opts && opts->streams ? opts->streams : 4u, n));
     const uint32_t chunk = opts && opts->chunk_samples ? opts->chunk_samples : (1u << 22);
 
-    std::vector<uint32_t> order(n);
+    // with opts->tiles, the plain jobs go to one tile render; the queue holds the rest
+    const bool tiles = opts && opts->tiles;
+    std::vector<uint32_t> order, tiled;
     const bool largest_first = opts && opts->largest_first;
     std::vector<double> cost(n);
     for (uint32_t i = 0; i < n; i++) {
-        order[i] = i;
+        if (tiles && !jobs[i].guide) tiled.push_back(i);
+        else order.push_back(i);
         jobs[i].samples = JobSamples(jobs[i]);
         cost[i] = (double)jobs[i].samples * (jobs[i].scene->impl->dev.max_depth + 1);
         jobs[i].status = AZ_OK;
         jobs[i].done_ms = 0.0f;
     }
+    const uint32_t queued = (uint32_t)order.size();
     std::stable_sort(order.begin(), order.end(),
                      [&](uint32_t a, uint32_t b) { return largest_first ? cost[a] > cost[b] : cost[a] < cost[b]; });
 
@@ -114,11 +121,40 @@ extern "C" int az_gpu_render_batch(az_job *jobs, uint32_t n, const az_batch_opts
 
     std::atomic<uint32_t> next{0};
     std::vector<std::string> messages(n);
-    auto work = [&](Worker *wk) {
+    std::vector<char> tile_done(n, 0);
+    auto render_tiled = [&](Worker *wk) {
+        std::vector<TileJob> tj(tiled.size());
+        for (size_t k = 0; k < tiled.size(); k++) {
+            const az_job &j = jobs[tiled[k]];
+            tj[k].scene = j.scene->impl;
+            tj[k].film = j.film;
+            tj[k].camera = j.camera;
+            tj[k].eps = j.epsilons;
+            tj[k].scissor = j.scissor;
+            tj[k].filter = j.filter_type;
+            tj[k].cull = j.backface_culling;
+            tj[k].seed = j.seed;
+        }
+        az_render_opts o;
+        memset(&o, 0, sizeof(o));
+        o.device = device;
+        o.flags = opts ? opts->flags : 0u;
+        const int trc = RenderTiles(*tj[0].scene, tj, &o, wk->st, nullptr, start);
+        const std::string msg = trc != AZ_OK ? az_gpu_last_error() : "";
+        for (size_t k = 0; k < tiled.size(); k++) {
+            az_job &j = jobs[tiled[k]];
+            j.status = trc;
+            j.done_ms = tj[k].done_ms;
+            if (trc != AZ_OK) messages[tiled[k]] = msg;
+            tile_done[tiled[k]] = 1;
+        }
+    };
+    auto work = [&](Worker *wk, bool tile_first) {
         cudaSetDevice(device);
+        if (tile_first) render_tiled(wk);
         for (;;) {
             const uint32_t k = next.fetch_add(1);
-            if (k >= n) break;
+            if (k >= queued) break;
             az_job &j = jobs[order[k]];
             az_render_opts o;
             memset(&o, 0, sizeof(o));
@@ -144,15 +180,18 @@ extern "C" int az_gpu_render_batch(az_job *jobs, uint32_t n, const az_batch_opts
         }
     };
     std::vector<std::thread> threads;
-    for (uint32_t w = 0; w < S; w++) threads.emplace_back(work, workers[w].get());
+    for (uint32_t w = 0; w < S; w++) threads.emplace_back(work, workers[w].get(), w == 0 && !tiled.empty());
     for (auto &t : threads) t.join();
     std::vector<float> times;
     uint32_t failed = 0;
     int first_rc = AZ_OK;
     std::string first_msg;
     for (uint32_t i = 0; i < n; i++) {
-        float ms = 0.0f;
-        if (cudaEventSynchronize(done[i]) == cudaSuccess) cudaEventElapsedTime(&ms, start, done[i]);
+        float ms = jobs[i].done_ms;   // a tiled job's: set by the tile render
+        if (!tile_done[i]) {
+            ms = 0.0f;
+            if (cudaEventSynchronize(done[i]) == cudaSuccess) cudaEventElapsedTime(&ms, start, done[i]);
+        }
         jobs[i].done_ms = ms;
         times.push_back(ms);
         if (jobs[i].status != AZ_OK) {
@@ -190,8 +229,11 @@ extern "C" int az_gpu_render_tiles(az_job *jobs, uint32_t n, const az_batch_opts
     std::vector<TileJob> tj(n);
     for (uint32_t i = 0; i < n; i++) {
         const az_job &j = jobs[i];
-        if (!j.scene || j.scene->impl != G || !G)
-            return SetError(AZ_ERR_INVALID_ARGUMENT, "job " + std::to_string(i) + ": every job needs the same scene");
+        if (!j.scene || !j.scene->impl)
+            return SetError(AZ_ERR_INVALID_ARGUMENT, "job " + std::to_string(i) + ": null scene");
+        if (j.scene->impl->device != G->device)
+            return SetError(AZ_ERR_INVALID_ARGUMENT, "job " + std::to_string(i) + ": scene on another device");
+        tj[i].scene = j.scene->impl;
         if (!j.film || !j.camera)
             return SetError(AZ_ERR_INVALID_ARGUMENT, "job " + std::to_string(i) + ": null film or camera");
         if (j.guide) return SetError(AZ_ERR_UNSUPPORTED, "job " + std::to_string(i) + ": guided jobs are not tiled");

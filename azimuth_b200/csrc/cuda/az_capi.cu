@@ -165,6 +165,25 @@ extern "C" int az_gpu_scene_info(const az_gpu_scene *scene, az_scene_info *out) 
     return AZ_OK;
 }
 
+extern "C" int az_gpu_scene_arrays(const az_gpu_scene *scene, az_scene_arrays *out) {
+    if (!scene || !scene->impl || !out) return SetError(AZ_ERR_INVALID_ARGUMENT, "null scene or output");
+    const GpuScene &G = *scene->impl;
+    memset(out, 0, sizeof(*out));
+    out->wide_nodes = (void *)G.dev.wnodes;
+    out->wide_node_count = G.node_count;
+    out->triangles = (void *)G.dev.tris;
+    out->triangle_count = G.triangle_count;
+    out->tlas_root = G.dev.tlas_root;
+    out->single_group_root = 0xFFFFFFFFu;
+    if (G.dev.tlas_single_group != 0xFFFFFFFFu) {
+        AZ_CUDA_TRY(cudaSetDevice(G.device));
+        azd::DevGroup g;
+        AZ_CUDA_TRY(cudaMemcpy(&g, G.dev.groups + G.dev.tlas_single_group, sizeof(g), cudaMemcpyDeviceToHost));
+        out->single_group_root = g.root;
+    }
+    return AZ_OK;
+}
+
 extern "C" void az_gpu_scene_destroy(az_gpu_scene *s) {
     if (!s) return;
     if (s->impl) {
@@ -184,6 +203,19 @@ extern "C" int az_gpu_render(az_gpu_scene *scene, az_pixel *film, const az_camer
     if (rc != AZ_OK) return rc;
     return Render(*scene->impl, film, camera, epsilons, scissor, filter_type, backface_culling, opts, ctx.stream,
                   stats);
+}
+
+extern "C" int az_gpu_render_samples(az_gpu_scene *scene, float *samples, const az_camera *camera,
+                                     const az_epsilon_values *epsilons, az_scissor scissor,
+                                     uint32_t backface_culling, const az_render_opts *opts,
+                                     az_render_stats *stats) {
+    if (!scene || !scene->impl || !samples || !camera) return SetError(AZ_ERR_INVALID_ARGUMENT, "null argument");
+    if ((uintptr_t)samples % 16 != 0) return SetError(AZ_ERR_INVALID_ARGUMENT, "samples must be 16-byte aligned");
+    CallContext ctx;
+    int rc = ctx.begin(opts);
+    if (rc != AZ_OK) return rc;
+    return Render(*scene->impl, nullptr, camera, epsilons, scissor, AZ_Filter_Box, backface_culling, opts, ctx.stream,
+                  stats, nullptr, false, nullptr, reinterpret_cast<float4 *>(samples));
 }
 
 extern "C" int az_gpu_render_host(az_gpu_scene *scene, az_pixel *pixels, const az_camera *camera,
@@ -398,7 +430,8 @@ extern "C" int az_gpu_closest_hit(az_gpu_scene *scene, const az_ray3 *rays, uint
     CallContext ctx;
     int rc = ctx.begin(opts);
     if (rc != AZ_OK) return rc;
-    return ClosestHit(*scene->impl, rays, count, cull, hit_epsilon, out_hit, out_uid, out_face, out_t, ctx.stream);
+    return ClosestHit(*scene->impl, rays, count, cull, hit_epsilon, out_hit, out_uid, out_face, out_t, ctx.stream,
+                      opts && (opts->flags & AZ_FLAG_WATERTIGHT));
 }
 
 extern "C" float az_rng_u01(uint64_t seed, uint32_t pixel, uint32_t sample, uint32_t digits, uint32_t level,

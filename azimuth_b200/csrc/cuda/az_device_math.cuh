@@ -1,10 +1,12 @@
 // Device-side float3 math with azimuth's operation order.
 //
-// Every translation unit that includes this header is compiled with
-// --fmad=false, so a*b+c rounds twice exactly as in azimuth's scalar C++
-// (src/azimuth_math.cpp:572-1348); divisions and square roots are IEEE
-// (-prec-div/-prec-sqrt default).  Fused multiply-adds appear only where the
-// code asks for them explicitly (box tests in the traversal).
+// The translation units whose results must round like azimuth's scalar C++
+// (src/azimuth_math.cpp:572-1348) -- primitive tests, camera rays, mesh
+// ingestion -- are compiled with --fmad=false, so a*b+c rounds twice there;
+// divisions and square roots are IEEE (-prec-div/-prec-sqrt default).  Fused
+// multiply-adds appear there only where the code asks for them explicitly
+// (box tests in the traversal).  The shading and guide units are compiled
+// with contraction (azimuth_b200/build.py, CONTRACTED).
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -126,7 +128,9 @@ struct NodeRng {
             philox4x32_10(pixel, sample, digits, (level << 24) | blk, k0, k1, cache);
             cached_block = blk;
         }
-        return u24(cache[dim++ & 3u]);
+        // select instead of indexing, so the block stays in registers
+        const uint32_t k = dim++ & 3u;
+        return u24(k == 0u ? cache[0] : (k == 1u ? cache[1] : (k == 2u ? cache[2] : cache[3])));
     }
 };
 

@@ -79,7 +79,7 @@ int SoupAreas(const SoupWork &w, std::vector<float> &areas);
 int SoupBoxes(const SoupWork &w, std::vector<float> &boxes, cudaStream_t st);
 int SoupRecords(const SoupWork &w, az_triangle *tris, az_face_attr *attrs, az_vec3 *vertex_normals, cudaStream_t st);
 int SoupTriangles(const SoupWork &w, uint32_t face_base, uint32_t count, az_triangle *tris, cudaStream_t st);
-int SoupEmitScene(const SoupWork &w, const std::vector<IngestMesh> &meshes, azd::DevTri *d_tris,
+int SoupEmitScene(const SoupWork &w, const std::vector<IngestMesh> &meshes, azd::DevTriVerts *d_tris,
                   azd::DevTriAttr *d_attr, cudaStream_t st);
 // A further placement of a soup mesh (a mesh instance besides the importer's
 // own one): `count` primitives copied from slot `src` to slot `dst` of the
@@ -87,7 +87,7 @@ int SoupEmitScene(const SoupWork &w, const std::vector<IngestMesh> &meshes, azd:
 struct IngestCopy {
     uint32_t src, dst, count, entity;
 };
-int SoupCopyPlacements(const std::vector<IngestCopy> &copies, azd::DevTri *d_tris, azd::DevTriAttr *d_attr,
+int SoupCopyPlacements(const std::vector<IngestCopy> &copies, azd::DevTriVerts *d_tris, azd::DevTriAttr *d_attr,
                        cudaStream_t st);
 
 // LBVH over `n` boxes (device arrays lo/hi of float4).  Writes nodes into
@@ -137,13 +137,18 @@ std::mutex &GuideLock(GuideState &g);
 // updates the network after every wave.
 // `wave_buffers`: the queues to use (null: the scene's own); concurrent
 // renders of one scene need their own.
+// `sample_out`: instead of splatting into `film` (which may then be null),
+// write every camera sample's radiance sum to sample_out[s], s the sample's
+// index in the scissor (sample number * scissor pixels + pixel).
 int Render(GpuScene &G, az_pixel *film, const az_camera *camera, const az_epsilon_values *eps, az_scissor sc,
            int32_t filter, uint32_t cull, const az_render_opts *opts, cudaStream_t st, az_render_stats *stats,
-           GuideState *guide = nullptr, bool train = false, WaveBuffers *wave_buffers = nullptr);
+           GuideState *guide = nullptr, bool train = false, WaveBuffers *wave_buffers = nullptr,
+           float4 *sample_out = nullptr);
 int Autotune(GpuScene &G, const az_camera *camera, const az_epsilon_values *eps, az_scissor sc, int32_t filter,
              uint32_t cull, const az_render_opts *opts, cudaStream_t st, uint32_t *best_out, float *ms_out);
 // One render job of a tile render (az_gpu_render_tiles).
 struct TileJob {
+    GpuScene *scene = nullptr;   // the job's scene (null: RenderTiles' own); all on one device
     az_pixel *film;              // device film of the job's camera
     const az_camera *camera;
     const az_epsilon_values *eps;
@@ -154,16 +159,20 @@ struct TileJob {
     uint64_t samples = 0;        // written: the job's camera samples
     float done_ms = 0.0f;        // written: device time from the call's start to its last wave's end
 };
-// Renders jobs of one scene together: their samples are cut into tiles, and
-// every wave takes the next tiles of all jobs from a device work queue, so one
-// chain of launches serves every job.  The jobs must share epsilons and culling.
+// Renders jobs together: their samples are cut into tiles, and every wave
+// takes the next tiles of all jobs from a device work queue, so one chain of
+// launches serves every job.  Jobs may render different scenes (up to 256,
+// one device): every queue entry then carries its scene's index and each
+// kernel reads that scene's record.  The jobs must share epsilons and
+// culling.  `origin`, when given, is an event recorded earlier on `st` from
+// which the jobs' completion times are measured (default: the call's start).
 int RenderTiles(GpuScene &G, std::vector<TileJob> &jobs, const az_render_opts *opts, cudaStream_t st,
-                az_render_stats *stats);
+                az_render_stats *stats, cudaEvent_t origin = nullptr);
 // OutputPixelsToFile's post-processing of a device film (az_post.cu).
 int PostProcess(const az_pixel *film, uint32_t w, uint32_t h, const az_tonemap *tm, float inv_gamma, uint32_t srgb,
                 uint32_t linear, float *rgb_out, uint8_t *rgb8_out, cudaStream_t st);
 int ClosestHit(GpuScene &G, const az_ray3 *rays, uint32_t n, int32_t cull, float eps, uint32_t *out_hit,
-               uint32_t *out_uid, uint32_t *out_face, float *out_t, cudaStream_t st);
+               uint32_t *out_uid, uint32_t *out_face, float *out_t, cudaStream_t st, bool watertight = false);
 
 }  // namespace az
 

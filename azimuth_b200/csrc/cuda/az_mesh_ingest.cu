@@ -166,12 +166,12 @@ __global__ void k_ingest_emit_records(const float *v, const uint32_t *faces, uin
 }
 
 // Device-scene primitives of every face that belongs to a mesh, at the
-// mesh's place in its group (out_base[mesh index] + face offset): the
-// operands of azimuth's Cramer test and the shading attributes, exactly as
-// the host flattening makes them from triangle entities.
+// mesh's place in its group (out_base[mesh index] + face offset): the exact
+// vertices and face normal and the shading attributes, exactly as the host
+// flattening makes them from triangle entities.
 __global__ void k_ingest_emit_scene(const float *v, const uint32_t *faces, uint32_t nf, const float *fn_unit,
                                     const float *vn, const float *uv, uint32_t nuv, const MeshRange *m, uint32_t nm,
-                                    const IngestMesh *meshes, azd::DevTri *tris, azd::DevTriAttr *attrs) {
+                                    const IngestMesh *meshes, azd::DevTriVerts *tris, azd::DevTriAttr *attrs) {
     const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= nf) return;
     const int mi = mesh_of(m, nm, f);
@@ -182,10 +182,10 @@ __global__ void k_ingest_emit_scene(const float *v, const uint32_t *faces, uint3
     const float p0x = v[3 * idx[0]], p0y = v[3 * idx[0] + 1], p0z = v[3 * idx[0] + 2];
     const float p1x = v[3 * idx[1]], p1y = v[3 * idx[1] + 1], p1z = v[3 * idx[1] + 2];
     const float p2x = v[3 * idx[2]], p2y = v[3 * idx[2] + 1], p2z = v[3 * idx[2] + 2];
-    azd::DevTri t;
-    t.a = make_float4(p0x, p0y, p0z, p0x - p1x);
-    t.b = make_float4(p0y - p1y, p0z - p1z, p0x - p2x, p0y - p2y);
-    t.c = make_float4(p0z - p2z, fn_unit[3 * f], fn_unit[3 * f + 1], fn_unit[3 * f + 2]);
+    azd::DevTriVerts t;
+    t.a = make_float4(p0x, p0y, p0z, p1x);
+    t.b = make_float4(p1y, p1z, p2x, p2y);
+    t.c = make_float4(p2z, fn_unit[3 * f], fn_unit[3 * f + 1], fn_unit[3 * f + 2]);
     tris[o] = t;
     float u[6];
     face_uvs(uv, nuv, m[mi].uv_offset, idx, u);
@@ -209,7 +209,7 @@ __global__ void k_ingest_emit_scene(const float *v, const uint32_t *faces, uint3
 // One thread per copied primitive; `start` holds each copy's first thread
 // (exclusive prefix of the counts), so a thread finds its copy by bisection.
 __global__ void k_ingest_copy(const IngestCopy *copies, const uint32_t *start, uint32_t nc, uint32_t total,
-                              azd::DevTri *tris, azd::DevTriAttr *attrs) {
+                              azd::DevTriVerts *tris, azd::DevTriAttr *attrs) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= total) return;
     int lo = 0, hi = (int)nc - 1, c = 0;
@@ -418,7 +418,7 @@ int SoupTriangles(const SoupWork &w, uint32_t face_base, uint32_t count, az_tria
     return AZ_OK;
 }
 
-int SoupEmitScene(const SoupWork &w, const std::vector<IngestMesh> &meshes, azd::DevTri *d_tris,
+int SoupEmitScene(const SoupWork &w, const std::vector<IngestMesh> &meshes, azd::DevTriVerts *d_tris,
                   azd::DevTriAttr *d_attr, cudaStream_t st) {
     if (w.nf == 0 || w.nm == 0) return AZ_OK;
     Dev<IngestMesh> dm;
@@ -431,7 +431,7 @@ int SoupEmitScene(const SoupWork &w, const std::vector<IngestMesh> &meshes, azd:
     return AZ_OK;
 }
 
-int SoupCopyPlacements(const std::vector<IngestCopy> &copies, azd::DevTri *d_tris, azd::DevTriAttr *d_attr,
+int SoupCopyPlacements(const std::vector<IngestCopy> &copies, azd::DevTriVerts *d_tris, azd::DevTriAttr *d_attr,
                        cudaStream_t st) {
     if (copies.empty()) return AZ_OK;
     std::vector<uint32_t> start(copies.size());

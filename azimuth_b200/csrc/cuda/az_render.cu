@@ -32,76 +32,12 @@
 #include "az_internal.h"
 #include "az_render.h"
 #include "az_shade.cuh"
+#include "az_wave.cuh"
 
 namespace az {
 namespace {
 
 using namespace azd;
-
-// Shadow-query kinds (CalculateLighting occlusion rules, src/azimuth_main.cpp:685-712)
-enum : uint32_t {
-    SHADOW_TMAX = 0,     // point/area/spot: occluded by a hit with t < 1 - ShadowRay epsilon
-    SHADOW_ANY = 1,      // directional light and environment ray: occluded by any hit
-    SHADOW_ENTITY = 2,   // entity light: occluded unless the nearest hit is the light's entity
-    SHADOW_ENTITY_FULL = 3   // the same for a light too large for the two-phase test: k_shadow_full
-};
-
-// flags packed into d.w of a path entry
-// PF_BRANCHED: an ancestor vertex spawned more than one child (its
-// descendants are not used for training the path guide)
-enum : uint32_t { PF_INSIDE = 1u, PF_ATTEN = 2u, PF_BRANCHED = 4u };
-
-__host__ __device__ __forceinline__ void sample_of(const CameraParams &cam, uint64_t s, uint32_t &row,
-                                                   uint32_t &col, uint32_t &sx, uint32_t &sy) {
-    uint64_t pix = s % cam.npix, k = s / cam.npix;
-    row = cam.r0 + (uint32_t)(pix / cam.wsc);
-    col = cam.c0 + (uint32_t)(pix % cam.wsc);
-    sx = (uint32_t)(k % cam.sqrt_spp);
-    sy = (uint32_t)(k / cam.sqrt_spp);
-}
-
-__device__ __forceinline__ uint32_t push_slot(uint32_t *counter) {
-    // warp-aggregated atomic increment
-    uint32_t mask = __activemask();
-    int lane = threadIdx.x & 31;
-    int leader = __ffs(mask) - 1;
-    uint32_t base = 0;
-    if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(mask));
-    base = __shfl_sync(mask, base, leader);
-    return base + (uint32_t)__popc(mask & ((1u << lane) - 1u));
-}
-
-__device__ __forceinline__ void add_accum(float4 *accum, uint32_t slot, f3 v) {
-    if (is_zero(v)) return;
-    atomicAdd(&accum[slot], make_float4(v.x, v.y, v.z, 0.0f));   // one vector atomic (sm_90 and later)
-}
-
-__device__ __forceinline__ void push_path(const WaveQueues &Q, int buf, uint32_t level, f3 o, float time, f3 d,
-                                          uint32_t flags, f3 tp, uint32_t slot, f3 att, uint32_t digits) {
-    uint32_t i = push_slot(&Q.counts[level]);
-    if (i >= Q.cap_q) {
-        Q.counts[AZ_COUNT_OVERFLOW] = 1;   // this wave is re-run with fewer samples
-        return;
-    }
-    Q.o[buf][i] = make_float4(o.x, o.y, o.z, time);
-    Q.d[buf][i] = make_float4(d.x, d.y, d.z, __uint_as_float(flags));
-    Q.tp[buf][i] = make_float4(tp.x, tp.y, tp.z, __uint_as_float(slot));
-    Q.att[buf][i] = make_float4(att.x, att.y, att.z, 0.0f);
-    Q.digits[buf][i] = digits;
-}
-
-__device__ __forceinline__ void push_shadow(const WaveQueues &Q, uint32_t level, f3 o, float time, f3 d,
-                                            float tmax, f3 c, uint32_t slot, uint32_t kind, uint32_t uid) {
-    uint32_t i = push_slot(&Q.counts[AZ_COUNT_SHADOW + level]);
-    if (i >= Q.cap_s) {
-        Q.counts[AZ_COUNT_OVERFLOW] = 1;
-        return;
-    }
-    Q.so[i] = make_float4(o.x, o.y, o.z, time);
-    Q.sd[i] = make_float4(d.x, d.y, d.z, tmax);
-    Q.sc[i] = make_float4(c.x, c.y, c.z, __uint_as_float(slot));
-    Q.smeta[i] = (kind << 30) | (uid & 0x3FFFFFFFu);
-}
 
 // GetSampleCoord + GetRayForPixel (src/azimuth_main.cpp:1135-1178) of camera
 // sample s into wave slot i.
@@ -124,7 +60,7 @@ __device__ __forceinline__ void camera_node(const CameraParams &cam, const WaveQ
     f3 o = cam.pos + offx + offy;
     float time = rng.next();
     Q.o[1][i] = make_float4(o.x, o.y, o.z, time);
-    Q.d[1][i] = make_float4(dir.x, dir.y, dir.z, __uint_as_float(0u));
+    Q.d[1][i] = make_float4(dir.x, dir.y, dir.z, __uint_as_float(cam.scene << PF_SCENE_SHIFT));
     Q.tp[1][i] = make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(i));
     Q.att[1][i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     Q.digits[1][i] = 0u;
@@ -249,16 +185,23 @@ __global__ void k_order_keys(DevScene S, WaveQueues Q, uint32_t level, int shado
 //                 step
 //   MODE_FETCH    persistent warps: a lane takes the next query of the queue
 //                 as soon as its own ends (batches of kFetchBatch per warp)
-enum : int { MODE_LOOP = 0, MODE_LOCKSTEP = 1, MODE_FETCH = 2 };
+//   MODE_FETCHP   the same, with traversal steps that pop the stack first
+//                 and visit the popped group in the same step (Tracer
+//                 POP_FIRST), so lanes coming back from a pop join the
+//                 warp's node visits instead of idling through them
+enum : int { MODE_LOOP = 0, MODE_LOCKSTEP = 1, MODE_FETCH = 2, MODE_FETCHP = 3 };
 
-template <int BLOCK, int MINB, int MODE>
+// WT: triangles by the watertight test (AZ_FLAG_WATERTIGHT) instead of azimuth's.
+// MULTI: a tile wave of several scenes (MODE_FETCHP only): each query is
+// traced in the scene its entry names (WaveQueues.scenes).
+template <int BLOCK, int MINB, int MODE, bool WT = false, bool MULTI = false>
 __global__ void __launch_bounds__(BLOCK, MINB) k_extend(DevScene S, CameraParams cam, WaveQueues Q, uint32_t level) {
     const int buf = level & 1;
     const uint32_t n = min(Q.counts[level], Q.cap_q);
     uint32_t *cnt = cam.count_traversal ? Q.counts + AZ_COUNT_NODES : nullptr;
     uint32_t *err = Q.counts + AZ_COUNT_ERROR;
     if (MODE == MODE_LOCKSTEP) {
-        Tracer<Q_CLOSEST> T;
+        Tracer<Q_CLOSEST, false, WT> T;
         uint2 stack[AZD_WSTACK];
         // warp-uniform loop bound: every lane of a warp sees the same base
         for (uint32_t base = blockIdx.x * BLOCK + (threadIdx.x & ~31u); base < n; base += gridDim.x * BLOCK) {
@@ -294,16 +237,17 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_extend(DevScene S, CameraParams
             r.d = mk(d.x, d.y, d.z);
             r.time = o.w;
             Hit h;
-            trace<Q_CLOSEST>(S, r, cam.cull != 0, cam.eps_isect, FLT_MAX, h, cnt, err);
+            trace<Q_CLOSEST, WT>(S, r, cam.cull != 0, cam.eps_isect, FLT_MAX, h, cnt, err);
             Q.hit[i] = make_uint4(__float_as_uint(h.t), __float_as_uint(h.tl), h.prim, h.ent);
         }
         return;
     }
     uint32_t *fetch = Q.counts + AZ_COUNT_FETCH + level;
-    Tracer<Q_CLOSEST> T;
+    Tracer<Q_CLOSEST, MODE == MODE_FETCHP, WT> T;
     uint2 stack[AZD_WSTACK];
     WarpFetch wf;
     uint32_t idx = kLaneIdle, qi = 0;   // work item and its queue entry
+    uint32_t si = 0;                    // MULTI: the entry's scene
     while (true) {
         if (wf.refill(fetch, n, idx)) {
             qi = Q.eorder ? Q.eorder[idx] : idx;
@@ -312,335 +256,15 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_extend(DevScene S, CameraParams
             r.o = mk(o.x, o.y, o.z);
             r.d = mk(d.x, d.y, d.z);
             r.time = o.w;
-            T.init(S, r, cam.cull != 0, cam.eps_isect, FLT_MAX, stack);
+            if (MULTI) si = (__float_as_uint(d.w) & PF_SCENE) >> PF_SCENE_SHIFT;
+            T.init(MULTI ? Q.scenes[si] : S, r, cam.cull != 0, cam.eps_isect, FLT_MAX, stack);
         }
         if (__all_sync(0xFFFFFFFFu, idx == kLaneDone)) break;
-        if (idx < n && T.step(S, stack, err)) {
+        if (idx < n && T.step(MULTI ? Q.scenes[si] : S, stack, err)) {
             const Hit &h = T.best;
             Q.hit[qi] = make_uint4(__float_as_uint(h.t), __float_as_uint(h.tl), h.prim, h.ent);
             T.flush_counts(cnt);
             idx = kLaneIdle;
-        }
-    }
-}
-
-__device__ __forceinline__ f3 ld3(const float *p) { return mk(p[0], p[1], p[2]); }
-
-// One tree node: direct light, ambient and children (TraceRay body,
-// src/azimuth_main.cpp:974-1130).  FEAT (DevScene.features) compiles out the
-// parts a scene cannot reach: textures, environment map, mirror/dielectric
-// branches, point/area/directional/spot lights.
-template <int BLOCK, uint32_t FEAT, bool GUIDED, bool TILES = false>
-__global__ void __launch_bounds__(BLOCK) k_shade(DevScene S, CameraParams cam, WaveQueues Q, uint64_t wave_start,
-                                                 uint32_t level) {
-    constexpr bool TEX = FEAT & FEAT_TEXTURES, ENV = FEAT & FEAT_ENV, SPECIAL = FEAT & FEAT_SPECIAL,
-                   LIGHTS = FEAT & FEAT_ANALYTIC_LIGHTS;
-    const int buf = level & 1, nbuf = buf ^ 1;
-    const uint32_t n = min(Q.counts[level], Q.cap_q);
-    const bool can_spawn = level + 1 <= S.max_depth + 1;   // child's RecursionDepth <= MaxRecursionDepth
-    const float seps = cam.eps_shadow;
-    uint64_t seed = cam.seed;
-    if (Q.wave) {
-        wave_start = Q.wave[0];
-        seed = Q.wave[2];
-    }
-    for (uint32_t i = blockIdx.x * BLOCK + threadIdx.x; i < n; i += gridDim.x * BLOCK) {
-        const float4 o4 = Q.o[buf][i], d4 = Q.d[buf][i], tp4 = Q.tp[buf][i];
-        const uint4 hh = Q.hit[i];
-        const uint32_t flags = __float_as_uint(d4.w);
-        const uint32_t slot = __float_as_uint(tp4.w);
-        f3 tp = mk(tp4.x, tp4.y, tp4.z);
-        Ray r;
-        r.o = mk(o4.x, o4.y, o4.z);
-        r.d = mk(d4.x, d4.y, d4.z);
-        r.time = o4.w;
-        Hit h;
-        h.t = __uint_as_float(hh.x);
-        h.tl = __uint_as_float(hh.y);
-        h.prim = hh.z;
-        h.ent = hh.w;
-        // the sample's pixel; in a tile wave (TILES) its own job's camera,
-        // whose seed and film size are read again where they are needed
-        uint32_t row, col, sx, sy;
-        uint32_t job = 0;
-        if (TILES) {
-            const uint2 js = Q.slot_map[slot];
-            job = js.x;
-            sample_of(Q.job_cams[job], js.y, row, col, sx, sy);
-        } else {
-            sample_of(cam, wave_start + slot, row, col, sx, sy);
-        }
-        // path-guide training: this node is the only child of the vertex recorded
-        // one level up, so the sample's sum now holds everything up to that
-        // vertex's level
-        const bool recordable = GUIDED && Q.rec && slot < Q.n_rec && !(flags & PF_BRANCHED);
-        if (recordable && level >= 2 && level - 2 < Q.rec_levels) {
-            const float4 a = Q.accum[slot];
-            Q.rec[(size_t)(level - 2) * Q.n_rec + slot].snap = make_float4(a.x, a.y, a.z, 1.0f);
-        }
-        if (h.ent == 0xFFFFFFFFu) {
-            // a miss returns 0, except for the primary ray, whose sample then takes
-            // the background (RayTravelDistance == 0, src/azimuth_main.cpp:1374-1384)
-            if (level == 1) {
-                const uint32_t fw = TILES ? Q.job_cams[job].width : cam.width;
-                const uint32_t fh = TILES ? Q.job_cams[job].height : cam.height;
-                add_accum(Q.accum, slot, background(S, r.d, (int32_t)fw - 1, (int32_t)fh - 1, row, col));
-            }
-            continue;
-        }
-        const bool inside = (flags & PF_INSIDE) != 0;
-        if (flags & PF_ATTEN) {
-            // Beer attenuation of a refracted or internally reflected subtree by
-            // the distance to its first hit (src/azimuth_main.cpp:921-935, :955-962)
-            float4 a = Q.att[buf][i];
-            tp = had(tp, mk(expf(a.x * h.t), expf(a.y * h.t), expf(a.z * h.t)));
-        }
-        const DevEntity &e = S.ents[h.ent];
-        if (e.is_emitter) {
-            add_accum(Q.accum, slot, had(tp, ld3(e.radiance)));   // :984-985
-            continue;
-        }
-        NodeRng rng;
-        const uint32_t digits = Q.digits[buf][i];
-        rng.init(TILES ? Q.job_cams[job].seed : seed, (row << 16) | col, (sy << 16) | sx, digits, level);
-        const Surface s = surface_at<TEX>(S, r, h);
-        const DevMaterial &m = S.materials[e.material];
-        f3 dcol = ld3(m.diffuse), scol = ld3(m.specular);
-        f3 local = mk(0.0f, 0.0f, 0.0f);   // this node's own radiance (before `tp`)
-        bool ignore_ambient = false;
-        if (TEX && e.texture_index) {
-            const DevTexture &tex = S.textures[e.texture_index - 1];
-            f3 ts = sample_texture(S, tex, s.p, s.u, s.v);
-            if (tex.blend == 0) {           // ReplaceAll: DiffuseContribution starts at (1,1,1)
-                dcol = ts;
-                local = dcol;
-                ignore_ambient = true;
-            } else if (tex.blend == 1) {    // ReplaceDiffuse
-                dcol = ts;
-            } else {                        // BlendDiffuse
-                dcol = dcol + ts;
-                dcol = dcol * 0.5f;
-            }
-        }
-        // CalculateLighting (:605-779): one sample and one visibility test per light
-        for (uint32_t li = 0; li < S.light_count; li++) {
-            const DevLight &L = S.lights[li];
-            f3 ldir = mk(0.0f, 0.0f, 0.0f), I = ld3(L.intensity);
-            uint32_t kind = SHADOW_TMAX;
-            float falloff = 1.0f, ldist = 1.0f, invpdf = 1.0f;
-            if (!LIGHTS || L.type == LIGHT_ENTITY) {
-                sample_entity_light(S, L, s.p, rng, ldir, invpdf);
-                I = ld3(L.intensity);
-                kind = entity_light_needs_full_query(L) ? SHADOW_ENTITY_FULL : SHADOW_ENTITY;
-            } else if (L.type == LIGHT_POINT) {
-                ldir = ld3(L.position) - s.p;
-                ldist = length(ldir);
-            } else if (L.type == LIGHT_AREA) {
-                // GCC evaluates the second Random01() of this sum first
-                float u1 = rng.next();
-                float u0 = rng.next();
-                f3 lp = ld3(L.position) + ld3(L.edge0) * u0 + ld3(L.edge1) * u1;
-                falloff = dot(normalize(lp - s.p), ld3(L.normal));
-                if (falloff < 0.0f) falloff *= -1.0f;
-                ldir = lp - s.p;
-                ldist = length(ldir);
-            } else if (L.type == LIGHT_DIRECTIONAL) {
-                ldir = normalize(-ld3(L.position));
-                kind = SHADOW_ANY;
-            } else if (L.type == LIGHT_SPOT) {
-                ldir = ld3(L.position) - s.p;
-                ldist = length(ldir);
-                float ct = dot(normalize(-ldir), normalize(ld3(L.spot_dir)));
-                if (ct < L.cos_half_coverage) {
-                    falloff = 0.0f;
-                } else if (ct > L.cos_half_falloff) {
-                    falloff = 1.0f;
-                } else {
-                    falloff = (ct - L.cos_half_coverage) / (L.cos_half_falloff - L.cos_half_coverage);
-                    falloff = powf(falloff, 4.0f);
-                    if (falloff < 0.0f) falloff = 0.0f;
-                    else if (falloff > 1.0f) falloff = 1.0f;
-                }
-            }
-            if (ldist == 0.0f) ldist = 0.001f;
-            if (inside) continue;   // no direct light inside a dielectric (:714)
-            f3 dc, sc;
-            if (!light_contribution(dc, sc, m, I, ldir, r.d, s.n, ldist, falloff, invpdf)) continue;
-            f3 c = had(tp, had(dcol, dc) + had(scol, sc));
-            if (is_zero(c)) continue;
-            // entity lights carry the light index (their identity test needs the light)
-            push_shadow(Q, level, s.p + (ldir * seps), r.time, ldir, 1.0f - seps, c, slot, kind,
-                        kind >= SHADOW_ENTITY ? li : 0u);
-        }
-        if (ENV && S.use_env_map) {
-            // cosine-sampled environment ray (:724-778); not gated by InsideDielectric
-            f3 Ld;
-            float env_invpdf;
-            if (cam.env_importance) {
-                // the same two draws, through one-sample MIS of the map's luminance CDF and cosine sampling
-                const float u1 = rng.next(), u2 = rng.next();
-                env_invpdf = sample_env_mis(S, s.n, u1, u2, Ld);
-            } else {
-                float phi = 2.0f * AZD_PI_F32 * rng.next();
-                float cp = cosf(phi), sp = sinf(phi);
-                float theta = asinf(sqrtf(rng.next()));
-                float ct = cosf(theta), st = sinf(theta);
-                f3 U, V;
-                onb(s.n, U, V);
-                Ld = normalize(U * st * cp + V * st * sp + s.n * ct);
-                float ca = dot(Ld, s.n);
-                if (ca == 0.0f) ca = 0.000001f;
-                env_invpdf = AZD_PI_F32 / ca;
-            }
-            float u = (-atan2f(Ld.z, Ld.x) + AZD_PI_F32) / (2.0f * AZD_PI_F32), v = acosf(Ld.y) / AZD_PI_F32;
-            f3 I = sample_texture(S, S.textures[S.env_texture], mk(u, v, 1.0f), u, v);
-            f3 dc, sc;
-            if (env_invpdf > 0.0f && light_contribution(dc, sc, m, I, Ld, r.d, s.n, 1.0f, 1.0f, env_invpdf)) {
-                f3 c = had(tp, had(dcol, dc) + had(scol, sc));
-                if (!is_zero(c)) push_shadow(Q, level, s.p + (Ld * seps), r.time, Ld, FLT_MAX, c, slot, SHADOW_ANY, 0u);
-            }
-        }
-        uint32_t next_child = 0;
-        // a vertex that may spawn more than one child marks its subtree
-        const bool multi = SPECIAL && S.path_trace && (m.is_mirror || m.transparent);
-        const uint32_t bflag = ((flags & PF_BRANCHED) || multi) ? PF_BRANCHED : 0u;
-        if (S.path_trace) {
-            // diffuse scatter ray (:1029-1083): child 0
-            f3 Sd;
-            float invpdf, qpdf = 0.0f;
-            if (GUIDED && can_spawn) {
-                // path guiding: one-sample MIS of the learned vMF mixture and
-                // cosine sampling, weighted by the mixture density (the deepest
-                // level spawns no child: it has no proposals, and its records
-                // keep density 0, which training skips)
-                const GuideLobes &G = Q.lobes[i];
-                const float alpha = fminf(G.alpha, Q.guide_alpha_max);
-                const float us = rng.next();
-                if (us < alpha) {
-                    const int k = guide_pick_lobe(G, rng.next());
-                    const float u1 = rng.next();
-                    Sd = guide_sample_lobe(G, k, u1, rng.next());
-                } else {
-                    const float theta = asinf(sqrtf(rng.next()));
-                    const float phi = 2.0f * AZD_PI_F32 * rng.next();
-                    f3 U, V;
-                    onb(s.n, U, V);
-                    Sd = normalize(U * (sinf(theta) * cosf(phi)) + V * (sinf(theta) * sinf(phi)) + s.n * cosf(theta));
-                }
-                qpdf = guide_mixture_pdf_alpha(G, alpha, s.n, Sd);
-                invpdf = qpdf > 0.0f ? 1.0f / qpdf : 0.0f;
-            } else {
-                float theta = S.importance_sampling ? asinf(sqrtf(rng.next())) : acosf(rng.next());
-                float ct = cosf(theta), st = sinf(theta);
-                float phi = 2.0f * AZD_PI_F32 * rng.next();
-                float cp = cosf(phi), sp = sinf(phi);
-                f3 U, V;
-                onb(s.n, U, V);
-                Sd = normalize(U * st * cp + V * st * sp + s.n * ct);
-                if (S.importance_sampling) {
-                    float cs = dot(Sd, s.n);
-                    if (cs == 0.0f) cs = 0.000001f;
-                    invpdf = AZD_PI_F32 / cs;
-                } else {
-                    invpdf = AZD_PI_F32 * 2.0f;
-                }
-            }
-            f3 dc, sc, ctp = mk(0.0f, 0.0f, 0.0f);
-            bool queued = false;
-            if (can_spawn && invpdf > 0.0f &&
-                light_contribution(dc, sc, m, mk(1.0f, 1.0f, 1.0f), Sd, r.d, s.n, 1.0f, 1.0f, invpdf)) {
-                ctp = had(tp, had(dcol, dc) + had(scol, sc));
-                if (!is_zero(ctp)) {
-                    push_path(Q, nbuf, level + 1, s.p + (Sd * seps), r.time, Sd, (flags & PF_INSIDE) | bflag, ctp,
-                              slot, mk(0.0f, 0.0f, 0.0f), child_digits(digits, level, 0));
-                    queued = true;
-                }
-            }
-            if (recordable && !multi && level - 1 < Q.rec_levels) {
-                f3 gp, gn;
-                guide_query(S, r, h, gp, gn);
-                GuideRecord &R = Q.rec[(size_t)(level - 1) * Q.n_rec + slot];
-                R.pos_q = make_float4(gp.x, gp.y, gp.z, qpdf);
-                R.n = make_float4(gn.x, gn.y, gn.z, 0.0f);
-                R.wo = make_float4(-r.d.x, -r.d.y, -r.d.z, 0.0f);
-                R.wi = make_float4(Sd.x, Sd.y, Sd.z, 0.0f);
-                R.tpc = make_float4(ctp.x, ctp.y, ctp.z, queued ? 1.0f : 0.0f);
-            }
-            next_child = 1;
-        }
-        // ReplaceAll's (1,1,1) start value and the ambient term (:1000-1020, :1086-1099)
-        f3 own = local;
-        if ((!inside || !m.transparent) && !ignore_ambient) own = own + had(ld3(m.ambient), ld3(S.ambient));
-        add_accum(Q.accum, slot, had(tp, own));
-        if (!SPECIAL) continue;
-        if (m.is_mirror) {
-            // CalculateMirrorContribution (:781-854)
-            f3 rd = reflect(-r.d, s.n);
-            if (m.glossiness != 0.0f) {
-                f3 rp = mk(fabsf(rd.x), fabsf(rd.y), fabsf(rd.z));
-                if (rp.x < rp.y) {
-                    if (rp.x < rp.z) { rp = rd; rp.x = rp.x < 0.0f ? -1.0f : 1.0f; }
-                    else { rp = rd; rp.z = rp.z < 0.0f ? -1.0f : 1.0f; }
-                } else {
-                    if (rp.y < rp.z) { rp = rd; rp.y = rp.y < 0.0f ? -1.0f : 1.0f; }
-                    else { rp = rd; rp.z = rp.z < 0.0f ? -1.0f : 1.0f; }
-                }
-                rp = normalize(rp);
-                f3 uu = cross(rp, rd), vv = cross(uu, rd);
-                // GCC evaluates the second Random01() of this sum first
-                float b = rng.next();
-                float a = rng.next();
-                rd = rd + (2.0f * m.glossiness) * (uu * (a - 0.5f) + vv * (b - 0.5f));
-                rd = normalize(rd);
-            }
-            f3 ctp = had(tp, ld3(m.mirror));
-            if (can_spawn && !is_zero(ctp))
-                push_path(Q, nbuf, level + 1, s.p + (rd * 0.000825f), r.time, rd, (flags & PF_INSIDE) | bflag, ctp,
-                          slot, mk(0.0f, 0.0f, 0.0f), child_digits(digits, level, next_child));
-            next_child++;
-        }
-        if (m.transparent) {
-            // CalculateTransparencyContribution (:856-964)
-            f3 T = ld3(m.transparency);
-            float to = m.refraction_index, from = 1.0f;
-            if (inside) {
-                from = m.refraction_index;
-                to = 1.0f;
-            }
-            f3 N = s.n;
-            float ct = -dot(r.d, N);
-            if (ct < 0.0f) {
-                N = -s.n;
-                ct = -dot(r.d, N);
-            }
-            float ratio = from / to;
-            float delta = 1.0f - (ratio * ratio) * (1.0f - ct * ct);
-            float refl;
-            f3 att = mk(T.x - 1.0f, T.y - 1.0f, T.z - 1.0f);
-            if (delta <= 0.0f) {
-                refl = 1.0f;
-            } else {
-                float cphi = sqrtf(delta);
-                float cair = inside ? cphi : ct;
-                float icair = 1.0f - cair;
-                float q = (from - to) / (from + to);
-                float r0 = q * q;
-                refl = r0 + (1.0f - r0) * powf(icair, 5.0f);
-                f3 td = (r.d + N * ct) * ratio - N * cphi;
-                td = normalize(td);
-                f3 ctp = tp * (1.0f - refl);
-                if (can_spawn && !is_zero(ctp))
-                    push_path(Q, nbuf, level + 1, s.p + (td * 0.0001f), r.time, td,
-                              (inside ? 0u : PF_INSIDE) | (inside ? 0u : PF_ATTEN) | bflag, ctp, slot, att,
-                              child_digits(digits, level, next_child));
-                next_child++;
-            }
-            f3 rd = reflect(-r.d, N);
-            f3 ctp = tp * refl;
-            if (can_spawn && !is_zero(ctp))
-                push_path(Q, nbuf, level + 1, s.p + (rd * 0.0001f), r.time, rd,
-                          (inside ? PF_INSIDE : 0u) | (inside ? PF_ATTEN : 0u) | bflag, ctp, slot, att,
-                          child_digits(digits, level, next_child));
         }
     }
 }
@@ -653,32 +277,34 @@ __global__ void __launch_bounds__(BLOCK) k_shade(DevScene S, CameraParams cam, W
 // lights too large for the two-phase test): one full nearest-hit query each,
 // visible when the nearest hit is the light's entity (src/azimuth_main.cpp:694-712).
 // Launched only for scenes that have such a light.
-__global__ void __launch_bounds__(128) k_shadow_full(DevScene S, CameraParams cam, WaveQueues Q, uint32_t level) {
+template <bool WT, bool MULTI = false>
+__global__ void __launch_bounds__(128) k_shadow_full(DevScene S0, CameraParams cam, WaveQueues Q, uint32_t level) {
     const uint32_t n = min(Q.counts[AZ_COUNT_SHADOW + level], Q.cap_s);
-    uint32_t *cnt = cam.count_traversal ? Q.counts + AZ_COUNT_NODES : nullptr;
+    uint32_t *cnt = cam.count_traversal ? Q.counts + AZ_COUNT_SNODES : nullptr;
     uint32_t *err = Q.counts + AZ_COUNT_ERROR;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t meta = Q.smeta[i];
-        if ((meta >> 30) != SHADOW_ENTITY_FULL) continue;
+        if (shadow_kind(meta) != SHADOW_ENTITY_FULL) continue;
+        const DevScene &S = MULTI ? Q.scenes[shadow_scene(meta)] : S0;
         const float4 o = Q.so[i], d = Q.sd[i], c = Q.sc[i];
-        const DevLight &L = S.lights[meta & 0x3FFFFFFFu];
+        const DevLight &L = S.lights[shadow_light(meta)];
         Ray r;
         r.o = mk(o.x, o.y, o.z);
         r.d = mk(d.x, d.y, d.z);
         r.time = o.w;
         Hit h;
-        const bool any = trace<Q_CLOSEST>(S, r, false, 0.0f, FLT_MAX, h, cnt, err);
+        const bool any = trace<Q_CLOSEST, WT>(S, r, false, 0.0f, FLT_MAX, h, cnt, err);
         if (!any || S.ents[h.ent].uid == L.uid) add_accum(Q.accum, __float_as_uint(c.w), mk(c.x, c.y, c.z));
     }
 }
 
-template <int BLOCK, int MINB, int MODE>
+template <int BLOCK, int MINB, int MODE, bool WT = false, bool MULTI = false>
 __global__ void __launch_bounds__(BLOCK, MINB) k_shadow(DevScene S, CameraParams cam, WaveQueues Q, uint32_t level) {
     const uint32_t n = min(Q.counts[AZ_COUNT_SHADOW + level], Q.cap_s);
-    uint32_t *cnt = cam.count_traversal ? Q.counts + AZ_COUNT_NODES : nullptr;
+    uint32_t *cnt = cam.count_traversal ? Q.counts + AZ_COUNT_SNODES : nullptr;
     uint32_t *err = Q.counts + AZ_COUNT_ERROR;
     if (MODE == MODE_LOCKSTEP) {
-        Tracer<Q_ANY> T;
+        Tracer<Q_ANY, false, WT> T;
         uint2 stack[AZD_WSTACK];
         for (uint32_t base = blockIdx.x * BLOCK + (threadIdx.x & ~31u); base < n; base += gridDim.x * BLOCK) {
             const uint32_t k = base + (threadIdx.x & 31u);
@@ -689,7 +315,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_shadow(DevScene S, CameraParams
                 const float4 o = Q.so[i], d = Q.sd[i];
                 c = Q.sc[i];
                 const uint32_t meta = Q.smeta[i];
-                const uint32_t kind = meta >> 30, li = meta & 0x3FFFFFFFu;
+                const uint32_t kind = shadow_kind(meta), li = shadow_light(meta);
                 Ray r;
                 r.o = mk(o.x, o.y, o.z);
                 r.d = mk(d.x, d.y, d.z);
@@ -720,7 +346,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_shadow(DevScene S, CameraParams
             const uint32_t i = Q.sorder ? Q.sorder[k] : k;
             const float4 o = Q.so[i], d = Q.sd[i], c = Q.sc[i];
             const uint32_t meta = Q.smeta[i];
-            const uint32_t kind = meta >> 30, li = meta & 0x3FFFFFFFu;
+            const uint32_t kind = shadow_kind(meta), li = shadow_light(meta);
             Ray r;
             r.o = mk(o.x, o.y, o.z);
             r.d = mk(d.x, d.y, d.z);
@@ -733,19 +359,20 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_shadow(DevScene S, CameraParams
                 const DevLight &L = S.lights[li];
                 float tl = FLT_MAX;
                 const int lh = light_entity_hit(S, L, r, tl);
-                visible = !trace<Q_ANY>(S, r, false, 0.0f, lh ? tl : FLT_MAX, h, cnt, err, L.ent_index);
+                visible = !trace<Q_ANY, WT>(S, r, false, 0.0f, lh ? tl : FLT_MAX, h, cnt, err, L.ent_index);
             } else {
-                visible = !trace<Q_ANY>(S, r, false, 0.0f, kind == SHADOW_ANY ? FLT_MAX : d.w, h, cnt, err);
+                visible = !trace<Q_ANY, WT>(S, r, false, 0.0f, kind == SHADOW_ANY ? FLT_MAX : d.w, h, cnt, err);
             }
             if (visible) add_accum(Q.accum, __float_as_uint(c.w), mk(c.x, c.y, c.z));
         }
         return;
     }
     uint32_t *fetch = Q.counts + AZ_COUNT_FETCH + AZ_MAX_LEVELS + level;
-    Tracer<Q_ANY> T;
+    Tracer<Q_ANY, MODE == MODE_FETCHP, WT> T;
     uint2 stack[AZD_WSTACK];
     WarpFetch wf;
     uint32_t idx = kLaneIdle;
+    uint32_t si = 0;   // MULTI: the entry's scene
     float4 c = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     while (true) {
         if (wf.refill(fetch, n, idx)) {
@@ -753,7 +380,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_shadow(DevScene S, CameraParams
             const float4 o = Q.so[qi], d = Q.sd[qi];
             c = Q.sc[qi];
             const uint32_t meta = Q.smeta[qi];
-            const uint32_t kind = meta >> 30, li = meta & 0x3FFFFFFFu;
+            const uint32_t kind = shadow_kind(meta), li = shadow_light(meta);
+            if (MULTI) si = shadow_scene(meta);
+            const DevScene &Sq = MULTI ? Q.scenes[si] : S;
             Ray r;
             r.o = mk(o.x, o.y, o.z);
             r.d = mk(d.x, d.y, d.z);
@@ -761,16 +390,16 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_shadow(DevScene S, CameraParams
             if (kind == SHADOW_ENTITY_FULL) {
                 idx = kLaneIdle;   // k_shadow_full
             } else if (kind == SHADOW_ENTITY) {
-                const DevLight &L = S.lights[li];
+                const DevLight &L = Sq.lights[li];
                 float tl = FLT_MAX;
-                const int lh = light_entity_hit(S, L, r, tl);
-                T.init(S, r, false, 0.0f, lh ? tl : FLT_MAX, stack, L.ent_index);
+                const int lh = light_entity_hit(Sq, L, r, tl);
+                T.init(Sq, r, false, 0.0f, lh ? tl : FLT_MAX, stack, L.ent_index);
             } else {
-                T.init(S, r, false, 0.0f, kind == SHADOW_ANY ? FLT_MAX : d.w, stack);
+                T.init(Sq, r, false, 0.0f, kind == SHADOW_ANY ? FLT_MAX : d.w, stack);
             }
         }
         if (__all_sync(0xFFFFFFFFu, idx == kLaneDone)) break;
-        if (idx < n && T.step(S, stack, err)) {
+        if (idx < n && T.step(MULTI ? Q.scenes[si] : S, stack, err)) {
             if (!T.hit_any) add_accum(Q.accum, __float_as_uint(c.w), mk(c.x, c.y, c.z));
             T.flush_counts(cnt);
             idx = kLaneIdle;
@@ -811,6 +440,10 @@ __global__ void k_splat(CameraParams cam, WaveQueues Q, uint64_t wave_start, uin
     }
     if (i >= n) return;
     if (Q.counts[AZ_COUNT_OVERFLOW]) return;   // the wave is re-run
+    if (cam.sample_out) {
+        cam.sample_out[wave_start + i] = Q.accum[i];
+        return;
+    }
     splat_sample(cam, film, wave_start + i, Q.accum[i]);
 }
 
@@ -822,8 +455,6 @@ __global__ void k_splat_tiles(WaveQueues Q, uint32_t n, az_pixel *const *films) 
     const uint2 js = Q.slot_map[i];
     splat_sample(Q.job_cams[js.x], films[js.x], js.y, Q.accum[i]);
 }
-
-constexpr int kBlock = 128;
 
 // Launch configurations of the two traversal kernels: threads per block,
 // minimum resident blocks per SM (which caps registers), and whether warps
@@ -837,42 +468,10 @@ constexpr Variant kVariants[] = {{128, 1, MODE_LOOP},     {128, 6, MODE_LOOP},  
                                  {256, 1, MODE_LOOP},     {256, 3, MODE_LOOP},     {64, 1, MODE_LOOP},
                                  {64, 12, MODE_LOOP},     {128, 8, MODE_FETCH},    {128, 6, MODE_FETCH},
                                  {256, 3, MODE_FETCH},    {128, 8, MODE_LOCKSTEP}, {128, 6, MODE_LOCKSTEP},
-                                 {256, 3, MODE_LOCKSTEP}, {64, 12, MODE_LOCKSTEP}};
+                                 {256, 3, MODE_LOCKSTEP}, {64, 12, MODE_LOCKSTEP}, {128, 7, MODE_FETCH},
+                                 {128, 6, MODE_FETCHP},   {128, 7, MODE_FETCHP},   {128, 8, MODE_FETCHP}};
 constexpr uint32_t kVariantCount = sizeof(kVariants) / sizeof(kVariants[0]);
 static_assert(kVariantCount == AZ_LAUNCH_VARIANTS, "variant table and header disagree");
-
-template <uint32_t F>
-void LaunchShadeF(int grid, const DevScene &S, const CameraParams &cam, const WaveQueues &Q, uint64_t start,
-                  uint32_t L, cudaStream_t st, bool guided) {
-    if (Q.slot_map) k_shade<kBlock, F, false, true><<<grid, kBlock, 0, st>>>(S, cam, Q, start, L);   // tile wave
-    else if (guided) k_shade<kBlock, F, true><<<grid, kBlock, 0, st>>>(S, cam, Q, start, L);
-    else k_shade<kBlock, F, false><<<grid, kBlock, 0, st>>>(S, cam, Q, start, L);
-}
-
-// The shading kernel specialised for the scene's features (DevScene.features)
-// and for guided scattering (Q.lobes set).
-void LaunchShade(int grid, const DevScene &S, const CameraParams &cam, const WaveQueues &Q, uint64_t start,
-                 uint32_t L, cudaStream_t st) {
-    const bool guided = Q.lobes != nullptr;
-    switch (S.features & 15u) {
-        case 0: LaunchShadeF<0>(grid, S, cam, Q, start, L, st, guided); break;
-        case 1: LaunchShadeF<1>(grid, S, cam, Q, start, L, st, guided); break;
-        case 2: LaunchShadeF<2>(grid, S, cam, Q, start, L, st, guided); break;
-        case 3: LaunchShadeF<3>(grid, S, cam, Q, start, L, st, guided); break;
-        case 4: LaunchShadeF<4>(grid, S, cam, Q, start, L, st, guided); break;
-        case 5: LaunchShadeF<5>(grid, S, cam, Q, start, L, st, guided); break;
-        case 6: LaunchShadeF<6>(grid, S, cam, Q, start, L, st, guided); break;
-        case 7: LaunchShadeF<7>(grid, S, cam, Q, start, L, st, guided); break;
-        case 8: LaunchShadeF<8>(grid, S, cam, Q, start, L, st, guided); break;
-        case 9: LaunchShadeF<9>(grid, S, cam, Q, start, L, st, guided); break;
-        case 10: LaunchShadeF<10>(grid, S, cam, Q, start, L, st, guided); break;
-        case 11: LaunchShadeF<11>(grid, S, cam, Q, start, L, st, guided); break;
-        case 12: LaunchShadeF<12>(grid, S, cam, Q, start, L, st, guided); break;
-        case 13: LaunchShadeF<13>(grid, S, cam, Q, start, L, st, guided); break;
-        case 14: LaunchShadeF<14>(grid, S, cam, Q, start, L, st, guided); break;
-        default: LaunchShadeF<15>(grid, S, cam, Q, start, L, st, guided); break;
-    }
-}
 
 template <int B, int M, int P>
 void LaunchTraversal(bool shadow, int sms, const DevScene &S, const CameraParams &cam, const WaveQueues &Q,
@@ -884,7 +483,28 @@ void LaunchTraversal(bool shadow, int sms, const DevScene &S, const CameraParams
 
 void LaunchTraversalVariant(uint32_t v, bool shadow, int sms, const DevScene &S, const CameraParams &cam,
                             const WaveQueues &Q, uint32_t L, cudaStream_t st) {
-    if (shadow && S.full_light_queries) k_shadow_full<<<sms * 16, 128, 0, st>>>(S, cam, Q, L);
+    const int fgrid = sms * 16;
+    if (Q.scenes) {
+        // a tile wave of several scenes: one launch configuration, 128 threads, pop-first persistent fetching
+        if (cam.watertight) {
+            if (shadow && S.full_light_queries) k_shadow_full<true, true><<<fgrid, 128, 0, st>>>(S, cam, Q, L);
+            if (shadow) k_shadow<128, 6, MODE_FETCHP, true, true><<<fgrid, 128, 0, st>>>(S, cam, Q, L);
+            else k_extend<128, 6, MODE_FETCHP, true, true><<<fgrid, 128, 0, st>>>(S, cam, Q, L);
+        } else {
+            if (shadow && S.full_light_queries) k_shadow_full<false, true><<<fgrid, 128, 0, st>>>(S, cam, Q, L);
+            if (shadow) k_shadow<128, 6, MODE_FETCHP, false, true><<<fgrid, 128, 0, st>>>(S, cam, Q, L);
+            else k_extend<128, 6, MODE_FETCHP, false, true><<<fgrid, 128, 0, st>>>(S, cam, Q, L);
+        }
+        return;
+    }
+    if (cam.watertight) {
+        // the watertight test has one launch configuration: 128 threads, pop-first persistent fetching
+        if (shadow && S.full_light_queries) k_shadow_full<true><<<fgrid, 128, 0, st>>>(S, cam, Q, L);
+        if (shadow) k_shadow<128, 6, MODE_FETCHP, true><<<fgrid, 128, 0, st>>>(S, cam, Q, L);
+        else k_extend<128, 6, MODE_FETCHP, true><<<fgrid, 128, 0, st>>>(S, cam, Q, L);
+        return;
+    }
+    if (shadow && S.full_light_queries) k_shadow_full<false><<<fgrid, 128, 0, st>>>(S, cam, Q, L);
     switch (v) {
         case 0: LaunchTraversal<128, 1, MODE_LOOP>(shadow, sms, S, cam, Q, L, st); break;
         case 1: LaunchTraversal<128, 6, MODE_LOOP>(shadow, sms, S, cam, Q, L, st); break;
@@ -899,6 +519,10 @@ void LaunchTraversalVariant(uint32_t v, bool shadow, int sms, const DevScene &S,
         case 11: LaunchTraversal<128, 6, MODE_LOCKSTEP>(shadow, sms, S, cam, Q, L, st); break;
         case 12: LaunchTraversal<256, 3, MODE_LOCKSTEP>(shadow, sms, S, cam, Q, L, st); break;
         case 13: LaunchTraversal<64, 12, MODE_LOCKSTEP>(shadow, sms, S, cam, Q, L, st); break;
+        case 14: LaunchTraversal<128, 7, MODE_FETCH>(shadow, sms, S, cam, Q, L, st); break;
+        case 15: LaunchTraversal<128, 6, MODE_FETCHP>(shadow, sms, S, cam, Q, L, st); break;
+        case 16: LaunchTraversal<128, 7, MODE_FETCHP>(shadow, sms, S, cam, Q, L, st); break;
+        case 17: LaunchTraversal<128, 8, MODE_FETCHP>(shadow, sms, S, cam, Q, L, st); break;
         default: LaunchTraversal<128, 8, MODE_LOOP>(shadow, sms, S, cam, Q, L, st); break;
     }
 }
@@ -978,6 +602,29 @@ WaveBuffers::~WaveBuffers() {
     if (guide_rec) cudaFree(guide_rec);
     for (void *p : {(void *)okey[0], (void *)okey[1], (void *)oval, (void *)oidx_e, (void *)oidx_s, otemp})
         if (p) cudaFree(p);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (side) cudaStreamDestroy(side);
+}
+
+int WaveBuffers::EnsureSide() {
+    if (side) return AZ_OK;
+    // non-blocking: the side stream only ever runs after waiting on an event
+    // of the render stream, which orders it after the caller's earlier work
+    cudaStream_t s = nullptr;
+    cudaEvent_t f = nullptr, j = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&f, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&j, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+        if (f) cudaEventDestroy(f);
+        if (s) cudaStreamDestroy(s);
+        return CudaError(e, "creating the wave's side stream");
+    }
+    side = s;
+    ev_fork = f;
+    ev_join = j;
+    return AZ_OK;
 }
 
 int WaveBuffers::EnsureOrder(uint32_t cap) {
@@ -1108,6 +755,8 @@ struct TileWave {
     uint2 *slot_map;
     const CameraParams *cams;
     az_pixel *const *films;
+    const DevScene *scenes;   // jobs of several scenes: their device records (null: one scene)
+    const DevScene *dev;      // and the host record the launches are chosen for (null: the scene's own)
 };
 
 static int RenderWave(const GpuScene &G, const CameraParams &cam, WaveBuffers &W, uint64_t start, uint32_t n,
@@ -1117,7 +766,11 @@ static int RenderWave(const GpuScene &G, const CameraParams &cam, WaveBuffers &W
     if (tw) {
         Q.slot_map = tw->slot_map;
         Q.job_cams = tw->cams;
+        Q.scenes = tw->scenes;
     }
+    // the scene the launches are chosen for: a tile wave of several scenes
+    // passes one whose features, depth and light kinds cover all of them
+    const DevScene &D = tw && tw->dev ? *tw->dev : G.dev;
     if (capture) Q.wave = W.wave_dev;
     if (cam.order & kOrderExtend) Q.eorder = W.oidx_e;
     if (cam.order & kOrderShadow) Q.sorder = W.oidx_s;
@@ -1126,7 +779,7 @@ static int RenderWave(const GpuScene &G, const CameraParams &cam, WaveBuffers &W
     // sample's weight within twice cosine sampling's (the estimate stays
     // unbiased for any cap).  Inference-only renders use the learned value.
     Q.guide_alpha_max = train ? 0.5f : 1.0f;
-    const uint32_t levels = std::min<uint32_t>(G.dev.max_depth + 1, AZ_MAX_LEVELS - 2);
+    const uint32_t levels = std::min<uint32_t>(D.max_depth + 1, AZ_MAX_LEVELS - 2);
     if (guide) {
         // proposals for every queue entry this wave can hold (the queue is capped to match)
         int grc = GuidePrepareWave(*guide, W, Q, std::min<uint32_t>(Q.cap_q, n + n / 2 + 1024), train ? levels : 0u, st);
@@ -1147,28 +800,53 @@ static int RenderWave(const GpuScene &G, const CameraParams &cam, WaveBuffers &W
     rc.launches++;
     const int grid = sms * 16;
     const uint32_t v = cam.variant;
-    for (uint32_t L = 1; L <= levels; L++) {
+    // Level L's visibility queries need only its shading; level L+1's
+    // closest-hit queries need the same.  Run them side by side (visibility
+    // on the side stream) so that the tail of one fills with the other's work;
+    // the next shading waits for both.  Not with stage timing, nor with queue
+    // ordering (both orderings share one sort scratch).
+    const bool overlap = W.side && !timer && !cam.order && !cam.serial_levels;
+    if (overlap) {
+        LaunchTraversalVariant(v, false, sms, D, cam, Q, 1, st);
+        for (uint32_t L = 1; L <= levels; L++) {
+            if (guide && L + 1 <= D.max_depth + 1) {   // the deepest level spawns nothing to guide
+                int grc = GuideInfer(*guide, G, Q, L, st);
+                if (grc != AZ_OK) return grc;
+                rc.launches++;
+            }
+            LaunchShade(grid, D, cam, Q, start, L, st);
+            AZ_CUDA_TRY(cudaEventRecord(W.ev_fork, st));
+            AZ_CUDA_TRY(cudaStreamWaitEvent(W.side, W.ev_fork, 0));
+            LaunchTraversalVariant(cam.shadow_variant, true, sms, D, cam, Q, L, W.side);
+            AZ_CUDA_TRY(cudaEventRecord(W.ev_join, W.side));
+            if (L < levels) LaunchTraversalVariant(v, false, sms, D, cam, Q, L + 1, st);
+            AZ_CUDA_TRY(cudaStreamWaitEvent(st, W.ev_join, 0));
+            rc.launches += D.full_light_queries ? 4 : 3;
+            rc.extend_launches++;
+        }
+    }
+    for (uint32_t L = 1; L <= levels && !overlap; L++) {
         if (timer) timer->Mark(st, 0);
         if (cam.order & kOrderExtend) {
             int orc = OrderQueue(G, Q, W, L, 0, sms, st, rc);
             if (orc != AZ_OK) return orc;
         }
-        LaunchTraversalVariant(v, false, sms, G.dev, cam, Q, L, st);
-        if (guide && L + 1 <= G.dev.max_depth + 1) {   // the deepest level spawns nothing to guide
+        LaunchTraversalVariant(v, false, sms, D, cam, Q, L, st);
+        if (guide && L + 1 <= D.max_depth + 1) {   // the deepest level spawns nothing to guide
             int grc = GuideInfer(*guide, G, Q, L, st);
             if (grc != AZ_OK) return grc;
             rc.launches++;
         }
         if (timer) timer->Mark(st, 1);
-        LaunchShade(grid, G.dev, cam, Q, start, L, st);
+        LaunchShade(grid, D, cam, Q, start, L, st);
         if (timer) timer->Mark(st, 2);
         if (cam.order & kOrderShadow) {
             int orc = OrderQueue(G, Q, W, L, 1, sms, st, rc);
             if (orc != AZ_OK) return orc;
         }
-        LaunchTraversalVariant(cam.shadow_variant, true, sms, G.dev, cam, Q, L, st);
+        LaunchTraversalVariant(cam.shadow_variant, true, sms, D, cam, Q, L, st);
         if (timer) timer->Mark(st, 3);
-        rc.launches += G.dev.full_light_queries ? 4 : 3;
+        rc.launches += D.full_light_queries ? 4 : 3;
         rc.extend_launches++;
     }
     if (guide && train) {
@@ -1273,10 +951,11 @@ static uint32_t DefaultWave(uint32_t per_node_shadow, const WaveBuffers &W) {
 
 int Render(GpuScene &G, az_pixel *film, const az_camera *camera, const az_epsilon_values *eps, az_scissor sc,
            int32_t filter, uint32_t cull, const az_render_opts *opts, cudaStream_t st, az_render_stats *stats,
-           GuideState *guide, bool train, WaveBuffers *wave_buffers) {
+           GuideState *guide, bool train, WaveBuffers *wave_buffers, float4 *sample_out) {
     CameraParams cam;
     int rc = SetupCamera(camera, sc, filter, cull, eps, opts ? opts->seed : 0, cam);
     if (rc != AZ_OK) return rc;
+    cam.sample_out = sample_out;
     cam.count_traversal = opts && (opts->flags & AZ_FLAG_COUNT_TRAVERSAL) ? 1u : 0u;
     cam.env_importance = opts && (opts->flags & AZ_FLAG_ENV_IMPORTANCE) && G.dev.env_rows ? 1u : 0u;
     cam.variant = opts && opts->variant ? opts->variant - 1 : G.variant;
@@ -1284,8 +963,20 @@ int Render(GpuScene &G, az_pixel *film, const az_camera *camera, const az_epsilo
     // a variant the caller names applies to both traversal kernels
     cam.shadow_variant = (opts && opts->variant) || G.shadow_variant >= kVariantCount ? cam.variant : G.shadow_variant;
     cam.order = QueueOrder(G, opts);
+    cam.serial_levels = opts && (opts->flags & AZ_FLAG_SERIAL_LEVELS) ? 1u : 0u;
+    cam.watertight = opts && (opts->flags & AZ_FLAG_WATERTIGHT) ? 1u : 0u;
     if (G.dev.max_depth + 1 > AZ_MAX_LEVELS - 2) return SetError(AZ_ERR_UNSUPPORTED, "MaxRecursionDepth above 61");
-    uint64_t total = cam.npix * (uint64_t)cam.sqrt_spp * cam.sqrt_spp;
+    const uint64_t all = cam.npix * (uint64_t)cam.sqrt_spp * cam.sqrt_spp;
+    // a part of the camera-sample sequence (one GPU's share of a frame)
+    uint64_t begin = 0, end = all;
+    if (opts && opts->sample_parts > 1) {
+        if (opts->sample_part >= opts->sample_parts)
+            return SetError(AZ_ERR_INVALID_ARGUMENT, "sample_part must be below sample_parts");
+        begin = all / opts->sample_parts * opts->sample_part +
+                std::min<uint64_t>(opts->sample_part, all % opts->sample_parts);
+        end = begin + all / opts->sample_parts + (opts->sample_part < all % opts->sample_parts ? 1 : 0);
+    }
+    const uint64_t total = end - begin;
     if (stats) memset(stats, 0, sizeof(*stats));
     if (total == 0) return AZ_OK;
     int sms = 148;
@@ -1315,15 +1006,16 @@ int Render(GpuScene &G, az_pixel *film, const az_camera *camera, const az_epsilo
     // captured).
     const bool use_graph = !(opts && (opts->flags & AZ_FLAG_NO_GRAPH)) && !timer && !guide && st != nullptr &&
                            st != cudaStreamLegacy && st != cudaStreamPerThread;
-    uint64_t pos = 0;
-    while (pos < total) {
-        uint32_t n = (uint32_t)std::min<uint64_t>(chunk, total - pos);
+    uint64_t pos = begin;
+    while (pos < end) {
+        uint32_t n = (uint32_t)std::min<uint64_t>(chunk, end - pos);
         uint32_t cap_q = std::max<uint32_t>(n + n / 2, 1024);
         uint32_t cap_s = std::max<uint32_t>((uint32_t)std::min<uint64_t>((uint64_t)cap_q * std::max(per_node_shadow, 1u),
                                                                          (uint64_t)n * 4), 1024);
         rc = W.Ensure(n, cap_q, cap_s);
         if (rc != AZ_OK) return rc;
         if (cam.order && (rc = W.EnsureOrder(std::max(W.q.cap_q, W.q.cap_s))) != AZ_OK) return rc;
+        if (!cam.serial_levels && (rc = W.EnsureSide()) != AZ_OK) return rc;
         if (use_graph) {
             rc = ReplayWave(G, cam, W, pos, n, chunk, film, st, sms, counters);
         } else {
@@ -1349,6 +1041,8 @@ int Render(GpuScene &G, az_pixel *film, const az_camera *camera, const az_epsilo
         }
         counters.nodes += host_counts[AZ_COUNT_NODES];
         counters.prims += host_counts[AZ_COUNT_NODES + 1];
+        counters.snodes += host_counts[AZ_COUNT_SNODES];
+        counters.sprims += host_counts[AZ_COUNT_SNODES + 1];
         counters.chunks++;
         pos += n;
     }
@@ -1368,6 +1062,8 @@ int Render(GpuScene &G, az_pixel *film, const az_camera *camera, const az_epsilo
         stats->gpu_ms = ms;
         stats->node_visits = counters.nodes;
         stats->prim_visits = counters.prims;
+        stats->shadow_node_visits = counters.snodes;
+        stats->shadow_prim_visits = counters.sprims;
         stats->extend_launches = (uint32_t)counters.extend_launches;
         if (timer) {
             stats->extend_ms = timer->ms[0];
@@ -1379,25 +1075,57 @@ int Render(GpuScene &G, az_pixel *film, const az_camera *camera, const az_epsilo
 }
 
 int RenderTiles(GpuScene &G, std::vector<TileJob> &jobs, const az_render_opts *opts, cudaStream_t st,
-                az_render_stats *stats) {
+                az_render_stats *stats, cudaEvent_t origin) {
     if (stats) memset(stats, 0, sizeof(*stats));
     if (jobs.empty()) return AZ_OK;
-    if (G.dev.max_depth + 1 > AZ_MAX_LEVELS - 2) return SetError(AZ_ERR_UNSUPPORTED, "MaxRecursionDepth above 61");
     const uint32_t nj = (uint32_t)jobs.size();
+    // the jobs' scenes: one, or a table the kernels index per queue entry
+    std::vector<GpuScene *> scenes;
+    std::vector<uint32_t> scene_of(nj, 0);
+    for (uint32_t j = 0; j < nj; j++) {
+        GpuScene *sg = jobs[j].scene ? jobs[j].scene : &G;
+        if (sg->device != G.device) return SetError(AZ_ERR_INVALID_ARGUMENT, "tile jobs on different devices");
+        auto it = std::find(scenes.begin(), scenes.end(), sg);
+        if (it == scenes.end()) {
+            if (scenes.size() == kMaxWaveScenes)
+                return SetError(AZ_ERR_UNSUPPORTED, "a tile render of more than 256 scenes");
+            scenes.push_back(sg);
+            it = scenes.end() - 1;
+        }
+        scene_of[j] = (uint32_t)(it - scenes.begin());
+    }
+    const bool multi = scenes.size() > 1;
+    // the record the launches are chosen for: the first scene's, with the
+    // features, light kinds and depth of all of them
+    DevScene wave_dev = scenes[0]->dev;
+    uint32_t per_node_shadow = 0;
+    for (GpuScene *sg : scenes) {
+        const DevScene &d = sg->dev;
+        if (d.max_depth + 1 > AZ_MAX_LEVELS - 2) return SetError(AZ_ERR_UNSUPPORTED, "MaxRecursionDepth above 61");
+        wave_dev.features |= d.features;
+        wave_dev.full_light_queries |= d.full_light_queries;
+        wave_dev.max_depth = std::max(wave_dev.max_depth, d.max_depth);
+        per_node_shadow = std::max(per_node_shadow, d.light_count + (d.use_env_map ? 1u : 0u));
+    }
     std::vector<CameraParams> cams(nj);
     uint64_t total = 0;
     for (uint32_t j = 0; j < nj; j++) {
         const TileJob &J = jobs[j];
+        const GpuScene &Gj = *scenes[scene_of[j]];
         if (!J.film || !J.camera) return SetError(AZ_ERR_INVALID_ARGUMENT, "tile job without film or camera");
         CameraParams &c = cams[j];
         int rc = SetupCamera(J.camera, J.scissor, J.filter, J.cull, J.eps, J.seed, c);
         if (rc != AZ_OK) return rc;
+        c.scene = scene_of[j];
         c.count_traversal = opts && (opts->flags & AZ_FLAG_COUNT_TRAVERSAL) ? 1u : 0u;
-        c.env_importance = opts && (opts->flags & AZ_FLAG_ENV_IMPORTANCE) && G.dev.env_rows ? 1u : 0u;
+        c.env_importance = opts && (opts->flags & AZ_FLAG_ENV_IMPORTANCE) && Gj.dev.env_rows ? 1u : 0u;
         c.variant = opts && opts->variant ? opts->variant - 1 : G.variant;
         if (c.variant >= kVariantCount) return SetError(AZ_ERR_INVALID_ARGUMENT, "unknown launch variant");
         c.shadow_variant = (opts && opts->variant) || G.shadow_variant >= kVariantCount ? c.variant : G.shadow_variant;
-        c.order = QueueOrder(G, opts);
+        // several scenes: no queue ordering (its keys use one scene's bounds)
+        c.order = multi ? 0u : QueueOrder(G, opts);
+        c.serial_levels = opts && (opts->flags & AZ_FLAG_SERIAL_LEVELS) ? 1u : 0u;
+        c.watertight = opts && (opts->flags & AZ_FLAG_WATERTIGHT) ? 1u : 0u;
         // the traversal and shading kernels take these from the wave's first job
         if (c.eps_isect != cams[0].eps_isect || c.eps_shadow != cams[0].eps_shadow || c.cull != cams[0].cull)
             return SetError(AZ_ERR_INVALID_ARGUMENT, "the jobs of a tile render need the same epsilons and culling");
@@ -1420,7 +1148,6 @@ int RenderTiles(GpuScene &G, std::vector<TileJob> &jobs, const az_render_opts *o
     }
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, G.device);
-    const uint32_t per_node_shadow = G.dev.light_count + (G.dev.use_env_map ? 1u : 0u);
     uint32_t chunk = opts && opts->chunk_samples ? opts->chunk_samples : DefaultWave(per_node_shadow, G.waves);
     chunk = std::max<uint32_t>(chunk, kTile);
     WaveBuffers &W = G.waves;
@@ -1430,7 +1157,7 @@ int RenderTiles(GpuScene &G, std::vector<TileJob> &jobs, const az_render_opts *o
         ~DevBuf() {
             if (p) cudaFree(p);
         }
-    } d_cams, d_films, d_tiles, d_next, d_slots;
+    } d_cams, d_films, d_tiles, d_next, d_slots, d_scenes;
     std::vector<az_pixel *> films(nj);
     for (uint32_t j = 0; j < nj; j++) films[j] = jobs[j].film;
     AZ_CUDA_TRY(cudaMalloc(&d_cams.p, nj * sizeof(CameraParams)));
@@ -1440,6 +1167,13 @@ int RenderTiles(GpuScene &G, std::vector<TileJob> &jobs, const az_render_opts *o
     AZ_CUDA_TRY(cudaMalloc(&d_slots.p, (size_t)chunk * sizeof(uint2)));
     AZ_CUDA_TRY(cudaMemcpyAsync(d_cams.p, cams.data(), nj * sizeof(CameraParams), cudaMemcpyHostToDevice, st));
     AZ_CUDA_TRY(cudaMemcpyAsync(d_films.p, films.data(), nj * sizeof(az_pixel *), cudaMemcpyHostToDevice, st));
+    std::vector<DevScene> scene_recs;
+    if (multi) {
+        for (GpuScene *sg : scenes) scene_recs.push_back(sg->dev);
+        AZ_CUDA_TRY(cudaMalloc(&d_scenes.p, scene_recs.size() * sizeof(DevScene)));
+        AZ_CUDA_TRY(cudaMemcpyAsync(d_scenes.p, scene_recs.data(), scene_recs.size() * sizeof(DevScene),
+                                    cudaMemcpyHostToDevice, st));
+    }
     struct Events {
         cudaEvent_t e0 = nullptr, e1 = nullptr;
         ~Events() {
@@ -1470,9 +1204,11 @@ int RenderTiles(GpuScene &G, std::vector<TileJob> &jobs, const az_render_opts *o
         int rc = W.Ensure(n, cap_q, cap_s);
         if (rc != AZ_OK) return rc;
         if (cams[0].order && (rc = W.EnsureOrder(std::max(W.q.cap_q, W.q.cap_s))) != AZ_OK) return rc;
+        if (!cams[0].serial_levels && (rc = W.EnsureSide()) != AZ_OK) return rc;
         AZ_CUDA_TRY(cudaMemcpyAsync(d_tiles.p, tiles.data() + ti, ntiles * sizeof(Tile), cudaMemcpyHostToDevice, st));
         TileWave tw{(const Tile *)d_tiles.p, ntiles, (uint32_t *)d_next.p, (uint2 *)d_slots.p,
-                    (const CameraParams *)d_cams.p, (az_pixel *const *)d_films.p};
+                    (const CameraParams *)d_cams.p, (az_pixel *const *)d_films.p,
+                    multi ? (const DevScene *)d_scenes.p : nullptr, multi ? &wave_dev : nullptr};
         rc = RenderWave(G, cams[0], W, 0, n, nullptr, st, sms, counters, nullptr, nullptr, false, false, &tw);
         if (rc != AZ_OK) return rc;
         AZ_CUDA_TRY(cudaMemcpyAsync(host_counts.data(), W.q.counts, AZ_COUNT_TOTAL * sizeof(uint32_t),
@@ -1489,7 +1225,7 @@ int RenderTiles(GpuScene &G, std::vector<TileJob> &jobs, const az_render_opts *o
             continue;
         }
         float ms = 0.0f;
-        cudaEventElapsedTime(&ms, ev.e0, ev.e1);
+        cudaEventElapsedTime(&ms, origin ? origin : ev.e0, ev.e1);
         for (uint32_t j = 0; j < nj; j++)
             if (last_tile[j] > ti && last_tile[j] <= te) jobs[j].done_ms = ms;
         for (uint32_t L = 1; L < AZ_MAX_LEVELS; L++) {
@@ -1498,6 +1234,8 @@ int RenderTiles(GpuScene &G, std::vector<TileJob> &jobs, const az_render_opts *o
         }
         counters.nodes += host_counts[AZ_COUNT_NODES];
         counters.prims += host_counts[AZ_COUNT_NODES + 1];
+        counters.snodes += host_counts[AZ_COUNT_SNODES];
+        counters.sprims += host_counts[AZ_COUNT_SNODES + 1];
         counters.chunks++;
         ti = te;
     }
@@ -1513,6 +1251,8 @@ int RenderTiles(GpuScene &G, std::vector<TileJob> &jobs, const az_render_opts *o
         stats->gpu_ms = ms;
         stats->node_visits = counters.nodes;
         stats->prim_visits = counters.prims;
+        stats->shadow_node_visits = counters.snodes;
+        stats->shadow_prim_visits = counters.sprims;
         stats->extend_launches = (uint32_t)counters.extend_launches;
     }
     return AZ_OK;
@@ -1618,6 +1358,7 @@ int Autotune(GpuScene &G, const az_camera *camera, const az_epsilon_values *eps,
 
 // ---- closest-hit queries for the parity tests ----
 namespace {
+template <bool WT>
 __global__ void k_closest(DevScene S, const az_ray3 *rays, uint32_t n, uint32_t cull, float eps, uint32_t *hit,
                           uint32_t *uid, uint32_t *face, float *t) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1628,7 +1369,7 @@ __global__ void k_closest(DevScene S, const az_ray3 *rays, uint32_t n, uint32_t 
     r.d = mk(rr.Direction.x, rr.Direction.y, rr.Direction.z);
     r.time = rr.T;
     Hit h;
-    bool ok = trace<Q_CLOSEST>(S, r, cull != 0, eps, FLT_MAX, h);
+    bool ok = trace<Q_CLOSEST, WT>(S, r, cull != 0, eps, FLT_MAX, h);
     hit[i] = ok ? 1u : 0u;
     uid[i] = ok ? S.ents[h.ent].uid : 0xFFFFFFFFu;
     face[i] = ok && h.prim != 0xFFFFFFFFu ? S.tri_attr[h.prim].face_id : 0xFFFFFFFFu;
@@ -1637,7 +1378,7 @@ __global__ void k_closest(DevScene S, const az_ray3 *rays, uint32_t n, uint32_t 
 }  // namespace
 
 int ClosestHit(GpuScene &G, const az_ray3 *rays, uint32_t n, int32_t cull, float eps, uint32_t *out_hit,
-               uint32_t *out_uid, uint32_t *out_face, float *out_t, cudaStream_t st) {
+               uint32_t *out_uid, uint32_t *out_face, float *out_t, cudaStream_t st, bool watertight) {
     if (n == 0) return AZ_OK;
     void *buf = nullptr;
     size_t bytes = (size_t)n * (sizeof(az_ray3) + 3 * sizeof(uint32_t) + sizeof(float)) + 64;
@@ -1652,7 +1393,12 @@ int ClosestHit(GpuScene &G, const az_ray3 *rays, uint32_t n, int32_t cull, float
     int rc = AZ_OK;
     cudaError_t e = cudaMemcpyAsync(d_rays, rays, (size_t)n * sizeof(az_ray3), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) {
-        k_closest<<<(n + 127) / 128, 128, 0, st>>>(G.dev, d_rays, n, (uint32_t)cull, eps, d_hit, d_uid, d_face, d_t);
+        if (watertight)
+            k_closest<true><<<(n + 127) / 128, 128, 0, st>>>(G.dev, d_rays, n, (uint32_t)cull, eps, d_hit, d_uid,
+                                                              d_face, d_t);
+        else
+            k_closest<false><<<(n + 127) / 128, 128, 0, st>>>(G.dev, d_rays, n, (uint32_t)cull, eps, d_hit, d_uid,
+                                                               d_face, d_t);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaMemcpyAsync(out_hit, d_hit, n * 4, cudaMemcpyDeviceToHost, st);
@@ -1755,6 +1501,15 @@ extern "C" int az_gpu_render_noalloc(az_gpu_scene *scene, az_pixel *film, const 
     if (cam.variant >= kVariantCount) return SetError(AZ_ERR_INVALID_ARGUMENT, "unknown launch variant");
     // a variant the caller names applies to both traversal kernels
     cam.shadow_variant = (opts && opts->variant) || G.shadow_variant >= kVariantCount ? cam.variant : G.shadow_variant;
+    // flags whose work would need buffers of their own or a statistics output
+    const uint32_t flags = opts ? opts->flags : 0u;
+    const uint32_t refused = AZ_FLAG_COUNT_TRAVERSAL | AZ_FLAG_TIME_STAGES | AZ_FLAG_ORDER_SHADOW | AZ_FLAG_ORDER_EXTEND;
+    if (flags & refused)
+        return SetError(AZ_ERR_INVALID_ARGUMENT,
+                        "az_gpu_render_noalloc does not take AZ_FLAG_COUNT_TRAVERSAL, AZ_FLAG_TIME_STAGES, "
+                        "AZ_FLAG_ORDER_SHADOW or AZ_FLAG_ORDER_EXTEND");
+    cam.env_importance = (flags & AZ_FLAG_ENV_IMPORTANCE) && G.dev.env_rows ? 1u : 0u;
+    cam.watertight = (flags & AZ_FLAG_WATERTIGHT) ? 1u : 0u;
     const uint64_t total = cam.npix * (uint64_t)cam.sqrt_spp * cam.sqrt_spp;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);

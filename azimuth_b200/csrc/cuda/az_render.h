@@ -8,6 +8,10 @@
 #include "az_device_math.cuh"
 #include "az_guide.cuh"
 
+namespace azd {
+struct DevScene;
+}
+
 namespace az {
 
 constexpr uint32_t AZ_MAX_LEVELS = 64;                   // tree levels kept in the counters
@@ -15,6 +19,7 @@ constexpr uint32_t AZ_COUNT_SHADOW = AZ_MAX_LEVELS;      // shadow-queue sizes p
 constexpr uint32_t AZ_COUNT_OVERFLOW = 2 * AZ_MAX_LEVELS;
 constexpr uint32_t AZ_COUNT_NODES = 2 * AZ_MAX_LEVELS + 2;  // node visits, primitive visits
 constexpr uint32_t AZ_COUNT_ERROR = 2 * AZ_MAX_LEVELS + 4;  // traversal step limit reached
+constexpr uint32_t AZ_COUNT_SNODES = 2 * AZ_MAX_LEVELS + 5; // visibility queries: node visits, primitive visits
 constexpr uint32_t AZ_COUNT_FETCH = 2 * AZ_MAX_LEVELS + 8;  // per level: extend, then shadow work counters
 constexpr uint32_t AZ_COUNT_TOTAL = 4 * AZ_MAX_LEVELS + 8;
 
@@ -37,6 +42,12 @@ struct CameraParams {
     uint32_t shadow_variant;       // launch configuration of the shadow queries
     uint32_t env_importance;       // AZ_FLAG_ENV_IMPORTANCE
     uint32_t order;                // kOrderShadow | kOrderExtend: queues visited in sorted order
+    uint32_t serial_levels;        // AZ_FLAG_SERIAL_LEVELS: no overlap of a level's visibility queries
+                                   // with the next level's closest-hit queries
+    uint32_t watertight;           // AZ_FLAG_WATERTIGHT: triangles by the watertight test
+    uint32_t scene;                // a tile wave of several scenes: the job's index in WaveQueues.scenes
+    float4 *sample_out;            // per-sample radiance output (az_gpu_render_samples): sample s of the
+                                   // scissor at [s] instead of a splat into the film; null: splat
 };
 
 constexpr uint32_t kOrderShadow = 1, kOrderExtend = 2;
@@ -69,6 +80,11 @@ struct WaveQueues {
     // camera; null: every sample belongs to the kernels' `cam`
     const uint2 *slot_map;
     const CameraParams *job_cams;
+    // a tile wave whose jobs render different scenes: the scenes' device
+    // records; every path entry carries its scene index in its flags (bits
+    // 16-23) and every shadow entry in its meta word (bits 22-29); null: the
+    // kernels' own scene argument
+    const azd::DevScene *scenes;
 };
 
 // One tile of a tile wave: samples [first, first + count) of job `job`, at
@@ -98,14 +114,20 @@ struct WaveBuffers {
     void *otemp = nullptr;
     size_t otemp_bytes = 0;
     uint32_t ocap = 0;
+    // second stream of a wave: a level's visibility queries run on it beside
+    // the next level's closest-hit queries (fork after shading, join before
+    // the next shading)
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     ~WaveBuffers();
+    int EnsureSide();
     int EnsureOrder(uint32_t cap);
     void DropGraph();
     int Ensure(uint32_t chunk, uint32_t cap_q, uint32_t cap_s);
 };
 
 struct RenderCounters {
-    uint64_t extend = 0, shadow = 0, nodes = 0, prims = 0, launches = 0, extend_launches = 0;
+    uint64_t extend = 0, shadow = 0, nodes = 0, prims = 0, snodes = 0, sprims = 0, launches = 0, extend_launches = 0;
     uint32_t chunks = 0, retries = 0;
 };
 

@@ -25,6 +25,15 @@ struct __align__(16) DevTri {
     float4 c;  // E2.z FN.x FN.y FN.z     (face normal, for back-face culling)
 };
 
+// The exact vertices of a triangle: the input of the hierarchy build (boxes)
+// and the operands of the watertight test (AZ_FLAG_WATERTIGHT), which needs the
+// shared vertices of neighbouring triangles bit for bit.
+struct __align__(16) DevTriVerts {
+    float4 a;  // P0.x P0.y P0.z P1.x
+    float4 b;  // P1.y P1.z P2.x P2.y
+    float4 c;  // P2.z FN.x FN.y FN.z     (face normal)
+};
+
 struct __align__(16) DevTriAttr {
     float n0[3], n1[3], n2[3];
     float uv0[2], uv1[2], uv2[2];
@@ -149,6 +158,7 @@ enum : uint32_t { FEAT_TEXTURES = 1u, FEAT_ENV = 2u, FEAT_SPECIAL = 4u, FEAT_ANA
 // Everything a kernel needs, passed by value.
 struct DevScene {
     const DevTri *tris;
+    const DevTriVerts *tri_verts;   // the same triangles' exact vertices (watertight test)
     const DevTriAttr *tri_attr;
     const DevEntity *ents;
     const DevGroup *groups;

@@ -99,7 +99,7 @@ struct GroupKey {
 
 struct HostGroup {
     azd::DevGroup g{};
-    std::vector<azd::DevTri> tris;
+    std::vector<azd::DevTriVerts> tris;   // exact vertices; the Cramer operands are made on the GPU
     std::vector<azd::DevTriAttr> attr;
     std::vector<uint32_t> soup_meshes;   // meshes of the soup whose triangles follow `tris` on the device
     std::vector<uint32_t> soup_extra;    // then further placements of soup meshes (Flattener::extra)
@@ -162,12 +162,11 @@ struct Flattener {
     }
 
     bool AddTriangle(HostGroup &g, const az_entity *t, uint32_t ent) {
-        azd::DevTri tr;
+        azd::DevTriVerts tr;
         const az_vec3 &p0 = t->P0, &p1 = t->P1, &p2 = t->P2;
-        // E1 = P0-P1 and E2 = P0-P2 in float: the A..H of src/azimuth_main.cpp:158-168
-        tr.a = make_float4(p0.x, p0.y, p0.z, p0.x - p1.x);
-        tr.b = make_float4(p0.y - p1.y, p0.z - p1.z, p0.x - p2.x, p0.y - p2.y);
-        tr.c = make_float4(p0.z - p2.z, t->FaceNormal.x, t->FaceNormal.y, t->FaceNormal.z);
+        tr.a = make_float4(p0.x, p0.y, p0.z, p1.x);
+        tr.b = make_float4(p1.y, p1.z, p2.x, p2.y);
+        tr.c = make_float4(p2.z, t->FaceNormal.x, t->FaceNormal.y, t->FaceNormal.z);
         g.tris.push_back(tr);
         azd::DevTriAttr a;
         memset(&a, 0, sizeof(a));
@@ -374,12 +373,24 @@ struct TempBuf {
     bool alloc(size_t n) { return cudaMalloc((void **)&p, (n ? n : 1) * sizeof(T)) != cudaSuccess; }   // true on failure
 };
 
-__global__ void k_gather_tris(const azd::DevTri *src, const azd::DevTriAttr *src_attr, const uint32_t *perm,
-                              uint32_t n, azd::DevTri *dst, azd::DevTriAttr *dst_attr) {
+// The primitives in wide-leaf order: the exact vertices, and the operands of
+// azimuth's Cramer test -- P0, E1 = P0 - P1 and E2 = P0 - P2 in float, the
+// A..H of src/azimuth_main.cpp:154-164 (a float subtraction rounds the same
+// on the host and here) -- plus the face normal.
+__global__ void k_gather_tris(const azd::DevTriVerts *src, const azd::DevTriAttr *src_attr, const uint32_t *perm,
+                              uint32_t n, azd::DevTri *dst, azd::DevTriVerts *dst_verts, azd::DevTriAttr *dst_attr) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     uint32_t s = perm[i];
-    dst[i] = src[s];
+    const azd::DevTriVerts v = src[s];
+    const float p0x = v.a.x, p0y = v.a.y, p0z = v.a.z, p1x = v.a.w, p1y = v.b.x, p1z = v.b.y;
+    const float p2x = v.b.z, p2y = v.b.w, p2z = v.c.x;
+    azd::DevTri t;
+    t.a = make_float4(p0x, p0y, p0z, __fsub_rn(p0x, p1x));
+    t.b = make_float4(__fsub_rn(p0y, p1y), __fsub_rn(p0z, p1z), __fsub_rn(p0x, p2x), __fsub_rn(p0y, p2y));
+    t.c = make_float4(__fsub_rn(p0z, p2z), v.c.y, v.c.z, v.c.w);
+    dst[i] = t;
+    dst_verts[i] = v;
     dst_attr[i] = src_attr[s];
 }
 
@@ -388,14 +399,12 @@ __global__ void k_gather_u32(const uint32_t *src, const uint32_t *perm, uint32_t
     if (i < n) dst[i] = src[perm[i]];
 }
 
-__global__ void k_tri_boxes(const azd::DevTri *t, uint32_t n, float4 *lo, float4 *hi) {
+__global__ void k_tri_boxes(const azd::DevTriVerts *t, uint32_t n, float4 *lo, float4 *hi) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    azd::DevTri tr = t[i];
-    float p0x = tr.a.x, p0y = tr.a.y, p0z = tr.a.z;
-    // P1 = P0 - E1, P2 = P0 - E2 recomputed only for bounds: widen by one ulp
-    float p1x = p0x - tr.a.w, p1y = p0y - tr.b.x, p1z = p0z - tr.b.y;
-    float p2x = p0x - tr.b.z, p2y = p0y - tr.b.w, p2z = p0z - tr.c.x;
+    const azd::DevTriVerts tr = t[i];
+    const float p0x = tr.a.x, p0y = tr.a.y, p0z = tr.a.z, p1x = tr.a.w, p1y = tr.b.x, p1z = tr.b.y;
+    const float p2x = tr.b.z, p2y = tr.b.w, p2z = tr.c.x;
     float4 l = make_float4(fminf(p0x, fminf(p1x, p2x)), fminf(p0y, fminf(p1y, p2y)), fminf(p0z, fminf(p1z, p2z)), 0);
     float4 h = make_float4(fmaxf(p0x, fmaxf(p1x, p2x)), fmaxf(p0y, fmaxf(p1y, p2y)), fmaxf(p0z, fmaxf(p1z, p2z)), 0);
     l.x = nextafterf(l.x, -FLT_MAX); l.y = nextafterf(l.y, -FLT_MAX); l.z = nextafterf(l.z, -FLT_MAX);
@@ -676,7 +685,7 @@ int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_
     // Build-only buffers are freed when the build ends; the scene keeps the
     // sorted primitives, the wide nodes and the top-level primitive list.
     const size_t nmax = std::max((size_t)total_tris, tlas.size()) + 1;
-    TempBuf<azd::DevTri> d_tris_unsorted;
+    TempBuf<azd::DevTriVerts> d_tris_unsorted;
     TempBuf<azd::DevTriAttr> d_attr_unsorted;
     TempBuf<azd::BVHNode> d_nodes;
     TempBuf<uint2> d_range;
@@ -684,9 +693,10 @@ int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_
     TempBuf<uint32_t> d_perm, d_comp, d_tlas_unsorted;
     TempBuf<azd::WideNode> d_wide_tmp;
     azd::DevTri *d_tris = (azd::DevTri *)G->Alloc(total_tris * sizeof(azd::DevTri));
+    azd::DevTriVerts *d_verts = (azd::DevTriVerts *)G->Alloc(total_tris * sizeof(azd::DevTriVerts));
     azd::DevTriAttr *d_attr = (azd::DevTriAttr *)G->Alloc(total_tris * sizeof(azd::DevTriAttr));
     uint32_t *d_tlas = (uint32_t *)G->Alloc((tlas.size() + 1) * sizeof(uint32_t));
-    if (!d_tris || !d_attr || !d_tlas || d_tris_unsorted.alloc(total_tris) ||
+    if (!d_tris || !d_verts || !d_attr || !d_tlas || d_tris_unsorted.alloc(total_tris) ||
         d_attr_unsorted.alloc(total_tris) || d_nodes.alloc(node_total) || d_range.alloc(node_total) ||
         d_lo.alloc(nmax) || d_hi.alloc(nmax) || d_perm.alloc(nmax) || d_comp.alloc(nmax) ||
         d_tlas_unsorted.alloc(tlas.size() + 1) || d_wide_tmp.alloc(node_total))
@@ -694,8 +704,8 @@ int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_
     const auto t_up0 = std::chrono::steady_clock::now();
     for (auto &g : F.groups) {
         if (g.tris.empty()) continue;
-        AZ_CUDA_TRY(cudaMemcpyAsync(d_tris_unsorted.p + g.g.tri_begin, g.tris.data(), g.tris.size() * sizeof(azd::DevTri),
-                                    cudaMemcpyHostToDevice, st));
+        AZ_CUDA_TRY(cudaMemcpyAsync(d_tris_unsorted.p + g.g.tri_begin, g.tris.data(),
+                                    g.tris.size() * sizeof(azd::DevTriVerts), cudaMemcpyHostToDevice, st));
         AZ_CUDA_TRY(cudaMemcpyAsync(d_attr_unsorted.p + g.g.tri_begin, g.attr.data(),
                                     g.attr.size() * sizeof(azd::DevTriAttr), cudaMemcpyHostToDevice, st));
     }
@@ -713,7 +723,7 @@ int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_
                                     cudaMemcpyHostToDevice, st));
     AZ_CUDA_TRY(cudaStreamSynchronize(st));
     for (auto &g : F.groups) {
-        std::vector<azd::DevTri>().swap(g.tris);
+        std::vector<azd::DevTriVerts>().swap(g.tris);
         std::vector<azd::DevTriAttr>().swap(g.attr);
     }
     const auto t_up1 = std::chrono::steady_clock::now();
@@ -741,7 +751,8 @@ int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_
         node_base += n > 1 ? n - 1 : 1;
         k_gather_tris<<<(n + B - 1) / B, B, 0, st>>>(d_tris_unsorted.p + g.g.tri_begin,
                                                      d_attr_unsorted.p + g.g.tri_begin, d_comp.p, n,
-                                                     d_tris + g.g.tri_begin, d_attr + g.g.tri_begin);
+                                                     d_tris + g.g.tri_begin, d_verts + g.g.tri_begin,
+                                                     d_attr + g.g.tri_begin);
         AZ_CUDA_TRY(cudaGetLastError());
         G->hierarchies++;
     }
@@ -780,6 +791,7 @@ int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_
 
     azd::DevScene &D = G->dev;
     D.tris = d_tris;
+    D.tri_verts = d_verts;
     D.tri_attr = d_attr;
     D.ents = Upload(*G, F.ents, st, rc);
     D.groups = Upload(*G, dgroups, st, rc);

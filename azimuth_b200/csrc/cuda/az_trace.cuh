@@ -110,6 +110,84 @@ __device__ __forceinline__ bool tri_test(const DevTri &tr, const Ray &r, bool cu
     return true;
 }
 
+// Watertight ray/triangle test (Woop, Benthin, Wald, "Watertight Ray/Triangle
+// Intersection", JCGT 2(1), 2013), the production alternative to azimuth's
+// Cramer test (AZ_FLAG_WATERTIGHT).  The ray is sheared once so that it runs
+// along +z; a triangle's vertices, taken relative to the origin and sheared
+// the same way, give three 2D edge functions whose signs decide the hit.
+// Neighbouring triangles compute the edge functions of a shared edge from the
+// same vertex bits with the same operations, so the values are exact
+// negatives of each other and no ray passes between them; a zero edge value
+// is recomputed in double precision.  Every product and sum below is an
+// explicit round-to-nearest operation, never fused.
+struct WtRay {
+    uint32_t kx, ky, kz;   // the axes of the sheared frame; kz = largest |d|
+    float sx, sy, sz;      // shear d[kx]/d[kz], d[ky]/d[kz] and scale 1/d[kz]
+};
+
+__device__ __forceinline__ WtRay wt_setup(f3 d) {
+    const float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
+    WtRay w;
+    w.kz = ax > ay ? (ax > az ? 0u : 2u) : (ay > az ? 1u : 2u);
+    w.kx = w.kz == 2u ? 0u : w.kz + 1u;
+    w.ky = w.kx == 2u ? 0u : w.kx + 1u;
+    const float dz = comp(d, (int)w.kz);
+    if (dz < 0.0f) {   // keep the winding: swap the other two axes
+        const uint32_t k = w.kx;
+        w.kx = w.ky;
+        w.ky = k;
+    }
+    w.sx = comp(d, (int)w.kx) / dz;
+    w.sy = comp(d, (int)w.ky) / dz;
+    w.sz = 1.0f / dz;
+    return w;
+}
+
+__device__ __forceinline__ bool tri_test_wt(const DevTriVerts &v, const Ray &r, const WtRay &w, bool cull, float eps,
+                                            float tmax, float &t_out) {
+    if (cull) {
+        f3 fn = mk(v.c.y, v.c.z, v.c.w);
+        if (!(dot(r.d, fn) < 0.0f)) return false;   // azimuth's back-face rule
+    }
+    const f3 A = mk(__fsub_rn(v.a.x, r.o.x), __fsub_rn(v.a.y, r.o.y), __fsub_rn(v.a.z, r.o.z));
+    const f3 B = mk(__fsub_rn(v.a.w, r.o.x), __fsub_rn(v.b.x, r.o.y), __fsub_rn(v.b.y, r.o.z));
+    const f3 C = mk(__fsub_rn(v.b.z, r.o.x), __fsub_rn(v.b.w, r.o.y), __fsub_rn(v.c.x, r.o.z));
+    const float Az = comp(A, (int)w.kz), Bz = comp(B, (int)w.kz), Cz = comp(C, (int)w.kz);
+    const float Ax = __fsub_rn(comp(A, (int)w.kx), __fmul_rn(w.sx, Az));
+    const float Ay = __fsub_rn(comp(A, (int)w.ky), __fmul_rn(w.sy, Az));
+    const float Bx = __fsub_rn(comp(B, (int)w.kx), __fmul_rn(w.sx, Bz));
+    const float By = __fsub_rn(comp(B, (int)w.ky), __fmul_rn(w.sy, Bz));
+    const float Cx = __fsub_rn(comp(C, (int)w.kx), __fmul_rn(w.sx, Cz));
+    const float Cy = __fsub_rn(comp(C, (int)w.ky), __fmul_rn(w.sy, Cz));
+    float U = __fsub_rn(__fmul_rn(Cx, By), __fmul_rn(Cy, Bx));
+    float V = __fsub_rn(__fmul_rn(Ax, Cy), __fmul_rn(Ay, Cx));
+    float W = __fsub_rn(__fmul_rn(Bx, Ay), __fmul_rn(By, Ax));
+    if (U == 0.0f || V == 0.0f || W == 0.0f) {
+        // on an edge in float: decide in double, where these products are exact
+        U = (float)__dsub_rn(__dmul_rn((double)Cx, (double)By), __dmul_rn((double)Cy, (double)Bx));
+        V = (float)__dsub_rn(__dmul_rn((double)Ax, (double)Cy), __dmul_rn((double)Ay, (double)Cx));
+        W = (float)__dsub_rn(__dmul_rn((double)Bx, (double)Ay), __dmul_rn((double)By, (double)Ax));
+    }
+    if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
+    const float det = __fadd_rn(__fadd_rn(U, V), W);
+    if (det == 0.0f) return false;
+    const float T = __fadd_rn(__fadd_rn(__fmul_rn(U, __fmul_rn(w.sz, Az)), __fmul_rn(V, __fmul_rn(w.sz, Bz))),
+                              __fmul_rn(W, __fmul_rn(w.sz, Cz)));
+    const float t = T / det;
+    if (!(t > eps && t < tmax)) return false;
+    t_out = t;
+    return true;
+}
+
+__device__ __forceinline__ DevTriVerts load_tri_verts(const DevTriVerts *v, uint32_t i) {
+    const float4 *p = reinterpret_cast<const float4 *>(v + i);
+    DevTriVerts t;
+    t.a = __ldg(p + 0);
+    t.b = __ldg(p + 1);
+    t.c = __ldg(p + 2);
+    return t;
+}
+
 // Reciprocal direction for the box tests; components are kept at most 1e18
 // in magnitude so that 2^23 * grid step * 1/d stays finite.
 __device__ __forceinline__ f3 safe_inv(f3 d) {
@@ -232,6 +310,14 @@ __device__ __forceinline__ float group_world_t(const DevGroup &g, const Ray &wr,
     return length(wp - o2 - motion) / length(wr.d);
 }
 
+// Factor from a world distance along d to the group's local distance
+// (|inv * d| / |d|) with a margin of 1e-4 for rounding; exactly 1.0001 for an
+// identity group, whose vector transform returns d unchanged.
+__device__ __forceinline__ float group_t_scale(const DevGroup &g, f3 d) {
+    if (g.identity) return 1.0001f;
+    return length(vector_xf(g.inv, d)) / length(d) * 1.0001f;
+}
+
 // Two-level traversal of the 8-wide hierarchy, after the node-group /
 // primitive-group scheme of Ylitie, Karras, Laine, "Efficient Incoherent Ray
 // Traversal on GPUs Through Compressed Wide BVHs" (HPG 2017): each step
@@ -244,11 +330,16 @@ __device__ __forceinline__ float group_world_t(const DevGroup &g, const Ray &wr,
 // Q_CLOSEST: nearest hit in `best` (best.ent == 0xFFFFFFFF: none).
 // Q_ANY: `hit_any` is set as soon as a primitive's world t < tmax.
 // `skip_ent` is an entity whose primitives are ignored (0xFFFFFFFF: none).
-template <QueryKind KIND>
+template <QueryKind KIND, bool WT = false>
 __device__ bool trace(const DevScene &S, const Ray &wr, bool cull, float eps, float tmax, Hit &best,
                       uint32_t *counts = nullptr, uint32_t *err = nullptr, uint32_t skip_ent = 0xFFFFFFFFu);
 
-template <QueryKind KIND>
+// POP_FIRST: a step that starts with both current groups empty pops the
+// stack until it holds a node or primitive group and visits it in the same
+// step (a finished query is reported at the end of its last step); otherwise
+// a step ends with the pop and the popped group waits for the next step.
+// WT: triangles by the watertight test instead of azimuth's Cramer test.
+template <QueryKind KIND, bool POP_FIRST = false, bool WT = false>
 struct Tracer {
     Ray wr;                    // world ray
     Ray r;                     // ray in the current space (world or a group's local space)
@@ -265,6 +356,7 @@ struct Tracer {
     uint32_t steps, nodes_visited, prims_visited;
     int sp;
     Hit best;
+    WtRay wt;                  // WT: shear of the current ray space
 
     // `stack`: the query's stack (AZD_WSTACK entries), which a scene whose top
     // level is a single group starts with that group's exit marker.
@@ -272,8 +364,6 @@ struct Tracer {
                                          uint2 *stack, uint32_t skip = 0xFFFFFFFFu) {
         wr = ray;
         r = ray;
-        inv = safe_inv(r.d);
-        oct = octant_of(r.d);
         tmax = tmax_;
         eps = eps_;
         cull = cull_;
@@ -292,14 +382,21 @@ struct Tracer {
         best.tl = 0.0f;
         best.prim = 0xFFFFFFFFu;
         best.ent = 0xFFFFFFFFu;
-        // current node group: the root alone (imask bit 0, hit bit 0 ^ oct)
-        ng_base = S.tlas_root;
-        ng_bits = S.tlas_root == 0xFFFFFFFFu ? 0u : ((1u << 8) | (1u << oct));
-        // a top level holding one group only: enter its hierarchy directly (the
-        // top-level root test and the group's leaf would only lead there)
         if (S.tlas_single_group != 0xFFFFFFFFu) {
+            // a top level holding one group only: enter its hierarchy directly
+            // (the top-level root test and the group's leaf would only lead there)
+            inv = mk(0.0f, 0.0f, 0.0f);
+            oct = 0u;
+            ng_base = 0u;
             ng_bits = 0u;
             enter_group(S, stack, S.tlas_single_group);
+        } else {
+            // current node group: the root alone (imask bit 0, hit bit 0 ^ oct)
+            inv = safe_inv(r.d);
+            oct = octant_of(r.d);
+            if (WT) wt = wt_setup(r.d);
+            ng_base = S.tlas_root;
+            ng_bits = S.tlas_root == 0xFFFFFFFFu ? 0u : ((1u << 8) | (1u << oct));
         }
     }
 
@@ -311,20 +408,20 @@ struct Tracer {
         const DevGroup &g = S.groups[g_idx];
         if (g.root == 0xFFFFFFFFu) return;
         stack[sp++] = make_uint2(0u, AZD_E_EXIT);
-        float blas_scale = 1.0f;
+        const float wlim = KIND == Q_ANY ? tmax : best.t;
+        tcur = FLT_MAX;
         if (g.raw) {
             r = wr;
+            if (wlim < FLT_MAX) tcur = wlim + 1e-30f;
         } else {
             Ray m = wr;
             m.o = wr.o - wr.time * mk(g.motion[0], g.motion[1], g.motion[2]);
             r = local_ray(m, g.inv);
-            // local t = world t * |inv * d| / |d| (up to rounding)
-            blas_scale = length(vector_xf(g.inv, wr.d)) / length(wr.d) * 1.0001f;
+            if (wlim < FLT_MAX) tcur = wlim * group_t_scale(g, wr.d) + 1e-30f;
         }
         inv = safe_inv(r.d);
         oct = octant_of(r.d);
-        float wlim = KIND == Q_ANY ? tmax : best.t;
-        tcur = wlim < FLT_MAX ? wlim * blas_scale + 1e-30f : FLT_MAX;
+        if (WT) wt = wt_setup(r.d);
         bl_t = FLT_MAX;
         bl_prim = 0xFFFFFFFFu;
         in_blas = true;
@@ -337,14 +434,54 @@ struct Tracer {
         else if (err) atomicOr(err, 2u);
     }
 
+    // Takes the top stack entry: leaves or enters a bottom-level hierarchy, or
+    // makes the entry the current primitive or node group.
+    __device__ __forceinline__ void pop(const DevScene &S, uint2 *stack) {
+        const uint2 e = stack[--sp];
+        if (e.y == AZD_E_EXIT) {
+            // leaving a BLAS: azimuth's instance path keeps the nearest local hit
+            // and recomputes its world t (src/azimuth_main.cpp:256-276)
+            if (KIND == Q_CLOSEST && bl_prim != 0xFFFFFFFFu) {
+                float wt_ = group_world_t(S.groups[g_idx], wr, r, bl_t);
+                if (wt_ > eps && wt_ < best.t) {
+                    best.t = wt_;
+                    best.tl = bl_t;
+                    best.prim = bl_prim;
+                    best.ent = S.tri_attr[bl_prim].entity;
+                }
+            }
+            in_blas = false;
+            if (sp == 0) return;   // the query is done: no world-space traversal follows
+            r = wr;
+            inv = safe_inv(r.d);
+            oct = octant_of(r.d);
+            if (WT) wt = wt_setup(r.d);
+            tcur = KIND == Q_ANY ? tmax : best.t;
+        } else if (e.y == AZD_E_GROUP) {
+            enter_group(S, stack, e.x);   // its exit marker reuses the popped entry's slot
+        } else if ((e.y & 0xC0000000u) == AZD_E_PRIMS) {
+            pg_base = e.x;
+            pg_mask = e.y & 0x00FFFFFFu;
+        } else {
+            ng_base = e.x;
+            ng_bits = e.y;
+        }
+    }
+
     // One step: visit the nearest node of the current group and test the
-    // primitives it hits, or pop the stack.  Returns true when finished.  The
-    // stack (AZD_WSTACK entries) is a separate array of the caller so that the
-    // state above stays in registers.
+    // primitives it hits, and pop the stack when both groups are empty.
+    // Returns true when finished.  The stack (AZD_WSTACK entries) is a
+    // separate array of the caller so that the state above stays in registers.
     __device__ __forceinline__ bool step(const DevScene &S, uint2 *stack, uint32_t *err) {
         if (++steps > AZD_MAX_STEPS) {
             if (err) atomicOr(err, 1u);
             return true;
+        }
+        if (POP_FIRST) {
+            while (!(ng_bits & 0xFFu) && !pg_mask) {
+                if (sp == 0) return true;
+                pop(S, stack);
+            }
         }
         if (ng_bits & 0xFFu) {
             const uint32_t hits = ng_bits & 0xFFu, imask = (ng_bits >> 8) & 0xFFu;
@@ -378,9 +515,14 @@ struct Tracer {
             const uint32_t pi = pg_base + bit;
             prims_visited++;
             if (in_blas) {
-                DevTri tr = load_tri(S.tris, pi);
                 float t, b, gm;
-                if (tri_test(tr, r, cull, eps, bl_t, t, b, gm)) {
+                bool hit;
+                if (WT) {
+                    hit = tri_test_wt(load_tri_verts(S.tri_verts, pi), r, wt, cull, eps, bl_t, t);
+                } else {
+                    hit = tri_test(load_tri(S.tris, pi), r, cull, eps, bl_t, t, b, gm);
+                }
+                if (hit) {
                     // a primitive of the skipped entity is ignored; its owner is
                     // looked up only for the few primitives that are hit
                     if (skip_ent != 0xFFFFFFFFu && __ldg(&S.tri_attr[pi].entity) == skip_ent) continue;
@@ -422,35 +564,11 @@ struct Tracer {
             }
         }
         if ((ng_bits & 0xFFu) || pg_mask) return false;
-        // nothing left in the current groups: pop
+        // nothing left in the current groups: pop (or, popping first, let the
+        // next step pop; a leftover BLAS exit marker must still be taken)
         if (sp == 0) return true;
-        const uint2 e = stack[--sp];
-        if (e.y == AZD_E_EXIT) {
-            // leaving a BLAS: azimuth's instance path keeps the nearest local hit
-            // and recomputes its world t (src/azimuth_main.cpp:256-276)
-            if (KIND == Q_CLOSEST && bl_prim != 0xFFFFFFFFu) {
-                float wt = group_world_t(S.groups[g_idx], wr, r, bl_t);
-                if (wt > eps && wt < best.t) {
-                    best.t = wt;
-                    best.tl = bl_t;
-                    best.prim = bl_prim;
-                    best.ent = S.tri_attr[bl_prim].entity;
-                }
-            }
-            r = wr;
-            inv = safe_inv(r.d);
-            oct = octant_of(r.d);
-            tcur = KIND == Q_ANY ? tmax : best.t;
-            in_blas = false;
-        } else if (e.y == AZD_E_GROUP) {
-            enter_group(S, stack, e.x);   // its exit marker reuses the popped entry's slot
-        } else if ((e.y & 0xC0000000u) == AZD_E_PRIMS) {
-            pg_base = e.x;
-            pg_mask = e.y & 0x00FFFFFFu;
-        } else {
-            ng_base = e.x;
-            ng_bits = e.y;
-        }
+        if (POP_FIRST) return false;
+        pop(S, stack);
         return false;
     }
 
@@ -468,7 +586,7 @@ struct Tracer {
 // something was hit and the nearest hit in `best`; for Q_ANY returns whether a
 // primitive lies closer than tmax.  `skip_ent` is an entity whose primitives
 // are ignored; `counts` accumulates node and primitive visits.
-template <QueryKind KIND>
+template <QueryKind KIND, bool WT>
 __device__ bool trace(const DevScene &S, const Ray &wr, bool cull, float eps, float tmax, Hit &best,
                       uint32_t *counts, uint32_t *err, uint32_t skip_ent) {
     best.t = FLT_MAX;
@@ -481,8 +599,11 @@ __device__ bool trace(const DevScene &S, const Ray &wr, bool cull, float eps, fl
     int sp = 0;
 
     Ray r = wr;                                    // current ray space
-    f3 inv = safe_inv(r.d);
-    uint32_t oct = octant_of(r.d);
+    const bool single = S.tlas_single_group != 0xFFFFFFFFu;
+    f3 inv = single ? mk(0.0f, 0.0f, 0.0f) : safe_inv(r.d);   // a single group sets its own
+    uint32_t oct = single ? 0u : octant_of(r.d);
+    WtRay wt;                                      // WT: shear of the current ray space
+    if (WT && !single) wt = wt_setup(r.d);
     float tcur = KIND == Q_ANY ? tmax : FLT_MAX;   // pruning distance in the current space
     bool in_blas = false;
     uint32_t g_idx = 0;
@@ -494,7 +615,7 @@ __device__ bool trace(const DevScene &S, const Ray &wr, bool cull, float eps, fl
     // current node group: the root alone (imask bit 0, hit bit 0 ^ oct)
     uint32_t ng_base = S.tlas_root, ng_bits = (1u << 8) | (1u << oct);
     uint32_t pg_base = 0, pg_mask = 0;             // current primitive group
-    if (S.tlas_single_group != 0xFFFFFFFFu) {
+    if (single) {
         // a top level holding one group only: start with its entry on the stack
         ng_bits = 0u;
         stack[sp++] = make_uint2(S.tlas_single_group, AZD_E_GROUP);
@@ -544,9 +665,14 @@ __device__ bool trace(const DevScene &S, const Ray &wr, bool cull, float eps, fl
             const uint32_t pi = pg_base + bit;
             prims_visited++;
             if (in_blas) {
-                DevTri tr = load_tri(S.tris, pi);
                 float t, b, gm;
-                if (tri_test(tr, r, cull, eps, bl_t, t, b, gm)) {
+                bool hit;
+                if (WT) {
+                    hit = tri_test_wt(load_tri_verts(S.tri_verts, pi), r, wt, cull, eps, bl_t, t);
+                } else {
+                    hit = tri_test(load_tri(S.tris, pi), r, cull, eps, bl_t, t, b, gm);
+                }
+                if (hit) {
                     // a primitive of the skipped entity is ignored; its owner is
                     // looked up only for the few primitives that are hit
                     if (skip_ent != 0xFFFFFFFFu && __ldg(&S.tri_attr[pi].entity) == skip_ent) continue;
@@ -609,6 +735,7 @@ __device__ bool trace(const DevScene &S, const Ray &wr, bool cull, float eps, fl
             r = wr;
             inv = safe_inv(r.d);
             oct = octant_of(r.d);
+            if (WT) wt = wt_setup(r.d);
             tcur = KIND == Q_ANY ? tmax : best.t;
             in_blas = false;
         } else if (e.y == AZD_E_GROUP) {
@@ -618,20 +745,20 @@ __device__ bool trace(const DevScene &S, const Ray &wr, bool cull, float eps, fl
             const DevGroup &g = S.groups[g_idx];
             if (g.root == 0xFFFFFFFFu) continue;
             stack[sp++] = make_uint2(0u, AZD_E_EXIT);   // room was kept when the entry was pushed
-            float blas_scale = 1.0f;
+            const float wlim = KIND == Q_ANY ? tmax : best.t;
+            tcur = FLT_MAX;
             if (g.raw) {
                 r = wr;
+                if (wlim < FLT_MAX) tcur = wlim + 1e-30f;
             } else {
                 Ray m = wr;
                 m.o = wr.o - wr.time * mk(g.motion[0], g.motion[1], g.motion[2]);
                 r = local_ray(m, g.inv);
-                // local t = world t * |inv * d| / |d| (up to rounding)
-                blas_scale = length(vector_xf(g.inv, wr.d)) / length(wr.d) * 1.0001f;
+                if (wlim < FLT_MAX) tcur = wlim * group_t_scale(g, wr.d) + 1e-30f;
             }
             inv = safe_inv(r.d);
             oct = octant_of(r.d);
-            float wlim = KIND == Q_ANY ? tmax : best.t;
-            tcur = wlim < FLT_MAX ? wlim * blas_scale + 1e-30f : FLT_MAX;
+            if (WT) wt = wt_setup(r.d);
             bl_t = FLT_MAX;
             bl_prim = 0xFFFFFFFFu;
             in_blas = true;

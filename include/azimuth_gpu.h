@@ -54,11 +54,19 @@ enum {
      * by default the scene's choice (az_gpu_autotune picks it). */
     AZ_FLAG_ORDER_SHADOW = 1u << 4,     /* visit each level's shadow queue in the order of the rays' origin cells */
     AZ_FLAG_ORDER_EXTEND = 1u << 5,     /* visit each level's extension queue by origin cell and direction octant */
-    AZ_FLAG_ORDER_NONE = 1u << 6        /* queues in the order they were filled */
+    AZ_FLAG_ORDER_NONE = 1u << 6,       /* queues in the order they were filled */
+    AZ_FLAG_SERIAL_LEVELS = 1u << 7,    /* run each tree level's visibility queries before the next level's
+                                           closest-hit queries (default: the two run side by side on two
+                                           streams, so one's tail overlaps the other's work) */
+    AZ_FLAG_WATERTIGHT = 1u << 8        /* production mode: triangles by the watertight test of Woop, Benthin
+                                           and Wald (JCGT 2013) on the exact vertices -- no ray passes between
+                                           triangles that share an edge or vertex -- instead of azimuth's
+                                           Cramer test with its -1e-6 barycentric tolerance (the parity
+                                           default); one launch configuration; also az_gpu_closest_hit */
 };
 
 /* Number of traversal launch configurations (az_render_opts.variant). */
-#define AZ_LAUNCH_VARIANTS 14
+#define AZ_LAUNCH_VARIANTS 18
 
 typedef struct az_render_opts {
     uint64_t seed;                  /* counter-RNG key */
@@ -81,7 +89,11 @@ typedef struct az_render_opts {
     uint32_t bvh_leaf;              /* az_gpu_scene_create: triangles per bottom-level leaf at most, 1..3 (0 = 2) */
     uint32_t bvh_builder;           /* az_gpu_scene_create: binary hierarchy before the wide collapse,
                                        AZ_BVH_LBVH or AZ_BVH_PLOC (0 = the default, AZ_BVH_PLOC) */
-    uint32_t reserved[2];
+    uint32_t sample_part;           /* with sample_parts > 1: render only part sample_part (0-based) of */
+    uint32_t sample_parts;          /* sample_parts equal ranges of the scissor's camera-sample sequence
+                                       (sample number x pixels, pixels fastest), i.e. about spp/parts
+                                       samples of every pixel; the parts of one frame sum to the whole
+                                       frame (one GPU per part); 0 or 1 = every sample */
 } az_render_opts;
 
 enum {
@@ -100,10 +112,13 @@ typedef struct az_render_stats {
     float extend_ms;                /* with AZ_FLAG_TIME_STAGES: closest-hit stage */
     float shade_ms;                 /* with AZ_FLAG_TIME_STAGES: shading stage */
     float shadow_ms;                /* with AZ_FLAG_TIME_STAGES: visibility stage */
-    uint64_t node_visits;           /* with AZ_FLAG_COUNT_TRAVERSAL: BVH nodes visited */
-    uint64_t prim_visits;           /* with AZ_FLAG_COUNT_TRAVERSAL: primitives tested */
+    uint64_t node_visits;           /* with AZ_FLAG_COUNT_TRAVERSAL: BVH nodes visited by closest-hit queries */
+    uint64_t prim_visits;           /* with AZ_FLAG_COUNT_TRAVERSAL: primitives tested by closest-hit queries */
     uint32_t extend_launches;       /* closest-hit stage launches */
-    uint32_t reserved[3];
+    uint32_t reserved0;
+    uint64_t shadow_node_visits;    /* with AZ_FLAG_COUNT_TRAVERSAL: BVH nodes visited by visibility queries */
+    uint64_t shadow_prim_visits;    /* with AZ_FLAG_COUNT_TRAVERSAL: primitives tested by visibility queries */
+    uint32_t reserved[2];
 } az_render_stats;
 
 typedef struct az_gpu_scene az_gpu_scene;
@@ -139,6 +154,31 @@ typedef struct az_scene_info {
 } az_scene_info;
 
 int az_gpu_scene_info(const az_gpu_scene *scene, az_scene_info *out);
+
+/* Device addresses of a resident scene's hierarchy and triangles (no
+ * counterpart in azimuth, whose BVH is a tree of host entities), for callers
+ * that run kernels of their own on the scene.  The arrays belong to the scene
+ * until az_gpu_scene_destroy; the renderer reads them on every query, so a
+ * caller that writes into them changes what later renders see (a damaged
+ * hierarchy makes a render fail with AZ_ERR_CUDA once a query exceeds its
+ * step limit, never hang).
+ *   wide node (80 B): grid origin (3 floats), 3 exponent bytes, an inner-child
+ *   mask byte, first inner child, first leaf primitive, 8 leaf-meta bytes
+ *   (count << 5 | offset), then the 8 children's quantised low x, y, z and
+ *   high x, y, z bytes;
+ *   triangle (48 B): P0, P0 - P1, P0 - P2, face normal, in leaf order. */
+typedef struct az_scene_arrays {
+    void *wide_nodes;
+    uint64_t wide_node_count;
+    void *triangles;
+    uint64_t triangle_count;
+    uint32_t tlas_root;          /* top-level root node; 0xFFFFFFFF: empty scene */
+    uint32_t single_group_root;  /* when the top level holds one group, the root of its hierarchy, which
+                                    queries enter directly; else 0xFFFFFFFF */
+    uint32_t reserved[4];
+} az_scene_arrays;
+
+int az_gpu_scene_arrays(const az_gpu_scene *scene, az_scene_arrays *out);
 
 /* ---- Scene ingestion on the GPU ----
  * azimuth's importer collects every mesh's vertices, faces and UVs into shared
@@ -212,6 +252,17 @@ int az_gpu_produce_image(az_pixel *pixels, const az_scene *scene, const az_camer
 int az_gpu_render(az_gpu_scene *scene, az_pixel *film, const az_camera *camera,
                   const az_epsilon_values *epsilons, az_scissor scissor, int32_t filter_type,
                   uint32_t backface_culling, const az_render_opts *opts, az_render_stats *stats);
+
+/* Per-sample radiance (the value ProduceImageInLinearSpace hands to
+ * ComputeSampleWeight, src/azimuth_main.cpp:1365-1391, before any filter):
+ * renders the scissor like az_gpu_render but writes camera sample s's RGB sum
+ * to samples[4 s .. 4 s + 2] (DEVICE memory, 16-byte aligned, 4 floats per
+ * sample; the 4th is 0) instead of splatting it, with s = (SampleY *
+ * SampleCountSqrt + SampleX) * scissor pixels + (Row - Min.y) * scissor width
+ * + (Col - Min.x).  For per-path comparisons with azimuth. */
+int az_gpu_render_samples(az_gpu_scene *scene, float *samples, const az_camera *camera,
+                          const az_epsilon_values *epsilons, az_scissor scissor, uint32_t backface_culling,
+                          const az_render_opts *opts, az_render_stats *stats);
 
 /* ProduceImageInLinearSpace on a device scene with a HOST film: copies
  * `pixels` to the device, renders into it and copies it back (synchronous). */
@@ -288,7 +339,10 @@ typedef struct az_batch_opts {
     uint32_t chunk_samples;         /* 0 = 2^22 per job in az_gpu_render_batch; az_gpu_render_tiles as
                                        az_render_opts.chunk_samples */
     uint32_t largest_first;         /* 0: shortest jobs first (low completion times); 1: largest first */
-    uint32_t reserved[3];
+    uint32_t tiles;                 /* az_gpu_render_batch: 1 = the plain jobs (guide NULL) render together
+                                       in tile waves (az_gpu_render_tiles) on one stream while the other
+                                       streams take the guided jobs; 0 = every job on its own */
+    uint32_t reserved[2];
 } az_batch_opts;
 
 typedef struct az_batch_stats {
@@ -303,17 +357,18 @@ typedef struct az_batch_stats {
  * (see each job's `status`). Synchronous. */
 int az_gpu_render_batch(az_job *jobs, uint32_t n, const az_batch_opts *opts, az_batch_stats *stats);
 
-/* The jobs of ONE device scene rendered together: every job's camera samples
- * are cut into tiles of 4096, and each wave of the render takes the next tiles
- * of all jobs from a device work queue (a camera kernel whose blocks pull
- * tiles), so one chain of extend/shade/shadow launches per wave serves every
- * job and small jobs share waves instead of running their own.  The jobs may
- * differ in camera, resolution, spp, scissor, filter, seed and film; they
- * must share the scene, the epsilon values and culling, and be plain renders
- * (guide NULL).  Each job's film gets exactly what az_gpu_render with the
- * job's seed would add (up to the order of float atomics).  opts->streams and
- * largest_first are ignored; a job's done_ms is the end of the wave holding
- * its last tile.  Synchronous. */
+/* Jobs rendered together: every job's camera samples are cut into tiles of
+ * 4096, and each wave of the render takes the next tiles of all jobs from a
+ * device work queue (a camera kernel whose blocks pull tiles), so one chain
+ * of extend/shade/shadow launches per wave serves every job and small jobs
+ * share waves instead of running their own.  The jobs may differ in scene
+ * (up to 256 device scenes of one device: every queue entry carries its
+ * scene's index, and the kernels trace and shade it in that scene), camera,
+ * resolution, spp, depth, scissor, filter, seed and film; they must share the
+ * epsilon values and culling, and be plain renders (guide NULL).  Each job's
+ * film gets exactly what az_gpu_render with the job's seed would add (up to
+ * the order of float atomics).  opts->streams and largest_first are ignored;
+ * a job's done_ms is the end of the wave holding its last tile.  Synchronous. */
 int az_gpu_render_tiles(az_job *jobs, uint32_t n, const az_batch_opts *opts, az_batch_stats *stats);
 
 /* ---- Neural path guiding (the learned proposal; no counterpart in azimuth) ----
@@ -367,20 +422,30 @@ int az_guide_train(az_guide *guide, const float *rows, uint32_t n, uint32_t step
 
 /* Allocation-free variant of az_gpu_render; it has no counterpart in azimuth.
  *
- * For callers that must not allocate device memory while rendering: code
- * running inside CUDA stream capture (where cudaMalloc is not permitted),
- * hosts whose caching allocator owns all device memory, and real-time loops
- * that keep a fixed memory budget.  The scene (created earlier with
- * az_gpu_scene_create) and the DEVICE film are passed in as usual; the wave
- * queues live in one static device array of 9,110,784 bytes (8.7 MiB) that
- * every GPU loading this library holds until the process exits, which caps a
- * wave at 16384 camera samples: opts->chunk_samples above 16384 is rejected
- * with AZ_ERR_INVALID_ARGUMENT.  The first call on a device looks up the
- * array's device address (cudaGetSymbolAddress), so make that first call
- * before any stream capture begins.  All calls share the array: calls that
- * overlap on the GPU (other threads or streams) race and must be serialised
- * by the caller.  Synchronous; runs on opts->stream, or on the per-thread
- * default stream when that is NULL; never calls cudaMalloc or cudaFree. */
+ * For callers that cannot allocate device memory while they render: hosts
+ * whose caching allocator has already reserved the GPU's memory (a cudaMalloc
+ * from the library would fail, or fragment the host's pool), plug-in hosts
+ * that forbid their plug-ins to allocate, and real-time loops that keep a
+ * fixed memory budget.  The scene (created earlier with az_gpu_scene_create)
+ * and the DEVICE film are passed in as usual; the wave queues live in one
+ * static device array of 9,110,784 bytes (8.7 MiB) that every GPU loading
+ * this library holds until the process exits, which caps a wave at 16384
+ * camera samples: opts->chunk_samples above 16384 is rejected with
+ * AZ_ERR_INVALID_ARGUMENT.  The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress), so make that first call before any
+ * stream capture begins.  All calls share the array and it keeps the last
+ * call's contents (the counters are cleared at the start of every wave):
+ * calls that overlap on the GPU (other threads or streams) race and must be
+ * serialised by the caller.  A wave whose queues overflow the array is run
+ * again with half the samples, down to 256.  opts->flags may hold
+ * AZ_FLAG_ENV_IMPORTANCE and AZ_FLAG_WATERTIGHT; flags that need allocations
+ * or statistics (AZ_FLAG_COUNT_TRAVERSAL, AZ_FLAG_TIME_STAGES,
+ * AZ_FLAG_ORDER_SHADOW, AZ_FLAG_ORDER_EXTEND) are rejected with
+ * AZ_ERR_INVALID_ARGUMENT, and the scene's own queue ordering is not applied
+ * (it never changes the film).  Synchronous: every wave copies its queue
+ * counters to the host and synchronises the stream.  Runs on opts->stream, or
+ * on the per-thread default stream when that is NULL; never calls cudaMalloc
+ * or cudaFree. */
 int az_gpu_render_noalloc(az_gpu_scene *scene, az_pixel *film, const az_camera *camera,
                           const az_epsilon_values *epsilons, az_scissor scissor, int32_t filter_type,
                           uint32_t backface_culling, const az_render_opts *opts);

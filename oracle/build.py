@@ -14,6 +14,7 @@ Two libraries come out of it:
   (plain C, no reference code), built wherever gcc exists.
 
 Usage: python oracle/build.py [--reference DIR] [--force]
+(DIR defaults to $AZIMUTH_REFERENCE, else ../reference beside the repository.)
 """
 import argparse
 import os
@@ -25,7 +26,11 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 REF_OUT = os.path.join(HERE, "_ref")
 PORT_OUT = os.path.join(HERE, "lib")
-DEFAULT_REFERENCE = "/root/reference"
+# the reference checkout: AZIMUTH_REFERENCE, else the checkout beside the
+# repository (../reference), else /root/reference
+DEFAULT_REFERENCE = os.environ.get("AZIMUTH_REFERENCE") or next(
+    (d for d in (os.path.join(os.path.dirname(REPO), "reference"), "/root/reference")
+     if os.path.isdir(os.path.join(d, "src"))), "/root/reference")
 
 PARITY_FLAGS = ["-O2", "-ffp-contract=off", "-fno-strict-aliasing"]
 # x86-64-v3 (AVX2/FMA) rather than -march=native: the library is built here and

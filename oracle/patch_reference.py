@@ -12,7 +12,9 @@ and applies mechanical edits.  None of them changes what the code computes:
    instead of libc ``rand()``.
 3. ``GetSampleCoord`` (src/azimuth_main.cpp:1135) announces the pixel and
    sample to the RNG; ``TraceRay`` (src/azimuth_main.cpp:966) opens one RNG
-   node per activation.  Both are one inserted line.
+   node per activation; ``ComputeSampleWeight`` (src/azimuth_main.cpp:1208)
+   hands the finished sample's colour to the harness, which records it when
+   asked for per-sample radiance.  Each is one inserted line.
 4. ``src/azimuth_platform.h`` selects the platform layer with ``#if _WIN32``;
    the oracle selects the POSIX stand-in in ``oracle/shim`` instead, and the
    Win32 platform files are not copied.
@@ -97,6 +99,10 @@ def main(src, dst):
                 text,
                 r"(\nTraceRay\(scene \*Scene, ray3 Ray, u32 RecursionDepth,[^{;]*\)\{\n)",
                 r"\1    AZ_ORACLE_NODE_SCOPE();\n", "TraceRay")
+            text = regex_once(
+                text,
+                r"(\nComputeSampleWeight\(vec3 Color, vec2 SampleCoord, pixel \*Pixels,[^{;]*\)\{\n)",
+                r"\1    AzOracleSampleDone(Color.x, Color.y, Color.z);\n", "ComputeSampleWeight")
         if name == "azimuth_platform.h":
             if text.count("#if _WIN32") != 2:
                 raise SystemExit("patch_reference: platform selector changed")

@@ -10,6 +10,8 @@
  *   azref_produce_image   ProduceImageInLinearSpace (src/azimuth_main.cpp:1256)
  *                         over N threads with RenderScene's scanline split
  *                         (src/azimuth_main.cpp:1815-1867), any filter
+ *   azref_sample_radiance the same loop, recording every camera sample's
+ *                         colour before ComputeSampleWeight splats it
  *   azref_closest_hit     RayEntityIntersection on the scene root
  *                         (src/azimuth_main.cpp:53-385), plus the face id of
  *                         a mesh-instance hit (src/azimuth_main.cpp:244-281)
@@ -23,7 +25,8 @@
  *                         back what it built
  *
  * It also defines the counter-RNG hooks that the patched Random01,
- * GetSampleCoord and TraceRay call (see oracle/shim/az_oracle_compat.h).
+ * GetSampleCoord and TraceRay call, and the sample hook of the patched
+ * ComputeSampleWeight (see oracle/shim/az_oracle_compat.h).
  */
 #include "azimuth_main.cpp"
 
@@ -130,6 +133,27 @@ extern "C" void AzOracleEnterNode(void) {
 
 extern "C" void AzOracleLeaveNode(void) { --TTop; }
 
+/* Per-sample radiance: while GSampleOut is set, every finished camera sample
+ * (ComputeSampleWeight's colour) is stored at its index in the scissor's
+ * sample order, s = (SampleY * SampleCountSqrt + SampleX) * pixels + pixel,
+ * pixel = (Row - RowMin) * Columns + (Col - ColMin); threads write disjoint
+ * entries. */
+namespace {
+float *GSampleOut = nullptr;
+uint32_t GSampleRow0 = 0, GSampleCol0 = 0, GSampleCols = 0, GSampleRows = 0, GSampleSqrt = 1;
+}
+
+extern "C" void AzOracleSampleDone(float R, float G, float B) {
+    if (!GSampleOut) { return; }
+    const uint32_t Row = TPixel >> 16, Col = TPixel & 0xFFFFu;
+    const uint32_t SX = TSample & 0xFFFFu, SY = TSample >> 16;
+    const uint64_t Pixels = (uint64_t)GSampleRows * GSampleCols;
+    const uint64_t Pix = (uint64_t)(Row - GSampleRow0) * GSampleCols + (Col - GSampleCol0);
+    const uint64_t S = ((uint64_t)SY * GSampleSqrt + SX) * Pixels + Pix;
+    float *O = GSampleOut + 4 * S;
+    O[0] = R; O[1] = G; O[2] = B; O[3] = 1.0f;
+}
+
 /* ------------------------------ C interface ---------------------------- */
 extern "C" {
 
@@ -174,6 +198,26 @@ void azref_produce_image(az_pixel *Pixels, az_scene *Scene, az_camera *Camera,
     PlatformWaitForThreads(ThreadCount, Handles, true, true, 0);
     free(Handles);
     free(Params);
+}
+
+/* Each camera sample's colour over the scissor, as ProduceImageInLinearSpace
+ * computes it before ComputeSampleWeight splats it: Out holds 4 floats (RGB,
+ * 1) per sample in the order of AzOracleSampleDone.  Runs azimuth's own render
+ * loop on `ThreadCount` threads (a scratch film takes the splats). */
+void azref_sample_radiance(float *Out, az_scene *Scene, az_camera *Camera, az_epsilon_values *Epsilons,
+                           az_scissor Scissor, int BackfaceCulling, uint32_t ThreadCount) {
+    const uint32_t W = Camera->Resolution.x, H = Camera->Resolution.y;
+    const uint32_t R1 = Scissor.Max.y < H ? Scissor.Max.y : H, C1 = Scissor.Max.x < W ? Scissor.Max.x : W;
+    GSampleRow0 = Scissor.Min.y;
+    GSampleCol0 = Scissor.Min.x;
+    GSampleRows = R1 > Scissor.Min.y ? R1 - Scissor.Min.y : 0;
+    GSampleCols = C1 > Scissor.Min.x ? C1 - Scissor.Min.x : 0;
+    GSampleSqrt = (uint32_t)Sqrt((f32)Camera->SampleCount);
+    az_pixel *Film = (az_pixel *)calloc((size_t)W * H, sizeof(az_pixel));
+    GSampleOut = Out;
+    azref_produce_image(Film, Scene, Camera, Epsilons, Scissor, 0, BackfaceCulling, ThreadCount);
+    GSampleOut = nullptr;
+    free(Film);
 }
 
 /* Closest hit on the scene root for a batch of rays (src/azimuth_main.cpp:53-385).

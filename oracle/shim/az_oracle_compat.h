@@ -30,6 +30,7 @@ float AzOracleRandom01(void);
 void  AzOracleBeginSample(unsigned Row, unsigned Col, unsigned SampleX, unsigned SampleY);
 void  AzOracleEnterNode(void);
 void  AzOracleLeaveNode(void);
+void  AzOracleSampleDone(float R, float G, float B);
 #ifdef __cplusplus
 }
 #endif

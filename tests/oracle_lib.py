@@ -48,6 +48,7 @@ def ref(fast=False):
         L.azref_write_image.restype = i32
         L.azref_produce_image.argtypes = [vp, vp, vp, vp, Scissor, i32, i32, u32]
         L.azref_closest_hit.argtypes = [vp, vp, u32, i32, C.c_float, vp, vp, vp, vp, vp, i32]
+        L.azref_sample_radiance.argtypes = [vp, vp, vp, vp, Scissor, i32, u32]
         L.azref_set_perlin_gradients.argtypes = [vp]
         L.azref_get_perlin_gradients.argtypes = [vp]
         L.azref_construct_bvh.argtypes = [vp, vp, u32]
@@ -135,6 +136,24 @@ def ref_film(scene, seed=0, threads=None, scissor=None, fast=False, filter_type=
     L.azref_produce_image(film.ctypes.data, scene.scene_ptr, scene.camera_ptr, scene.epsilons_ptr,
                           scissor or scissor_of(scene), ft, 0, threads or os.cpu_count())
     return film
+
+
+def ref_samples(scene, seed=0, threads=None, scissor=None):
+    """azimuth's colour of every camera sample of the scissor (before ComputeSampleWeight), as an array
+    (samples, 4) in the order sample number * scissor pixels + pixel (row-major in the scissor)."""
+    L = ref()
+    sc = scissor or scissor_of(scene)
+    w, h = scene.resolution()
+    rows = min(sc.Max.y, h) - sc.Min.y
+    cols = min(sc.Max.x, w) - sc.Min.x
+    k = int(np.sqrt(np.float32(scene.sample_count())))   # (u32)Sqrt((f32)SampleCount)
+    out = np.zeros((k * k * rows * cols, 4), np.float32)
+    L.azref_set_seed(seed)
+    if scene.perlin_gradients:
+        L.azref_set_perlin_gradients(scene.perlin_gradients)
+    L.azref_sample_radiance(out.ctypes.data, scene.scene_ptr, scene.camera_ptr, scene.epsilons_ptr, sc, 0,
+                            threads or os.cpu_count())
+    return out
 
 
 def port_film(scene, seed=0, threads=None, scissor=None, filter_type=None):

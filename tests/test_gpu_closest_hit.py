@@ -32,12 +32,21 @@ CASES = [
     ("motion_env", az.SCENE_MOTION_ENV, dict(detail=2000), (0.0, 0.0, 0.0), (10.0, 10.0, 10.0)),
     ("env_spheres", az.SCENE_ENV_SPHERES, {}, (-2.0, 0.05, -2.0), (2.0, 2.0, 2.0)),
     ("interior", az.SCENE_INTERIOR, dict(detail=8), (0.5, 0.2, 0.5), (24.0, 3.8, 7.5)),
+    # the benchmark configurations at their full size: C1's 1,310,720-triangle
+    # icosphere (and its 8-level hierarchy), C2's 10,000 moving spheres, C3's
+    # 3,955,978-triangle interior
+    ("dense_mesh_full", az.SCENE_DENSE_MESH, {}, (-0.45, 0.05, -0.45), (0.45, 0.95, 0.45)),
+    ("motion_env_full", az.SCENE_MOTION_ENV, {}, (0.0, 0.0, 0.0), (10.0, 10.0, 10.0)),
+    ("interior_full", az.SCENE_INTERIOR, {}, (0.5, 0.2, 0.5), (24.0, 3.8, 7.5)),
 ]
+FULL = {"dense_mesh_full": 1310732, "motion_env_full": 10000, "interior_full": 3955978}
 
 
 @pytest.mark.parametrize("name,sid,kw,lo,hi", CASES, ids=[c[0] for c in CASES])
 def test_nearest_hit_ids_match(gpu, name, sid, kw, lo, hi):
     scene = az.generate_scene(sid, seed=5, width=8, height=8, spp=1, **kw)
+    if name in FULL:
+        assert scene.triangle_count + scene.sphere_count == FULL[name]
     rays = random_rays(200000, lo, hi, seed=len(name))
     with az.GpuScene(scene) as g:
         gh, gu, gf, gt = g.closest_hit(rays)

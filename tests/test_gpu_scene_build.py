@@ -99,5 +99,6 @@ def test_ploc_visits_fewer_nodes(gpu, dense):
     for builder in (az.BVH_LBVH, az.BVH_PLOC):
         with az.GpuScene(dense, bvh_builder=builder) as g:
             st = g.render_device(film.data_ptr(), seed=1, stats=True, flags=az.FLAG_COUNT_TRAVERSAL)
-            visits[builder] = (st["node_visits"] + st["prim_visits"]) / (st["extend_rays"] + st["shadow_rays"])
+            visits[builder] = (st["node_visits"] + st["prim_visits"] + st["shadow_node_visits"] +
+                               st["shadow_prim_visits"]) / (st["extend_rays"] + st["shadow_rays"])
     assert visits[az.BVH_PLOC] < visits[az.BVH_LBVH]

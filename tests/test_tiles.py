@@ -1,8 +1,9 @@
-"""az_gpu_render_tiles: jobs of one scene rendered together in shared waves,
-every wave's camera kernel pulling 4096-sample tiles of all jobs from a device
-work queue.  Each job's film must equal what az_gpu_render adds for that job
-alone (same seed, same samples; only the order of float atomics differs), for
-jobs that differ in camera, resolution, spp, scissor, filter and seed."""
+"""az_gpu_render_tiles: jobs rendered together in shared waves, every wave's
+camera kernel pulling 4096-sample tiles of all jobs from a device work queue.
+Each job's film must equal what az_gpu_render adds for that job alone (same
+seed, same samples; only the order of float atomics differs), for jobs that
+differ in camera, resolution, spp, scissor, filter and seed, and for jobs of
+different scenes in the same waves (every queue entry carries its scene)."""
 import ctypes as C
 
 import numpy as np
@@ -76,22 +77,66 @@ def test_tile_render_gives_every_job_its_own_render(gpu, scene_id):
 
 
 @pytest.mark.gpu
-def test_tile_render_rejects_mixed_scenes_and_guides(gpu):
+def test_tile_render_of_several_scenes_gives_every_job_its_own_render(gpu):
+    import torch
+    # the benchmark generators' scenes (small sizes): Cornell box (uniform sampling, box filter,
+    # depth 5), dense mesh (7 BRDFs, cosine sampling, Gaussian filter, depth 8), moving spheres with an
+    # HDR map (dielectrics, environment light, depth 12), plus the features scene (textures, every
+    # light type) and a second Cornell box of another depth
+    specs = [(az.SCENE_CORNELL, dict(width=40, height=30, spp=4)),
+             (az.SCENE_DENSE_MESH, dict(width=48, height=36, spp=4, detail=4)),
+             (az.SCENE_MOTION_ENV, dict(width=64, height=36, spp=4, detail=300)),
+             (az.SCENE_FEATURES, dict(width=32, height=24, spp=9)),
+             (az.SCENE_CORNELL, dict(width=24, height=24, spp=16, max_depth=9))]
+    scenes = [az.generate_scene(sid, seed=7 + k, **kw) for k, (sid, kw) in enumerate(specs)]
+    gss = [az.GpuScene(s) for s in scenes]
+    try:
+        tiled, alone, jobs = [], [], []
+        for k, (s, g) in enumerate(zip(scenes, gss)):
+            w, h = s.resolution()
+            f = torch.zeros((h, w, 4), device="cuda")
+            tiled.append(f)
+            jobs.append({"gpu_scene": g, "film_ptr": f.data_ptr(), "seed": 20 + k})
+            a = torch.zeros((h, w, 4), device="cuda")
+            g.render_device(a.data_ptr(), seed=20 + k)
+            alone.append(a)
+        # the second job twice more, with other seeds: one scene for several jobs of the wave
+        for k in (1, 2):
+            w, h = scenes[1].resolution()
+            f = torch.zeros((h, w, 4), device="cuda")
+            tiled.append(f)
+            jobs.append({"gpu_scene": gss[1], "film_ptr": f.data_ptr(), "seed": 40 + k})
+            a = torch.zeros((h, w, 4), device="cuda")
+            gss[1].render_device(a.data_ptr(), seed=40 + k)
+            alone.append(a)
+        torch.cuda.synchronize()
+        # small waves: every wave holds tiles of several scenes
+        per, stats = az.render_tiles(jobs, chunk_samples=2 * 4096)
+        torch.cuda.synchronize()
+        assert all(p["status"] == 0 for p in per)
+        for k, (t, a) in enumerate(zip(tiled, alone)):
+            t, a = t.cpu().numpy(), a.cpu().numpy()
+            assert a[..., 3].sum() > 0, k
+            assert ol.film_compare(t, a, 1e-4)[0] == 1.0, k
+    finally:
+        for g in gss:
+            g.close()
+        for s in scenes:
+            s.close()
+
+
+@pytest.mark.gpu
+def test_tile_render_rejects_guides(gpu):
     import torch
     a = az.generate_scene(az.SCENE_CORNELL, seed=1, width=16, height=16, spp=1)
-    b = az.generate_scene(az.SCENE_CORNELL, seed=2, width=16, height=16, spp=1)
     try:
-        with az.GpuScene(a) as ga, az.GpuScene(b) as gb:
+        with az.GpuScene(a) as ga:
             f = torch.zeros((16, 16, 4), device="cuda")
-            with pytest.raises(az.AzError):
-                az.render_tiles([{"gpu_scene": ga, "film_ptr": f.data_ptr()},
-                                 {"gpu_scene": gb, "film_ptr": f.data_ptr()}])
             with az.Guide(ga) as guide:
                 with pytest.raises(az.AzError):
                     az.render_tiles([{"gpu_scene": ga, "film_ptr": f.data_ptr(), "guide": guide}])
     finally:
         a.close()
-        b.close()
 
 
 def test_tile_entry_checks_its_arguments_before_the_device():
