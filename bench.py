@@ -39,10 +39,12 @@ METRIC = "Mpaths/s on 1 B200; equal-time relMSE guided vs plain GPU vs FP64 conv
 WORKLOAD = "dense mesh + importance sampling: 1,310,720-triangle Perlin-displaced icosphere in a Cornell box, " \
            "7 BRDFs, 1024x1024, 64 spp, depth 8, cosine sampling + area-light NEE, Gaussian filter"
 SCENE_ARGS = dict(scene_id=1, seed=0)
-# mean DRAM read + write of the nine k_extend launches (tree levels 1-9) of this
-# workload's first frame, one 2^26-sample wave, measured with ncu (see the
-# roofline below)
-EXTEND_DRAM_BYTES_PER_LAUNCH = 6610635235.6
+# DRAM read + write per query of the two traversal kernels on this scene, from
+# one single-pass ncu capture (dram__bytes_read.sum + dram__bytes_write.sum)
+# of every k_extend / k_shadow launch of one 256x256, 16-spp frame (one wave of
+# 2^20 samples): the capture's bytes over the frame's queries
+DRAM_BYTES_PER_QUERY = {"k_extend": None, "k_shadow": None}
+PROFILE_NOTE = "profiles/k_extend_dense_mesh_256x256_16spp.md"
 
 
 def parse():
@@ -53,6 +55,9 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--chunk", type=int, default=0, help="camera samples per wave (0 = library default)")
+    ap.add_argument("--split", action="store_true",
+                    help="N>1: render ONE frame per step over the ranks (equal parts of its camera samples, "
+                         "then an NCCL reduce of the films into rank 0) instead of one frame per rank")
     ap.add_argument("--no-autotune", action="store_true",
                     help="skip az_gpu_autotune_scene (BVH width and traversal launch variant) before timing")
     return ap.parse_args()
@@ -234,11 +239,22 @@ def main():
     torch.cuda.set_stream(stream)
     sptr = stream.cuda_stream
     film = torch.zeros((h, w, 4), device="cuda", dtype=torch.float32)
-    seed = seed_base(rank)
+    # one frame over the ranks needs the same random numbers on every rank
+    seed = seed_base(0) if (args.split and world > 1) else seed_base(rank)
+
+    split = args.split and world > 1
 
     def step(i, flags=0, stats=False):
-        return gs.render_device(film.data_ptr(), seed=seed + i, stream=sptr, flags=flags, stats=stats,
-                                chunk_samples=args.chunk)
+        if not split:
+            return gs.render_device(film.data_ptr(), seed=seed + i, stream=sptr, flags=flags, stats=stats,
+                                    chunk_samples=args.chunk)
+        # one frame over the ranks: this rank's part of the camera-sample sequence, then one
+        # NCCL reduce of the films into rank 0 (azimuth_b200.scanlines, "samples" split)
+        film.zero_()
+        st_ = gs.render_device(film.data_ptr(), seed=seed + i, stream=sptr, flags=flags, stats=stats,
+                               chunk_samples=args.chunk, sample_part=rank, sample_parts=world)
+        dist.reduce(film, dst=0)
+        return st_
 
     for i in range(args.warmup):
         step(i)
@@ -276,7 +292,8 @@ def main():
     if dist:
         dist.barrier()
     ms_per_step = ms / args.steps
-    value = aggregate(world, paths_per_frame, args.steps, ms / 1000.0) / 1e6
+    # weak scaling: every rank's frame; split: one frame per step over all ranks
+    value = aggregate(1 if split else world, paths_per_frame, args.steps, ms / 1000.0) / 1e6
 
     # end to end through the host-film entry point (film in and out every step)
     host_film = torch.zeros((h, w, 4), dtype=torch.float32).pin_memory()
@@ -286,17 +303,18 @@ def main():
     if dist:
         dist.barrier()
     t0 = time.monotonic()
-    e_steps = max(1, min(args.steps, 3))
+    e_steps = args.steps   # as many frames as the device-timed region
     for i in range(e_steps):
         gs.render_host(hf, seed=seed + i, stream=sptr, chunk_samples=args.chunk)
     e2e_s = time.monotonic() - t0
     e2e_s = max_over_ranks(dist, e2e_s, "cuda")
     e2e = {"value": aggregate(world, paths_per_frame, e_steps, e2e_s) / 1e6, "unit": "Mpaths/s",
-           "h2d_bytes_per_step": int(w * h * 16), "d2h_bytes_per_step": int(w * h * 16),
+           "h2d_bytes_per_step": int(w * h * 16), "d2h_bytes_per_step": int(w * h * 16), "steps": e_steps,
            "api": "az_gpu_render_host (device scene resident, host film copied in and out)"}
 
-    # roofline of the closest-hit (extend) kernel: algorithmic bytes from a
-    # counting pass over one frame (node/primitive visits), time from the timed run
+    # rooflines of the two traversal kernels: algorithmic bytes from a counting
+    # pass over one frame (node and primitive visits of each query kind, counted
+    # by the kernels themselves), time per launch from the stage-timed frame
     cnt = step(0, flags=az.FLAG_COUNT_TRAVERSAL, stats=True)
     torch.cuda.synchronize()
     peaks = {}
@@ -305,32 +323,47 @@ def main():
     except (OSError, ValueError):
         pass
     hbm = float(peaks.get("hbm_gbs", 6650.0))
-    # node visits are counted in both extend and shadow queries; scale to the
-    # extend share by ray count (visits per query are similar within 2x)
-    frac_ext = cnt["extend_rays"] / max(1, cnt["extend_rays"] + cnt["shadow_rays"])
-    ext_nodes = cnt["node_visits"] * frac_ext
-    ext_prims = cnt["prim_visits"] * frac_ext
-    # per query: ray read (32 B) + hit written (16 B); 80 B per wide node, 48 B per triangle
-    bytes_per_frame = cnt["extend_rays"] * (32 + 16) + ext_nodes * 80 + ext_prims * 48
-    # one frame's bytes over the timed frame's extend launches (the counting pass
-    # renders the same frame, whatever its wave size)
-    per_launch_bytes = bytes_per_frame / max(1, stg["extend_launches"])
-    per_launch_ms = extend_ms / max(1, extend_launches)
-    achieved = per_launch_bytes / (per_launch_ms / 1000.0) / 1e9
-    # DRAM bytes (read + write) per k_extend launch of this workload, from one
-    # ncu capture of the nine launches of the first frame (dram__bytes_read.sum +
-    # dram__bytes_write.sum, a single-pass capture of the full-size run; see
-    # profiles/k_extend_traffic_dense_mesh_1024x1024_64spp.md).  ncu flushes the
-    # caches before each captured launch, so this is the cold-cache figure.
-    traffic = EXTEND_DRAM_BYTES_PER_LAUNCH if SCENE_ARGS["scene_id"] == az.SCENE_DENSE_MESH else None
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                "traffic": traffic, "traffic_unit": "bytes per launch (ncu capture)",
-                "algorithmic_bytes_per_launch": per_launch_bytes, "kernel": "k_extend (closest-hit traversal)",
+    launches_per_frame = max(1, stg["extend_launches"])
+    ext_q, sh_q = max(1, cnt["extend_rays"]), max(1, cnt["shadow_rays"])
+    # closest hit, per query: ray read (32 B) + hit written (16 B); 80 B per wide node, 48 B per triangle
+    ext_bytes = cnt["extend_rays"] * (32 + 16) + cnt["node_visits"] * 80 + cnt["prim_visits"] * 48
+    # visibility, per query: origin, direction and contribution read (48 B) + kind (4 B) + one 16-byte sum
+    # for a visible sample (counted for every query); the same node and triangle bytes
+    sh_bytes = cnt["shadow_rays"] * (48 + 4 + 16) + cnt["shadow_node_visits"] * 80 + cnt["shadow_prim_visits"] * 48
+    per_launch_ext_ms = stg["extend_ms"] / launches_per_frame
+    per_launch_sh_ms = stg["shadow_ms"] / launches_per_frame
+    ext_achieved = ext_bytes / launches_per_frame / (per_launch_ext_ms / 1000.0) / 1e9
+    sh_achieved = sh_bytes / launches_per_frame / (per_launch_sh_ms / 1000.0) / 1e9
+    # DRAM read + write per query from a single-pass ncu capture of every launch
+    # of one small frame of the same scene (DRAM_BYTES_PER_QUERY), scaled to a
+    # launch of this frame by its query count
+    dense = SCENE_ARGS["scene_id"] == az.SCENE_DENSE_MESH
+    ext_traffic = (DRAM_BYTES_PER_QUERY["k_extend"] * ext_q / launches_per_frame
+                   if dense and DRAM_BYTES_PER_QUERY["k_extend"] else None)
+    sh_traffic = (DRAM_BYTES_PER_QUERY["k_shadow"] * sh_q / launches_per_frame
+                  if dense and DRAM_BYTES_PER_QUERY["k_shadow"] else None)
+    limiter = ("instruction issue of divergent traversal (about 8 of 32 lanes active per warp instruction, "
+               "two thirds of issue slots used; DRAM at a few percent of peak: %s)" % PROFILE_NOTE)
+    roofline = {"bound": "hbm", "achieved": ext_achieved, "peak": hbm, "unit": "GB/s", "frac": ext_achieved / hbm,
+                "traffic": ext_traffic, "traffic_unit": "DRAM bytes per launch (ncu, scaled from a small frame)",
+                "algorithmic_bytes_per_launch": ext_bytes / launches_per_frame,
+                "kernel": "k_extend (closest-hit traversal)", "limiter": limiter,
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650",
-                "bytes_per_segment": bytes_per_frame / max(1, cnt["extend_rays"]),
-                "node_visits_per_segment": ext_nodes / max(1, cnt["extend_rays"]),
-                "prim_visits_per_segment": ext_prims / max(1, cnt["extend_rays"]),
-                "extend_share_of_step": extend_ms / max(ms, 1e-9)}
+                "bytes_per_segment": ext_bytes / ext_q,
+                "node_visits_per_segment": cnt["node_visits"] / ext_q,
+                "prim_visits_per_segment": cnt["prim_visits"] / ext_q,
+                "launch_ms": per_launch_ext_ms,
+                "extend_share_of_serial_frame": stg["extend_ms"] / max(stg["gpu_ms"], 1e-9)}
+    roofline_shadow = {"bound": "hbm", "achieved": sh_achieved, "peak": hbm, "unit": "GB/s",
+                       "frac": sh_achieved / hbm, "traffic": sh_traffic,
+                       "traffic_unit": "DRAM bytes per launch (ncu, scaled from a small frame)",
+                       "algorithmic_bytes_per_launch": sh_bytes / launches_per_frame,
+                       "kernel": "k_shadow (visibility, any hit)", "limiter": limiter,
+                       "bytes_per_query": sh_bytes / sh_q,
+                       "node_visits_per_query": cnt["shadow_node_visits"] / sh_q,
+                       "prim_visits_per_query": cnt["shadow_prim_visits"] / sh_q,
+                       "launch_ms": per_launch_sh_ms,
+                       "shadow_share_of_serial_frame": stg["shadow_ms"] / max(stg["gpu_ms"], 1e-9)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -346,16 +379,21 @@ def main():
 
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
-               "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+               "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+               "scaling": "strong" if split else "weak",
                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator, azimuth structs)",
                "config": {"workload": WORKLOAD, "triangles": int(scene.triangle_count), "width": w, "height": h,
-                          "spp": spp, "max_depth": scene.max_depth(), "paths_per_step_per_gpu": paths_per_frame,
-                          "parallelism": "dp%d (one frame per GPU, own seed)" % world,
+                          "spp": spp, "max_depth": scene.max_depth(),
+                          "paths_per_step_per_gpu": paths_per_frame // world if split else paths_per_frame,
+                          "parallelism": ("split%d (one frame per step: equal parts of its camera samples per "
+                                          "GPU, one NCCL reduce of the films)" % world) if split else
+                                         "dp%d (one frame per GPU, own seed)" % world,
                           "l2": "inputs larger than L2 (scene %.0f MB on device)" % (
                               gs.info()["device_bytes"] / 1e6),
                           "scene_upload_s": upload_s, "scene_build": build, "autotune": tune},
                "segments_per_s": world * seg / (ms / 1000.0), "rays_per_s": world * (seg + shadow) / (ms / 1000.0),
                "gpu_launches": int(launches), "stages_one_frame": stages, "e2e": e2e, "roofline": roofline,
+               "roofline_shadow": roofline_shadow,
                "clocks": clk}
         if cpu:
             out["cpu_baseline"] = cpu
