@@ -11,8 +11,11 @@ largest square at or below); depth uniform in 5..16; odd jobs render with a
 path guide that trains while rendering.  Scene generation and upload happen
 before the timed batch.  Reported: aggregate Mpaths/s (all jobs' camera
 samples / device time from the batch start to the last completion), job
-completion-time p50 / p99 (jobs shortest first on `--streams` streams), and
-the same batch largest first and on one stream for comparison.
+completion-time p50 / p99 (jobs shortest first on `--streams` streams), the
+same batch largest first and on one stream for comparison, and the batch with
+its plain jobs in multi-scene tile waves (one persistent chain of launches
+pulling 4096-sample tiles of every plain job from a device work queue) while
+the other streams take the guided jobs.
 """
 import argparse
 import json
@@ -82,12 +85,13 @@ def run(n_jobs=256, streams=8, seed=0, log=lambda m: print(m, file=sys.stderr, f
            "triangles": int(sum(p[3]["triangles"] for p in prepared)),
            "spheres": int(sum(p[3]["spheres"] for p in prepared)),
            "configs": [int(sum(1 for s in specs if s["config"] == c)) for c in range(3)]}
-    for label, nstreams, lf in (("concurrent", streams, False), ("concurrent_largest_first", streams, True),
-                                ("one_stream", 1, False)):
+    for label, nstreams, lf, tiles in (("tiles", streams, True, True), ("concurrent", streams, False, False),
+                                       ("concurrent_largest_first", streams, True, False),
+                                       ("one_stream", 1, False, False)):
         for f in films:
             f.zero_()
         torch.cuda.synchronize()
-        per, st = az.render_batch(jobs, streams=nstreams, largest_first=lf)
+        per, st = az.render_batch(jobs, streams=nstreams, largest_first=lf, tiles=tiles)
         done = np.array([p["done_ms"] for p in per])
         out[label] = {"streams": st["streams"], "gpu_ms": st["gpu_ms"], "samples": st["samples"],
                       "mpaths_per_s": st["samples"] / (st["gpu_ms"] / 1000.0) / 1e6,

@@ -34,7 +34,8 @@ def test_graph_replay_renders_the_same_film(gpu):
         assert ol.film_compare(f2.cpu().numpy(), films[0], 1e-4)[0] < 0.9   # different samples
 
 
-def test_batch_jobs_equal_their_own_renders(gpu):
+@pytest.mark.parametrize("tiles", [False, True], ids=["streams", "tile_waves"])
+def test_batch_jobs_equal_their_own_renders(gpu, tiles):
     import torch
     rng = np.random.default_rng(5)
     specs = [(az.SCENE_CORNELL, dict(width=64, height=48, spp=4)),
@@ -55,7 +56,8 @@ def test_batch_jobs_equal_their_own_renders(gpu):
         jobs.append({"gpu_scene": gs, "film_ptr": f.data_ptr(), "seed": int(rng.integers(1 << 30))})
     guide = az.Guide(gscenes[4], seed=3)
     jobs[4]["guide"] = guide
-    per, st = az.render_batch(jobs, streams=3, chunk_samples=4096)
+    # tiles: the five plain jobs (five scenes) share tile waves on one stream, the guided job runs beside
+    per, st = az.render_batch(jobs, streams=3, chunk_samples=4096, tiles=tiles)
     assert st["jobs"] == len(jobs) and st["failed"] == 0 and st["streams"] == 3
     assert all(p["status"] == 0 for p in per)
     assert 0 < st["p50_ms"] <= st["p99_ms"] <= st["gpu_ms"] + 1e-3
