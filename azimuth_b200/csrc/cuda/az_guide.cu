@@ -11,9 +11,12 @@
 // backward pass: dX = dY W^T on the tensor cores with a second, transposed
 // copy of the fragments, dW = X^T dY on the tensor cores with operands
 // gathered from the row-major copies and accumulated per block in shared
-// memory, and the encoding gradient scattered into the hash grid with
-// atomics.  Adam keeps FP32 master weights and refreshes the BF16 fragments
-// and the FP16 grid after every step.
+// memory (each entry summed by one warp in a fixed order), and the encoding
+// gradient scattered into the hash grid as fixed-point integers; training is
+// therefore deterministic: the same rows give the same step bit for bit.
+// Adam keeps FP32 master weights and refreshes the BF16 fragments and the
+// FP16 grid after every step.
+#include <cub/cub.cuh>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
@@ -342,54 +345,84 @@ __global__ void __launch_bounds__(kInferWarps * 32) k_guide_infer(DevScene S, Wa
 }
 
 // ---- training targets from the recorded vertices of a finished wave ----
-__global__ void k_guide_targets(const GuideRecord *rec, uint32_t n_rec, uint32_t levels, const float4 *accum,
-                                GuideRow *rows, uint32_t cap, uint32_t *count, float *wsum) {
-    const uint32_t total = n_rec * levels;
+// Deterministic: every record gets its weight (0: unusable) and flag, an
+// exclusive scan of the flags gives each usable record its row, so rows keep
+// the records' order whatever order the threads run in.
+__global__ void k_guide_weights(const GuideRecord *rec, uint32_t total, uint32_t n_rec, const float4 *accum,
+                                float *weight, uint32_t *flag) {
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x) {
         const GuideRecord R = rec[k];
-        if (R.tpc.w != 1.0f || R.snap.w != 1.0f || !(R.pos_q.w > 0.0f)) continue;
-        const float4 a = accum[k % n_rec];
-        // radiance along wi: what the child's subtree added, divided by its throughput
-        const float lx = R.tpc.x > 1e-20f ? (a.x - R.snap.x) / R.tpc.x : 0.0f;
-        const float ly = R.tpc.y > 1e-20f ? (a.y - R.snap.y) / R.tpc.y : 0.0f;
-        const float lz = R.tpc.z > 1e-20f ? (a.z - R.snap.z) / R.tpc.z : 0.0f;
-        const float lum = fmaxf(0.0f, 0.2126f * lx + 0.7152f * ly + 0.0722f * lz);
-        const float cs = fmaxf(0.0f, R.n.x * R.wi.x + R.n.y * R.wi.y + R.n.z * R.wi.z);
-        // KL objective toward the density proportional to L(wi) cos: weight F / q
-        const float w = lum * cs / R.pos_q.w;
-        if (!(w > 0.0f) || !isfinite(w)) continue;
-        const uint32_t j = atomicAdd(count, 1u);
-        if (j >= cap) continue;
-        atomicAdd(wsum, w);
+        float w = 0.0f;
+        if (R.tpc.w == 1.0f && R.snap.w == 1.0f && R.pos_q.w > 0.0f) {
+            const float4 a = accum[k % n_rec];
+            // radiance along wi: what the child's subtree added, divided by its throughput
+            const float lx = R.tpc.x > 1e-20f ? (a.x - R.snap.x) / R.tpc.x : 0.0f;
+            const float ly = R.tpc.y > 1e-20f ? (a.y - R.snap.y) / R.tpc.y : 0.0f;
+            const float lz = R.tpc.z > 1e-20f ? (a.z - R.snap.z) / R.tpc.z : 0.0f;
+            const float lum = fmaxf(0.0f, 0.2126f * lx + 0.7152f * ly + 0.0722f * lz);
+            const float cs = fmaxf(0.0f, R.n.x * R.wi.x + R.n.y * R.wi.y + R.n.z * R.wi.z);
+            // KL objective toward the density proportional to L(wi) cos: weight F / q
+            w = lum * cs / R.pos_q.w;
+            if (!(w > 0.0f) || !isfinite(w)) w = 0.0f;
+        }
+        weight[k] = w;
+        flag[k] = w > 0.0f ? 1u : 0u;
+    }
+}
+
+// Usable record k to row pos[k] (the first `cap` only); the kept weights also
+// go to wk[pos] (zero elsewhere) for the weight sum; count = kept rows.
+__global__ void k_guide_compact(const GuideRecord *rec, uint32_t total, const float *weight, const uint32_t *flag,
+                                const uint32_t *pos, GuideRow *rows, float *wk, uint32_t cap, uint32_t *count) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x) {
+        if (k == total - 1) *count = min(pos[k] + flag[k], cap);
+        if (!flag[k] || pos[k] >= cap) continue;
+        const GuideRecord R = rec[k];
         GuideRow r;
-        r.pos_w = make_float4(R.pos_q.x, R.pos_q.y, R.pos_q.z, w);
+        r.pos_w = make_float4(R.pos_q.x, R.pos_q.y, R.pos_q.z, weight[k]);
         r.n = R.n;
         r.wo = R.wo;
         r.wi = R.wi;
-        rows[j] = r;
+        rows[pos[k]] = r;
+        wk[pos[k]] = weight[k];
     }
 }
 
 // ---- forward, loss and backward over training rows ----
-// Gradients accumulate into w_grad (MLP), b_grad (output bias) and
-// grid_grad; the loss sum into *loss.  Weights are scaled by
-// count / wsum (mean weight 1).  Optional outputs for tests: raw outputs
-// (n x 64) and encoding gradients (n x 32).
+// Deterministic gradients: within a block the MLP weight and output-bias
+// gradients are summed by the warp that owns them (dW rows 16w..16w+15 and
+// bias columns 16w..16w+15 belong to warp w), over the block's four tiles in
+// a fixed order; every block writes its sums, its loss and nothing else to
+// its own slot of `part`, which k_guide_reduce adds up block by block.  The
+// hash-grid gradient is scattered as 64-bit fixed point (2^-32 units), whose
+// integer additions give the same sum in any order.  Row weights are scaled
+// by count / wsum (mean weight 1) and then capped at `wcap`, so that a rare
+// path with a huge radiance estimate cannot pull the proposal onto itself
+// (any proposal leaves the estimator unbiased).  Optional outputs for tests:
+// raw outputs (n x 64) and encoding gradients (n x 32).
+constexpr int kPart = NW + W + 4;            // floats per block slot: dW, db, loss (padded)
+constexpr float kGridFix = 4294967296.0f;    // fixed-point scale of the grid gradient
+
 struct TrainArgs {
     const GuideRow *rows;
     const uint32_t *count;    // rows used: min(*count, cap)
     uint32_t cap;
     const float *wsum;        // null: weights used as given
-    float *w_grad, *b_grad;
-    float2 *grid_grad;
-    float *loss;
+    float wcap;               // cap on a normalised row weight (with wsum)
+    float *part;              // [gridDim.x][kPart]
+    unsigned long long *grid_grad;   // [entry][2] fixed point, or null
     float *dbg_out, *dbg_enc;
 };
 
 constexpr size_t kTrainSmem = 2 * NFRAG * sizeof(uint2) + (size_t)GUIDE_LAYERS * W * W * sizeof(float) +
-                              W * sizeof(float) * 2 +
+                              W * sizeof(float) * 2 + kWarps * sizeof(float) +
                               (size_t)kWarps * ((GUIDE_LAYERS + 1) * 16 * XS * sizeof(__nv_bfloat16) +
                                                 16 * OS * sizeof(float));
+
+__device__ __forceinline__ unsigned long long to_fixed(float v) {
+    v = fminf(fmaxf(v, -1e8f), 1e8f);
+    return (unsigned long long)__float2ll_rn(v * kGridFix);
+}
 
 __global__ void __launch_bounds__(kWarps * 32) k_guide_train(GuideNetDev N, TrainArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -398,10 +431,14 @@ __global__ void __launch_bounds__(kWarps * 32) k_guide_train(GuideNetDev N, Trai
     float *s_dw = reinterpret_cast<float *>(s_wt + NFRAG);
     float *s_bias = s_dw + GUIDE_LAYERS * W * W;
     float *s_db = s_bias + W;
-    unsigned char *per_warp = reinterpret_cast<unsigned char *>(s_db + W);
+    float *s_loss = s_db + W;
+    unsigned char *per_warp = reinterpret_cast<unsigned char *>(s_loss + kWarps);
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3u;
     const size_t warp_bytes = (GUIDE_LAYERS + 1) * 16 * XS * sizeof(__nv_bfloat16) + 16 * OS * sizeof(float);
-    __nv_bfloat16 *s_x = reinterpret_cast<__nv_bfloat16 *>(per_warp + warp * warp_bytes);   // [layer][16][XS]
+    auto warp_x = [&](uint32_t w) {   // [layer][16][XS] inputs of warp w's tile
+        return reinterpret_cast<__nv_bfloat16 *>(per_warp + w * warp_bytes);
+    };
+    __nv_bfloat16 *s_x = warp_x(warp);
     __nv_bfloat16 *s_dy = s_x + GUIDE_LAYERS * 16 * XS;                                    // [16][XS]
     float *s_o = reinterpret_cast<float *>(s_dy + 16 * XS);                                 // [16][OS]
     load_frags(s_wf, N.wf);
@@ -414,9 +451,14 @@ __global__ void __launch_bounds__(kWarps * 32) k_guide_train(GuideNetDev N, Trai
     __syncthreads();
     const uint32_t n = min(*A.count, A.cap);
     const float wscale = A.wsum ? (float)n / fmaxf(*A.wsum, 1e-30f) : 1.0f;
+    const float wcap = A.wsum && A.wcap > 0.0f ? A.wcap : FLT_MAX;
     float loss_acc = 0.0f;
     const uint32_t tiles = (n + 15u) / 16u;
-    for (uint32_t tile = blockIdx.x * kWarps + warp; tile < tiles; tile += gridDim.x * kWarps) {
+    const uint32_t groups = (tiles + kWarps - 1u) / kWarps;
+    // every warp of the block runs the same iterations (a warp past the last
+    // tile works on rows past n, which contribute nothing)
+    for (uint32_t grp = blockIdx.x; grp < groups; grp += gridDim.x) {
+        const uint32_t tile = grp * kWarps + warp;
         // ---- forward, keeping each layer's input ----
         f3 p[2], nr[2], wo[2];
 #pragma unroll
@@ -450,19 +492,15 @@ __global__ void __launch_bounds__(kWarps * 32) k_guide_train(GuideNetDev N, Trai
             float d[W];
             if (i < n) {
                 const GuideRow r = A.rows[i];
-                loss_acc += loss_grad(o, mk(r.n.x, r.n.y, r.n.z), mk(r.wi.x, r.wi.y, r.wi.z), r.pos_w.w * wscale, d);
+                loss_acc += loss_grad(o, mk(r.n.x, r.n.y, r.n.z), mk(r.wi.x, r.wi.y, r.wi.z),
+                                      fminf(r.pos_w.w * wscale, wcap), d);
             } else {
                 for (int j = 0; j < W; j++) d[j] = 0.0f;
             }
             for (int j = 0; j < W; j++) o[j] = d[j];
         }
         __syncwarp();
-        // output-bias gradient and the BF16 row-major copy of dY
-        for (int j = lane; j < W; j += 32) {
-            float sacc = 0.0f;
-            for (int r = 0; r < 16; r++) sacc += s_o[r * OS + j];
-            atomicAdd(&s_db[j], sacc);
-        }
+        // BF16 row-major copy of dY of the output layer
         for (int e = lane; e < 16 * W; e += 32) {
             const int r = e / W, c = e % W;
             s_dy[r * XS + c] = __float2bfloat16_rn(s_o[r * OS + c]);
@@ -479,36 +517,57 @@ __global__ void __launch_bounds__(kWarps * 32) k_guide_train(GuideNetDev N, Trai
         }
         // ---- backward through the layers ----
         for (int l = GUIDE_LAYERS - 1; l >= 0; l--) {
-            const __nv_bfloat16 *X = s_x + l * 16 * XS;
-            // dW_l += X_l^T dY_l: M = input unit, K = row, N = output unit
+            __syncthreads();   // every warp's X_l and dY_l are in shared memory
+            // dW_l += X_l^T dY_l over the block's four tiles in order: warp w
+            // owns the input units 16w..16w+15 (M), all 64 output units (N)
+            {
+                const int c0 = 16 * (int)warp + (int)g;
+                float c[8][4];
 #pragma unroll
-            for (int mt = 0; mt < 4; mt++) {
-                const int c0 = 16 * mt + (int)g;
-                uint32_t a[4];
-                a[0] = pack2(X, 2 * t, 2 * t + 1, c0);
-                a[1] = pack2(X, 2 * t, 2 * t + 1, c0 + 8);
-                a[2] = pack2(X, 2 * t + 8, 2 * t + 9, c0);
-                a[3] = pack2(X, 2 * t + 8, 2 * t + 9, c0 + 8);
+                for (int nn = 0; nn < 8; nn++) c[nn][0] = c[nn][1] = c[nn][2] = c[nn][3] = 0.0f;
+                for (uint32_t src = 0; src < (uint32_t)kWarps; src++) {
+                    const __nv_bfloat16 *X = warp_x(src) + l * 16 * XS;
+                    const __nv_bfloat16 *DY = warp_x(src) + GUIDE_LAYERS * 16 * XS;
+                    uint32_t a[4];
+                    a[0] = pack2(X, 2 * t, 2 * t + 1, c0);
+                    a[1] = pack2(X, 2 * t, 2 * t + 1, c0 + 8);
+                    a[2] = pack2(X, 2 * t + 8, 2 * t + 9, c0);
+                    a[3] = pack2(X, 2 * t + 8, 2 * t + 9, c0 + 8);
+#pragma unroll
+                    for (int nn = 0; nn < 8; nn++) {
+                        const int oc = 8 * nn + (int)g;
+                        uint2 b;
+                        b.x = pack2(DY, 2 * t, 2 * t + 1, oc);
+                        b.y = pack2(DY, 2 * t + 8, 2 * t + 9, oc);
+                        mma16816(c[nn], a, b);
+                    }
+                }
+                float *dw = s_dw + l * W * W;
 #pragma unroll
                 for (int nn = 0; nn < 8; nn++) {
-                    const int oc = 8 * nn + (int)g;
-                    uint2 b;
-                    b.x = pack2(s_dy, 2 * t, 2 * t + 1, oc);
-                    b.y = pack2(s_dy, 2 * t + 8, 2 * t + 9, oc);
-                    float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-                    mma16816(c, a, b);
-                    float *dw = s_dw + l * W * W;
                     const int col = 8 * nn + 2 * (int)t;
-                    atomicAdd(&dw[c0 * W + col], c[0]);
-                    atomicAdd(&dw[c0 * W + col + 1], c[1]);
-                    atomicAdd(&dw[(c0 + 8) * W + col], c[2]);
-                    atomicAdd(&dw[(c0 + 8) * W + col + 1], c[3]);
+                    dw[c0 * W + col] += c[nn][0];
+                    dw[c0 * W + col + 1] += c[nn][1];
+                    dw[(c0 + 8) * W + col] += c[nn][2];
+                    dw[(c0 + 8) * W + col + 1] += c[nn][3];
+                }
+                if (l == GUIDE_LAYERS - 1 && lane < 16) {
+                    // output-bias gradient: warp w owns columns 16w..16w+15
+                    const int j = 16 * (int)warp + (int)lane;
+                    float sacc = 0.0f;
+                    for (uint32_t src = 0; src < (uint32_t)kWarps; src++) {
+                        const float *o = reinterpret_cast<const float *>(warp_x(src) + (GUIDE_LAYERS + 1) * 16 * XS);
+                        for (int r = 0; r < 16; r++) sacc += o[r * OS + j];
+                    }
+                    s_db[j] += sacc;
                 }
             }
+            __syncthreads();   // the dW reads are done before dY_{l-1} replaces dY_l
             // dX_l = dY_l W_l^T
             float dx[8][4];
             layer_mma(dya, s_wt + l * 4 * 8 * 32, lane, dx);
             __syncwarp();
+            const __nv_bfloat16 *X = s_x + l * 16 * XS;
             if (l > 0) {
                 // through the ReLU that produced X_l: dY_{l-1} = dX_l where X_l > 0
 #pragma unroll
@@ -542,8 +601,10 @@ __global__ void __launch_bounds__(kWarps * 32) k_guide_train(GuideNetDev N, Trai
                             Corners c;
                             grid_corners(N, lv, p[h], c);
 #pragma unroll
-                            for (int k = 0; k < 8; k++)
-                                atomicAdd(&A.grid_grad[c.idx[k]], make_float2(c.w[k] * gx, c.w[k] * gy));
+                            for (int k = 0; k < 8; k++) {
+                                atomicAdd(&A.grid_grad[2 * (size_t)c.idx[k]], to_fixed(c.w[k] * gx));
+                                atomicAdd(&A.grid_grad[2 * (size_t)c.idx[k] + 1], to_fixed(c.w[k] * gy));
+                            }
                         }
                     }
                 }
@@ -551,12 +612,30 @@ __global__ void __launch_bounds__(kWarps * 32) k_guide_train(GuideNetDev N, Trai
         }
         __syncwarp();
     }
-    if (lane < 16 && loss_acc != 0.0f) atomicAdd(A.loss, loss_acc);
+    // the block's loss: lanes, then warps, in a fixed order
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) loss_acc += __shfl_down_sync(0xFFFFFFFFu, loss_acc, off);
+    if (lane == 0) s_loss[warp] = loss_acc;
     __syncthreads();
-    for (int i = threadIdx.x; i < GUIDE_LAYERS * W * W; i += blockDim.x)
-        if (s_dw[i] != 0.0f) atomicAdd(&A.w_grad[i], s_dw[i]);
-    for (int i = threadIdx.x; i < W; i += blockDim.x)
-        if (s_db[i] != 0.0f) atomicAdd(&A.b_grad[i], s_db[i]);
+    float *part = A.part + (size_t)blockIdx.x * kPart;
+    for (int i = threadIdx.x; i < GUIDE_LAYERS * W * W; i += blockDim.x) part[i] = s_dw[i];
+    for (int i = threadIdx.x; i < W; i += blockDim.x) part[NW + i] = s_db[i];
+    if (threadIdx.x == 0) {
+        float l = 0.0f;
+        for (int w = 0; w < kWarps; w++) l += s_loss[w];
+        part[NW + W] = l;
+    }
+}
+
+// Block slots of k_guide_train added up in block order: w_grad, b_grad, loss.
+__global__ void k_guide_reduce(const float *part, uint32_t blocks, float *w_grad, float *b_grad, float *loss) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < (uint32_t)(NW + W + 1); i += gridDim.x * blockDim.x) {
+        float s = 0.0f;
+        for (uint32_t b = 0; b < blocks; b++) s += part[(size_t)b * kPart + i];
+        if (i < (uint32_t)NW) w_grad[i] = s;
+        else if (i < (uint32_t)(NW + W)) b_grad[i - NW] = s;
+        else *loss = s;
+    }
 }
 
 // ---- Adam (Kingma, Ba 2015) with FP32 master weights; gradients are cleared ----
@@ -575,11 +654,15 @@ __global__ void k_adam(float *w, float *g, float *m, float *v, uint32_t n, AdamS
     }
 }
 
-__global__ void k_adam_grid(float2 *w, float2 *g, float2 *m, float2 *v, __half2 *feat, uint32_t n, AdamStep a) {
+__global__ void k_adam_grid(float2 *w, unsigned long long *gq, float2 *m, float2 *v, __half2 *feat, uint32_t n,
+                            AdamStep a) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const float2 gi = g[i];
+        // the fixed-point sums back to float (two's complement: a negative sum wraps)
+        const float2 gi = make_float2((float)(long long)gq[2 * (size_t)i] * (1.0f / kGridFix),
+                                      (float)(long long)gq[2 * (size_t)i + 1] * (1.0f / kGridFix));
         if (gi.x == 0.0f && gi.y == 0.0f && m[i].x == 0.0f && m[i].y == 0.0f) continue;   // never touched
-        g[i] = make_float2(0.0f, 0.0f);
+        gq[2 * (size_t)i] = 0ull;
+        gq[2 * (size_t)i + 1] = 0ull;
         float2 mi = m[i], vi = v[i], wi = w[i];
         mi.x = a.b1 * mi.x + (1.0f - a.b1) * gi.x;
         mi.y = a.b1 * mi.y + (1.0f - a.b1) * gi.y;
@@ -636,7 +719,14 @@ struct GuideState {
     float *bias = nullptr, *b_grad = nullptr, *b_m = nullptr, *b_v = nullptr;
     uint2 *wf = nullptr, *wt = nullptr;
     __half2 *feat = nullptr;
-    float2 *grid = nullptr, *grid_grad = nullptr, *grid_m = nullptr, *grid_v = nullptr;
+    float2 *grid = nullptr, *grid_m = nullptr, *grid_v = nullptr;
+    unsigned long long *grid_grad = nullptr;   // [entry][2], fixed point (k_guide_train)
+    float *part = nullptr;                     // per-block gradient slots of k_guide_train
+    // scratch of the deterministic row compaction (k_guide_weights / k_guide_compact)
+    float *rec_weight = nullptr, *kept_weight = nullptr;
+    uint32_t *rec_flag = nullptr, *rec_pos = nullptr;
+    void *cub_temp = nullptr;
+    size_t rec_cap = 0, cub_bytes = 0;
     uint32_t n_rec = 0;             // samples per wave whose vertices are recorded
     uint32_t steps_per_wave = 1;    // Adam steps on each wave's rows
     GuideRow *rows = nullptr;
@@ -653,6 +743,8 @@ struct GuideState {
 
     ~GuideState() {
         for (void *p : allocs)
+            if (p) cudaFree(p);
+        for (void *p : {(void *)rec_weight, (void *)rec_flag, (void *)rec_pos, cub_temp})
             if (p) cudaFree(p);
     }
     template <typename T>
@@ -700,6 +792,9 @@ int RefreshFragments(GuideState &g, cudaStream_t st) {
     return AZ_OK;
 }
 
+// A normalised training row weight (mean 1) counts at most this much.
+constexpr float kWeightCap = 25.0f;
+
 // One training step over rows[0 .. min(*count, cap)): gradients, then Adam.
 int TrainStep(GuideState &g, const GuideRow *rows, const uint32_t *count, uint32_t cap, const float *wsum,
               cudaStream_t st, float *dbg_out = nullptr, float *dbg_enc = nullptr, bool apply = true) {
@@ -708,14 +803,13 @@ int TrainStep(GuideState &g, const GuideRow *rows, const uint32_t *count, uint32
     A.count = count;
     A.cap = cap;
     A.wsum = wsum;
-    A.w_grad = g.w_grad;
-    A.b_grad = g.b_grad;
+    A.wcap = kWeightCap;
+    A.part = g.part;
     A.grid_grad = g.grid_grad;
-    A.loss = g.loss;
     A.dbg_out = dbg_out;
     A.dbg_enc = dbg_enc;
-    AZ_CUDA_TRY(cudaMemsetAsync(g.loss, 0, sizeof(float), st));
     k_guide_train<<<g.sms, kWarps * 32, kTrainSmem, st>>>(g.net, A);
+    k_guide_reduce<<<(NW + W + 1 + 255) / 256, 256, 0, st>>>(g.part, (uint32_t)g.sms, g.w_grad, g.b_grad, g.loss);
     AZ_CUDA_TRY(cudaGetLastError());
     if (!apply) return AZ_OK;
     g.step++;
@@ -756,7 +850,8 @@ int CreateGuide(const GpuScene &G, const az_guide_config *cfg, GuideState **out)
     g->wt = g->Alloc<uint2>(NFRAG);
     g->feat = g->Alloc<__half2>(kGridN);
     g->grid = g->Alloc<float2>(kGridN);
-    g->grid_grad = g->Alloc<float2>(kGridN);
+    g->grid_grad = g->Alloc<unsigned long long>(2 * (size_t)kGridN);
+    g->part = g->Alloc<float>((size_t)g->sms * kPart);
     g->grid_m = g->Alloc<float2>(kGridN);
     g->grid_v = g->Alloc<float2>(kGridN);
     g->rows = g->Alloc<GuideRow>(g->rows_cap);
@@ -785,7 +880,7 @@ int CreateGuide(const GpuScene &G, const az_guide_config *cfg, GuideState **out)
     AZ_CUDA_TRY(cudaMemset(g->b_grad, 0, W * sizeof(float)));
     AZ_CUDA_TRY(cudaMemset(g->b_m, 0, W * sizeof(float)));
     AZ_CUDA_TRY(cudaMemset(g->b_v, 0, W * sizeof(float)));
-    AZ_CUDA_TRY(cudaMemset(g->grid_grad, 0, kGridN * sizeof(float2)));
+    AZ_CUDA_TRY(cudaMemset(g->grid_grad, 0, 2 * (size_t)kGridN * sizeof(unsigned long long)));
     AZ_CUDA_TRY(cudaMemset(g->grid_m, 0, kGridN * sizeof(float2)));
     AZ_CUDA_TRY(cudaMemset(g->grid_v, 0, kGridN * sizeof(float2)));
     k_half_grid<<<g->sms * 8, 256>>>(g->grid, g->feat, kGridN);
@@ -854,8 +949,36 @@ int GuideInfer(GuideState &g, const GpuScene &G, const WaveQueues &Q, uint32_t l
 int GuideTrainWave(GuideState &g, const WaveQueues &Q, cudaStream_t st) {
     AZ_CUDA_TRY(cudaMemsetAsync(g.count, 0, 4 * sizeof(uint32_t), st));
     AZ_CUDA_TRY(cudaMemsetAsync(g.wsum, 0, sizeof(float), st));
-    k_guide_targets<<<g.sms * 4, 256, 0, st>>>(Q.rec, Q.n_rec, Q.rec_levels, Q.accum, g.rows, g.rows_cap, g.count,
-                                               g.wsum);
+    const uint32_t total = Q.n_rec * Q.rec_levels;
+    if (total == 0) return AZ_OK;
+    if (g.rec_cap < total) {
+        for (void **p : {(void **)&g.rec_weight, (void **)&g.rec_flag, (void **)&g.rec_pos, &g.cub_temp}) {
+            if (*p) cudaFree(*p);
+            *p = nullptr;
+        }
+        g.rec_cap = 0;
+        size_t scan_bytes = 0, sum_bytes = 0;
+        AZ_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, g.rec_flag, g.rec_pos, (int)total));
+        AZ_CUDA_TRY(cub::DeviceReduce::Sum(nullptr, sum_bytes, g.kept_weight, g.wsum, (int)g.rows_cap));
+        g.cub_bytes = std::max(scan_bytes, sum_bytes);
+        if (cudaMalloc((void **)&g.rec_weight, (size_t)total * sizeof(float) + (size_t)g.rows_cap * sizeof(float)) !=
+                cudaSuccess ||
+            cudaMalloc((void **)&g.rec_flag, (size_t)total * sizeof(uint32_t)) != cudaSuccess ||
+            cudaMalloc((void **)&g.rec_pos, (size_t)total * sizeof(uint32_t)) != cudaSuccess ||
+            cudaMalloc(&g.cub_temp, g.cub_bytes) != cudaSuccess)
+            return SetError(AZ_ERR_OUT_OF_MEMORY, "path guide training scratch");
+        g.rec_cap = total;
+    }
+    g.kept_weight = g.rec_weight + g.rec_cap;   // rows_cap floats after the records' weights
+    const int grid = g.sms * 4;
+    k_guide_weights<<<grid, 256, 0, st>>>(Q.rec, total, Q.n_rec, Q.accum, g.rec_weight, g.rec_flag);
+    size_t bytes = g.cub_bytes;
+    AZ_CUDA_TRY(cub::DeviceScan::ExclusiveSum(g.cub_temp, bytes, g.rec_flag, g.rec_pos, (int)total, st));
+    AZ_CUDA_TRY(cudaMemsetAsync(g.kept_weight, 0, (size_t)g.rows_cap * sizeof(float), st));
+    k_guide_compact<<<grid, 256, 0, st>>>(Q.rec, total, g.rec_weight, g.rec_flag, g.rec_pos, g.rows, g.kept_weight,
+                                          g.rows_cap, g.count);
+    bytes = g.cub_bytes;
+    AZ_CUDA_TRY(cub::DeviceReduce::Sum(g.cub_temp, bytes, g.kept_weight, g.wsum, (int)g.rows_cap, st));
     AZ_CUDA_TRY(cudaGetLastError());
     for (uint32_t k = 0; k < g.steps_per_wave; k++) {
         int rc = TrainStep(g, g.rows, g.count, g.rows_cap, g.wsum, st);
@@ -964,7 +1087,7 @@ extern "C" int az_guide_eval(az_guide *g, const float *rows, uint32_t n, float *
         cudaMemset(s.w_grad, 0, NW * sizeof(float));
         cudaMemset(s.b_grad, 0, W * sizeof(float));
         // the grid gradient is not needed here: pass none
-        float2 *gg = s.grid_grad;
+        unsigned long long *gg = s.grid_grad;
         s.grid_grad = nullptr;
         rc = TrainStep(s, d_rows, d_count, n, nullptr, nullptr, d_out, d_enc, false);
         s.grid_grad = gg;

@@ -252,3 +252,51 @@ def test_guided_render_beats_cosine_sampling(gpu):
     e_plain, e_guided = float(np.median(e_plain)), float(np.median(e_guided))
     print("interior 64x36, 16 spp: median relMSE plain %.4g, guided %.4g" % (e_plain, e_guided))
     assert e_guided < e_plain
+
+
+@pytest.mark.gpu
+def test_adam_step_matches_the_oracle_and_training_is_deterministic(gpu):
+    """One Adam step (learning rate 1e-2, betas 0.9 / 0.99, eps 1e-8) on the
+    gradients az_guide_eval reports: the first step moves every parameter by
+    lr * g / (|g| + eps) (both moments bias-corrected), the MLP and bias from
+    the reported gradients, the hash grid from the encoding gradients scattered
+    to the corners of each row's cells.  Two guides with the same seed trained
+    on the same rows end with bit-identical parameters: the gradient sums do
+    not depend on the order in which the GPU's threads add them."""
+    rng = np.random.default_rng(6)
+    scene = az.generate_scene(az.SCENE_CORNELL, width=8, height=8, spp=1)
+    lr, eps = 1e-2, 1e-8
+    with az.GpuScene(scene) as g:
+        with _guide(g, seed=2) as guide:
+            info = guide.info()
+            lo, hi = _bounds(info)
+            rows = _rows(rng, 4096, lo, hi)
+            mlp0, bias0, grid0 = guide.params()
+            grads = guide.eval(rows)
+            guide.train(rows, 1)
+            mlp1, bias1, grid1 = guide.params()
+        finals = []
+        for _ in range(2):
+            with _guide(g, seed=9) as gd:
+                gd.train(rows, 3)
+                finals.append(gd.params())
+    for p0, p1, gr in ((mlp0, mlp1, grads["mlp_grad"]), (bias0, bias1, grads["bias_grad"])):
+        gr = gr.astype(np.float64)
+        want = p0.astype(np.float64) - lr * gr / (np.abs(gr) + eps)
+        assert np.abs(p1 - want).max() <= 2e-7 + 1e-6 * lr, np.abs(p1 - want).max()
+    # the grid: encoding gradients of every row scattered to its cells' corners
+    p01 = go.normalise_positions(rows[:, 0:3].astype(np.float64), info["lo"], info["inv_ext"])
+    res = go.level_res()
+    gg = np.zeros((16, 1 << 19, 2))
+    enc = grads["enc_grad"].astype(np.float64)
+    for lv in range(16):
+        idx, wts = go.corners(p01, lv, res)
+        for k in range(8):
+            np.add.at(gg[lv], idx[:, k], wts[:, k:k + 1] * enc[:, 2 * lv:2 * lv + 2])
+    touched = np.abs(gg) > 1e-5
+    step = grid1.astype(np.float64) - grid0.astype(np.float64)
+    assert touched.sum() > 1000
+    assert np.abs(step[touched] + lr * np.sign(gg[touched])).max() <= 2e-4 * lr + 1e-7
+    assert np.abs(step[np.abs(gg) == 0.0]).max() == 0.0
+    for a, b in zip(finals[0], finals[1]):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
