@@ -1,11 +1,16 @@
 """Equal-time comparison of the guided and the plain GPU renderer.
 
     python -m azimuth_b200.guiding_eval [--width 480 --height 270 --detail 49 --ref-spp 4096 --pass-spp 4]
+    python -m azimuth_b200.guiding_eval --width 1920 --height 1080 --ref-file REF.npz --ref-spp 8192 --ref-only
 
 Workload: the interior scene (three 8x4x8 rooms joined by 1x2 doorways,
 Perlin-displaced panels and clutter, ~4 M triangles at the default detail,
 one 1x1 light in room 1, camera in room 3, depth 10).  A converged reference
-is accumulated in FP64 from plain renders (`--ref-spp` samples per pixel).
+is accumulated in FP64 from plain renders (`--ref-spp` samples per pixel, in
+renders of 1024 samples per pixel); with `--ref-file` the FP64 sum and its
+sample count are kept in that file and every run adds `--ref-spp` more, so a
+reference of many thousand samples per pixel can be built over several runs
+(`--ref-only` stops after that).
 Then each renderer runs passes of `--pass-spp` samples per pixel until
 `--passes`; after every pass the running average's relMSE against the
 reference, mean over pixels and channels of (x - ref)^2 / (ref^2 + 1e-2), is
@@ -44,8 +49,17 @@ def _log(msg):
     print(msg, file=sys.stderr, flush=True)
 
 
+def _camera_with_spp(scene, spp):
+    """A copy of the scene's camera (az_camera, 396 bytes) with another sample count."""
+    import ctypes as C
+    buf = (C.c_ubyte * 396)()
+    C.memmove(buf, scene.camera_ptr, 396)
+    C.c_uint32.from_address(C.addressof(buf) + 384).value = spp   # az_camera.SampleCount
+    return buf
+
+
 def run(width=480, height=270, detail=49, ref_spp=4096, pass_spp=4, passes=64, train_passes=16, seed=0,
-        log=_log):
+        log=_log, ref_file=None, ref_only=False):
     import torch
     import azimuth_b200 as az
     t0 = time.time()
@@ -70,17 +84,36 @@ def run(width=480, height=270, detail=49, ref_spp=4096, pass_spp=4, passes=64, t
             f = film.cpu().numpy().astype(np.float64)
             return f[..., :3] / np.maximum(f[..., 3:4], 1e-30), e0.elapsed_time(e1) / 1000.0
 
-        # converged reference, FP64 accumulation of plain passes
-        ref = np.zeros((h, w, 3))
-        n_ref = max(1, ref_spp // spp)
+        # converged reference: FP64 sum of plain renders of 1024 spp (or fewer), each
+        # with its own seeds; the image is the sum over the renders' sample count
+        import ctypes as C
+        import os
+        ref_sum, ref_n, runs = np.zeros((h, w, 3)), 0, 0
+        if ref_file and os.path.exists(ref_file):
+            z = np.load(ref_file)
+            assert tuple(z["shape"]) == (h, w, 3) and int(z["detail"]) == detail and int(z["seed"]) == seed
+            ref_sum, ref_n, runs = z["sum"], int(z["spp"]), int(z["runs"])
+        per = min(1024, max(1, ref_spp))
+        cam = _camera_with_spp(scene, per)
+        per = int(int(per ** 0.5) ** 2)
         t_ref = 0.0
-        for k in range(n_ref):
-            img, dt = one(lambda: g.render_device(film.data_ptr(), seed=100000 + k, stream=stream.cuda_stream))
-            ref += img
+        for k in range(max(1, ref_spp // per)):
+            s = 100000 + 1000 * runs + k
+            img, dt = one(lambda: g.render_device(film.data_ptr(), camera_ptr=C.addressof(cam), seed=s,
+                                                  stream=stream.cuda_stream))
+            ref_sum += img * per
+            ref_n += per
             t_ref += dt
-        ref /= n_ref
-        out["reference"] = {"spp": n_ref * spp, "gpu_s": t_ref, "mean": float(ref.mean())}
-        log("reference: %d spp in %.1f s GPU" % (n_ref * spp, t_ref))
+        runs += 1
+        if ref_file:
+            np.savez(ref_file, sum=ref_sum, spp=ref_n, runs=runs, shape=np.array([h, w, 3]), detail=detail,
+                     seed=seed)
+        ref = ref_sum / ref_n
+        out["reference"] = {"spp": ref_n, "gpu_s_this_run": t_ref, "runs": runs, "mean": float(ref.mean()),
+                            "file": ref_file}
+        log("reference: %d spp (%.1f s GPU in this run)" % (ref_n, t_ref))
+        if ref_only:
+            return out
 
         curves = {}
         # plain
@@ -128,8 +161,11 @@ def main():
     ap.add_argument("--passes", type=int, default=64)
     ap.add_argument("--train-passes", type=int, default=16)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--ref-file", default=None, help="npz keeping the FP64 reference sum across runs")
+    ap.add_argument("--ref-only", action="store_true", help="only add --ref-spp samples to the reference")
     a = ap.parse_args()
-    res = run(a.width, a.height, a.detail, a.ref_spp, a.pass_spp, a.passes, a.train_passes, a.seed)
+    res = run(a.width, a.height, a.detail, a.ref_spp, a.pass_spp, a.passes, a.train_passes, a.seed,
+              ref_file=a.ref_file, ref_only=a.ref_only)
     print(json.dumps(res), flush=True)
 
 
