@@ -7,8 +7,9 @@ azimuth's; CUDA sources are compiled by nvcc for sm_100a only
 compiled without FMA contraction (``--fmad=false``: primitive tests, mesh
 ingestion, BVH quantisation and the post-process round like azimuth's scalar
 code), except the ones in ``CONTRACTED``, whose results are compared within a
-tolerance and feed no bit-exact distance: the shading stage and the path
-guide.  The result links the CUDA
+tolerance and feed no bit-exact distance: the path guide.  (The shading stage
+stays uncontracted: contraction changed the finite differences of Perlin bump
+mapping enough to move textured pixels beyond the 1e-4 parity bar.)  The result links the CUDA
 runtime statically, so the library needs only the driver and the system zlib
 at run time.
 
@@ -29,7 +30,7 @@ LIB = os.path.join(PKG, "libazimuth_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # CUDA files compiled with FMA contraction (see above)
-CONTRACTED = {"az_shade_kernel.cu", "az_guide.cu"}
+CONTRACTED = {"az_guide.cu"}
 INCLUDES = ["-I", os.path.join(REPO, "include"), "-I", os.path.join(CSRC, "host"), "-I", os.path.join(CSRC, "cuda")]
 
 

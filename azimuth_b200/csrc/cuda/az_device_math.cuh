@@ -1,11 +1,11 @@
 // Device-side float3 math with azimuth's operation order.
 //
 // The translation units whose results must round like azimuth's scalar C++
-// (src/azimuth_math.cpp:572-1348) -- primitive tests, camera rays, mesh
-// ingestion -- are compiled with --fmad=false, so a*b+c rounds twice there;
-// divisions and square roots are IEEE (-prec-div/-prec-sqrt default).  Fused
-// multiply-adds appear there only where the code asks for them explicitly
-// (box tests in the traversal).  The shading and guide units are compiled
+// (src/azimuth_math.cpp:572-1348) -- primitive tests, camera rays, shading,
+// mesh ingestion -- are compiled with --fmad=false, so a*b+c rounds twice
+// there; divisions and square roots are IEEE (-prec-div/-prec-sqrt default).
+// Fused multiply-adds appear there only where the code asks for them
+// explicitly (box tests in the traversal).  The path guide's unit is compiled
 // with contraction (azimuth_b200/build.py, CONTRACTED).
 #pragma once
 #include <cstdint>

@@ -137,6 +137,7 @@ struct __align__(16) DevLight {
     m34 inv, xf;
     float motion[3];          // the light entity's MotionVector
     uint32_t ent_index;       // dense index of the light's entity in ents[], or 0xFFFFFFFF
+    uint32_t identity;        // inv/xf are the identity and motion is zero
 };
 
 // An entity light whose visibility needs a full nearest-hit query: its entity

@@ -592,6 +592,8 @@ int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_
             memcpy(d.intensity, &E.Radiance, 12);
             d.inv = ToM34(E.InvTransformationMatrix);
             d.xf = ToM34(E.TransformationMatrix);
+            d.identity = IsIdentity(d.inv) && IsIdentity(d.xf) && d.motion[0] == 0.0f && d.motion[1] == 0.0f &&
+                         d.motion[2] == 0.0f;
             if (E.Type == AZ_Entity_Sphere) {
                 d.entity_type = azd::ENT_SPHERE;
                 memcpy(d.center, &E.Center, 12);

@@ -433,7 +433,7 @@ static __device__ int light_entity_hit(const DevScene &S, const DevLight &L, con
     f3 motion = wr.time * mk(L.motion[0], L.motion[1], L.motion[2]);
     Ray m = wr;
     m.o = wr.o - motion;
-    Ray lr = local_ray(m, L.inv);
+    Ray lr = L.identity ? local_ray_identity(wr) : local_ray(m, L.inv);
     float best = FLT_MAX;
     for (uint32_t k = 0; k < L.tri_count; k++) {
         const DevLightTri &T = S.light_tris[L.tri_offset + k];

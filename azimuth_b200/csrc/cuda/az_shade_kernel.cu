@@ -1,9 +1,8 @@
-// Shading stage of the wave (TraceRay body, src/azimuth_main.cpp:974-1130).
-//
-// This translation unit is compiled with FMA contraction: shading results
-// are compared with azimuth's within 1e-4, and nothing here feeds a primitive
-// test whose distance must be bit-exact (those run in az_render.cu, compiled
-// without contraction).
+// Shading stage of the wave (TraceRay body, src/azimuth_main.cpp:974-1130),
+// in a translation unit of its own (its 48 specialisations compile beside the
+// traversal kernels).  Like the traversal it is compiled without FMA
+// contraction, so that textures, Perlin noise and the finite differences of
+// bump mapping round like azimuth's.
 #include <cfloat>
 
 #include "az_render.h"

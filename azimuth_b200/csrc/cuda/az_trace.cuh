@@ -30,6 +30,18 @@ __device__ __forceinline__ Ray local_ray(Ray r, const m34 &m) {
     return l;
 }
 
+// GetLocalRay for a transform that is the identity with no motion: the bits
+// local_ray() gives (x * 1 + y * 0 + z * 0 + 0 is x, a -0 becoming +0; the
+// re-normalised direction), without the matrix products.  Only the sign of an
+// exactly zero direction component can differ, which changes no distance.
+__device__ __forceinline__ Ray local_ray_identity(const Ray &r) {
+    Ray l;
+    l.o = mk(r.o.x + 0.0f, r.o.y + 0.0f, r.o.z + 0.0f);
+    l.d = normalize(r.d);
+    l.time = r.time;
+    return l;
+}
+
 struct Hit {
     float t;        // azimuth's Hit.t (world)
     float tl;       // local t of the primitive test (triangle: in its mesh space)
@@ -413,6 +425,9 @@ struct Tracer {
         if (g.raw) {
             r = wr;
             if (wlim < FLT_MAX) tcur = wlim + 1e-30f;
+        } else if (g.identity) {
+            r = local_ray_identity(wr);
+            if (wlim < FLT_MAX) tcur = wlim * 1.0001f + 1e-30f;
         } else {
             Ray m = wr;
             m.o = wr.o - wr.time * mk(g.motion[0], g.motion[1], g.motion[2]);
@@ -750,6 +765,9 @@ __device__ bool trace(const DevScene &S, const Ray &wr, bool cull, float eps, fl
             if (g.raw) {
                 r = wr;
                 if (wlim < FLT_MAX) tcur = wlim + 1e-30f;
+            } else if (g.identity) {
+                r = local_ray_identity(wr);
+                if (wlim < FLT_MAX) tcur = wlim * 1.0001f + 1e-30f;
             } else {
                 Ray m = wr;
                 m.o = wr.o - wr.time * mk(g.motion[0], g.motion[1], g.motion[2]);

@@ -41,7 +41,8 @@ def per_path(scene, seed, scissor=None):
     n = k * k * rows * cols
     with az.GpuScene(scene) as g:
         buf = torch.zeros((n, 4), device="cuda", dtype=torch.float32)
-        g.render_samples(buf.data_ptr(), scissor=sc, seed=seed)
+        g.render_samples(buf.data_ptr(), scissor=az.Scissor(az.Vec2u(sc.Max.x, sc.Max.y), az.Vec2u(sc.Min.x, sc.Min.y)),
+                         seed=seed)
         torch.cuda.synchronize()
         gpu = buf.cpu().numpy()
     ref = ol.ref_samples(scene, seed=seed, scissor=sc)
