@@ -41,6 +41,7 @@ FLAG_ORDER_EXTEND = 32     # visit extension queues by origin cell and direction
 FLAG_ORDER_NONE = 64       # queues in fill order
 FLAG_SERIAL_LEVELS = 128   # visibility queries of a level before the next level's closest-hit queries
 FLAG_WATERTIGHT = 256      # triangles by the watertight test (production mode) instead of azimuth's Cramer test
+GUIDE_TCGEN05, GUIDE_MMA_SYNC = 0, 1   # az_guide_config.inference
 LAUNCH_VARIANTS = 18   # AZ_LAUNCH_VARIANTS
 
 STATUS = {0: "AZ_OK", 1: "AZ_ERR_INVALID_ARGUMENT", 2: "AZ_ERR_INVALID_SCENE", 3: "AZ_ERR_OUT_OF_MEMORY",
@@ -320,9 +321,12 @@ class Guide:
     LEVELS = 16
     TABLE = 1 << 19
 
-    def __init__(self, gpu_scene, seed=0, learning_rate=0.0, train_batch=0, record_samples=0, steps_per_wave=0):
+    def __init__(self, gpu_scene, seed=0, learning_rate=0.0, train_batch=0, record_samples=0, steps_per_wave=0,
+                 inference=0):
+        """inference: GUIDE_TCGEN05 (default) or GUIDE_MMA_SYNC, the kernel that computes the proposals."""
         self.gs = gpu_scene
         cfg = GuideConfig()
+        cfg.inference = inference
         cfg.learning_rate = learning_rate
         cfg.train_batch = train_batch
         cfg.record_samples = record_samples
@@ -377,6 +381,13 @@ class Guide:
         _check(lib().az_guide_eval(self._h, rows.ctypes.data, n, out.ctypes.data, loss.ctypes.data, mg.ctypes.data,
                                    bg.ctypes.data, eg.ctypes.data), "az_guide_eval")
         return {"outputs": out, "loss": float(loss[0]), "mlp_grad": mg, "bias_grad": bg, "enc_grad": eg}
+
+    def infer(self, rows):
+        """az_guide_infer: raw outputs (N, 64) of rows by the tcgen05 inference kernel."""
+        rows = np.ascontiguousarray(rows, np.float32)
+        out = np.zeros((rows.shape[0], 64), np.float32)
+        _check(lib().az_guide_infer(self._h, rows.ctypes.data, rows.shape[0], out.ctypes.data), "az_guide_infer")
+        return out
 
     def train(self, rows, steps):
         rows = np.ascontiguousarray(rows, np.float32)

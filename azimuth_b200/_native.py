@@ -74,7 +74,8 @@ class BatchStats(C.Structure):
 
 class GuideConfig(C.Structure):
     _fields_ = [("learning_rate", C.c_float), ("train_batch", C.c_uint32), ("record_samples", C.c_uint32),
-                ("steps_per_wave", C.c_uint32), ("seed", C.c_uint64), ("reserved", C.c_uint32 * 6)]
+                ("steps_per_wave", C.c_uint32), ("seed", C.c_uint64), ("inference", C.c_uint32),
+                ("reserved", C.c_uint32 * 5)]
 
 
 class RenderStats(C.Structure):
@@ -202,6 +203,8 @@ def _declare(L):
         L.az_guide_eval.restype = i32
         L.az_guide_train.argtypes = [vp, vp, u32, u32, vp]
         L.az_guide_train.restype = i32
+        L.az_guide_infer.argtypes = [vp, vp, u32, vp]
+        L.az_guide_infer.restype = i32
         L.az_gpu_render_noalloc.restype = i32
         L.az_gpu_closest_hit.argtypes = [vp, vp, u32, i32, C.c_float, vp, vp, vp, vp, vp]
         L.az_gpu_closest_hit.restype = i32

@@ -355,8 +355,10 @@ extern "C" int az_gpu_render_guided(az_gpu_scene *scene, az_guide *guide, az_pix
     int rc = ctx.begin(opts);
     if (rc != AZ_OK) return rc;
     std::lock_guard<std::mutex> lock(GuideLock(*g));
-    return Render(*scene->impl, film, camera, epsilons, scissor, filter_type, backface_culling, opts, ctx.stream, stats,
-                  g, train != 0);
+    rc = Render(*scene->impl, film, camera, epsilons, scissor, filter_type, backface_culling, opts, ctx.stream, stats,
+                g, train != 0);
+    if (rc == AZ_OK) rc = GuideCheck(*g, ctx.stream);
+    return rc;
 }
 
 extern "C" int az_gpu_postprocess(const az_pixel *film, uint32_t width, uint32_t height, const az_tonemap *tonemap,

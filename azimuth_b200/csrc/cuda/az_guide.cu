@@ -48,6 +48,7 @@ constexpr int kInferWarps = 8;                       // warps per block of the i
 
 // Parameters of the network as the kernels see them.
 struct GuideNetDev {
+    const __nv_bfloat16 *wtc; // tcgen05 B operands: per layer W^T (64 x 64, K-major) in 8x8 core matrices
     const uint2 *wf;          // forward B fragments [layer][kk][nn][lane]
     const uint2 *wt;          // transposed B fragments for dX = dY W^T
     const float *bias;        // output-layer bias [64]
@@ -55,6 +56,15 @@ struct GuideNetDev {
     uint32_t res[GUIDE_LEVELS];
     float lo[3], inv_ext[3];  // position normalisation onto [0, 1]^3
 };
+
+// Byte offset of element (r, k) of a 64-column K-major operand in the
+// canonical no-swizzle layout of tcgen05.mma: 8 x 8 core matrices of 128
+// contiguous bytes (8 rows of 16 bytes), the 8 core matrices of a row group
+// along K at 128-byte steps (leading byte offset), row groups at 1024-byte
+// steps (stride byte offset).
+__host__ __device__ __forceinline__ uint32_t tc_offset(uint32_t r, uint32_t k) {
+    return ((r >> 3) * 8u + (k >> 3)) * 128u + (r & 7u) * 16u + (k & 7u) * 2u;
+}
 
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
     __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
@@ -342,6 +352,220 @@ __global__ void __launch_bounds__(kInferWarps * 32) k_guide_infer(DevScene S, Wa
         }
         __syncwarp();
     }
+}
+
+// ---- the same inference on the 5th-generation tensor cores (tcgen05) ----
+// One CTA of 128 threads takes 128 rows at a time, one row per thread: the
+// thread encodes its row (hash-grid gathers, normal, outgoing direction) into
+// the shared-memory A operand; one elected thread issues, per layer, four
+// tcgen05.mma (M = 128 rows, N = 64 units, K = 16 each; BF16 operands in
+// shared memory, FP32 accumulator in tensor memory) and commits them to an
+// mbarrier; every thread then reads its row of the accumulator back from
+// tensor memory (warp w holds lanes 32w..32w+31), applies the ReLU and
+// writes the next layer's A operand, or, after the output layer, decodes its
+// proposal.  Waits on the mbarrier are bounded: on a timeout the kernel sets
+// *err, stops issuing work and frees its tensor memory.
+// ROWS: caller rows (GuideRow, normalised weights ignored) to raw outputs
+// (64 floats per row) instead of a level's queue entries to proposals.
+constexpr uint32_t kTcRows = 128;
+constexpr size_t kTcSmem = (size_t)kTcRows * W * 2 + (size_t)NW * 2 + W * sizeof(float) + 16;
+constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(W >> 3) << 17) | ((kTcRows >> 4) << 24);
+constexpr uint32_t kTcWaitLimit = 1u << 20;   // polls of an mbarrier (a layer completes in microseconds)
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Shared-memory matrix descriptor (no swizzle, K-major, sm_100 version field).
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128u >> 4) << 16) | ((uint64_t)(1024u >> 4) << 32) |
+           ((uint64_t)1 << 46);
+}
+
+__device__ __forceinline__ bool tc_wait(uint32_t mbar, uint32_t parity) {
+    for (uint32_t it = 0; it < kTcWaitLimit; it++) {
+        uint32_t done;
+        asm volatile("{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.b32 %0, 1, 0, p;\n}"
+                     : "=r"(done)
+                     : "r"(mbar), "r"(parity)
+                     : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// 16 consecutive accumulator columns of this thread's lane.
+__device__ __forceinline__ void tc_load16(uint32_t taddr, float *v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+#pragma unroll
+    for (int j = 0; j < 16; j++) v[j] = __uint_as_float(r[j]);
+}
+
+// Row `r` of the A operand from 64 floats (BF16, 8 chunks of 16 bytes).
+__device__ __forceinline__ void tc_store_row(unsigned char *A, uint32_t r, const float *x, bool relu) {
+#pragma unroll
+    for (int kc = 0; kc < 8; kc++) {
+        uint4 q;
+        uint32_t *u = reinterpret_cast<uint32_t *>(&q);
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            float a = x[8 * kc + 2 * j], b = x[8 * kc + 2 * j + 1];
+            if (relu) {
+                a = fmaxf(a, 0.0f);
+                b = fmaxf(b, 0.0f);
+            }
+            u[j] = pack_bf16(a, b);
+        }
+        *reinterpret_cast<uint4 *>(A + tc_offset(r, 8u * kc)) = q;
+    }
+}
+
+template <bool ROWS>
+__global__ void __launch_bounds__(kTcRows) k_guide_mlp_tc(DevScene S, WaveQueues Q, uint32_t level, GuideNetDev N,
+                                                          GuideLobes *out, const GuideRow *rows, uint32_t nrows,
+                                                          float *raw, uint32_t *err) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    unsigned char *A = smem;                                   // 128 x 64 BF16
+    unsigned char *B = A + kTcRows * W * 2;                    // 4 layers x 64 x 64 BF16
+    float *s_bias = reinterpret_cast<float *>(B + NW * 2);
+    uint64_t *s_mbar = reinterpret_cast<uint64_t *>(s_bias + W);
+    uint32_t *s_tmem = reinterpret_cast<uint32_t *>(s_mbar + 1);
+    const uint32_t tid = threadIdx.x, warp = tid >> 5;
+    {
+        const uint4 *src = reinterpret_cast<const uint4 *>(N.wtc);
+        uint4 *dst = reinterpret_cast<uint4 *>(B);
+        for (uint32_t i = tid; i < (uint32_t)NW * 2 / 16; i += blockDim.x) dst[i] = src[i];
+    }
+    for (uint32_t i = tid; i < (uint32_t)W; i += blockDim.x) s_bias[i] = N.bias[i];
+    const uint32_t mbar = smem_u32(s_mbar);
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(s_tmem)),
+                     "r"((uint32_t)W)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // the B operands, for the tensor cores
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *s_tmem;
+    const uint32_t lane_addr = tmem + ((32u * warp) << 16);   // this warp's 32 lanes, column 0
+    const int buf = level & 1;
+    const uint32_t n = ROWS ? nrows : min(Q.counts[level], Q.cap_q);
+    const uint32_t tiles = (n + kTcRows - 1) / kTcRows;
+    const uint32_t adesc0 = smem_u32(A), bdesc0 = smem_u32(B);
+    uint32_t phase = 0;
+    bool ok = true;
+    for (uint32_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+        const uint32_t i = tile * kTcRows + tid;
+        // ---- this thread's row of network inputs ----
+        f3 p = mk(0.0f, 0.0f, 1.0f), nr = p, wo = p;
+        if (i < n) {
+            if (ROWS) {
+                const GuideRow r = rows[i];
+                p = normalise_pos(N, mk(r.pos_w.x, r.pos_w.y, r.pos_w.z));
+                nr = mk(r.n.x, r.n.y, r.n.z);
+                wo = mk(r.wo.x, r.wo.y, r.wo.z);
+            } else {
+                const uint4 hh = Q.hit[i];
+                if (hh.w != 0xFFFFFFFFu) {
+                    const float4 o4 = Q.o[buf][i], d4 = Q.d[buf][i];
+                    Ray r;
+                    r.o = mk(o4.x, o4.y, o4.z);
+                    r.d = mk(d4.x, d4.y, d4.z);
+                    r.time = o4.w;
+                    Hit hit;
+                    hit.t = __uint_as_float(hh.x);
+                    hit.tl = __uint_as_float(hh.y);
+                    hit.prim = hh.z;
+                    hit.ent = hh.w;
+                    guide_query(S, r, hit, p, nr);
+                    p = normalise_pos(N, p);
+                    wo = -r.d;
+                }
+            }
+        }
+        float x[W];
+#pragma unroll
+        for (int l = 0; l < GUIDE_LEVELS; l++) {
+            const float2 f = grid_feature(N, l, p);
+            x[2 * l] = f.x;
+            x[2 * l + 1] = f.y;
+        }
+        x[32] = nr.x; x[33] = nr.y; x[34] = nr.z;
+        x[35] = wo.x; x[36] = wo.y; x[37] = wo.z;
+        x[38] = 1.0f;
+#pragma unroll
+        for (int j = 39; j < W; j++) x[j] = 0.0f;
+        tc_store_row(A, tid, x, false);
+        for (int l = 0; l < GUIDE_LAYERS; l++) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // A written by this thread
+            tc_fence_before();
+            __syncthreads();
+            tc_fence_after();
+            if (tid == 0) {
+                const uint32_t bl = bdesc0 + (uint32_t)l * W * W * 2;
+#pragma unroll
+                for (uint32_t ks = 0; ks < (uint32_t)W / 16; ks++) {
+                    const uint64_t ad = tc_desc(adesc0 + ks * 256u), bd = tc_desc(bl + ks * 256u);
+                    // no output lane disabled; accumulate after the first K step
+                    asm volatile(
+                        "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n}" ::"r"(tmem),
+                        "l"(ad), "l"(bd), "r"(kTcIdesc), "r"(ks), "r"(0u)
+                        : "memory");
+                }
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+                             : "memory");
+            }
+            // every thread decides alike whether the layer arrived
+            const bool got = tc_wait(mbar, phase);
+            if (__syncthreads_or(!got)) {
+                ok = false;
+                if (tid == 0 && err) atomicOr(err, 1u);
+                break;
+            }
+            phase ^= 1u;
+            tc_fence_after();
+#pragma unroll
+            for (int c = 0; c < 4; c++) tc_load16(lane_addr + 16u * c, x + 16 * c);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (l + 1 < GUIDE_LAYERS) {
+                tc_store_row(A, tid, x, true);
+            } else if (i < n) {
+#pragma unroll
+                for (int j = 0; j < W; j++) x[j] += s_bias[j];
+                if (ROWS) {
+                    for (int j = 0; j < W; j++) raw[(size_t)i * W + j] = x[j];
+                } else {
+                    GuideLobes G;
+                    decode_lobes(x, G);
+                    float4 *dst = reinterpret_cast<float4 *>(out + i);
+                    const float4 *src = reinterpret_cast<const float4 *>(&G);
+#pragma unroll
+                    for (int j = 0; j < 13; j++) dst[j] = src[j];
+                }
+            }
+        }
+    }
+    // every thread is past its last tensor-memory read (or the failed wait)
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (!ok && tid == 0) tc_wait(mbar, phase);   // let a commit still in flight land before freeing
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)W) : "memory");
 }
 
 // ---- training targets from the recorded vertices of a finished wave ----
@@ -679,6 +903,15 @@ __global__ void k_adam_grid(float2 *w, unsigned long long *gq, float2 *m, float2
 
 // BF16 B fragments of every layer from the FP32 master weights W[l][k][n]:
 // forward (k = input unit, n = output unit) and transposed (for dY W^T).
+// W^T of every layer in the tcgen05 operand layout (row n = output unit, K = input unit).
+__global__ void k_tc_weights(const float *w, __nv_bfloat16 *wtc) {
+    const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (uint32_t)NW) return;
+    const uint32_t l = idx / (W * W), n = (idx / W) % W, k = idx % W;
+    unsigned char *base = reinterpret_cast<unsigned char *>(wtc) + (size_t)l * W * W * 2;
+    *reinterpret_cast<__nv_bfloat16 *>(base + tc_offset(n, k)) = __float2bfloat16_rn(w[l * W * W + k * W + n]);
+}
+
 __global__ void k_frags(const float *w, uint2 *wf, uint2 *wt) {
     const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (uint32_t)NFRAG) return;
@@ -718,6 +951,9 @@ struct GuideState {
     float *w = nullptr, *w_grad = nullptr, *w_m = nullptr, *w_v = nullptr;
     float *bias = nullptr, *b_grad = nullptr, *b_m = nullptr, *b_v = nullptr;
     uint2 *wf = nullptr, *wt = nullptr;
+    __nv_bfloat16 *wtc = nullptr;
+    uint32_t *tc_error = nullptr;   // set by the tcgen05 kernel when a wait gives up
+    bool use_tc = true;             // proposals by the tcgen05 kernel (else the mma.sync one)
     __half2 *feat = nullptr;
     float2 *grid = nullptr, *grid_m = nullptr, *grid_v = nullptr;
     unsigned long long *grid_grad = nullptr;   // [entry][2], fixed point (k_guide_train)
@@ -788,6 +1024,7 @@ void SceneBounds(const GpuScene &G, float lo[3], float hi[3]) {
 
 int RefreshFragments(GuideState &g, cudaStream_t st) {
     k_frags<<<(NFRAG + 255) / 256, 256, 0, st>>>(g.w, g.wf, g.wt);
+    k_tc_weights<<<(NW + 255) / 256, 256, 0, st>>>(g.w, g.wtc);
     AZ_CUDA_TRY(cudaGetLastError());
     return AZ_OK;
 }
@@ -837,6 +1074,7 @@ int CreateGuide(const GpuScene &G, const az_guide_config *cfg, GuideState **out)
     g->n_rec = cfg && cfg->record_samples ? cfg->record_samples : (1u << 17);
     g->steps_per_wave = cfg && cfg->steps_per_wave ? cfg->steps_per_wave : 1u;
     g->rows_cap = cfg && cfg->train_batch ? cfg->train_batch : (1u << 18);
+    g->use_tc = !(cfg && cfg->inference == AZ_GUIDE_MMA_SYNC);
     const uint64_t seed = cfg ? cfg->seed : 0;
     g->w = g->Alloc<float>(NW);
     g->w_grad = g->Alloc<float>(NW);
@@ -848,6 +1086,8 @@ int CreateGuide(const GpuScene &G, const az_guide_config *cfg, GuideState **out)
     g->b_v = g->Alloc<float>(W);
     g->wf = g->Alloc<uint2>(NFRAG);
     g->wt = g->Alloc<uint2>(NFRAG);
+    g->wtc = g->Alloc<__nv_bfloat16>(NW);
+    g->tc_error = g->Alloc<uint32_t>(1);
     g->feat = g->Alloc<__half2>(kGridN);
     g->grid = g->Alloc<float2>(kGridN);
     g->grid_grad = g->Alloc<unsigned long long>(2 * (size_t)kGridN);
@@ -888,7 +1128,11 @@ int CreateGuide(const GpuScene &G, const az_guide_config *cfg, GuideState **out)
     if (rc != AZ_OK) return rc;
     AZ_CUDA_TRY(cudaFuncSetAttribute(k_guide_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrainSmem));
     AZ_CUDA_TRY(cudaFuncSetAttribute(k_guide_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInferSmem));
+    AZ_CUDA_TRY(cudaMemset(g->tc_error, 0, sizeof(uint32_t)));
+    AZ_CUDA_TRY(cudaFuncSetAttribute(k_guide_mlp_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
+    AZ_CUDA_TRY(cudaFuncSetAttribute(k_guide_mlp_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
     // network view
+    g->net.wtc = g->wtc;
     g->net.wf = g->wf;
     g->net.wt = g->wt;
     g->net.bias = g->bias;
@@ -941,7 +1185,11 @@ int GuidePrepareWave(GuideState &g, WaveBuffers &W, WaveQueues &Q, uint32_t cap_
 }
 
 int GuideInfer(GuideState &g, const GpuScene &G, const WaveQueues &Q, uint32_t level, cudaStream_t st) {
-    k_guide_infer<<<g.sms * 3, kInferWarps * 32, kInferSmem, st>>>(G.dev, Q, level, g.net, Q.lobes);
+    if (g.use_tc)
+        k_guide_mlp_tc<false><<<g.sms * 2, 128, kTcSmem, st>>>(G.dev, Q, level, g.net, Q.lobes, nullptr, 0, nullptr,
+                                                               g.tc_error);
+    else
+        k_guide_infer<<<g.sms * 3, kInferWarps * 32, kInferSmem, st>>>(G.dev, Q, level, g.net, Q.lobes);
     AZ_CUDA_TRY(cudaGetLastError());
     return AZ_OK;
 }
@@ -997,6 +1245,14 @@ struct az_guide {
 
 namespace az {
 GuideState *GuideOf(az_guide *g) { return g ? g->impl : nullptr; }
+int GuideCheck(GuideState &g, cudaStream_t st) {
+    uint32_t e = 0;
+    AZ_CUDA_TRY(cudaMemcpyAsync(&e, g.tc_error, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    AZ_CUDA_TRY(cudaStreamSynchronize(st));
+    if (!e) return AZ_OK;
+    AZ_CUDA_TRY(cudaMemsetAsync(g.tc_error, 0, sizeof(uint32_t), st));
+    return SetError(AZ_ERR_CUDA, "tensor-core proposals: a wait on the MMA gave up");
+}
 std::mutex &GuideLock(GuideState &g) { return g.mu; }
 }  // namespace az
 
@@ -1130,5 +1386,38 @@ extern "C" int az_guide_train(az_guide *g, const float *rows, uint32_t n, uint32
     }
     cudaFree(d_rows);
     cudaFree(d_count);
+    return rc;
+}
+
+extern "C" int az_guide_infer(az_guide *g, const float *rows, uint32_t n, float *outputs) {
+    if (!g || (n && (!rows || !outputs))) return SetError(AZ_ERR_INVALID_ARGUMENT, "null argument");
+    GuideState &s = *g->impl;
+    AZ_CUDA_TRY(cudaSetDevice(s.device));
+    if (n == 0) return AZ_OK;
+    GuideRow *d_rows = nullptr;
+    uint32_t *d_count = nullptr;
+    float *d_out = nullptr;
+    int rc = UploadRows(s, rows, n, &d_rows, &d_count);
+    if (rc == AZ_OK && cudaMalloc((void **)&d_out, (size_t)n * W * sizeof(float)) != cudaSuccess)
+        rc = SetError(AZ_ERR_OUT_OF_MEMORY, "inference outputs");
+    if (rc == AZ_OK) {
+        cudaMemset(s.tc_error, 0, sizeof(uint32_t));
+        DevScene none;
+        memset(&none, 0, sizeof(none));
+        WaveQueues q;
+        memset(&q, 0, sizeof(q));
+        k_guide_mlp_tc<true><<<std::min<uint32_t>((n + kTcRows - 1) / kTcRows, (uint32_t)s.sms * 2), kTcRows, kTcSmem>>>(
+            none, q, 0, s.net, nullptr, d_rows, n, d_out, s.tc_error);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) rc = CudaError(e, "guide inference");
+    }
+    uint32_t terr = 0;
+    if (rc == AZ_OK) cudaMemcpy(&terr, s.tc_error, sizeof(uint32_t), cudaMemcpyDeviceToHost);
+    if (rc == AZ_OK && terr) rc = SetError(AZ_ERR_CUDA, "tensor-core inference: a wait on the MMA gave up");
+    if (rc == AZ_OK) cudaMemcpy(outputs, d_out, (size_t)n * W * sizeof(float), cudaMemcpyDeviceToHost);
+    cudaFree(d_rows);
+    cudaFree(d_count);
+    if (d_out) cudaFree(d_out);
     return rc;
 }

@@ -130,6 +130,8 @@ int GuideInfer(GuideState &g, const GpuScene &G, const WaveQueues &Q, uint32_t l
 // Training targets of the finished wave and one Adam step.
 int GuideTrainWave(GuideState &g, const WaveQueues &Q, cudaStream_t st);
 GuideState *GuideOf(az_guide *g);
+// AZ_ERR_CUDA if a tensor-core wait of the proposal kernel gave up since the last check (the flag is cleared).
+int GuideCheck(GuideState &g, cudaStream_t st);
 // Serialises the renders that use one guide (its proposal and record buffers).
 std::mutex &GuideLock(GuideState &g);
 

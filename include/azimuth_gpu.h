@@ -388,8 +388,14 @@ typedef struct az_guide_config {
     uint32_t record_samples;        /* camera samples per wave whose vertices are recorded; 0 = 2^17 */
     uint32_t steps_per_wave;        /* Adam steps on each wave's rows when training; 0 = 1 */
     uint64_t seed;                  /* weight initialisation */
-    uint32_t reserved[6];
+    uint32_t inference;             /* proposal kernel: AZ_GUIDE_TCGEN05 (0, default) runs the MLP on the
+                                       5th-generation tensor cores (tcgen05.mma, operands in shared memory,
+                                       accumulator in tensor memory, 128 rows per CTA); AZ_GUIDE_MMA_SYNC
+                                       runs it warp-synchronously with mma.sync (16 rows per warp) */
+    uint32_t reserved[5];
 } az_guide_config;
+
+enum { AZ_GUIDE_TCGEN05 = 0, AZ_GUIDE_MMA_SYNC = 1 };
 
 int az_guide_create(az_gpu_scene *scene, const az_guide_config *cfg, az_guide **out);
 void az_guide_destroy(az_guide *guide);
@@ -419,6 +425,10 @@ int az_guide_eval(az_guide *guide, const float *rows, uint32_t n, float *outputs
                   float *bias_grad, float *enc_grad);
 /* `steps` Adam steps on the given rows; per-step loss (before the step) in losses. */
 int az_guide_train(az_guide *guide, const float *rows, uint32_t n, uint32_t steps, float *losses);
+/* Raw network outputs (n x 64) of caller rows (the layout of az_guide_eval)
+ * computed by the tcgen05 inference kernel that makes the render's proposals.
+ * AZ_ERR_CUDA if a tensor-core wait gave up (the kernel then stops). */
+int az_guide_infer(az_guide *guide, const float *rows, uint32_t n, float *outputs);
 
 /* Allocation-free variant of az_gpu_render; it has no counterpart in azimuth.
  *
