@@ -42,7 +42,7 @@ FLAG_ORDER_NONE = 64       # queues in fill order
 FLAG_SERIAL_LEVELS = 128   # visibility queries of a level before the next level's closest-hit queries
 FLAG_WATERTIGHT = 256      # triangles by the watertight test (production mode) instead of azimuth's Cramer test
 GUIDE_TCGEN05, GUIDE_MMA_SYNC = 0, 1   # az_guide_config.inference
-LAUNCH_VARIANTS = 18   # AZ_LAUNCH_VARIANTS
+LAUNCH_VARIANTS = 20   # AZ_LAUNCH_VARIANTS
 
 STATUS = {0: "AZ_OK", 1: "AZ_ERR_INVALID_ARGUMENT", 2: "AZ_ERR_INVALID_SCENE", 3: "AZ_ERR_OUT_OF_MEMORY",
           4: "AZ_ERR_CUDA", 5: "AZ_ERR_TIMEOUT", 6: "AZ_ERR_UNSUPPORTED", 7: "AZ_ERR_NO_DEVICE"}

@@ -189,7 +189,9 @@ __global__ void k_order_keys(DevScene S, WaveQueues Q, uint32_t level, int shado
 //                 and visit the popped group in the same step (Tracer
 //                 POP_FIRST), so lanes coming back from a pop join the
 //                 warp's node visits instead of idling through them
-enum : int { MODE_LOOP = 0, MODE_LOCKSTEP = 1, MODE_FETCH = 2, MODE_FETCHP = 3 };
+//   MODE_STAGED   MODE_FETCHP with the node fetches of each step staged
+//                 through shared memory by the whole warp (stage_nodes)
+enum : int { MODE_LOOP = 0, MODE_LOCKSTEP = 1, MODE_FETCH = 2, MODE_FETCHP = 3, MODE_STAGED = 4 };
 
 // WT: triangles by the watertight test (AZ_FLAG_WATERTIGHT) instead of azimuth's.
 // MULTI: a tile wave of several scenes (MODE_FETCHP only): each query is
@@ -243,7 +245,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_extend(DevScene S, CameraParams
         return;
     }
     uint32_t *fetch = Q.counts + AZ_COUNT_FETCH + level;
-    Tracer<Q_CLOSEST, MODE == MODE_FETCHP, WT> T;
+    constexpr bool STAGED = MODE == MODE_STAGED;
+    static_assert(!(STAGED && MULTI), "staged fetching serves one scene");
+    __shared__ uint4 s_stage[STAGED ? BLOCK / 32 * 160 : 1];
+    Tracer<Q_CLOSEST, MODE == MODE_FETCHP || STAGED, WT> T;
     uint2 stack[AZD_WSTACK];
     WarpFetch wf;
     uint32_t idx = kLaneIdle, qi = 0;   // work item and its queue entry
@@ -260,7 +265,18 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_extend(DevScene S, CameraParams
             T.init(MULTI ? Q.scenes[si] : S, r, cam.cull != 0, cam.eps_isect, FLT_MAX, stack);
         }
         if (__all_sync(0xFFFFFFFFu, idx == kLaneDone)) break;
-        if (idx < n && T.step(MULTI ? Q.scenes[si] : S, stack, err)) {
+        bool fin;
+        if (STAGED) {
+            const bool live = idx < n;
+            uint32_t node = T.kNoNode;
+            fin = live && T.begin(S, stack, err, node);
+            uint4 w[5];
+            stage_nodes(S.wnodes, node, s_stage + (threadIdx.x >> 5) * 160u, w);
+            fin = live && (fin || T.finish(S, stack, err, node, w));
+        } else {
+            fin = idx < n && T.step(MULTI ? Q.scenes[si] : S, stack, err);
+        }
+        if (fin) {
             const Hit &h = T.best;
             Q.hit[qi] = make_uint4(__float_as_uint(h.t), __float_as_uint(h.tl), h.prim, h.ent);
             T.flush_counts(cnt);
@@ -368,7 +384,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_shadow(DevScene S, CameraParams
         return;
     }
     uint32_t *fetch = Q.counts + AZ_COUNT_FETCH + AZ_MAX_LEVELS + level;
-    Tracer<Q_ANY, MODE == MODE_FETCHP, WT> T;
+    constexpr bool STAGED = MODE == MODE_STAGED;
+    static_assert(!(STAGED && MULTI), "staged fetching serves one scene");
+    __shared__ uint4 s_stage[STAGED ? BLOCK / 32 * 160 : 1];
+    Tracer<Q_ANY, MODE == MODE_FETCHP || STAGED, WT> T;
     uint2 stack[AZD_WSTACK];
     WarpFetch wf;
     uint32_t idx = kLaneIdle;
@@ -399,7 +418,18 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_shadow(DevScene S, CameraParams
             }
         }
         if (__all_sync(0xFFFFFFFFu, idx == kLaneDone)) break;
-        if (idx < n && T.step(MULTI ? Q.scenes[si] : S, stack, err)) {
+        bool fin;
+        if (STAGED) {
+            const bool live = idx < n;
+            uint32_t node = T.kNoNode;
+            fin = live && T.begin(S, stack, err, node);
+            uint4 w[5];
+            stage_nodes(S.wnodes, node, s_stage + (threadIdx.x >> 5) * 160u, w);
+            fin = live && (fin || T.finish(S, stack, err, node, w));
+        } else {
+            fin = idx < n && T.step(MULTI ? Q.scenes[si] : S, stack, err);
+        }
+        if (fin) {
             if (!T.hit_any) add_accum(Q.accum, __float_as_uint(c.w), mk(c.x, c.y, c.z));
             T.flush_counts(cnt);
             idx = kLaneIdle;
@@ -469,7 +499,8 @@ constexpr Variant kVariants[] = {{128, 1, MODE_LOOP},     {128, 6, MODE_LOOP},  
                                  {64, 12, MODE_LOOP},     {128, 8, MODE_FETCH},    {128, 6, MODE_FETCH},
                                  {256, 3, MODE_FETCH},    {128, 8, MODE_LOCKSTEP}, {128, 6, MODE_LOCKSTEP},
                                  {256, 3, MODE_LOCKSTEP}, {64, 12, MODE_LOCKSTEP}, {128, 7, MODE_FETCH},
-                                 {128, 6, MODE_FETCHP},   {128, 7, MODE_FETCHP},   {128, 8, MODE_FETCHP}};
+                                 {128, 6, MODE_FETCHP},   {128, 7, MODE_FETCHP},   {128, 8, MODE_FETCHP},
+                                 {128, 6, MODE_STAGED},   {128, 8, MODE_STAGED}};
 constexpr uint32_t kVariantCount = sizeof(kVariants) / sizeof(kVariants[0]);
 static_assert(kVariantCount == AZ_LAUNCH_VARIANTS, "variant table and header disagree");
 
@@ -523,6 +554,8 @@ void LaunchTraversalVariant(uint32_t v, bool shadow, int sms, const DevScene &S,
         case 15: LaunchTraversal<128, 6, MODE_FETCHP>(shadow, sms, S, cam, Q, L, st); break;
         case 16: LaunchTraversal<128, 7, MODE_FETCHP>(shadow, sms, S, cam, Q, L, st); break;
         case 17: LaunchTraversal<128, 8, MODE_FETCHP>(shadow, sms, S, cam, Q, L, st); break;
+        case 18: LaunchTraversal<128, 6, MODE_STAGED>(shadow, sms, S, cam, Q, L, st); break;
+        case 19: LaunchTraversal<128, 8, MODE_STAGED>(shadow, sms, S, cam, Q, L, st); break;
         default: LaunchTraversal<128, 8, MODE_LOOP>(shadow, sms, S, cam, Q, L, st); break;
     }
 }

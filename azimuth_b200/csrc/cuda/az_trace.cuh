@@ -353,6 +353,7 @@ __device__ bool trace(const DevScene &S, const Ray &wr, bool cull, float eps, fl
 // WT: triangles by the watertight test instead of azimuth's Cramer test.
 template <QueryKind KIND, bool POP_FIRST = false, bool WT = false>
 struct Tracer {
+    static constexpr uint32_t kNoNode = 0xFFFFFFFFu;
     Ray wr;                    // world ray
     Ray r;                     // ray in the current space (world or a group's local space)
     f3 inv;
@@ -488,6 +489,24 @@ struct Tracer {
     // Returns true when finished.  The stack (AZD_WSTACK entries) is a
     // separate array of the caller so that the state above stays in registers.
     __device__ __forceinline__ bool step(const DevScene &S, uint2 *stack, uint32_t *err) {
+        uint32_t node;
+        if (begin(S, stack, err, node)) return true;
+        uint4 w[5];
+        if (node != kNoNode) {
+            const uint4 *np = reinterpret_cast<const uint4 *>(S.wnodes + node);
+#pragma unroll
+            for (int k = 0; k < 5; k++) w[k] = __ldg(np + k);
+        }
+        return finish(S, stack, err, node, w);
+    }
+
+    // The first half of a step: the step count, the pops of a pop-first
+    // tracer, and the choice of the node to visit (`node`, kNoNode when the
+    // step visits none).  Returns true when the query is finished.  A caller
+    // that fetches the node itself (stage_nodes) runs begin, the fetch, then
+    // finish.
+    __device__ __forceinline__ bool begin(const DevScene &S, uint2 *stack, uint32_t *err, uint32_t &node) {
+        node = kNoNode;
         if (++steps > AZD_MAX_STEPS) {
             if (err) atomicOr(err, 1u);
             return true;
@@ -502,19 +521,26 @@ struct Tracer {
             const uint32_t hits = ng_bits & 0xFFu, imask = (ng_bits >> 8) & 0xFFu;
             const uint32_t key = __ffs(hits) - 1u;
             const uint32_t slot = key ^ oct;
-            const uint32_t node = ng_base + __popc(imask & ((1u << slot) - 1u));
+            node = ng_base + __popc(imask & ((1u << slot) - 1u));
             ng_bits &= ~(1u << key);
             if (ng_bits & 0xFFu) push(stack, ng_base, ng_bits, err);
-            const uint4 *np = reinterpret_cast<const uint4 *>(S.wnodes + node);
-            const uint4 w0 = __ldg(np + 0), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3),
-                        w4 = __ldg(np + 4);
+        }
+        return false;
+    }
+
+    // The second half: the eight child tests of `node` (w: its five 16-byte
+    // words), the primitives, and the pop of exhausted groups.  Returns true
+    // when the query is finished.
+    __device__ __forceinline__ bool finish(const DevScene &S, uint2 *stack, uint32_t *err, uint32_t node,
+                                           const uint4 (&w)[5]) {
+        if (node != kNoNode) {
             nodes_visited++;
-            const WideHits h = wide_test(w0, w1, w2, w3, w4, r.o, inv, oct, tcur);
-            ng_base = w1.x;
-            ng_bits = h.inner | ((w0.w >> 24) << 8);
+            const WideHits h = wide_test(w[0], w[1], w[2], w[3], w[4], r.o, inv, oct, tcur);
+            ng_base = w[1].x;
+            ng_bits = h.inner | ((w[0].w >> 24) << 8);
             if (h.prims) {
                 if (pg_mask) push(stack, pg_base, AZD_E_PRIMS | pg_mask, err);   // keep the older group for later
-                pg_base = w1.y;
+                pg_base = w[1].y;
                 pg_mask = h.prims;
             }
         }
@@ -594,6 +620,34 @@ struct Tracer {
         }
     }
 };
+
+// Node fetch staged through shared memory, called by all 32 lanes of a warp
+// between Tracer::begin and Tracer::finish.  The nodes that the lanes visit
+// this step (node: kNoNode for none) are loaded together: 16-byte word c of
+// the warp's list (word c % 5 of lane c / 5's node) is read by lane c % 32 in
+// round c / 32, so five neighbouring lanes read one node's 80 contiguous bytes
+// instead of every lane reading 16 bytes of its own node per instruction;
+// each lane then takes its node's five words from `stage` (the warp's 160
+// words of shared memory).
+__device__ __forceinline__ void stage_nodes(const WideNode *nodes, uint32_t node, uint4 *stage, uint4 (&w)[5]) {
+    constexpr uint32_t kNone = 0xFFFFFFFFu;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t want = __ballot_sync(0xFFFFFFFFu, node != kNone);
+    if (!want) return;
+    const uint4 *base = reinterpret_cast<const uint4 *>(nodes);
+#pragma unroll
+    for (uint32_t it = 0; it < 5; it++) {
+        const uint32_t c = 32u * it + lane, j = c / 5u, part = c - 5u * j;
+        const uint32_t nj = __shfl_sync(0xFFFFFFFFu, node, j);
+        if ((want >> j) & 1u) stage[c] = __ldg(base + (size_t)nj * 5u + part);
+    }
+    __syncwarp();
+    if (node != kNone) {
+#pragma unroll
+        for (int k = 0; k < 5; k++) w[k] = stage[5u * lane + k];
+    }
+    __syncwarp();   // the stage is free for the next step
+}
 
 // A whole query in one loop: the same traversal as Tracer written as a single
 // function, which the compiler schedules better when one thread runs one

@@ -66,7 +66,7 @@ enum {
 };
 
 /* Number of traversal launch configurations (az_render_opts.variant). */
-#define AZ_LAUNCH_VARIANTS 18
+#define AZ_LAUNCH_VARIANTS 20
 
 typedef struct az_render_opts {
     uint64_t seed;                  /* counter-RNG key */
@@ -84,7 +84,8 @@ typedef struct az_render_opts {
     uint32_t variant;               /* traversal launch configuration 1..AZ_LAUNCH_VARIANTS (threads per
                                        block, register cap, how queries map to threads: one per thread
                                        to its end, warp lockstep per traversal step, or persistent
-                                       fetching); 0 = the scene's choice: 8 (128 threads, at most 64
+                                       fetching, with node fetches staged through shared memory in
+                                       variants 19 and 20); 0 = the scene's choice: 8 (128 threads, at most 64
                                        registers, persistent fetching) until az_gpu_autotune picks another */
     uint32_t bvh_leaf;              /* az_gpu_scene_create: triangles per bottom-level leaf at most, 1..3 (0 = 2) */
     uint32_t bvh_builder;           /* az_gpu_scene_create: binary hierarchy before the wide collapse,
