@@ -15,7 +15,10 @@ completion-time p50 / p99 (jobs shortest first on `--streams` streams), the
 same batch largest first and on one stream for comparison, and the batch with
 its plain jobs in multi-scene tile waves (one persistent chain of launches
 pulling 4096-sample tiles of every plain job from a device work queue) while
-the other streams take the guided jobs.
+the other streams take the guided jobs.  After the tile-wave batch, eight of
+its plain jobs are rendered again one at a time (a batch of one job) and the
+relMSE of each tile-wave film against that film is reported: the tile waves
+trace the same samples, so the images agree to float summation order.
 """
 import argparse
 import json
@@ -97,6 +100,18 @@ def run(n_jobs=256, streams=8, seed=0, log=lambda m: print(m, file=sys.stderr, f
                       "mpaths_per_s": st["samples"] / (st["gpu_ms"] / 1000.0) / 1e6,
                       "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "failed": st["failed"],
                       "guided_p50_ms": float(np.median(done[1::2])), "plain_p50_ms": float(np.median(done[0::2]))}
+        if tiles:
+            check = [k for k, s in enumerate(specs) if not s["guided"]][:8]
+            snap = {k: films[k].clone() for k in check}
+            worst = 0.0
+            for k in check:
+                films[k].zero_()
+                az.render_batch([jobs[k]], streams=1)
+                torch.cuda.synchronize()
+                a = snap[k][..., :3] / snap[k][..., 3:].clamp_min(1e-30)
+                b = films[k][..., :3] / films[k][..., 3:].clamp_min(1e-30)
+                worst = max(worst, float(((a - b) ** 2 / (b ** 2 + 1e-2)).mean()))
+            out[label]["equal_image_check"] = {"jobs": len(check), "max_relmse_vs_own_render": worst}
         log("%s: %s" % (label, json.dumps(out[label])))
     for gd in guides:
         gd.close()

@@ -975,6 +975,7 @@ struct GuideState {
     float last_loss = 0.0f;
     std::vector<void *> allocs;
     int sms = 148;
+    int tc_blocks = 2;              // resident CTAs per SM of the tcgen05 inference kernel
     std::mutex mu;
 
     ~GuideState() {
@@ -1131,6 +1132,11 @@ int CreateGuide(const GpuScene &G, const az_guide_config *cfg, GuideState **out)
     AZ_CUDA_TRY(cudaMemset(g->tc_error, 0, sizeof(uint32_t)));
     AZ_CUDA_TRY(cudaFuncSetAttribute(k_guide_mlp_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
     AZ_CUDA_TRY(cudaFuncSetAttribute(k_guide_mlp_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
+    // as many resident CTAs per SM as shared memory allows, at most 4: each
+    // holds 64 of the SM's 512 tensor-memory columns while it runs
+    int per_sm = 0;
+    AZ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_guide_mlp_tc<false>, (int)kTcRows, kTcSmem));
+    g->tc_blocks = std::max(1, std::min(per_sm, 4));
     // network view
     g->net.wtc = g->wtc;
     g->net.wf = g->wf;
@@ -1186,8 +1192,8 @@ int GuidePrepareWave(GuideState &g, WaveBuffers &W, WaveQueues &Q, uint32_t cap_
 
 int GuideInfer(GuideState &g, const GpuScene &G, const WaveQueues &Q, uint32_t level, cudaStream_t st) {
     if (g.use_tc)
-        k_guide_mlp_tc<false><<<g.sms * 2, 128, kTcSmem, st>>>(G.dev, Q, level, g.net, Q.lobes, nullptr, 0, nullptr,
-                                                               g.tc_error);
+        k_guide_mlp_tc<false><<<g.sms * g.tc_blocks, kTcRows, kTcSmem, st>>>(G.dev, Q, level, g.net, Q.lobes,
+                                                                             nullptr, 0, nullptr, g.tc_error);
     else
         k_guide_infer<<<g.sms * 3, kInferWarps * 32, kInferSmem, st>>>(G.dev, Q, level, g.net, Q.lobes);
     AZ_CUDA_TRY(cudaGetLastError());
@@ -1406,7 +1412,8 @@ extern "C" int az_guide_infer(az_guide *g, const float *rows, uint32_t n, float 
         memset(&none, 0, sizeof(none));
         WaveQueues q;
         memset(&q, 0, sizeof(q));
-        k_guide_mlp_tc<true><<<std::min<uint32_t>((n + kTcRows - 1) / kTcRows, (uint32_t)s.sms * 2), kTcRows, kTcSmem>>>(
+        k_guide_mlp_tc<true><<<std::min<uint32_t>((n + kTcRows - 1) / kTcRows, (uint32_t)(s.sms * s.tc_blocks)),
+                               kTcRows, kTcSmem>>>(
             none, q, 0, s.net, nullptr, d_rows, n, d_out, s.tc_error);
         cudaError_t e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaDeviceSynchronize();

@@ -2,6 +2,7 @@
 
     python -m azimuth_b200.guiding_eval [--width 480 --height 270 --detail 49 --ref-spp 4096 --pass-spp 4]
     python -m azimuth_b200.guiding_eval --width 1920 --height 1080 --ref-file REF.npz --ref-spp 8192 --ref-only
+    python -m azimuth_b200.guiding_eval --width 1920 --height 1080 --ref-file REF.npz --ref-spp 0 --runs 5
 
 Workload: the interior scene (three 8x4x8 rooms joined by 1x2 doorways,
 Perlin-displaced panels and clutter, ~4 M triangles at the default detail,
@@ -19,6 +20,10 @@ recording and training included).  The guided renderer trains during the
 first `--train-passes` passes and keeps every pass in its average (all are
 unbiased).  Reported: both curves and the time the guided renderer needs to
 reach the plain renderer's final relMSE, as a fraction of the plain time.
+With `--runs R` the comparison is repeated R times against the same
+reference, run r drawing its passes' random numbers and the guide's initial
+weights from seeds of its own (`--ref-spp 0` with `--ref-file` adds no
+reference samples).
 """
 import argparse
 import json
@@ -59,7 +64,7 @@ def _camera_with_spp(scene, spp):
 
 
 def run(width=480, height=270, detail=49, ref_spp=4096, pass_spp=4, passes=64, train_passes=16, seed=0,
-        log=_log, ref_file=None, ref_only=False):
+        log=_log, ref_file=None, ref_only=False, runs=1):
     import torch
     import azimuth_b200 as az
     t0 = time.time()
@@ -97,15 +102,16 @@ def run(width=480, height=270, detail=49, ref_spp=4096, pass_spp=4, passes=64, t
         cam = _camera_with_spp(scene, per)
         per = int(int(per ** 0.5) ** 2)
         t_ref = 0.0
-        for k in range(max(1, ref_spp // per)):
+        assert ref_spp > 0 or ref_n > 0, "--ref-spp 0 needs a reference file with samples"
+        for k in range(ref_spp // per if ref_spp > 0 else 0):
             s = 100000 + 1000 * runs + k
             img, dt = one(lambda: g.render_device(film.data_ptr(), camera_ptr=C.addressof(cam), seed=s,
                                                   stream=stream.cuda_stream))
             ref_sum += img * per
             ref_n += per
             t_ref += dt
-        runs += 1
-        if ref_file:
+        runs += 1 if ref_spp > 0 else 0
+        if ref_file and ref_spp > 0:
             np.savez(ref_file, sum=ref_sum, spp=ref_n, runs=runs, shape=np.array([h, w, 3]), detail=detail,
                      seed=seed)
         ref = ref_sum / ref_n
@@ -115,39 +121,51 @@ def run(width=480, height=270, detail=49, ref_spp=4096, pass_spp=4, passes=64, t
         if ref_only:
             return out
 
-        curves = {}
-        # plain
-        acc = np.zeros_like(ref)
-        t, curve = 0.0, []
-        for k in range(passes):
-            img, dt = one(lambda: g.render_device(film.data_ptr(), seed=k, stream=stream.cuda_stream))
-            acc += img
-            t += dt
-            curve.append((t, _relmse(acc / (k + 1), ref)))
-        curves["plain"] = curve
-        # guided (trains during the first passes)
-        with az.Guide(g, seed=seed) as guide:
+        results = []
+        for rn in range(runs):
+            base = 7919 * rn   # run rn's pass seeds (run 0: passes 0, 1, ...)
+            curves = {}
+            # plain
             acc = np.zeros_like(ref)
             t, curve = 0.0, []
             for k in range(passes):
-                tr = k < train_passes
-                img, dt = one(lambda: guide.render(film.data_ptr(), train=tr, seed=k, stream=stream.cuda_stream,
-                                                   stats=False))
+                img, dt = one(lambda: g.render_device(film.data_ptr(), seed=base + k, stream=stream.cuda_stream))
                 acc += img
                 t += dt
                 curve.append((t, _relmse(acc / (k + 1), ref)))
-            curves["guided"] = curve
-            out["guide_steps"] = guide.info()["steps"]
-    target = curves["plain"][-1][1]
-    t_plain = curves["plain"][-1][0]
-    t_guided = _time_to(curves["guided"], target)
-    out["plain"] = {"gpu_s": t_plain, "relmse": target, "s_per_pass": t_plain / passes}
-    out["guided"] = {"gpu_s": curves["guided"][-1][0], "relmse": curves["guided"][-1][1],
-                     "s_per_pass": curves["guided"][-1][0] / passes,
-                     "time_to_plain_relmse_s": t_guided}
-    out["time_ratio_at_equal_relmse"] = (t_guided / t_plain) if t_guided is not None else None
-    out["relmse_ratio_at_equal_passes"] = curves["guided"][-1][1] / target
-    out["curves"] = {k: [[round(a, 5), b] for a, b in v] for k, v in curves.items()}
+            curves["plain"] = curve
+            # guided (trains during the first passes)
+            res = {"run": rn}
+            with az.Guide(g, seed=seed + rn) as guide:
+                acc = np.zeros_like(ref)
+                t, curve = 0.0, []
+                for k in range(passes):
+                    tr = k < train_passes
+                    img, dt = one(lambda: guide.render(film.data_ptr(), train=tr, seed=base + k,
+                                                       stream=stream.cuda_stream, stats=False))
+                    acc += img
+                    t += dt
+                    curve.append((t, _relmse(acc / (k + 1), ref)))
+                curves["guided"] = curve
+                res["guide_steps"] = guide.info()["steps"]
+            target = curves["plain"][-1][1]
+            t_plain = curves["plain"][-1][0]
+            t_guided = _time_to(curves["guided"], target)
+            res["plain"] = {"gpu_s": t_plain, "relmse": target, "s_per_pass": t_plain / passes}
+            res["guided"] = {"gpu_s": curves["guided"][-1][0], "relmse": curves["guided"][-1][1],
+                             "s_per_pass": curves["guided"][-1][0] / passes,
+                             "time_to_plain_relmse_s": t_guided}
+            res["time_ratio_at_equal_relmse"] = (t_guided / t_plain) if t_guided is not None else None
+            res["relmse_ratio_at_equal_passes"] = curves["guided"][-1][1] / target
+            res["curves"] = {k: [[round(a, 5), b] for a, b in v] for k, v in curves.items()}
+            log("run %d: time ratio %s, relMSE plain %.5g guided %.5g" % (
+                rn, res["time_ratio_at_equal_relmse"], target, res["guided"]["relmse"]))
+            results.append(res)
+    if runs == 1:
+        out.update(results[0])
+    else:
+        out["runs"] = results
+        out["time_ratios"] = [r["time_ratio_at_equal_relmse"] for r in results]
     return out
 
 
@@ -163,9 +181,10 @@ def main():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--ref-file", default=None, help="npz keeping the FP64 reference sum across runs")
     ap.add_argument("--ref-only", action="store_true", help="only add --ref-spp samples to the reference")
+    ap.add_argument("--runs", type=int, default=1, help="comparisons against the same reference")
     a = ap.parse_args()
     res = run(a.width, a.height, a.detail, a.ref_spp, a.pass_spp, a.passes, a.train_passes, a.seed,
-              ref_file=a.ref_file, ref_only=a.ref_only)
+              ref_file=a.ref_file, ref_only=a.ref_only, runs=a.runs)
     print(json.dumps(res), flush=True)
 
 

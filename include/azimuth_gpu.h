@@ -443,8 +443,7 @@ int az_guide_infer(az_guide *guide, const float *rows, uint32_t n, float *output
  * this library holds until the process exits, which caps a wave at 16384
  * camera samples: opts->chunk_samples above 16384 is rejected with
  * AZ_ERR_INVALID_ARGUMENT.  The first call on a device looks up the array's
- * device address (cudaGetSymbolAddress), so make that first call before any
- * stream capture begins.  All calls share the array and it keeps the last
+ * device address (cudaGetSymbolAddress).  All calls share the array and it keeps the last
  * call's contents (the counters are cleared at the start of every wave):
  * calls that overlap on the GPU (other threads or streams) race and must be
  * serialised by the caller.  A wave whose queues overflow the array is run
