@@ -41,7 +41,7 @@ FLAG_ORDER_EXTEND = 32     # visit extension queues by origin cell and direction
 FLAG_ORDER_NONE = 64       # queues in fill order
 FLAG_SERIAL_LEVELS = 128   # visibility queries of a level before the next level's closest-hit queries
 FLAG_WATERTIGHT = 256      # triangles by the watertight test (production mode) instead of azimuth's Cramer test
-GUIDE_TCGEN05, GUIDE_MMA_SYNC = 0, 1   # az_guide_config.inference
+GUIDE_TCGEN05, GUIDE_MMA_SYNC = 0, 1   # az_guide_config.kernels
 LAUNCH_VARIANTS = 20   # AZ_LAUNCH_VARIANTS
 
 STATUS = {0: "AZ_OK", 1: "AZ_ERR_INVALID_ARGUMENT", 2: "AZ_ERR_INVALID_SCENE", 3: "AZ_ERR_OUT_OF_MEMORY",
@@ -322,11 +322,11 @@ class Guide:
     TABLE = 1 << 19
 
     def __init__(self, gpu_scene, seed=0, learning_rate=0.0, train_batch=0, record_samples=0, steps_per_wave=0,
-                 inference=0):
-        """inference: GUIDE_TCGEN05 (default) or GUIDE_MMA_SYNC, the kernel that computes the proposals."""
+                 kernels=0):
+        """kernels: GUIDE_TCGEN05 (default) or GUIDE_MMA_SYNC, the network kernels (proposals and training)."""
         self.gs = gpu_scene
         cfg = GuideConfig()
-        cfg.inference = inference
+        cfg.kernels = kernels
         cfg.learning_rate = learning_rate
         cfg.train_batch = train_batch
         cfg.record_samples = record_samples

@@ -48,7 +48,8 @@ constexpr int kInferWarps = 8;                       // warps per block of the i
 
 // Parameters of the network as the kernels see them.
 struct GuideNetDev {
-    const __nv_bfloat16 *wtc; // tcgen05 B operands: per layer W^T (64 x 64, K-major) in 8x8 core matrices
+    const __nv_bfloat16 *wtc; // tcgen05 B operands, 64 x 64 K-major in 8x8 core matrices: per layer W^T
+                              // (forward), then per layer W (dX of the backward pass)
     const uint2 *wf;          // forward B fragments [layer][kk][nn][lane]
     const uint2 *wt;          // transposed B fragments for dX = dY W^T
     const float *bias;        // output-layer bias [64]
@@ -374,10 +375,28 @@ constexpr uint32_t kTcWaitLimit = 1u << 20;   // polls of an mbarrier (a layer c
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-// Shared-memory matrix descriptor (no swizzle, K-major, sm_100 version field).
-__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr) {
-    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128u >> 4) << 16) | ((uint64_t)(1024u >> 4) << 32) |
+// Shared-memory matrix descriptor (no swizzle, K-major, sm_100 version
+// field): core matrices along K 128 bytes apart, row groups `sbo` bytes apart
+// (1024 for a 64-wide K, 2048 for the 128-wide K of the transposed operands).
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr, uint32_t sbo = 1024u) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128u >> 4) << 16) | ((uint64_t)(sbo >> 4) << 32) |
            ((uint64_t)1 << 46);
+}
+
+// One tcgen05.mma (M = 128, N = 64, K = 16, BF16 in, FP32 accumulator at
+// tensor-memory address d): D = A B^T, plus D when `accumulate`; no output
+// lane disabled.  Issued by one thread.
+__device__ __forceinline__ void tc_mma(uint32_t d, uint64_t a, uint64_t b, uint32_t accumulate) {
+    asm volatile(
+        "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n}" ::"r"(d),
+        "l"(a), "l"(b), "r"(kTcIdesc), "r"(accumulate), "r"(0u)
+        : "memory");
+}
+
+// Arrives on the mbarrier once every tcgen05.mma issued so far has completed.
+__device__ __forceinline__ void tc_commit(uint32_t mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar) : "memory");
 }
 
 __device__ __forceinline__ bool tc_wait(uint32_t mbar, uint32_t parity) {
@@ -516,17 +535,9 @@ __global__ void __launch_bounds__(kTcRows) k_guide_mlp_tc(DevScene S, WaveQueues
             if (tid == 0) {
                 const uint32_t bl = bdesc0 + (uint32_t)l * W * W * 2;
 #pragma unroll
-                for (uint32_t ks = 0; ks < (uint32_t)W / 16; ks++) {
-                    const uint64_t ad = tc_desc(adesc0 + ks * 256u), bd = tc_desc(bl + ks * 256u);
-                    // no output lane disabled; accumulate after the first K step
-                    asm volatile(
-                        "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
-                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n}" ::"r"(tmem),
-                        "l"(ad), "l"(bd), "r"(kTcIdesc), "r"(ks), "r"(0u)
-                        : "memory");
-                }
-                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
-                             : "memory");
+                for (uint32_t ks = 0; ks < (uint32_t)W / 16; ks++)   // accumulate after the first K step
+                    tc_mma(tmem, tc_desc(adesc0 + ks * 256u), tc_desc(bl + ks * 256u), ks);
+                tc_commit(mbar);
             }
             // every thread decides alike whether the layer arrived
             const bool got = tc_wait(mbar, phase);
@@ -851,6 +862,268 @@ __global__ void __launch_bounds__(kWarps * 32) k_guide_train(GuideNetDev N, Trai
     }
 }
 
+// ---- the same training step on the 5th-generation tensor cores (tcgen05) ----
+// One CTA of 128 threads per SM takes 128 rows at a time, one row per thread,
+// and keeps the whole step's tensor work on tcgen05.mma (M = 128, N = 64,
+// K = 16 per instruction, BF16 operands in shared memory, FP32 accumulators in
+// tensor memory):
+//   forward   X_{l+1} = ReLU(X_l W_l), Y = X_3 W_3 + b  (A = X_l, 64-wide K)
+//   backward  dX_l = dY_l W_l^T                          (A = dY_l, 64-wide K)
+//             dW_l += X_l^T dY_l                         (K = the tile's 128 rows)
+// The dW products need the rows as K: every thread also writes its row of X_l
+// and dY_l into transposed operands (element (unit u, row r) at
+// tc_offset_t(u, r)).  Their M is the 64 input units; the instruction's other
+// 64 rows read the next 16 KB of shared memory and land in tensor-memory
+// lanes 64..127, which are never read.  dW_l accumulates in its own 64
+// tensor-memory columns over all the CTA's tiles in tile order, so the sums
+// do not depend on timing; after the last tile warps 0 and 1 (lanes 0..63)
+// write them to the CTA's slot of `part`, which k_guide_reduce adds up in
+// block order like the mma.sync kernel's.  Output-bias gradients and the loss
+// are summed in fixed order through shared memory; the hash-grid gradient is
+// scattered in fixed point as in k_guide_train.  Waits on the mbarrier are
+// bounded: on a timeout *err is set and the CTA stops (its slot then holds
+// what it had).
+__host__ __device__ __forceinline__ uint32_t tc_offset_t(uint32_t u, uint32_t r) {
+    return ((u >> 3) * 16u + (r >> 3)) * 128u + (u & 7u) * 16u + (r & 7u) * 2u;
+}
+
+constexpr uint32_t kTcOp = kTcRows * W * 2;             // bytes of one 128 x 64 BF16 operand
+constexpr uint32_t kTcTrainCols = 512;                  // tensor memory: scratch + 4 dW accumulators (320 used)
+// shared memory: X (A layout), X_l^T for l = 0..3, dY (A layout), dY^T, W^T
+// and W per layer (B operands of the forward and of dX), dY in FP32 for the
+// bias gradient, bias, bias gradient, loss, mbarrier, tensor-memory address
+constexpr size_t kTcTrainSmem = (size_t)kTcOp * 7 + (size_t)NW * 2 * 2 + (size_t)kTcRows * W * sizeof(float) +
+                                2 * W * sizeof(float) + kTcRows / 32 * sizeof(float) + 16;
+
+// this thread's row of a transposed operand (u = 0..63 at row r), as BF16
+__device__ __forceinline__ void tc_store_col(unsigned char *T, uint32_t r, const float *x) {
+#pragma unroll
+    for (int u = 0; u < W; u++)
+        *reinterpret_cast<__nv_bfloat16 *>(T + tc_offset_t((uint32_t)u, r)) = __float2bfloat16_rn(x[u]);
+}
+
+__global__ void __launch_bounds__(kTcRows, 1) k_guide_train_tc(GuideNetDev N, TrainArgs A, uint32_t *err) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    unsigned char *XA = smem;                      // X_l, rows (A operand of the forward)
+    unsigned char *XT = XA + kTcOp;                // X_l^T, l = 0..3
+    unsigned char *DYA = XT + 4 * kTcOp;           // dY_l, rows (A operand of dX)
+    unsigned char *DYT = DYA + kTcOp;              // dY_l^T (B operand of dW)
+    unsigned char *WF = DYT + kTcOp;               // per layer W^T: row = output unit (forward)
+    unsigned char *WB = WF + NW * 2;               // per layer W: row = input unit (dX)
+    float *s_o = reinterpret_cast<float *>(WB + NW * 2);   // [128][64] dY in FP32
+    float *s_bias = s_o + kTcRows * W;
+    float *s_db = s_bias + W;
+    float *s_loss = s_db + W;
+    uint64_t *s_mbar = reinterpret_cast<uint64_t *>(s_loss + kTcRows / 32);
+    uint32_t *s_tmem = reinterpret_cast<uint32_t *>(s_mbar + 1);
+    const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
+    {
+        const uint4 *src = reinterpret_cast<const uint4 *>(N.wtc);
+        uint4 *dst = reinterpret_cast<uint4 *>(WF);
+        for (uint32_t i = tid; i < (uint32_t)NW * 2 * 2 / 16; i += blockDim.x) dst[i] = src[i];
+    }
+    for (uint32_t i = tid; i < (uint32_t)W; i += blockDim.x) {
+        s_bias[i] = N.bias[i];
+        s_db[i] = 0.0f;
+    }
+    const uint32_t mbar = smem_u32(s_mbar);
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(s_tmem)),
+                     "r"(kTcTrainCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *s_tmem;
+    const uint32_t lane_addr = (32u * warp) << 16;
+    const uint32_t sXA = smem_u32(XA), sXT = smem_u32(XT), sDYA = smem_u32(DYA), sDYT = smem_u32(DYT),
+                   sWF = smem_u32(WF), sWB = smem_u32(WB);
+    const uint32_t n = min(*A.count, A.cap);
+    const float wscale = A.wsum ? (float)n / fmaxf(*A.wsum, 1e-30f) : 1.0f;
+    const float wcap = A.wsum && A.wcap > 0.0f ? A.wcap : FLT_MAX;
+    const uint32_t tiles = (n + kTcRows - 1) / kTcRows;
+    float loss_acc = 0.0f;
+    uint32_t phase = 0;
+    bool ok = true, has_acc = false;
+    // every thread: make the operands written so far visible to the tensor
+    // cores, then one thread issues; false when the wait gave up
+    auto sync_issue_wait = [&](auto issue) -> bool {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+        if (tid == 0) {
+            issue();
+            tc_commit(mbar);
+        }
+        const bool got = tc_wait(mbar, phase);
+        if (__syncthreads_or(!got)) {
+            if (tid == 0 && err) atomicOr(err, 1u);
+            return false;
+        }
+        phase ^= 1u;
+        tc_fence_after();
+        return true;
+    };
+    for (uint32_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+        const uint32_t i = tile * kTcRows + tid;
+        f3 p = mk(0.0f, 0.0f, 1.0f), nr = p, wo = p;
+        GuideRow row;
+        if (i < n) {
+            row = A.rows[i];
+            p = normalise_pos(N, mk(row.pos_w.x, row.pos_w.y, row.pos_w.z));
+            nr = mk(row.n.x, row.n.y, row.n.z);
+            wo = mk(row.wo.x, row.wo.y, row.wo.z);
+        }
+        float x[W];
+#pragma unroll
+        for (int l = 0; l < GUIDE_LEVELS; l++) {
+            const float2 f = grid_feature(N, l, p);
+            x[2 * l] = f.x;
+            x[2 * l + 1] = f.y;
+        }
+        x[32] = nr.x; x[33] = nr.y; x[34] = nr.z;
+        x[35] = wo.x; x[36] = wo.y; x[37] = wo.z;
+        x[38] = 1.0f;
+#pragma unroll
+        for (int j = 39; j < W; j++) x[j] = 0.0f;
+        tc_store_row(XA, tid, x, false);
+        tc_store_col(XT, tid, x);
+        // ---- forward ----
+        for (int l = 0; l < GUIDE_LAYERS && ok; l++) {
+            ok = sync_issue_wait([&] {
+#pragma unroll
+                for (uint32_t ks = 0; ks < (uint32_t)W / 16; ks++)
+                    tc_mma(tmem, tc_desc(sXA + ks * 256u), tc_desc(sWF + (uint32_t)l * W * W * 2 + ks * 256u), ks);
+            });
+            if (!ok) break;
+#pragma unroll
+            for (int c = 0; c < 4; c++) tc_load16(tmem + lane_addr + 16u * c, x + 16 * c);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (l + 1 < GUIDE_LAYERS) {
+#pragma unroll
+                for (int j = 0; j < W; j++) x[j] = fmaxf(x[j], 0.0f);
+                tc_store_row(XA, tid, x, false);
+                tc_store_col(XT + (l + 1) * kTcOp, tid, x);
+            }
+        }
+        if (!ok) break;
+        // ---- loss and output gradient of this thread's row ----
+#pragma unroll
+        for (int j = 0; j < W; j++) x[j] += s_bias[j];
+        if (A.dbg_out && i < n)
+            for (int j = 0; j < W; j++) A.dbg_out[(size_t)i * W + j] = x[j];
+        float d[W];
+        if (i < n) {
+            loss_acc += loss_grad(x, mk(row.n.x, row.n.y, row.n.z), mk(row.wi.x, row.wi.y, row.wi.z),
+                                  fminf(row.pos_w.w * wscale, wcap), d);
+        } else {
+#pragma unroll
+            for (int j = 0; j < W; j++) d[j] = 0.0f;
+        }
+#pragma unroll
+        for (int j = 0; j < W; j++) s_o[tid * W + j] = d[j];
+        tc_store_row(DYA, tid, d, false);
+        tc_store_col(DYT, tid, d);
+        // ---- backward ----
+        for (int l = GUIDE_LAYERS - 1; l >= 0 && ok; l--) {
+            const bool acc = has_acc;
+            ok = sync_issue_wait([&] {
+                // dW_l (+)= X_l^T dY_l over this tile's rows
+#pragma unroll
+                for (uint32_t ks = 0; ks < kTcRows / 16; ks++)
+                    tc_mma(tmem + 64u * (uint32_t)(l + 1), tc_desc(sXT + (uint32_t)l * kTcOp + ks * 256u, 2048u),
+                           tc_desc(sDYT + ks * 256u, 2048u), (acc || ks) ? 1u : 0u);
+                // dX_l = dY_l W_l^T
+#pragma unroll
+                for (uint32_t ks = 0; ks < (uint32_t)W / 16; ks++)
+                    tc_mma(tmem, tc_desc(sDYA + ks * 256u), tc_desc(sWB + (uint32_t)l * W * W * 2 + ks * 256u), ks);
+            });
+            if (!ok) break;
+            if (l == GUIDE_LAYERS - 1 && tid < (uint32_t)W) {
+                // output-bias gradient: thread j sums column j over the rows in order
+                float s = 0.0f;
+                for (uint32_t r = 0; r < kTcRows; r++) s += s_o[r * W + tid];
+                s_db[tid] += s;
+            }
+#pragma unroll
+            for (int c = 0; c < 4; c++) tc_load16(tmem + lane_addr + 16u * c, x + 16 * c);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (l > 0) {
+                // through the ReLU that produced X_l: dY_{l-1} = dX_l where X_l > 0
+                const unsigned char *T = XT + l * kTcOp;
+#pragma unroll
+                for (int u = 0; u < W; u++) {
+                    const float xv = __bfloat162float(
+                        *reinterpret_cast<const __nv_bfloat16 *>(T + tc_offset_t((uint32_t)u, tid)));
+                    d[u] = xv > 0.0f ? x[u] : 0.0f;
+                }
+                tc_store_row(DYA, tid, d, false);
+                tc_store_col(DYT, tid, d);
+            } else if (i < n) {
+                // encoding gradient: columns 2 lv, 2 lv + 1 of dX_0
+                for (int lv = 0; lv < GUIDE_LEVELS; lv++) {
+                    const float gx = x[2 * lv], gy = x[2 * lv + 1];
+                    if (A.dbg_enc) {
+                        A.dbg_enc[(size_t)i * 32 + 2 * lv] = gx;
+                        A.dbg_enc[(size_t)i * 32 + 2 * lv + 1] = gy;
+                    }
+                    if (A.grid_grad) {
+                        Corners c;
+                        grid_corners(N, lv, p, c);
+#pragma unroll
+                        for (int k = 0; k < 8; k++) {
+                            atomicAdd(&A.grid_grad[2 * (size_t)c.idx[k]], to_fixed(c.w[k] * gx));
+                            atomicAdd(&A.grid_grad[2 * (size_t)c.idx[k] + 1], to_fixed(c.w[k] * gy));
+                        }
+                    }
+                }
+            }
+        }
+        has_acc = true;
+    }
+    // every thread is past its last tensor-memory read (or the failed wait)
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (!ok && tid == 0) tc_wait(mbar, phase);   // let a commit still in flight land
+    __syncthreads();
+    float *part = A.part + (size_t)blockIdx.x * kPart;
+    if (warp < 2) {
+        // dW_l[u][o] at tensor-memory lane u (0..63), column 64 (l + 1) + o
+        const uint32_t u = 32u * warp + lane;
+        for (int l = 0; l < GUIDE_LAYERS; l++) {
+            float v[W];
+#pragma unroll
+            for (int c = 0; c < 4; c++) tc_load16(tmem + lane_addr + 64u * (uint32_t)(l + 1) + 16u * c, v + 16 * c);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            for (int o = 0; o < W; o++) part[(size_t)l * W * W + u * W + o] = has_acc && ok ? v[o] : 0.0f;
+        }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) loss_acc += __shfl_down_sync(0xFFFFFFFFu, loss_acc, off);
+    if (lane == 0) s_loss[warp] = loss_acc;
+    __syncthreads();
+    for (uint32_t j = tid; j < (uint32_t)W; j += blockDim.x) part[NW + j] = s_db[j];
+    if (tid == 0) {
+        float l = 0.0f;
+        for (uint32_t w = 0; w < kTcRows / 32; w++) l += s_loss[w];
+        part[NW + W] = l;
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcTrainCols) : "memory");
+}
+
 // Block slots of k_guide_train added up in block order: w_grad, b_grad, loss.
 __global__ void k_guide_reduce(const float *part, uint32_t blocks, float *w_grad, float *b_grad, float *loss) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < (uint32_t)(NW + W + 1); i += gridDim.x * blockDim.x) {
@@ -909,7 +1182,10 @@ __global__ void k_tc_weights(const float *w, __nv_bfloat16 *wtc) {
     if (idx >= (uint32_t)NW) return;
     const uint32_t l = idx / (W * W), n = (idx / W) % W, k = idx % W;
     unsigned char *base = reinterpret_cast<unsigned char *>(wtc) + (size_t)l * W * W * 2;
+    // forward: row n = output unit, K = input unit; backward (dX): row n = input unit, K = output unit
     *reinterpret_cast<__nv_bfloat16 *>(base + tc_offset(n, k)) = __float2bfloat16_rn(w[l * W * W + k * W + n]);
+    *reinterpret_cast<__nv_bfloat16 *>(base + (size_t)NW * 2 + tc_offset(n, k)) =
+        __float2bfloat16_rn(w[l * W * W + n * W + k]);
 }
 
 __global__ void k_frags(const float *w, uint2 *wf, uint2 *wt) {
@@ -953,7 +1229,7 @@ struct GuideState {
     uint2 *wf = nullptr, *wt = nullptr;
     __nv_bfloat16 *wtc = nullptr;
     uint32_t *tc_error = nullptr;   // set by the tcgen05 kernel when a wait gives up
-    bool use_tc = true;             // proposals by the tcgen05 kernel (else the mma.sync one)
+    bool use_tc = true;             // network on the tcgen05 kernels (else the mma.sync ones)
     __half2 *feat = nullptr;
     float2 *grid = nullptr, *grid_m = nullptr, *grid_v = nullptr;
     unsigned long long *grid_grad = nullptr;   // [entry][2], fixed point (k_guide_train)
@@ -1046,7 +1322,8 @@ int TrainStep(GuideState &g, const GuideRow *rows, const uint32_t *count, uint32
     A.grid_grad = g.grid_grad;
     A.dbg_out = dbg_out;
     A.dbg_enc = dbg_enc;
-    k_guide_train<<<g.sms, kWarps * 32, kTrainSmem, st>>>(g.net, A);
+    if (g.use_tc) k_guide_train_tc<<<g.sms, kTcRows, kTcTrainSmem, st>>>(g.net, A, g.tc_error);
+    else k_guide_train<<<g.sms, kWarps * 32, kTrainSmem, st>>>(g.net, A);
     k_guide_reduce<<<(NW + W + 1 + 255) / 256, 256, 0, st>>>(g.part, (uint32_t)g.sms, g.w_grad, g.b_grad, g.loss);
     AZ_CUDA_TRY(cudaGetLastError());
     if (!apply) return AZ_OK;
@@ -1075,7 +1352,7 @@ int CreateGuide(const GpuScene &G, const az_guide_config *cfg, GuideState **out)
     g->n_rec = cfg && cfg->record_samples ? cfg->record_samples : (1u << 17);
     g->steps_per_wave = cfg && cfg->steps_per_wave ? cfg->steps_per_wave : 1u;
     g->rows_cap = cfg && cfg->train_batch ? cfg->train_batch : (1u << 18);
-    g->use_tc = !(cfg && cfg->inference == AZ_GUIDE_MMA_SYNC);
+    g->use_tc = !(cfg && cfg->kernels == AZ_GUIDE_MMA_SYNC);
     const uint64_t seed = cfg ? cfg->seed : 0;
     g->w = g->Alloc<float>(NW);
     g->w_grad = g->Alloc<float>(NW);
@@ -1087,7 +1364,7 @@ int CreateGuide(const GpuScene &G, const az_guide_config *cfg, GuideState **out)
     g->b_v = g->Alloc<float>(W);
     g->wf = g->Alloc<uint2>(NFRAG);
     g->wt = g->Alloc<uint2>(NFRAG);
-    g->wtc = g->Alloc<__nv_bfloat16>(NW);
+    g->wtc = g->Alloc<__nv_bfloat16>(2 * NW);
     g->tc_error = g->Alloc<uint32_t>(1);
     g->feat = g->Alloc<__half2>(kGridN);
     g->grid = g->Alloc<float2>(kGridN);
@@ -1132,6 +1409,8 @@ int CreateGuide(const GpuScene &G, const az_guide_config *cfg, GuideState **out)
     AZ_CUDA_TRY(cudaMemset(g->tc_error, 0, sizeof(uint32_t)));
     AZ_CUDA_TRY(cudaFuncSetAttribute(k_guide_mlp_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
     AZ_CUDA_TRY(cudaFuncSetAttribute(k_guide_mlp_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
+    AZ_CUDA_TRY(
+        cudaFuncSetAttribute(k_guide_train_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcTrainSmem));
     // as many resident CTAs per SM as shared memory allows, at most 4: each
     // holds 64 of the SM's 512 tensor-memory columns while it runs
     int per_sm = 0;
@@ -1358,6 +1637,7 @@ extern "C" int az_guide_eval(az_guide *g, const float *rows, uint32_t n, float *
         cudaError_t e = cudaDeviceSynchronize();
         if (e != cudaSuccess) rc = CudaError(e, "guide eval");
     }
+    if (rc == AZ_OK) rc = GuideCheck(s, nullptr);
     if (rc == AZ_OK && outputs) cudaMemcpy(outputs, d_out, (size_t)n * W * sizeof(float), cudaMemcpyDeviceToHost);
     if (rc == AZ_OK && enc_grad) cudaMemcpy(enc_grad, d_enc, (size_t)n * 32 * sizeof(float), cudaMemcpyDeviceToHost);
     if (rc == AZ_OK && loss) cudaMemcpy(loss, s.loss, sizeof(float), cudaMemcpyDeviceToHost);
@@ -1390,6 +1670,7 @@ extern "C" int az_guide_train(az_guide *g, const float *rows, uint32_t n, uint32
         cudaError_t e = cudaDeviceSynchronize();
         if (e != cudaSuccess) rc = CudaError(e, "guide train");
     }
+    if (rc == AZ_OK) rc = GuideCheck(s, nullptr);
     cudaFree(d_rows);
     cudaFree(d_count);
     return rc;

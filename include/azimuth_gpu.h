@@ -389,10 +389,11 @@ typedef struct az_guide_config {
     uint32_t record_samples;        /* camera samples per wave whose vertices are recorded; 0 = 2^17 */
     uint32_t steps_per_wave;        /* Adam steps on each wave's rows when training; 0 = 1 */
     uint64_t seed;                  /* weight initialisation */
-    uint32_t inference;             /* proposal kernel: AZ_GUIDE_TCGEN05 (0, default) runs the MLP on the
-                                       5th-generation tensor cores (tcgen05.mma, operands in shared memory,
-                                       accumulator in tensor memory, 128 rows per CTA); AZ_GUIDE_MMA_SYNC
-                                       runs it warp-synchronously with mma.sync (16 rows per warp) */
+    uint32_t kernels;               /* network kernels (proposals and training): AZ_GUIDE_TCGEN05 (0, the
+                                       default) runs the MLP on the 5th-generation tensor cores
+                                       (tcgen05.mma, operands in shared memory, accumulators in tensor
+                                       memory, 128 rows per CTA); AZ_GUIDE_MMA_SYNC runs it warp by warp
+                                       with mma.sync (16 rows per warp) */
     uint32_t reserved[5];
 } az_guide_config;
 

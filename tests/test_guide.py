@@ -115,11 +115,18 @@ def _bounds(info):
     return lo, lo + 1.0 / info["inv_ext"].astype(np.float64)
 
 
+KERNELS = pytest.mark.parametrize("kernels", [az.GUIDE_TCGEN05, az.GUIDE_MMA_SYNC], ids=["tcgen05", "mma_sync"])
+
+
 @pytest.mark.gpu
-def test_guide_forward_and_gradients_match_oracle(gpu):
+@KERNELS
+def test_guide_forward_and_gradients_match_oracle(gpu, kernels):
+    """Outputs, loss and every gradient of both network kernel sets (tcgen05:
+    128-row tiles; mma.sync: 16-row warp tiles) against the FP64 oracle, on a
+    row count that leaves a partial tile."""
     rng = np.random.default_rng(3)
     scene = az.generate_scene(az.SCENE_CORNELL, width=8, height=8, spp=1)
-    with az.GpuScene(scene) as g, _guide(g) as guide:
+    with az.GpuScene(scene) as g, _guide(g, kernels=kernels) as guide:
         info = guide.info()
         assert list(info["res"]) == list(go.level_res())
         mlp = rng.normal(scale=0.2, size=(4, 64, 64)).astype(np.float32)
@@ -127,7 +134,7 @@ def test_guide_forward_and_gradients_match_oracle(gpu):
         grid = rng.uniform(-1.0, 1.0, size=(16, 1 << 19, 2)).astype(np.float32)
         guide.set_params(mlp, bias, grid)
         lo, hi = _bounds(info)
-        rows = _rows(rng, 512, lo, hi)
+        rows = _rows(rng, 500, lo, hi)
         got = guide.eval(rows)
         ref = go.evaluate({"mlp": mlp.astype(np.float64), "bias": bias.astype(np.float64)},
                           grid.astype(np.float16).astype(np.float64), rows, info["lo"], info["inv_ext"])
@@ -255,7 +262,8 @@ def test_guided_render_beats_cosine_sampling(gpu):
 
 
 @pytest.mark.gpu
-def test_adam_step_matches_the_oracle_and_training_is_deterministic(gpu):
+@KERNELS
+def test_adam_step_matches_the_oracle_and_training_is_deterministic(gpu, kernels):
     """One Adam step (learning rate 1e-2, betas 0.9 / 0.99, eps 1e-8) on the
     gradients az_guide_eval reports: the first step moves every parameter by
     lr * g / (|g| + eps) (both moments bias-corrected), the MLP and bias from
@@ -267,7 +275,7 @@ def test_adam_step_matches_the_oracle_and_training_is_deterministic(gpu):
     scene = az.generate_scene(az.SCENE_CORNELL, width=8, height=8, spp=1)
     lr, eps = 1e-2, 1e-8
     with az.GpuScene(scene) as g:
-        with _guide(g, seed=2) as guide:
+        with _guide(g, seed=2, kernels=kernels) as guide:
             info = guide.info()
             lo, hi = _bounds(info)
             rows = _rows(rng, 4096, lo, hi)
@@ -277,7 +285,7 @@ def test_adam_step_matches_the_oracle_and_training_is_deterministic(gpu):
             mlp1, bias1, grid1 = guide.params()
         finals = []
         for _ in range(2):
-            with _guide(g, seed=9) as gd:
+            with _guide(g, seed=9, kernels=kernels) as gd:
                 gd.train(rows, 3)
                 finals.append(gd.params())
     for p0, p1, gr in ((mlp0, mlp1, grads["mlp_grad"]), (bias0, bias1, grads["bias_grad"])):
@@ -324,7 +332,7 @@ def test_tensor_core_inference_matches_oracle_and_the_mma_sync_path(gpu):
                           grid.astype(np.float16).astype(np.float64), rows, info["lo"], info["inv_ext"])
         films = []
         for kind in (az.GUIDE_TCGEN05, az.GUIDE_MMA_SYNC):
-            with _guide(g, seed=5, inference=kind) as gd:
+            with _guide(g, seed=5, kernels=kind) as gd:
                 gd.set_params(mlp, bias, grid)
                 w, h = scene.resolution()
                 f = torch.zeros((h, w, 4), device="cuda")
