@@ -339,10 +339,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_shadow(DevScene S, CameraParams
                 if (kind == SHADOW_ENTITY_FULL) {
                     live = false;   // k_shadow_full
                 } else if (kind == SHADOW_ENTITY) {
-                    const DevLight &L = S.lights[li];
-                    float tl = FLT_MAX;
-                    const int lh = light_entity_hit(S, L, r, tl);
-                    T.init(S, r, false, 0.0f, lh ? tl : FLT_MAX, stack, L.ent_index);
+                    const LightHit lh = light_entity_hit_call(S.ents, S.light_tris, S.lights + li, r);
+                    T.init(S, r, false, 0.0f, lh.hit ? lh.t : FLT_MAX, stack, S.lights[li].ent_index);
                 } else {
                     T.init(S, r, false, 0.0f, kind == SHADOW_ANY ? FLT_MAX : d.w, stack);
                 }
@@ -372,10 +370,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_shadow(DevScene S, CameraParams
             if (kind == SHADOW_ENTITY_FULL) {
                 continue;   // k_shadow_full
             } else if (kind == SHADOW_ENTITY) {
-                const DevLight &L = S.lights[li];
-                float tl = FLT_MAX;
-                const int lh = light_entity_hit(S, L, r, tl);
-                visible = !trace<Q_ANY, WT>(S, r, false, 0.0f, lh ? tl : FLT_MAX, h, cnt, err, L.ent_index);
+                const LightHit lh = light_entity_hit_call(S.ents, S.light_tris, S.lights + li, r);
+                visible = !trace<Q_ANY, WT>(S, r, false, 0.0f, lh.hit ? lh.t : FLT_MAX, h, cnt, err,
+                                            S.lights[li].ent_index);
             } else {
                 visible = !trace<Q_ANY, WT>(S, r, false, 0.0f, kind == SHADOW_ANY ? FLT_MAX : d.w, h, cnt, err);
             }
@@ -409,10 +406,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_shadow(DevScene S, CameraParams
             if (kind == SHADOW_ENTITY_FULL) {
                 idx = kLaneIdle;   // k_shadow_full
             } else if (kind == SHADOW_ENTITY) {
-                const DevLight &L = Sq.lights[li];
-                float tl = FLT_MAX;
-                const int lh = light_entity_hit(Sq, L, r, tl);
-                T.init(Sq, r, false, 0.0f, lh ? tl : FLT_MAX, stack, L.ent_index);
+                const LightHit lh = light_entity_hit_call(Sq.ents, Sq.light_tris, Sq.lights + li, r);
+                T.init(Sq, r, false, 0.0f, lh.hit ? lh.t : FLT_MAX, stack, Sq.lights[li].ent_index);
             } else {
                 T.init(Sq, r, false, 0.0f, kind == SHADOW_ANY ? FLT_MAX : d.w, stack);
             }

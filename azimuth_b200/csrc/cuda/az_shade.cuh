@@ -424,11 +424,27 @@ static __device__ void sample_entity_light(const DevScene &S, const DevLight &L,
 // `triangle` array, whose vertices are the triangle entities' vertices).
 // Returns 1 with the world t, 0 if the light is not hit, -1 if the light
 // needs a full nearest-hit query instead (entity_light_needs_full_query).
-static __device__ int light_entity_hit(const DevScene &S, const DevLight &L, const Ray &wr, float &t_world) {
+// Called out of line by the visibility kernels (values and global pointers
+// only), which keeps their traversal loop small.
+struct LightHit {
+    int hit;
+    float t;   // world t when hit; FLT_MAX otherwise
+};
+static __device__ int light_entity_hit(const DevEntity *ents, const DevLightTri *light_tris, const DevLight &L,
+                                       const Ray &wr, float &t_world);
+static __device__ __noinline__ LightHit light_entity_hit_call(const DevEntity *ents, const DevLightTri *light_tris,
+                                                             const DevLight *L, Ray wr) {
+    LightHit h;
+    h.t = FLT_MAX;
+    h.hit = light_entity_hit(ents, light_tris, *L, wr, h.t);
+    return h;
+}
+static __device__ int light_entity_hit(const DevEntity *ents, const DevLightTri *light_tris, const DevLight &L,
+                                       const Ray &wr, float &t_world) {
     if (entity_light_needs_full_query(L)) return -1;
     if (L.entity_type == ENT_SPHERE) {
         float tl;
-        return sphere_test(S.ents[L.ent_index], wr, 0.0f, t_world, tl) ? 1 : 0;
+        return sphere_test(ents[L.ent_index], wr, 0.0f, t_world, tl) ? 1 : 0;
     }
     f3 motion = wr.time * mk(L.motion[0], L.motion[1], L.motion[2]);
     Ray m = wr;
@@ -436,7 +452,7 @@ static __device__ int light_entity_hit(const DevScene &S, const DevLight &L, con
     Ray lr = L.identity ? local_ray_identity(wr) : local_ray(m, L.inv);
     float best = FLT_MAX;
     for (uint32_t k = 0; k < L.tri_count; k++) {
-        const DevLightTri &T = S.light_tris[L.tri_offset + k];
+        const DevLightTri &T = light_tris[L.tri_offset + k];
         DevTri tr;
         tr.a = make_float4(T.p0n.x, T.p0n.y, T.p0n.z, T.p0n.x - T.p1n.x);
         tr.b = make_float4(T.p0n.y - T.p1n.y, T.p0n.z - T.p1n.z, T.p0n.x - T.p2n.x, T.p0n.y - T.p2n.y);

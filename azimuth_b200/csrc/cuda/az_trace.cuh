@@ -330,6 +330,39 @@ __device__ __forceinline__ float group_t_scale(const DevGroup &g, f3 d) {
     return length(vector_xf(g.inv, d)) / length(d) * 1.0001f;
 }
 
+// The traversal loops call the rarely taken paths below out of line, with
+// values and global pointers only, so that the loops' own code stays small
+// (the instruction cache of an SM holds the hot loop; a scene's spheres,
+// transformed instances and entity lights take these calls).
+
+// sphere_test of entity e for the world ray.
+struct SphereHit {
+    float t_world, t_local;
+    uint32_t hit;
+};
+static __device__ __noinline__ SphereHit sphere_test_call(const DevEntity *e, Ray wr, float eps) {
+    SphereHit h;
+    h.t_world = h.t_local = FLT_MAX;
+    h.hit = sphere_test(*e, wr, eps, h.t_world, h.t_local) ? 1u : 0u;
+    return h;
+}
+
+// The local ray of a transformed, possibly moving group (GetLocalRay of the
+// motion-shifted ray) and the group_t_scale of the world direction.
+struct GroupRay {
+    Ray r;
+    float scale;
+};
+static __device__ __noinline__ GroupRay group_ray_call(const DevGroup *gp, Ray wr) {
+    const DevGroup &g = *gp;
+    Ray m = wr;
+    m.o = wr.o - wr.time * mk(g.motion[0], g.motion[1], g.motion[2]);
+    GroupRay out;
+    out.r = local_ray(m, g.inv);
+    out.scale = group_t_scale(g, wr.d);
+    return out;
+}
+
 // Two-level traversal of the 8-wide hierarchy, after the node-group /
 // primitive-group scheme of Ylitie, Karras, Laine, "Efficient Incoherent Ray
 // Traversal on GPUs Through Compressed Wide BVHs" (HPG 2017): each step
@@ -430,10 +463,9 @@ struct Tracer {
             r = local_ray_identity(wr);
             if (wlim < FLT_MAX) tcur = wlim * 1.0001f + 1e-30f;
         } else {
-            Ray m = wr;
-            m.o = wr.o - wr.time * mk(g.motion[0], g.motion[1], g.motion[2]);
-            r = local_ray(m, g.inv);
-            if (wlim < FLT_MAX) tcur = wlim * group_t_scale(g, wr.d) + 1e-30f;
+            const GroupRay gr = group_ray_call(S.groups + g_idx, wr);
+            r = gr.r;
+            if (wlim < FLT_MAX) tcur = wlim * gr.scale + 1e-30f;
         }
         inv = safe_inv(r.d);
         oct = octant_of(r.d);
@@ -584,21 +616,20 @@ struct Tracer {
                 const uint32_t p = __ldg(S.tlas_prims + pi);
                 if (p & AZD_TLAS_GROUP) {
                     push(stack, p & ~AZD_TLAS_GROUP, AZD_E_GROUP, err);   // entered when popped
-                } else if (p != skip_ent) {
-                    const DevEntity &e = S.ents[p];
-                    float wt, tl;
-                    if (e.type == ENT_SPHERE && sphere_test(e, wr, eps, wt, tl)) {
+                } else if (p != skip_ent && S.ents[p].type == ENT_SPHERE) {
+                    const SphereHit sh = sphere_test_call(S.ents + p, wr, eps);
+                    if (sh.hit) {
                         if (KIND == Q_ANY) {
-                            if (wt < tmax) {
+                            if (sh.t_world < tmax) {
                                 hit_any = true;
                                 return true;
                             }
-                        } else if (wt < best.t) {
-                            best.t = wt;
-                            best.tl = tl;
+                        } else if (sh.t_world < best.t) {
+                            best.t = sh.t_world;
+                            best.tl = sh.t_local;
                             best.prim = 0xFFFFFFFFu;
                             best.ent = p;
-                            tcur = wt;
+                            tcur = sh.t_world;
                         }
                     }
                 }
@@ -764,21 +795,20 @@ __device__ bool trace(const DevScene &S, const Ray &wr, bool cull, float eps, fl
                     // entered when popped; leave room for its exit marker
                     if (sp + 1 < AZD_WSTACK) stack[sp++] = make_uint2(p & ~AZD_TLAS_GROUP, AZD_E_GROUP);
                     else if (err) atomicOr(err, 2u);
-                } else if (p != skip_ent) {
-                    const DevEntity &e = S.ents[p];
-                    float wt, tl;
-                    if (e.type == ENT_SPHERE && sphere_test(e, wr, eps, wt, tl)) {
+                } else if (p != skip_ent && S.ents[p].type == ENT_SPHERE) {
+                    const SphereHit sh = sphere_test_call(S.ents + p, wr, eps);
+                    if (sh.hit) {
                         if (KIND == Q_ANY) {
-                            if (wt < tmax) {
+                            if (sh.t_world < tmax) {
                                 hit_any = true;
                                 break;
                             }
-                        } else if (wt < best.t) {
-                            best.t = wt;
-                            best.tl = tl;
+                        } else if (sh.t_world < best.t) {
+                            best.t = sh.t_world;
+                            best.tl = sh.t_local;
                             best.prim = 0xFFFFFFFFu;
                             best.ent = p;
-                            tcur = wt;
+                            tcur = sh.t_world;
                         }
                     }
                 }
@@ -823,10 +853,9 @@ __device__ bool trace(const DevScene &S, const Ray &wr, bool cull, float eps, fl
                 r = local_ray_identity(wr);
                 if (wlim < FLT_MAX) tcur = wlim * 1.0001f + 1e-30f;
             } else {
-                Ray m = wr;
-                m.o = wr.o - wr.time * mk(g.motion[0], g.motion[1], g.motion[2]);
-                r = local_ray(m, g.inv);
-                if (wlim < FLT_MAX) tcur = wlim * group_t_scale(g, wr.d) + 1e-30f;
+                const GroupRay gr = group_ray_call(S.groups + g_idx, wr);
+                r = gr.r;
+                if (wlim < FLT_MAX) tcur = wlim * gr.scale + 1e-30f;
             }
             inv = safe_inv(r.d);
             oct = octant_of(r.d);

@@ -2,6 +2,7 @@
 
     python -m azimuth_b200.profile_cases dense_mesh [--variant V] [--frames F]
     python -m azimuth_b200.profile_cases guide_interior [--frames F]
+    python -m azimuth_b200.profile_cases guide_interior_full [--frames F]
 
 dense_mesh: the dense-mesh scene (1,310,720-triangle displaced icosphere in
 the Cornell box, 7 BRDFs, depth 8) at 256x256 and 16 samples per pixel, one
@@ -9,6 +10,8 @@ wave per frame, traversal launch variant V (default: the library's).
 guide_interior: the interior scene (detail 12, about 250 k triangles) at
 320x180, 4 samples per pixel; the first frame trains the path guide, the
 rest render with it.
+guide_interior_full: the same at the guided comparison's size (detail 49,
+about 4 M triangles, 1920x1080, 4 samples per pixel).
 """
 import argparse
 import sys
@@ -16,7 +19,7 @@ import sys
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["dense_mesh", "guide_interior"])
+    ap.add_argument("case", choices=["dense_mesh", "guide_interior", "guide_interior_full"])
     ap.add_argument("--variant", type=int, default=0)
     ap.add_argument("--frames", type=int, default=2)
     a = ap.parse_args(argv)
@@ -24,8 +27,10 @@ def main(argv=None):
     import azimuth_b200 as az
     if a.case == "dense_mesh":
         sc = az.generate_scene(az.SCENE_DENSE_MESH, seed=0, width=256, height=256, spp=16)
-    else:
+    elif a.case == "guide_interior":
         sc = az.generate_scene(az.SCENE_INTERIOR, seed=0, width=320, height=180, spp=4, detail=12)
+    else:
+        sc = az.generate_scene(az.SCENE_INTERIOR, seed=0, width=1920, height=1080, spp=4, detail=49)
     w, h = sc.resolution()
     film = torch.zeros((h, w, 4), device="cuda")
     with az.GpuScene(sc) as g:

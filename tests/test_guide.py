@@ -304,7 +304,8 @@ def test_adam_step_matches_the_oracle_and_training_is_deterministic(gpu, kernels
     touched = np.abs(gg) > 1e-5
     step = grid1.astype(np.float64) - grid0.astype(np.float64)
     assert touched.sum() > 1000
-    assert np.abs(step[touched] + lr * np.sign(gg[touched])).max() <= 2e-4 * lr + 1e-7
+    want = -lr * gg[touched] / (np.abs(gg[touched]) + eps)
+    assert np.abs(step[touched] - want).max() <= 2e-4 * lr + 1e-7
     assert np.abs(step[np.abs(gg) == 0.0]).max() == 0.0
     for a, b in zip(finals[0], finals[1]):
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
