@@ -43,8 +43,11 @@ SCENE_ARGS = dict(scene_id=1, seed=0)
 # one single-pass ncu capture (dram__bytes_read.sum + dram__bytes_write.sum)
 # of every k_extend / k_shadow launch of one 256x256, 16-spp frame (one wave of
 # 2^20 samples): the capture's bytes over the frame's queries
-DRAM_BYTES_PER_QUERY = {"k_extend": None, "k_shadow": None}
-PROFILE_NOTE = "profiles/k_extend_dense_mesh_256x256_16spp.md"
+DRAM_BYTES_PER_QUERY = {"k_extend": 207.1, "k_shadow": 246.2}
+PROFILE_NOTE = "profiles/traversal_dram_dense_mesh_256x256_16spp.md, profiles/k_extend_k_shadow_dense_mesh_256x256_16spp.md"
+# issue statistics of the two traversal kernels from the ncu capture of that small case
+ISSUE = {"k_extend": {"threads_per_warp_instruction": 8.49, "issue_active_pct": 60.0, "warps_active_pct": 36.4},
+         "k_shadow": {"threads_per_warp_instruction": 8.40, "issue_active_pct": 51.8, "warps_active_pct": 35.0}}
 
 
 def parse():
@@ -355,12 +358,12 @@ def main():
                    if dense and DRAM_BYTES_PER_QUERY["k_extend"] else None)
     sh_traffic = (DRAM_BYTES_PER_QUERY["k_shadow"] * sh_q / launches_per_frame
                   if dense and DRAM_BYTES_PER_QUERY["k_shadow"] else None)
-    limiter = ("instruction issue of divergent traversal (about 8 of 32 lanes active per warp instruction, "
-               "two thirds of issue slots used; DRAM at a few percent of peak: %s)" % PROFILE_NOTE)
+    limiter = ("instruction issue of divergent traversal, not HBM: about 8 of 32 lanes active per warp "
+               "instruction, DRAM traffic a quarter of the algorithmic bytes (%s)" % PROFILE_NOTE)
     roofline = {"bound": "hbm", "achieved": ext_achieved, "peak": hbm, "unit": "GB/s", "frac": ext_achieved / hbm,
                 "traffic": ext_traffic, "traffic_unit": "DRAM bytes per launch (ncu, scaled from a small frame)",
                 "algorithmic_bytes_per_launch": ext_bytes / launches_per_frame,
-                "kernel": "k_extend (closest-hit traversal)", "limiter": limiter,
+                "kernel": "k_extend (closest-hit traversal)", "limiter": limiter, "issue": ISSUE["k_extend"],
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650",
                 "bytes_per_segment": ext_bytes / ext_q,
                 "node_visits_per_segment": cnt["node_visits"] / ext_q,
@@ -371,7 +374,7 @@ def main():
                        "frac": sh_achieved / hbm, "traffic": sh_traffic,
                        "traffic_unit": "DRAM bytes per launch (ncu, scaled from a small frame)",
                        "algorithmic_bytes_per_launch": sh_bytes / launches_per_frame,
-                       "kernel": "k_shadow (visibility, any hit)", "limiter": limiter,
+                       "kernel": "k_shadow (visibility, any hit)", "limiter": limiter, "issue": ISSUE["k_shadow"],
                        "bytes_per_query": sh_bytes / sh_q,
                        "node_visits_per_query": cnt["shadow_node_visits"] / sh_q,
                        "prim_visits_per_query": cnt["shadow_prim_visits"] / sh_q,
