@@ -194,16 +194,17 @@ __global__ void k_order_keys(DevScene S, WaveQueues Q, uint32_t level, int shado
 enum : int { MODE_LOOP = 0, MODE_LOCKSTEP = 1, MODE_FETCH = 2, MODE_FETCHP = 3, MODE_STAGED = 4 };
 
 // WT: triangles by the watertight test (AZ_FLAG_WATERTIGHT) instead of azimuth's.
-// MULTI: a tile wave of several scenes (MODE_FETCHP only): each query is
+// MULTI: a tile wave of several scenes (persistent modes only): each query is
 // traced in the scene its entry names (WaveQueues.scenes).
-template <int BLOCK, int MINB, int MODE, bool WT = false, bool MULTI = false>
+// SPH: the top-level sphere test inline (Tracer SPH).
+template <int BLOCK, int MINB, int MODE, bool WT = false, bool MULTI = false, bool SPH = false>
 __global__ void __launch_bounds__(BLOCK, MINB) k_extend(DevScene S, CameraParams cam, WaveQueues Q, uint32_t level) {
     const int buf = level & 1;
     const uint32_t n = min(Q.counts[level], Q.cap_q);
     uint32_t *cnt = cam.count_traversal ? Q.counts + AZ_COUNT_NODES : nullptr;
     uint32_t *err = Q.counts + AZ_COUNT_ERROR;
     if (MODE == MODE_LOCKSTEP) {
-        Tracer<Q_CLOSEST, false, WT> T;
+        Tracer<Q_CLOSEST, false, WT, SPH> T;
         uint2 stack[AZD_WSTACK];
         // warp-uniform loop bound: every lane of a warp sees the same base
         for (uint32_t base = blockIdx.x * BLOCK + (threadIdx.x & ~31u); base < n; base += gridDim.x * BLOCK) {
@@ -248,7 +249,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_extend(DevScene S, CameraParams
     constexpr bool STAGED = MODE == MODE_STAGED;
     static_assert(!(STAGED && MULTI), "staged fetching serves one scene");
     __shared__ uint4 s_stage[STAGED ? BLOCK / 32 * 160 : 1];
-    Tracer<Q_CLOSEST, MODE == MODE_FETCHP || STAGED, WT> T;
+    Tracer<Q_CLOSEST, MODE == MODE_FETCHP || STAGED, WT, SPH> T;
     uint2 stack[AZD_WSTACK];
     WarpFetch wf;
     uint32_t idx = kLaneIdle, qi = 0;   // work item and its queue entry
@@ -314,13 +315,13 @@ __global__ void __launch_bounds__(128) k_shadow_full(DevScene S0, CameraParams c
     }
 }
 
-template <int BLOCK, int MINB, int MODE, bool WT = false, bool MULTI = false>
+template <int BLOCK, int MINB, int MODE, bool WT = false, bool MULTI = false, bool SPH = false>
 __global__ void __launch_bounds__(BLOCK, MINB) k_shadow(DevScene S, CameraParams cam, WaveQueues Q, uint32_t level) {
     const uint32_t n = min(Q.counts[AZ_COUNT_SHADOW + level], Q.cap_s);
     uint32_t *cnt = cam.count_traversal ? Q.counts + AZ_COUNT_SNODES : nullptr;
     uint32_t *err = Q.counts + AZ_COUNT_ERROR;
     if (MODE == MODE_LOCKSTEP) {
-        Tracer<Q_ANY, false, WT> T;
+        Tracer<Q_ANY, false, WT, SPH> T;
         uint2 stack[AZD_WSTACK];
         for (uint32_t base = blockIdx.x * BLOCK + (threadIdx.x & ~31u); base < n; base += gridDim.x * BLOCK) {
             const uint32_t k = base + (threadIdx.x & 31u);
@@ -384,7 +385,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_shadow(DevScene S, CameraParams
     constexpr bool STAGED = MODE == MODE_STAGED;
     static_assert(!(STAGED && MULTI), "staged fetching serves one scene");
     __shared__ uint4 s_stage[STAGED ? BLOCK / 32 * 160 : 1];
-    Tracer<Q_ANY, MODE == MODE_FETCHP || STAGED, WT> T;
+    Tracer<Q_ANY, MODE == MODE_FETCHP || STAGED, WT, SPH> T;
     uint2 stack[AZD_WSTACK];
     WarpFetch wf;
     uint32_t idx = kLaneIdle;
@@ -499,10 +500,17 @@ constexpr Variant kVariants[] = {{128, 1, MODE_LOOP},     {128, 6, MODE_LOOP},  
 constexpr uint32_t kVariantCount = sizeof(kVariants) / sizeof(kVariants[0]);
 static_assert(kVariantCount == AZ_LAUNCH_VARIANTS, "variant table and header disagree");
 
+// Scenes with spheres at the top level get the kernels with the sphere test
+// inline (a one-thread-per-query loop always has it inline).
 template <int B, int M, int P>
 void LaunchTraversal(bool shadow, int sms, const DevScene &S, const CameraParams &cam, const WaveQueues &Q,
                      uint32_t L, cudaStream_t st) {
     const int grid = sms * (2048 / B);
+    if (P != MODE_LOOP && S.top_spheres) {
+        if (shadow) k_shadow<B, M, P, false, false, true><<<grid, B, 0, st>>>(S, cam, Q, L);
+        else k_extend<B, M, P, false, false, true><<<grid, B, 0, st>>>(S, cam, Q, L);
+        return;
+    }
     if (shadow) k_shadow<B, M, P><<<grid, B, 0, st>>>(S, cam, Q, L);
     else k_extend<B, M, P><<<grid, B, 0, st>>>(S, cam, Q, L);
 }
@@ -511,15 +519,21 @@ void LaunchTraversalVariant(uint32_t v, bool shadow, int sms, const DevScene &S,
                             const WaveQueues &Q, uint32_t L, cudaStream_t st) {
     const int fgrid = sms * 16;
     if (Q.scenes) {
-        // a tile wave of several scenes: one launch configuration, 128 threads, pop-first persistent fetching
+        // a tile wave of several scenes: one launch configuration, 128 threads, at most 64 registers,
+        // persistent fetching (variant 8), the sphere test inline when any scene has top-level spheres
         if (cam.watertight) {
             if (shadow && S.full_light_queries) k_shadow_full<true, true><<<fgrid, 128, 0, st>>>(S, cam, Q, L);
-            if (shadow) k_shadow<128, 6, MODE_FETCHP, true, true><<<fgrid, 128, 0, st>>>(S, cam, Q, L);
-            else k_extend<128, 6, MODE_FETCHP, true, true><<<fgrid, 128, 0, st>>>(S, cam, Q, L);
+            if (shadow) k_shadow<128, 8, MODE_FETCH, true, true><<<fgrid, 128, 0, st>>>(S, cam, Q, L);
+            else k_extend<128, 8, MODE_FETCH, true, true><<<fgrid, 128, 0, st>>>(S, cam, Q, L);
         } else {
             if (shadow && S.full_light_queries) k_shadow_full<false, true><<<fgrid, 128, 0, st>>>(S, cam, Q, L);
-            if (shadow) k_shadow<128, 6, MODE_FETCHP, false, true><<<fgrid, 128, 0, st>>>(S, cam, Q, L);
-            else k_extend<128, 6, MODE_FETCHP, false, true><<<fgrid, 128, 0, st>>>(S, cam, Q, L);
+            if (S.top_spheres) {
+                if (shadow) k_shadow<128, 8, MODE_FETCH, false, true, true><<<fgrid, 128, 0, st>>>(S, cam, Q, L);
+                else k_extend<128, 8, MODE_FETCH, false, true, true><<<fgrid, 128, 0, st>>>(S, cam, Q, L);
+            } else {
+                if (shadow) k_shadow<128, 8, MODE_FETCH, false, true><<<fgrid, 128, 0, st>>>(S, cam, Q, L);
+                else k_extend<128, 8, MODE_FETCH, false, true><<<fgrid, 128, 0, st>>>(S, cam, Q, L);
+            }
         }
         return;
     }
@@ -1132,6 +1146,7 @@ int RenderTiles(GpuScene &G, std::vector<TileJob> &jobs, const az_render_opts *o
         if (d.max_depth + 1 > AZ_MAX_LEVELS - 2) return SetError(AZ_ERR_UNSUPPORTED, "MaxRecursionDepth above 61");
         wave_dev.features |= d.features;
         wave_dev.full_light_queries |= d.full_light_queries;
+        wave_dev.top_spheres += d.top_spheres;
         wave_dev.max_depth = std::max(wave_dev.max_depth, d.max_depth);
         per_node_shadow = std::max(per_node_shadow, d.light_count + (d.use_env_map ? 1u : 0u));
     }

@@ -186,6 +186,8 @@ struct DevScene {
     uint32_t light_draws;           // RNG draws made by the light loop at every vertex
     uint32_t features;              // FEAT_* bits
     uint32_t full_light_queries;    // 1: an entity light needs full nearest-hit visibility queries
+    uint32_t top_spheres;           // sphere entities at the top level (the traversal kernels with the
+                                    // sphere test inline serve scenes that have any)
     // luminance CDF of a 2D environment map (null when the scene has none):
     // env_rows[0..H] over rows (weighted by sin theta), env_cols[r * (W + 1) + 0..W] within row r
     const float *env_rows;

@@ -916,6 +916,7 @@ int BuildGpuScene(const az_scene *scene, const az_render_opts *opts, cudaStream_
     for (const azd::DevMaterial &m : mats)
         if (m.transparent || m.is_mirror) D.features |= azd::FEAT_SPECIAL;
     D.full_light_queries = 0;
+    D.top_spheres = (uint32_t)(tlas.size() - dgroups.size());
     for (const azd::DevLight &l : lights) {
         if (l.type != azd::LIGHT_ENTITY) D.features |= azd::FEAT_ANALYTIC_LIGHTS;
         else if (azd::entity_light_needs_full_query(l)) D.full_light_queries = 1;

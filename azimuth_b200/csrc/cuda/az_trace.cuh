@@ -315,6 +315,12 @@ __device__ __forceinline__ uint32_t octant_of(f3 d) {
 // src/azimuth_main.cpp:256-262).
 __device__ __forceinline__ float group_world_t(const DevGroup &g, const Ray &wr, const Ray &lr, float t) {
     if (g.raw) return t;
+    if (g.identity) {
+        // point_xf of the identity returns the point (x * 1 + y * 0 + z * 0 + 0
+        // is x) and the motion is zero: the same world t without the products
+        const f3 lp = lr.o + (lr.d * t);
+        return length(lp - wr.o) / length(wr.d);
+    }
     f3 motion = wr.time * mk(g.motion[0], g.motion[1], g.motion[2]);
     f3 o2 = wr.o - motion;
     f3 lp = lr.o + (lr.d * t);
@@ -335,12 +341,21 @@ __device__ __forceinline__ float group_t_scale(const DevGroup &g, f3 d) {
 // (the instruction cache of an SM holds the hot loop; a scene's spheres,
 // transformed instances and entity lights take these calls).
 
-// sphere_test of entity e for the world ray.
+// sphere_test of entity e for the world ray: out of line, or inline (INL)
+// in the kernels that serve scenes with spheres at the top level.
 struct SphereHit {
     float t_world, t_local;
     uint32_t hit;
 };
 static __device__ __noinline__ SphereHit sphere_test_call(const DevEntity *e, Ray wr, float eps) {
+    SphereHit h;
+    h.t_world = h.t_local = FLT_MAX;
+    h.hit = sphere_test(*e, wr, eps, h.t_world, h.t_local) ? 1u : 0u;
+    return h;
+}
+template <bool INL>
+__device__ __forceinline__ SphereHit sphere_hit(const DevEntity *e, const Ray &wr, float eps) {
+    if (!INL) return sphere_test_call(e, wr, eps);
     SphereHit h;
     h.t_world = h.t_local = FLT_MAX;
     h.hit = sphere_test(*e, wr, eps, h.t_world, h.t_local) ? 1u : 0u;
@@ -384,7 +399,9 @@ __device__ bool trace(const DevScene &S, const Ray &wr, bool cull, float eps, fl
 // step (a finished query is reported at the end of its last step); otherwise
 // a step ends with the pop and the popped group waits for the next step.
 // WT: triangles by the watertight test instead of azimuth's Cramer test.
-template <QueryKind KIND, bool POP_FIRST = false, bool WT = false>
+// SPH: the top-level sphere test inline (scenes with spheres at the top
+// level); otherwise it is called out of line.
+template <QueryKind KIND, bool POP_FIRST = false, bool WT = false, bool SPH = false>
 struct Tracer {
     static constexpr uint32_t kNoNode = 0xFFFFFFFFu;
     Ray wr;                    // world ray
@@ -617,7 +634,7 @@ struct Tracer {
                 if (p & AZD_TLAS_GROUP) {
                     push(stack, p & ~AZD_TLAS_GROUP, AZD_E_GROUP, err);   // entered when popped
                 } else if (p != skip_ent && S.ents[p].type == ENT_SPHERE) {
-                    const SphereHit sh = sphere_test_call(S.ents + p, wr, eps);
+                    const SphereHit sh = sphere_hit<SPH>(S.ents + p, wr, eps);
                     if (sh.hit) {
                         if (KIND == Q_ANY) {
                             if (sh.t_world < tmax) {
@@ -796,7 +813,7 @@ __device__ bool trace(const DevScene &S, const Ray &wr, bool cull, float eps, fl
                     if (sp + 1 < AZD_WSTACK) stack[sp++] = make_uint2(p & ~AZD_TLAS_GROUP, AZD_E_GROUP);
                     else if (err) atomicOr(err, 2u);
                 } else if (p != skip_ent && S.ents[p].type == ENT_SPHERE) {
-                    const SphereHit sh = sphere_test_call(S.ents + p, wr, eps);
+                    const SphereHit sh = sphere_hit<true>(S.ents + p, wr, eps);
                     if (sh.hit) {
                         if (KIND == Q_ANY) {
                             if (sh.t_world < tmax) {

@@ -14,9 +14,9 @@ reports each sample), with the same counter-RNG keys on both sides:
 
 Bar per path: |gpu - ref| <= 1e-4 * max(|ref|, floor) in every channel, floor
 = 1e-3 of the mean sample radiance.  Paths above the bar are split by size:
-"rounding" (relative error up to 1e-2: CUDA's transcendental functions and the
-contracted shading arithmetic differ from glibc's in the last bits, and a path
-of up to nine vertices compounds them) and "branch flips" (above 1e-2: some
+"rounding" (relative error up to 1e-2: CUDA's transcendental functions differ
+from glibc's in the last bits, and a path of up to nine vertices compounds
+them) and "branch flips" (above 1e-2: some
 vertex of the path tree found a different primitive, at a near tie or for a
 direction a few ulps off).  Both counts are printed and bounded.
 """
