@@ -8,10 +8,11 @@ Workload: the interior scene (three 8x4x8 rooms joined by 1x2 doorways,
 Perlin-displaced panels and clutter, ~4 M triangles at the default detail,
 one 1x1 light in room 1, camera in room 3, depth 10).  A converged reference
 is accumulated in FP64 from plain renders (`--ref-spp` samples per pixel, in
-renders of 1024 samples per pixel); with `--ref-file` the FP64 sum and its
-sample count are kept in that file and every run adds `--ref-spp` more, so a
-reference of many thousand samples per pixel can be built over several runs
-(`--ref-only` stops after that).
+renders of 1024 samples per pixel); with `--ref-file` the reference's mean
+(rounded to float32 for the file: 6e-8 relative, far below the noise of any
+reference) and its sample count are kept in that file and every run adds
+`--ref-spp` more in FP64, so a reference of many thousand samples per pixel
+can be built over several runs (`--ref-only` stops after that).
 Then each renderer runs passes of `--pass-spp` samples per pixel until
 `--passes`; after every pass the running average's relMSE against the
 reference, mean over pixels and channels of (x - ref)^2 / (ref^2 + 1e-2), is
@@ -97,7 +98,8 @@ def run(width=480, height=270, detail=49, ref_spp=4096, pass_spp=4, passes=64, t
         if ref_file and os.path.exists(ref_file):
             z = np.load(ref_file)
             assert tuple(z["shape"]) == (h, w, 3) and int(z["detail"]) == detail and int(z["seed"]) == seed
-            ref_sum, ref_n, runs = z["sum"], int(z["spp"]), int(z["runs"])
+            ref_n, runs = int(z["spp"]), int(z["runs"])
+            ref_sum = z["mean"].astype(np.float64) * ref_n
         per = min(1024, max(1, ref_spp))
         cam = _camera_with_spp(scene, per)
         per = int(int(per ** 0.5) ** 2)
@@ -112,8 +114,8 @@ def run(width=480, height=270, detail=49, ref_spp=4096, pass_spp=4, passes=64, t
             t_ref += dt
         runs += 1 if ref_spp > 0 else 0
         if ref_file and ref_spp > 0:
-            np.savez(ref_file, sum=ref_sum, spp=ref_n, runs=runs, shape=np.array([h, w, 3]), detail=detail,
-                     seed=seed)
+            np.savez(ref_file, mean=(ref_sum / ref_n).astype(np.float32), spp=ref_n, runs=runs,
+                     shape=np.array([h, w, 3]), detail=detail, seed=seed)
         ref = ref_sum / ref_n
         out["reference"] = {"spp": ref_n, "gpu_s_this_run": t_ref, "runs": runs, "mean": float(ref.mean()),
                             "file": ref_file}
