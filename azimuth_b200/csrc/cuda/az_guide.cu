@@ -356,20 +356,27 @@ __global__ void __launch_bounds__(kInferWarps * 32) k_guide_infer(DevScene S, Wa
 }
 
 // ---- the same inference on the 5th-generation tensor cores (tcgen05) ----
-// One CTA of 128 threads takes 128 rows at a time, one row per thread: the
-// thread encodes its row (hash-grid gathers, normal, outgoing direction) into
-// the shared-memory A operand; one elected thread issues, per layer, four
-// tcgen05.mma (M = 128 rows, N = 64 units, K = 16 each; BF16 operands in
-// shared memory, FP32 accumulator in tensor memory) and commits them to an
-// mbarrier; every thread then reads its row of the accumulator back from
-// tensor memory (warp w holds lanes 32w..32w+31), applies the ReLU and
-// writes the next layer's A operand, or, after the output layer, decodes its
-// proposal.  Waits on the mbarrier are bounded: on a timeout the kernel sets
-// *err, stops issuing work and frees its tensor memory.
+// One CTA of 256 threads takes 128 rows at a time, two threads per row (the
+// row's two halves): each thread gathers eight of the row's sixteen hash-grid
+// levels (the half of the row that also holds the normal, direction and
+// constant writes those) straight into the shared-memory A operand; one
+// elected thread issues, per layer, four tcgen05.mma (M = 128 rows, N = 64
+// units, K = 16 each; BF16 operands in shared memory, FP32 accumulator in
+// tensor memory) and commits them to an mbarrier; every thread then reads
+// its half of its row (32 columns) back from tensor memory (warps w and
+// w + 4 share lanes 32 (w % 4) ..), applies the ReLU and writes its half of
+// the next layer's A operand, or, after the output layer, the first half
+// decodes the proposal with outputs 32..40 from the second.  Two threads per
+// row keep twice the gathers in flight per row at 64 registers a thread.
+// Waits on the mbarrier are bounded: on a timeout the kernel sets *err, stops
+// issuing work and frees its tensor memory.
 // ROWS: caller rows (GuideRow, normalised weights ignored) to raw outputs
 // (64 floats per row) instead of a level's queue entries to proposals.
 constexpr uint32_t kTcRows = 128;
-constexpr size_t kTcSmem = (size_t)kTcRows * W * 2 + (size_t)NW * 2 + W * sizeof(float) + 16;
+constexpr uint32_t kTcThreads = 256;
+constexpr int kTcHi = 9;   // outputs 32..40 handed from the second half of a row to the first
+constexpr size_t kTcSmem = (size_t)kTcRows * W * 2 + (size_t)NW * 2 + (size_t)kTcRows * kTcHi * sizeof(float) +
+                           W * sizeof(float) + 16;
 constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(W >> 3) << 17) | ((kTcRows >> 4) << 24);
 constexpr uint32_t kTcWaitLimit = 1u << 20;   // polls of an mbarrier (a layer completes in microseconds)
 
@@ -445,17 +452,40 @@ __device__ __forceinline__ void tc_store_row(unsigned char *A, uint32_t r, const
     }
 }
 
+// Chunks KC0 .. KC0 + NKC - 1 (8 columns each) of row r of the A operand from
+// x[0 .. 8 NKC), as BF16.
+template <int KC0, int NKC>
+__device__ __forceinline__ void tc_store_chunks(unsigned char *A, uint32_t r, const float *x, bool relu) {
+#pragma unroll
+    for (int c = 0; c < NKC; c++) {
+        uint4 q;
+        uint32_t *u = reinterpret_cast<uint32_t *>(&q);
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            float a = x[8 * c + 2 * j], b = x[8 * c + 2 * j + 1];
+            if (relu) {
+                a = fmaxf(a, 0.0f);
+                b = fmaxf(b, 0.0f);
+            }
+            u[j] = pack_bf16(a, b);
+        }
+        *reinterpret_cast<uint4 *>(A + tc_offset(r, 8u * (KC0 + c))) = q;
+    }
+}
+
 template <bool ROWS>
-__global__ void __launch_bounds__(kTcRows) k_guide_mlp_tc(DevScene S, WaveQueues Q, uint32_t level, GuideNetDev N,
-                                                          GuideLobes *out, const GuideRow *rows, uint32_t nrows,
-                                                          float *raw, uint32_t *err) {
+__global__ void __launch_bounds__(kTcThreads, 4) k_guide_mlp_tc(DevScene S, WaveQueues Q, uint32_t level,
+                                                                GuideNetDev N, GuideLobes *out, const GuideRow *rows,
+                                                                uint32_t nrows, float *raw, uint32_t *err) {
     extern __shared__ __align__(16) unsigned char smem[];
     unsigned char *A = smem;                                   // 128 x 64 BF16
     unsigned char *B = A + kTcRows * W * 2;                    // 4 layers x 64 x 64 BF16
-    float *s_bias = reinterpret_cast<float *>(B + NW * 2);
+    float *s_hi = reinterpret_cast<float *>(B + NW * 2);       // [128][kTcHi] outputs 32..40 for the decode
+    float *s_bias = s_hi + kTcRows * kTcHi;
     uint64_t *s_mbar = reinterpret_cast<uint64_t *>(s_bias + W);
     uint32_t *s_tmem = reinterpret_cast<uint32_t *>(s_mbar + 1);
     const uint32_t tid = threadIdx.x, warp = tid >> 5;
+    const uint32_t r = tid & (kTcRows - 1u), half = tid / kTcRows;   // row of the tile, which half of it
     {
         const uint4 *src = reinterpret_cast<const uint4 *>(N.wtc);
         uint4 *dst = reinterpret_cast<uint4 *>(B);
@@ -478,7 +508,8 @@ __global__ void __launch_bounds__(kTcRows) k_guide_mlp_tc(DevScene S, WaveQueues
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *s_tmem;
-    const uint32_t lane_addr = tmem + ((32u * warp) << 16);   // this warp's 32 lanes, column 0
+    // this warp's 32 lanes (warps w and w + 4 share lanes 32 (w % 4) ..), this half's 32 columns
+    const uint32_t lane_addr = tmem + ((32u * (warp & 3u)) << 16) + 32u * half;
     const int buf = level & 1;
     const uint32_t n = ROWS ? nrows : min(Q.counts[level], Q.cap_q);
     const uint32_t tiles = (n + kTcRows - 1) / kTcRows;
@@ -486,47 +517,53 @@ __global__ void __launch_bounds__(kTcRows) k_guide_mlp_tc(DevScene S, WaveQueues
     uint32_t phase = 0;
     bool ok = true;
     for (uint32_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
-        const uint32_t i = tile * kTcRows + tid;
-        // ---- this thread's row of network inputs ----
+        const uint32_t i = tile * kTcRows + r;
+        // ---- this row's network inputs: half 0 gathers grid levels 0..7,
+        // half 1 levels 8..15 and writes the normal, direction and constant ----
         f3 p = mk(0.0f, 0.0f, 1.0f), nr = p, wo = p;
         if (i < n) {
             if (ROWS) {
-                const GuideRow r = rows[i];
-                p = normalise_pos(N, mk(r.pos_w.x, r.pos_w.y, r.pos_w.z));
-                nr = mk(r.n.x, r.n.y, r.n.z);
-                wo = mk(r.wo.x, r.wo.y, r.wo.z);
+                const GuideRow row = rows[i];
+                p = normalise_pos(N, mk(row.pos_w.x, row.pos_w.y, row.pos_w.z));
+                nr = mk(row.n.x, row.n.y, row.n.z);
+                wo = mk(row.wo.x, row.wo.y, row.wo.z);
             } else {
                 const uint4 hh = Q.hit[i];
                 if (hh.w != 0xFFFFFFFFu) {
                     const float4 o4 = Q.o[buf][i], d4 = Q.d[buf][i];
-                    Ray r;
-                    r.o = mk(o4.x, o4.y, o4.z);
-                    r.d = mk(d4.x, d4.y, d4.z);
-                    r.time = o4.w;
+                    Ray ray;
+                    ray.o = mk(o4.x, o4.y, o4.z);
+                    ray.d = mk(d4.x, d4.y, d4.z);
+                    ray.time = o4.w;
                     Hit hit;
                     hit.t = __uint_as_float(hh.x);
                     hit.tl = __uint_as_float(hh.y);
                     hit.prim = hh.z;
                     hit.ent = hh.w;
-                    guide_query(S, r, hit, p, nr);
+                    guide_query(S, ray, hit, p, nr);
                     p = normalise_pos(N, p);
-                    wo = -r.d;
+                    wo = -ray.d;
                 }
             }
         }
-        float x[W];
+        float x[32];
 #pragma unroll
-        for (int l = 0; l < GUIDE_LEVELS; l++) {
-            const float2 f = grid_feature(N, l, p);
+        for (int l = 0; l < GUIDE_LEVELS / 2; l++) {
+            const float2 f = grid_feature(N, l + (int)half * (GUIDE_LEVELS / 2), p);
             x[2 * l] = f.x;
             x[2 * l + 1] = f.y;
         }
-        x[32] = nr.x; x[33] = nr.y; x[34] = nr.z;
-        x[35] = wo.x; x[36] = wo.y; x[37] = wo.z;
-        x[38] = 1.0f;
+        if (half == 0) {
+            tc_store_chunks<0, 2>(A, r, x, false);
+        } else {
+            tc_store_chunks<2, 2>(A, r, x, false);
+            x[0] = nr.x; x[1] = nr.y; x[2] = nr.z;
+            x[3] = wo.x; x[4] = wo.y; x[5] = wo.z;
+            x[6] = 1.0f;
 #pragma unroll
-        for (int j = 39; j < W; j++) x[j] = 0.0f;
-        tc_store_row(A, tid, x, false);
+            for (int j = 7; j < 32; j++) x[j] = 0.0f;
+            tc_store_chunks<4, 4>(A, r, x, false);
+        }
         for (int l = 0; l < GUIDE_LAYERS; l++) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // A written by this thread
             tc_fence_before();
@@ -548,23 +585,38 @@ __global__ void __launch_bounds__(kTcRows) k_guide_mlp_tc(DevScene S, WaveQueues
             }
             phase ^= 1u;
             tc_fence_after();
-#pragma unroll
-            for (int c = 0; c < 4; c++) tc_load16(lane_addr + 16u * c, x + 16 * c);
+            tc_load16(lane_addr, x);
+            tc_load16(lane_addr + 16u, x + 16);
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
             if (l + 1 < GUIDE_LAYERS) {
-                tc_store_row(A, tid, x, true);
-            } else if (i < n) {
+                if (half == 0) tc_store_chunks<0, 4>(A, r, x, true);
+                else tc_store_chunks<4, 4>(A, r, x, true);
+            } else {
 #pragma unroll
-                for (int j = 0; j < W; j++) x[j] += s_bias[j];
+                for (int j = 0; j < 32; j++) x[j] += s_bias[32 * half + j];
                 if (ROWS) {
-                    for (int j = 0; j < W; j++) raw[(size_t)i * W + j] = x[j];
+                    if (i < n)
+                        for (int j = 0; j < 32; j++) raw[(size_t)i * W + 32 * half + j] = x[j];
                 } else {
-                    GuideLobes G;
-                    decode_lobes(x, G);
-                    float4 *dst = reinterpret_cast<float4 *>(out + i);
-                    const float4 *src = reinterpret_cast<const float4 *>(&G);
+                    // the decode reads outputs 0..40: half 1 hands 32..40 to half 0
+                    if (half == 1) {
 #pragma unroll
-                    for (int j = 0; j < 13; j++) dst[j] = src[j];
+                        for (int j = 0; j < kTcHi; j++) s_hi[r * kTcHi + j] = x[j];
+                    }
+                    __syncthreads();
+                    if (half == 0 && i < n) {
+                        float o[41];
+#pragma unroll
+                        for (int j = 0; j < 32; j++) o[j] = x[j];
+#pragma unroll
+                        for (int j = 0; j < 41 - 32; j++) o[32 + j] = s_hi[r * kTcHi + j];
+                        GuideLobes G;
+                        decode_lobes(o, G);
+                        float4 *dst = reinterpret_cast<float4 *>(out + i);
+                        const float4 *src = reinterpret_cast<const float4 *>(&G);
+#pragma unroll
+                        for (int j = 0; j < 13; j++) dst[j] = src[j];
+                    }
                 }
             }
         }
@@ -1414,7 +1466,7 @@ int CreateGuide(const GpuScene &G, const az_guide_config *cfg, GuideState **out)
     // as many resident CTAs per SM as shared memory allows, at most 4: each
     // holds 64 of the SM's 512 tensor-memory columns while it runs
     int per_sm = 0;
-    AZ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_guide_mlp_tc<false>, (int)kTcRows, kTcSmem));
+    AZ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_guide_mlp_tc<false>, (int)kTcThreads, kTcSmem));
     g->tc_blocks = std::max(1, std::min(per_sm, 4));
     // network view
     g->net.wtc = g->wtc;
@@ -1471,7 +1523,7 @@ int GuidePrepareWave(GuideState &g, WaveBuffers &W, WaveQueues &Q, uint32_t cap_
 
 int GuideInfer(GuideState &g, const GpuScene &G, const WaveQueues &Q, uint32_t level, cudaStream_t st) {
     if (g.use_tc)
-        k_guide_mlp_tc<false><<<g.sms * g.tc_blocks, kTcRows, kTcSmem, st>>>(G.dev, Q, level, g.net, Q.lobes,
+        k_guide_mlp_tc<false><<<g.sms * g.tc_blocks, kTcThreads, kTcSmem, st>>>(G.dev, Q, level, g.net, Q.lobes,
                                                                              nullptr, 0, nullptr, g.tc_error);
     else
         k_guide_infer<<<g.sms * 3, kInferWarps * 32, kInferSmem, st>>>(G.dev, Q, level, g.net, Q.lobes);
@@ -1694,7 +1746,7 @@ extern "C" int az_guide_infer(az_guide *g, const float *rows, uint32_t n, float 
         WaveQueues q;
         memset(&q, 0, sizeof(q));
         k_guide_mlp_tc<true><<<std::min<uint32_t>((n + kTcRows - 1) / kTcRows, (uint32_t)(s.sms * s.tc_blocks)),
-                               kTcRows, kTcSmem>>>(
+                               kTcThreads, kTcSmem>>>(
             none, q, 0, s.net, nullptr, d_rows, n, d_out, s.tc_error);
         cudaError_t e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaDeviceSynchronize();
