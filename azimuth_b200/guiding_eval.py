@@ -17,7 +17,10 @@ Then each renderer runs passes of `--pass-spp` samples per pixel until
 `--passes`; after every pass the running average's relMSE against the
 reference, mean over pixels and channels of (x - ref)^2 / (ref^2 + 1e-2), is
 recorded with the GPU time spent so far (CUDA events; the guide's inference,
-recording and training included).  The guided renderer trains during the
+recording and training included).  Both renderers run with their buffers
+already allocated: the plain renderer's by the reference renders, the
+guided renderer's (proposals, records) by one training and one inference
+render of a throwaway guide before the timed passes.  The guided renderer trains during the
 first `--train-passes` passes and keeps every pass in its average (all are
 unbiased).  Reported: both curves and the time the guided renderer needs to
 reach the plain renderer's final relMSE, as a fraction of the plain time.
@@ -65,7 +68,7 @@ def _camera_with_spp(scene, spp):
 
 
 def run(width=480, height=270, detail=49, ref_spp=4096, pass_spp=4, passes=64, train_passes=16, seed=0,
-        log=_log, ref_file=None, ref_only=False, runs=1):
+        log=_log, ref_file=None, ref_only=False, runs=1, guide_kw=None):
     import torch
     import azimuth_b200 as az
     t0 = time.time()
@@ -94,11 +97,11 @@ def run(width=480, height=270, detail=49, ref_spp=4096, pass_spp=4, passes=64, t
         # with its own seeds; the image is the sum over the renders' sample count
         import ctypes as C
         import os
-        ref_sum, ref_n, runs = np.zeros((h, w, 3)), 0, 0
+        ref_sum, ref_n, ref_runs = np.zeros((h, w, 3)), 0, 0
         if ref_file and os.path.exists(ref_file):
             z = np.load(ref_file)
             assert tuple(z["shape"]) == (h, w, 3) and int(z["detail"]) == detail and int(z["seed"]) == seed
-            ref_n, runs = int(z["spp"]), int(z["runs"])
+            ref_n, ref_runs = int(z["spp"]), int(z["runs"])
             ref_sum = z["mean"].astype(np.float64) * ref_n
         per = min(1024, max(1, ref_spp))
         cam = _camera_with_spp(scene, per)
@@ -106,23 +109,31 @@ def run(width=480, height=270, detail=49, ref_spp=4096, pass_spp=4, passes=64, t
         t_ref = 0.0
         assert ref_spp > 0 or ref_n > 0, "--ref-spp 0 needs a reference file with samples"
         for k in range(ref_spp // per if ref_spp > 0 else 0):
-            s = 100000 + 1000 * runs + k
+            s = 100000 + 1000 * ref_runs + k
             img, dt = one(lambda: g.render_device(film.data_ptr(), camera_ptr=C.addressof(cam), seed=s,
                                                   stream=stream.cuda_stream))
             ref_sum += img * per
             ref_n += per
             t_ref += dt
-        runs += 1 if ref_spp > 0 else 0
+        ref_runs += 1 if ref_spp > 0 else 0
         if ref_file and ref_spp > 0:
-            np.savez(ref_file, mean=(ref_sum / ref_n).astype(np.float32), spp=ref_n, runs=runs,
+            np.savez(ref_file, mean=(ref_sum / ref_n).astype(np.float32), spp=ref_n, runs=ref_runs,
                      shape=np.array([h, w, 3]), detail=detail, seed=seed)
         ref = ref_sum / ref_n
-        out["reference"] = {"spp": ref_n, "gpu_s_this_run": t_ref, "runs": runs, "mean": float(ref.mean()),
+        out["reference"] = {"spp": ref_n, "gpu_s_this_run": t_ref, "runs": ref_runs, "mean": float(ref.mean()),
                             "file": ref_file}
         log("reference: %d spp (%.1f s GPU in this run)" % (ref_n, t_ref))
         if ref_only:
             return out
 
+        guide_kw = dict(guide_kw or {})
+        out["guide_config"] = guide_kw
+        # the plain renderer's wave queues were allocated by the reference renders; let the guided
+        # renderer's proposal and record buffers be allocated outside its timed passes as well
+        with az.Guide(g, seed=seed + 7777, **guide_kw) as warm:
+            one(lambda: warm.render(film.data_ptr(), train=True, seed=999999, stream=stream.cuda_stream, stats=False))
+            one(lambda: warm.render(film.data_ptr(), train=False, seed=999998, stream=stream.cuda_stream,
+                                    stats=False))
         results = []
         for rn in range(runs):
             base = 7919 * rn   # run rn's pass seeds (run 0: passes 0, 1, ...)
@@ -138,7 +149,7 @@ def run(width=480, height=270, detail=49, ref_spp=4096, pass_spp=4, passes=64, t
             curves["plain"] = curve
             # guided (trains during the first passes)
             res = {"run": rn}
-            with az.Guide(g, seed=seed + rn) as guide:
+            with az.Guide(g, seed=seed + rn, **guide_kw) as guide:
                 acc = np.zeros_like(ref)
                 t, curve = 0.0, []
                 for k in range(passes):
@@ -184,9 +195,14 @@ def main():
     ap.add_argument("--ref-file", default=None, help="npz keeping the FP64 reference sum across runs")
     ap.add_argument("--ref-only", action="store_true", help="only add --ref-spp samples to the reference")
     ap.add_argument("--runs", type=int, default=1, help="comparisons against the same reference")
+    ap.add_argument("--steps-per-wave", type=int, default=0, help="Adam steps per training wave (0: the default)")
+    ap.add_argument("--learning-rate", type=float, default=0.0)
+    ap.add_argument("--record-samples", type=int, default=0)
     a = ap.parse_args()
+    kw = {k: v for k, v in (("steps_per_wave", a.steps_per_wave), ("learning_rate", a.learning_rate),
+                            ("record_samples", a.record_samples)) if v}
     res = run(a.width, a.height, a.detail, a.ref_spp, a.pass_spp, a.passes, a.train_passes, a.seed,
-              ref_file=a.ref_file, ref_only=a.ref_only, runs=a.runs)
+              ref_file=a.ref_file, ref_only=a.ref_only, runs=a.runs, guide_kw=kw)
     print(json.dumps(res), flush=True)
 
 
