@@ -1463,8 +1463,15 @@ int CreateGuide(const GpuScene &G, const az_guide_config *cfg, GuideState **out)
     AZ_CUDA_TRY(cudaFuncSetAttribute(k_guide_mlp_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
     AZ_CUDA_TRY(
         cudaFuncSetAttribute(k_guide_train_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcTrainSmem));
-    // as many resident CTAs per SM as shared memory allows, at most 4: each
-    // holds 64 of the SM's 512 tensor-memory columns while it runs
+    // the whole unified L1/shared array as shared memory for the kernels that
+    // keep their weights there: without the preference the driver may keep the
+    // larger L1 split, and one inference CTA of 54 KB per SM fits instead of four
+    for (const void *k : {(const void *)k_guide_mlp_tc<false>, (const void *)k_guide_mlp_tc<true>,
+                          (const void *)k_guide_train_tc, (const void *)k_guide_infer, (const void *)k_guide_train})
+        AZ_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                         (int)cudaSharedmemCarveoutMaxShared));
+    // as many resident CTAs per SM as registers and shared memory allow, at
+    // most 4: each holds 64 of the SM's 512 tensor-memory columns while it runs
     int per_sm = 0;
     AZ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_guide_mlp_tc<false>, (int)kTcThreads, kTcSmem));
     g->tc_blocks = std::max(1, std::min(per_sm, 4));
