@@ -1303,7 +1303,7 @@ struct GuideState {
     float last_loss = 0.0f;
     std::vector<void *> allocs;
     int sms = 148;
-    int tc_blocks = 2;              // resident CTAs per SM of the tcgen05 inference kernel
+    int tc_blocks = 4;              // resident CTAs per SM of the tcgen05 inference kernel
     std::mutex mu;
 
     ~GuideState() {
@@ -1470,11 +1470,10 @@ int CreateGuide(const GpuScene &G, const az_guide_config *cfg, GuideState **out)
                           (const void *)k_guide_train_tc, (const void *)k_guide_infer, (const void *)k_guide_train})
         AZ_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
                                          (int)cudaSharedmemCarveoutMaxShared));
-    // as many resident CTAs per SM as registers and shared memory allow, at
-    // most 4: each holds 64 of the SM's 512 tensor-memory columns while it runs
-    int per_sm = 0;
-    AZ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_guide_mlp_tc<false>, (int)kTcThreads, kTcSmem));
-    g->tc_blocks = std::max(1, std::min(per_sm, 4));
+    // four resident inference CTAs per SM: the most that 64 registers a thread
+    // and 55 KB of shared memory a CTA allow (each holds 64 of the SM's 512
+    // tensor-memory columns while it runs); a grid of that many per SM
+    g->tc_blocks = 4;
     // network view
     g->net.wtc = g->wtc;
     g->net.wf = g->wf;
