@@ -37,7 +37,10 @@ constexpr int GUIDE_LAYERS = 4;                     // 3 hidden + output
 constexpr int GUIDE_LOBES = 8;
 constexpr int GUIDE_OUTPUTS = GUIDE_LOBES * 5 + 1;  // 41 used outputs
 constexpr float GUIDE_LOGK_MIN = -3.0f, GUIDE_LOGK_MAX = 5.0f;   // kappa in [0.05, 148]
-constexpr float GUIDE_ALPHA_MIN = 0.05f, GUIDE_ALPHA_SPAN = 0.9f;
+// alpha in [0.05, 0.8]: at least a fifth of the samples stay cosine-distributed
+// (defensive mixture), so a direction the guide misjudges gains at most 5x the
+// cosine-sampling weight at a vertex
+constexpr float GUIDE_ALPHA_MIN = 0.05f, GUIDE_ALPHA_SPAN = 0.75f;
 constexpr float GUIDE_PI = 3.14159265358979f;
 
 // Grid resolution of level l: floor(16 * b^l), b = (2048 / 16)^(1 / 15),

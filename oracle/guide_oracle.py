@@ -15,7 +15,7 @@ kernels with it:
   bias) over [grid features (32), normal (3), outgoing direction (3), 1, 0...];
 * the proposal: per lobe k a mean direction (normalised outputs 5k..5k+2),
   kappa = exp(clamp(o[5k+3], -3, 5)), mixture weight softmax(o[5k+4]);
-  alpha = 0.05 + 0.9 sigmoid(o[40]); density
+  alpha = 0.05 + 0.75 sigmoid(o[40]); density
   q(w) = alpha sum_k pi_k vMF(w; mu_k, kappa_k) + (1 - alpha) max(0, n.w) / pi;
 * the loss -w log q(wi) (the KL-divergence estimator of Mueller, McWilliams,
   Rousselle, Gross, Novak, "Neural Importance Sampling", ToG 2019) and its
@@ -35,7 +35,7 @@ T = 1 << LOG2_T
 WIDTH = 64
 LOBES = 8
 LOGK_MIN, LOGK_MAX = -3.0, 5.0
-ALPHA_MIN, ALPHA_SPAN = 0.05, 0.9
+ALPHA_MIN, ALPHA_SPAN = 0.05, 0.75
 
 
 def level_res():
