@@ -1292,7 +1292,7 @@ struct GuideState {
     void *cub_temp = nullptr;
     size_t rec_cap = 0, cub_bytes = 0;
     uint32_t n_rec = 0;             // samples per wave whose vertices are recorded
-    uint32_t steps_per_wave = 1;    // Adam steps on each wave's rows
+    uint32_t steps_per_wave = 4;    // Adam steps on each wave's rows
     GuideRow *rows = nullptr;
     uint32_t rows_cap = 0;
     uint32_t *count = nullptr;      // [0] rows, then scratch
@@ -1402,7 +1402,7 @@ int CreateGuide(const GpuScene &G, const az_guide_config *cfg, GuideState **out)
     cudaDeviceGetAttribute(&g->sms, cudaDevAttrMultiProcessorCount, G.device);
     g->lr = cfg && cfg->learning_rate > 0.0f ? cfg->learning_rate : 1e-2f;
     g->n_rec = cfg && cfg->record_samples ? cfg->record_samples : (1u << 17);
-    g->steps_per_wave = cfg && cfg->steps_per_wave ? cfg->steps_per_wave : 1u;
+    g->steps_per_wave = cfg && cfg->steps_per_wave ? cfg->steps_per_wave : 4u;
     g->rows_cap = cfg && cfg->train_batch ? cfg->train_batch : (1u << 18);
     g->use_tc = !(cfg && cfg->kernels == AZ_GUIDE_MMA_SYNC);
     const uint64_t seed = cfg ? cfg->seed : 0;

@@ -380,14 +380,14 @@ int az_gpu_render_tiles(az_job *jobs, uint32_t n, const az_batch_opts *opts, az_
  * MLP of position, normal and outgoing direction) and cosine sampling, with a
  * learned selection probability; the mixture density weights the sample, so
  * the estimate stays unbiased.  With `train` set, every wave also trains the
- * network (one Adam step) on the radiance its own paths brought back. */
+ * network (four Adam steps by default) on the radiance its own paths brought back. */
 typedef struct az_guide az_guide;
 
 typedef struct az_guide_config {
     float learning_rate;            /* Adam step size; 0 = 1e-2 */
     uint32_t train_batch;           /* training rows per step at most; 0 = 2^18 */
     uint32_t record_samples;        /* camera samples per wave whose vertices are recorded; 0 = 2^17 */
-    uint32_t steps_per_wave;        /* Adam steps on each wave's rows when training; 0 = 1 */
+    uint32_t steps_per_wave;        /* Adam steps on each wave's rows when training; 0 = 4 */
     uint64_t seed;                  /* weight initialisation */
     uint32_t kernels;               /* network kernels (proposals and training): AZ_GUIDE_TCGEN05 (0, the
                                        default) runs the MLP on the 5th-generation tensor cores
