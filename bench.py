@@ -46,8 +46,8 @@ SCENE_ARGS = dict(scene_id=1, seed=0)
 DRAM_BYTES_PER_QUERY = {"k_extend": 207.1, "k_shadow": 246.2}
 PROFILE_NOTE = "profiles/traversal_dram_dense_mesh_256x256_16spp.md, profiles/k_extend_k_shadow_dense_mesh_256x256_16spp.md"
 # issue statistics of the two traversal kernels from the ncu capture of that small case
-ISSUE = {"k_extend": {"threads_per_warp_instruction": 8.49, "issue_active_pct": 60.0, "warps_active_pct": 36.4},
-         "k_shadow": {"threads_per_warp_instruction": 8.40, "issue_active_pct": 51.8, "warps_active_pct": 35.0}}
+ISSUE = {"k_extend": {"threads_per_warp_instruction": 8.63, "issue_active_pct": 57.1, "warps_active_pct": 36.2},
+         "k_shadow": {"threads_per_warp_instruction": 8.47, "issue_active_pct": 56.2, "warps_active_pct": 34.3}}
 
 
 def parse():
