@@ -1597,11 +1597,6 @@ int GuideCheck(GuideState &g, cudaStream_t st) {
     return SetError(AZ_ERR_CUDA, "tensor-core proposals: a wait on the MMA gave up");
 }
 std::mutex &GuideLock(GuideState &g) { return g.mu; }
-float GuideAlphaCap(const GuideState &g, bool train) {
-    if (!train) return 1.0f;
-    constexpr float kRampSteps = 32.0f;   // one training pass of a 1080p, 4-spp frame at four steps a wave
-    return 0.5f * std::min(1.0f, (float)g.step / kRampSteps);
-}
 }  // namespace az
 
 extern "C" int az_guide_create(az_gpu_scene *scene, const az_guide_config *cfg, az_guide **out) {

@@ -132,9 +132,6 @@ int GuideTrainWave(GuideState &g, const WaveQueues &Q, cudaStream_t st);
 GuideState *GuideOf(az_guide *g);
 // AZ_ERR_CUDA if a tensor-core wait of the proposal kernel gave up since the last check (the flag is cleared).
 int GuideCheck(GuideState &g, cudaStream_t st);
-// Largest chance of sampling the guide in a wave: the learned value when not
-// training; while training one half, reached linearly over the first 32 Adam steps.
-float GuideAlphaCap(const GuideState &g, bool train);
 // Serialises the renders that use one guide (its proposal and record buffers).
 std::mutex &GuideLock(GuideState &g);
 

@@ -817,11 +817,10 @@ static int RenderWave(const GpuScene &G, const CameraParams &cam, WaveBuffers &W
     if (cam.order & kOrderExtend) Q.eorder = W.oidx_e;
     if (cam.order & kOrderShadow) Q.sorder = W.oidx_s;
     // While the guide trains, its early proposals can be far from the light
-    // field; capping the chance of sampling them (at most one half, rising from
-    // zero over the first Adam steps, GuideAlphaCap) keeps every sample's
-    // weight within twice cosine sampling's (the estimate stays unbiased for
-    // any cap).  Inference-only renders use the learned value.
-    Q.guide_alpha_max = guide ? GuideAlphaCap(*guide, train) : 1.0f;
+    // field; capping the chance of sampling them at one half keeps every
+    // sample's weight within twice cosine sampling's (the estimate stays
+    // unbiased for any cap).  Inference-only renders use the learned value.
+    Q.guide_alpha_max = train ? 0.5f : 1.0f;
     const uint32_t levels = std::min<uint32_t>(D.max_depth + 1, AZ_MAX_LEVELS - 2);
     if (guide) {
         // proposals for every queue entry this wave can hold (the queue is capped to match)
