@@ -322,11 +322,13 @@ class Guide:
     TABLE = 1 << 19
 
     def __init__(self, gpu_scene, seed=0, learning_rate=0.0, train_batch=0, record_samples=0, steps_per_wave=0,
-                 kernels=0):
-        """kernels: GUIDE_TCGEN05 (default) or GUIDE_MMA_SYNC, the network kernels (proposals and training)."""
+                 kernels=0, queue_order_rows=False):
+        """kernels: GUIDE_TCGEN05 (default) or GUIDE_MMA_SYNC, the network kernels (proposals and training);
+        queue_order_rows: the tcgen05 proposals visit rows in queue order instead of spatial order."""
         self.gs = gpu_scene
         cfg = GuideConfig()
         cfg.kernels = kernels
+        cfg.queue_order_rows = 1 if queue_order_rows else 0
         cfg.learning_rate = learning_rate
         cfg.train_batch = train_batch
         cfg.record_samples = record_samples

@@ -75,7 +75,7 @@ class BatchStats(C.Structure):
 class GuideConfig(C.Structure):
     _fields_ = [("learning_rate", C.c_float), ("train_batch", C.c_uint32), ("record_samples", C.c_uint32),
                 ("steps_per_wave", C.c_uint32), ("seed", C.c_uint64), ("kernels", C.c_uint32),
-                ("reserved", C.c_uint32 * 5)]
+                ("queue_order_rows", C.c_uint32), ("reserved", C.c_uint32 * 4)]
 
 
 class RenderStats(C.Structure):

@@ -476,7 +476,8 @@ __device__ __forceinline__ void tc_store_chunks(unsigned char *A, uint32_t r, co
 template <bool ROWS>
 __global__ void __launch_bounds__(kTcThreads, 4) k_guide_mlp_tc(DevScene S, WaveQueues Q, uint32_t level,
                                                                 GuideNetDev N, GuideLobes *out, const GuideRow *rows,
-                                                                uint32_t nrows, float *raw, uint32_t *err) {
+                                                                uint32_t nrows, float *raw, uint32_t *err,
+                                                                const uint32_t *order = nullptr) {
     extern __shared__ __align__(16) unsigned char smem[];
     unsigned char *A = smem;                                   // 128 x 64 BF16
     unsigned char *B = A + kTcRows * W * 2;                    // 4 layers x 64 x 64 BF16
@@ -517,7 +518,9 @@ __global__ void __launch_bounds__(kTcThreads, 4) k_guide_mlp_tc(DevScene S, Wave
     uint32_t phase = 0;
     bool ok = true;
     for (uint32_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
-        const uint32_t i = tile * kTcRows + r;
+        // the tile's rows: queue entries in order, or in the spatial order of `order`
+        const uint32_t k = tile * kTcRows + r;
+        const uint32_t i = order && k < n ? order[k] : k;
         // ---- this row's network inputs: half 0 gathers grid levels 0..7,
         // half 1 levels 8..15 and writes the normal, direction and constant ----
         f3 p = mk(0.0f, 0.0f, 1.0f), nr = p, wo = p;
@@ -1304,12 +1307,19 @@ struct GuideState {
     std::vector<void *> allocs;
     int sms = 148;
     int tc_blocks = 4;              // resident CTAs per SM of the tcgen05 inference kernel
+    bool order_rows = true;         // tcgen05 inference visits a level's rows in spatial order
+    uint32_t *row_keys = nullptr, *row_order = nullptr;   // [row_cap] (OrderRows)
+    uint32_t row_cap = 0;
+    uint32_t *bin_counts = nullptr, *bin_offsets = nullptr;
+    unsigned char *bin_scan_temp = nullptr;
+    size_t bin_scan_bytes = 0;
     std::mutex mu;
 
     ~GuideState() {
         for (void *p : allocs)
             if (p) cudaFree(p);
-        for (void *p : {(void *)rec_weight, (void *)rec_flag, (void *)rec_pos, cub_temp})
+        for (void *p : {(void *)rec_weight, (void *)rec_flag, (void *)rec_pos, cub_temp, (void *)row_keys,
+                        (void *)row_order})
             if (p) cudaFree(p);
     }
     template <typename T>
@@ -1405,6 +1415,7 @@ int CreateGuide(const GpuScene &G, const az_guide_config *cfg, GuideState **out)
     g->steps_per_wave = cfg && cfg->steps_per_wave ? cfg->steps_per_wave : 4u;
     g->rows_cap = cfg && cfg->train_batch ? cfg->train_batch : (1u << 18);
     g->use_tc = !(cfg && cfg->kernels == AZ_GUIDE_MMA_SYNC);
+    g->order_rows = !(cfg && cfg->queue_order_rows);
     const uint64_t seed = cfg ? cfg->seed : 0;
     g->w = g->Alloc<float>(NW);
     g->w_grad = g->Alloc<float>(NW);
@@ -1527,12 +1538,108 @@ int GuidePrepareWave(GuideState &g, WaveBuffers &W, WaveQueues &Q, uint32_t cap_
     return AZ_OK;
 }
 
+// ---- spatial order of a level's inference rows ----
+// Neighbouring rows of a tile gather the same coarse hash-grid cells when
+// their hit points are close, and those gathers then hit in L1.  A level's
+// queue entries are bucketed by the 12-bit Morton code of the cell of their
+// hit point (o + t d) in a 16^3 grid over the guide's box (misses in bucket
+// 0): a histogram, an exclusive scan, a scatter with warp-aggregated
+// atomics.  Rows within a bucket keep no particular order; the proposals do
+// not depend on the order in which rows are evaluated.
+constexpr uint32_t kSortBins = 4096;
+
+__device__ __forceinline__ uint32_t spread4(uint32_t v) {   // bits b3..b0 to b9, b6, b3, b0
+    return (v & 1u) | ((v & 2u) << 2) | ((v & 4u) << 4) | ((v & 8u) << 6);
+}
+
+__device__ __forceinline__ uint32_t row_bin(const WaveQueues &Q, int buf, uint32_t i, const GuideNetDev &N) {
+    const uint4 hh = Q.hit[i];
+    if (hh.w == 0xFFFFFFFFu) return 0u;
+    const float4 o = Q.o[buf][i], d = Q.d[buf][i];
+    const float t = __uint_as_float(hh.x);
+    const f3 p = normalise_pos(N, mk(o.x + t * d.x, o.y + t * d.y, o.z + t * d.z));
+    const uint32_t x = min((uint32_t)(p.x * 16.0f), 15u), y = min((uint32_t)(p.y * 16.0f), 15u),
+                   z = min((uint32_t)(p.z * 16.0f), 15u);
+    return (spread4(x) << 2) | (spread4(y) << 1) | spread4(z);
+}
+
+// PASS 0: count rows per bin (keys kept); PASS 1: place every row at its bin's
+// next slot.  Loop bounds are warp-uniform so that lanes with equal keys can
+// share one atomic.
+template <int PASS>
+__global__ void k_guide_bins(WaveQueues Q, uint32_t level, GuideNetDev N, uint32_t *keys, uint32_t *bins,
+                             uint32_t *order) {
+    const uint32_t n = min(Q.counts[level], Q.cap_q);
+    const int buf = level & 1;
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t b = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); b < n; b += gridDim.x * blockDim.x) {
+        const uint32_t i = b + lane;
+        const bool live = i < n;
+        uint32_t key = 0xFFFFFFFFu;
+        if (live) {
+            if (PASS == 0) {
+                key = row_bin(Q, buf, i, N);
+                keys[i] = key;
+            } else {
+                key = keys[i];
+            }
+        }
+        const uint32_t peers = __match_any_sync(0xFFFFFFFFu, key);
+        const uint32_t leader = __ffs(peers) - 1u;
+        uint32_t base = 0;
+        if (live && lane == leader) base = atomicAdd(&bins[key], (uint32_t)__popc(peers));
+        if (PASS == 1) {
+            base = __shfl_sync(0xFFFFFFFFu, base, leader);
+            if (live) order[base + __popc(peers & ((1u << lane) - 1u))] = i;
+        }
+    }
+}
+
+static int OrderRows(GuideState &g, const WaveQueues &Q, uint32_t level, cudaStream_t st);
+
 int GuideInfer(GuideState &g, const GpuScene &G, const WaveQueues &Q, uint32_t level, cudaStream_t st) {
-    if (g.use_tc)
+    if (g.use_tc) {
+        const uint32_t *order = nullptr;
+        if (g.order_rows) {
+            int rc = OrderRows(g, Q, level, st);
+            if (rc != AZ_OK) return rc;
+            order = g.row_order;
+        }
         k_guide_mlp_tc<false><<<g.sms * g.tc_blocks, kTcThreads, kTcSmem, st>>>(G.dev, Q, level, g.net, Q.lobes,
-                                                                             nullptr, 0, nullptr, g.tc_error);
-    else
+                                                                             nullptr, 0, nullptr, g.tc_error, order);
+    } else
         k_guide_infer<<<g.sms * 3, kInferWarps * 32, kInferSmem, st>>>(G.dev, Q, level, g.net, Q.lobes);
+    AZ_CUDA_TRY(cudaGetLastError());
+    return AZ_OK;
+}
+
+static int OrderRows(GuideState &g, const WaveQueues &Q, uint32_t level, cudaStream_t st) {
+    if (g.row_cap < Q.cap_q) {
+        for (void **p : {(void **)&g.row_keys, (void **)&g.row_order}) {
+            if (*p) cudaFree(*p);
+            *p = nullptr;
+        }
+        g.row_cap = 0;
+        if (cudaMalloc((void **)&g.row_keys, (size_t)Q.cap_q * sizeof(uint32_t)) != cudaSuccess ||
+            cudaMalloc((void **)&g.row_order, (size_t)Q.cap_q * sizeof(uint32_t)) != cudaSuccess)
+            return SetError(AZ_ERR_OUT_OF_MEMORY, "path guide row order");
+        g.row_cap = Q.cap_q;
+    }
+    if (!g.bin_counts) {
+        size_t bytes = 0;
+        AZ_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, bytes, g.bin_counts, g.bin_offsets, (int)kSortBins));
+        g.bin_scan_bytes = bytes;
+        g.bin_counts = g.Alloc<uint32_t>(kSortBins);
+        g.bin_offsets = g.Alloc<uint32_t>(kSortBins);
+        g.bin_scan_temp = g.Alloc<unsigned char>(std::max<size_t>(bytes, 16));
+        if (!g.bin_counts || !g.bin_offsets || !g.bin_scan_temp) return SetError(AZ_ERR_OUT_OF_MEMORY, "row bins");
+    }
+    AZ_CUDA_TRY(cudaMemsetAsync(g.bin_counts, 0, kSortBins * sizeof(uint32_t), st));
+    const int grid = g.sms * 8;
+    k_guide_bins<0><<<grid, 256, 0, st>>>(Q, level, g.net, g.row_keys, g.bin_counts, nullptr);
+    size_t bytes = g.bin_scan_bytes;
+    AZ_CUDA_TRY(cub::DeviceScan::ExclusiveSum(g.bin_scan_temp, bytes, g.bin_counts, g.bin_offsets, (int)kSortBins, st));
+    k_guide_bins<1><<<grid, 256, 0, st>>>(Q, level, g.net, g.row_keys, g.bin_offsets, g.row_order);
     AZ_CUDA_TRY(cudaGetLastError());
     return AZ_OK;
 }

@@ -394,7 +394,10 @@ typedef struct az_guide_config {
                                        (tcgen05.mma, operands in shared memory, accumulators in tensor
                                        memory, 128 rows per CTA); AZ_GUIDE_MMA_SYNC runs it warp by warp
                                        with mma.sync (16 rows per warp) */
-    uint32_t reserved[5];
+    uint32_t queue_order_rows;      /* 1: the tcgen05 proposals visit a level's rows in queue order; 0 (the
+                                       default): bucketed by the cell of their hit point first, so a
+                                       tile's hash-grid gathers share cells */
+    uint32_t reserved[4];
 } az_guide_config;
 
 enum { AZ_GUIDE_TCGEN05 = 0, AZ_GUIDE_MMA_SYNC = 1 };
